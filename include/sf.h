@@ -1,0 +1,174 @@
+/*
+ * sf.h — C ABI of the B200 (sm_100a) Shatterforge physics path.
+ *
+ * The reference engine is a wasm32 Rust module driven through a handful of `extern "C"` exports on one static
+ * world (src/lib.rs:3613-4057). This header is the drop-in boundary for its two hot-path entry points:
+ *
+ *   sf_world_step        replaces `pub extern "C" fn step(dt: f32)`               src/lib.rs:3639-3651
+ *                        (the rigid part: two substeps of update_cache, build_hash, gen_contacts, prep_contacts,
+ *                        the impulse iterations, pinch clamps, integrate — src/lib.rs:1769-1783)
+ *   sf_structure_solve   replaces the load-path sweeps of `structural(w, dt)` and `warm_step(w)`
+ *                        (sor_struct / sor_brick, src/lib.rs:1005-1079, 1268-1281)
+ *   sf_structure_check   replaces the joint pass of `structural` (stress_brick, src/lib.rs:1153-1227, 1323-1339)
+ *
+ * and for the read-outs the reference hands out as raw pointers (`ptr_stats`, `ptr_structs`, … src/lib.rs:4026-4057)
+ * it offers copy-out readers into caller buffers. Plain pointers and sizes only; every call returns an sf_status
+ * and never aborts. A world handle is not thread-safe; distinct handles are.
+ *
+ * Units and frames follow the reference: metres, seconds, kilograms; the lattice is 640 x 136 x 640 cells of
+ * 0.5 m whose cell (x, y, z) has its centre at ((x - 320) * 0.5 + 0.25, y * 0.5 + 0.25, (z - 320) * 0.5 + 0.25)
+ * (src/lib.rs:113-120, 355-357). Quaternions are (x, y, z, w).
+ */
+#ifndef SHATTERFORGE_SF_H
+#define SHATTERFORGE_SF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t sf_status;
+#define SF_OK 0
+#define SF_ERR_ARG 1        /* bad argument: null pointer, out-of-lattice brick, duplicate cell, unknown id */
+#define SF_ERR_CAPACITY 2   /* a device capacity was exceeded (contacts, colours); counts are in sf_stats */
+#define SF_ERR_CUDA 3       /* a CUDA call failed (no device, out of memory, launch failure) */
+#define SF_ERR_TIMEOUT 4    /* a bounded device wait (grid barrier) gave up; the context stays usable */
+#define SF_ERR_BUDGET 5     /* the serving memory budget cannot hold the request */
+#define SF_ERR_STATE 6      /* call out of order (e.g. reading contacts before any step) */
+#define SF_ERR_VERIFY 7     /* a device self-check failed (improper colouring, island invariant) */
+
+/* solve and sleep switches */
+#define SF_SLEEP_BODY 0     /* per-body rest timer, src/lib.rs:1720-1734 (the reference's rule) */
+#define SF_SLEEP_ISLAND 1   /* island rule of gpu/gpu_world.js:1660-1668 over the same timers */
+
+typedef struct sf_world sf_world;
+
+/* One independent world (scene). Static bricks sit on lattice cells; body bricks are given in local lattice
+ * coordinates and turned into a compound body by setup_body (src/lib.rs:844-891) about the parent pose. */
+typedef struct sf_scene_desc {
+    uint32_t n_static;
+    const int32_t *static_xyz;      /* 3 per brick: lattice x (0..639), y (0..135), z (0..639) */
+    const uint8_t *static_mat;      /* material 1..8 (src/lib.rs:163-164) */
+    const int32_t *static_sid;      /* structure id >= 0, or -1 for loose static geometry */
+    const uint8_t *static_infill;   /* 1 = infill (non-bearing); glass is always infill (src/lib.rs:632) */
+    uint32_t n_bodies;
+    const uint32_t *body_first;     /* n_bodies + 1 prefix offsets into the body-brick arrays */
+    const int32_t *body_brick_xyz;  /* 3 per body brick: local lattice cell */
+    const uint8_t *body_brick_mat;
+    const float *body_pose;         /* 13 per body: parent position 3, quaternion 4, velocity 3, spin 3 */
+} sf_scene_desc;
+
+typedef struct sf_world_desc {
+    uint32_t n_scenes;
+    const sf_scene_desc *scenes;
+    int32_t structure_offset_per_scene; /* 0: structure ids are world-global as given */
+} sf_world_desc;
+
+typedef struct sf_params {
+    uint32_t substeps;          /* substeps per step (reference: 2, src/lib.rs:3650) */
+    uint32_t iterations;        /* impulse iterations per substep (reference: 10, src/lib.rs:1779) */
+    uint32_t sleep_mode;        /* SF_SLEEP_BODY or SF_SLEEP_ISLAND */
+    uint32_t pinch_kill;        /* 1: small pinched bodies are removed as the reference does (src/lib.rs:1755) */
+    uint32_t max_colors;        /* manifold colour limit, <= 128 */
+    uint32_t contact_capacity;  /* 0 = automatic (grows between steps) */
+    uint32_t verify;            /* 1: check the colouring is proper every substep (SF_ERR_VERIFY on failure) */
+    uint32_t solve_blocks;      /* persistent-kernel blocks per SM for the solve (0 = autotuned) */
+    uint32_t reserved[8];
+} sf_params;
+
+typedef struct sf_stats {
+    uint64_t contacts;          /* last substep */
+    uint64_t manifolds;
+    uint64_t ref_would_drop;    /* contacts past the reference's MAXC = 30000 (src/lib.rs:1397), per scene summed */
+    uint32_t colors;            /* colours used by the last substep's manifold colouring */
+    uint32_t color_rounds;      /* Jones-Plassmann rounds */
+    uint32_t islands;           /* islands of awake bodies (last substep) */
+    uint32_t alive, awake;      /* bodies after the last step */
+    uint32_t error_word;        /* device error bits (0 = none) */
+    uint64_t contact_capacity;
+    double ms_last_step;        /* device time of the last sf_world_step call (CUDA events) */
+} sf_stats;
+
+typedef struct sf_solve_report {
+    uint32_t structures;        /* structures solved */
+    uint32_t max_sweeps_done;   /* the most sweeps any structure took */
+    uint64_t brick_sweeps;      /* sum over structures of bricks x sweeps */
+    double max_residual;        /* the largest final residual (reference measure: max|dphi| / max(phi, 1)) */
+    double ms;                  /* device time of the solve (CUDA events) */
+} sf_solve_report;
+
+typedef struct sf_check_report {
+    uint64_t joints;            /* joints evaluated */
+    uint64_t over;              /* joints with ratio > 1 */
+    uint64_t failed;            /* bond failures (tension / shear) */
+    uint64_t crushed;           /* compressive crushes (a brick removed) */
+    float max_ratio;
+    double ms;
+} sf_check_report;
+
+/* ---- lifecycle */
+void sf_params_default(sf_params *p);
+sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf_world **out);
+void sf_world_destroy(sf_world *w);
+const char *sf_status_string(sf_status s);
+const char *sf_last_error(void);
+int32_t sf_version(void);
+
+/* ---- hot path */
+/* nsteps world steps of dt each (dt clamped to [0, 1/30] as src/lib.rs:3642 does), all scenes at once. */
+sf_status sf_world_step(sf_world *w, float dt, uint32_t nsteps);
+/* Load-path solve of one structure (>= 0) or of every structure (-1): red-black SOR with relaxation omega until
+ * the reference's residual max|dphi| / max(phi, 1) < tol or max_sweeps. */
+sf_status sf_structure_solve(sf_world *w, int32_t structure, float omega, float tol, uint32_t max_sweeps,
+                             sf_solve_report *report);
+/* Joint checks of one structure (or -1 = all) on the current potentials; live != 0 applies fatigue, failures and
+ * crushes as stress_brick does. */
+sf_status sf_structure_check(sf_world *w, int32_t structure, float dt, int32_t live, sf_check_report *report);
+/* Per-structure sweeps and final residuals of the last sf_structure_solve (n_structures entries each). */
+sf_status sf_read_solve_detail(sf_world *w, uint32_t *sweeps, double *resid);
+
+/* ---- read-outs (copy into caller buffers; body and brick order is world-global, scene-major) */
+typedef struct sf_world_info {
+    uint32_t n_scenes, n_static, n_bodies, n_body_bricks, n_structures, n_chunks;
+} sf_world_info;
+sf_status sf_world_get_info(const sf_world *w, sf_world_info *info);
+sf_status sf_get_stats(const sf_world *w, sf_stats *stats);
+/* 13 floats per body (pos 3, quat 4, v 3, spin 3); sleep timer; flags bit0 alive, bit1 asleep */
+sf_status sf_read_bodies(sf_world *w, float *state13, float *sleep, uint8_t *flags);
+sf_status sf_write_bodies(sf_world *w, const float *state13, const float *sleep, const uint8_t *flags);
+/* per body: mass, 1/mass, radius, local inverse inertia 9; per body brick: local offset 3 */
+sf_status sf_read_body_setup(sf_world *w, float *body12, float *local3);
+sf_status sf_read_brick_positions(sf_world *w, float *wpos3);
+/* contacts of one scene in the reference's list order (last substep): ids 5 (a, b, bo, ba, bb; scene-local body
+ * ids, 0xFFFFFFFF = static, scene-local combined brick ids: static k, body brick n_static + k), f 7 (p 3, n 3,
+ * depth), s 8 (jn, jt1, jt2, mn, mt1, mt2, bias, vn0). *n receives the count; buffers may be NULL to query it. */
+sf_status sf_read_contacts(sf_world *w, uint32_t scene, uint32_t *ids5, float *f7, float *s8, uint64_t cap,
+                           uint64_t *n);
+/* manifolds of one scene in (a, b) order: a, b, colour, contact count */
+sf_status sf_read_manifolds(sf_world *w, uint32_t scene, uint32_t *out4, uint64_t cap, uint64_t *n);
+/* island label per body (world-global id of the island's smallest body; 0xFFFFFFFF = not awake) */
+sf_status sf_read_islands(sf_world *w, uint32_t *label);
+sf_status sf_read_phi(sf_world *w, float *phi);
+/* the solver's f64 potentials (sf_read_phi returns them rounded to f32, the reference's type) */
+sf_status sf_read_phi64(sf_world *w, double *phi);
+sf_status sf_write_phi(sf_world *w, const float *phi);
+sf_status sf_write_ext(sf_world *w, const float *ext);
+sf_status sf_read_ext(sf_world *w, float *ext);
+/* per static brick: bond 4 (+x, +y, +z, foundation), neighbour 6 (static brick id or 0xFFFFFFFF), material */
+sf_status sf_read_bonds(sf_world *w, float *bond4, uint32_t *nb6, uint8_t *mat);
+/* joints of the last sf_structure_check, 4 per static brick (+x, +y, +z, foundation): ratio, bond after, and the
+ * decision (0 hold, 1 fatigue, 2 fail, 3 crush, 255 absent) with the crushed brick id for crushes */
+sf_status sf_read_joints(sf_world *w, float *ratio4, float *bond4, uint8_t *decision4, uint32_t *crushed4);
+
+/* ---- narrow phase entry points (batched) */
+/* Box-box SAT with face clipping and edge-edge, reduced to 4 points (engine/src/phys.rs:502-628). Boxes are
+ * 10 floats: centre 3, quaternion 4, half extents 3. out per pair: count, normal 3, 4 x (point 3, separation). */
+sf_status sf_collide_boxes(const float *boxes_a, const float *boxes_b, uint32_t n_pairs, float margin,
+                           float *out20, int32_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,207 @@
+"""ORACLE — test infrastructure only (tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg).
+
+ctypes face of oracle/sf_oracle.cpp, the CPU restatement of the reference's hot path. The product library never
+imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "libsf_oracle.so"
+
+ORDER_LIST, ORDER_COLOR = 0, 1
+SLEEP_BODY, SLEEP_ISLAND = 0, 1
+MODE_LEX_F32, MODE_LEX_F64, MODE_REDBLACK_F32, MODE_REDBLACK_F64 = 0, 1, 2, 3
+
+_u8p = C.POINTER(C.c_uint8)
+_u32p = C.POINTER(C.c_uint32)
+_i32p = C.POINTER(C.c_int32)
+_f32p = C.POINTER(C.c_float)
+_f64p = C.POINTER(C.c_double)
+_u64p = C.POINTER(C.c_uint64)
+
+
+class StepParams(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("substeps", C.c_uint32), ("order", C.c_uint32), ("sleep_mode", C.c_uint32),
+                ("pinch_kill", C.c_uint32)]
+
+
+_lib = None
+
+
+def build() -> Path:
+    src = HERE / "sf_oracle.cpp"
+    if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB.exists():
+        build()
+    lib = C.CDLL(str(LIB))
+    lib.ow_create.restype = C.c_void_p
+    lib.ow_create.argtypes = [C.c_uint32, _i32p, _u8p, _i32p, _u8p, C.c_uint32, _u32p, _i32p, _u8p, _f32p]
+    lib.ow_destroy.argtypes = [C.c_void_p]
+    lib.ow_counts.argtypes = [C.c_void_p, _u64p]
+    lib.ow_get_bodies.argtypes = [C.c_void_p, _f32p, _f32p, _u8p]
+    lib.ow_set_bodies.argtypes = [C.c_void_p, _f32p, _f32p, _u8p]
+    lib.ow_get_setup.argtypes = [C.c_void_p, _f32p, _f32p]
+    lib.ow_get_wpos.argtypes = [C.c_void_p, _f32p]
+    lib.ow_get_bonds.argtypes = [C.c_void_p, _f32p, _u32p]
+    lib.ow_step.argtypes = [C.c_void_p, C.c_float, C.POINTER(StepParams)]
+    lib.ow_contacts_only.argtypes = [C.c_void_p, C.c_float, C.c_int]
+    lib.ow_get_contacts.restype = C.c_uint64
+    lib.ow_get_contacts.argtypes = [C.c_void_p, _u32p, _f32p, _f32p]
+    lib.ow_get_islands.argtypes = [C.c_void_p, _u32p]
+    lib.ow_get_manifolds.restype = C.c_uint64
+    lib.ow_get_manifolds.argtypes = [C.c_void_p, _u32p]
+    lib.ow_sor.restype = C.c_double
+    lib.ow_sor.argtypes = [C.c_void_p, C.c_int32, C.c_float, C.c_double, C.c_uint32, C.c_int32, _u32p]
+    lib.ow_get_phi.argtypes = [C.c_void_p, _f32p]
+    lib.ow_get_phi64.argtypes = [C.c_void_p, _f64p]
+    lib.ow_set_phi.argtypes = [C.c_void_p, _f32p]
+    lib.ow_set_ext.argtypes = [C.c_void_p, _f32p]
+    lib.ow_stress.restype = C.c_uint64
+    lib.ow_stress.argtypes = [C.c_void_p, C.c_int32, C.c_float, C.c_int32, C.c_uint64, _u32p, _f32p, _f32p]
+    lib.ow_remove_static.argtypes = [C.c_void_p, C.c_uint32]
+    lib.ow_collide_boxes.restype = C.c_int32
+    lib.ow_collide_boxes.argtypes = [_f32p, _f32p, C.c_float, C.c_int32, _f32p]
+    _lib = lib
+    return lib
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+class OracleWorld:
+    """One scene in the CPU restatement."""
+
+    def __init__(self, scene):
+        self.lib = load()
+        s = scene.contiguous()
+        self.scene = s
+        self.h = self.lib.ow_create(s.n_static, _p(s.static_xyz, C.c_int32), _p(s.static_mat, C.c_uint8),
+                                    _p(s.static_sid, C.c_int32), _p(s.static_infill, C.c_uint8), s.n_bodies,
+                                    _p(s.body_first, C.c_uint32), _p(s.body_brick_xyz, C.c_int32),
+                                    _p(s.body_brick_mat, C.c_uint8), _p(s.body_pose, C.c_float))
+        if not self.h:
+            raise ValueError("oracle rejected the scene")
+        self.ns, self.nd, self.nb = s.n_static, s.n_body_bricks, s.n_bodies
+
+    def close(self):
+        if self.h:
+            self.lib.ow_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def counts(self):
+        out = np.zeros(9, np.uint64)
+        self.lib.ow_counts(self.h, _p(out, C.c_uint64))
+        keys = ["n_static", "n_body_bricks", "n_bodies", "contacts", "manifolds", "colors", "would_drop", "frame", "chunks"]
+        return dict(zip(keys, (int(x) for x in out)))
+
+    def bodies(self):
+        st = np.zeros((self.nb, 13), np.float32)
+        sl = np.zeros(self.nb, np.float32)
+        fl = np.zeros(self.nb, np.uint8)
+        self.lib.ow_get_bodies(self.h, _p(st, C.c_float), _p(sl, C.c_float), _p(fl, C.c_uint8))
+        return st, sl, fl
+
+    def set_bodies(self, st, sl, fl):
+        st = np.ascontiguousarray(st, np.float32); sl = np.ascontiguousarray(sl, np.float32); fl = np.ascontiguousarray(fl, np.uint8)
+        self.lib.ow_set_bodies(self.h, _p(st, C.c_float), _p(sl, C.c_float), _p(fl, C.c_uint8))
+
+    def setup(self):
+        b12 = np.zeros((self.nb, 12), np.float32)
+        l3 = np.zeros((self.nd, 3), np.float32)
+        self.lib.ow_get_setup(self.h, _p(b12, C.c_float), _p(l3, C.c_float))
+        return b12, l3
+
+    def brick_positions(self):
+        p = np.zeros((self.nd, 3), np.float32)
+        self.lib.ow_get_wpos(self.h, _p(p, C.c_float))
+        return p
+
+    def bonds(self):
+        b = np.zeros((self.ns, 4), np.float32)
+        nb = np.zeros((self.ns, 6), np.uint32)
+        self.lib.ow_get_bonds(self.h, _p(b, C.c_float), _p(nb, C.c_uint32))
+        return b, nb
+
+    def step(self, dt=1.0 / 60.0, iterations=10, substeps=2, order=ORDER_COLOR, sleep_mode=SLEEP_BODY, pinch_kill=1):
+        p = StepParams(iterations, substeps, order, sleep_mode, pinch_kill)
+        self.lib.ow_step(self.h, float(dt), C.byref(p))
+
+    def contacts(self):
+        n = self.counts()["contacts"]
+        ids = np.zeros((n, 5), np.uint32)
+        f = np.zeros((n, 7), np.float32)
+        s = np.zeros((n, 8), np.float32)
+        self.lib.ow_get_contacts(self.h, _p(ids, C.c_uint32), _p(f, C.c_float), _p(s, C.c_float))
+        return ids, f, s
+
+    def islands(self):
+        lab = np.zeros(self.nb, np.uint32)
+        self.lib.ow_get_islands(self.h, _p(lab, C.c_uint32))
+        return lab
+
+    def manifolds(self):
+        n = self.counts()["manifolds"]
+        out = np.zeros((n, 4), np.uint32)
+        self.lib.ow_get_manifolds(self.h, _p(out, C.c_uint32))
+        return out
+
+    def sor(self, structure, omega=1.7, tol=1e-6, max_sweeps=100000, mode=MODE_LEX_F32):
+        sw = C.c_uint32()
+        r = self.lib.ow_sor(self.h, int(structure), float(omega), float(tol), int(max_sweeps), int(mode), C.byref(sw))
+        return sw.value, r
+
+    def phi(self):
+        p = np.zeros(self.ns, np.float32)
+        self.lib.ow_get_phi(self.h, _p(p, C.c_float))
+        return p
+
+    def phi64(self):
+        p = np.zeros(self.ns, np.float64)
+        self.lib.ow_get_phi64(self.h, _p(p, C.c_double))
+        return p
+
+    def set_phi(self, phi):
+        p = np.ascontiguousarray(phi, np.float32)
+        self.lib.ow_set_phi(self.h, _p(p, C.c_float))
+
+    def set_ext(self, ext):
+        e = np.ascontiguousarray(ext, np.float32)
+        self.lib.ow_set_ext(self.h, _p(e, C.c_float))
+
+    def stress(self, structure, dt=1.0 / 60.0, live=True, cap=None):
+        cap = cap or self.ns * 4 + 16
+        ids = np.zeros((cap, 5), np.uint32)
+        vals = np.zeros((cap, 2), np.float32)
+        mr = C.c_float()
+        n = self.lib.ow_stress(self.h, int(structure), float(dt), 1 if live else 0, cap, _p(ids, C.c_uint32),
+                               _p(vals, C.c_float), C.byref(mr))
+        return ids[:n], vals[:n], mr.value
+
+    def remove_static(self, i):
+        self.lib.ow_remove_static(self.h, int(i))
+
+
+def collide_boxes(a, b, margin=0.02, reduce=True):
+    lib = load()
+    out = np.zeros(3 + 8 * 4, np.float32)
+    a = np.ascontiguousarray(a, np.float32); b = np.ascontiguousarray(b, np.float32)
+    n = lib.ow_collide_boxes(_p(a, C.c_float), _p(b, C.c_float), float(margin), 1 if reduce else 0, _p(out, C.c_float))
+    return n, out[:3].copy(), out[3:3 + 4 * n].reshape(n, 4).copy()

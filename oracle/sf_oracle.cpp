@@ -1,0 +1,1114 @@
+// ============================================================================================================
+// ORACLE — TEST INFRASTRUCTURE ONLY.
+//
+// A CPU restatement of Shatterforge's per-step physics hot path, used by tests/, __graft_entry__.smoke() and the
+// CPU-baseline leg of bench.py as the checker. Nothing in the product library links, loads or calls this file.
+//
+// What it restates (file:line inside the reference project):
+//   math helpers ........................ src/lib.rs:25-108   (minf/maxf are `if a < b {a} else {b}`, not fminf)
+//   constants ........................... src/lib.rs:110-215
+//   sparse chunk grid gget/gset ......... src/lib.rs:300-321
+//   linked() ............................ src/lib.rs:378-383
+//   bond_cap / finalize_brick ........... src/lib.rs:646-696
+//   setup_body .......................... src/lib.rs:844-891
+//   clamp_vel ........................... src/lib.rs:917-924
+//   sor_brick / sor_struct .............. src/lib.rs:1005-1040
+//   cond / axis_up / cond_w ............. src/lib.rs:1142-1151
+//   stress_brick ........................ src/lib.rs:1153-1227  (decisions only; particles/shards/meshing left out)
+//   update_cache / hkey / build_hash .... src/lib.rs:1367-1395
+//   push_contact / gen_contacts ......... src/lib.rs:1396-1471
+//   vel_at / eff_mass / apply_imp ....... src/lib.rs:1472-1492
+//   prep_contacts / solve ............... src/lib.rs:1551-1601
+//   integrate / pinch_check / substep ... src/lib.rs:1703-1783
+//   step (rigid part) ................... src/lib.rs:3640-3651
+//   union-find islands + island sleep ... engine/src/phys.rs:326-354, gpu/gpu_world.js:1634-1668
+//   box SAT collide_boxes / reduce4 ..... engine/src/phys.rs:507-628
+//
+// Floating point: every f32 expression keeps the reference's evaluation order, and the file is compiled with
+// -ffp-contract=off (wasm32 f32 has no fused multiply-add), so the restatement is op-for-op IEEE-equivalent.
+//
+// Parity status: the reference is a wasm32-only Rust crate with no buildable toolchain here, and its own tests
+// hold no numeric golden vectors for this path. Numeric parity of this oracle is therefore UNPINNED; it is pinned
+// only by behavioural known answers (intact frames hold under self-weight, src/lib.rs stab test; sor fixed point
+// against an FP64 solve; hull library volumes) that tests/test_oracle.py checks.
+//
+// Extensions beyond the reference, each behind a switch so the reference behaviour stays the default:
+//   * capacities are dynamic (the reference drops contacts past MAXC = 30000; the count it would drop is reported);
+//   * ORDER_COLOR solves contacts grouped by body-pair manifold in a greedy priority colouring order (the GPU's
+//     order), ORDER_LIST keeps the reference's list order;
+//   * SLEEP_ISLAND composes the per-body rest timer of src/lib.rs with the island rule of gpu/gpu_world.js:1660-1668;
+//   * pinch_kill = 0 clamps small pinched bodies instead of removing them.
+// ============================================================================================================
+#include <cstdint>
+#include <cstring>
+#include <cmath>
+#include <vector>
+#include <algorithm>
+#include <numeric>
+
+namespace {
+
+// ---------------------------------------------------------------- math (src/lib.rs:25-108)
+struct V { float x[3]; float& operator[](int i) { return x[i]; } float operator[](int i) const { return x[i]; } };
+typedef float M[9];
+static inline float minf(float a, float b) { return a < b ? a : b; }
+static inline float maxf(float a, float b) { return a > b ? a : b; }
+static inline float clampf(float x, float a, float b) { return minf(maxf(x, a), b); }
+static inline float fabs_(float x) { uint32_t u; std::memcpy(&u, &x, 4); u &= 0x7fffffffu; float r; std::memcpy(&r, &u, 4); return r; }
+static inline V vv(float a, float b, float c) { V r; r.x[0] = a; r.x[1] = b; r.x[2] = c; return r; }
+static inline V add(V a, V b) { return vv(a[0] + b[0], a[1] + b[1], a[2] + b[2]); }
+static inline V sub(V a, V b) { return vv(a[0] - b[0], a[1] - b[1], a[2] - b[2]); }
+static inline V mul(V a, float s) { return vv(a[0] * s, a[1] * s, a[2] * s); }
+static inline V madd(V a, V b, float s) { return vv(a[0] + b[0] * s, a[1] + b[1] * s, a[2] + b[2] * s); }
+static inline float dot(V a, V b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static inline V cross(V a, V b) { return vv(a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]); }
+static inline float len(V a) { return std::sqrt(dot(a, a)); }
+static inline V mv(const float* m, V v) {
+    return vv(m[0] * v[0] + m[1] * v[1] + m[2] * v[2], m[3] * v[0] + m[4] * v[1] + m[5] * v[2], m[6] * v[0] + m[7] * v[1] + m[8] * v[2]);
+}
+static inline void mmul(const float* a, const float* b, float* r) {
+    float t[9];
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) t[i * 3 + j] = a[i * 3] * b[j] + a[i * 3 + 1] * b[3 + j] + a[i * 3 + 2] * b[6 + j];
+    std::memcpy(r, t, sizeof t);
+}
+static inline void mt(const float* a, float* r) { float t[9] = {a[0], a[3], a[6], a[1], a[4], a[7], a[2], a[5], a[8]}; std::memcpy(r, t, sizeof t); }
+static void minv(const float* a, float* r) {
+    float c0 = a[4] * a[8] - a[5] * a[7];
+    float c1 = a[5] * a[6] - a[3] * a[8];
+    float c2 = a[3] * a[7] - a[4] * a[6];
+    float det = a[0] * c0 + a[1] * c1 + a[2] * c2;
+    if (fabs_(det) < 1e-12f) { for (int k = 0; k < 9; k++) r[k] = 0.0f; return; }
+    float id = 1.0f / det;
+    float t[9] = {c0 * id, (a[2] * a[7] - a[1] * a[8]) * id, (a[1] * a[5] - a[2] * a[4]) * id,
+                  c1 * id, (a[0] * a[8] - a[2] * a[6]) * id, (a[2] * a[3] - a[0] * a[5]) * id,
+                  c2 * id, (a[1] * a[6] - a[0] * a[7]) * id, (a[0] * a[4] - a[1] * a[3]) * id};
+    std::memcpy(r, t, sizeof t);
+}
+static void q_to_m(const float* q, float* r) {
+    float x = q[0], y = q[1], z = q[2], w = q[3];
+    float t[9] = {1.0f - 2.0f * (y * y + z * z), 2.0f * (x * y - z * w), 2.0f * (x * z + y * w),
+                  2.0f * (x * y + z * w), 1.0f - 2.0f * (x * x + z * z), 2.0f * (y * z - x * w),
+                  2.0f * (x * z - y * w), 2.0f * (y * z + x * w), 1.0f - 2.0f * (x * x + y * y)};
+    std::memcpy(r, t, sizeof t);
+}
+static void q_int(float* q, V w, float dt) {
+    V qv = vv(q[0], q[1], q[2]);
+    V d = add(mul(w, q[3]), cross(w, qv));
+    float dw = -dot(w, qv);
+    float r[4] = {q[0] + 0.5f * dt * d[0], q[1] + 0.5f * dt * d[1], q[2] + 0.5f * dt * d[2], q[3] + 0.5f * dt * dw};
+    float l = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+    if (l > 1e-9f) { for (int k = 0; k < 4; k++) r[k] /= l; } else { r[0] = 0; r[1] = 0; r[2] = 0; r[3] = 1; }
+    for (int k = 0; k < 4; k++) q[k] = r[k];
+}
+
+// ---------------------------------------------------------------- constants (src/lib.rs:110-215)
+const float S = 0.5f, H = 0.25f, RB = 0.27f, GR = 9.81f, MU = 0.65f, GROUNDK = 4.0f;
+const int NX = 640, NY = 136, NZ = 640, CXN = NX / 8, CYN = NY / 8, CZN = NZ / 8, NCT = CXN * CYN * CZN;
+const uint32_t HSIZE = 32768;
+const uint32_t NONE = 0xFFFFFFFFu;
+const uint32_t STATIC = 0xFFFFFFFFu;
+const uint32_t MAXC_REF = 30000;
+const uint8_t GLASS = 4, SLUG = 6;
+const float MASS[9] = {0.0f, 300.0f, 230.0f, 250.0f, 60.0f, 70.0f, 2000.0f, 8.0f, 44.0f};
+const float CAPV[9] = {0.0f, 140000.0f, 50000.0f, 150000.0f, 1500.0f, 9000.0f, 1e12f, 1e12f, 1e12f};
+const float CAPH[9] = {0.0f, 12000.0f, 12000.0f, 90000.0f, 400.0f, 5000.0f, 1e12f, 1e12f, 1e12f};
+const float TENS[9] = {0.0f, 0.35f, 0.1f, 0.9f, 0.5f, 0.7f, 1.0f, 1.0f, 1.0f};
+const float STIFF[9] = {0.0f, 1.0f, 0.8f, 2.0f, 0.02f, 0.4f, 1.0f, 1.0f, 1.0f};
+const float DUCT[9] = {0.0f, 6.0f, 12.0f, 3.0f, 40.0f, 8.0f, 1.0f, 1.0f, 1.0f};
+const int DIRS[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+
+static inline bool inb(int x, int y, int z) { return x >= 0 && y >= 0 && z >= 0 && x < NX && y < NY && z < NZ; }
+static inline V lat_pos(int x, int y, int z) { return vv((float)(x - NX / 2) * S + H, (float)y * S + H, (float)(z - NZ / 2) * S + H); }
+static inline uint32_t hkey(int x, int y, int z) {
+    return ((uint32_t)(x * 73856093) ^ (uint32_t)(y * 19349663) ^ (uint32_t)(z * 83492791)) & (HSIZE - 1);
+}
+static inline int wrap_mul(int a, int b) { return (int)((uint32_t)a * (uint32_t)b); }
+static inline uint32_t hkey_w(int x, int y, int z) {
+    return ((uint32_t)wrap_mul(x, 73856093) ^ (uint32_t)wrap_mul(y, 19349663) ^ (uint32_t)wrap_mul(z, 83492791)) & (HSIZE - 1);
+}
+
+struct Contact {
+    uint32_t a, b, bo, ba, bb;
+    V n, p, ra, rb, t1, t2;
+    float depth, mn, mt1, mt2, jn, jt1, jt2, bias, vn0;
+};
+
+enum { ORDER_LIST = 0, ORDER_COLOR = 1 };
+enum { SLEEP_BODY = 0, SLEEP_ISLAND = 1 };
+
+struct StepParams { uint32_t iterations, substeps, order, sleep_mode, pinch_kill; };
+
+// manifold priority for the colouring: a fixed mix of the body pair (b' = 0 for the static side, else b + 1)
+static inline uint32_t pair_priority(uint32_t a, uint32_t bp) {
+    uint32_t h = a * 0x9E3779B1u + bp * 0x85EBCA6Bu;
+    h ^= h >> 16; h *= 0x7FEB352Du; h ^= h >> 15; h *= 0x846CA68Bu; h ^= h >> 16;
+    return h;
+}
+
+struct World {
+    // grid
+    std::vector<uint32_t> ctab, cpool;
+    uint32_t ncpool = 0;
+    // bricks: static [0, ns), body bricks [ns, ns + nd)
+    uint32_t ns = 0, nd = 0;
+    std::vector<uint8_t> mat, infill;
+    std::vector<int32_t> bx, by, bz, sid;
+    std::vector<uint32_t> body, next, sup;
+    std::vector<V> local, wpos;
+    std::vector<uint32_t> nb6;     // 6 per brick
+    std::vector<float> bond, bmax; // 4 per brick
+    std::vector<float> phi, ext, stress;
+    std::vector<double> phi64;
+    // bodies
+    uint32_t nbody = 0;
+    std::vector<uint8_t> alive, asleep, wake;
+    std::vector<uint32_t> first, count, nc;
+    std::vector<V> pos, v, w, vpre, wpre;
+    std::vector<float> q;           // 4 per body
+    std::vector<float> rot, iil, iiw; // 9 per body
+    std::vector<float> m, im, sleep, rad, maxr;
+    // per-step
+    std::vector<uint32_t> hhead, hnext;
+    std::vector<Contact> cs;
+    std::vector<uint32_t> island;    // per body, last substep
+    std::vector<uint32_t> man_a, man_b, man_color, man_start, man_count, man_contacts;
+    uint32_t ncolors = 0;
+    uint32_t frame = 0;
+    uint64_t would_drop = 0;         // contacts the reference would have dropped past MAXC
+    uint32_t crush_n = 0;
+
+    uint32_t gget(int x, int y, int z) const {
+        if (!inb(x, y, z)) return 0;
+        uint32_t t = ctab[((y >> 3) * CZN + (z >> 3)) * CXN + (x >> 3)];
+        if (t == 0) return 0;
+        return cpool[(size_t)(t - 1) * 512 + (((y & 7) * 8 + (z & 7)) * 8 + (x & 7))];
+    }
+    bool gset(int x, int y, int z, uint32_t val) {
+        if (!inb(x, y, z)) return false;
+        uint32_t ci = ((y >> 3) * CZN + (z >> 3)) * CXN + (x >> 3);
+        uint32_t t = ctab[ci];
+        if (t == 0) {
+            if (val == 0) return true;
+            ncpool++;
+            t = ncpool;
+            ctab[ci] = t;
+            cpool.resize((size_t)ncpool * 512, 0);
+        }
+        cpool[(size_t)(t - 1) * 512 + (((y & 7) * 8 + (z & 7)) * 8 + (x & 7))] = val;
+        return true;
+    }
+    uint32_t static_brick(int x, int y, int z) const {
+        uint32_t g = gget(x, y, z);
+        if (g == 0) return NONE;
+        uint32_t j = g - 1;
+        return (mat[j] != 0 && body[j] == STATIC) ? j : NONE;
+    }
+    // src/lib.rs:378-383
+    bool linked(uint32_t i, int d, uint32_t& jo, float& hp) const {
+        uint32_t j = nb6[(size_t)i * 6 + d];
+        if (j == NONE || mat[j] == 0 || body[j] != body[i]) return false;
+        float h = (d & 1) == 0 ? bond[(size_t)i * 4 + (d >> 1)] : bond[(size_t)j * 4 + (d >> 1)];
+        if (h > 0.0f) { jo = j; hp = h; return true; }
+        return false;
+    }
+    float axis_up(uint32_t i, int a) const { return body[i] == STATIC ? (a == 1 ? 1.0f : 0.0f) : rot[(size_t)body[i] * 9 + 3 + a]; }
+    float cond_w(uint32_t i, uint32_t j, int a) const {
+        float k = minf(STIFF[mat[i]], STIFF[mat[j]]);
+        if (body[i] == STATIC) return k * (a == 1 ? 1.0f : 0.3f);
+        float u = fabs_(axis_up(i, a));
+        return k * (0.3f + 0.7f * u);
+    }
+    bool in_struct(uint32_t i, int s) const { return sid[i] == s && mat[i] != 0 && mat[i] < SLUG && body[i] == STATIC; }
+};
+
+static float bond_cap(uint8_t mi, uint8_t mj, int axis) {
+    float a = axis == 1 ? CAPV[mi] : CAPH[mi];
+    float b = axis == 1 ? CAPV[mj] : CAPH[mj];
+    return minf(a, b);
+}
+
+// src/lib.rs:668-696 (corner jitter and face masks are rendering data and are left out)
+static void finalize_brick(World& w, uint32_t i) {
+    if (w.mat[i] == 0) return;
+    for (int d = 0; d < 6; d++) {
+        uint32_t g = w.gget(w.bx[i] + DIRS[d][0], w.by[i] + DIRS[d][1], w.bz[i] + DIRS[d][2]);
+        w.nb6[(size_t)i * 6 + d] = g == 0 ? NONE : g - 1;
+    }
+    for (int a = 0; a < 3; a++) {
+        uint32_t j = w.nb6[(size_t)i * 6 + a * 2];
+        bool gap = j != NONE && w.infill[i] != w.infill[j] && (a != 1 || w.infill[i] == 1);
+        if (j != NONE && !gap && w.mat[j] != 0 && w.body[j] == w.body[i] && w.sid[j] == w.sid[i]) {
+            float c = bond_cap(w.mat[i], w.mat[j], a);
+            w.bond[(size_t)i * 4 + a] = c; w.bmax[(size_t)i * 4 + a] = c;
+        } else { w.bond[(size_t)i * 4 + a] = 0.0f; w.bmax[(size_t)i * 4 + a] = 0.0f; }
+    }
+    if (w.by[i] == 0 && w.body[i] == STATIC) {
+        float c = CAPV[w.mat[i]] * 2.0f;
+        w.bond[(size_t)i * 4 + 3] = c; w.bmax[(size_t)i * 4 + 3] = c;
+    } else { w.bond[(size_t)i * 4 + 3] = 0.0f; w.bmax[(size_t)i * 4 + 3] = 0.0f; }
+}
+
+// src/lib.rs:844-891, for the body's bricks lst[0..n) with local[] already holding lattice positions
+static void setup_body(World& w, uint32_t b, const uint32_t* lst, uint32_t n, V ppos, const float* prot, const float* pq, V pv, V pw) {
+    float mass = 0.0f;
+    V cl = vv(0, 0, 0);
+    for (uint32_t t = 0; t < n; t++) { uint32_t i = lst[t]; float mm = MASS[w.mat[i]]; mass += mm; cl = madd(cl, w.local[i], mm); }
+    cl = mul(cl, 1.0f / mass);
+    float it[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    float rad = 0.0f;
+    const float cube = S * S / 6.0f;
+    for (uint32_t t = 0; t < n; t++) {
+        uint32_t i = lst[t];
+        float mm = MASS[w.mat[i]];
+        V r = sub(w.local[i], cl);
+        w.local[i] = r;
+        float rr = dot(r, r);
+        rad = maxf(rad, rr);
+        it[0] += mm * (rr - r[0] * r[0] + cube); it[4] += mm * (rr - r[1] * r[1] + cube); it[8] += mm * (rr - r[2] * r[2] + cube);
+        it[1] -= mm * r[0] * r[1]; it[2] -= mm * r[0] * r[2]; it[5] -= mm * r[1] * r[2];
+        w.body[i] = b;
+        w.next[i] = t + 1 < n ? lst[t + 1] : NONE;
+    }
+    it[3] = it[1]; it[6] = it[2]; it[7] = it[5];
+    float* iil = &w.iil[(size_t)b * 9];
+    minv(it, iil);
+    V off = mv(prot, cl);
+    w.alive[b] = 1;
+    w.first[b] = lst[0];
+    w.count[b] = n;
+    w.pos[b] = add(ppos, off);
+    for (int k = 0; k < 4; k++) w.q[(size_t)b * 4 + k] = pq[k];
+    std::memcpy(&w.rot[(size_t)b * 9], prot, 9 * sizeof(float));
+    w.v[b] = add(pv, cross(pw, off));
+    w.w[b] = pw;
+    w.m[b] = mass; w.im[b] = 1.0f / mass;
+    float t1[9], t2[9];
+    mmul(prot, iil, t1); mt(prot, t2); mmul(t1, t2, &w.iiw[(size_t)b * 9]);
+    w.sleep[b] = 0.0f; w.asleep[b] = 0; w.wake[b] = 0; w.maxr[b] = 0.0f;
+    w.rad[b] = std::sqrt(rad) + H * 1.8f;
+    for (uint32_t t = 0; t < n; t++) { uint32_t i = lst[t]; w.wpos[i] = add(w.pos[b], mv(prot, w.local[i])); }
+}
+
+static void clamp_vel(World& w, uint32_t b) {
+    float vl = len(w.v[b]);
+    if (vl > 60.0f) w.v[b] = mul(w.v[b], 60.0f / vl);
+    float a = len(w.w[b]);
+    float amax = minf(25.0f, 16.0f / maxf(w.rad[b], 0.3f));
+    if (a > amax) w.w[b] = mul(w.w[b], amax / a);
+}
+
+static void kill_body(World& w, uint32_t b) {
+    uint32_t k = w.first[b];
+    while (k != NONE) { uint32_t nx = w.next[k]; if (w.body[k] == b) { w.mat[k] = 0; w.body[k] = STATIC; } k = nx; }
+    w.alive[b] = 0; w.first[b] = NONE;
+}
+
+// ---------------------------------------------------------------- SOR (src/lib.rs:1005-1040)
+template <class T> struct PhiRef;
+static float sor_brick(World& w, uint32_t i, float omega) {
+    uint8_t mi = w.mat[i];
+    float sk = 0.0f, skp = 0.0f;
+    for (int d = 0; d < 6; d++) {
+        uint32_t j; float hp;
+        if (!w.linked(i, d, j, hp)) continue;
+        float k = w.cond_w(i, j, d >> 1);
+        sk += k; skp += k * w.phi[j];
+    }
+    if (w.body[i] == STATIC) { if (w.by[i] == 0 && w.bond[(size_t)i * 4 + 3] > 0.0f) sk += GROUNDK * STIFF[mi]; }
+    else if (w.frame - w.sup[i] < 10u) sk += GROUNDK * STIFF[mi];
+    if (sk > 0.0f) {
+        float target = (MASS[mi] + w.ext[i] + skp) / sk;
+        float d = omega * (target - w.phi[i]);
+        w.phi[i] += d;
+        return fabs_(d);
+    }
+    return 0.0f;
+}
+// the same system in double precision (coefficients are the reference's f32 values, promoted)
+static double sor_brick64(World& w, uint32_t i, double omega) {
+    uint8_t mi = w.mat[i];
+    double sk = 0.0, skp = 0.0;
+    for (int d = 0; d < 6; d++) {
+        uint32_t j; float hp;
+        if (!w.linked(i, d, j, hp)) continue;
+        double k = (double)w.cond_w(i, j, d >> 1);
+        sk += k; skp += k * w.phi64[j];
+    }
+    if (w.body[i] == STATIC && w.by[i] == 0 && w.bond[(size_t)i * 4 + 3] > 0.0f) sk += (double)(GROUNDK * STIFF[mi]);
+    if (sk > 0.0) {
+        double target = ((double)(MASS[mi] + w.ext[i]) + skp) / sk;
+        double d = omega * (target - w.phi64[i]);
+        w.phi64[i] += d;
+        return std::fabs(d);
+    }
+    return 0.0;
+}
+
+struct SorResult { uint32_t sweeps; double resid; };
+
+// mode 0: reference lexicographic f32 sweeps; 1: the same in f64; 2: red-black f32 (red = even (x+y+z));
+// 3: red-black f64
+static SorResult sor_solve(World& w, int s, float omega, double tol, uint32_t max_sweeps, int mode) {
+    std::vector<uint32_t> list;
+    for (uint32_t i = 0; i < w.ns; i++) if (w.in_struct(i, s)) list.push_back(i);
+    SorResult r{0, 1e30};
+    if (list.empty()) { r.resid = 0.0; return r; }
+    if (mode == 1 || mode == 3) {
+        for (uint32_t i : list) w.phi64[i] = (double)w.phi[i];
+    }
+    while (r.sweeps < max_sweeps) {
+        if (mode == 0) {
+            float md = 0.0f, mp = 1.0f;
+            for (uint32_t i : list) { float d = sor_brick(w, i, omega); if (d > md) md = d; if (w.phi[i] > mp) mp = w.phi[i]; }
+            r.resid = (double)(md / mp);
+        } else if (mode == 1) {
+            double md = 0.0, mp = 1.0;
+            for (uint32_t i : list) { double d = sor_brick64(w, i, (double)omega); if (d > md) md = d; if (w.phi64[i] > mp) mp = w.phi64[i]; }
+            r.resid = md / mp;
+        } else if (mode == 3) {
+            double md = 0.0, mp = 1.0;
+            for (int colour = 0; colour < 2; colour++)
+                for (uint32_t i : list) {
+                    if (((w.bx[i] + w.by[i] + w.bz[i]) & 1) != colour) continue;
+                    double d = sor_brick64(w, i, (double)omega); if (d > md) md = d;
+                }
+            for (uint32_t i : list) if (w.phi64[i] > mp) mp = w.phi64[i];
+            r.resid = md / mp;
+        } else {
+            float md = 0.0f, mp = 1.0f;
+            for (int colour = 0; colour < 2; colour++)
+                for (uint32_t i : list) {
+                    if (((w.bx[i] + w.by[i] + w.bz[i]) & 1) != colour) continue;
+                    float d = sor_brick(w, i, omega); if (d > md) md = d;
+                }
+            for (uint32_t i : list) if (w.phi[i] > mp) mp = w.phi[i];
+            r.resid = (double)(md / mp);
+        }
+        r.sweeps++;
+        if (r.resid < tol) break;
+    }
+    if (mode == 1 || mode == 3) for (uint32_t i : list) w.phi[i] = (float)w.phi64[i];
+    return r;
+}
+
+// ---------------------------------------------------------------- joint checks (src/lib.rs:1153-1227)
+enum { J_HOLD = 0, J_FATIGUE = 1, J_FAIL = 2, J_CRUSH = 3 };
+struct Joint { uint32_t i, axis, j, decision, crushed; float ratio, bond_after; };
+
+static float stress_brick(World& w, uint32_t i, float dt, bool live, std::vector<Joint>& out) {
+    uint8_t mi = w.mat[i];
+    bool dynb = w.body[i] != STATIC;
+    float maxr = 0.0f;
+    for (int a = 0; a < 3; a++) {
+        uint32_t j; float hp;
+        if (!w.linked(i, a * 2, j, hp)) continue;
+        float f = w.cond_w(i, j, a) * (w.phi[i] - w.phi[j]);
+        float u = w.axis_up(i, a);
+        float up = f > 0.0f ? maxf(u, 0.0f) : maxf(-u, 0.0f);
+        float tens = minf(TENS[mi], TENS[w.mat[j]]);
+        float capm = 1.0f - (1.0f - tens) * up;
+        float hpw = hp;
+        if (dynb) {
+            float cv = minf(CAPV[mi], CAPV[w.mat[j]]), ch = minf(CAPH[mi], CAPH[w.mat[j]]);
+            float lat = a == 1 ? cv : ch;
+            float au = fabs_(u);
+            hpw = hp * (cv * au + ch * (1.0f - au)) / maxf(lat, 1.0f);
+        }
+        float r = fabs_(f) / (hpw * capm);
+        if (r > w.stress[i]) w.stress[i] = r;
+        if (r > w.stress[j]) w.stress[j] = r;
+        if (r > maxr) maxr = r;
+        Joint jr{i, (uint32_t)a, j, J_HOLD, NONE, r, hp};
+        if (live && r > 1.0f) {
+            float nhp = dynb ? hp - hp * dt * DUCT[mi] * minf(r - 0.85f, 40.0f) : hp - hp * dt * 2.2f * minf(r - 0.85f, 2.5f);
+            if (nhp < w.bmax[(size_t)i * 4 + a] * 0.08f) {
+                if (up == 0.0f && fabs_(u) > 0.5f && w.crush_n < 300) {
+                    w.crush_n++;
+                    uint32_t k = CAPV[w.mat[j]] < CAPV[mi] ? j : i;
+                    jr.decision = J_CRUSH; jr.crushed = k; jr.bond_after = hp;
+                    out.push_back(jr);
+                    w.gset(w.bx[k], w.by[k], w.bz[k], 0);
+                    w.mat[k] = 0;
+                    return maxf(maxr, r);
+                }
+                w.bond[(size_t)i * 4 + a] = 0.0f;
+                jr.decision = J_FAIL; jr.bond_after = 0.0f;
+            } else {
+                w.bond[(size_t)i * 4 + a] = nhp;
+                jr.decision = J_FATIGUE; jr.bond_after = nhp;
+            }
+        }
+        out.push_back(jr);
+    }
+    if (!dynb && w.by[i] == 0 && w.bond[(size_t)i * 4 + 3] > 0.0f) {
+        float f = GROUNDK * STIFF[mi] * w.phi[i];
+        float r = f / w.bond[(size_t)i * 4 + 3];
+        if (r > w.stress[i]) w.stress[i] = r;
+        if (r > maxr) maxr = r;
+        Joint jr{i, 3u, NONE, J_HOLD, NONE, r, w.bond[(size_t)i * 4 + 3]};
+        if (live && r > 1.0f) {
+            float& b3 = w.bond[(size_t)i * 4 + 3];
+            b3 -= b3 * dt * 2.2f * (r - 0.85f);
+            if (b3 < w.bmax[(size_t)i * 4 + 3] * 0.08f) { b3 = 0.0f; jr.decision = J_FAIL; }
+            else jr.decision = J_FATIGUE;
+            jr.bond_after = b3;
+        }
+        out.push_back(jr);
+    }
+    return maxr;
+}
+
+// ---------------------------------------------------------------- rigid step (src/lib.rs:1367-1783)
+static void update_cache(World& w) {
+    for (uint32_t b = 0; b < w.nbody; b++) {
+        if (!w.alive[b] || w.asleep[b]) continue;
+        float* r = &w.rot[(size_t)b * 9];
+        q_to_m(&w.q[(size_t)b * 4], r);
+        float t1[9], t2[9];
+        mmul(r, &w.iil[(size_t)b * 9], t1); mt(r, t2); mmul(t1, t2, &w.iiw[(size_t)b * 9]);
+        V p = w.pos[b];
+        uint32_t k = w.first[b];
+        while (k != NONE) { w.wpos[k] = add(p, mv(r, w.local[k])); k = w.next[k]; }
+    }
+}
+static void build_hash(World& w) {
+    std::fill(w.hhead.begin(), w.hhead.end(), NONE);
+    for (uint32_t b = 0; b < w.nbody; b++) {
+        if (!w.alive[b]) continue;
+        uint32_t k = w.first[b];
+        while (k != NONE) {
+            V p = w.wpos[k];
+            uint32_t h = hkey_w((int)std::floor(p[0] / S), (int)std::floor(p[1] / S), (int)std::floor(p[2] / S));
+            w.hnext[k] = w.hhead[h]; w.hhead[h] = k;
+            k = w.next[k];
+        }
+    }
+}
+static void push_contact(World& w, uint32_t a, uint32_t b, uint32_t bo, uint32_t ba, uint32_t bb, V p, V n, float depth) {
+    if (w.cs.size() >= MAXC_REF) w.would_drop++;
+    Contact c;
+    std::memset(&c, 0, sizeof c);
+    c.a = a; c.b = b; c.bo = bo; c.ba = ba; c.bb = bb; c.p = p; c.n = n; c.depth = depth;
+    w.cs.push_back(c);
+    w.nc[a] += 1;
+    if (b != STATIC) w.nc[b] += 1;
+}
+static void gen_contacts(World& w) {
+    w.cs.clear();
+    for (uint32_t b = 0; b < w.nbody; b++) w.nc[b] = 0;
+    for (uint32_t a = 0; a < w.nbody; a++) {
+        if (!w.alive[a] || w.asleep[a]) continue;
+        const float* rot = &w.rot[(size_t)a * 9];
+        float speed = len(w.v[a]) + len(w.w[a]) * w.rad[a] * 0.5f;
+        uint32_t k = w.first[a];
+        while (k != NONE) {
+            uint32_t i = k;
+            V p = w.wpos[i];
+            if (p[1] < 0.5f) {
+                for (int c = 0; c < 8; c++) {
+                    V l = vv((c & 1) == 0 ? -H : H, (c & 2) == 0 ? -H : H, (c & 4) == 0 ? -H : H);
+                    V cp = add(p, mv(rot, l));
+                    if (cp[1] < 0.0f) { push_contact(w, a, STATIC, STATIC, i, NONE, cp, vv(0.0f, 1.0f, 0.0f), -cp[1]); w.sup[i] = w.frame; }
+                }
+            }
+            int cx = (int)std::floor(p[0] / S) + NX / 2, cy = (int)std::floor(p[1] / S), cz = (int)std::floor(p[2] / S) + NZ / 2;
+            for (int dz = -1; dz <= 1; dz++) for (int dy = -1; dy <= 1; dy++) for (int dx = -1; dx <= 1; dx++) {
+                int x = cx + dx, y = cy + dy, z = cz + dz;
+                uint32_t j = w.static_brick(x, y, z);
+                if (j == NONE) continue;
+                V c = lat_pos(x, y, z);
+                V qq = vv(clampf(p[0], c[0] - H, c[0] + H), clampf(p[1], c[1] - H, c[1] + H), clampf(p[2], c[2] - H, c[2] + H));
+                V d = sub(p, qq);
+                float dist = len(d);
+                if (dist >= RB) continue;
+                if (dist > 1e-4f) {
+                    if (d[1] > 0.3f * dist) w.sup[i] = w.frame;
+                    push_contact(w, a, STATIC, STATIC, i, j, qq, mul(d, 1.0f / dist), RB - dist);
+                } else {
+                    V r = sub(p, c);
+                    int ax = 0; for (int t = 1; t < 3; t++) if (fabs_(r[t]) > fabs_(r[ax])) ax = t;
+                    V n = vv(0, 0, 0); n[ax] = r[ax] >= 0.0f ? 1.0f : -1.0f;
+                    push_contact(w, a, STATIC, STATIC, i, j, p, n, H + RB - fabs_(r[ax]));
+                }
+            }
+            int hx = (int)std::floor(p[0] / S), hy = (int)std::floor(p[1] / S), hz = (int)std::floor(p[2] / S);
+            for (int dz = -1; dz <= 1; dz++) for (int dy = -1; dy <= 1; dy++) for (int dx = -1; dx <= 1; dx++) {
+                uint32_t mm = w.hhead[hkey_w(hx + dx, hy + dy, hz + dz)];
+                while (mm != NONE) {
+                    uint32_t j = mm;
+                    mm = w.hnext[j];
+                    uint32_t bj = w.body[j];
+                    if (bj == a || w.mat[j] == 0) continue;
+                    bool other_awake = !w.asleep[bj];
+                    if (other_awake && j < i) continue;
+                    V d = sub(p, w.wpos[j]);
+                    float dd = dot(d, d);
+                    if (dd >= 4.0f * RB * RB || dd < 1e-10f) continue;
+                    float dist = std::sqrt(dd);
+                    V n = mul(d, 1.0f / dist);
+                    V cp = madd(w.wpos[j], n, dist * 0.5f);
+                    if (n[1] > 0.3f) w.sup[i] = w.frame; else if (n[1] < -0.3f) w.sup[j] = w.frame;
+                    if (other_awake) push_contact(w, a, bj, bj, i, j, cp, n, 2.0f * RB - dist);
+                    else {
+                        if (speed > 0.7f) w.wake[bj] = 1;
+                        push_contact(w, a, STATIC, bj, i, j, cp, n, 2.0f * RB - dist);
+                    }
+                }
+            }
+            k = w.next[i];
+        }
+    }
+}
+static inline V vel_at(const World& w, uint32_t b, V r) { if (b == STATIC) return vv(0, 0, 0); return add(w.v[b], cross(w.w[b], r)); }
+static float eff_mass(const World& w, uint32_t a, uint32_t b, V ra, V rb, V n) {
+    float k = w.im[a] + dot(n, cross(mv(&w.iiw[(size_t)a * 9], cross(ra, n)), ra));
+    if (b != STATIC) k += w.im[b] + dot(n, cross(mv(&w.iiw[(size_t)b * 9], cross(rb, n)), rb));
+    return k > 1e-12f ? 1.0f / k : 0.0f;
+}
+static void apply_imp(World& w, uint32_t a, uint32_t b, V ra, V rb, V p) {
+    w.v[a] = madd(w.v[a], p, w.im[a]);
+    V dw = mv(&w.iiw[(size_t)a * 9], cross(ra, p));
+    w.w[a] = add(w.w[a], dw);
+    if (b != STATIC) {
+        w.v[b] = madd(w.v[b], p, -w.im[b]);
+        V dw2 = mv(&w.iiw[(size_t)b * 9], cross(rb, p));
+        w.w[b] = sub(w.w[b], dw2);
+    }
+}
+static void prep_contacts(World& w, float h) {
+    for (Contact& c : w.cs) {
+        uint32_t a = c.a;
+        c.ra = sub(c.p, w.pos[a]);
+        c.rb = c.b != STATIC ? sub(c.p, w.pos[c.b]) : vv(0, 0, 0);
+        c.mn = eff_mass(w, a, c.b, c.ra, c.rb, c.n);
+        V dv = sub(vel_at(w, c.a, c.ra), vel_at(w, c.b, c.rb));
+        float vn = dot(dv, c.n);
+        c.vn0 = maxf(-vn, 0.0f);
+        V vt = sub(dv, mul(c.n, vn));
+        float lt = len(vt);
+        if (lt > 1e-4f) c.t1 = mul(vt, 1.0f / lt);
+        else {
+            V t = fabs_(c.n[0]) < 0.9f ? vv(1, 0, 0) : vv(0, 1, 0);
+            V x = cross(c.n, t); c.t1 = mul(x, 1.0f / len(x));
+        }
+        c.t2 = cross(c.n, c.t1);
+        c.mt1 = eff_mass(w, a, c.b, c.ra, c.rb, c.t1);
+        c.mt2 = eff_mass(w, a, c.b, c.ra, c.rb, c.t2);
+        float bias = minf(0.2f / h * maxf(c.depth - 0.01f, 0.0f), 1.0f);
+        if (vn < -2.0f) bias = maxf(bias, -0.12f * vn);
+        c.bias = bias;
+    }
+}
+static inline void solve_contact(World& w, Contact& c) {
+    uint32_t a = c.a;
+    V dv = sub(vel_at(w, c.a, c.ra), vel_at(w, c.b, c.rb));
+    float vn = dot(dv, c.n);
+    float lam = c.mn * (-vn + c.bias);
+    float old = c.jn;
+    c.jn = maxf(old + lam, 0.0f);
+    float d = c.jn - old;
+    apply_imp(w, a, c.b, c.ra, c.rb, mul(c.n, d));
+    float lim = MU * c.jn;
+    dv = sub(vel_at(w, c.a, c.ra), vel_at(w, c.b, c.rb));
+    float l1 = -c.mt1 * dot(dv, c.t1);
+    float o1 = c.jt1; c.jt1 = clampf(o1 + l1, -lim, lim);
+    float l2 = -c.mt2 * dot(dv, c.t2);
+    float o2 = c.jt2; c.jt2 = clampf(o2 + l2, -lim, lim);
+    V p = add(mul(c.t1, c.jt1 - o1), mul(c.t2, c.jt2 - o2));
+    apply_imp(w, a, c.b, c.ra, c.rb, p);
+}
+
+// Manifolds: contacts grouped by (a, b) in list order, sorted by key (a, b') with b' = 0 for the static side.
+// Colours: greedy in decreasing priority (ties: lower manifold index first), smallest colour free at both bodies;
+// this is the colouring Jones-Plassmann rounds produce with the same priorities.
+static void build_manifolds(World& w) {
+    size_t n = w.cs.size();
+    std::vector<uint32_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0u);
+    auto key = [&](uint32_t k) -> uint64_t {
+        const Contact& c = w.cs[k];
+        uint64_t bp = c.b == STATIC ? 0 : (uint64_t)c.b + 1;
+        return ((uint64_t)c.a << 32) | bp;
+    };
+    std::stable_sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
+    w.man_a.clear(); w.man_b.clear(); w.man_start.clear(); w.man_count.clear(); w.man_contacts = idx;
+    for (size_t t = 0; t < n; t++) {
+        if (t == 0 || key(idx[t]) != key(idx[t - 1])) {
+            const Contact& c = w.cs[idx[t]];
+            w.man_a.push_back(c.a); w.man_b.push_back(c.b); w.man_start.push_back((uint32_t)t); w.man_count.push_back(0);
+        }
+        w.man_count.back()++;
+    }
+    size_t nm = w.man_a.size();
+    std::vector<uint32_t> order(nm);
+    std::iota(order.begin(), order.end(), 0u);
+    std::vector<uint32_t> prio(nm);
+    for (size_t k = 0; k < nm; k++) prio[k] = pair_priority(w.man_a[k], w.man_b[k] == STATIC ? 0u : w.man_b[k] + 1);
+    std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return prio[x] != prio[y] ? prio[x] > prio[y] : x < y; });
+    std::vector<std::vector<uint64_t>> used(w.nbody, std::vector<uint64_t>(4, 0));
+    w.man_color.assign(nm, 0);
+    w.ncolors = 0;
+    for (uint32_t mi : order) {
+        uint32_t a = w.man_a[mi], b = w.man_b[mi];
+        uint32_t c = 0;
+        for (;; c++) {
+            bool busy = (used[a][c >> 6] >> (c & 63)) & 1;
+            if (b != STATIC) busy = busy || ((used[b][c >> 6] >> (c & 63)) & 1);
+            if (!busy) break;
+        }
+        w.man_color[mi] = c;
+        used[a][c >> 6] |= 1ull << (c & 63);
+        if (b != STATIC) used[b][c >> 6] |= 1ull << (c & 63);
+        if (c + 1 > w.ncolors) w.ncolors = c + 1;
+    }
+}
+static void solve_list(World& w) { for (Contact& c : w.cs) solve_contact(w, c); }
+static void solve_colored(World& w) {
+    // manifolds of one colour share no awake body, so their order inside a colour does not change the result
+    std::vector<std::vector<uint32_t>> bycol(w.ncolors);
+    for (size_t m = 0; m < w.man_a.size(); m++) bycol[w.man_color[m]].push_back((uint32_t)m);
+    for (auto& lst : bycol)
+        for (uint32_t m : lst)
+            for (uint32_t t = 0; t < w.man_count[m]; t++) solve_contact(w, w.cs[w.man_contacts[w.man_start[m] + t]]);
+}
+
+// islands over manifolds between two awake bodies; label = smallest body id of the island (root = min id)
+static void islands(World& w) {
+    std::vector<uint32_t> par(w.nbody);
+    std::iota(par.begin(), par.end(), 0u);
+    auto find = [&](uint32_t x) { while (par[x] != x) { par[x] = par[par[x]]; x = par[x]; } return x; };
+    for (size_t m = 0; m < w.man_a.size(); m++) {
+        uint32_t b = w.man_b[m];
+        if (b == STATIC) continue;
+        uint32_t x = find(w.man_a[m]), y = find(b);
+        if (x == y) continue;
+        if (x < y) std::swap(x, y);
+        par[x] = y;
+    }
+    w.island.assign(w.nbody, NONE);
+    for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b] && !w.asleep[b]) w.island[b] = find(b);
+}
+
+static void pinch_check(World& w, bool kill) {
+    for (uint32_t b = 0; b < w.nbody; b++) {
+        if (!w.alive[b] || w.asleep[b]) continue;
+        V dw = sub(w.w[b], w.wpre[b]);
+        float tip = len(dw) * w.rad[b];
+        if (tip > 6.0f) w.w[b] = madd(w.wpre[b], dw, 6.0f / tip);
+        V dv = sub(w.v[b], w.vpre[b]);
+        float mm = len(dv);
+        if (mm < 8.0f) continue;
+        uint32_t f = w.first[b];
+        if (f == NONE || w.mat[f] >= SLUG) continue;
+        if (kill && w.count[b] <= 6) kill_body(w, b);
+        else w.v[b] = madd(w.vpre[b], dv, 8.0f / mm);
+    }
+}
+static void integrate(World& w, float h, int sleep_mode) {
+    std::vector<uint8_t> rest(w.nbody, 0);
+    for (uint32_t b = 0; b < w.nbody; b++) {
+        if (!w.alive[b] || w.asleep[b]) continue;
+        clamp_vel(w, b);
+        w.pos[b] = madd(w.pos[b], w.v[b], h);
+        q_int(&w.q[(size_t)b * 4], w.w[b], h);
+        w.v[b] = mul(w.v[b], 1.0f - 0.01f * h);
+        w.w[b] = mul(w.w[b], 1.0f - 0.05f * h);
+        bool small = w.count[b] <= 3;
+        if (w.nc[b] > 0 && small) {
+            w.w[b] = mul(w.w[b], 1.0f - minf(7.0f * h, 0.5f));
+            w.v[b] = mul(w.v[b], 1.0f - minf(2.0f * h, 0.3f));
+        }
+        float v2 = dot(w.v[b], w.v[b]);
+        float rr = w.rad[b];
+        float w2 = dot(w.w[b], w.w[b]) * rr * rr;
+        float vt = small ? 0.16f : 0.06f, wt = small ? 0.3f : 0.04f;
+        if (v2 < vt && w2 < wt && w.nc[b] > 0 && w.maxr[b] < 0.95f) {
+            w.sleep[b] += h;
+            if (sleep_mode == SLEEP_BODY && w.sleep[b] > 0.45f) { w.asleep[b] = 1; w.v[b] = vv(0, 0, 0); w.w[b] = vv(0, 0, 0); }
+        } else w.sleep[b] = 0.0f;
+        V p = w.pos[b];
+        if (p[1] < -15.0f || fabs_(p[0]) > 190.0f || fabs_(p[2]) > 190.0f || p[1] > 120.0f) kill_body(w, b);
+    }
+    if (sleep_mode == SLEEP_ISLAND) {
+        // an island sleeps when its least-rested body has rested past the threshold, a body alone at twice it
+        std::vector<float> mint(w.nbody, 3.4e38f);
+        for (uint32_t b = 0; b < w.nbody; b++) {
+            uint32_t r = w.island[b];
+            if (r == NONE || !w.alive[b]) continue;
+            if (w.sleep[b] < mint[r]) mint[r] = w.sleep[b];
+        }
+        for (uint32_t b = 0; b < w.nbody; b++) {
+            uint32_t r = w.island[b];
+            if (r == NONE || !w.alive[b] || w.asleep[b]) continue;
+            if (mint[r] > 0.45f || w.sleep[b] > 0.9f) { w.asleep[b] = 1; w.v[b] = vv(0, 0, 0); w.w[b] = vv(0, 0, 0); }
+        }
+    }
+    for (uint32_t b = 0; b < w.nbody; b++) {
+        if (w.wake[b]) { w.wake[b] = 0; if (w.alive[b]) { w.asleep[b] = 0; w.sleep[b] = 0.0f; } }
+    }
+}
+static void substep(World& w, float h, const StepParams& P) {
+    update_cache(w);
+    for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b] && !w.asleep[b]) w.v[b][1] -= GR * h;
+    build_hash(w);
+    gen_contacts(w);
+    prep_contacts(w, h);
+    for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b]) { w.vpre[b] = w.v[b]; w.wpre[b] = w.w[b]; }
+    build_manifolds(w);
+    islands(w);
+    for (uint32_t it = 0; it < P.iterations; it++) {
+        if (P.order == ORDER_COLOR) solve_colored(w); else solve_list(w);
+    }
+    pinch_check(w, P.pinch_kill != 0);
+    integrate(w, h, (int)P.sleep_mode);
+}
+static void step(World& w, float dt, const StepParams& P) {
+    dt = clampf(dt, 0.0f, 1.0f / 30.0f);
+    w.frame += 1;
+    uint32_t ns = P.substeps ? P.substeps : 2;
+    float h = ns == 2 ? dt * 0.5f : dt / (float)ns;
+    for (uint32_t s = 0; s < ns; s++) substep(w, h, P);
+}
+
+// ---------------------------------------------------------------- box SAT (engine/src/phys.rs:502-628)
+struct P3 { float x, y, z; };
+static inline P3 p3(float a, float b, float c) { return P3{a, b, c}; }
+static inline P3 operator+(P3 a, P3 b) { return p3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline P3 operator-(P3 a, P3 b) { return p3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline P3 operator*(P3 a, float s) { return p3(a.x * s, a.y * s, a.z * s); }
+static inline P3 operator-(P3 a) { return p3(-a.x, -a.y, -a.z); }
+static inline float pdot(P3 a, P3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline P3 pcross(P3 a, P3 b) { return p3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static inline float plen2(P3 a) { return pdot(a, a); }
+static inline float pget(P3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+static inline float sqrt_e(float x) { return x <= 0.0f ? 0.0f : std::sqrt(x); }  // engine/src/math.rs:87-90
+struct M3 { P3 c[3]; };
+static M3 quat_m3(const float* q) {  // engine/src/math.rs:60-66 (columns)
+    float x = q[0], y = q[1], z = q[2], w = q[3];
+    M3 m;
+    m.c[0] = p3(1.0f - 2.0f * (y * y + z * z), 2.0f * (x * y + z * w), 2.0f * (x * z - y * w));
+    m.c[1] = p3(2.0f * (x * y - z * w), 1.0f - 2.0f * (x * x + z * z), 2.0f * (y * z + x * w));
+    m.c[2] = p3(2.0f * (x * z + y * w), 2.0f * (y * z - x * w), 1.0f - 2.0f * (x * x + y * y));
+    return m;
+}
+struct CP { P3 p; float s; };
+
+static int reduce4(CP* pts, int cnt, P3 n) {
+    if (cnt <= 4) return cnt;
+    int i0 = 0; for (int k = 1; k < cnt; k++) if (pts[k].s < pts[i0].s) i0 = k;
+    P3 q0 = pts[i0].p;
+    int i1 = 0; float best = -1.0f;
+    for (int k = 0; k < cnt; k++) { float d = plen2(pts[k].p - q0); if (d > best) { best = d; i1 = k; } }
+    P3 q1 = pts[i1].p;
+    P3 e = q1 - q0;
+    int i2 = 0; float b2 = -3.4028235e38f;
+    for (int k = 0; k < cnt; k++) { float a = pdot(pcross(pts[k].p - q0, e), n); if (a > b2) { b2 = a; i2 = k; } }
+    int i3 = 0; float b3 = -3.4028235e38f;
+    for (int k = 0; k < cnt; k++) { float a = -pdot(pcross(pts[k].p - q0, e), n); if (a > b3) { b3 = a; i3 = k; } }
+    int ids[4] = {i0, i1, i2, i3};
+    CP sel[4] = {pts[i0], pts[i1], pts[i2], pts[i3]};
+    int out = 0;
+    for (int k = 0; k < 4; k++) {
+        bool dup = false;
+        for (int t = 0; t < k; t++) if (ids[t] == ids[k]) dup = true;
+        if (dup) continue;
+        pts[out++] = sel[k];
+    }
+    return out;
+}
+
+// returns the point count (0 = separated); normal from A to B
+static int collide_boxes(P3 pa, const M3& ra, P3 ha, P3 pb, const M3& rb, P3 hb, float margin, CP* out, P3* nout) {
+    P3 t = pb - pa;
+    float ac[3][3];
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) ac[i][j] = fabs_(pdot(ra.c[i], rb.c[j])) + 1e-6f;
+    float hav[3] = {ha.x, ha.y, ha.z}, hbv[3] = {hb.x, hb.y, hb.z};
+    float sa = -3.4028235e38f; int ia = 0;
+    for (int i = 0; i < 3; i++) {
+        float s = fabs_(pdot(t, ra.c[i])) - (hav[i] + hbv[0] * ac[i][0] + hbv[1] * ac[i][1] + hbv[2] * ac[i][2]);
+        if (s > margin) return 0;
+        if (s > sa) { sa = s; ia = i; }
+    }
+    float sbm = -3.4028235e38f; int jb = 0;
+    for (int j = 0; j < 3; j++) {
+        float s = fabs_(pdot(t, rb.c[j])) - (hbv[j] + hav[0] * ac[0][j] + hav[1] * ac[1][j] + hav[2] * ac[2][j]);
+        if (s > margin) return 0;
+        if (s > sbm) { sbm = s; jb = j; }
+    }
+    float se = -3.4028235e38f; int ei = 0, ej = 0; P3 el = p3(0, 0, 0);
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) {
+        P3 l = pcross(ra.c[i], rb.c[j]);
+        float l2 = plen2(l);
+        if (l2 < 1e-8f) continue;
+        l = l * (1.0f / sqrt_e(l2));
+        float r = hav[0] * fabs_(pdot(ra.c[0], l)) + hav[1] * fabs_(pdot(ra.c[1], l)) + hav[2] * fabs_(pdot(ra.c[2], l))
+                + hbv[0] * fabs_(pdot(rb.c[0], l)) + hbv[1] * fabs_(pdot(rb.c[1], l)) + hbv[2] * fabs_(pdot(rb.c[2], l));
+        float s = fabs_(pdot(t, l)) - r;
+        if (s > margin) return 0;
+        if (s > se) { se = s; ei = i; ej = j; el = l; }
+    }
+    const float face_tol = 0.005f;
+    bool use_b = sbm > sa + face_tol;
+    float face_best = use_b ? sbm : sa;
+    if (se > face_best + 0.01f) {
+        P3 n = pdot(t, el) < 0.0f ? -el : el;
+        P3 ca = pa, cb = pb;
+        for (int k = 0; k < 3; k++) {
+            if (k != ei) { float s = pdot(ra.c[k], n) > 0.0f ? 1.0f : -1.0f; ca = ca + ra.c[k] * (s * hav[k]); }
+            if (k != ej) { float s = pdot(rb.c[k], n) > 0.0f ? -1.0f : 1.0f; cb = cb + rb.c[k] * (s * hbv[k]); }
+        }
+        P3 d1 = ra.c[ei], d2 = rb.c[ej];
+        P3 r = ca - cb;
+        float bb = pdot(d1, d2), c = pdot(d1, r), f = pdot(d2, r);
+        float den = 1.0f - bb * bb;
+        float s = den > 1e-6f ? (bb * f - c) / den : 0.0f;
+        s = std::fmin(std::fmax(s, -hav[ei]), hav[ei]);
+        float tt = bb * s + f;
+        tt = std::fmin(std::fmax(tt, -hbv[ej]), hbv[ej]);
+        s = std::fmin(std::fmax(bb * tt - c, -hav[ei]), hav[ei]);
+        P3 q1 = ca + d1 * s, q2 = cb + d2 * tt;
+        float sep = pdot(q2 - q1, n);
+        out[0].p = (q1 + q2) * 0.5f; out[0].s = sep;
+        *nout = n;
+        return 1;
+    }
+    P3 pr, pi; const M3 *rr, *ri; const float *hr, *hi; int k; bool flip;
+    if (use_b) { pr = pb; rr = &rb; hr = hbv; pi = pa; ri = &ra; hi = hav; k = jb; flip = true; }
+    else { pr = pa; rr = &ra; hr = hav; pi = pb; ri = &rb; hi = hbv; k = ia; flip = false; }
+    P3 n = rr->c[k];
+    if (pdot(pi - pr, n) < 0.0f) n = -n;
+    int j = 0; float bd = -1.0f;
+    for (int qq = 0; qq < 3; qq++) { float d = fabs_(pdot(ri->c[qq], n)); if (d > bd) { bd = d; j = qq; } }
+    float sgn = pdot(ri->c[j], n) > 0.0f ? -1.0f : 1.0f;
+    P3 fc = pi + ri->c[j] * (sgn * hi[j]);
+    int u = (j + 1) % 3, vq = (j + 2) % 3;
+    P3 eu = ri->c[u] * hi[u], ev = ri->c[vq] * hi[vq];
+    P3 poly[8], tmp[8];
+    poly[0] = fc + eu + ev; poly[1] = fc - eu + ev; poly[2] = fc - eu - ev; poly[3] = fc + eu - ev;
+    int pn = 4;
+    int u2 = (k + 1) % 3, v2 = (k + 2) % 3;
+    const int axs[4] = {u2, u2, v2, v2};
+    const float sg[4] = {1.0f, -1.0f, 1.0f, -1.0f};
+    for (int e = 0; e < 4; e++) {
+        P3 dir = rr->c[axs[e]] * sg[e];
+        float off = pdot(dir, pr) + hr[axs[e]];
+        int tn = 0;
+        for (int qq = 0; qq < pn; qq++) {
+            P3 p0 = poly[qq], p1 = poly[(qq + 1) % pn];
+            float d0 = pdot(p0, dir) - off, d1 = pdot(p1, dir) - off;
+            if (d0 <= 0.0f) { if (tn < 8) { tmp[tn++] = p0; } }
+            if ((d0 <= 0.0f) != (d1 <= 0.0f)) { float ttt = d0 / (d0 - d1); if (tn < 8) { tmp[tn++] = p0 + (p1 - p0) * ttt; } }
+        }
+        pn = tn;
+        for (int qq = 0; qq < pn; qq++) poly[qq] = tmp[qq];
+        if (pn == 0) return 0;
+    }
+    P3 rc = pr + n * hr[k];
+    int cnt = 0;
+    for (int qq = 0; qq < pn; qq++) {
+        P3 p = poly[qq];
+        float sep = pdot(p - rc, n);
+        if (sep <= margin) { out[cnt].p = p - n * (0.5f * sep); out[cnt].s = sep; cnt++; }
+    }
+    if (cnt == 0) return 0;
+    *nout = flip ? -n : n;
+    return cnt;
+}
+
+}  // namespace
+
+// ============================================================================================================
+// C interface for the tests (ctypes)
+// ============================================================================================================
+extern "C" {
+
+struct ow_step_params { uint32_t iterations, substeps, order, sleep_mode, pinch_kill; };
+
+void* ow_create(uint32_t n_static, const int32_t* static_xyz, const uint8_t* static_mat, const int32_t* static_sid,
+                const uint8_t* static_infill, uint32_t n_bodies, const uint32_t* body_first, const int32_t* body_brick_xyz,
+                const uint8_t* body_brick_mat, const float* body_pose) {
+    World* w = new World();
+    uint32_t nd = n_bodies ? body_first[n_bodies] : 0;
+    w->ns = n_static; w->nd = nd;
+    uint32_t nt = n_static + nd;
+    w->ctab.assign(NCT, 0);
+    w->mat.assign(nt, 0); w->infill.assign(nt, 0); w->bx.assign(nt, 0); w->by.assign(nt, 0); w->bz.assign(nt, 0);
+    w->sid.assign(nt, -1); w->body.assign(nt, STATIC); w->next.assign(nt, NONE); w->sup.assign(nt, 0);
+    w->local.assign(nt, vv(0, 0, 0)); w->wpos.assign(nt, vv(0, 0, 0));
+    w->nb6.assign((size_t)nt * 6, NONE); w->bond.assign((size_t)nt * 4, 0.0f); w->bmax.assign((size_t)nt * 4, 0.0f);
+    w->phi.assign(nt, 0.0f); w->ext.assign(nt, 0.0f); w->stress.assign(nt, 0.0f); w->phi64.assign(nt, 0.0);
+    w->hhead.assign(HSIZE, NONE); w->hnext.assign(nt, NONE);
+    for (uint32_t i = 0; i < n_static; i++) {
+        int x = static_xyz[3 * i], y = static_xyz[3 * i + 1], z = static_xyz[3 * i + 2];
+        uint8_t m = static_mat[i];
+        if (!inb(x, y, z) || w->gget(x, y, z) != 0) { delete w; return nullptr; }
+        w->mat[i] = m; w->bx[i] = x; w->by[i] = y; w->bz[i] = z; w->sid[i] = static_sid[i];
+        w->infill[i] = (m == GLASS || static_infill[i]) ? 1 : 0;
+        w->body[i] = STATIC;
+        w->gset(x, y, z, i + 1);
+        w->local[i] = lat_pos(x, y, z); w->wpos[i] = w->local[i];
+    }
+    for (uint32_t i = 0; i < n_static; i++) finalize_brick(*w, i);
+    w->nbody = n_bodies;
+    uint32_t nb = n_bodies;
+    w->alive.assign(nb, 0); w->asleep.assign(nb, 0); w->wake.assign(nb, 0);
+    w->first.assign(nb, NONE); w->count.assign(nb, 0); w->nc.assign(nb, 0);
+    w->pos.assign(nb, vv(0, 0, 0)); w->v = w->pos; w->w = w->pos; w->vpre = w->pos; w->wpre = w->pos;
+    w->q.assign((size_t)nb * 4, 0.0f); w->rot.assign((size_t)nb * 9, 0.0f); w->iil = w->rot; w->iiw = w->rot;
+    w->m.assign(nb, 0.0f); w->im = w->m; w->sleep = w->m; w->rad = w->m; w->maxr = w->m;
+    w->island.assign(nb, NONE);
+    std::vector<uint32_t> lst;
+    for (uint32_t b = 0; b < nb; b++) {
+        uint32_t s = body_first[b], e = body_first[b + 1];
+        if (e <= s) { delete w; return nullptr; }
+        lst.clear();
+        for (uint32_t k = s; k < e; k++) {
+            uint32_t i = n_static + k;
+            int x = body_brick_xyz[3 * k], y = body_brick_xyz[3 * k + 1], z = body_brick_xyz[3 * k + 2];
+            w->mat[i] = body_brick_mat[k]; w->bx[i] = x; w->by[i] = y; w->bz[i] = z; w->sid[i] = -1;
+            w->local[i] = lat_pos(x, y, z);
+            lst.push_back(i);
+        }
+        const float* ps = body_pose + (size_t)b * 13;
+        float prot[9];
+        q_to_m(ps + 3, prot);
+        setup_body(*w, b, lst.data(), (uint32_t)lst.size(), vv(ps[0], ps[1], ps[2]), prot, ps + 3, vv(ps[7], ps[8], ps[9]), vv(ps[10], ps[11], ps[12]));
+    }
+    return w;
+}
+void ow_destroy(void* h) { delete (World*)h; }
+
+void ow_counts(void* h, uint64_t* out) {
+    World* w = (World*)h;
+    out[0] = w->ns; out[1] = w->nd; out[2] = w->nbody; out[3] = w->cs.size(); out[4] = w->man_a.size();
+    out[5] = w->ncolors; out[6] = w->would_drop; out[7] = w->frame; out[8] = w->ncpool;
+}
+
+// body state: pos3 q4 v3 w3 (13 floats), plus sleep timer; flags bit0 alive, bit1 asleep
+void ow_get_bodies(void* h, float* state13, float* sleep, uint8_t* flags) {
+    World* w = (World*)h;
+    for (uint32_t b = 0; b < w->nbody; b++) {
+        float* s = state13 + (size_t)b * 13;
+        for (int k = 0; k < 3; k++) { s[k] = w->pos[b][k]; s[7 + k] = w->v[b][k]; s[10 + k] = w->w[b][k]; }
+        for (int k = 0; k < 4; k++) s[3 + k] = w->q[(size_t)b * 4 + k];
+        sleep[b] = w->sleep[b];
+        flags[b] = (w->alive[b] ? 1 : 0) | (w->asleep[b] ? 2 : 0);
+    }
+}
+void ow_set_bodies(void* h, const float* state13, const float* sleep, const uint8_t* flags) {
+    World* w = (World*)h;
+    for (uint32_t b = 0; b < w->nbody; b++) {
+        const float* s = state13 + (size_t)b * 13;
+        for (int k = 0; k < 3; k++) { w->pos[b][k] = s[k]; w->v[b][k] = s[7 + k]; w->w[b][k] = s[10 + k]; }
+        for (int k = 0; k < 4; k++) w->q[(size_t)b * 4 + k] = s[3 + k];
+        w->sleep[b] = sleep[b];
+        bool was = w->alive[b];
+        w->alive[b] = flags[b] & 1; w->asleep[b] = (flags[b] >> 1) & 1;
+        if (was && !w->alive[b]) kill_body(*w, b);
+    }
+}
+// per-body setup: m, im, rad, iil9 (12 floats); per body brick: local3
+void ow_get_setup(void* h, float* body12, float* local3) {
+    World* w = (World*)h;
+    for (uint32_t b = 0; b < w->nbody; b++) {
+        float* s = body12 + (size_t)b * 12;
+        s[0] = w->m[b]; s[1] = w->im[b]; s[2] = w->rad[b];
+        for (int k = 0; k < 9; k++) s[3 + k] = w->iil[(size_t)b * 9 + k];
+    }
+    for (uint32_t k = 0; k < w->nd; k++) for (int c = 0; c < 3; c++) local3[(size_t)k * 3 + c] = w->local[w->ns + k][c];
+}
+void ow_get_wpos(void* h, float* wpos3) {
+    World* w = (World*)h;
+    for (uint32_t k = 0; k < w->nd; k++) for (int c = 0; c < 3; c++) wpos3[(size_t)k * 3 + c] = w->wpos[w->ns + k][c];
+}
+void ow_get_bonds(void* h, float* bond4, uint32_t* nb6) {
+    World* w = (World*)h;
+    for (uint32_t i = 0; i < w->ns; i++) {
+        for (int k = 0; k < 4; k++) bond4[(size_t)i * 4 + k] = w->bond[(size_t)i * 4 + k];
+        for (int k = 0; k < 6; k++) nb6[(size_t)i * 6 + k] = w->nb6[(size_t)i * 6 + k];
+    }
+}
+
+void ow_step(void* h, float dt, const ow_step_params* p) {
+    StepParams P{p->iterations, p->substeps, p->order, p->sleep_mode, p->pinch_kill};
+    step(*(World*)h, dt, P);
+}
+// substep pieces for per-phase parity: update_cache + gravity + hash + contacts (+ prep)
+void ow_contacts_only(void* h, float hsub, int with_prep) {
+    World* w = (World*)h;
+    update_cache(*w);
+    for (uint32_t b = 0; b < w->nbody; b++) if (w->alive[b] && !w->asleep[b]) w->v[b][1] -= GR * hsub;
+    build_hash(*w);
+    gen_contacts(*w);
+    if (with_prep) prep_contacts(*w, hsub);
+    build_manifolds(*w);
+    islands(*w);
+}
+
+// contacts in list order. ids: a, b, bo, ba, bb (5 u32); f: p3 n3 depth (7 floats); s: jn jt1 jt2 mn mt1 mt2 bias vn0 (8)
+uint64_t ow_get_contacts(void* h, uint32_t* ids, float* f, float* s) {
+    World* w = (World*)h;
+    for (size_t k = 0; k < w->cs.size(); k++) {
+        const Contact& c = w->cs[k];
+        uint32_t* o = ids + k * 5; o[0] = c.a; o[1] = c.b; o[2] = c.bo; o[3] = c.ba; o[4] = c.bb;
+        float* g = f + k * 7; for (int t = 0; t < 3; t++) { g[t] = c.p[t]; g[3 + t] = c.n[t]; } g[6] = c.depth;
+        float* x = s + k * 8; x[0] = c.jn; x[1] = c.jt1; x[2] = c.jt2; x[3] = c.mn; x[4] = c.mt1; x[5] = c.mt2; x[6] = c.bias; x[7] = c.vn0;
+    }
+    return w->cs.size();
+}
+void ow_get_islands(void* h, uint32_t* label) { World* w = (World*)h; for (uint32_t b = 0; b < w->nbody; b++) label[b] = w->island[b]; }
+// manifolds: a, b, colour, count (4 u32 each), in manifold order
+uint64_t ow_get_manifolds(void* h, uint32_t* out4) {
+    World* w = (World*)h;
+    for (size_t m = 0; m < w->man_a.size(); m++) {
+        out4[m * 4] = w->man_a[m]; out4[m * 4 + 1] = w->man_b[m]; out4[m * 4 + 2] = w->man_color[m]; out4[m * 4 + 3] = w->man_count[m];
+    }
+    return w->man_a.size();
+}
+
+// ---- load path
+double ow_sor(void* h, int32_t s, float omega, double tol, uint32_t max_sweeps, int32_t mode, uint32_t* sweeps) {
+    SorResult r = sor_solve(*(World*)h, s, omega, tol, max_sweeps, mode);
+    if (sweeps) *sweeps = r.sweeps;
+    return r.resid;
+}
+void ow_get_phi(void* h, float* phi) { World* w = (World*)h; for (uint32_t i = 0; i < w->ns; i++) phi[i] = w->phi[i]; }
+void ow_get_phi64(void* h, double* phi) { World* w = (World*)h; for (uint32_t i = 0; i < w->ns; i++) phi[i] = w->phi64[i]; }
+void ow_set_phi(void* h, const float* phi) { World* w = (World*)h; for (uint32_t i = 0; i < w->ns; i++) { w->phi[i] = phi[i]; w->phi64[i] = phi[i]; } }
+void ow_set_ext(void* h, const float* ext) { World* w = (World*)h; for (uint32_t i = 0; i < w->ns; i++) w->ext[i] = ext[i]; }
+// joints: i, axis, j, decision, crushed (5 u32) + ratio, bond_after (2 floats). Returns the count; maxr in *maxr.
+uint64_t ow_stress(void* h, int32_t s, float dt, int32_t live, uint64_t cap, uint32_t* ids, float* vals, float* maxr) {
+    World* w = (World*)h;
+    std::vector<Joint> out;
+    float mr = 0.0f;
+    w->crush_n = 0;
+    for (uint32_t i = 0; i < w->ns; i++) if (w->in_struct(i, s)) w->stress[i] = 0.0f;
+    for (uint32_t i = 0; i < w->ns; i++) if (w->in_struct(i, s)) { float r = stress_brick(*w, i, dt, live != 0, out); if (r > mr) mr = r; }
+    if (maxr) *maxr = mr;
+    for (size_t k = 0; k < out.size() && k < cap; k++) {
+        uint32_t* o = ids + k * 5; o[0] = out[k].i; o[1] = out[k].axis; o[2] = out[k].j; o[3] = out[k].decision; o[4] = out[k].crushed;
+        vals[k * 2] = out[k].ratio; vals[k * 2 + 1] = out[k].bond_after;
+    }
+    return out.size();
+}
+void ow_remove_static(void* h, uint32_t i) {
+    World* w = (World*)h;
+    if (i >= w->ns || w->mat[i] == 0) return;
+    w->gset(w->bx[i], w->by[i], w->bz[i], 0);
+    w->mat[i] = 0;
+}
+
+// ---- box SAT: boxes are p3 q4 h3 (10 floats). Output: normal3 + up to 8 points (p3, sep), reduced to 4.
+int32_t ow_collide_boxes(const float* A, const float* B, float margin, int32_t do_reduce, float* out) {
+    P3 pa = p3(A[0], A[1], A[2]), pb = p3(B[0], B[1], B[2]);
+    M3 ra = quat_m3(A + 3), rb = quat_m3(B + 3);
+    CP pts[8]; P3 n;
+    int cnt = collide_boxes(pa, ra, p3(A[7], A[8], A[9]), pb, rb, p3(B[7], B[8], B[9]), margin, pts, &n);
+    if (cnt == 0) return 0;
+    if (do_reduce) cnt = reduce4(pts, cnt, n);
+    out[0] = n.x; out[1] = n.y; out[2] = n.z;
+    for (int k = 0; k < cnt; k++) { out[3 + 4 * k] = pts[k].p.x; out[4 + 4 * k] = pts[k].p.y; out[5 + 4 * k] = pts[k].p.z; out[6 + 4 * k] = pts[k].s; }
+    return cnt;
+}
+
+}  // extern "C"

@@ -1,0 +1,355 @@
+"""shatterforge_b200 — B200 (sm_100a) implementation of Shatterforge's per-step physics path.
+
+Python face of the C ABI in include/sf.h (loaded with ctypes from the in-tree shared library). The calls mirror
+the reference engine's entry points:
+
+    World.step(dt)             the rigid part of `step(dt)` (src/lib.rs:3640-3651)
+    World.structure_solve()    the load-path sweeps of `structural` / `warm_step` (src/lib.rs:1005-1079)
+    World.structure_check()    the joint pass of `structural` (stress_brick, src/lib.rs:1153-1227)
+
+Errors raise SfError carrying the sf_status code; nothing falls back to a CPU path — if the library or a CUDA
+device is missing, the call fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+from .scenes import Scene  # noqa: F401
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_lib" / "libsf_b200.so"
+
+SF_OK, SF_ERR_ARG, SF_ERR_CAPACITY, SF_ERR_CUDA, SF_ERR_TIMEOUT, SF_ERR_BUDGET, SF_ERR_STATE, SF_ERR_VERIFY = range(8)
+SF_SLEEP_BODY, SF_SLEEP_ISLAND = 0, 1
+STATIC = 0xFFFFFFFF
+J_HOLD, J_FATIGUE, J_FAIL, J_CRUSH, J_ABSENT = 0, 1, 2, 3, 255
+
+_u8p = C.POINTER(C.c_uint8)
+_u32p = C.POINTER(C.c_uint32)
+_i32p = C.POINTER(C.c_int32)
+_f32p = C.POINTER(C.c_float)
+
+
+class SfError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        super().__init__(f"{what}: status {status} ({_status_name(status)}): {last_error()}")
+        self.status = status
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("n_static", C.c_uint32), ("static_xyz", _i32p), ("static_mat", _u8p), ("static_sid", _i32p),
+                ("static_infill", _u8p), ("n_bodies", C.c_uint32), ("body_first", _u32p), ("body_brick_xyz", _i32p),
+                ("body_brick_mat", _u8p), ("body_pose", _f32p)]
+
+
+class WorldDesc(C.Structure):
+    _fields_ = [("n_scenes", C.c_uint32), ("scenes", C.POINTER(SceneDesc)), ("structure_offset_per_scene", C.c_int32)]
+
+
+class Params(C.Structure):
+    _fields_ = [("substeps", C.c_uint32), ("iterations", C.c_uint32), ("sleep_mode", C.c_uint32),
+                ("pinch_kill", C.c_uint32), ("max_colors", C.c_uint32), ("contact_capacity", C.c_uint32),
+                ("verify", C.c_uint32), ("solve_blocks", C.c_uint32), ("reserved", C.c_uint32 * 8)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("contacts", C.c_uint64), ("manifolds", C.c_uint64), ("ref_would_drop", C.c_uint64),
+                ("colors", C.c_uint32), ("color_rounds", C.c_uint32), ("islands", C.c_uint32), ("alive", C.c_uint32),
+                ("awake", C.c_uint32), ("error_word", C.c_uint32), ("contact_capacity", C.c_uint64),
+                ("ms_last_step", C.c_double)]
+
+
+class SolveReport(C.Structure):
+    _fields_ = [("structures", C.c_uint32), ("max_sweeps_done", C.c_uint32), ("brick_sweeps", C.c_uint64),
+                ("max_residual", C.c_double), ("ms", C.c_double)]
+
+
+class CheckReport(C.Structure):
+    _fields_ = [("joints", C.c_uint64), ("over", C.c_uint64), ("failed", C.c_uint64), ("crushed", C.c_uint64),
+                ("max_ratio", C.c_float), ("ms", C.c_double)]
+
+
+class WorldInfo(C.Structure):
+    _fields_ = [("n_scenes", C.c_uint32), ("n_static", C.c_uint32), ("n_bodies", C.c_uint32),
+                ("n_body_bricks", C.c_uint32), ("n_structures", C.c_uint32), ("n_chunks", C.c_uint32)]
+
+
+# every exported function: name -> (restype, argtypes)
+PROTOTYPES = {
+    "sf_params_default": (None, [C.POINTER(Params)]),
+    "sf_world_create": (C.c_int32, [C.POINTER(WorldDesc), C.POINTER(Params), C.POINTER(C.c_void_p)]),
+    "sf_world_destroy": (None, [C.c_void_p]),
+    "sf_status_string": (C.c_char_p, [C.c_int32]),
+    "sf_last_error": (C.c_char_p, []),
+    "sf_version": (C.c_int32, []),
+    "sf_world_step": (C.c_int32, [C.c_void_p, C.c_float, C.c_uint32]),
+    "sf_structure_solve": (C.c_int32, [C.c_void_p, C.c_int32, C.c_float, C.c_float, C.c_uint32, C.POINTER(SolveReport)]),
+    "sf_structure_check": (C.c_int32, [C.c_void_p, C.c_int32, C.c_float, C.c_int32, C.POINTER(CheckReport)]),
+    "sf_read_solve_detail": (C.c_int32, [C.c_void_p, _u32p, C.POINTER(C.c_double)]),
+    "sf_world_get_info": (C.c_int32, [C.c_void_p, C.POINTER(WorldInfo)]),
+    "sf_get_stats": (C.c_int32, [C.c_void_p, C.POINTER(Stats)]),
+    "sf_read_bodies": (C.c_int32, [C.c_void_p, _f32p, _f32p, _u8p]),
+    "sf_write_bodies": (C.c_int32, [C.c_void_p, _f32p, _f32p, _u8p]),
+    "sf_read_body_setup": (C.c_int32, [C.c_void_p, _f32p, _f32p]),
+    "sf_read_brick_positions": (C.c_int32, [C.c_void_p, _f32p]),
+    "sf_read_contacts": (C.c_int32, [C.c_void_p, C.c_uint32, _u32p, _f32p, _f32p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "sf_read_manifolds": (C.c_int32, [C.c_void_p, C.c_uint32, _u32p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "sf_read_islands": (C.c_int32, [C.c_void_p, _u32p]),
+    "sf_read_phi": (C.c_int32, [C.c_void_p, _f32p]),
+    "sf_read_phi64": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
+    "sf_write_phi": (C.c_int32, [C.c_void_p, _f32p]),
+    "sf_write_ext": (C.c_int32, [C.c_void_p, _f32p]),
+    "sf_read_ext": (C.c_int32, [C.c_void_p, _f32p]),
+    "sf_read_bonds": (C.c_int32, [C.c_void_p, _f32p, _u32p, _u8p]),
+    "sf_read_joints": (C.c_int32, [C.c_void_p, _f32p, _f32p, _u8p, _u32p]),
+    "sf_collide_boxes": (C.c_int32, [_f32p, _f32p, C.c_uint32, C.c_float, _f32p, _i32p]),
+}
+
+_lib = None
+
+
+def library_path() -> Path:
+    return Path(os.environ.get("SF_B200_LIB", LIB_PATH))
+
+
+def load(build_if_missing: bool = True) -> C.CDLL:
+    """Load the sm_100a library (building it first if the sources are newer and nvcc is present)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if build_if_missing and "SF_B200_LIB" not in os.environ:
+        from . import build as _b
+        try:
+            if _b.needs_build():
+                _b.build()
+        except RuntimeError:
+            if not path.exists():
+                raise
+    if not path.exists():
+        raise FileNotFoundError(f"{path} is missing: build it with python -m shatterforge_b200.build")
+    lib = C.CDLL(str(path))
+    for name, (res, args) in PROTOTYPES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    try:
+        return (load().sf_last_error() or b"").decode()
+    except Exception:  # pragma: no cover - only when the library itself cannot load
+        return ""
+
+
+def _status_name(s: int) -> str:
+    names = ["ok", "bad argument", "capacity exceeded", "CUDA error", "device wait timed out",
+             "memory budget exceeded", "call out of order", "device self-check failed"]
+    return names[s] if 0 <= s < len(names) else "unknown"
+
+
+def _check(status: int, what: str) -> None:
+    if status != SF_OK:
+        raise SfError(status, what)
+
+
+def _ptr(a: np.ndarray, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    load().sf_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class World:
+    """A set of independent scenes resident on the GPU, stepped together (one launch per phase for all)."""
+
+    def __init__(self, scenes, params: Params | None = None, **param_kw):
+        lib = load()
+        self._lib = lib
+        if isinstance(scenes, Scene):
+            scenes = [scenes]
+        self.scenes = [s.contiguous() for s in scenes]
+        descs = (SceneDesc * len(self.scenes))()
+        for d, s in zip(descs, self.scenes):
+            d.n_static = s.n_static
+            d.static_xyz = _ptr(s.static_xyz, C.c_int32)
+            d.static_mat = _ptr(s.static_mat, C.c_uint8)
+            d.static_sid = _ptr(s.static_sid, C.c_int32)
+            d.static_infill = _ptr(s.static_infill, C.c_uint8)
+            d.n_bodies = s.n_bodies
+            d.body_first = _ptr(s.body_first, C.c_uint32)
+            d.body_brick_xyz = _ptr(s.body_brick_xyz, C.c_int32)
+            d.body_brick_mat = _ptr(s.body_brick_mat, C.c_uint8)
+            d.body_pose = _ptr(s.body_pose, C.c_float)
+        wd = WorldDesc(len(self.scenes), descs, 0)
+        self.params = params if params is not None else default_params(**param_kw)
+        h = C.c_void_p()
+        _check(lib.sf_world_create(C.byref(wd), C.byref(self.params), C.byref(h)), "sf_world_create")
+        self._h = h
+        info = WorldInfo()
+        _check(lib.sf_world_get_info(h, C.byref(info)), "sf_world_get_info")
+        self.info = info
+        self.static_off = np.cumsum([0] + [s.n_static for s in self.scenes])
+        self.body_off = np.cumsum([0] + [s.n_bodies for s in self.scenes])
+        self.brick_off = np.cumsum([0] + [s.n_body_bricks for s in self.scenes])
+
+    # -- lifecycle
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sf_world_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- hot path
+    def step(self, dt: float = 1.0 / 60.0, nsteps: int = 1) -> "Stats":
+        _check(self._lib.sf_world_step(self._h, float(dt), int(nsteps)), "sf_world_step")
+        return self.stats()
+
+    def structure_solve(self, structure: int = -1, omega: float = 1.7, tol: float = 1e-6, max_sweeps: int = 20000) -> SolveReport:
+        r = SolveReport()
+        _check(self._lib.sf_structure_solve(self._h, int(structure), float(omega), float(tol), int(max_sweeps), C.byref(r)),
+               "sf_structure_solve")
+        return r
+
+    def solve_detail(self):
+        n = self.info.n_structures
+        sw = np.zeros(max(n, 1), np.uint32)
+        rs = np.zeros(max(n, 1), np.float64)
+        _check(self._lib.sf_read_solve_detail(self._h, _ptr(sw, C.c_uint32), _ptr(rs, C.c_double)), "sf_read_solve_detail")
+        return sw[:n], rs[:n]
+
+    def structure_check(self, structure: int = -1, dt: float = 1.0 / 60.0, live: bool = True) -> CheckReport:
+        r = CheckReport()
+        _check(self._lib.sf_structure_check(self._h, int(structure), float(dt), 1 if live else 0, C.byref(r)),
+               "sf_structure_check")
+        return r
+
+    # -- read-outs
+    def stats(self) -> Stats:
+        s = Stats()
+        _check(self._lib.sf_get_stats(self._h, C.byref(s)), "sf_get_stats")
+        return s
+
+    def bodies(self):
+        nb = self.info.n_bodies
+        st = np.zeros((nb, 13), np.float32)
+        sl = np.zeros(nb, np.float32)
+        fl = np.zeros(nb, np.uint8)
+        _check(self._lib.sf_read_bodies(self._h, _ptr(st, C.c_float), _ptr(sl, C.c_float), _ptr(fl, C.c_uint8)), "sf_read_bodies")
+        return st, sl, fl
+
+    def set_bodies(self, state13, sleep, flags):
+        st = np.ascontiguousarray(state13, np.float32)
+        sl = np.ascontiguousarray(sleep, np.float32)
+        fl = np.ascontiguousarray(flags, np.uint8)
+        _check(self._lib.sf_write_bodies(self._h, _ptr(st, C.c_float), _ptr(sl, C.c_float), _ptr(fl, C.c_uint8)), "sf_write_bodies")
+
+    def body_setup(self):
+        b12 = np.zeros((self.info.n_bodies, 12), np.float32)
+        l3 = np.zeros((self.info.n_body_bricks, 3), np.float32)
+        _check(self._lib.sf_read_body_setup(self._h, _ptr(b12, C.c_float), _ptr(l3, C.c_float)), "sf_read_body_setup")
+        return b12, l3
+
+    def brick_positions(self):
+        p = np.zeros((self.info.n_body_bricks, 3), np.float32)
+        _check(self._lib.sf_read_brick_positions(self._h, _ptr(p, C.c_float)), "sf_read_brick_positions")
+        return p
+
+    def contacts(self, scene: int = 0):
+        n = C.c_uint64()
+        _check(self._lib.sf_read_contacts(self._h, scene, None, None, None, 0, C.byref(n)), "sf_read_contacts")
+        k = n.value
+        ids = np.zeros((k, 5), np.uint32)
+        f = np.zeros((k, 7), np.float32)
+        s = np.zeros((k, 8), np.float32)
+        _check(self._lib.sf_read_contacts(self._h, scene, _ptr(ids, C.c_uint32), _ptr(f, C.c_float), _ptr(s, C.c_float), k,
+                                          C.byref(n)), "sf_read_contacts")
+        return ids, f, s
+
+    def manifolds(self, scene: int = 0):
+        n = C.c_uint64()
+        _check(self._lib.sf_read_manifolds(self._h, scene, None, 0, C.byref(n)), "sf_read_manifolds")
+        out = np.zeros((n.value, 4), np.uint32)
+        _check(self._lib.sf_read_manifolds(self._h, scene, _ptr(out, C.c_uint32), n.value, C.byref(n)), "sf_read_manifolds")
+        return out
+
+    def islands(self):
+        lab = np.zeros(self.info.n_bodies, np.uint32)
+        _check(self._lib.sf_read_islands(self._h, _ptr(lab, C.c_uint32)), "sf_read_islands")
+        return lab
+
+    def phi(self):
+        p = np.zeros(self.info.n_static, np.float32)
+        _check(self._lib.sf_read_phi(self._h, _ptr(p, C.c_float)), "sf_read_phi")
+        return p
+
+    def phi64(self):
+        p = np.zeros(self.info.n_static, np.float64)
+        _check(self._lib.sf_read_phi64(self._h, _ptr(p, C.c_double)), "sf_read_phi64")
+        return p
+
+    def set_phi(self, phi):
+        p = np.ascontiguousarray(phi, np.float32)
+        _check(self._lib.sf_write_phi(self._h, _ptr(p, C.c_float)), "sf_write_phi")
+
+    def set_ext(self, ext):
+        e = np.ascontiguousarray(ext, np.float32)
+        _check(self._lib.sf_write_ext(self._h, _ptr(e, C.c_float)), "sf_write_ext")
+
+    def ext(self):
+        e = np.zeros(self.info.n_static, np.float32)
+        _check(self._lib.sf_read_ext(self._h, _ptr(e, C.c_float)), "sf_read_ext")
+        return e
+
+    def bonds(self):
+        ns = self.info.n_static
+        b = np.zeros((ns, 4), np.float32)
+        nb = np.zeros((ns, 6), np.uint32)
+        m = np.zeros(ns, np.uint8)
+        _check(self._lib.sf_read_bonds(self._h, _ptr(b, C.c_float), _ptr(nb, C.c_uint32), _ptr(m, C.c_uint8)), "sf_read_bonds")
+        return b, nb, m
+
+    def joints(self):
+        ns = self.info.n_static
+        r = np.zeros((ns, 4), np.float32)
+        b = np.zeros((ns, 4), np.float32)
+        d = np.zeros((ns, 4), np.uint8)
+        k = np.zeros((ns, 4), np.uint32)
+        _check(self._lib.sf_read_joints(self._h, _ptr(r, C.c_float), _ptr(b, C.c_float), _ptr(d, C.c_uint8), _ptr(k, C.c_uint32)),
+               "sf_read_joints")
+        return r, b, d, k
+
+
+def collide_boxes(boxes_a: np.ndarray, boxes_b: np.ndarray, margin: float = 0.02):
+    """Batched box-box SAT (engine/src/phys.rs:502-628): returns (count[n], normal[n,3], points[n,4,4])."""
+    lib = load()
+    a = np.ascontiguousarray(boxes_a, np.float32).reshape(-1, 10)
+    b = np.ascontiguousarray(boxes_b, np.float32).reshape(-1, 10)
+    n = a.shape[0]
+    out = np.zeros((n, 20), np.float32)
+    cnt = np.zeros(n, np.int32)
+    _check(lib.sf_collide_boxes(_ptr(a, C.c_float), _ptr(b, C.c_float), n, float(margin), _ptr(out, C.c_float),
+                                _ptr(cnt, C.c_int32)), "sf_collide_boxes")
+    return cnt, out[:, :3], out[:, 4:].reshape(n, 4, 4)

@@ -1,0 +1,257 @@
+// Internal declarations of the B200 physics library: constants, f32 helpers in the reference's evaluation order,
+// device buffers and the world object. Every physics kernel is compiled with --fmad=false so each multiply and
+// add rounds separately, as the reference's wasm32 f32 code does; together with the evaluation order below this
+// makes the device arithmetic op-for-op equal to the reference's.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/sf.h"
+
+namespace sf {
+
+// ---------------------------------------------------------------- constants (src/lib.rs:110-215)
+constexpr float S = 0.5f, H = 0.25f, RB = 0.27f, GR = 9.81f, MU = 0.65f, GROUNDK = 4.0f;
+constexpr int NX = 640, NY = 136, NZ = 640, CXN = NX / 8, CYN = NY / 8, CZN = NZ / 8, NCT = CXN * CYN * CZN;
+constexpr uint32_t HSIZE = 32768;
+constexpr uint32_t NONE = 0xFFFFFFFFu;
+constexpr uint32_t STATIC = 0xFFFFFFFFu;
+constexpr uint8_t GLASS = 4, SLUG = 6;
+constexpr int MAXCOL = 128;
+
+struct MatTables {
+    float mass[9], capv[9], caph[9], tens[9], stiff[9], duct[9];
+    float gk[9];       // GROUNDK * STIFF[m], rounded once as the reference computes it
+};
+void host_mat_tables(MatTables &t);
+// each translation unit that reads the tables holds its own copy and uploads it at world creation
+static __constant__ MatTables c_mat;
+static inline cudaError_t upload_mat_tables(cudaStream_t s) {
+    MatTables t;
+    host_mat_tables(t);
+    return cudaMemcpyToSymbolAsync(c_mat, &t, sizeof t, 0, cudaMemcpyHostToDevice, s);
+}
+
+// error bits of the device error word
+enum : uint32_t {
+    ERR_TIMEOUT = 1u << 0,
+    ERR_CAPACITY_CONTACTS = 1u << 1,
+    ERR_CAPACITY_COLORS = 1u << 2,
+    ERR_VERIFY_COLOR = 1u << 3,
+    ERR_JP_ROUNDS = 1u << 4,
+    ERR_SOR_NONFINITE = 1u << 5,
+};
+
+// ---------------------------------------------------------------- f32 helpers (src/lib.rs:25-108 order)
+struct V3 { float x, y, z; };
+__host__ __device__ __forceinline__ V3 v3(float a, float b, float c) { V3 r; r.x = a; r.y = b; r.z = c; return r; }
+__host__ __device__ __forceinline__ float minf(float a, float b) { return a < b ? a : b; }
+__host__ __device__ __forceinline__ float maxf(float a, float b) { return a > b ? a : b; }
+__host__ __device__ __forceinline__ float clampf(float x, float a, float b) { return minf(maxf(x, a), b); }
+__host__ __device__ __forceinline__ V3 add(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__host__ __device__ __forceinline__ V3 sub(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__host__ __device__ __forceinline__ V3 mul(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ __forceinline__ V3 madd(V3 a, V3 b, float s) { return v3(a.x + b.x * s, a.y + b.y * s, a.z + b.z * s); }
+__host__ __device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ __forceinline__ V3 cross(V3 a, V3 b) {
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float sqrt_rn(float x) { return __fsqrt_rn(x); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float len(V3 a) { return __fsqrt_rn(dot(a, a)); }
+__host__ __device__ __forceinline__ float fabs_bits(float x) { return fabsf(x); }
+__host__ __device__ __forceinline__ V3 mv(const float *m, V3 v) {
+    return v3(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[3] * v.x + m[4] * v.y + m[5] * v.z, m[6] * v.x + m[7] * v.y + m[8] * v.z);
+}
+__host__ __device__ __forceinline__ void mmul(const float *a, const float *b, float *r) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) r[i * 3 + j] = a[i * 3] * b[j] + a[i * 3 + 1] * b[3 + j] + a[i * 3 + 2] * b[6 + j];
+}
+__host__ __device__ __forceinline__ void mtr(const float *a, float *r) {
+    r[0] = a[0]; r[1] = a[3]; r[2] = a[6]; r[3] = a[1]; r[4] = a[4]; r[5] = a[7]; r[6] = a[2]; r[7] = a[5]; r[8] = a[8];
+}
+__host__ __device__ __forceinline__ void q_to_m(float x, float y, float z, float w, float *r) {
+    r[0] = 1.0f - 2.0f * (y * y + z * z); r[1] = 2.0f * (x * y - z * w); r[2] = 2.0f * (x * z + y * w);
+    r[3] = 2.0f * (x * y + z * w); r[4] = 1.0f - 2.0f * (x * x + z * z); r[5] = 2.0f * (y * z - x * w);
+    r[6] = 2.0f * (x * z - y * w); r[7] = 2.0f * (y * z + x * w); r[8] = 1.0f - 2.0f * (x * x + y * y);
+}
+__host__ __device__ __forceinline__ V3 lat_pos(int x, int y, int z) {
+    return v3((float)(x - NX / 2) * S + H, (float)y * S + H, (float)(z - NZ / 2) * S + H);
+}
+__host__ __device__ __forceinline__ uint32_t hkey(int x, int y, int z) {
+    return ((uint32_t)x * 73856093u ^ (uint32_t)y * 19349663u ^ (uint32_t)z * 83492791u) & (HSIZE - 1);
+}
+__host__ __device__ __forceinline__ uint32_t pair_priority(uint32_t a, uint32_t bp) {
+    uint32_t h = a * 0x9E3779B1u + bp * 0x85EBCA6Bu;
+    h ^= h >> 16; h *= 0x7FEB352Du; h ^= h >> 15; h *= 0x846CA68Bu; h ^= h >> 16;
+    return h;
+}
+__host__ __device__ __forceinline__ uint32_t pack_cell(int x, int y, int z) {
+    return (uint32_t)x | ((uint32_t)y << 10) | ((uint32_t)z << 18);
+}
+__host__ __device__ __forceinline__ void unpack_cell(uint32_t c, int &x, int &y, int &z) {
+    x = (int)(c & 1023u); y = (int)((c >> 10) & 255u); z = (int)(c >> 18);
+}
+__host__ __device__ __forceinline__ uint32_t chunk_slot(int x, int y, int z) { return (uint32_t)(((y >> 3) * CZN + (z >> 3)) * CXN + (x >> 3)); }
+__host__ __device__ __forceinline__ uint32_t cell_in_chunk(int x, int y, int z) { return (uint32_t)(((y & 7) * 8 + (z & 7)) * 8 + (x & 7)); }
+__host__ __device__ __forceinline__ bool inb(int x, int y, int z) { return x >= 0 && y >= 0 && z >= 0 && x < NX && y < NY && z < NZ; }
+
+// ---------------------------------------------------------------- device buffers
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    ~DBuf() { release(); }
+    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+    cudaError_t alloc(size_t count) {
+        if (count <= n && p) return cudaSuccess;
+        release();
+        size_t c = count ? count : 1;
+        cudaError_t e = cudaMalloc((void **)&p, c * sizeof(T));
+        if (e == cudaSuccess) n = c; else p = nullptr;
+        return e;
+    }
+    cudaError_t grow(size_t count) { return count <= n && p ? cudaSuccess : alloc(count + count / 4 + 1024); }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// persistent-kernel grid barrier state (bounded spin, see grid_sync)
+struct GridBarrier { unsigned count; unsigned gen; };
+
+struct SorState;     // sf_sor.cu
+struct StepState;    // sf_step.cu
+
+struct Scene {
+    uint32_t static_off, n_static;
+    uint32_t body_off, n_bodies;
+    uint32_t brick_off, n_bricks;
+    uint32_t chunk_off, n_chunks;
+};
+
+}  // namespace sf
+
+struct sf_world {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    sf_params P{};
+    uint32_t n_scenes = 0, ns = 0, nd = 0, nb = 0, n_struct = 0, n_chunks = 0;
+    uint32_t frame = 0;
+    std::vector<sf::Scene> scenes;
+
+    // static grid: per scene chunk table (NCT entries, global chunk index + 1) and chunk pool (static id + 1)
+    sf::DBuf<uint32_t> ctab, cpool;
+    std::vector<uint32_t> h_chunk_cell;  // per chunk: packed lattice origin
+    std::vector<uint32_t> h_chunk_scene;
+    // static bricks
+    sf::DBuf<uint32_t> s_cell, s_scene, s_nb6;
+    sf::DBuf<uint8_t> s_mat, s_infill;
+    sf::DBuf<int32_t> s_sid;
+    sf::DBuf<float> s_bond, s_bmax, s_phi, s_ext, s_stress;
+    sf::DBuf<double> s_phi64;        // the solver's potential; s_phi is its f32 copy (the reference's type)
+    std::vector<int32_t> h_sid;
+    std::vector<uint32_t> h_s_cell;
+    // bodies
+    sf::DBuf<float4> b_pos, b_q, b_v, b_w, b_vpre, b_wpre;
+    sf::DBuf<float> b_rot, b_iil, b_iiw, b_m, b_im, b_rad, b_sleep, b_maxr;
+    sf::DBuf<uint8_t> b_alive, b_asleep, b_wake;
+    sf::DBuf<uint32_t> b_first, b_count, b_nc, b_scene;
+    // body bricks
+    sf::DBuf<float4> k_local, k_wpos;
+    sf::DBuf<uint32_t> k_body;
+    sf::DBuf<uint8_t> k_mat;
+    sf::DBuf<int32_t> k_xyz;
+
+    sf::DBuf<uint32_t> err;      // [0] error bits, [1..] counters
+    sf::DBuf<sf::GridBarrier> barrier;
+
+    sf::SorState *sor = nullptr;
+    sf::StepState *step = nullptr;
+    sf_stats stats{};
+};
+
+namespace sf {
+// error helpers
+void set_error(const char *fmt, ...);
+#define SF_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            ::sf::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return SF_ERR_CUDA;                                                                \
+        }                                                                                      \
+    } while (0)
+
+inline unsigned grid_for(size_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
+
+// scratch for scans and sorts (grows on demand, never shrinks)
+struct Work {
+    DBuf<uint32_t> scan_a, scan_b, hist;
+};
+// exclusive scan of n uint32 values (in place allowed); the total is written to *d_total if non-null
+cudaError_t exclusive_scan_u32(const uint32_t *in, uint32_t *out, size_t n, uint32_t *d_total, Work &wk, cudaStream_t s);
+// stable LSD radix sort of (key, value) pairs on key bits [0, bits); the result ends in keys/vals (the alt buffers,
+// n entries each, are scratch)
+cudaError_t radix_sort_u64(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt, uint32_t *vals_alt, size_t n, int bits,
+                           Work &wk, cudaStream_t s);
+
+// ---------------------------------------------------------------- bounded grid barrier for persistent kernels
+// Every block of a cooperative launch calls it; a wait that outlasts the limit sets ERR_TIMEOUT and returns false
+// (the caller then leaves the kernel and the host reports SF_ERR_TIMEOUT). The barrier state must be zeroed before
+// each launch that uses it.
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+constexpr unsigned long long BARRIER_LIMIT_NS = 4000000000ull;   // 4 s
+__device__ __forceinline__ bool grid_sync(GridBarrier *gb, unsigned nblocks, unsigned *err) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned gen = ld_acquire_u32(&gb->gen);
+        __threadfence();
+        unsigned arrived = atomicAdd(&gb->count, 1u);
+        int ok = 1;
+        if (arrived == nblocks - 1) {
+            atomicExch(&gb->count, 0u);
+            __threadfence();
+            atomicAdd(&gb->gen, 1u);
+        } else {
+            unsigned long long t0 = globaltimer_ns();
+            unsigned spins = 0;
+            while (ld_acquire_u32(&gb->gen) == gen) {
+                if ((++spins & 255u) == 0 && globaltimer_ns() - t0 > BARRIER_LIMIT_NS) {
+                    atomicOr(err, (unsigned)ERR_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(20);
+            }
+        }
+        __threadfence();
+        if (ld_acquire_u32(err) & ERR_TIMEOUT) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+sf_status sor_create(sf_world *w);
+void sor_destroy(sf_world *w);
+sf_status step_create(sf_world *w);
+void step_destroy(sf_world *w);
+sf_status read_error_word(sf_world *w);
+}  // namespace sf

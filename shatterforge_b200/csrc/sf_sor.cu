@@ -1,0 +1,680 @@
+// Load path: scalar potential-flow SOR and the joint checks (src/lib.rs:1005-1040, 1142-1227).
+//
+// Layout. The solve runs on the sparse chunk grid itself (src/lib.rs:302-321): every occupied 8^3 chunk owns 512
+// cells of four arrays —
+//   cphi  f64   the potential (the reference keeps f32; f32 stalls above a 1e-5 relative error on tall frames,
+//               so the device iterates in f64 on the reference's f32 coefficients)
+//   crhs  f32   MASS[mat] + ext (the constant part of sor_brick's numerator)
+//   ccode u32   six 4-bit link codes (the material whose STIFF is the smaller of the pair; 0 = no link), the
+//               cell's own material in bits 24-27 and the foundation bit 28
+//   csid  i32   structure id of the cell (-1 = not a structure brick)
+// — 16 B of reads per brick and 8 B of writes per sweep; links never need an index array because a link always
+// goes to the face-adjacent cell, in this chunk or in the neighbour chunk recorded in chunk_nbr.
+//
+// Order. The reference sweeps Gauss-Seidel in brick-index order. Here the sweep is red-black: every lattice link
+// joins cells of opposite parity (x + y + z), so all red cells are independent given the black ones and vice
+// versa. Each cell's update keeps sor_brick's arithmetic (links in the direction order +x, -x, +y, -y, +z, -z,
+// then the foundation term; target = ((MASS + ext) + sum k phi) / sum k). The iteration converges to the same
+// fixed point as the reference's; tests compare against an FP64 solve of the same system.
+//
+// Residual. As sor_struct: max |dphi| over the sweep divided by max(phi, 1) over the structure, per structure.
+#include <algorithm>
+#include <cstring>
+
+#include "sf_internal.cuh"
+
+namespace sf {
+
+struct SorState {
+    DBuf<double> cphi;
+    DBuf<float> crhs;
+    DBuf<uint32_t> ccode;
+    DBuf<int32_t> csid;
+    DBuf<int32_t> chunk_nbr;        // 6 per chunk
+    DBuf<int32_t> chunk_sid;        // the one structure a chunk's bricks belong to, -2 = several, -1 = none
+    DBuf<uint32_t> work;            // chunk ids of the current solve
+    DBuf<unsigned long long> resid_buf;  // [3][2][n_struct]: md, mp as f64 bits
+    DBuf<uint32_t> sweeps;          // per structure
+    DBuf<double> resid;             // per structure, last sweep
+    DBuf<uint32_t> active0;         // per structure: 1 = solve it
+    DBuf<uint32_t> st_count;        // bricks per structure
+    std::vector<uint32_t> h_st_count;
+    std::vector<uint32_t> st_chunk_start, st_chunk_list, all_chunks;
+    // joints: 4 per static brick
+    DBuf<float> j_ratio, j_bond;
+    DBuf<uint8_t> j_dec;
+    DBuf<uint32_t> j_crushed;
+    DBuf<uint32_t> cand_flag, cand_pos, cand_list;
+    DBuf<uint32_t> counters;        // joints, over, failed, crushed, maxr bits, ncand
+    DBuf<uint32_t> st_req;          // requested structures list for the apply pass
+    Work wk;
+    int occ = 1;
+};
+
+enum : uint8_t { J_HOLD = 0, J_FATIGUE = 1, J_FAIL = 2, J_CRUSH = 3, J_ABSENT = 255 };
+
+__device__ __forceinline__ uint32_t cell_of_static(const uint32_t *ctab, uint32_t scene, uint32_t packed, uint32_t &chunk) {
+    int x, y, z;
+    unpack_cell(packed, x, y, z);
+    chunk = ctab[(size_t)scene * NCT + chunk_slot(x, y, z)] - 1;
+    return cell_in_chunk(x, y, z);
+}
+
+// ---------------------------------------------------------------- prepare: bricks -> chunk cells
+__global__ void k_sor_clear(uint32_t ncells, uint32_t *ccode, int32_t *csid) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ncells) return;
+    ccode[i] = 0;
+    csid[i] = -1;
+}
+
+__global__ void k_sor_scatter(uint32_t ns, const uint32_t *cell, const uint32_t *scene, const uint8_t *mat,
+                              const int32_t *sid, const uint32_t *nb6, const float *bond, const double *phi,
+                              const float *ext, const uint32_t *ctab, double *cphi, float *crhs, uint32_t *ccode,
+                              int32_t *csid) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    uint8_t mi = mat[i];
+    if (mi == 0) return;
+    uint32_t chunk;
+    uint32_t c = cell_of_static(ctab, scene[i], cell[i], chunk);
+    size_t at = (size_t)chunk * 512 + c;
+    cphi[at] = phi[i];
+    int32_t s = sid[i];
+    if (s < 0 || mi >= SLUG) return;
+    uint32_t code = 0;
+#pragma unroll
+    for (int d = 0; d < 6; d++) {
+        uint32_t j = nb6[(size_t)i * 6 + d];
+        if (j == NONE) continue;
+        uint8_t mj = mat[j];
+        if (mj == 0) continue;
+        float hp = (d & 1) == 0 ? bond[(size_t)i * 4 + (d >> 1)] : bond[(size_t)j * 4 + (d >> 1)];
+        if (!(hp > 0.0f)) continue;
+        uint32_t lm = c_mat.stiff[mi] < c_mat.stiff[mj] ? mi : mj;
+        code |= lm << (4 * d);
+    }
+    int x, y, z;
+    unpack_cell(cell[i], x, y, z);
+    code |= (uint32_t)mi << 24;
+    if (y == 0 && bond[(size_t)i * 4 + 3] > 0.0f) code |= 1u << 28;
+    ccode[at] = code;
+    csid[at] = s;
+    crhs[at] = c_mat.mass[mi] + ext[i];
+}
+
+__global__ void k_sor_gather(uint32_t ns, const uint32_t *cell, const uint32_t *scene, const uint8_t *mat, const int32_t *sid,
+                             const uint32_t *active, const uint32_t *ctab, const double *cphi, double *phi64, float *phi) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    int32_t s = sid[i];
+    if (mat[i] == 0 || s < 0 || !active[s]) return;
+    uint32_t chunk;
+    uint32_t c = cell_of_static(ctab, scene[i], cell[i], chunk);
+    double v = cphi[(size_t)chunk * 512 + c];
+    phi64[i] = v;
+    phi[i] = (float)v;
+}
+
+__global__ void k_sor_init(uint32_t nst, unsigned long long *resid_buf, uint32_t *sweeps, double *resid) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nst) return;
+    for (int b = 0; b < 3; b++) {
+        resid_buf[(size_t)(b * 2) * nst + s] = 0ull;
+        resid_buf[(size_t)(b * 2 + 1) * nst + s] = (unsigned long long)__double_as_longlong(1.0);
+    }
+    sweeps[s] = 0;
+    resid[s] = 0.0;
+}
+
+// ---------------------------------------------------------------- the persistent red-black kernel
+constexpr int SOR_BLOCK = 256;
+constexpr int SOR_MAX_LOCAL_STRUCT = 8192;   // active flags kept in shared memory as bits
+
+struct SorArgs {
+    double *cphi;
+    const float *crhs;
+    const uint32_t *ccode;
+    const int32_t *csid;
+    const int32_t *chunk_nbr;
+    const int32_t *chunk_sid;
+    const uint32_t *work;
+    uint32_t n_work;
+    uint32_t n_struct;
+    const uint32_t *active0;
+    unsigned long long *resid_buf;
+    uint32_t *sweeps;
+    double *resid;
+    double omega, tol;
+    uint32_t max_sweeps;
+    GridBarrier *gb;
+    uint32_t *err;
+};
+
+__device__ __forceinline__ bool is_active(const uint32_t *bits, int32_t s) { return (bits[s >> 5] >> (s & 31)) & 1u; }
+
+// block-wide max of (d, p) for one structure, one atomic pair per block (non-negative f64 bits order as u64)
+__device__ __forceinline__ void sor_flush(int32_t s, unsigned long long d, unsigned long long p, unsigned long long *md,
+                                          unsigned long long *mp) {
+    __shared__ unsigned long long sd[SOR_BLOCK / 32], sp[SOR_BLOCK / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        d = max(d, __shfl_xor_sync(0xffffffffu, d, o));
+        p = max(p, __shfl_xor_sync(0xffffffffu, p, o));
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { sd[wid] = d; sp[wid] = p; }
+    __syncthreads();
+    if (threadIdx.x == 0 && s >= 0) {
+        unsigned long long dm = 0, pm = 0;
+        for (int k = 0; k < SOR_BLOCK / 32; k++) { dm = max(dm, sd[k]); pm = max(pm, sp[k]); }
+        if (dm) atomicMax(&md[s], dm);
+        if (pm) atomicMax(&mp[s], pm);
+    }
+    __syncthreads();
+}
+
+// Potentials written by other blocks during the launch are read with ld.global.cg (L2), never through L1.
+// Work: chunk ids sorted by (structure, chunk); each block owns a contiguous range, so its maxima stay in
+// registers while the structure is unchanged. Chunks holding bricks of several structures (chunk_sid = -2) fall
+// back to per-cell atomics.
+__global__ void __launch_bounds__(SOR_BLOCK) k_sor_redblack(SorArgs A) {
+    __shared__ uint32_t act[SOR_MAX_LOCAL_STRUCT / 32];
+    __shared__ int s_any;
+    const uint32_t nst = A.n_struct;
+    const uint32_t nwords = (nst + 31) / 32;
+    for (uint32_t k = threadIdx.x; k < nwords; k += blockDim.x) act[k] = 0;
+    __syncthreads();
+    for (uint32_t s = threadIdx.x; s < nst; s += blockDim.x) if (A.active0[s]) atomicOr(&act[s >> 5], 1u << (s & 31));
+    __syncthreads();
+    const int t = threadIdx.x;
+    const int ly = t >> 5, lz = (t >> 2) & 7, lxp = (t & 3) << 1;
+    const float axis_f[3] = {0.3f, 1.0f, 0.3f};
+    const uint32_t per = (A.n_work + gridDim.x - 1) / gridDim.x;
+    const uint32_t w0 = min(A.n_work, blockIdx.x * per), w1 = min(A.n_work, w0 + per);
+    const unsigned long long one = (unsigned long long)__double_as_longlong(1.0);
+    for (uint32_t sweep = 0; sweep < A.max_sweeps; sweep++) {
+        unsigned long long *md = A.resid_buf + (size_t)((sweep % 3) * 2) * nst;
+        unsigned long long *mp = md + nst;
+        if (blockIdx.x == 0) {
+            unsigned long long *nmd = A.resid_buf + (size_t)(((sweep + 1) % 3) * 2) * nst;
+            for (uint32_t s = threadIdx.x; s < nst; s += blockDim.x) { nmd[s] = 0ull; nmd[nst + s] = one; }
+        }
+        for (int colour = 0; colour < 2; colour++) {
+            const int lx = lxp | ((ly + lz + colour) & 1);
+            const int cell = (ly * 8 + lz) * 8 + lx;
+            int32_t cur = -1;
+            unsigned long long accd = 0, accp = 0;
+            for (uint32_t wi = w0; wi < w1; wi++) {
+                const uint32_t chunk = A.work[wi];
+                const int32_t cs = A.chunk_sid[chunk];
+                if (cs != cur) {
+                    sor_flush(cur, accd, accp, md, mp);
+                    cur = cs; accd = 0; accp = 0;
+                }
+                if (cs >= 0 && !is_active(act, cs)) continue;
+                const size_t at = (size_t)chunk * 512 + cell;
+                const int32_t s = A.csid[at];
+                if (s < 0 || !is_active(act, s)) continue;
+                const uint32_t code = A.ccode[at];
+                double sk = 0.0, skp = 0.0;
+#pragma unroll
+                for (int d = 0; d < 6; d++) {
+                    const uint32_t lm = (code >> (4 * d)) & 15u;
+                    if (lm == 0) continue;
+                    const int ax = d >> 1;
+                    const int sg = (d & 1) ? -1 : 1;
+                    int nx = lx, ny = ly, nz = lz;
+                    if (ax == 0) nx += sg; else if (ax == 1) ny += sg; else nz += sg;
+                    size_t nat;
+                    if (nx >= 0 && nx < 8 && ny >= 0 && ny < 8 && nz >= 0 && nz < 8) {
+                        nat = (size_t)chunk * 512 + (ny * 8 + nz) * 8 + nx;
+                    } else {
+                        const int32_t nc = A.chunk_nbr[(size_t)chunk * 6 + d];
+                        if (nc < 0) { atomicOr(A.err, (unsigned)ERR_SOR_NONFINITE); continue; }
+                        nat = (size_t)nc * 512 + (((ny & 7) * 8 + (nz & 7)) * 8 + (nx & 7));
+                    }
+                    // cond (src/lib.rs:1142): the f32 conductance, promoted
+                    const double k = (double)(c_mat.stiff[lm] * axis_f[ax]);
+                    sk += k;
+                    skp += k * __ldcg(&A.cphi[nat]);
+                }
+                const uint32_t mi = (code >> 24) & 15u;
+                if (code & (1u << 28)) sk += (double)c_mat.gk[mi];
+                double p = __ldcg(&A.cphi[at]);
+                double dabs = 0.0;
+                if (sk > 0.0) {
+                    const double target = ((double)A.crhs[at] + skp) / sk;
+                    const double dd = A.omega * (target - p);
+                    p += dd;
+                    A.cphi[at] = p;
+                    dabs = fabs(dd);
+                    if (!isfinite(p)) atomicOr(A.err, (unsigned)ERR_SOR_NONFINITE);
+                }
+                const unsigned long long db = (unsigned long long)__double_as_longlong(dabs);
+                const unsigned long long pb = p > 0.0 ? (unsigned long long)__double_as_longlong(p) : 0ull;
+                if (cs >= 0) { accd = max(accd, db); accp = max(accp, pb); }
+                else { if (db) atomicMax(&md[s], db); if (pb) atomicMax(&mp[s], pb); }
+            }
+            sor_flush(cur, accd, accp, md, mp);
+            if (!grid_sync(A.gb, gridDim.x, A.err)) return;
+        }
+        // convergence: every block evaluates the same maxima and drops the same structures
+        if (threadIdx.x == 0) s_any = 0;
+        __syncthreads();
+        for (uint32_t s = threadIdx.x; s < nst; s += blockDim.x) {
+            if (!is_active(act, (int32_t)s)) continue;
+            const double r = __longlong_as_double((long long)__ldcg(&md[s])) / __longlong_as_double((long long)__ldcg(&mp[s]));
+            if (blockIdx.x == 0) { A.sweeps[s] = sweep + 1; A.resid[s] = r; }
+            if (r < A.tol || sweep + 1 >= A.max_sweeps) atomicAnd(&act[s >> 5], ~(1u << (s & 31)));
+            else s_any = 1;
+        }
+        __syncthreads();
+        if (!s_any) break;
+    }
+}
+
+// ---------------------------------------------------------------- joint checks
+struct StressArgs {
+    uint32_t ns;
+    const uint32_t *cell;
+    const uint8_t *mat;
+    const int32_t *sid;
+    const uint32_t *nb6;
+    const float *bond, *bmax, *phi;
+    const uint32_t *active;
+    float dt;
+    int live;
+    float *ratio, *bond_after;
+    uint8_t *dec;
+    uint32_t *crushed, *cand_flag;
+};
+
+// every joint evaluated as if nothing failed before it; failures are applied in reference order afterwards
+__global__ void k_stress_eval(StressArgs A) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.ns) return;
+    uint8_t mi = A.mat[i];
+    int32_t s = A.sid[i];
+    bool in = mi != 0 && mi < SLUG && s >= 0 && A.active[s];
+    uint32_t flag = 0;
+    int x, y, z;
+    unpack_cell(A.cell[i], x, y, z);
+    for (int a = 0; a < 3; a++) {
+        size_t o = (size_t)i * 4 + a;
+        uint8_t dec = J_ABSENT;
+        float r = 0.0f, hpo = 0.0f;
+        uint32_t kc = NONE;
+        uint32_t j = in ? A.nb6[(size_t)i * 6 + a * 2] : NONE;
+        if (j != NONE && A.mat[j] != 0) {
+            float hp = A.bond[o];
+            if (hp > 0.0f) {
+                uint8_t mj = A.mat[j];
+                float k = minf(c_mat.stiff[mi], c_mat.stiff[mj]) * (a == 1 ? 1.0f : 0.3f);
+                float f = k * (A.phi[i] - A.phi[j]);
+                float u = a == 1 ? 1.0f : 0.0f;
+                float up = f > 0.0f ? maxf(u, 0.0f) : maxf(-u, 0.0f);
+                float tens = minf(c_mat.tens[mi], c_mat.tens[mj]);
+                float capm = 1.0f - (1.0f - tens) * up;
+                r = div_rn(fabsf(f), hp * capm);
+                dec = J_HOLD;
+                hpo = hp;
+                if (A.live && r > 1.0f) {
+                    float nhp = hp - hp * A.dt * 2.2f * minf(r - 0.85f, 2.5f);
+                    if (nhp < A.bmax[o] * 0.08f) {
+                        if (up == 0.0f && fabsf(u) > 0.5f) { dec = J_CRUSH; kc = c_mat.capv[mj] < c_mat.capv[mi] ? j : i; }
+                        else { dec = J_FAIL; hpo = 0.0f; }
+                    } else { dec = J_FATIGUE; hpo = nhp; }
+                    flag = 1;
+                }
+            }
+        }
+        A.ratio[o] = r; A.bond_after[o] = hpo; A.dec[o] = dec; A.crushed[o] = kc;
+    }
+    {
+        size_t o = (size_t)i * 4 + 3;
+        uint8_t dec = J_ABSENT;
+        float r = 0.0f, b3 = 0.0f;
+        if (in && y == 0 && A.bond[o] > 0.0f) {
+            float f = c_mat.gk[mi] * A.phi[i];
+            b3 = A.bond[o];
+            r = div_rn(f, b3);
+            dec = J_HOLD;
+            if (A.live && r > 1.0f) {
+                b3 = b3 - b3 * A.dt * 2.2f * (r - 0.85f);
+                if (b3 < A.bmax[o] * 0.08f) { b3 = 0.0f; dec = J_FAIL; } else dec = J_FATIGUE;
+                flag = 1;
+            }
+        }
+        A.ratio[o] = r; A.bond_after[o] = b3; A.dec[o] = dec; A.crushed[o] = NONE;
+    }
+    A.cand_flag[i] = flag;
+}
+
+__global__ void k_stress_compact(uint32_t ns, const uint32_t *flag, const uint32_t *pos, uint32_t *list) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ns && flag[i]) list[pos[i]] = i;
+}
+
+__device__ __forceinline__ bool joint_later(uint32_t i2, int a2, uint32_t i, int a) { return i2 > i || (i2 == i && a2 > a); }
+
+// Reference-order application of the over-stressed joints (src/lib.rs:1182-1222): a compressive crush removes a
+// brick at once, so every later joint that touches it disappears, and the crushing brick's own remaining joints
+// are not evaluated (stress_brick returns). The crush budget of 300 per pass turns later crushes into failures.
+__global__ void k_stress_apply(const uint32_t *cand, const uint32_t *ncand_p, const uint32_t *req, uint32_t nreq,
+                               const int32_t *sid, uint8_t *mat, const uint32_t *nb6, const uint32_t *cell,
+                               const uint32_t *scene, const uint32_t *ctab, uint32_t *cpool, float *bond, uint8_t *dec,
+                               float *bond_after, uint32_t *crushed) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t ncand = *ncand_p;
+    uint32_t crush_n = 0;
+    for (uint32_t r = 0; r < nreq; r++) {
+        int32_t s = (int32_t)req[r];
+        for (uint32_t c = 0; c < ncand; c++) {
+            uint32_t i = cand[c];
+            if (sid[i] != s) continue;
+            for (int a = 0; a < 4; a++) {
+                size_t o = (size_t)i * 4 + a;
+                uint8_t d = dec[o];
+                if (d == J_ABSENT || d == J_HOLD) continue;
+                if (mat[i] == 0) { dec[o] = J_ABSENT; continue; }
+                if (d == J_CRUSH) {
+                    if (crush_n >= 300) { d = J_FAIL; dec[o] = J_FAIL; bond_after[o] = 0.0f; crushed[o] = NONE; }
+                    else {
+                        crush_n++;
+                        uint32_t k = crushed[o];
+                        mat[k] = 0;
+                        uint32_t chunk;
+                        uint32_t cc = cell_of_static(ctab, scene[k], cell[k], chunk);
+                        cpool[(size_t)chunk * 512 + cc] = 0;
+                        // the rest of brick i's joints
+                        for (int a2 = a + 1; a2 < 4; a2++) dec[(size_t)i * 4 + a2] = J_ABSENT;
+                        // brick k's own joints, if it comes later
+                        if (k > i) for (int a2 = 0; a2 < 4; a2++) dec[(size_t)k * 4 + a2] = J_ABSENT;
+                        // joints of the bricks below k along each axis, pointing at k
+                        for (int a2 = 0; a2 < 3; a2++) {
+                            uint32_t i2 = nb6[(size_t)k * 6 + a2 * 2 + 1];
+                            if (i2 != NONE && joint_later(i2, a2, i, a)) dec[(size_t)i2 * 4 + a2] = J_ABSENT;
+                        }
+                        break;
+                    }
+                }
+                bond[o] = bond_after[o];
+            }
+        }
+    }
+}
+
+__global__ void k_stress_tally(uint32_t ns, const uint8_t *dec, const float *ratio, const uint32_t *nb6,
+                               const int32_t *sid, const uint32_t *active, float *stress, uint32_t *counters) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    int32_t s = sid[i];
+    if (s < 0 || !active[s]) return;
+    uint32_t nj = 0, over = 0, fail = 0, crush = 0;
+    float mr = 0.0f;
+    for (int a = 0; a < 4; a++) {
+        size_t o = (size_t)i * 4 + a;
+        uint8_t d = dec[o];
+        if (d == J_ABSENT) continue;
+        float r = ratio[o];
+        nj++;
+        if (r > 1.0f) over++;
+        if (d == J_FAIL) fail++;
+        if (d == J_CRUSH) crush++;
+        mr = maxf(mr, r);
+        atomicMax((unsigned *)&stress[i], __float_as_uint(r));
+        if (a < 3) atomicMax((unsigned *)&stress[nb6[(size_t)i * 6 + a * 2]], __float_as_uint(r));
+    }
+    if (nj) {
+        atomicAdd(&counters[0], nj);
+        if (over) atomicAdd(&counters[1], over);
+        if (fail) atomicAdd(&counters[2], fail);
+        if (crush) atomicAdd(&counters[3], crush);
+        atomicMax(&counters[4], __float_as_uint(mr));
+    }
+}
+
+__global__ void k_stress_zero(uint32_t ns, const int32_t *sid, const uint8_t *mat, const uint32_t *active, float *stress) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    int32_t s = sid[i];
+    if (s >= 0 && mat[i] != 0 && active[s]) stress[i] = 0.0f;
+}
+
+// ---------------------------------------------------------------- host side
+sf_status sor_create(sf_world *w) {
+    SorState *st = new SorState();
+    w->sor = st;
+    SF_CUDA(upload_mat_tables(w->stream));
+    uint32_t nch = w->n_chunks, nst = w->n_struct;
+    cudaStream_t s = w->stream;
+    // chunk neighbours (host; the grid is static)
+    std::vector<int32_t> nbr((size_t)nch * 6, -1);
+    std::vector<uint32_t> h_ctab;
+    if (nch) {
+        h_ctab.resize((size_t)w->n_scenes * NCT);
+        SF_CUDA(cudaMemcpyAsync(h_ctab.data(), w->ctab.p, h_ctab.size() * 4, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaStreamSynchronize(s));
+    }
+    const int D[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    for (uint32_t c = 0; c < nch; c++) {
+        int x, y, z;
+        unpack_cell(w->h_chunk_cell[c], x, y, z);
+        uint32_t sc = w->h_chunk_scene[c];
+        for (int d = 0; d < 6; d++) {
+            int nx = x + 8 * D[d][0], ny = y + 8 * D[d][1], nz = z + 8 * D[d][2];
+            if (!inb(nx, ny, nz)) continue;
+            uint32_t t = h_ctab[(size_t)sc * NCT + chunk_slot(nx, ny, nz)];
+            if (t) nbr[(size_t)c * 6 + d] = (int32_t)(t - 1);
+        }
+    }
+    SF_CUDA(st->chunk_nbr.alloc(nbr.size()));
+    if (!nbr.empty()) SF_CUDA(cudaMemcpyAsync(st->chunk_nbr.p, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice, s));
+    // chunks of each structure
+    std::vector<std::vector<uint32_t>> per(nst);
+    st->h_st_count.assign(nst, 0);
+    std::vector<int32_t> csole(nch, -1);
+    for (uint32_t i = 0; i < w->ns; i++) {
+        int32_t sid = w->h_sid[i];
+        if (sid < 0) continue;
+        int x, y, z;
+        unpack_cell(w->h_s_cell[i], x, y, z);
+        uint32_t sc = 0;
+        // scene of brick i: find by static offset
+        for (uint32_t q = 0; q < w->n_scenes; q++)
+            if (i >= w->scenes[q].static_off && i < w->scenes[q].static_off + w->scenes[q].n_static) { sc = q; break; }
+        uint32_t c = h_ctab[(size_t)sc * NCT + chunk_slot(x, y, z)] - 1;
+        if (per[sid].empty() || per[sid].back() != c) per[sid].push_back(c);
+        st->h_st_count[sid]++;
+        csole[c] = csole[c] == -1 ? sid : (csole[c] == sid ? sid : -2);
+    }
+    st->st_chunk_start.assign(nst + 1, 0);
+    for (uint32_t q = 0; q < nst; q++) {
+        std::sort(per[q].begin(), per[q].end());
+        per[q].erase(std::unique(per[q].begin(), per[q].end()), per[q].end());
+        st->st_chunk_start[q + 1] = st->st_chunk_start[q] + (uint32_t)per[q].size();
+        st->st_chunk_list.insert(st->st_chunk_list.end(), per[q].begin(), per[q].end());
+    }
+    for (uint32_t c = 0; c < nch; c++) if (csole[c] != -1) st->all_chunks.push_back(c);
+    std::stable_sort(st->all_chunks.begin(), st->all_chunks.end(), [&](uint32_t x, uint32_t y) { return csole[x] < csole[y]; });
+    SF_CUDA(st->chunk_sid.alloc(nch));
+    if (nch) SF_CUDA(cudaMemcpyAsync(st->chunk_sid.p, csole.data(), nch * 4, cudaMemcpyHostToDevice, s));
+    size_t ncell = (size_t)nch * 512;
+    SF_CUDA(st->cphi.alloc(ncell)); SF_CUDA(st->crhs.alloc(ncell)); SF_CUDA(st->ccode.alloc(ncell)); SF_CUDA(st->csid.alloc(ncell));
+    SF_CUDA(cudaMemsetAsync(st->cphi.p, 0, st->cphi.bytes(), s));
+    SF_CUDA(cudaMemsetAsync(st->crhs.p, 0, st->crhs.bytes(), s));
+    SF_CUDA(st->work.alloc(std::max<size_t>(st->all_chunks.size(), 1)));
+    SF_CUDA(st->resid_buf.alloc((size_t)6 * std::max<uint32_t>(nst, 1)));
+    SF_CUDA(st->sweeps.alloc(std::max<uint32_t>(nst, 1)));
+    SF_CUDA(st->resid.alloc(std::max<uint32_t>(nst, 1)));
+    SF_CUDA(st->active0.alloc(std::max<uint32_t>(nst, 1)));
+    SF_CUDA(st->st_req.alloc(std::max<uint32_t>(nst, 1)));
+    size_t nj = (size_t)std::max<uint32_t>(w->ns, 1) * 4;
+    SF_CUDA(st->j_ratio.alloc(nj)); SF_CUDA(st->j_bond.alloc(nj)); SF_CUDA(st->j_dec.alloc(nj)); SF_CUDA(st->j_crushed.alloc(nj));
+    SF_CUDA(cudaMemsetAsync(st->j_dec.p, 0xFF, st->j_dec.bytes(), s));
+    SF_CUDA(st->cand_flag.alloc(std::max<uint32_t>(w->ns, 1) + 1));
+    SF_CUDA(st->cand_pos.alloc(std::max<uint32_t>(w->ns, 1) + 1));
+    SF_CUDA(st->cand_list.alloc(std::max<uint32_t>(w->ns, 1)));
+    SF_CUDA(st->counters.alloc(16));
+    int occ = 0;
+    SF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sor_redblack, SOR_BLOCK, 0));
+    st->occ = std::max(1, occ);
+    if (nst > (uint32_t)SOR_MAX_LOCAL_STRUCT) { set_error("more than %d structures", SOR_MAX_LOCAL_STRUCT); return SF_ERR_CAPACITY; }
+    return SF_OK;
+}
+
+void sor_destroy(sf_world *w) {
+    delete w->sor;
+    w->sor = nullptr;
+}
+
+// which structures a call covers, and the chunk list of that set
+static sf_status sor_select(sf_world *w, int32_t structure, std::vector<uint32_t> &act, std::vector<uint32_t> &chunks,
+                            std::vector<uint32_t> &req) {
+    SorState *st = w->sor;
+    uint32_t nst = w->n_struct;
+    act.assign(std::max<uint32_t>(nst, 1), 0);
+    chunks.clear();
+    req.clear();
+    if (structure >= 0) {
+        if ((uint32_t)structure >= nst) { set_error("structure %d does not exist", structure); return SF_ERR_ARG; }
+        if (st->h_st_count[structure]) {
+            act[structure] = 1;
+            req.push_back((uint32_t)structure);
+            chunks.assign(st->st_chunk_list.begin() + st->st_chunk_start[structure],
+                          st->st_chunk_list.begin() + st->st_chunk_start[structure + 1]);
+        }
+    } else {
+        for (uint32_t q = 0; q < nst; q++) if (st->h_st_count[q]) { act[q] = 1; req.push_back(q); }
+        chunks = st->all_chunks;
+    }
+    return SF_OK;
+}
+
+}  // namespace sf
+
+using namespace sf;
+
+extern "C" {
+
+sf_status sf_structure_solve(sf_world *w, int32_t structure, float omega, float tol, uint32_t max_sweeps,
+                             sf_solve_report *report) {
+    if (!w) return SF_ERR_ARG;
+    if (!(omega > 0.0f && omega < 2.0f)) { set_error("omega %g outside (0, 2)", (double)omega); return SF_ERR_ARG; }
+    SorState *st = w->sor;
+    std::vector<uint32_t> act, chunks, req;
+    sf_status r = sor_select(w, structure, act, chunks, req);
+    if (r != SF_OK) return r;
+    sf_solve_report rep{};
+    if (chunks.empty() || max_sweeps == 0) { if (report) *report = rep; return SF_OK; }
+    cudaStream_t s = w->stream;
+    uint32_t nst = w->n_struct;
+    SF_CUDA(cudaMemcpyAsync(st->active0.p, act.data(), nst * 4, cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemcpyAsync(st->work.p, chunks.data(), chunks.size() * 4, cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaEventRecord(w->ev0, s));
+    size_t ncell = (size_t)w->n_chunks * 512;
+    k_sor_clear<<<grid_for(ncell, 256), 256, 0, s>>>((uint32_t)ncell, st->ccode.p, st->csid.p);
+    k_sor_scatter<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p, w->s_nb6.p,
+                                                       w->s_bond.p, w->s_phi64.p, w->s_ext.p, w->ctab.p, st->cphi.p,
+                                                       st->crhs.p, st->ccode.p, st->csid.p);
+    k_sor_init<<<grid_for(nst, 256), 256, 0, s>>>(nst, st->resid_buf.p, st->sweeps.p, st->resid.p);
+    SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s));
+    SF_CUDA(cudaMemsetAsync(w->err.p, 0, sizeof(uint32_t), s));
+    SorArgs A;
+    A.cphi = st->cphi.p; A.crhs = st->crhs.p; A.ccode = st->ccode.p; A.csid = st->csid.p; A.chunk_nbr = st->chunk_nbr.p;
+    A.chunk_sid = st->chunk_sid.p; A.work = st->work.p; A.n_work = (uint32_t)chunks.size(); A.n_struct = nst;
+    A.active0 = st->active0.p; A.resid_buf = st->resid_buf.p; A.sweeps = st->sweeps.p; A.resid = st->resid.p;
+    A.omega = (double)omega; A.tol = (double)tol; A.max_sweeps = max_sweeps; A.gb = w->barrier.p; A.err = w->err.p;
+    unsigned grid = (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * st->occ);
+    void *args[] = {&A};
+    SF_CUDA(cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s));
+    k_sor_gather<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p,
+                                                      st->active0.p, w->ctab.p, st->cphi.p, w->s_phi64.p, w->s_phi.p);
+    SF_CUDA(cudaEventRecord(w->ev1, s));
+    SF_CUDA(cudaGetLastError());
+    std::vector<uint32_t> sw(nst);
+    std::vector<double> rs(nst);
+    SF_CUDA(cudaMemcpyAsync(sw.data(), st->sweeps.p, nst * 4, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaMemcpyAsync(rs.data(), st->resid.p, nst * 8, cudaMemcpyDeviceToHost, s));
+    sf_status e = read_error_word(w);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, w->ev0, w->ev1);
+    rep.ms = ms;
+    for (uint32_t q : req) {
+        rep.structures++;
+        rep.max_sweeps_done = std::max(rep.max_sweeps_done, sw[q]);
+        rep.brick_sweeps += (uint64_t)sw[q] * st->h_st_count[q];
+        rep.max_residual = std::max(rep.max_residual, (double)rs[q]);
+    }
+    if (report) *report = rep;
+    if (e == SF_OK && (w->stats.error_word & ERR_SOR_NONFINITE)) { set_error("non-finite potential (ungrounded piece?)"); return SF_ERR_VERIFY; }
+    return e;
+}
+
+// per-structure sweeps and residuals of the last solve (n_struct entries each)
+sf_status sf_read_solve_detail(sf_world *w, uint32_t *sweeps, double *resid) {
+    if (!w) return SF_ERR_ARG;
+    uint32_t nst = w->n_struct;
+    if (sweeps) SF_CUDA(cudaMemcpyAsync(sweeps, w->sor->sweeps.p, nst * 4, cudaMemcpyDeviceToHost, w->stream));
+    if (resid) SF_CUDA(cudaMemcpyAsync(resid, w->sor->resid.p, nst * 8, cudaMemcpyDeviceToHost, w->stream));
+    SF_CUDA(cudaStreamSynchronize(w->stream));
+    return SF_OK;
+}
+
+sf_status sf_structure_check(sf_world *w, int32_t structure, float dt, int32_t live, sf_check_report *report) {
+    if (!w) return SF_ERR_ARG;
+    SorState *st = w->sor;
+    std::vector<uint32_t> act, chunks, req;
+    sf_status r = sor_select(w, structure, act, chunks, req);
+    if (r != SF_OK) return r;
+    cudaStream_t s = w->stream;
+    uint32_t ns = w->ns, nst = w->n_struct;
+    sf_check_report rep{};
+    if (ns == 0 || req.empty()) { if (report) *report = rep; return SF_OK; }
+    SF_CUDA(cudaMemcpyAsync(st->active0.p, act.data(), nst * 4, cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemcpyAsync(st->st_req.p, req.data(), req.size() * 4, cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemsetAsync(st->counters.p, 0, st->counters.bytes(), s));
+    SF_CUDA(cudaEventRecord(w->ev0, s));
+    k_stress_zero<<<grid_for(ns, 256), 256, 0, s>>>(ns, w->s_sid.p, w->s_mat.p, st->active0.p, w->s_stress.p);
+    StressArgs A;
+    A.ns = ns; A.cell = w->s_cell.p; A.mat = w->s_mat.p; A.sid = w->s_sid.p; A.nb6 = w->s_nb6.p; A.bond = w->s_bond.p;
+    A.bmax = w->s_bmax.p; A.phi = w->s_phi.p; A.active = st->active0.p; A.dt = dt; A.live = live ? 1 : 0;
+    A.ratio = st->j_ratio.p; A.bond_after = st->j_bond.p; A.dec = st->j_dec.p; A.crushed = st->j_crushed.p;
+    A.cand_flag = st->cand_flag.p;
+    k_stress_eval<<<grid_for(ns, 256), 256, 0, s>>>(A);
+    SF_CUDA(exclusive_scan_u32(st->cand_flag.p, st->cand_pos.p, ns, st->counters.p + 5, st->wk, s));
+    k_stress_compact<<<grid_for(ns, 256), 256, 0, s>>>(ns, st->cand_flag.p, st->cand_pos.p, st->cand_list.p);
+    k_stress_apply<<<1, 32, 0, s>>>(st->cand_list.p, st->counters.p + 5, st->st_req.p, (uint32_t)req.size(), w->s_sid.p,
+                                    w->s_mat.p, w->s_nb6.p, w->s_cell.p, w->s_scene.p, w->ctab.p, w->cpool.p, w->s_bond.p,
+                                    st->j_dec.p, st->j_bond.p, st->j_crushed.p);
+    k_stress_tally<<<grid_for(ns, 256), 256, 0, s>>>(ns, st->j_dec.p, st->j_ratio.p, w->s_nb6.p, w->s_sid.p, st->active0.p,
+                                                      w->s_stress.p, st->counters.p);
+    SF_CUDA(cudaEventRecord(w->ev1, s));
+    SF_CUDA(cudaGetLastError());
+    uint32_t c[16];
+    SF_CUDA(cudaMemcpyAsync(c, st->counters.p, sizeof c, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, w->ev0, w->ev1);
+    rep.joints = c[0]; rep.over = c[1]; rep.failed = c[2]; rep.crushed = c[3];
+    std::memcpy(&rep.max_ratio, &c[4], 4);
+    rep.ms = ms;
+    if (report) *report = rep;
+    return SF_OK;
+}
+
+sf_status sf_read_joints(sf_world *w, float *ratio4, float *bond4, uint8_t *decision4, uint32_t *crushed4) {
+    if (!w) return SF_ERR_ARG;
+    SorState *st = w->sor;
+    size_t nj = (size_t)w->ns * 4;
+    cudaStream_t s = w->stream;
+    if (ratio4) SF_CUDA(cudaMemcpyAsync(ratio4, st->j_ratio.p, nj * 4, cudaMemcpyDeviceToHost, s));
+    if (bond4) SF_CUDA(cudaMemcpyAsync(bond4, st->j_bond.p, nj * 4, cudaMemcpyDeviceToHost, s));
+    if (decision4) SF_CUDA(cudaMemcpyAsync(decision4, st->j_dec.p, nj, cudaMemcpyDeviceToHost, s));
+    if (crushed4) SF_CUDA(cudaMemcpyAsync(crushed4, st->j_crushed.p, nj * 4, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    return SF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1066 @@
+// Rigid-body step over brick spheres (src/lib.rs:1367-1783), all scenes of a world per launch.
+//
+// One substep:
+//   k_update_cache   rotation and world inverse inertia of awake bodies, then gravity       src/lib.rs:1368-1378, 1772
+//   k_brick_pos      world position of each awake body's bricks                                src/lib.rs:1375
+//   k_cell_keys      64-bit cell key (scene, hashed cell) of every live brick; radix-sorted, stable, so each
+//                    bucket holds its bricks in ascending index order; k_bucket_ranges marks each bucket's range
+//                    — the same 32768 buckets as build_hash (src/lib.rs:1379-1395), hash collisions included
+//   k_contacts       count, scan, fill: every brick of an awake body finds its ground corners, static cells and
+//                    hashed neighbours exactly as gen_contacts (src/lib.rs:1405-1471); walking each bucket from its
+//                    highest index down reproduces the reference's chain order, so the filled list IS the
+//                    reference's contact list order
+//   manifolds        contacts grouped by body pair (a, b; b = static side for ground, static cells and sleeping
+//                    partners) with a stable radix sort, so each manifold keeps its contacts in list order
+//   k_prep           prep_contacts (src/lib.rs:1551-1577) per contact, written in manifold order
+//   colouring        Jones-Plassmann rounds on the manifold conflict graph (two manifolds conflict when they share
+//                    an awake body); priority = hash of the pair, ties to the lower manifold index; the smallest
+//                    colour free at both bodies — the same colouring as a greedy pass in priority order
+//   k_solve          persistent kernel: for each iteration, for each colour, each manifold's contacts solved in list
+//                    order with solve()'s sequential-impulse math (src/lib.rs:1579-1601); a bounded grid barrier
+//                    separates colours. Manifolds of one colour share no awake body, so the result does not
+//                    depend on their order inside a colour.
+//   islands          union-find over manifolds between two awake bodies, larger root linked under the smaller by
+//                    CAS with path halving (gpu/gpu_world.js:1634-1655, engine/src/phys.rs:326-354)
+//   k_integrate      pinch clamps (src/lib.rs:1746-1768) and integrate (src/lib.rs:1703-1742)
+#include <algorithm>
+#include <cstring>
+
+#include "sf_internal.cuh"
+
+namespace sf {
+
+struct StepState {
+    Work wk;
+    // hashed cell sort
+    DBuf<uint64_t> ckey, ckey_alt;
+    DBuf<uint32_t> cval, cval_alt;
+    DBuf<uint32_t> bstart, bend;
+    // contacts, list order
+    DBuf<uint32_t> ccount, coff;
+    DBuf<uint32_t> L_a, L_b, L_bo, L_ba, L_bb;
+    DBuf<float4> L_p, L_n;
+    // manifold order
+    DBuf<uint64_t> mkey, mkey_alt;
+    DBuf<uint32_t> perm, perm_alt, invperm;
+    DBuf<uint32_t> mflag, mpos;
+    DBuf<uint32_t> man_a, man_b, man_start, man_count, man_prio, man_color, man_round;
+    DBuf<float4> S_n, S_t1, S_t2, S_ra, S_rb, S_j;
+    // colouring
+    DBuf<uint32_t> bm_count, bm_start, bm_fill, bm_list;
+    DBuf<uint32_t> masks, vmasks;
+    DBuf<uint32_t> wl0, wl1;
+    DBuf<uint32_t> col_count, col_start, col_fill, col_list;
+    // islands
+    DBuf<uint32_t> parent, label, mint;
+    // per-scene body offsets (for scene-local priorities)
+    DBuf<uint32_t> body_off_of_body;
+    // device scalars: [0] contacts, [1] manifolds, [2] colours, [3] rounds, [4..6] jp counts, [7] alive, [8] awake,
+    // [9] islands
+    DBuf<uint32_t> dev;
+    uint32_t *h_dev = nullptr;   // pinned mirror
+    uint64_t capacity = 0;
+    uint64_t last_contacts = 0;
+    int solve_occ = 1, jp_occ = 1;
+    bool have_contacts = false;
+};
+
+enum { DV_CONTACTS = 0, DV_MANIFOLDS = 1, DV_COLORS = 2, DV_ROUNDS = 3, DV_WL0 = 4, DV_WL1 = 5, DV_WL2 = 6,
+       DV_ALIVE = 7, DV_AWAKE = 8, DV_ISLANDS = 9, DV_N = 16 };
+
+// ---------------------------------------------------------------- pose cache
+__global__ void k_update_cache(uint32_t nb, float h, const uint8_t *alive, const uint8_t *asleep, const float4 *q,
+                               const float *iil, float *rot, float *iiw, float4 *v) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb || !alive[b] || asleep[b]) return;
+    float4 qq = q[b];
+    float r[9], il[9], t1[9], t2[9], t3[9];
+    q_to_m(qq.x, qq.y, qq.z, qq.w, r);
+#pragma unroll
+    for (int k = 0; k < 9; k++) il[k] = iil[(size_t)b * 9 + k];
+    mmul(r, il, t1);
+    mtr(r, t2);
+    mmul(t1, t2, t3);
+#pragma unroll
+    for (int k = 0; k < 9; k++) { rot[(size_t)b * 9 + k] = r[k]; iiw[(size_t)b * 9 + k] = t3[k]; }
+    float4 vv = v[b];
+    vv.y -= GR * h;
+    v[b] = vv;
+}
+
+__global__ void k_brick_pos(uint32_t nd, const uint32_t *kbody, const uint8_t *alive, const uint8_t *asleep,
+                            const float4 *pos, const float *rot, const float4 *local, float4 *wpos) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nd) return;
+    uint32_t b = kbody[i];
+    if (!alive[b] || asleep[b]) return;
+    float r[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) r[k] = rot[(size_t)b * 9 + k];
+    float4 l = local[i], p = pos[b];
+    V3 wp = add(v3(p.x, p.y, p.z), mv(r, v3(l.x, l.y, l.z)));
+    wpos[i] = make_float4(wp.x, wp.y, wp.z, 0.0f);
+}
+
+__device__ __forceinline__ int floor_cell(float x) { return __float2int_rz(floorf(x / S)); }
+
+__global__ void k_cell_keys(uint32_t nd, uint64_t none_key, const uint32_t *kbody, const uint32_t *bscene,
+                            const uint8_t *alive, const float4 *wpos, uint64_t *key, uint32_t *val) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nd) return;
+    uint32_t b = kbody[i];
+    uint64_t k = none_key;
+    if (alive[b]) {
+        float4 p = wpos[i];
+        k = (uint64_t)bscene[b] * HSIZE + hkey(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z));
+    }
+    key[i] = k;
+    val[i] = i;
+}
+
+__global__ void k_bucket_ranges(uint32_t nd, uint64_t none_key, const uint64_t *key, uint32_t *bstart, uint32_t *bend) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nd) return;
+    uint64_t k = key[p];
+    if (k >= none_key) return;
+    if (p == 0 || key[p - 1] != k) bstart[k] = p;
+    if (p == nd - 1 || key[p + 1] != k) bend[k] = p + 1;
+}
+
+// ---------------------------------------------------------------- contacts
+struct ContactArgs {
+    uint32_t nd;
+    const uint32_t *kbody, *bscene, *ctab, *cpool;
+    const uint8_t *alive, *asleep, *kmat, *smat;
+    const float4 *wpos, *v, *w;
+    const float *rot, *rad;
+    const uint32_t *bstart, *bend, *cval;
+    uint32_t *ccount;
+    const uint32_t *coff;
+    uint8_t *wake;
+    uint32_t *L_a, *L_b, *L_bo, *L_ba, *L_bb;
+    float4 *L_p, *L_n;
+};
+
+template <bool FILL>
+__global__ void __launch_bounds__(128) k_contacts(ContactArgs A) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.nd) return;
+    uint32_t a = A.kbody[i];
+    if (!A.alive[a] || A.asleep[a]) { if (!FILL) A.ccount[i] = 0; return; }
+    const uint32_t sc = A.bscene[a];
+    uint32_t n = 0;
+    const uint32_t base = FILL ? A.coff[i] : 0;
+    float4 p4 = A.wpos[i];
+    const V3 p = v3(p4.x, p4.y, p4.z);
+    auto emit = [&](uint32_t b, uint32_t bo, uint32_t bb, V3 cp, V3 nn, float depth) {
+        if (FILL) {
+            uint32_t o = base + n;
+            A.L_a[o] = a; A.L_b[o] = b; A.L_bo[o] = bo; A.L_ba[o] = i; A.L_bb[o] = bb;
+            A.L_p[o] = make_float4(cp.x, cp.y, cp.z, 0.0f);
+            A.L_n[o] = make_float4(nn.x, nn.y, nn.z, depth);
+        }
+        n++;
+    };
+    // ground: the brick's 8 cube corners below y = 0 (src/lib.rs:1415-1421)
+    if (p.y < 0.5f) {
+        float r[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) r[k] = A.rot[(size_t)a * 9 + k];
+        for (int c = 0; c < 8; c++) {
+            V3 l = v3((c & 1) == 0 ? -H : H, (c & 2) == 0 ? -H : H, (c & 4) == 0 ? -H : H);
+            V3 cp = add(p, mv(r, l));
+            if (cp.y < 0.0f) emit(STATIC, STATIC, NONE, cp, v3(0.0f, 1.0f, 0.0f), -cp.y);
+        }
+    }
+    // static cells of the 3^3 block (src/lib.rs:1422-1440)
+    {
+        const int cx = floor_cell(p.x) + NX / 2, cy = floor_cell(p.y), cz = floor_cell(p.z) + NZ / 2;
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    const int x = cx + dx, y = cy + dy, z = cz + dz;
+                    if (!inb(x, y, z)) continue;
+                    const uint32_t t = A.ctab[(size_t)sc * NCT + chunk_slot(x, y, z)];
+                    if (t == 0) continue;
+                    const uint32_t g = A.cpool[(size_t)(t - 1) * 512 + cell_in_chunk(x, y, z)];
+                    if (g == 0) continue;
+                    const uint32_t j = g - 1;
+                    if (A.smat[j] == 0) continue;
+                    const V3 c = lat_pos(x, y, z);
+                    const V3 qq = v3(clampf(p.x, c.x - H, c.x + H), clampf(p.y, c.y - H, c.y + H), clampf(p.z, c.z - H, c.z + H));
+                    const V3 d = sub(p, qq);
+                    const float dist = len(d);
+                    if (dist >= RB) continue;
+                    if (dist > 1e-4f) {
+                        emit(STATIC, STATIC, j, qq, mul(d, div_rn(1.0f, dist)), RB - dist);
+                    } else {
+                        const V3 r = sub(p, c);
+                        const float ar[3] = {r.x, r.y, r.z};
+                        int ax = 0;
+                        for (int k = 1; k < 3; k++) if (fabsf(ar[k]) > fabsf(ar[ax])) ax = k;
+                        float nv[3] = {0.0f, 0.0f, 0.0f};
+                        nv[ax] = ar[ax] >= 0.0f ? 1.0f : -1.0f;
+                        emit(STATIC, STATIC, j, p, v3(nv[0], nv[1], nv[2]), H + RB - fabsf(ar[ax]));
+                    }
+                }
+    }
+    // hashed neighbours in the 27 buckets around the brick (src/lib.rs:1441-1466)
+    {
+        const int hx = floor_cell(p.x), hy = floor_cell(p.y), hz = floor_cell(p.z);
+        float speed = 0.0f;
+        if (FILL) {
+            float4 vv = A.v[a], ww = A.w[a];
+            speed = len(v3(vv.x, vv.y, vv.z)) + len(v3(ww.x, ww.y, ww.z)) * A.rad[a] * 0.5f;
+        }
+        const float lim2 = 4.0f * RB * RB;
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    const size_t hb = (size_t)sc * HSIZE + hkey(hx + dx, hy + dy, hz + dz);
+                    const uint32_t s0 = A.bstart[hb], s1 = A.bend[hb];
+                    for (uint32_t q = s1; q > s0; q--) {
+                        const uint32_t j = A.cval[q - 1];
+                        const uint32_t bj = A.kbody[j];
+                        if (bj == a || A.kmat[j] == 0) continue;
+                        const bool other_awake = !A.asleep[bj];
+                        if (other_awake && j < i) continue;
+                        const float4 pj4 = A.wpos[j];
+                        const V3 pj = v3(pj4.x, pj4.y, pj4.z);
+                        const V3 d = sub(p, pj);
+                        const float dd = dot(d, d);
+                        if (dd >= lim2 || dd < 1e-10f) continue;
+                        const float dist = sqrt_rn(dd);
+                        const V3 nn = mul(d, div_rn(1.0f, dist));
+                        const V3 cp = madd(pj, nn, dist * 0.5f);
+                        if (other_awake) emit(bj, bj, j, cp, nn, 2.0f * RB - dist);
+                        else {
+                            if (FILL && speed > 0.7f) A.wake[bj] = 1;
+                            emit(STATIC, bj, j, cp, nn, 2.0f * RB - dist);
+                        }
+                    }
+                }
+    }
+    if (!FILL) A.ccount[i] = n;
+}
+
+__global__ void k_body_nc(uint32_t nc, const uint32_t *L_a, const uint32_t *L_b, uint32_t *bnc) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nc) return;
+    atomicAdd(&bnc[L_a[k]], 1u);
+    uint32_t b = L_b[k];
+    if (b != STATIC) atomicAdd(&bnc[b], 1u);
+}
+
+// ---------------------------------------------------------------- manifolds
+__global__ void k_man_keys(uint32_t nc, uint64_t nb1, const uint32_t *L_a, const uint32_t *L_b, uint64_t *key, uint32_t *val) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nc) return;
+    uint32_t b = L_b[k];
+    uint64_t bp = b == STATIC ? 0 : (uint64_t)b + 1;
+    key[k] = (uint64_t)L_a[k] * nb1 + bp;
+    val[k] = k;
+}
+__global__ void k_man_flags(uint32_t nc, const uint64_t *key, uint32_t *flag) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nc) return;
+    flag[t] = (t == 0 || key[t] != key[t - 1]) ? 1u : 0u;
+}
+__global__ void k_man_write(uint32_t nc, const uint32_t *flag, const uint32_t *pos, const uint32_t *perm, const uint32_t *L_a,
+                            const uint32_t *L_b, const uint32_t *bscene, const uint32_t *body_off_of_body,
+                            uint32_t *man_a, uint32_t *man_b, uint32_t *man_start, uint32_t *man_prio) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nc || !flag[t]) return;
+    uint32_t m = pos[t];
+    uint32_t k = perm[t];
+    uint32_t a = L_a[k], b = L_b[k];
+    man_a[m] = a; man_b[m] = b; man_start[m] = t;
+    uint32_t off = body_off_of_body[a];
+    man_prio[m] = pair_priority(a - off, b == STATIC ? 0u : b - off + 1u);
+}
+__global__ void k_man_count(const uint32_t *nm_p, uint32_t nc, const uint32_t *man_start, uint32_t *man_count) {
+    uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t nm = *nm_p;
+    if (m >= nm) return;
+    uint32_t e = m + 1 < nm ? man_start[m + 1] : nc;
+    man_count[m] = e - man_start[m];
+}
+
+__device__ __forceinline__ float eff_mass(float ima, const float *iia, bool hasb, float imb, const float *iib, V3 ra, V3 rb, V3 n) {
+    float k = ima + dot(n, cross(mv(iia, cross(ra, n)), ra));
+    if (hasb) k += imb + dot(n, cross(mv(iib, cross(rb, n)), rb));
+    return k > 1e-12f ? div_rn(1.0f, k) : 0.0f;
+}
+
+struct PrepArgs {
+    uint32_t nc;
+    float h;
+    const uint32_t *perm, *L_a, *L_b;
+    const float4 *L_p, *L_n, *pos, *v, *w;
+    const float *im, *iiw;
+    float4 *S_n, *S_t1, *S_t2, *S_ra, *S_rb, *S_j;
+    uint32_t *invperm;
+};
+
+__global__ void k_prep(PrepArgs A) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= A.nc) return;
+    uint32_t k = A.perm[t];
+    uint32_t a = A.L_a[k], b = A.L_b[k];
+    bool hasb = b != STATIC;
+    float4 p4 = A.L_p[k], n4 = A.L_n[k];
+    V3 p = v3(p4.x, p4.y, p4.z), n = v3(n4.x, n4.y, n4.z);
+    float depth = n4.w;
+    float4 pa = A.pos[a];
+    V3 ra = sub(p, v3(pa.x, pa.y, pa.z));
+    V3 rb = v3(0.0f, 0.0f, 0.0f);
+    float iia[9], iib[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) iia[q] = A.iiw[(size_t)a * 9 + q];
+    float ima = A.im[a], imb = 0.0f;
+    V3 vela, velb = v3(0.0f, 0.0f, 0.0f);
+    {
+        float4 va = A.v[a], wa = A.w[a];
+        vela = add(v3(va.x, va.y, va.z), cross(v3(wa.x, wa.y, wa.z), ra));
+    }
+    if (hasb) {
+        float4 pb = A.pos[b];
+        rb = sub(p, v3(pb.x, pb.y, pb.z));
+#pragma unroll
+        for (int q = 0; q < 9; q++) iib[q] = A.iiw[(size_t)b * 9 + q];
+        imb = A.im[b];
+        float4 vb = A.v[b], wb = A.w[b];
+        velb = add(v3(vb.x, vb.y, vb.z), cross(v3(wb.x, wb.y, wb.z), rb));
+    }
+    float mn = eff_mass(ima, iia, hasb, imb, iib, ra, rb, n);
+    V3 dv = sub(vela, velb);
+    float vn = dot(dv, n);
+    float vn0 = maxf(-vn, 0.0f);
+    V3 vt = sub(dv, mul(n, vn));
+    float lt = len(vt);
+    V3 t1;
+    if (lt > 1e-4f) t1 = mul(vt, div_rn(1.0f, lt));
+    else {
+        V3 tt = fabsf(n.x) < 0.9f ? v3(1.0f, 0.0f, 0.0f) : v3(0.0f, 1.0f, 0.0f);
+        V3 x = cross(n, tt);
+        t1 = mul(x, div_rn(1.0f, len(x)));
+    }
+    V3 t2 = cross(n, t1);
+    float mt1 = eff_mass(ima, iia, hasb, imb, iib, ra, rb, t1);
+    float mt2 = eff_mass(ima, iia, hasb, imb, iib, ra, rb, t2);
+    float bias = minf(div_rn(0.2f, A.h) * maxf(depth - 0.01f, 0.0f), 1.0f);
+    if (vn < -2.0f) bias = maxf(bias, -0.12f * vn);
+    A.S_n[t] = make_float4(n.x, n.y, n.z, mn);
+    A.S_t1[t] = make_float4(t1.x, t1.y, t1.z, mt1);
+    A.S_t2[t] = make_float4(t2.x, t2.y, t2.z, mt2);
+    A.S_ra[t] = make_float4(ra.x, ra.y, ra.z, bias);
+    A.S_rb[t] = make_float4(rb.x, rb.y, rb.z, vn0);
+    A.S_j[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    A.invperm[k] = t;
+}
+
+// ---------------------------------------------------------------- colouring
+__global__ void k_bm_count(const uint32_t *nm_p, const uint32_t *man_a, const uint32_t *man_b, uint32_t *bm_count) {
+    uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= *nm_p) return;
+    atomicAdd(&bm_count[man_a[m]], 1u);
+    uint32_t b = man_b[m];
+    if (b != STATIC) atomicAdd(&bm_count[b], 1u);
+}
+__global__ void k_bm_fill(const uint32_t *nm_p, const uint32_t *man_a, const uint32_t *man_b, const uint32_t *bm_start,
+                          uint32_t *bm_fill, uint32_t *bm_list) {
+    uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= *nm_p) return;
+    uint32_t a = man_a[m];
+    bm_list[bm_start[a] + atomicAdd(&bm_fill[a], 1u)] = m;
+    uint32_t b = man_b[m];
+    if (b != STATIC) bm_list[bm_start[b] + atomicAdd(&bm_fill[b], 1u)] = m;
+}
+
+struct JpArgs {
+    const uint32_t *nm_p;
+    const uint32_t *man_a, *man_b, *prio, *bm_start, *bm_list;
+    uint32_t *man_round, *man_color, *masks;
+    uint32_t *wl0, *wl1, *dev;
+    uint32_t max_colors, max_rounds;
+    GridBarrier *gb;
+    uint32_t *err;
+};
+
+__device__ __forceinline__ bool jp_blocked(const JpArgs &A, uint32_t body, uint32_t m, uint32_t pm, uint32_t r) {
+    const uint32_t s0 = A.bm_start[body], s1 = A.bm_start[body + 1];
+    for (uint32_t q = s0; q < s1; q++) {
+        const uint32_t nbr = A.bm_list[q];
+        if (nbr == m) continue;
+        if (__ldcg(&A.man_round[nbr]) < r) continue;   // coloured in an earlier round
+        const uint32_t pn = A.prio[nbr];
+        if (pn > pm || (pn == pm && nbr < m)) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(256) k_jp(JpArgs A) {
+    const uint32_t nm = *A.nm_p;
+    uint32_t r = 0;
+    for (; r < A.max_rounds; r++) {
+        const uint32_t n_in = r == 0 ? nm : __ldcg(&A.dev[DV_WL0 + (r % 3)]);
+        if (n_in == 0) break;
+        const uint32_t *wl_in = (r & 1) ? A.wl1 : A.wl0;
+        uint32_t *wl_out = (r & 1) ? A.wl0 : A.wl1;
+        uint32_t *cnt_out = &A.dev[DV_WL0 + ((r + 1) % 3)];
+        if (blockIdx.x == 0 && threadIdx.x == 0) A.dev[DV_WL0 + ((r + 2) % 3)] = 0;
+        for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_in; t += gridDim.x * blockDim.x) {
+            const uint32_t m = r == 0 ? t : __ldcg(&wl_in[t]);
+            const uint32_t a = A.man_a[m], b = A.man_b[m], pm = A.prio[m];
+            bool blocked = jp_blocked(A, a, m, pm, r);
+            if (!blocked && b != STATIC) blocked = jp_blocked(A, b, m, pm, r);
+            if (blocked) {
+                wl_out[atomicAdd(cnt_out, 1u)] = m;
+                continue;
+            }
+            uint32_t used[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) used[k] = __ldcg(&A.masks[(size_t)a * 4 + k]) | (b != STATIC ? __ldcg(&A.masks[(size_t)b * 4 + k]) : 0u);
+            uint32_t c = 0xFFFFFFFFu;
+#pragma unroll
+            for (int k = 0; k < 4; k++) if (c == 0xFFFFFFFFu && ~used[k]) c = 32 * k + (__ffs(~used[k]) - 1);
+            if (c >= A.max_colors) { atomicOr(A.err, (unsigned)ERR_CAPACITY_COLORS); c = A.max_colors - 1; }
+            A.man_color[m] = c;
+            atomicExch(&A.man_round[m], r);
+            atomicOr(&A.masks[(size_t)a * 4 + (c >> 5)], 1u << (c & 31));
+            if (b != STATIC) atomicOr(&A.masks[(size_t)b * 4 + (c >> 5)], 1u << (c & 31));
+        }
+        if (!grid_sync(A.gb, gridDim.x, A.err)) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        A.dev[DV_ROUNDS] = r;
+        if (r >= A.max_rounds) atomicOr(A.err, (unsigned)ERR_JP_ROUNDS);
+    }
+}
+
+__global__ void k_col_count(const uint32_t *nm_p, const uint32_t *man_color, uint32_t *col_count, uint32_t *dev) {
+    uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= *nm_p) return;
+    uint32_t c = man_color[m];
+    atomicAdd(&col_count[c], 1u);
+    atomicMax(&dev[DV_COLORS], c + 1);
+}
+__global__ void k_col_fill(const uint32_t *nm_p, const uint32_t *man_color, const uint32_t *col_start, uint32_t *col_fill,
+                           uint32_t *col_list) {
+    uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= *nm_p) return;
+    uint32_t c = man_color[m];
+    col_list[col_start[c] + atomicAdd(&col_fill[c], 1u)] = m;
+}
+// proper-colouring check: no two manifolds of one colour at one awake body
+__global__ void k_col_verify(const uint32_t *nm_p, const uint32_t *man_a, const uint32_t *man_b, const uint32_t *man_color,
+                             uint32_t *vmasks, uint32_t *err) {
+    uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= *nm_p) return;
+    uint32_t c = man_color[m];
+    uint32_t bit = 1u << (c & 31);
+    if (atomicOr(&vmasks[(size_t)man_a[m] * 4 + (c >> 5)], bit) & bit) atomicOr(err, (unsigned)ERR_VERIFY_COLOR);
+    uint32_t b = man_b[m];
+    if (b != STATIC && (atomicOr(&vmasks[(size_t)b * 4 + (c >> 5)], bit) & bit)) atomicOr(err, (unsigned)ERR_VERIFY_COLOR);
+}
+
+// ---------------------------------------------------------------- the coloured sequential-impulse solve
+struct SolveArgs {
+    uint32_t iterations;
+    const uint32_t *dev;           // DV_COLORS
+    const uint32_t *col_start, *col_list;
+    const uint32_t *man_a, *man_b, *man_start, *man_count;
+    const float4 *S_n, *S_t1, *S_t2, *S_ra, *S_rb;
+    float4 *S_j;
+    float4 *v, *w;
+    const float *im, *iiw;
+    GridBarrier *gb;
+    uint32_t *err;
+};
+
+__device__ __forceinline__ void solve_manifold(const SolveArgs &A, uint32_t m) {
+    const uint32_t a = A.man_a[m], b = A.man_b[m];
+    const bool hasb = b != STATIC;
+    const uint32_t s0 = A.man_start[m], cnt = A.man_count[m];
+    float4 t4 = __ldcg(&A.v[a]);
+    V3 va = v3(t4.x, t4.y, t4.z);
+    t4 = __ldcg(&A.w[a]);
+    V3 wa = v3(t4.x, t4.y, t4.z);
+    const float ima = A.im[a];
+    float ia[9], ib[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) ia[q] = A.iiw[(size_t)a * 9 + q];
+    V3 vb = v3(0.0f, 0.0f, 0.0f), wb = v3(0.0f, 0.0f, 0.0f);
+    float imb = 0.0f;
+    if (hasb) {
+        t4 = __ldcg(&A.v[b]); vb = v3(t4.x, t4.y, t4.z);
+        t4 = __ldcg(&A.w[b]); wb = v3(t4.x, t4.y, t4.z);
+        imb = A.im[b];
+#pragma unroll
+        for (int q = 0; q < 9; q++) ib[q] = A.iiw[(size_t)b * 9 + q];
+    }
+    for (uint32_t k = s0; k < s0 + cnt; k++) {
+        const float4 n4 = A.S_n[k], t14 = A.S_t1[k], t24 = A.S_t2[k], ra4 = A.S_ra[k], rb4 = A.S_rb[k];
+        float4 j4 = __ldcg(&A.S_j[k]);
+        const V3 n = v3(n4.x, n4.y, n4.z), t1 = v3(t14.x, t14.y, t14.z), t2 = v3(t24.x, t24.y, t24.z);
+        const V3 ra = v3(ra4.x, ra4.y, ra4.z), rb = v3(rb4.x, rb4.y, rb4.z);
+        const float mn = n4.w, mt1 = t14.w, mt2 = t24.w, bias = ra4.w;
+        // normal
+        V3 dv = sub(add(va, cross(wa, ra)), hasb ? add(vb, cross(wb, rb)) : v3(0.0f, 0.0f, 0.0f));
+        float vn = dot(dv, n);
+        float lam = mn * (-vn + bias);
+        float old = j4.x;
+        j4.x = maxf(old + lam, 0.0f);
+        float d = j4.x - old;
+        {
+            V3 P = mul(n, d);
+            va = madd(va, P, ima);
+            wa = add(wa, mv(ia, cross(ra, P)));
+            if (hasb) { vb = madd(vb, P, -imb); wb = sub(wb, mv(ib, cross(rb, P))); }
+        }
+        // friction, two independent clamps
+        float lim = MU * j4.x;
+        dv = sub(add(va, cross(wa, ra)), hasb ? add(vb, cross(wb, rb)) : v3(0.0f, 0.0f, 0.0f));
+        float l1 = -mt1 * dot(dv, t1);
+        float o1 = j4.y;
+        j4.y = clampf(o1 + l1, -lim, lim);
+        float l2 = -mt2 * dot(dv, t2);
+        float o2 = j4.z;
+        j4.z = clampf(o2 + l2, -lim, lim);
+        {
+            V3 P = add(mul(t1, j4.y - o1), mul(t2, j4.z - o2));
+            va = madd(va, P, ima);
+            wa = add(wa, mv(ia, cross(ra, P)));
+            if (hasb) { vb = madd(vb, P, -imb); wb = sub(wb, mv(ib, cross(rb, P))); }
+        }
+        A.S_j[k] = j4;
+    }
+    A.v[a] = make_float4(va.x, va.y, va.z, 0.0f);
+    A.w[a] = make_float4(wa.x, wa.y, wa.z, 0.0f);
+    if (hasb) {
+        A.v[b] = make_float4(vb.x, vb.y, vb.z, 0.0f);
+        A.w[b] = make_float4(wb.x, wb.y, wb.z, 0.0f);
+    }
+}
+
+constexpr int SOLVE_BLOCK = 128;
+
+__global__ void __launch_bounds__(SOLVE_BLOCK) k_solve(SolveArgs A) {
+    const uint32_t ncol = A.dev[DV_COLORS];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t it = 0; it < A.iterations; it++) {
+        for (uint32_t c = 0; c < ncol; c++) {
+            const uint32_t s0 = A.col_start[c], s1 = A.col_start[c + 1];
+            for (uint32_t t = s0 + blockIdx.x * blockDim.x + threadIdx.x; t < s1; t += stride) solve_manifold(A, A.col_list[t]);
+            if (!grid_sync(A.gb, gridDim.x, A.err)) return;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- islands
+__global__ void k_uf_init(uint32_t nb, uint32_t *parent, uint32_t *mint) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    parent[b] = b;
+    mint[b] = 0x7f7fffffu;
+}
+__device__ __forceinline__ uint32_t uf_find(uint32_t *parent, uint32_t x) {
+    for (int guard = 0; guard < (1 << 20); guard++) {
+        uint32_t p = __ldcg(&parent[x]);
+        if (p == x) return x;
+        uint32_t gp = __ldcg(&parent[p]);
+        if (gp != p) atomicCAS(&parent[x], p, gp);
+        x = p;
+    }
+    return x;
+}
+__global__ void k_uf_union(const uint32_t *nm_p, const uint32_t *man_a, const uint32_t *man_b, uint32_t *parent) {
+    uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= *nm_p) return;
+    uint32_t b = man_b[m];
+    if (b == STATIC) return;
+    uint32_t x = man_a[m], y = b;
+    for (int it = 0; it < (1 << 16); it++) {
+        x = uf_find(parent, x);
+        y = uf_find(parent, y);
+        if (x == y) return;
+        if (x < y) { uint32_t t = x; x = y; y = t; }
+        if (atomicCAS(&parent[x], x, y) == x) return;
+    }
+}
+__global__ void k_uf_label(uint32_t nb, const uint8_t *alive, const uint8_t *asleep, uint32_t *parent, uint32_t *label,
+                           uint32_t *dev) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    if (!alive[b] || asleep[b]) { label[b] = NONE; return; }
+    uint32_t r = uf_find(parent, b);
+    label[b] = r;
+    if (r == b) atomicAdd(&dev[DV_ISLANDS], 1u);
+}
+
+// ---------------------------------------------------------------- pinch clamps + integrate
+struct IntArgs {
+    uint32_t nb;
+    float h;
+    int pinch_kill, island_mode;
+    uint8_t *alive, *asleep;
+    float4 *pos, *q, *v, *w;
+    const float4 *vpre, *wpre;
+    const float *rad;
+    float *sleep;
+    const float *maxr;
+    const uint32_t *nc, *count, *first;
+    const uint8_t *kmat;
+};
+
+__device__ __forceinline__ void kill_mark(const IntArgs &A, uint32_t b) { A.alive[b] = 0; }
+
+__global__ void k_integrate(IntArgs A) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= A.nb || !A.alive[b] || A.asleep[b]) return;
+    float4 t4 = A.v[b];
+    V3 v = v3(t4.x, t4.y, t4.z);
+    t4 = A.w[b];
+    V3 w = v3(t4.x, t4.y, t4.z);
+    const float rad = A.rad[b];
+    // pinch_check (src/lib.rs:1746-1768)
+    {
+        float4 p4 = A.wpre[b];
+        V3 wpre = v3(p4.x, p4.y, p4.z);
+        p4 = A.vpre[b];
+        V3 vpre = v3(p4.x, p4.y, p4.z);
+        V3 dw = sub(w, wpre);
+        float tip = len(dw) * rad;
+        if (tip > 6.0f) w = madd(wpre, dw, div_rn(6.0f, tip));
+        V3 dv = sub(v, vpre);
+        float m = len(dv);
+        if (m >= 8.0f && A.kmat[A.first[b]] < SLUG) {
+            if (A.pinch_kill && A.count[b] <= 6) {
+                A.alive[b] = 0;
+                A.w[b] = make_float4(w.x, w.y, w.z, 0.0f);
+                return;
+            }
+            v = madd(vpre, dv, div_rn(8.0f, m));
+        }
+    }
+    // clamp_vel (src/lib.rs:917-924)
+    {
+        float vl = len(v);
+        if (vl > 60.0f) v = mul(v, div_rn(60.0f, vl));
+        float al = len(w);
+        float amax = minf(25.0f, div_rn(16.0f, maxf(rad, 0.3f)));
+        if (al > amax) w = mul(w, div_rn(amax, al));
+    }
+    const float h = A.h;
+    t4 = A.pos[b];
+    V3 p = madd(v3(t4.x, t4.y, t4.z), v, h);
+    // q_int (src/lib.rs:100-108)
+    float4 q4 = A.q[b];
+    {
+        V3 qv = v3(q4.x, q4.y, q4.z);
+        V3 d = add(mul(w, q4.w), cross(w, qv));
+        float dw = -dot(w, qv);
+        float r0 = q4.x + 0.5f * h * d.x, r1 = q4.y + 0.5f * h * d.y, r2 = q4.z + 0.5f * h * d.z, r3 = q4.w + 0.5f * h * dw;
+        float l = sqrt_rn(r0 * r0 + r1 * r1 + r2 * r2 + r3 * r3);
+        if (l > 1e-9f) q4 = make_float4(div_rn(r0, l), div_rn(r1, l), div_rn(r2, l), div_rn(r3, l));
+        else q4 = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    }
+    v = mul(v, 1.0f - 0.01f * h);
+    w = mul(w, 1.0f - 0.05f * h);
+    const bool small = A.count[b] <= 3;
+    const uint32_t nc = A.nc[b];
+    if (nc > 0 && small) {
+        w = mul(w, 1.0f - minf(7.0f * h, 0.5f));
+        v = mul(v, 1.0f - minf(2.0f * h, 0.3f));
+    }
+    float v2 = dot(v, v);
+    float w2 = dot(w, w) * rad * rad;
+    float vt = small ? 0.16f : 0.06f, wt = small ? 0.3f : 0.04f;
+    float sl = A.sleep[b];
+    uint8_t asl = 0;
+    if (v2 < vt && w2 < wt && nc > 0 && A.maxr[b] < 0.95f) {
+        sl += h;
+        if (!A.island_mode && sl > 0.45f) { asl = 1; v = v3(0.0f, 0.0f, 0.0f); w = v3(0.0f, 0.0f, 0.0f); }
+    } else sl = 0.0f;
+    A.sleep[b] = sl;
+    if (asl) A.asleep[b] = 1;
+    A.pos[b] = make_float4(p.x, p.y, p.z, 0.0f);
+    A.q[b] = q4;
+    A.v[b] = make_float4(v.x, v.y, v.z, 0.0f);
+    A.w[b] = make_float4(w.x, w.y, w.z, 0.0f);
+    if (p.y < -15.0f || fabsf(p.x) > 190.0f || fabsf(p.z) > 190.0f || p.y > 120.0f) A.alive[b] = 0;
+}
+
+__global__ void k_island_min(uint32_t nb, const uint8_t *alive, const uint32_t *label, const float *sleep, uint32_t *mint) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    uint32_t r = label[b];
+    if (r == NONE || !alive[b]) return;
+    atomicMin(&mint[r], __float_as_uint(sleep[b]));
+}
+__global__ void k_island_sleep(uint32_t nb, const uint8_t *alive, uint8_t *asleep, const uint32_t *label, const float *sleep,
+                               const uint32_t *mint, float4 *v, float4 *w) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    uint32_t r = label[b];
+    if (r == NONE || !alive[b] || asleep[b]) return;
+    if (__uint_as_float(mint[r]) > 0.45f || sleep[b] > 0.9f) {
+        asleep[b] = 1;
+        v[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        w[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+__global__ void k_wake(uint32_t nb, uint8_t *wake, const uint8_t *alive, uint8_t *asleep, float *sleep) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb || !wake[b]) return;
+    wake[b] = 0;
+    if (alive[b]) { asleep[b] = 0; sleep[b] = 0.0f; }
+}
+__global__ void k_save_pre(uint32_t nb, const uint8_t *alive, const float4 *v, const float4 *w, float4 *vpre, float4 *wpre) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb || !alive[b]) return;
+    vpre[b] = v[b];
+    wpre[b] = w[b];
+}
+__global__ void k_count_bodies(uint32_t nb, const uint8_t *alive, const uint8_t *asleep, uint32_t *dev) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t al = 0, aw = 0;
+    if (b < nb && alive[b]) { al = 1; aw = asleep[b] ? 0 : 1; }
+    al = __reduce_add_sync(0xffffffffu, al);
+    aw = __reduce_add_sync(0xffffffffu, aw);
+    if ((threadIdx.x & 31) == 0) {
+        if (al) atomicAdd(&dev[DV_ALIVE], al);
+        if (aw) atomicAdd(&dev[DV_AWAKE], aw);
+    }
+}
+// the kill of a body also removes its bricks (kill_body, src/lib.rs:826-843)
+__global__ void k_kill_bricks(uint32_t nd, const uint32_t *kbody, const uint8_t *alive, uint8_t *kmat) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nd) return;
+    if (!alive[kbody[i]]) kmat[i] = 0;
+}
+
+// ---------------------------------------------------------------- host side
+static int bits_for(uint64_t v) { int b = 0; while (b < 64 && (v >> b) != 0) b++; return b; }
+
+static cudaError_t grow_contacts(StepState *S, uint64_t need) {
+    if (need <= S->capacity) return cudaSuccess;
+    uint64_t cap = std::max<uint64_t>(need + need / 2, 4096);
+    cudaError_t e;
+#define G(buf) if ((e = S->buf.alloc(cap)) != cudaSuccess) return e
+    G(L_a); G(L_b); G(L_bo); G(L_ba); G(L_bb); G(L_p); G(L_n);
+    G(mkey); G(mkey_alt); G(perm); G(perm_alt); G(invperm); G(mflag); G(mpos);
+    G(man_a); G(man_b); G(man_start); G(man_count); G(man_prio); G(man_color); G(man_round);
+    G(S_n); G(S_t1); G(S_t2); G(S_ra); G(S_rb); G(S_j);
+    G(wl0); G(wl1); G(col_list);
+#undef G
+    if ((e = S->bm_list.alloc(2 * cap)) != cudaSuccess) return e;
+    S->capacity = cap;
+    return cudaSuccess;
+}
+
+sf_status step_create(sf_world *w) {
+    StepState *S = new StepState();
+    w->step = S;
+    uint32_t nb = w->nb, nd = w->nd;
+    cudaStream_t s = w->stream;
+    SF_CUDA(S->ckey.alloc(nd)); SF_CUDA(S->ckey_alt.alloc(nd)); SF_CUDA(S->cval.alloc(nd)); SF_CUDA(S->cval_alt.alloc(nd));
+    SF_CUDA(S->bstart.alloc((size_t)w->n_scenes * HSIZE)); SF_CUDA(S->bend.alloc((size_t)w->n_scenes * HSIZE));
+    SF_CUDA(S->ccount.alloc((size_t)nd + 1)); SF_CUDA(S->coff.alloc((size_t)nd + 1));
+    SF_CUDA(S->bm_count.alloc((size_t)nb + 1)); SF_CUDA(S->bm_start.alloc((size_t)nb + 1)); SF_CUDA(S->bm_fill.alloc((size_t)nb + 1));
+    SF_CUDA(S->masks.alloc((size_t)nb * 4 + 4)); SF_CUDA(S->vmasks.alloc((size_t)nb * 4 + 4));
+    SF_CUDA(S->col_count.alloc(MAXCOL + 2)); SF_CUDA(S->col_start.alloc(MAXCOL + 2)); SF_CUDA(S->col_fill.alloc(MAXCOL + 2));
+    SF_CUDA(S->parent.alloc(nb)); SF_CUDA(S->label.alloc(nb)); SF_CUDA(S->mint.alloc(nb));
+    SF_CUDA(cudaMemsetAsync(S->label.p, 0xFF, S->label.bytes(), s));
+    SF_CUDA(S->dev.alloc(DV_N));
+    SF_CUDA(cudaMallocHost((void **)&S->h_dev, DV_N * sizeof(uint32_t)));
+    std::vector<uint32_t> off(nb);
+    for (const Scene &sc : w->scenes) for (uint32_t b = 0; b < sc.n_bodies; b++) off[sc.body_off + b] = sc.body_off;
+    SF_CUDA(S->body_off_of_body.alloc(nb));
+    if (nb) SF_CUDA(cudaMemcpyAsync(S->body_off_of_body.p, off.data(), nb * 4, cudaMemcpyHostToDevice, s));
+    uint64_t initial = w->P.contact_capacity ? w->P.contact_capacity : (uint64_t)std::max<uint32_t>(nd, 1) * 4;
+    SF_CUDA(grow_contacts(S, initial));
+    int occ = 0;
+    SF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve, SOLVE_BLOCK, 0));
+    S->solve_occ = std::max(1, occ);
+    SF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jp, 256, 0));
+    S->jp_occ = std::max(1, occ);
+    return SF_OK;
+}
+
+void step_destroy(sf_world *w) {
+    if (w->step && w->step->h_dev) cudaFreeHost(w->step->h_dev);
+    delete w->step;
+    w->step = nullptr;
+}
+
+static sf_status substep(sf_world *w, float h) {
+    StepState *S = w->step;
+    cudaStream_t s = w->stream;
+    const uint32_t nb = w->nb, nd = w->nd;
+    const uint64_t none_key = (uint64_t)w->n_scenes * HSIZE;
+    if (nb == 0 || nd == 0) return SF_OK;
+    // pose cache + gravity, brick positions
+    k_update_cache<<<grid_for(nb, 128), 128, 0, s>>>(nb, h, w->b_alive.p, w->b_asleep.p, w->b_q.p, w->b_iil.p, w->b_rot.p,
+                                                     w->b_iiw.p, w->b_v.p);
+    k_brick_pos<<<grid_for(nd, 256), 256, 0, s>>>(nd, w->k_body.p, w->b_alive.p, w->b_asleep.p, w->b_pos.p, w->b_rot.p,
+                                                  w->k_local.p, w->k_wpos.p);
+    // hashed cells
+    k_cell_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, w->k_body.p, w->b_scene.p, w->b_alive.p, w->k_wpos.p,
+                                                  S->ckey.p, S->cval.p);
+    SF_CUDA(radix_sort_u64(S->ckey.p, S->cval.p, S->ckey_alt.p, S->cval_alt.p, nd, bits_for(none_key), S->wk, s));
+    SF_CUDA(cudaMemsetAsync(S->bstart.p, 0, S->bstart.bytes(), s));
+    SF_CUDA(cudaMemsetAsync(S->bend.p, 0, S->bend.bytes(), s));
+    k_bucket_ranges<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, S->ckey.p, S->bstart.p, S->bend.p);
+    // contacts: count, scan, fill
+    ContactArgs C;
+    C.nd = nd; C.kbody = w->k_body.p; C.bscene = w->b_scene.p; C.ctab = w->ctab.p; C.cpool = w->cpool.p;
+    C.alive = w->b_alive.p; C.asleep = w->b_asleep.p; C.kmat = w->k_mat.p; C.smat = w->s_mat.p; C.wpos = w->k_wpos.p;
+    C.v = w->b_v.p; C.w = w->b_w.p; C.rot = w->b_rot.p; C.rad = w->b_rad.p; C.bstart = S->bstart.p; C.bend = S->bend.p;
+    C.cval = S->cval.p; C.ccount = S->ccount.p; C.coff = S->coff.p; C.wake = w->b_wake.p;
+    C.L_a = S->L_a.p; C.L_b = S->L_b.p; C.L_bo = S->L_bo.p; C.L_ba = S->L_ba.p; C.L_bb = S->L_bb.p; C.L_p = S->L_p.p; C.L_n = S->L_n.p;
+    k_contacts<false><<<grid_for(nd, 128), 128, 0, s>>>(C);
+    SF_CUDA(exclusive_scan_u32(S->ccount.p, S->coff.p, nd, S->dev.p + DV_CONTACTS, S->wk, s));
+    SF_CUDA(cudaMemcpyAsync(S->h_dev, S->dev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    const uint32_t nc = S->h_dev[DV_CONTACTS];
+    S->last_contacts = nc;
+    if (nc > S->capacity) {
+        if (w->P.contact_capacity) { set_error("%u contacts exceed the fixed capacity %llu", nc, (unsigned long long)S->capacity); return SF_ERR_CAPACITY; }
+        SF_CUDA(grow_contacts(S, nc));
+        C.L_a = S->L_a.p; C.L_b = S->L_b.p; C.L_bo = S->L_bo.p; C.L_ba = S->L_ba.p; C.L_bb = S->L_bb.p; C.L_p = S->L_p.p; C.L_n = S->L_n.p;
+    }
+    k_contacts<true><<<grid_for(nd, 128), 128, 0, s>>>(C);
+    SF_CUDA(cudaMemsetAsync(w->b_nc.p, 0, w->b_nc.bytes(), s));
+    SF_CUDA(cudaMemsetAsync(S->dev.p + DV_MANIFOLDS, 0, (DV_N - DV_MANIFOLDS) * sizeof(uint32_t), s));
+    const uint32_t g_nc = grid_for(std::max<uint32_t>(nc, 1), 256);
+    if (nc) k_body_nc<<<g_nc, 256, 0, s>>>(nc, S->L_a.p, S->L_b.p, w->b_nc.p);
+    // manifolds
+    const uint64_t nb1 = (uint64_t)nb + 1;
+    if (nc) {
+        k_man_keys<<<g_nc, 256, 0, s>>>(nc, nb1, S->L_a.p, S->L_b.p, S->mkey.p, S->perm.p);
+        SF_CUDA(radix_sort_u64(S->mkey.p, S->perm.p, S->mkey_alt.p, S->perm_alt.p, nc, bits_for((uint64_t)nb * nb1 + nb1), S->wk, s));
+        k_man_flags<<<g_nc, 256, 0, s>>>(nc, S->mkey.p, S->mflag.p);
+        SF_CUDA(exclusive_scan_u32(S->mflag.p, S->mpos.p, nc, S->dev.p + DV_MANIFOLDS, S->wk, s));
+        k_man_write<<<g_nc, 256, 0, s>>>(nc, S->mflag.p, S->mpos.p, S->perm.p, S->L_a.p, S->L_b.p, w->b_scene.p,
+                                         S->body_off_of_body.p, S->man_a.p, S->man_b.p, S->man_start.p, S->man_prio.p);
+        k_man_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, nc, S->man_start.p, S->man_count.p);
+        PrepArgs PA;
+        PA.nc = nc; PA.h = h; PA.perm = S->perm.p; PA.L_a = S->L_a.p; PA.L_b = S->L_b.p; PA.L_p = S->L_p.p; PA.L_n = S->L_n.p;
+        PA.pos = w->b_pos.p; PA.v = w->b_v.p; PA.w = w->b_w.p; PA.im = w->b_im.p; PA.iiw = w->b_iiw.p;
+        PA.S_n = S->S_n.p; PA.S_t1 = S->S_t1.p; PA.S_t2 = S->S_t2.p; PA.S_ra = S->S_ra.p; PA.S_rb = S->S_rb.p; PA.S_j = S->S_j.p;
+        PA.invperm = S->invperm.p;
+        k_prep<<<g_nc, 256, 0, s>>>(PA);
+        // colouring
+        SF_CUDA(cudaMemsetAsync(S->bm_count.p, 0, S->bm_count.bytes(), s));
+        SF_CUDA(cudaMemsetAsync(S->bm_fill.p, 0, S->bm_fill.bytes(), s));
+        SF_CUDA(cudaMemsetAsync(S->masks.p, 0, S->masks.bytes(), s));
+        SF_CUDA(cudaMemsetAsync(S->man_round.p, 0xFF, (size_t)nc * 4, s));
+        k_bm_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_a.p, S->man_b.p, S->bm_count.p);
+        SF_CUDA(exclusive_scan_u32(S->bm_count.p, S->bm_start.p, (size_t)nb + 1, nullptr, S->wk, s));
+        k_bm_fill<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_a.p, S->man_b.p, S->bm_start.p, S->bm_fill.p, S->bm_list.p);
+        SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s));
+        JpArgs J;
+        J.nm_p = S->dev.p + DV_MANIFOLDS; J.man_a = S->man_a.p; J.man_b = S->man_b.p; J.prio = S->man_prio.p;
+        J.bm_start = S->bm_start.p; J.bm_list = S->bm_list.p; J.man_round = S->man_round.p; J.man_color = S->man_color.p;
+        J.masks = S->masks.p; J.wl0 = S->wl0.p; J.wl1 = S->wl1.p; J.dev = S->dev.p; J.max_colors = w->P.max_colors;
+        J.max_rounds = 1u << 16; J.gb = w->barrier.p; J.err = w->err.p;
+        unsigned jgrid = (unsigned)std::min<uint64_t>((uint64_t)w->sms * S->jp_occ, (nc + 255) / 256 + 1);
+        void *jargs[] = {&J};
+        SF_CUDA(cudaLaunchCooperativeKernel((void *)k_jp, dim3(jgrid), dim3(256), jargs, 0, s));
+        SF_CUDA(cudaMemsetAsync(S->col_count.p, 0, S->col_count.bytes(), s));
+        SF_CUDA(cudaMemsetAsync(S->col_fill.p, 0, S->col_fill.bytes(), s));
+        k_col_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_color.p, S->col_count.p, S->dev.p);
+        SF_CUDA(exclusive_scan_u32(S->col_count.p, S->col_start.p, MAXCOL + 1, nullptr, S->wk, s));
+        k_col_fill<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_color.p, S->col_start.p, S->col_fill.p, S->col_list.p);
+        if (w->P.verify) {
+            SF_CUDA(cudaMemsetAsync(S->vmasks.p, 0, S->vmasks.bytes(), s));
+            k_col_verify<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_a.p, S->man_b.p, S->man_color.p, S->vmasks.p, w->err.p);
+        }
+    }
+    k_save_pre<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, w->b_v.p, w->b_w.p, w->b_vpre.p, w->b_wpre.p);
+    if (nc && w->P.iterations) {
+        SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s));
+        SolveArgs A;
+        A.iterations = w->P.iterations; A.dev = S->dev.p; A.col_start = S->col_start.p; A.col_list = S->col_list.p;
+        A.man_a = S->man_a.p; A.man_b = S->man_b.p; A.man_start = S->man_start.p; A.man_count = S->man_count.p;
+        A.S_n = S->S_n.p; A.S_t1 = S->S_t1.p; A.S_t2 = S->S_t2.p; A.S_ra = S->S_ra.p; A.S_rb = S->S_rb.p; A.S_j = S->S_j.p;
+        A.v = w->b_v.p; A.w = w->b_w.p; A.im = w->b_im.p; A.iiw = w->b_iiw.p; A.gb = w->barrier.p; A.err = w->err.p;
+        unsigned per_sm = w->P.solve_blocks ? std::min<unsigned>(w->P.solve_blocks, S->solve_occ) : S->solve_occ;
+        unsigned sgrid = (unsigned)std::min<uint64_t>((uint64_t)w->sms * per_sm, (nc + SOLVE_BLOCK - 1) / SOLVE_BLOCK + 1);
+        void *sargs[] = {&A};
+        SF_CUDA(cudaLaunchCooperativeKernel((void *)k_solve, dim3(sgrid), dim3(SOLVE_BLOCK), sargs, 0, s));
+    }
+    // islands over the manifolds of this substep
+    k_uf_init<<<grid_for(nb, 256), 256, 0, s>>>(nb, S->parent.p, S->mint.p);
+    if (nc) k_uf_union<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_a.p, S->man_b.p, S->parent.p);
+    k_uf_label<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, w->b_asleep.p, S->parent.p, S->label.p, S->dev.p);
+    IntArgs I;
+    I.nb = nb; I.h = h; I.pinch_kill = w->P.pinch_kill ? 1 : 0; I.island_mode = w->P.sleep_mode == SF_SLEEP_ISLAND;
+    I.alive = w->b_alive.p; I.asleep = w->b_asleep.p; I.pos = w->b_pos.p; I.q = w->b_q.p; I.v = w->b_v.p; I.w = w->b_w.p;
+    I.vpre = w->b_vpre.p; I.wpre = w->b_wpre.p; I.rad = w->b_rad.p; I.sleep = w->b_sleep.p; I.maxr = w->b_maxr.p;
+    I.nc = w->b_nc.p; I.count = w->b_count.p; I.first = w->b_first.p; I.kmat = w->k_mat.p;
+    k_integrate<<<grid_for(nb, 128), 128, 0, s>>>(I);
+    if (I.island_mode) {
+        k_island_min<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, S->label.p, w->b_sleep.p, S->mint.p);
+        k_island_sleep<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, w->b_asleep.p, S->label.p, w->b_sleep.p, S->mint.p,
+                                                         w->b_v.p, w->b_w.p);
+    }
+    k_wake<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_wake.p, w->b_alive.p, w->b_asleep.p, w->b_sleep.p);
+    k_kill_bricks<<<grid_for(nd, 256), 256, 0, s>>>(nd, w->k_body.p, w->b_alive.p, w->k_mat.p);
+    SF_CUDA(cudaGetLastError());
+    S->have_contacts = true;
+    return SF_OK;
+}
+
+}  // namespace sf
+
+using namespace sf;
+
+extern "C" {
+
+sf_status sf_world_step(sf_world *w, float dt, uint32_t nsteps) {
+    if (!w) return SF_ERR_ARG;
+    if (!(dt == dt)) { set_error("dt is NaN"); return SF_ERR_ARG; }
+    StepState *S = w->step;
+    cudaStream_t s = w->stream;
+    dt = clampf(dt, 0.0f, 1.0f / 30.0f);
+    const uint32_t ns = w->P.substeps;
+    const float h = ns == 2 ? dt * 0.5f : dt / (float)ns;
+    SF_CUDA(cudaMemsetAsync(w->err.p, 0, sizeof(uint32_t), s));
+    SF_CUDA(cudaEventRecord(w->ev0, s));
+    for (uint32_t k = 0; k < nsteps; k++) {
+        w->frame++;
+        for (uint32_t q = 0; q < ns; q++) {
+            sf_status r = substep(w, h);
+            if (r != SF_OK) return r;
+        }
+    }
+    SF_CUDA(cudaMemsetAsync(S->dev.p + DV_ALIVE, 0, 2 * sizeof(uint32_t), s));
+    if (w->nb) k_count_bodies<<<grid_for(w->nb, 256), 256, 0, s>>>(w->nb, w->b_alive.p, w->b_asleep.p, S->dev.p);
+    SF_CUDA(cudaEventRecord(w->ev1, s));
+    SF_CUDA(cudaMemcpyAsync(S->h_dev, S->dev.p, DV_N * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    sf_status r = read_error_word(w);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, w->ev0, w->ev1);
+    sf_stats &st = w->stats;
+    st.contacts = S->h_dev[DV_CONTACTS];
+    st.manifolds = S->h_dev[DV_MANIFOLDS];
+    st.colors = S->h_dev[DV_COLORS];
+    st.color_rounds = S->h_dev[DV_ROUNDS];
+    st.islands = S->h_dev[DV_ISLANDS];
+    st.alive = S->h_dev[DV_ALIVE];
+    st.awake = S->h_dev[DV_AWAKE];
+    st.contact_capacity = S->capacity;
+    st.ms_last_step = ms;
+    return r;
+}
+
+sf_status sf_read_contacts(sf_world *w, uint32_t scene, uint32_t *ids5, float *f7, float *s8, uint64_t cap, uint64_t *n) {
+    if (!w || scene >= w->n_scenes) return SF_ERR_ARG;
+    StepState *S = w->step;
+    if (!S->have_contacts) { set_error("no step has run yet"); return SF_ERR_STATE; }
+    const Scene &sc = w->scenes[scene];
+    uint32_t nc = (uint32_t)S->last_contacts;
+    cudaStream_t s = w->stream;
+    // the scene's contacts are the list range of its bricks
+    uint32_t lo = 0, hi = 0;
+    if (sc.n_bricks) {
+        SF_CUDA(cudaMemcpyAsync(&lo, S->coff.p + sc.brick_off, 4, cudaMemcpyDeviceToHost, s));
+        if (sc.brick_off + sc.n_bricks < w->nd) SF_CUDA(cudaMemcpyAsync(&hi, S->coff.p + sc.brick_off + sc.n_bricks, 4, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaStreamSynchronize(s));
+        if (sc.brick_off + sc.n_bricks >= w->nd) hi = nc;
+    }
+    uint64_t cnt = hi - lo;
+    if (n) *n = cnt;
+    if (!ids5 && !f7 && !s8) return SF_OK;
+    if (cap < cnt) { set_error("contact buffer holds %llu, need %llu", (unsigned long long)cap, (unsigned long long)cnt); return SF_ERR_CAPACITY; }
+    std::vector<uint32_t> a(cnt), b(cnt), bo(cnt), ba(cnt), bb(cnt), inv(cnt);
+    std::vector<float4> p(cnt), nn(cnt);
+    if (cnt) {
+        SF_CUDA(cudaMemcpyAsync(a.data(), S->L_a.p + lo, cnt * 4, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(b.data(), S->L_b.p + lo, cnt * 4, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(bo.data(), S->L_bo.p + lo, cnt * 4, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(ba.data(), S->L_ba.p + lo, cnt * 4, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(bb.data(), S->L_bb.p + lo, cnt * 4, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(p.data(), S->L_p.p + lo, cnt * 16, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(nn.data(), S->L_n.p + lo, cnt * 16, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(inv.data(), S->invperm.p + lo, cnt * 4, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaStreamSynchronize(s));
+    }
+    std::vector<float4> sn, st1, st2, sra, srb, sj;
+    if (s8 && cnt) {
+        uint32_t mlo = *std::min_element(inv.begin(), inv.end()), mhi = *std::max_element(inv.begin(), inv.end()) + 1;
+        size_t m = mhi - mlo;
+        sn.resize(m); st1.resize(m); st2.resize(m); sra.resize(m); srb.resize(m); sj.resize(m);
+        SF_CUDA(cudaMemcpyAsync(sn.data(), S->S_n.p + mlo, m * 16, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(st1.data(), S->S_t1.p + mlo, m * 16, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(st2.data(), S->S_t2.p + mlo, m * 16, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(sra.data(), S->S_ra.p + mlo, m * 16, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(srb.data(), S->S_rb.p + mlo, m * 16, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(sj.data(), S->S_j.p + mlo, m * 16, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaStreamSynchronize(s));
+        for (auto &x : inv) x -= mlo;
+    }
+    auto loc_body = [&](uint32_t g) { return g == STATIC ? STATIC : g - sc.body_off; };
+    auto loc_dyn = [&](uint32_t g) { return sc.n_static + (g - sc.brick_off); };
+    for (uint64_t k = 0; k < cnt; k++) {
+        if (ids5) {
+            uint32_t *o = ids5 + k * 5;
+            o[0] = loc_body(a[k]); o[1] = loc_body(b[k]); o[2] = loc_body(bo[k]); o[3] = loc_dyn(ba[k]);
+            if (bb[k] == NONE) o[4] = NONE;
+            else if (bo[k] == STATIC) o[4] = bb[k] - sc.static_off;
+            else o[4] = loc_dyn(bb[k]);
+        }
+        if (f7) {
+            float *g = f7 + k * 7;
+            g[0] = p[k].x; g[1] = p[k].y; g[2] = p[k].z; g[3] = nn[k].x; g[4] = nn[k].y; g[5] = nn[k].z; g[6] = nn[k].w;
+        }
+        if (s8) {
+            uint32_t t = inv[k];
+            float *x = s8 + k * 8;
+            x[0] = sj[t].x; x[1] = sj[t].y; x[2] = sj[t].z; x[3] = sn[t].w; x[4] = st1[t].w; x[5] = st2[t].w; x[6] = sra[t].w; x[7] = srb[t].w;
+        }
+    }
+    return SF_OK;
+}
+
+sf_status sf_read_manifolds(sf_world *w, uint32_t scene, uint32_t *out4, uint64_t cap, uint64_t *n) {
+    if (!w || scene >= w->n_scenes) return SF_ERR_ARG;
+    StepState *S = w->step;
+    if (!S->have_contacts) { set_error("no step has run yet"); return SF_ERR_STATE; }
+    const Scene &sc = w->scenes[scene];
+    cudaStream_t s = w->stream;
+    uint32_t nm = 0;
+    SF_CUDA(cudaMemcpyAsync(&nm, S->dev.p + DV_MANIFOLDS, 4, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    std::vector<uint32_t> a(nm), b(nm), c(nm), k(nm);
+    if (nm) {
+        SF_CUDA(cudaMemcpyAsync(a.data(), S->man_a.p, nm * 4, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(b.data(), S->man_b.p, nm * 4, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(c.data(), S->man_color.p, nm * 4, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaMemcpyAsync(k.data(), S->man_count.p, nm * 4, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaStreamSynchronize(s));
+    }
+    uint64_t cnt = 0;
+    for (uint32_t m = 0; m < nm; m++) {
+        if (a[m] < sc.body_off || a[m] >= sc.body_off + sc.n_bodies) continue;
+        if (out4 && cnt < cap) {
+            uint32_t *o = out4 + cnt * 4;
+            o[0] = a[m] - sc.body_off; o[1] = b[m] == STATIC ? STATIC : b[m] - sc.body_off; o[2] = c[m]; o[3] = k[m];
+        }
+        cnt++;
+    }
+    if (n) *n = cnt;
+    if (out4 && cap < cnt) return SF_ERR_CAPACITY;
+    return SF_OK;
+}
+
+sf_status sf_read_islands(sf_world *w, uint32_t *label) {
+    if (!w || !label) return SF_ERR_ARG;
+    SF_CUDA(cudaMemcpyAsync(label, w->step->label.p, (size_t)w->nb * 4, cudaMemcpyDeviceToHost, w->stream));
+    SF_CUDA(cudaStreamSynchronize(w->stream));
+    return SF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,217 @@
+// Scans, the stable LSD radix sort, material tables and error reporting.
+#include <cstdarg>
+#include <mutex>
+
+#include "sf_internal.cuh"
+
+namespace sf {
+
+void host_mat_tables(MatTables &t) {
+    // src/lib.rs:166-183
+    const float mass[9] = {0.0f, 300.0f, 230.0f, 250.0f, 60.0f, 70.0f, 2000.0f, 8.0f, 44.0f};
+    const float capv[9] = {0.0f, 140000.0f, 50000.0f, 150000.0f, 1500.0f, 9000.0f, 1e12f, 1e12f, 1e12f};
+    const float caph[9] = {0.0f, 12000.0f, 12000.0f, 90000.0f, 400.0f, 5000.0f, 1e12f, 1e12f, 1e12f};
+    const float tens[9] = {0.0f, 0.35f, 0.1f, 0.9f, 0.5f, 0.7f, 1.0f, 1.0f, 1.0f};
+    const float stiff[9] = {0.0f, 1.0f, 0.8f, 2.0f, 0.02f, 0.4f, 1.0f, 1.0f, 1.0f};
+    const float duct[9] = {0.0f, 6.0f, 12.0f, 3.0f, 40.0f, 8.0f, 1.0f, 1.0f, 1.0f};
+    for (int k = 0; k < 9; k++) {
+        t.mass[k] = mass[k]; t.capv[k] = capv[k]; t.caph[k] = caph[k]; t.tens[k] = tens[k]; t.stiff[k] = stiff[k];
+        t.duct[k] = duct[k];
+        volatile float g = GROUNDK;   // keep the product a runtime f32 multiply
+        t.gk[k] = g * stiff[k];
+    }
+}
+
+static std::mutex g_err_mu;
+static char g_err[512] = "";
+void set_error(const char *fmt, ...) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+// ---------------------------------------------------------------- exclusive scan (three-phase, recursive)
+constexpr int SCAN_BLOCK = 512;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *total) {
+    __shared__ uint32_t warp_sums[SCAN_BLOCK / 32];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t s = lane < SCAN_BLOCK / 32 ? warp_sums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < SCAN_BLOCK / 32) warp_sums[lane] = s;
+    }
+    __syncthreads();
+    uint32_t before = wid ? warp_sums[wid - 1] : 0u;
+    *total = warp_sums[SCAN_BLOCK / 32 - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void k_scan_reduce(const uint32_t *in, size_t n, uint32_t *sums) {
+    size_t base = (size_t)blockIdx.x * SCAN_TILE;
+    uint32_t s = 0;
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        size_t i = base + (size_t)k * SCAN_BLOCK + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+    uint32_t tot;
+    block_exclusive_scan(s, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+// each thread owns SCAN_ITEMS consecutive values of the tile
+__global__ void k_scan_tile(const uint32_t *in, uint32_t *out, size_t n, const uint32_t *offsets, uint32_t *d_total) {
+    size_t base = (size_t)blockIdx.x * SCAN_TILE + (size_t)threadIdx.x * SCAN_ITEMS;
+    uint32_t v[SCAN_ITEMS];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) { size_t i = base + k; v[k] = i < n ? in[i] : 0u; s += v[k]; }
+    uint32_t tot;
+    uint32_t run = block_exclusive_scan(s, &tot) + (offsets ? offsets[blockIdx.x] : 0u);
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) { size_t i = base + k; if (i < n) out[i] = run; run += v[k]; }
+    if (d_total && blockIdx.x == gridDim.x - 1 && threadIdx.x == SCAN_BLOCK - 1) *d_total = run;
+}
+
+static cudaError_t scan_rec(const uint32_t *in, uint32_t *out, size_t n, uint32_t *d_total, uint32_t *tmp, cudaStream_t s) {
+    size_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (nb <= 1) {
+        k_scan_tile<<<1, SCAN_BLOCK, 0, s>>>(in, out, n, nullptr, d_total);
+        return cudaGetLastError();
+    }
+    uint32_t *sums = tmp, *rest = tmp + nb;
+    k_scan_reduce<<<(unsigned)nb, SCAN_BLOCK, 0, s>>>(in, n, sums);
+    cudaError_t e = scan_rec(sums, sums, nb, nullptr, rest, s);
+    if (e != cudaSuccess) return e;
+    k_scan_tile<<<(unsigned)nb, SCAN_BLOCK, 0, s>>>(in, out, n, sums, d_total);
+    return cudaGetLastError();
+}
+
+cudaError_t exclusive_scan_u32(const uint32_t *in, uint32_t *out, size_t n, uint32_t *d_total, Work &wk, cudaStream_t s) {
+    if (n == 0) {
+        if (d_total) return cudaMemsetAsync(d_total, 0, sizeof(uint32_t), s);
+        return cudaSuccess;
+    }
+    size_t need = 0, m = n;
+    while (m > (size_t)SCAN_TILE) { m = (m + SCAN_TILE - 1) / SCAN_TILE; need += m; }
+    cudaError_t e = wk.scan_a.grow(need + 16);
+    if (e != cudaSuccess) return e;
+    return scan_rec(in, out, n, d_total, wk.scan_a.p, s);
+}
+
+// ---------------------------------------------------------------- stable LSD radix sort, 8-bit digits
+constexpr int RS_BLOCK = 256;
+constexpr int RS_ITEMS = 16;
+constexpr int RS_TILE = RS_BLOCK * RS_ITEMS;
+constexpr int RS_WARPS = RS_BLOCK / 32;
+
+__global__ void k_rs_hist(const uint64_t *keys, size_t n, int shift, uint32_t *hist, unsigned nblocks) {
+    __shared__ uint32_t cnt[256];
+    cnt[threadIdx.x] = 0;
+    __syncthreads();
+    size_t base = (size_t)blockIdx.x * RS_TILE;
+    for (int k = 0; k < RS_ITEMS; k++) {
+        size_t i = base + (size_t)k * RS_BLOCK + threadIdx.x;
+        if (i < n) atomicAdd(&cnt[(unsigned)(keys[i] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    hist[(size_t)threadIdx.x * nblocks + blockIdx.x] = cnt[threadIdx.x];
+}
+
+// Ranks keys of the tile in (item, thread) order, which is input order, so equal digits keep their order.
+__global__ void k_rs_scatter(const uint64_t *kin, const uint32_t *vin, uint64_t *kout, uint32_t *vout, size_t n, int shift,
+                             const uint32_t *offs, unsigned nblocks) {
+    __shared__ uint32_t base[256];
+    __shared__ uint32_t wcnt[RS_WARPS][256];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    base[threadIdx.x] = offs[(size_t)threadIdx.x * nblocks + blockIdx.x];
+    size_t tile = (size_t)blockIdx.x * RS_TILE;
+    unsigned lt = (1u << lane) - 1u;
+    for (int k = 0; k < RS_ITEMS; k++) {
+#pragma unroll
+        for (int w = 0; w < RS_WARPS; w++) wcnt[w][threadIdx.x] = 0;
+        __syncthreads();
+        size_t i = tile + (size_t)k * RS_BLOCK + threadIdx.x;
+        bool valid = i < n;
+        uint64_t key = valid ? kin[i] : 0ull;
+        uint32_t val = valid ? vin[i] : 0u;
+        unsigned d = valid ? (unsigned)(key >> shift) & 255u : 256u;
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        unsigned rank = __popc(peers & lt);
+        if (valid && rank == 0) wcnt[wid][d] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            uint32_t pos = base[d] + rank;
+            for (int w = 0; w < wid; w++) pos += wcnt[w][d];
+            kout[pos] = key;
+            vout[pos] = val;
+        }
+        __syncthreads();
+        uint32_t add = 0;
+#pragma unroll
+        for (int w = 0; w < RS_WARPS; w++) add += wcnt[w][threadIdx.x];
+        base[threadIdx.x] += add;
+        __syncthreads();
+    }
+}
+
+cudaError_t radix_sort_u64(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt, uint32_t *vals_alt, size_t n, int bits,
+                           Work &wk, cudaStream_t s) {
+    if (n <= 1 || bits <= 0) return cudaSuccess;
+    unsigned nblocks = (unsigned)((n + RS_TILE - 1) / RS_TILE);
+    cudaError_t e = wk.hist.grow((size_t)256 * nblocks);
+    if (e != cudaSuccess) return e;
+    int passes = (bits + 7) / 8;
+    uint64_t *ki = keys, *ko = keys_alt;
+    uint32_t *vi = vals, *vo = vals_alt;
+    for (int p = 0; p < passes; p++) {
+        int shift = p * 8;
+        k_rs_hist<<<nblocks, RS_BLOCK, 0, s>>>(ki, n, shift, wk.hist.p, nblocks);
+        e = exclusive_scan_u32(wk.hist.p, wk.hist.p, (size_t)256 * nblocks, nullptr, wk, s);
+        if (e != cudaSuccess) return e;
+        k_rs_scatter<<<nblocks, RS_BLOCK, 0, s>>>(ki, vi, ko, vo, n, shift, wk.hist.p, nblocks);
+        std::swap(ki, ko);
+        std::swap(vi, vo);
+    }
+    if (ki != keys) {
+        cudaMemcpyAsync(keys, ki, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(vals, vi, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace sf
+
+extern "C" {
+const char *sf_last_error(void) { return sf::g_err; }
+int32_t sf_version(void) { return 100; }
+const char *sf_status_string(sf_status s) {
+    switch (s) {
+        case SF_OK: return "ok";
+        case SF_ERR_ARG: return "bad argument";
+        case SF_ERR_CAPACITY: return "capacity exceeded";
+        case SF_ERR_CUDA: return "CUDA error";
+        case SF_ERR_TIMEOUT: return "device wait timed out";
+        case SF_ERR_BUDGET: return "memory budget exceeded";
+        case SF_ERR_STATE: return "call out of order";
+        case SF_ERR_VERIFY: return "device self-check failed";
+        default: return "unknown status";
+    }
+}
+}

@@ -1,0 +1,502 @@
+// World lifecycle: validation, the sparse chunk grid, brick and body set-up on the device, and the read-outs.
+//
+// Set-up kernels follow the reference op for op:
+//   k_finalize_bricks  finalize_brick's neighbour links and bond capacities (src/lib.rs:646-690)
+//   k_setup_bodies     setup_body's mass, centre, inertia, radius and local offsets (src/lib.rs:844-891)
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "sf_internal.cuh"
+
+using namespace sf;
+
+namespace sf {
+
+__device__ __forceinline__ uint32_t grid_get(const uint32_t *ctab, const uint32_t *cpool, uint32_t scene, int x, int y, int z) {
+    if (!inb(x, y, z)) return 0;
+    uint32_t t = ctab[(size_t)scene * NCT + chunk_slot(x, y, z)];
+    if (t == 0) return 0;
+    return cpool[(size_t)(t - 1) * 512 + cell_in_chunk(x, y, z)];
+}
+
+__global__ void k_finalize_bricks(uint32_t ns, const uint32_t *cell, const uint32_t *scene, const uint8_t *mat,
+                                  const uint8_t *infill, const int32_t *sid, const uint32_t *ctab, const uint32_t *cpool,
+                                  uint32_t *nb6, float *bond, float *bmax) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    int x, y, z;
+    unpack_cell(cell[i], x, y, z);
+    uint32_t sc = scene[i];
+    const int D[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    uint32_t nb[6];
+#pragma unroll
+    for (int d = 0; d < 6; d++) {
+        uint32_t g = grid_get(ctab, cpool, sc, x + D[d][0], y + D[d][1], z + D[d][2]);
+        nb[d] = g == 0 ? NONE : g - 1;
+        nb6[(size_t)i * 6 + d] = nb[d];
+    }
+    uint8_t mi = mat[i];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        uint32_t j = nb[a * 2];
+        float c = 0.0f;
+        if (j != NONE) {
+            bool gap = infill[i] != infill[j] && (a != 1 || infill[i] == 1);
+            if (!gap && mat[j] != 0 && sid[j] == sid[i] && mi != 0) {
+                uint8_t mj = mat[j];
+                float ca = a == 1 ? c_mat.capv[mi] : c_mat.caph[mi];
+                float cb = a == 1 ? c_mat.capv[mj] : c_mat.caph[mj];
+                c = minf(ca, cb);
+            }
+        }
+        bond[(size_t)i * 4 + a] = c;
+        bmax[(size_t)i * 4 + a] = c;
+    }
+    float f = (y == 0 && mi != 0) ? c_mat.capv[mi] * 2.0f : 0.0f;
+    bond[(size_t)i * 4 + 3] = f;
+    bmax[(size_t)i * 4 + 3] = f;
+}
+
+// one thread per body, its bricks in list order (the sums must round in the reference's order)
+__global__ void k_setup_bodies(uint32_t nb, const uint32_t *first, const uint32_t *count, const int32_t *xyz,
+                               const uint8_t *kmat, const float *pose13, float4 *local, float4 *wpos, uint32_t *kbody,
+                               float4 *pos, float4 *q, float4 *v, float4 *w, float *rot, float *iil, float *iiw,
+                               float *m, float *im, float *rad, float *sleep, float *maxr, uint8_t *alive, uint8_t *asleep,
+                               uint8_t *wake) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    uint32_t s = first[b], n = count[b];
+    float mass = 0.0f;
+    V3 cl = v3(0.0f, 0.0f, 0.0f);
+    for (uint32_t t = 0; t < n; t++) {
+        uint32_t i = s + t;
+        V3 l = lat_pos(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        float mm = c_mat.mass[kmat[i]];
+        mass += mm;
+        cl = madd(cl, l, mm);
+    }
+    cl = mul(cl, div_rn(1.0f, mass));
+    float it[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    float rr_max = 0.0f;
+    const float cube = S * S / 6.0f;
+    for (uint32_t t = 0; t < n; t++) {
+        uint32_t i = s + t;
+        V3 l = lat_pos(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        float mm = c_mat.mass[kmat[i]];
+        V3 r = sub(l, cl);
+        local[i] = make_float4(r.x, r.y, r.z, 0.0f);
+        float rr = dot(r, r);
+        rr_max = maxf(rr_max, rr);
+        it[0] += mm * (rr - r.x * r.x + cube); it[4] += mm * (rr - r.y * r.y + cube); it[8] += mm * (rr - r.z * r.z + cube);
+        it[1] -= mm * r.x * r.y; it[2] -= mm * r.x * r.z; it[5] -= mm * r.y * r.z;
+        kbody[i] = b;
+    }
+    it[3] = it[1]; it[6] = it[2]; it[7] = it[5];
+    // minv (src/lib.rs:79-91)
+    float inv[9];
+    {
+        const float *a = it;
+        float c0 = a[4] * a[8] - a[5] * a[7];
+        float c1 = a[5] * a[6] - a[3] * a[8];
+        float c2 = a[3] * a[7] - a[4] * a[6];
+        float det = a[0] * c0 + a[1] * c1 + a[2] * c2;
+        if (fabsf(det) < 1e-12f) {
+            for (int k = 0; k < 9; k++) inv[k] = 0.0f;
+        } else {
+            float id = div_rn(1.0f, det);
+            inv[0] = c0 * id; inv[1] = (a[2] * a[7] - a[1] * a[8]) * id; inv[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+            inv[3] = c1 * id; inv[4] = (a[0] * a[8] - a[2] * a[6]) * id; inv[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+            inv[6] = c2 * id; inv[7] = (a[1] * a[6] - a[0] * a[7]) * id; inv[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+        }
+    }
+    const float *ps = pose13 + (size_t)b * 13;
+    float prot[9];
+    q_to_m(ps[3], ps[4], ps[5], ps[6], prot);
+    V3 off = mv(prot, cl);
+    V3 p = add(v3(ps[0], ps[1], ps[2]), off);
+    V3 pv = v3(ps[7], ps[8], ps[9]), pw = v3(ps[10], ps[11], ps[12]);
+    V3 vel = add(pv, cross(pw, off));
+    pos[b] = make_float4(p.x, p.y, p.z, 0.0f);
+    q[b] = make_float4(ps[3], ps[4], ps[5], ps[6]);
+    v[b] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+    w[b] = make_float4(pw.x, pw.y, pw.z, 0.0f);
+    for (int k = 0; k < 9; k++) { rot[(size_t)b * 9 + k] = prot[k]; iil[(size_t)b * 9 + k] = inv[k]; }
+    float t1[9], t2[9], t3[9];
+    mmul(prot, inv, t1); mtr(prot, t2); mmul(t1, t2, t3);
+    for (int k = 0; k < 9; k++) iiw[(size_t)b * 9 + k] = t3[k];
+    m[b] = mass; im[b] = div_rn(1.0f, mass);
+    rad[b] = sqrt_rn(rr_max) + H * 1.8f;
+    sleep[b] = 0.0f; maxr[b] = 0.0f;
+    alive[b] = 1; asleep[b] = 0; wake[b] = 0;
+    for (uint32_t t = 0; t < n; t++) {
+        uint32_t i = s + t;
+        float4 l = local[i];
+        V3 wp = add(p, mv(prot, v3(l.x, l.y, l.z)));
+        wpos[i] = make_float4(wp.x, wp.y, wp.z, 0.0f);
+    }
+}
+
+__global__ void k_kill_marked(uint32_t nb, const uint8_t *alive, const uint32_t *first, const uint32_t *count, uint8_t *kmat) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb || alive[b]) return;
+    for (uint32_t t = 0; t < count[b]; t++) kmat[first[b] + t] = 0;
+}
+
+sf_status read_error_word(sf_world *w) {
+    uint32_t e = 0;
+    SF_CUDA(cudaMemcpyAsync(&e, w->err.p, sizeof e, cudaMemcpyDeviceToHost, w->stream));
+    SF_CUDA(cudaStreamSynchronize(w->stream));
+    w->stats.error_word = e;
+    if (e & ERR_TIMEOUT) { set_error("a device barrier wait timed out"); return SF_ERR_TIMEOUT; }
+    if (e & (ERR_CAPACITY_CONTACTS | ERR_CAPACITY_COLORS)) { set_error("device capacity exceeded (error bits 0x%x)", e); return SF_ERR_CAPACITY; }
+    if (e & (ERR_VERIFY_COLOR | ERR_JP_ROUNDS)) { set_error("device self-check failed (error bits 0x%x)", e); return SF_ERR_VERIFY; }
+    return SF_OK;
+}
+
+}  // namespace sf
+
+template <class T>
+static cudaError_t upload(sf::DBuf<T> &d, const std::vector<T> &h, cudaStream_t s) {
+    cudaError_t e = d.alloc(h.size());
+    if (e != cudaSuccess) return e;
+    if (h.empty()) return cudaSuccess;
+    return cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+extern "C" {
+
+void sf_params_default(sf_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->substeps = 2;
+    p->iterations = 10;
+    p->sleep_mode = SF_SLEEP_BODY;
+    p->pinch_kill = 1;
+    p->max_colors = 128;
+    p->contact_capacity = 0;
+    p->verify = 1;
+    p->solve_blocks = 0;
+}
+
+sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf_world **out) {
+    if (!desc || !out || (desc->n_scenes && !desc->scenes)) { set_error("null argument"); return SF_ERR_ARG; }
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { set_error("no CUDA device"); return SF_ERR_CUDA; }
+    std::unique_ptr<sf_world> w(new sf_world());
+    if (params) w->P = *params; else sf_params_default(&w->P);
+    if (w->P.substeps == 0) w->P.substeps = 2;
+    if (w->P.max_colors == 0 || w->P.max_colors > (uint32_t)MAXCOL) w->P.max_colors = MAXCOL;
+    SF_CUDA(cudaGetDevice(&w->device));
+    SF_CUDA(cudaDeviceGetAttribute(&w->sms, cudaDevAttrMultiProcessorCount, w->device));
+    SF_CUDA(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
+    SF_CUDA(cudaEventCreate(&w->ev0));
+    SF_CUDA(cudaEventCreate(&w->ev1));
+    SF_CUDA(upload_mat_tables(w->stream));
+
+    // ---- validate and lay out scenes
+    uint32_t n_scenes = desc->n_scenes;
+    w->n_scenes = n_scenes;
+    w->scenes.resize(n_scenes);
+    uint64_t ns = 0, nd = 0, nb = 0;
+    int32_t max_sid = -1;
+    for (uint32_t s = 0; s < n_scenes; s++) {
+        const sf_scene_desc &d = desc->scenes[s];
+        if (d.n_static && (!d.static_xyz || !d.static_mat || !d.static_sid || !d.static_infill)) { set_error("scene %u: null static array", s); return SF_ERR_ARG; }
+        if (d.n_bodies && (!d.body_first || !d.body_brick_xyz || !d.body_brick_mat || !d.body_pose)) { set_error("scene %u: null body array", s); return SF_ERR_ARG; }
+        Scene &sc = w->scenes[s];
+        sc.static_off = (uint32_t)ns; sc.n_static = d.n_static;
+        sc.body_off = (uint32_t)nb; sc.n_bodies = d.n_bodies;
+        uint32_t nbr = d.n_bodies ? d.body_first[d.n_bodies] : 0;
+        if (d.n_bodies && d.body_first[0] != 0) { set_error("scene %u: body_first[0] must be 0", s); return SF_ERR_ARG; }
+        for (uint32_t b = 0; b < d.n_bodies; b++)
+            if (d.body_first[b + 1] <= d.body_first[b]) { set_error("scene %u body %u: no bricks", s, b); return SF_ERR_ARG; }
+        sc.brick_off = (uint32_t)nd; sc.n_bricks = nbr;
+        for (uint32_t k = 0; k < nbr; k++) {
+            uint8_t m = d.body_brick_mat[k];
+            if (m == 0 || m > 8) { set_error("scene %u body brick %u: material %u", s, k, m); return SF_ERR_ARG; }
+        }
+        for (uint32_t b = 0; b < d.n_bodies; b++)
+            for (int k = 0; k < 13; k++)
+                if (!std::isfinite(d.body_pose[(size_t)b * 13 + k])) { set_error("scene %u body %u: non-finite pose", s, b); return SF_ERR_ARG; }
+        for (uint32_t i = 0; i < d.n_static; i++) max_sid = std::max(max_sid, d.static_sid[i]);
+        ns += d.n_static; nd += nbr; nb += d.n_bodies;
+    }
+    if (ns >= 0x7fffffffu || nd >= 0x7fffffffu || nb >= 0x7fffffffu) { set_error("world too large"); return SF_ERR_CAPACITY; }
+    w->ns = (uint32_t)ns; w->nd = (uint32_t)nd; w->nb = (uint32_t)nb;
+    w->n_struct = (uint32_t)(max_sid + 1);
+
+    // ---- static bricks and the chunk grid (host-side table build, uploaded once)
+    std::vector<uint32_t> h_ctab((size_t)n_scenes * NCT, 0), h_cpool;
+    std::vector<uint32_t> s_cell(ns), s_scene(ns);
+    std::vector<uint8_t> s_mat(ns), s_inf(ns);
+    std::vector<int32_t> s_sid(ns);
+    uint32_t nchunks = 0;
+    for (uint32_t s = 0; s < n_scenes; s++) {
+        const sf_scene_desc &d = desc->scenes[s];
+        Scene &sc = w->scenes[s];
+        sc.chunk_off = nchunks;
+        for (uint32_t k = 0; k < d.n_static; k++) {
+            int x = d.static_xyz[3 * k], y = d.static_xyz[3 * k + 1], z = d.static_xyz[3 * k + 2];
+            uint8_t m = d.static_mat[k];
+            if (!inb(x, y, z)) { set_error("scene %u static %u: cell (%d,%d,%d) outside the lattice", s, k, x, y, z); return SF_ERR_ARG; }
+            if (m == 0 || m > 8) { set_error("scene %u static %u: material %u", s, k, m); return SF_ERR_ARG; }
+            if (d.static_sid[k] < -1) { set_error("scene %u static %u: structure id %d", s, k, d.static_sid[k]); return SF_ERR_ARG; }
+            uint32_t gi = sc.static_off + k;
+            uint32_t &t = h_ctab[(size_t)s * NCT + chunk_slot(x, y, z)];
+            if (t == 0) {
+                nchunks++;
+                t = nchunks;
+                h_cpool.resize((size_t)nchunks * 512, 0);
+                w->h_chunk_cell.push_back(pack_cell(x & ~7, y & ~7, z & ~7));
+                w->h_chunk_scene.push_back(s);
+            }
+            uint32_t &slot = h_cpool[(size_t)(t - 1) * 512 + cell_in_chunk(x, y, z)];
+            if (slot != 0) { set_error("scene %u static %u: cell (%d,%d,%d) already holds a brick", s, k, x, y, z); return SF_ERR_ARG; }
+            slot = gi + 1;
+            s_cell[gi] = pack_cell(x, y, z); s_scene[gi] = s; s_mat[gi] = m;
+            s_inf[gi] = (m == GLASS || d.static_infill[k]) ? 1 : 0;
+            s_sid[gi] = d.static_sid[k];
+        }
+        sc.n_chunks = nchunks - sc.chunk_off;
+    }
+    w->n_chunks = nchunks;
+    w->h_sid = s_sid;
+    w->h_s_cell = s_cell;
+    cudaStream_t st = w->stream;
+    SF_CUDA(upload(w->ctab, h_ctab, st));
+    SF_CUDA(upload(w->cpool, h_cpool, st));
+    SF_CUDA(upload(w->s_cell, s_cell, st));
+    SF_CUDA(upload(w->s_scene, s_scene, st));
+    SF_CUDA(upload(w->s_mat, s_mat, st));
+    SF_CUDA(upload(w->s_infill, s_inf, st));
+    SF_CUDA(upload(w->s_sid, s_sid, st));
+    SF_CUDA(w->s_nb6.alloc((size_t)ns * 6));
+    SF_CUDA(w->s_bond.alloc((size_t)ns * 4));
+    SF_CUDA(w->s_bmax.alloc((size_t)ns * 4));
+    SF_CUDA(w->s_phi.alloc(ns));
+    SF_CUDA(w->s_phi64.alloc(ns));
+    SF_CUDA(cudaMemsetAsync(w->s_phi64.p, 0, w->s_phi64.bytes(), st));
+    SF_CUDA(w->s_ext.alloc(ns));
+    SF_CUDA(w->s_stress.alloc(ns));
+    SF_CUDA(cudaMemsetAsync(w->s_phi.p, 0, w->s_phi.bytes(), st));
+    SF_CUDA(cudaMemsetAsync(w->s_ext.p, 0, w->s_ext.bytes(), st));
+    SF_CUDA(cudaMemsetAsync(w->s_stress.p, 0, w->s_stress.bytes(), st));
+    if (ns) {
+        k_finalize_bricks<<<grid_for(ns, 256), 256, 0, st>>>((uint32_t)ns, w->s_cell.p, w->s_scene.p, w->s_mat.p,
+                                                           w->s_infill.p, w->s_sid.p, w->ctab.p, w->cpool.p, w->s_nb6.p,
+                                                           w->s_bond.p, w->s_bmax.p);
+        SF_CUDA(cudaGetLastError());
+    }
+
+    // ---- bodies and body bricks
+    std::vector<uint32_t> b_first(nb), b_count(nb), b_scene(nb);
+    std::vector<int32_t> k_xyz((size_t)nd * 3);
+    std::vector<uint8_t> k_mat(nd);
+    std::vector<float> pose((size_t)nb * 13);
+    for (uint32_t s = 0; s < n_scenes; s++) {
+        const sf_scene_desc &d = desc->scenes[s];
+        const Scene &sc = w->scenes[s];
+        for (uint32_t b = 0; b < d.n_bodies; b++) {
+            uint32_t gb = sc.body_off + b;
+            b_first[gb] = sc.brick_off + d.body_first[b];
+            b_count[gb] = d.body_first[b + 1] - d.body_first[b];
+            b_scene[gb] = s;
+            std::memcpy(&pose[(size_t)gb * 13], d.body_pose + (size_t)b * 13, 13 * sizeof(float));
+        }
+        if (sc.n_bricks) {
+            std::memcpy(&k_xyz[(size_t)sc.brick_off * 3], d.body_brick_xyz, (size_t)sc.n_bricks * 3 * sizeof(int32_t));
+            std::memcpy(&k_mat[sc.brick_off], d.body_brick_mat, sc.n_bricks);
+        }
+    }
+    SF_CUDA(upload(w->b_first, b_first, st));
+    SF_CUDA(upload(w->b_count, b_count, st));
+    SF_CUDA(upload(w->b_scene, b_scene, st));
+    SF_CUDA(upload(w->k_xyz, k_xyz, st));
+    SF_CUDA(upload(w->k_mat, k_mat, st));
+    sf::DBuf<float> d_pose;
+    SF_CUDA(upload(d_pose, pose, st));
+    SF_CUDA(w->b_pos.alloc(nb)); SF_CUDA(w->b_q.alloc(nb)); SF_CUDA(w->b_v.alloc(nb)); SF_CUDA(w->b_w.alloc(nb));
+    SF_CUDA(w->b_vpre.alloc(nb)); SF_CUDA(w->b_wpre.alloc(nb));
+    SF_CUDA(w->b_rot.alloc((size_t)nb * 9)); SF_CUDA(w->b_iil.alloc((size_t)nb * 9)); SF_CUDA(w->b_iiw.alloc((size_t)nb * 9));
+    SF_CUDA(w->b_m.alloc(nb)); SF_CUDA(w->b_im.alloc(nb)); SF_CUDA(w->b_rad.alloc(nb)); SF_CUDA(w->b_sleep.alloc(nb));
+    SF_CUDA(w->b_maxr.alloc(nb));
+    SF_CUDA(w->b_alive.alloc(nb)); SF_CUDA(w->b_asleep.alloc(nb)); SF_CUDA(w->b_wake.alloc(nb));
+    SF_CUDA(w->b_nc.alloc(nb));
+    SF_CUDA(cudaMemsetAsync(w->b_nc.p, 0, w->b_nc.bytes(), st));
+    SF_CUDA(w->k_local.alloc(nd)); SF_CUDA(w->k_wpos.alloc(nd)); SF_CUDA(w->k_body.alloc(nd));
+    if (nb) {
+        k_setup_bodies<<<grid_for(nb, 128), 128, 0, st>>>((uint32_t)nb, w->b_first.p, w->b_count.p, w->k_xyz.p, w->k_mat.p,
+                                                        d_pose.p, w->k_local.p, w->k_wpos.p, w->k_body.p, w->b_pos.p,
+                                                        w->b_q.p, w->b_v.p, w->b_w.p, w->b_rot.p, w->b_iil.p, w->b_iiw.p,
+                                                        w->b_m.p, w->b_im.p, w->b_rad.p, w->b_sleep.p, w->b_maxr.p,
+                                                        w->b_alive.p, w->b_asleep.p, w->b_wake.p);
+        SF_CUDA(cudaGetLastError());
+    }
+    SF_CUDA(w->err.alloc(64));
+    SF_CUDA(cudaMemsetAsync(w->err.p, 0, w->err.bytes(), st));
+    SF_CUDA(w->barrier.alloc(4));
+    SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, w->barrier.bytes(), st));
+    sf_status r = sor_create(w.get());
+    if (r != SF_OK) return r;
+    r = step_create(w.get());
+    if (r != SF_OK) return r;
+    SF_CUDA(cudaStreamSynchronize(st));
+    *out = w.release();
+    return SF_OK;
+}
+
+void sf_world_destroy(sf_world *w) {
+    if (!w) return;
+    cudaStreamSynchronize(w->stream);
+    sor_destroy(w);
+    step_destroy(w);
+    if (w->ev0) cudaEventDestroy(w->ev0);
+    if (w->ev1) cudaEventDestroy(w->ev1);
+    cudaStream_t s = w->stream;
+    delete w;
+    if (s) cudaStreamDestroy(s);
+}
+
+sf_status sf_world_get_info(const sf_world *w, sf_world_info *info) {
+    if (!w || !info) return SF_ERR_ARG;
+    info->n_scenes = w->n_scenes; info->n_static = w->ns; info->n_bodies = w->nb; info->n_body_bricks = w->nd;
+    info->n_structures = w->n_struct; info->n_chunks = w->n_chunks;
+    return SF_OK;
+}
+
+sf_status sf_get_stats(const sf_world *w, sf_stats *st) {
+    if (!w || !st) return SF_ERR_ARG;
+    *st = w->stats;
+    return SF_OK;
+}
+
+sf_status sf_read_bodies(sf_world *w, float *state13, float *sleep, uint8_t *flags) {
+    if (!w) return SF_ERR_ARG;
+    uint32_t nb = w->nb;
+    std::vector<float4> p(nb), q(nb), v(nb), om(nb);
+    cudaStream_t s = w->stream;
+    SF_CUDA(cudaMemcpyAsync(p.data(), w->b_pos.p, nb * sizeof(float4), cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaMemcpyAsync(q.data(), w->b_q.p, nb * sizeof(float4), cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaMemcpyAsync(v.data(), w->b_v.p, nb * sizeof(float4), cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaMemcpyAsync(om.data(), w->b_w.p, nb * sizeof(float4), cudaMemcpyDeviceToHost, s));
+    std::vector<uint8_t> al(nb), as(nb);
+    if (sleep) SF_CUDA(cudaMemcpyAsync(sleep, w->b_sleep.p, nb * sizeof(float), cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaMemcpyAsync(al.data(), w->b_alive.p, nb, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaMemcpyAsync(as.data(), w->b_asleep.p, nb, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t b = 0; b < nb; b++) {
+        if (state13) {
+            float *o = state13 + (size_t)b * 13;
+            o[0] = p[b].x; o[1] = p[b].y; o[2] = p[b].z;
+            o[3] = q[b].x; o[4] = q[b].y; o[5] = q[b].z; o[6] = q[b].w;
+            o[7] = v[b].x; o[8] = v[b].y; o[9] = v[b].z;
+            o[10] = om[b].x; o[11] = om[b].y; o[12] = om[b].z;
+        }
+        if (flags) flags[b] = (al[b] ? 1 : 0) | (as[b] ? 2 : 0);
+    }
+    return SF_OK;
+}
+
+sf_status sf_write_bodies(sf_world *w, const float *state13, const float *sleep, const uint8_t *flags) {
+    if (!w || !state13 || !sleep || !flags) return SF_ERR_ARG;
+    uint32_t nb = w->nb;
+    std::vector<float4> p(nb), q(nb), v(nb), om(nb);
+    std::vector<uint8_t> al(nb), as(nb);
+    for (uint32_t b = 0; b < nb; b++) {
+        const float *o = state13 + (size_t)b * 13;
+        p[b] = make_float4(o[0], o[1], o[2], 0.0f);
+        q[b] = make_float4(o[3], o[4], o[5], o[6]);
+        v[b] = make_float4(o[7], o[8], o[9], 0.0f);
+        om[b] = make_float4(o[10], o[11], o[12], 0.0f);
+        al[b] = flags[b] & 1; as[b] = (flags[b] >> 1) & 1;
+    }
+    cudaStream_t s = w->stream;
+    SF_CUDA(cudaMemcpyAsync(w->b_pos.p, p.data(), nb * sizeof(float4), cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemcpyAsync(w->b_q.p, q.data(), nb * sizeof(float4), cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemcpyAsync(w->b_v.p, v.data(), nb * sizeof(float4), cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemcpyAsync(w->b_w.p, om.data(), nb * sizeof(float4), cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemcpyAsync(w->b_sleep.p, sleep, nb * sizeof(float), cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemcpyAsync(w->b_alive.p, al.data(), nb, cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemcpyAsync(w->b_asleep.p, as.data(), nb, cudaMemcpyHostToDevice, s));
+    if (nb) k_kill_marked<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, w->b_first.p, w->b_count.p, w->k_mat.p);
+    SF_CUDA(cudaGetLastError());
+    SF_CUDA(cudaStreamSynchronize(s));
+    return SF_OK;
+}
+
+sf_status sf_read_body_setup(sf_world *w, float *body12, float *local3) {
+    if (!w) return SF_ERR_ARG;
+    uint32_t nb = w->nb, nd = w->nd;
+    std::vector<float> m(nb), im(nb), rad(nb), iil((size_t)nb * 9);
+    std::vector<float4> loc(nd);
+    cudaStream_t s = w->stream;
+    SF_CUDA(cudaMemcpyAsync(m.data(), w->b_m.p, nb * 4, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaMemcpyAsync(im.data(), w->b_im.p, nb * 4, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaMemcpyAsync(rad.data(), w->b_rad.p, nb * 4, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaMemcpyAsync(iil.data(), w->b_iil.p, (size_t)nb * 36, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaMemcpyAsync(loc.data(), w->k_local.p, nd * sizeof(float4), cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t b = 0; b < nb && body12; b++) {
+        float *o = body12 + (size_t)b * 12;
+        o[0] = m[b]; o[1] = im[b]; o[2] = rad[b];
+        for (int k = 0; k < 9; k++) o[3 + k] = iil[(size_t)b * 9 + k];
+    }
+    for (uint32_t k = 0; k < nd && local3; k++) { local3[3 * k] = loc[k].x; local3[3 * k + 1] = loc[k].y; local3[3 * k + 2] = loc[k].z; }
+    return SF_OK;
+}
+
+sf_status sf_read_brick_positions(sf_world *w, float *wpos3) {
+    if (!w || !wpos3) return SF_ERR_ARG;
+    std::vector<float4> p(w->nd);
+    SF_CUDA(cudaMemcpyAsync(p.data(), w->k_wpos.p, w->nd * sizeof(float4), cudaMemcpyDeviceToHost, w->stream));
+    SF_CUDA(cudaStreamSynchronize(w->stream));
+    for (uint32_t k = 0; k < w->nd; k++) { wpos3[3 * k] = p[k].x; wpos3[3 * k + 1] = p[k].y; wpos3[3 * k + 2] = p[k].z; }
+    return SF_OK;
+}
+
+sf_status sf_read_phi(sf_world *w, float *phi) {
+    if (!w || !phi) return SF_ERR_ARG;
+    SF_CUDA(cudaMemcpyAsync(phi, w->s_phi.p, (size_t)w->ns * 4, cudaMemcpyDeviceToHost, w->stream));
+    SF_CUDA(cudaStreamSynchronize(w->stream));
+    return SF_OK;
+}
+sf_status sf_write_phi(sf_world *w, const float *phi) {
+    if (!w || !phi) return SF_ERR_ARG;
+    std::vector<double> p64(phi, phi + w->ns);
+    SF_CUDA(cudaMemcpyAsync(w->s_phi.p, phi, (size_t)w->ns * 4, cudaMemcpyHostToDevice, w->stream));
+    SF_CUDA(cudaMemcpyAsync(w->s_phi64.p, p64.data(), (size_t)w->ns * 8, cudaMemcpyHostToDevice, w->stream));
+    SF_CUDA(cudaStreamSynchronize(w->stream));
+    return SF_OK;
+}
+sf_status sf_read_phi64(sf_world *w, double *phi) {
+    if (!w || !phi) return SF_ERR_ARG;
+    SF_CUDA(cudaMemcpyAsync(phi, w->s_phi64.p, (size_t)w->ns * 8, cudaMemcpyDeviceToHost, w->stream));
+    SF_CUDA(cudaStreamSynchronize(w->stream));
+    return SF_OK;
+}
+sf_status sf_write_ext(sf_world *w, const float *ext) {
+    if (!w || !ext) return SF_ERR_ARG;
+    SF_CUDA(cudaMemcpyAsync(w->s_ext.p, ext, (size_t)w->ns * 4, cudaMemcpyHostToDevice, w->stream));
+    SF_CUDA(cudaStreamSynchronize(w->stream));
+    return SF_OK;
+}
+sf_status sf_read_ext(sf_world *w, float *ext) {
+    if (!w || !ext) return SF_ERR_ARG;
+    SF_CUDA(cudaMemcpyAsync(ext, w->s_ext.p, (size_t)w->ns * 4, cudaMemcpyDeviceToHost, w->stream));
+    SF_CUDA(cudaStreamSynchronize(w->stream));
+    return SF_OK;
+}
+sf_status sf_read_bonds(sf_world *w, float *bond4, uint32_t *nb6, uint8_t *mat) {
+    if (!w) return SF_ERR_ARG;
+    cudaStream_t s = w->stream;
+    if (bond4) SF_CUDA(cudaMemcpyAsync(bond4, w->s_bond.p, (size_t)w->ns * 16, cudaMemcpyDeviceToHost, s));
+    if (nb6) SF_CUDA(cudaMemcpyAsync(nb6, w->s_nb6.p, (size_t)w->ns * 24, cudaMemcpyDeviceToHost, s));
+    if (mat) SF_CUDA(cudaMemcpyAsync(mat, w->s_mat.p, (size_t)w->ns, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    return SF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,369 @@
+"""Seeded synthetic scenes for the Shatterforge physics path.
+
+A *scene* is one independent world in the 640 x 136 x 640 lattice of 0.5 m cells (src/lib.rs:110-120): static
+bricks on lattice cells (structures and obstacles) plus compound rigid bodies, each a set of bricks given in local
+lattice coordinates and a parent pose.  Arrays use the layout of ``sf_scene_desc`` in include/sf.h:
+
+    static_xyz   int32 [n, 3]   lattice cell of each static brick
+    static_mat   uint8 [n]      material 1..5 (concrete, masonry, steel, glass, timber; src/lib.rs:163)
+    static_sid   int32 [n]      structure id, -1 for loose static geometry
+    static_infill uint8 [n]     1 = infill brick (glass always is; src/lib.rs:632)
+    body_first   uint32 [nb+1]  prefix offsets of each body's bricks
+    body_brick_xyz int32 [nd,3] local lattice cell of each body brick
+    body_brick_mat uint8 [nd]
+    body_pose    float32 [nb,13] parent position, quaternion (x, y, z, w), velocity, angular velocity
+
+setup_body (src/lib.rs:844-891) turns a body's lattice cells into its mass, centre and inertia; the parent pose
+is applied about the lattice origin exactly as the reference does.
+
+Random numbers: small scenes draw from the reference's own xorshift32 stream (src/lib.rs:324-329); bulk scenes
+(tens of thousands of bodies) draw from numpy's PCG64 seeded from that stream, so every scene is a pure function
+of its seed.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+CONC, MASON, STEEL, GLASS, WOOD = 1, 2, 3, 4, 5
+NX, NY, NZ = 640, 136, 640
+ORIGIN = (NX // 2, 0, NZ // 2)   # lattice cell whose centre is (0.25, 0.25, 0.25) m
+
+
+class XorShift32:
+    """src/lib.rs:324-329: x ^= x << 13; x ^= x >> 17; x ^= x << 5; value = (x >> 8) / 2^24."""
+
+    def __init__(self, seed: int):
+        self.x = (seed or 0x9E3779B9) & 0xFFFFFFFF
+
+    def u32(self) -> int:
+        x = self.x
+        x ^= (x << 13) & 0xFFFFFFFF
+        x ^= x >> 17
+        x ^= (x << 5) & 0xFFFFFFFF
+        self.x = x
+        return x
+
+    def rnd(self) -> float:
+        return (self.u32() >> 8) / 16777216.0
+
+
+@dataclass
+class Scene:
+    static_xyz: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
+    static_mat: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint8))
+    static_sid: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    static_infill: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint8))
+    body_first: np.ndarray = field(default_factory=lambda: np.zeros(1, np.uint32))
+    body_brick_xyz: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
+    body_brick_mat: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint8))
+    body_pose: np.ndarray = field(default_factory=lambda: np.zeros((0, 13), np.float32))
+    name: str = ""
+
+    @property
+    def n_static(self) -> int:
+        return int(self.static_mat.shape[0])
+
+    @property
+    def n_bodies(self) -> int:
+        return int(self.body_pose.shape[0])
+
+    @property
+    def n_body_bricks(self) -> int:
+        return int(self.body_brick_mat.shape[0])
+
+    def contiguous(self) -> "Scene":
+        self.static_xyz = np.ascontiguousarray(self.static_xyz, np.int32).reshape(-1, 3)
+        self.static_mat = np.ascontiguousarray(self.static_mat, np.uint8)
+        self.static_sid = np.ascontiguousarray(self.static_sid, np.int32)
+        self.static_infill = np.ascontiguousarray(self.static_infill, np.uint8)
+        self.body_first = np.ascontiguousarray(self.body_first, np.uint32)
+        self.body_brick_xyz = np.ascontiguousarray(self.body_brick_xyz, np.int32).reshape(-1, 3)
+        self.body_brick_mat = np.ascontiguousarray(self.body_brick_mat, np.uint8)
+        self.body_pose = np.ascontiguousarray(self.body_pose, np.float32).reshape(-1, 13)
+        return self
+
+    def structure_ids(self) -> list[int]:
+        return sorted(int(s) for s in np.unique(self.static_sid) if s >= 0)
+
+    def without_static(self, mask: np.ndarray) -> "Scene":
+        keep = ~mask
+        return Scene(self.static_xyz[keep], self.static_mat[keep], self.static_sid[keep], self.static_infill[keep],
+                     self.body_first, self.body_brick_xyz, self.body_brick_mat, self.body_pose, self.name).contiguous()
+
+
+def _concat_static(parts):
+    if not parts:
+        return (np.zeros((0, 3), np.int32), np.zeros(0, np.uint8), np.zeros(0, np.int32), np.zeros(0, np.uint8))
+    xyz = np.concatenate([p[0] for p in parts]).astype(np.int32)
+    mat = np.concatenate([p[1] for p in parts]).astype(np.uint8)
+    sid = np.concatenate([p[2] for p in parts]).astype(np.int32)
+    inf = np.concatenate([p[3] for p in parts]).astype(np.uint8)
+    return xyz, mat, sid, inf
+
+
+def frame_structure(x0: int, z0: int, wx: int, wz: int, storeys: int, storey_h: int, col_xs, col_zs, sid: int,
+                    mat_of=None, y0: int = 0):
+    """A column/slab frame: per storey, (storey_h - 1)-cell columns at (col_xs x col_zs) and a full slab on top."""
+    cells = []
+    for s in range(storeys):
+        yb = y0 + s * storey_h
+        for cx in col_xs:
+            for cz in col_zs:
+                for y in range(yb, yb + storey_h - 1):
+                    cells.append((x0 + cx, y, z0 + cz))
+        ys = yb + storey_h - 1
+        xs, zs = np.meshgrid(np.arange(wx), np.arange(wz), indexing="ij")
+        slab = np.stack([x0 + xs.ravel(), np.full(xs.size, ys), z0 + zs.ravel()], 1)
+        cells.extend(map(tuple, slab))
+    xyz = np.array(cells, np.int32).reshape(-1, 3)
+    if mat_of is None:
+        mat = np.full(len(xyz), CONC, np.uint8)
+    else:
+        mat = mat_of(xyz)
+    infill = (mat == GLASS).astype(np.uint8)
+    return xyz, mat, np.full(len(xyz), sid, np.int32), infill
+
+
+def _quat_uniform(u1, u2, u3):
+    """Shoemake's uniform random unit quaternion (x, y, z, w) from three uniforms."""
+    a = np.sqrt(1.0 - u1)
+    b = np.sqrt(u1)
+    t1 = 2.0 * math.pi * u2
+    t2 = 2.0 * math.pi * u3
+    return np.stack([a * np.sin(t1), a * np.cos(t1), b * np.sin(t2), b * np.cos(t2)], -1)
+
+
+def config1_frame(seed: int = 1, remove_columns: int = 2):
+    """5-storey concrete frame on 24 x 24 cells; storeys of 7 cells (6-cell 1 x 1 columns on a 3 x 3 grid, then a
+    full 24 x 24 slab): 5 * (9 * 6 + 576) = 3150 bricks, structure 0, centred on the lattice origin.
+    Returns (scene, removed_mask) where removed_mask marks the bricks of `remove_columns` seed-chosen ground columns."""
+    rng = XorShift32(seed)
+    x0, z0 = ORIGIN[0] - 12, ORIGIN[2] - 12
+    cols = [0, 11, 23]
+    xyz, mat, sid, inf = frame_structure(x0, z0, 24, 24, 5, 7, cols, cols, 0)
+    sc = Scene(xyz, mat, sid, inf, name="frame5").contiguous()
+    ground_cols = [(x0 + cx, z0 + cz) for cx in cols for cz in cols]
+    chosen = []
+    while len(chosen) < remove_columns:
+        k = int(rng.rnd() * len(ground_cols)) % len(ground_cols)
+        if k not in chosen:
+            chosen.append(k)
+    removed = np.zeros(sc.n_static, bool)
+    for k in chosen:
+        cx, cz = ground_cols[k]
+        removed |= (xyz[:, 0] == cx) & (xyz[:, 2] == cz) & (xyz[:, 1] < 6)
+    return sc, removed
+
+
+def loose_debris(n: int, seed: int, box_lo=(8.0, 2.0, -5.0), box_hi=(18.0, 12.0, 5.0),
+                 mats=(CONC, MASON, WOOD)):
+    """n single-brick bodies at xorshift32-uniform positions in an axis-aligned box, at rest (config 1 debris)."""
+    rng = XorShift32(seed)
+    pose = np.zeros((n, 13), np.float32)
+    mat = np.zeros(n, np.uint8)
+    for b in range(n):
+        p = [box_lo[k] + (box_hi[k] - box_lo[k]) * rng.rnd() for k in range(3)]
+        # the brick's lattice centre is (0.25, 0.25, 0.25) about the parent origin
+        pose[b, 0:3] = [p[0] - 0.25, p[1] - 0.25, p[2] - 0.25]
+        pose[b, 6] = 1.0
+        mat[b] = mats[int(rng.rnd() * len(mats)) % len(mats)]
+    xyz = np.tile(np.array(ORIGIN, np.int32), (n, 1))
+    return np.arange(n + 1, dtype=np.uint32), xyz, mat, pose
+
+
+def config1_scene(seed: int = 1, n_debris: int = 1024, removed: bool = False) -> Scene:
+    """Config 1: the 5-storey frame plus 1,024 loose single-brick bodies 2 m above the ground beside it."""
+    frame, rm = config1_frame(seed)
+    if removed:
+        frame = frame.without_static(rm)
+    bf, bxyz, bmat, pose = loose_debris(n_debris, seed + 101)
+    frame.body_first, frame.body_brick_xyz, frame.body_brick_mat, frame.body_pose = bf, bxyz, bmat, pose
+    frame.name = "config1"
+    return frame.contiguous()
+
+
+# ---------------------------------------------------------------- compound debris (config 4)
+_NBR = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]], np.int32)
+
+
+def random_cluster(k: int, rng: np.random.Generator) -> np.ndarray:
+    """A connected random lattice cluster of k cells: grow from one cell by attaching a random free face
+    neighbour of a random member."""
+    cells = [(0, 0, 0)]
+    seen = {(0, 0, 0)}
+    while len(cells) < k:
+        c = cells[int(rng.integers(len(cells)))]
+        d = _NBR[int(rng.integers(6))]
+        nc = (c[0] + int(d[0]), c[1] + int(d[1]), c[2] + int(d[2]))
+        if nc not in seen:
+            seen.add(nc)
+            cells.append(nc)
+    return np.array(cells, np.int32)
+
+
+class ClusterLibrary:
+    """Random connected clusters, `variants` per brick count, reused across bodies of the same count."""
+
+    def __init__(self, seed: int, variants: int = 6, kmax: int = 256):
+        self.rng = np.random.default_rng(seed)
+        self.variants = variants
+        self.kmax = kmax
+        self.cache: dict[int, list[np.ndarray]] = {}
+
+    def get(self, k: int, pick: int) -> np.ndarray:
+        if k not in self.cache:
+            self.cache[k] = [random_cluster(k, self.rng) for _ in range(self.variants if k > 1 else 1)]
+        lst = self.cache[k]
+        return lst[pick % len(lst)]
+
+
+def debris_scene(n_bodies: int, seed: int, lib: ClusterLibrary | None = None, p_geom: float = 0.3, kmax: int = 256,
+                 obstacles: tuple[int, int] = (4, 16), spacing: float = 2.5, v_sigma: float = 3.0,
+                 mats=(CONC, MASON, WOOD), name: str = "debris") -> Scene:
+    """Config 4 scene: n compound bodies of k ~ Geometric(p) bricks (capped at kmax) in connected random lattice
+    clusters, uniform random orientation, N(0, v_sigma) velocities, falling onto the ground plane among 4-16
+    static box obstacles (static bricks, no structure)."""
+    rng = np.random.default_rng(seed)
+    lib = lib or ClusterLibrary(seed ^ 0x5F3759DF)
+    ks = np.minimum(rng.geometric(p_geom, n_bodies), kmax).astype(np.int64)
+    picks = rng.integers(0, 1 << 30, n_bodies)
+    clusters = [lib.get(int(k), int(p)) for k, p in zip(ks, picks)]
+    first = np.zeros(n_bodies + 1, np.uint32)
+    first[1:] = np.cumsum(ks)
+    cl = np.concatenate(clusters, 0)
+    # spread bricks of a body over lattice cells about the origin cell
+    bxyz = (cl + np.array(ORIGIN, np.int32)).astype(np.int32)
+    bmat = np.array(mats, np.uint8)[rng.integers(0, len(mats), n_bodies)]
+    bmat = np.repeat(bmat, ks)
+    # spawn slots: a jittered grid, at most 60 per side, layers above 2 m
+    side = int(min(60, math.ceil(math.sqrt(n_bodies))))
+    layers = int(math.ceil(n_bodies / (side * side)))
+    slot = np.arange(n_bodies)
+    rng.shuffle(slot)
+    sx = slot % side
+    sz = (slot // side) % side
+    sy = slot // (side * side)
+    jitter = rng.uniform(-0.25, 0.25, (n_bodies, 3))
+    # big bodies take more room: shift by their extent in the layer above
+    ext = np.array([float(np.abs(c).max()) * 0.5 + 0.5 for c in clusters])
+    half = (side - 1) * spacing * 0.5
+    px = sx * spacing - half + jitter[:, 0]
+    pz = sz * spacing - half + jitter[:, 2]
+    py = 2.5 + sy * (spacing + 0.5) + ext + jitter[:, 1]
+    q = _quat_uniform(rng.random(n_bodies), rng.random(n_bodies), rng.random(n_bodies))
+    v = rng.normal(0.0, v_sigma, (n_bodies, 3))
+    pose = np.zeros((n_bodies, 13), np.float32)
+    pose[:, 0], pose[:, 1], pose[:, 2] = px - 0.25, py - 0.25, pz - 0.25
+    pose[:, 3:7] = q
+    pose[:, 7:10] = v
+    # static box obstacles on the ground inside the spawn footprint
+    nob = int(rng.integers(obstacles[0], obstacles[1] + 1)) if obstacles[1] > 0 else 0
+    parts = []
+    for _ in range(nob):
+        w = rng.integers(2, 9, 3)
+        w[1] = rng.integers(2, 7)
+        cx = int(rng.uniform(-half, half) / 0.5) + ORIGIN[0]
+        cz = int(rng.uniform(-half, half) / 0.5) + ORIGIN[2]
+        xs, ys, zs = np.meshgrid(np.arange(w[0]), np.arange(w[1]), np.arange(w[2]), indexing="ij")
+        xyz = np.stack([cx + xs.ravel(), ys.ravel(), cz + zs.ravel()], 1)
+        m = np.full(len(xyz), CONC, np.uint8)
+        parts.append((xyz, m, np.full(len(xyz), -1, np.int32), np.zeros(len(xyz), np.uint8)))
+    sxyz, smat, ssid, sinf = _concat_static(parts)
+    if len(sxyz):
+        key = sxyz[:, 0].astype(np.int64) * (NY * NZ) + sxyz[:, 1].astype(np.int64) * NZ + sxyz[:, 2]
+        _, uniq = np.unique(key, return_index=True)
+        uniq.sort()
+        sxyz, smat, ssid, sinf = sxyz[uniq], smat[uniq], ssid[uniq], sinf[uniq]
+    return Scene(sxyz, smat, ssid, sinf, first, bxyz, bmat, pose, name).contiguous()
+
+
+def config4_scenes(seed: int = 3, n_scenes: int = 256, lo: int = 500, hi: int = 20000, scale: float = 1.0,
+                   **kw) -> list[Scene]:
+    """Config 4: n_scenes independent debris scenes, body counts log-uniform in [lo, hi] (times `scale`)."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(math.log(lo), math.log(hi), n_scenes)) * scale
+    counts = np.maximum(1, counts.astype(np.int64))
+    lib = ClusterLibrary(seed ^ 0x2545F491)
+    return [debris_scene(int(c), seed * 1000003 + s, lib=lib, name=f"debris{s}", **kw) for s, c in enumerate(counts)]
+
+
+# ---------------------------------------------------------------- structures (config 3)
+def config3_world(seed: int = 2, n_struct: int = 37, lo: int = 1000, hi: int = 40000, cap: int = 500000,
+                  scale: float = 1.0) -> Scene:
+    """Config 3: n_struct column/slab frames in one 640 x 136 x 640 lattice; brick counts log-uniform in [lo, hi]
+    (total capped at `cap`), storey height 6-8 cells, footprints 8-60 cells a side, materials 50 % concrete,
+    25 % masonry, 10 % steel, 10 % timber, 5 % glass (glass is infill, non-bearing)."""
+    rng = np.random.default_rng(seed)
+    targets = np.exp(rng.uniform(math.log(lo), math.log(hi), n_struct)) * scale
+    if targets.sum() > cap:
+        targets *= cap / targets.sum()
+    slots_x, slots_z = 7, 6
+    parts = []
+    for s in range(n_struct):
+        target = float(targets[s])
+        h = int(rng.integers(6, 9))
+        wmax = int(min(60, max(8, math.sqrt(target / 2.0))))
+        wx = int(rng.integers(8, wmax + 1))
+        wz = int(rng.integers(8, wmax + 1))
+        spacing = int(rng.integers(5, 13))
+        col_xs = sorted(set(list(range(0, wx, spacing)) + [wx - 1]))
+        col_zs = sorted(set(list(range(0, wz, spacing)) + [wz - 1]))
+        per = wx * wz + len(col_xs) * len(col_zs) * (h - 1)
+        storeys = int(max(1, min((NY - 1) // h, round(target / per))))
+        gx, gz = s % slots_x, s // slots_x
+        x0 = 8 + gx * (NX - 16) // slots_x
+        z0 = 8 + gz * (NZ - 16) // slots_z
+
+        def mat_of(xyz, _rng=rng):
+            u = _rng.random(len(xyz))
+            m = np.full(len(xyz), CONC, np.uint8)
+            m[u >= 0.50] = MASON
+            m[u >= 0.75] = STEEL
+            m[u >= 0.85] = WOOD
+            m[u >= 0.95] = GLASS
+            return m
+
+        parts.append(frame_structure(x0, z0, wx, wz, storeys, h, col_xs, col_zs, s, mat_of))
+    xyz, mat, sid, inf = _concat_static(parts)
+    keep = grounded_mask(xyz, mat, sid, inf)
+    return Scene(xyz[keep], mat[keep], sid[keep], inf[keep], name="structures").contiguous()
+
+
+def bond_edges(xyz, mat, sid, infill):
+    """Bonded + axis neighbour pairs (i, j) under finalize_brick's rules (src/lib.rs:668-690): same structure,
+    both bricks present, and no infill gap (infill bonds to nothing sideways and to no structural brick above)."""
+    key = (xyz[:, 0].astype(np.int64) * NY + xyz[:, 1]) * NZ + xyz[:, 2]
+    order = np.argsort(key)
+    skey = key[order]
+    inf = ((mat == GLASS) | (infill != 0)).astype(np.uint8)
+    out_i, out_j = [], []
+    for a, d in enumerate(((1, 0, 0), (0, 1, 0), (0, 0, 1))):
+        nk = ((xyz[:, 0].astype(np.int64) + d[0]) * NY + (xyz[:, 1] + d[1])) * NZ + (xyz[:, 2] + d[2])
+        pos = np.searchsorted(skey, nk)
+        pos = np.minimum(pos, len(skey) - 1)
+        hit = skey[pos] == nk
+        i = np.nonzero(hit)[0]
+        j = order[pos[hit]]
+        gap = (inf[i] != inf[j]) & ((a != 1) | (inf[i] == 1))
+        ok = ~gap & (sid[i] == sid[j])
+        out_i.append(i[ok]); out_j.append(j[ok])
+    return np.concatenate(out_i), np.concatenate(out_j)
+
+
+def grounded_mask(xyz, mat, sid, infill):
+    """Bricks whose bond network reaches the ground (y = 0): an ungrounded piece would be detached as debris by
+    the reference's connectivity pass (src/lib.rs:1085-1141) and has no finite load potential."""
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+    n = len(mat)
+    if n == 0:
+        return np.zeros(0, bool)
+    i, j = bond_edges(xyz, mat, sid, infill)
+    g = coo_matrix((np.ones(len(i), np.int8), (i, j)), shape=(n, n))
+    _, lab = connected_components(g, directed=False)
+    good = np.zeros(lab.max() + 1, bool)
+    good[lab[xyz[:, 1] == 0]] = True
+    return good[lab]

@@ -1,0 +1,262 @@
+"""Parity of the sm_100a path (through the C ABI) with the CPU oracle on the same seeded inputs.
+
+Bars: integer and index results (contact lists, manifolds, colours, islands, joint decisions) bit-exact; f32 state
+bit-exact where both sides run the same order (the colour order); load potentials within 1e-5 relative to the FP64
+fixed point, and equal to the FP64 red-black oracle at the same residual.
+"""
+import numpy as np
+import pytest
+
+from shatterforge_b200 import scenes as S
+
+pytestmark = pytest.mark.gpu
+
+STATIC = 0xFFFFFFFF
+POT_RTOL = 1e-5          # load potentials against the FP64 fixed point, relative to max |phi|
+STATE_RTOL = 1e-4        # body state after 60 steps, relative
+
+
+def small_debris(seed=11, n=240):
+    return S.debris_scene(n, seed=seed, obstacles=(3, 5), spacing=1.3, p_geom=0.4, kmax=12)
+
+
+# ---------------------------------------------------------------- set-up
+def test_body_setup_bit_exact(sf, oracle):
+    sc = small_debris()
+    w = sf.World(sc)
+    ow = oracle.OracleWorld(sc)
+    b12, l3 = w.body_setup()
+    o12, ol3 = ow.setup()
+    np.testing.assert_array_equal(b12, o12)
+    np.testing.assert_array_equal(l3, ol3)
+    st, _, _ = w.bodies()
+    ost, _, _ = ow.bodies()
+    np.testing.assert_array_equal(st, ost)
+    np.testing.assert_array_equal(w.brick_positions(), ow.brick_positions())
+
+
+def test_bonds_bit_exact(sf, oracle):
+    w3 = S.config3_world(scale=0.05, n_struct=6)
+    w = sf.World(w3)
+    ow = oracle.OracleWorld(w3)
+    b, nb, _ = w.bonds()
+    ob, onb = ow.bonds()
+    np.testing.assert_array_equal(b, ob)
+    np.testing.assert_array_equal(nb, onb)
+
+
+# ---------------------------------------------------------------- load path
+@pytest.mark.parametrize("removed", [False, True])
+def test_sor_matches_fp64_redblack_at_same_residual(sf, oracle, removed):
+    sc, rm = S.config1_frame()
+    if removed:
+        sc = sc.without_static(rm)
+    w = sf.World(sc)
+    rep = w.structure_solve(0, omega=1.7, tol=1e-6, max_sweeps=50000)
+    sw, rs = w.solve_detail()
+    ow = oracle.OracleWorld(sc)
+    osw, ors = ow.sor(0, 1.7, 1e-6, 50000, mode=oracle.MODE_REDBLACK_F64)
+    assert sw[0] == osw and rep.max_sweeps_done == osw
+    assert rs[0] == ors
+    np.testing.assert_array_equal(w.phi64(), ow.phi64())
+
+
+def test_sor_within_tolerance_of_fp64_fixed_point(sf, oracle):
+    sc, rm = S.config1_frame()
+    sc = sc.without_static(rm)
+    w = sf.World(sc)
+    w.structure_solve(0, omega=1.7, tol=1e-9, max_sweeps=100000)
+    ex = oracle.OracleWorld(sc)
+    ex.sor(0, 1.7, 1e-14, 400000, mode=oracle.MODE_LEX_F64)
+    exact = ex.phi64()
+    err = np.abs(w.phi64() - exact).max() / np.abs(exact).max()
+    assert err <= POT_RTOL, err
+
+
+def test_sor_many_structures_one_launch(sf, oracle):
+    sc = S.config3_world(scale=0.05, n_struct=8)
+    w = sf.World(sc)
+    w.structure_solve(-1, omega=1.7, tol=1e-6, max_sweeps=50000)
+    sw, rs = w.solve_detail()
+    phi = w.phi64()
+    for s in sc.structure_ids():
+        ow = oracle.OracleWorld(sc)
+        osw, ors = ow.sor(s, 1.7, 1e-6, 50000, mode=oracle.MODE_REDBLACK_F64)
+        mask = sc.static_sid == s
+        assert sw[s] == osw, (s, sw[s], osw)
+        np.testing.assert_array_equal(phi[mask], ow.phi64()[mask])
+
+
+def _joint_table(ids, vals, ns):
+    dec = np.full((ns, 4), 255, np.uint8)
+    rat = np.zeros((ns, 4), np.float32)
+    bnd = np.zeros((ns, 4), np.float32)
+    crushed = np.full((ns, 4), STATIC, np.uint32)
+    for (i, ax, j, d, k), (r, b) in zip(ids, vals):
+        dec[i, ax] = d; rat[i, ax] = r; bnd[i, ax] = b; crushed[i, ax] = k
+    return dec, rat, bnd, crushed
+
+
+@pytest.mark.parametrize("case", ["intact", "removed", "weak"])
+def test_joint_decisions_bit_exact(sf, oracle, case):
+    sc, rm = S.config1_frame()
+    if case != "intact":
+        sc = sc.without_static(rm)
+    if case == "weak":
+        # timber ground storey under concrete slabs: overloaded columns crush, slab joints fail
+        sc.static_mat[(sc.static_xyz[:, 1] < 6)] = S.WOOD
+    w = sf.World(sc)
+    w.structure_solve(0, omega=1.7, tol=1e-7, max_sweeps=100000)
+    phi = w.phi()
+    ow = oracle.OracleWorld(sc)
+    ow.set_phi(phi)
+    ids, vals, mr = ow.stress(0, dt=1 / 60, live=True)
+    rep = w.structure_check(0, dt=1 / 60, live=True)
+    r, b, d, k = w.joints()
+    odec, orat, obnd, ocr = _joint_table(ids, vals, sc.n_static)
+    np.testing.assert_array_equal(d, odec)
+    present = odec != 255
+    np.testing.assert_array_equal(r[present], orat[present])
+    np.testing.assert_array_equal(b[present], obnd[present])
+    crush = odec == 3
+    np.testing.assert_array_equal(k[crush], ocr[crush])
+    assert rep.max_ratio == pytest.approx(mr, rel=0, abs=0)
+    if case == "weak":
+        assert rep.over > 0
+
+
+# ---------------------------------------------------------------- rigid step
+def _compare_step_outputs(w, ow, scene=0):
+    ids, f, s = w.contacts(scene)
+    oids, of, os_ = ow.contacts()
+    assert len(ids) == len(oids)
+    np.testing.assert_array_equal(ids, oids)
+    np.testing.assert_array_equal(f, of)
+    np.testing.assert_array_equal(s, os_)
+    m = w.manifolds(scene)
+    om = ow.manifolds()
+    np.testing.assert_array_equal(m, om)
+
+
+def test_one_step_bit_exact(sf, oracle):
+    sc = small_debris()
+    w = sf.World(sc, iterations=8)
+    ow = oracle.OracleWorld(sc)
+    for k in range(40):
+        w.step(1 / 60)
+        ow.step(1 / 60, iterations=8, order=oracle.ORDER_COLOR)
+    # 40 steps in, bodies are landing on the ground and on each other
+    st, sl, fl = w.bodies()
+    ost, osl, ofl = ow.bodies()
+    np.testing.assert_array_equal(fl, ofl)
+    np.testing.assert_array_equal(st, ost)
+    np.testing.assert_array_equal(sl, osl)
+    _compare_step_outputs(w, ow)
+    lab = w.islands()
+    np.testing.assert_array_equal(lab, ow.islands())
+    assert w.stats().contacts > 0
+
+
+def test_step_from_gpu_state(sf, oracle):
+    """Per-step parity from the same input state: the GPU's state after 80 steps is fed to the oracle."""
+    sc = small_debris(seed=12)
+    w = sf.World(sc, iterations=8)
+    w.step(1 / 60, nsteps=80)
+    st, sl, fl = w.bodies()
+    ow = oracle.OracleWorld(sc)
+    ow.set_bodies(st, sl, fl)
+    w.step(1 / 60)
+    ow.step(1 / 60, iterations=8, order=oracle.ORDER_COLOR)
+    _compare_step_outputs(w, ow)
+    st2, _, fl2 = w.bodies()
+    ost2, _, ofl2 = ow.bodies()
+    np.testing.assert_array_equal(fl2, ofl2)
+    np.testing.assert_array_equal(st2, ost2)
+
+
+def test_sixty_steps_within_tolerance(sf, oracle):
+    sc = small_debris(seed=13, n=400)
+    w = sf.World(sc, iterations=8, sleep_mode=sf.SF_SLEEP_ISLAND)
+    ow = oracle.OracleWorld(sc)
+    for _ in range(60):
+        w.step(1 / 60)
+        ow.step(1 / 60, iterations=8, order=oracle.ORDER_COLOR, sleep_mode=oracle.SLEEP_ISLAND)
+    st, _, fl = w.bodies()
+    ost, _, ofl = ow.bodies()
+    np.testing.assert_array_equal(fl, ofl)
+    scale = np.maximum(np.abs(ost), 1.0)
+    assert (np.abs(st - ost) / scale).max() <= STATE_RTOL
+    np.testing.assert_array_equal(w.islands(), ow.islands())
+
+
+def test_colouring_is_proper_and_reported(sf):
+    sc = S.debris_scene(1500, seed=21, spacing=1.0)
+    w = sf.World(sc, iterations=8, verify=1)
+    w.step(1 / 60, nsteps=90)
+    st = w.stats()
+    assert st.error_word == 0
+    m = w.manifolds()
+    assert len(m) == st.manifolds
+    # at every awake body, no two of its manifolds share a colour
+    seen = set()
+    for a, b, c, n in m:
+        for body in (a, b):
+            if body == STATIC:
+                continue
+            assert (body, c) not in seen
+            seen.add((body, c))
+
+
+def test_scenes_batched_equal_alone(sf):
+    scenes = [small_debris(seed=30 + k, n=100 + 37 * k) for k in range(4)]
+    big = sf.World(scenes, iterations=8)
+    big.step(1 / 60, nsteps=30)
+    bst, _, bfl = big.bodies()
+    off = big.body_off
+    for k, sc in enumerate(scenes):
+        w = sf.World(sc, iterations=8)
+        w.step(1 / 60, nsteps=30)
+        st, _, fl = w.bodies()
+        np.testing.assert_array_equal(st, bst[off[k]:off[k + 1]])
+        np.testing.assert_array_equal(fl, bfl[off[k]:off[k + 1]])
+        ids, f, s = w.contacts(0)
+        bids, bf, bs = big.contacts(k)
+        np.testing.assert_array_equal(ids, bids)
+        np.testing.assert_array_equal(s, bs)
+
+
+def test_config1_scene_runs(sf, oracle):
+    sc = S.config1_scene()
+    w = sf.World(sc, iterations=8)
+    ow = oracle.OracleWorld(sc)
+    for _ in range(20):
+        w.step(1 / 60)
+        ow.step(1 / 60, iterations=8, order=oracle.ORDER_COLOR)
+    st, _, fl = w.bodies()
+    ost, _, ofl = ow.bodies()
+    np.testing.assert_array_equal(fl, ofl)
+    np.testing.assert_array_equal(st, ost)
+
+
+# ---------------------------------------------------------------- box SAT
+def test_box_sat_bit_exact(sf, oracle):
+    rng = np.random.default_rng(5)
+    n = 2000
+    def boxes(n):
+        b = np.zeros((n, 10), np.float32)
+        b[:, :3] = rng.uniform(-0.6, 0.6, (n, 3))
+        q = rng.normal(size=(n, 4))
+        b[:, 3:7] = q / np.linalg.norm(q, axis=1, keepdims=True)
+        b[:, 7:] = rng.uniform(0.1, 0.6, (n, 3))
+        return b
+    a, b = boxes(n), boxes(n)
+    cnt, nrm, pts = sf.collide_boxes(a, b, margin=0.02)
+    hits = 0
+    for i in range(n):
+        on, onrm, opts = oracle.collide_boxes(a[i], b[i], margin=0.02)
+        assert cnt[i] == on, i
+        if on:
+            hits += 1
+            np.testing.assert_array_equal(nrm[i], onrm)
+            np.testing.assert_array_equal(pts[i, :on], opts)
+    assert hits > n // 4
