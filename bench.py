@@ -1,0 +1,449 @@
+#!/usr/bin/env python
+"""Benchmark of the sm_100a Shatterforge physics path.
+
+Headline: body-steps/s of the batched rigid step on the 256-scene debris mix (256 independent scenes, body counts
+log-uniform in 500-20,000, compound bodies of Geometric(0.3) bricks, 4-16 static box obstacles each; dt = 1/60 s,
+8 impulse iterations, 2 substeps), every scene stepped in the same launches. Beside it, in the same JSON line:
+  * the plain path (one scene per launch sequence) timed on the same simulated state, and the batched/plain ratio;
+  * the load path: all 37 structures of the structures-in-one-lattice configuration solved in one persistent launch
+    to residual 1e-6 (omega 1.7), as brick-sweeps/s;
+  * e2e: the same metric through the public C ABI with the body state written from and read back to pinned host
+    buffers every step;
+  * roofline of the dominant kernel (CUDA events around each launch, algorithmic bytes per unit as documented);
+  * cpu_baseline: the CPU restatement of the reference (the oracle) on a bounded sample of the same workload.
+
+`--impl reference` times only the CPU restatement (the reference itself is a wasm32 Rust crate that cannot be
+built here) with every host thread, and prints its own line.
+
+Multi-GPU (torchrun): each rank runs its own 256-scene mix (seeded by rank), no collective on the data path;
+value = all ranks' body-steps / the slowest rank's device time ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "body-steps/s & SOR brick-sweeps/s; served p50/p99 ms vs plain GPU path"
+UNIT = "body-steps/s"
+DT = 1.0 / 60.0
+ITERS = 8
+SOLVE_BYTES_PER_CONTACT_ITER = 184     # contact 64 + impulse r/w 24 + both bodies' v, w r/w 96
+SOR_BYTES_PER_BRICK_SWEEP = 24         # f64 potential r/w 16 + rhs 4 + link word 4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=600)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scenes", type=int, default=256)
+    ap.add_argument("--scale", type=float, default=1.0, help="body-count scale of the debris mix (1.0 = as specified)")
+    ap.add_argument("--plain-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="0 = as --steps")
+    ap.add_argument("--no-sor", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        try:
+            rows = [r.split(",") for r in Path(self.path).read_text().strip().splitlines() if r.strip()]
+        except OSError:
+            return out
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1])); mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if sm:
+            out.update(sm_mhz=statistics.median(sm), sm_max_mhz=max(mx), reasons=sorted(reasons), samples=len(sm))
+        return out
+
+
+# ---------------------------------------------------------------- distributed plumbing
+def dist_setup(args):
+    rank, world, local = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        if args.impl == "ours":
+            torch.cuda.set_device(local)
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg, args):
+    if pg is None:
+        return
+    import torch
+    if args.impl == "ours":
+        pg.barrier(device_ids=[torch.cuda.current_device()])
+    else:
+        pg.barrier()
+
+
+def allreduce_max(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- CPU restatement (oracle) timing
+def cpu_body_steps(scenes, states, seconds: float, threads: int):
+    """Steps the oracle on the given scenes from the given states, one scene per thread, for about `seconds`."""
+    from oracle import binding as orc
+    results = []
+    lock = threading.Lock()
+
+    def work(sc, st):
+        ow = orc.OracleWorld(sc)
+        if st is not None:
+            ow.set_bodies(*st)
+        _, _, fl = ow.bodies()
+        alive = int((fl & 1).sum())
+        t0 = time.perf_counter()
+        n = 0
+        while time.perf_counter() - t0 < seconds:
+            ow.step(DT, iterations=ITERS, order=orc.ORDER_COLOR, pinch_kill=0)
+            n += 1
+        el = time.perf_counter() - t0
+        _, _, fl = ow.bodies()
+        # bodies only leave by falling out of the world (pinch removal is off): count the mean of start and end
+        bsteps = n * (alive + int((fl & 1).sum())) // 2
+        with lock:
+            results.append((bsteps, el, n))
+
+    ths = [threading.Thread(target=work, args=(sc, st)) for sc, st in zip(scenes, states)]
+    for i in range(0, len(ths), threads):
+        batch = ths[i:i + threads]
+        for t in batch:
+            t.start()
+        for t in batch:
+            t.join()
+    bsteps = sum(r[0] for r in results)
+    el = max(r[1] for r in results) if results else 1.0
+    return bsteps / el, sum(r[2] for r in results)
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_arm(args, rank, world, pg):
+    """The reference's CPU path, restated (the Rust/wasm reference cannot be built here), on every host thread."""
+    if rank != 0:
+        return
+    from shatterforge_b200 import scenes as S
+    scenes = S.config4_scenes(n_scenes=args.scenes, scale=args.scale)
+    threads = host_threads()
+    # bounded sample: `threads` scenes spread over the size range, each stepped for the time budget from rest
+    order = np.argsort([s.n_bodies for s in scenes])
+    pick = order[np.linspace(0, len(order) - 1, min(threads, len(order))).astype(int)]
+    sample = [scenes[i] for i in pick]
+    per = max(1.0, args.cpu_seconds)
+    rate, steps = cpu_body_steps(sample, [None] * len(sample), per, threads)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": 0, "steps": int(steps),
+        "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"config4: {args.scenes} debris scenes, 1/60 s, {ITERS} iterations, 2 substeps",
+                   "sample": f"{len(sample)} scenes ({sum(s.n_bodies for s in sample)} bodies) stepped {per:.0f} s each from rest"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{len(sample)} of {args.scenes} scenes, one per thread, {per:.0f} s each"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+def run_steps(w, k: int):
+    """k world steps, one call each; returns (summed alive bodies, device ms from the library's events)."""
+    alive = 0
+    ms = 0.0
+    for _ in range(k):
+        st = w.step(DT, 1)
+        alive += st.alive
+        ms += st.ms_last_step
+    return alive, ms
+
+
+def our_arm(args, rank, world, local, pg):
+    import torch
+
+    import shatterforge_b200 as sf
+    from shatterforge_b200 import scenes as S
+
+    dev = torch.cuda.current_device()
+    seed = 3 + 7919 * rank
+    scenes = S.config4_scenes(seed=seed, n_scenes=args.scenes, scale=args.scale)
+    n_bodies = sum(s.n_bodies for s in scenes)
+    n_bricks = sum(s.n_body_bricks for s in scenes)
+    stream = torch.cuda.current_stream()
+    params = dict(iterations=ITERS, pinch_kill=0, verify=1)
+
+    # ---- device-resident timed run
+    w = sf.World(scenes, **params)
+    w.set_stream(stream.cuda_stream)
+    run_steps(w, args.warmup)
+    w.set_profiling(True)
+    w.reset_profile()
+    barrier(pg, args)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev) as clk:
+        e0.record(stream)
+        alive_sum, _ = run_steps(w, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(pg, args)
+    ms = e0.elapsed_time(e1)
+    clocks = clk.summary()
+    prof = w.profile()
+    stats = w.stats()
+    ms_max = allreduce_max(pg, ms)
+    alive_total = allreduce_sum(pg, alive_sum)
+    value = alive_total / (ms_max * 1e-3)
+
+    # roofline of the dominant phase
+    phase_ms = prof["ms"]
+    top = max(phase_ms, key=phase_ms.get)
+    solve_ms = phase_ms["solve"]
+    solve_bytes = SOLVE_BYTES_PER_CONTACT_ITER * prof["solve_contact_iters"]
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    per_launch_ms = solve_ms / max(prof["solve_launches"], 1)
+    achieved = solve_bytes / max(solve_ms * 1e-3, 1e-12) / 1e9
+    roofline = {"kernel": "k_solve (coloured sequential-impulse solve, persistent)", "bound": "hbm", "achieved": achieved,
+                "peak": hbm, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback", "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None,
+                "bytes_per_launch": solve_bytes / max(prof["solve_launches"], 1), "ms_per_launch": per_launch_ms,
+                "unit_bytes": f"{SOLVE_BYTES_PER_CONTACT_ITER} B per contact-iteration"}
+    state_after = w.bodies()
+    sample_states = None
+
+    # ---- plain path on the same simulated state: each scene alone, one launch sequence per scene
+    plain = None
+    if not args.no_plain and rank == 0 and args.plain_steps > 0:
+        st, sl, fl = state_after
+        worlds = []
+        for k, sc in enumerate(scenes):
+            pw = sf.World(sc, **params)
+            pw.set_stream(stream.cuda_stream)
+            a, b = w.body_off[k], w.body_off[k + 1]
+            pw.set_bodies(st[a:b], sl[a:b], fl[a:b])
+            worlds.append(pw)
+        # the batched path over the same steps from the same state
+        wb = sf.World(scenes, **params)
+        wb.set_stream(stream.cuda_stream)
+        wb.set_bodies(st, sl, fl)
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        b_alive, _ = run_steps(wb, args.plain_steps)
+        t1.record(stream); torch.cuda.synchronize()
+        b_ms = t0.elapsed_time(t1)
+        t0.record(stream)
+        p_alive = 0
+        for _ in range(args.plain_steps):
+            for pw in worlds:
+                p_alive += pw.step(DT, 1).alive
+        t1.record(stream); torch.cuda.synchronize()
+        p_ms = t0.elapsed_time(t1)
+        plain = {"value": p_alive / (p_ms * 1e-3), "unit": UNIT, "steps": args.plain_steps,
+                 "batched_same_steps": b_alive / (b_ms * 1e-3),
+                 "batched_over_plain": (b_alive / b_ms) / max(p_alive / p_ms, 1e-30),
+                 "note": "steps after the timed run, from the same state, each scene stepped by its own launches"}
+        for pw in worlds:
+            pw.close()
+        wb.close()
+    w.close()
+
+    # ---- end to end through the C ABI with pinned host buffers
+    e2e_steps = args.e2e_steps or args.steps
+    we = sf.World(scenes, **params)
+    we.set_stream(stream.cuda_stream)
+    run_steps(we, args.warmup)
+    nb = we.info.n_bodies
+    h_state = torch.empty((nb, 13), dtype=torch.float32, pin_memory=True).numpy()
+    h_sleep = torch.empty((nb,), dtype=torch.float32, pin_memory=True).numpy()
+    h_flags = torch.empty((nb,), dtype=torch.uint8, pin_memory=True).numpy()
+    s0, s1, s2 = we.bodies()
+    h_state[:] = s0; h_sleep[:] = s1; h_flags[:] = s2
+    barrier(pg, args)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e_alive = 0
+    for _ in range(e2e_steps):
+        we.set_bodies(h_state, h_sleep, h_flags)
+        e_alive += we.step(DT, 1).alive
+        a, b, c = we.bodies()
+        h_state[:] = a; h_sleep[:] = b; h_flags[:] = c
+    torch.cuda.synchronize()
+    e_s = time.perf_counter() - t0
+    barrier(pg, args)
+    e_s = allreduce_max(pg, e_s)
+    e_alive = allreduce_sum(pg, e_alive)
+    bytes_io = nb * (13 * 4 + 4 + 1)
+    e2e = {"value": e_alive / e_s, "unit": UNIT, "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io,
+           "steps": e2e_steps, "note": "host-owned state: write bodies, step, read bodies, every step (pinned buffers)"}
+    we.close()
+
+    # ---- load path: 37 structures in one lattice, one persistent launch to residual 1e-6
+    sor = None
+    if not args.no_sor:
+        c3 = S.config3_world(seed=2 + rank)
+        ws = sf.World(c3)
+        ws.set_stream(stream.cuda_stream)
+        ws.structure_solve(-1, omega=1.7, tol=1e-6, max_sweeps=200000)   # warm-up (same work)
+        ws.set_phi(np.zeros(c3.n_static, np.float32))
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        rep = ws.structure_solve(-1, omega=1.7, tol=1e-6, max_sweeps=200000)
+        t1.record(stream); torch.cuda.synchronize()
+        s_ms = t0.elapsed_time(t1)
+        bs = rep.brick_sweeps
+        sor = {"brick_sweeps_per_s": bs / (s_ms * 1e-3), "bricks": c3.n_static, "structures": rep.structures,
+               "max_sweeps": rep.max_sweeps_done, "brick_sweeps": bs, "ms": s_ms, "max_residual": rep.max_residual,
+               "roofline": {"bound": "hbm", "unit": "GB/s", "achieved": SOR_BYTES_PER_BRICK_SWEEP * bs / (s_ms * 1e-3) / 1e9,
+                            "peak": hbm, "frac": SOR_BYTES_PER_BRICK_SWEEP * bs / (s_ms * 1e-3) / 1e9 / hbm,
+                            "unit_bytes": f"{SOR_BYTES_PER_BRICK_SWEEP} B per brick-sweep"}}
+        ws.close()
+
+    # ---- CPU baseline: the oracle on a bounded sample of the same workload, from the GPU's state
+    cpu = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        st, sl, fl = state_after
+        order = np.argsort([s.n_bodies for s in scenes])
+        pick = order[np.linspace(0, len(order) - 1, 4).astype(int)]
+        samp = [scenes[i] for i in pick]
+        body_off = np.cumsum([0] + [s.n_bodies for s in scenes])
+        states = [(st[body_off[i]:body_off[i + 1]], sl[body_off[i]:body_off[i + 1]], fl[body_off[i]:body_off[i + 1]])
+                  for i in pick]
+        rate1, n1 = cpu_body_steps(samp[:1], states[:1], args.cpu_seconds / 2, 1)
+        threads = host_threads()
+        rate_n, n_n = cpu_body_steps(samp, states, args.cpu_seconds / 2, threads)
+        cpu = {"value": rate1, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"1 scene ({samp[0].n_bodies} bodies) from the GPU state after the timed run, {n1} steps",
+               "all_cores": {"value": rate_n, "cores": min(threads, len(samp)),
+                             "sample": f"{len(samp)} scenes, one per thread, {n_n} steps in all"}}
+
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded generators of the configured shapes)",
+        "config": {"workload": f"config4: {args.scenes} debris scenes in one batch, {n_bodies} bodies, {n_bricks} brick spheres"
+                               f" per GPU, dt 1/60 s, {ITERS} iterations, 2 substeps",
+                   "scenes": args.scenes, "bodies_per_gpu": n_bodies, "bricks_per_gpu": n_bricks, "iterations": ITERS,
+                   "substeps": 2, "pinch_kill": 0, "l2": "inputs larger than L2 (world state several hundred MB)",
+                   "parallelism": f"{world} independent replica(s)"},
+        "clocks": clocks,
+        "e2e": e2e,
+        "gpu_launches": int(prof["launches"]),
+        "roofline": roofline,
+        "phases_ms": {k: round(v, 3) for k, v in phase_ms.items()},
+        "top_phase": top,
+        "last_step": {"contacts": int(stats.contacts), "manifolds": int(stats.manifolds), "colors": int(stats.colors),
+                      "color_rounds": int(stats.color_rounds), "islands": int(stats.islands), "alive": int(stats.alive),
+                      "awake": int(stats.awake)},
+        "plain": plain,
+        "sor": sor,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            reference_arm(args, rank, world, pg)
+        else:
+            our_arm(args, rank, world, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

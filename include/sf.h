@@ -89,7 +89,19 @@ typedef struct sf_stats {
     uint32_t error_word;        /* device error bits (0 = none) */
     uint64_t contact_capacity;
     double ms_last_step;        /* device time of the last sf_world_step call (CUDA events) */
+    uint64_t launches;          /* kernels this world has launched (all entry points) */
 } sf_stats;
+
+/* Per-phase device time of the rigid step, from CUDA events around each phase of each substep (profiling on). */
+#define SF_PHASES 9             /* pose, hash, contacts, manifolds, prep, colour, solve, islands, integrate */
+typedef struct sf_profile {
+    double ms[SF_PHASES];
+    uint64_t substeps;
+    uint64_t solve_launches;
+    uint64_t solve_contact_iters;   /* sum over solve launches of contacts x iterations */
+    uint64_t contacts_sum;          /* sum over substeps of contacts */
+    uint64_t launches;
+} sf_profile;
 
 typedef struct sf_solve_report {
     uint32_t structures;        /* structures solved */
@@ -115,6 +127,13 @@ void sf_world_destroy(sf_world *w);
 const char *sf_status_string(sf_status s);
 const char *sf_last_error(void);
 int32_t sf_version(void);
+
+/* All of the world's device work goes to `stream` (a cudaStream_t; NULL = the world's own stream). */
+sf_status sf_world_set_stream(sf_world *w, void *stream);
+/* Phase timing with CUDA events (off by default; costs ten event records per substep). */
+sf_status sf_set_profiling(sf_world *w, int32_t on);
+sf_status sf_read_profile(sf_world *w, sf_profile *out);
+sf_status sf_reset_profile(sf_world *w);
 
 /* ---- hot path */
 /* nsteps world steps of dt each (dt clamped to [0, 1/30] as src/lib.rs:3642 does), all scenes at once. */

@@ -60,7 +60,16 @@ class Stats(C.Structure):
     _fields_ = [("contacts", C.c_uint64), ("manifolds", C.c_uint64), ("ref_would_drop", C.c_uint64),
                 ("colors", C.c_uint32), ("color_rounds", C.c_uint32), ("islands", C.c_uint32), ("alive", C.c_uint32),
                 ("awake", C.c_uint32), ("error_word", C.c_uint32), ("contact_capacity", C.c_uint64),
-                ("ms_last_step", C.c_double)]
+                ("ms_last_step", C.c_double), ("launches", C.c_uint64)]
+
+
+SF_PHASES = 9
+PHASE_NAMES = ["pose", "hash", "contacts", "manifolds", "prep", "colour", "solve", "islands", "integrate"]
+
+
+class Profile(C.Structure):
+    _fields_ = [("ms", C.c_double * SF_PHASES), ("substeps", C.c_uint64), ("solve_launches", C.c_uint64),
+                ("solve_contact_iters", C.c_uint64), ("contacts_sum", C.c_uint64), ("launches", C.c_uint64)]
 
 
 class SolveReport(C.Structure):
@@ -87,6 +96,10 @@ PROTOTYPES = {
     "sf_last_error": (C.c_char_p, []),
     "sf_version": (C.c_int32, []),
     "sf_world_step": (C.c_int32, [C.c_void_p, C.c_float, C.c_uint32]),
+    "sf_world_set_stream": (C.c_int32, [C.c_void_p, C.c_void_p]),
+    "sf_set_profiling": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "sf_read_profile": (C.c_int32, [C.c_void_p, C.POINTER(Profile)]),
+    "sf_reset_profile": (C.c_int32, [C.c_void_p]),
     "sf_structure_solve": (C.c_int32, [C.c_void_p, C.c_int32, C.c_float, C.c_float, C.c_uint32, C.POINTER(SolveReport)]),
     "sf_structure_check": (C.c_int32, [C.c_void_p, C.c_int32, C.c_float, C.c_int32, C.POINTER(CheckReport)]),
     "sf_read_solve_detail": (C.c_int32, [C.c_void_p, _u32p, C.POINTER(C.c_double)]),
@@ -221,6 +234,23 @@ class World:
 
     def __exit__(self, *a):
         self.close()
+
+    # -- streams and profiling
+    def set_stream(self, stream_handle: int | None):
+        """Route the world's device work to a cudaStream_t (an integer handle, e.g. torch's .cuda_stream)."""
+        _check(self._lib.sf_world_set_stream(self._h, C.c_void_p(stream_handle or 0)), "sf_world_set_stream")
+
+    def set_profiling(self, on: bool = True):
+        _check(self._lib.sf_set_profiling(self._h, 1 if on else 0), "sf_set_profiling")
+
+    def profile(self) -> dict:
+        p = Profile()
+        _check(self._lib.sf_read_profile(self._h, C.byref(p)), "sf_read_profile")
+        return {"ms": dict(zip(PHASE_NAMES, list(p.ms))), "substeps": p.substeps, "solve_launches": p.solve_launches,
+                "solve_contact_iters": p.solve_contact_iters, "contacts_sum": p.contacts_sum, "launches": p.launches}
+
+    def reset_profile(self):
+        _check(self._lib.sf_reset_profile(self._h), "sf_reset_profile")
 
     # -- hot path
     def step(self, dt: float = 1.0 / 60.0, nsteps: int = 1) -> "Stats":

@@ -124,8 +124,10 @@ struct DBuf {
 // persistent-kernel grid barrier state (bounded spin, see grid_sync)
 struct GridBarrier { unsigned count; unsigned gen; };
 
-struct SorState;     // sf_sor.cu
 struct StepState;    // sf_step.cu
+struct SorState;     // sf_sor.cu
+uint64_t sor_launches(const SorState *st);
+void sor_reset_launches(SorState *st);
 
 struct Scene {
     uint32_t static_off, n_static;
@@ -139,7 +141,9 @@ struct Scene {
 struct sf_world {
     int device = 0;
     int sms = 148;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // where all device work goes (the caller's, or own_stream)
+    cudaStream_t own_stream = nullptr;
+    uint64_t launches = 0;              // kernels this world launched (scans and sorts counted in their Work)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     sf_params P{};
     uint32_t n_scenes = 0, ns = 0, nd = 0, nb = 0, n_struct = 0, n_chunks = 0;
@@ -169,6 +173,8 @@ struct sf_world {
     sf::DBuf<uint8_t> k_mat;
     sf::DBuf<int32_t> k_xyz;
 
+    sf::DBuf<float> stage13;     // packed body state for the read/write calls
+    sf::DBuf<uint8_t> stage_flags;
     sf::DBuf<uint32_t> err;      // [0] error bits, [1..] counters
     sf::DBuf<sf::GridBarrier> barrier;
 
@@ -194,6 +200,7 @@ inline unsigned grid_for(size_t n, unsigned block) { return (unsigned)((n + bloc
 // scratch for scans and sorts (grows on demand, never shrinks)
 struct Work {
     DBuf<uint32_t> scan_a, scan_b, hist;
+    uint64_t launches = 0;   // kernels launched by the scans and sorts
 };
 // exclusive scan of n uint32 values (in place allowed); the total is written to *d_total if non-null
 cudaError_t exclusive_scan_u32(const uint32_t *in, uint32_t *out, size_t n, uint32_t *d_total, Work &wk, cudaStream_t s);

@@ -48,6 +48,7 @@ struct SorState {
     DBuf<uint32_t> counters;        // joints, over, failed, crushed, maxr bits, ncand
     DBuf<uint32_t> st_req;          // requested structures list for the apply pass
     Work wk;
+    uint64_t launches = 0;
     int occ = 1;
 };
 
@@ -524,6 +525,9 @@ sf_status sor_create(sf_world *w) {
     return SF_OK;
 }
 
+uint64_t sor_launches(const SorState *st) { return st ? st->wk.launches + st->launches : 0; }
+void sor_reset_launches(SorState *st) { if (st) { st->wk.launches = 0; st->launches = 0; } }
+
 void sor_destroy(sf_world *w) {
     delete w->sor;
     w->sor = nullptr;
@@ -575,6 +579,7 @@ sf_status sf_structure_solve(sf_world *w, int32_t structure, float omega, float 
     SF_CUDA(cudaEventRecord(w->ev0, s));
     size_t ncell = (size_t)w->n_chunks * 512;
     k_sor_clear<<<grid_for(ncell, 256), 256, 0, s>>>((uint32_t)ncell, st->ccode.p, st->csid.p);
+    st->launches += 5;   // clear, scatter, init, red-black, gather
     k_sor_scatter<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p, w->s_nb6.p,
                                                        w->s_bond.p, w->s_phi64.p, w->s_ext.p, w->ctab.p, st->cphi.p,
                                                        st->crhs.p, st->ccode.p, st->csid.p);
@@ -637,6 +642,7 @@ sf_status sf_structure_check(sf_world *w, int32_t structure, float dt, int32_t l
     SF_CUDA(cudaMemsetAsync(st->counters.p, 0, st->counters.bytes(), s));
     SF_CUDA(cudaEventRecord(w->ev0, s));
     k_stress_zero<<<grid_for(ns, 256), 256, 0, s>>>(ns, w->s_sid.p, w->s_mat.p, st->active0.p, w->s_stress.p);
+    st->launches += 5;   // zero, eval, compact, apply, tally
     StressArgs A;
     A.ns = ns; A.cell = w->s_cell.p; A.mat = w->s_mat.p; A.sid = w->s_sid.p; A.nb6 = w->s_nb6.p; A.bond = w->s_bond.p;
     A.bmax = w->s_bmax.p; A.phi = w->s_phi.p; A.active = st->active0.p; A.dt = dt; A.live = live ? 1 : 0;

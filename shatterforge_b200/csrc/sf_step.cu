@@ -63,7 +63,25 @@ struct StepState {
     uint64_t last_contacts = 0;
     int solve_occ = 1, jp_occ = 1;
     bool have_contacts = false;
+    // profiling: PH_N + 1 events per substep, elapsed times folded in after each sf_world_step
+    bool profile = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<uint32_t> sub_nc;
+    double ph_ms[SF_PHASES] = {};
+    uint64_t ph_substeps = 0, solve_contact_iters = 0, solve_launches = 0;
 };
+
+static void prof_mark(sf_world *w) {
+    StepState *S = w->step;
+    if (!S->profile) return;
+    if (S->ev_used == S->ev_pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) { S->profile = false; return; }
+        S->ev_pool.push_back(e);
+    }
+    cudaEventRecord(S->ev_pool[S->ev_used++], w->stream);
+}
 
 enum { DV_CONTACTS = 0, DV_MANIFOLDS = 1, DV_COLORS = 2, DV_ROUNDS = 3, DV_WL0 = 4, DV_WL1 = 5, DV_WL2 = 6,
        DV_ALIVE = 7, DV_AWAKE = 8, DV_ISLANDS = 9, DV_N = 16 };
@@ -800,11 +818,15 @@ static sf_status substep(sf_world *w, float h) {
     const uint32_t nb = w->nb, nd = w->nd;
     const uint64_t none_key = (uint64_t)w->n_scenes * HSIZE;
     if (nb == 0 || nd == 0) return SF_OK;
+    uint64_t &L = w->launches;
     // pose cache + gravity, brick positions
+    prof_mark(w);
     k_update_cache<<<grid_for(nb, 128), 128, 0, s>>>(nb, h, w->b_alive.p, w->b_asleep.p, w->b_q.p, w->b_iil.p, w->b_rot.p,
                                                      w->b_iiw.p, w->b_v.p);
     k_brick_pos<<<grid_for(nd, 256), 256, 0, s>>>(nd, w->k_body.p, w->b_alive.p, w->b_asleep.p, w->b_pos.p, w->b_rot.p,
                                                   w->k_local.p, w->k_wpos.p);
+    L += 2;
+    prof_mark(w);
     // hashed cells
     k_cell_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, w->k_body.p, w->b_scene.p, w->b_alive.p, w->k_wpos.p,
                                                   S->ckey.p, S->cval.p);
@@ -812,6 +834,8 @@ static sf_status substep(sf_world *w, float h) {
     SF_CUDA(cudaMemsetAsync(S->bstart.p, 0, S->bstart.bytes(), s));
     SF_CUDA(cudaMemsetAsync(S->bend.p, 0, S->bend.bytes(), s));
     k_bucket_ranges<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, S->ckey.p, S->bstart.p, S->bend.p);
+    L += 2;
+    prof_mark(w);
     // contacts: count, scan, fill
     ContactArgs C;
     C.nd = nd; C.kbody = w->k_body.p; C.bscene = w->b_scene.p; C.ctab = w->ctab.p; C.cpool = w->cpool.p;
@@ -834,7 +858,10 @@ static sf_status substep(sf_world *w, float h) {
     SF_CUDA(cudaMemsetAsync(w->b_nc.p, 0, w->b_nc.bytes(), s));
     SF_CUDA(cudaMemsetAsync(S->dev.p + DV_MANIFOLDS, 0, (DV_N - DV_MANIFOLDS) * sizeof(uint32_t), s));
     const uint32_t g_nc = grid_for(std::max<uint32_t>(nc, 1), 256);
-    if (nc) k_body_nc<<<g_nc, 256, 0, s>>>(nc, S->L_a.p, S->L_b.p, w->b_nc.p);
+    if (nc) { k_body_nc<<<g_nc, 256, 0, s>>>(nc, S->L_a.p, S->L_b.p, w->b_nc.p); L++; }
+    L += 2;
+    if (S->profile) S->sub_nc.push_back(nc);
+    prof_mark(w);
     // manifolds
     const uint64_t nb1 = (uint64_t)nb + 1;
     if (nc) {
@@ -845,12 +872,16 @@ static sf_status substep(sf_world *w, float h) {
         k_man_write<<<g_nc, 256, 0, s>>>(nc, S->mflag.p, S->mpos.p, S->perm.p, S->L_a.p, S->L_b.p, w->b_scene.p,
                                          S->body_off_of_body.p, S->man_a.p, S->man_b.p, S->man_start.p, S->man_prio.p);
         k_man_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, nc, S->man_start.p, S->man_count.p);
+        L += 4;
+        prof_mark(w);
         PrepArgs PA;
         PA.nc = nc; PA.h = h; PA.perm = S->perm.p; PA.L_a = S->L_a.p; PA.L_b = S->L_b.p; PA.L_p = S->L_p.p; PA.L_n = S->L_n.p;
         PA.pos = w->b_pos.p; PA.v = w->b_v.p; PA.w = w->b_w.p; PA.im = w->b_im.p; PA.iiw = w->b_iiw.p;
         PA.S_n = S->S_n.p; PA.S_t1 = S->S_t1.p; PA.S_t2 = S->S_t2.p; PA.S_ra = S->S_ra.p; PA.S_rb = S->S_rb.p; PA.S_j = S->S_j.p;
         PA.invperm = S->invperm.p;
         k_prep<<<g_nc, 256, 0, s>>>(PA);
+        L++;
+        prof_mark(w);
         // colouring
         SF_CUDA(cudaMemsetAsync(S->bm_count.p, 0, S->bm_count.bytes(), s));
         SF_CUDA(cudaMemsetAsync(S->bm_fill.p, 0, S->bm_fill.bytes(), s));
@@ -873,14 +904,21 @@ static sf_status substep(sf_world *w, float h) {
         k_col_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_color.p, S->col_count.p, S->dev.p);
         SF_CUDA(exclusive_scan_u32(S->col_count.p, S->col_start.p, MAXCOL + 1, nullptr, S->wk, s));
         k_col_fill<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_color.p, S->col_start.p, S->col_fill.p, S->col_list.p);
+        L += 6;
         if (w->P.verify) {
             SF_CUDA(cudaMemsetAsync(S->vmasks.p, 0, S->vmasks.bytes(), s));
             k_col_verify<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_a.p, S->man_b.p, S->man_color.p, S->vmasks.p, w->err.p);
+            L++;
         }
+    } else {
+        prof_mark(w);
+        prof_mark(w);
     }
     k_save_pre<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, w->b_v.p, w->b_w.p, w->b_vpre.p, w->b_wpre.p);
+    L++;
+    SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s));
+    prof_mark(w);
     if (nc && w->P.iterations) {
-        SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s));
         SolveArgs A;
         A.iterations = w->P.iterations; A.dev = S->dev.p; A.col_start = S->col_start.p; A.col_list = S->col_list.p;
         A.man_a = S->man_a.p; A.man_b = S->man_b.p; A.man_start = S->man_start.p; A.man_count = S->man_count.p;
@@ -890,11 +928,17 @@ static sf_status substep(sf_world *w, float h) {
         unsigned sgrid = (unsigned)std::min<uint64_t>((uint64_t)w->sms * per_sm, (nc + SOLVE_BLOCK - 1) / SOLVE_BLOCK + 1);
         void *sargs[] = {&A};
         SF_CUDA(cudaLaunchCooperativeKernel((void *)k_solve, dim3(sgrid), dim3(SOLVE_BLOCK), sargs, 0, s));
+        L++;
+        S->solve_launches++;
+        S->solve_contact_iters += (uint64_t)nc * w->P.iterations;
     }
+    prof_mark(w);
     // islands over the manifolds of this substep
     k_uf_init<<<grid_for(nb, 256), 256, 0, s>>>(nb, S->parent.p, S->mint.p);
-    if (nc) k_uf_union<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_a.p, S->man_b.p, S->parent.p);
+    if (nc) { k_uf_union<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_a.p, S->man_b.p, S->parent.p); L++; }
     k_uf_label<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, w->b_asleep.p, S->parent.p, S->label.p, S->dev.p);
+    L += 2;
+    prof_mark(w);
     IntArgs I;
     I.nb = nb; I.h = h; I.pinch_kill = w->P.pinch_kill ? 1 : 0; I.island_mode = w->P.sleep_mode == SF_SLEEP_ISLAND;
     I.alive = w->b_alive.p; I.asleep = w->b_asleep.p; I.pos = w->b_pos.p; I.q = w->b_q.p; I.v = w->b_v.p; I.w = w->b_w.p;
@@ -908,6 +952,8 @@ static sf_status substep(sf_world *w, float h) {
     }
     k_wake<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_wake.p, w->b_alive.p, w->b_asleep.p, w->b_sleep.p);
     k_kill_bricks<<<grid_for(nd, 256), 256, 0, s>>>(nd, w->k_body.p, w->b_alive.p, w->k_mat.p);
+    L += I.island_mode ? 5 : 3;
+    prof_mark(w);
     SF_CUDA(cudaGetLastError());
     S->have_contacts = true;
     return SF_OK;
@@ -953,7 +999,58 @@ sf_status sf_world_step(sf_world *w, float dt, uint32_t nsteps) {
     st.awake = S->h_dev[DV_AWAKE];
     st.contact_capacity = S->capacity;
     st.ms_last_step = ms;
+    st.launches = w->launches + S->wk.launches + sor_launches(w->sor);
+    if (S->profile) {
+        // each substep recorded SF_PHASES + 1 events
+        const size_t per = SF_PHASES + 1;
+        for (size_t base = 0; base + per <= S->ev_used; base += per) {
+            for (int p = 0; p < SF_PHASES; p++) {
+                float e = 0.0f;
+                if (cudaEventElapsedTime(&e, S->ev_pool[base + p], S->ev_pool[base + p + 1]) == cudaSuccess) S->ph_ms[p] += e;
+            }
+            S->ph_substeps++;
+        }
+        S->ev_used = 0;
+    }
     return r;
+}
+
+sf_status sf_set_profiling(sf_world *w, int32_t on) {
+    if (!w) return SF_ERR_ARG;
+    w->step->profile = on != 0;
+    w->step->ev_used = 0;
+    return SF_OK;
+}
+
+sf_status sf_read_profile(sf_world *w, sf_profile *out) {
+    if (!w || !out) return SF_ERR_ARG;
+    StepState *S = w->step;
+    std::memset(out, 0, sizeof *out);
+    for (int p = 0; p < SF_PHASES; p++) out->ms[p] = S->ph_ms[p];
+    out->substeps = S->ph_substeps;
+    out->solve_launches = S->solve_launches;
+    out->solve_contact_iters = S->solve_contact_iters;
+    uint64_t sum = 0;
+    for (uint32_t n : S->sub_nc) sum += n;
+    out->contacts_sum = sum;
+    out->launches = w->launches + S->wk.launches + sor_launches(w->sor);
+    return SF_OK;
+}
+
+sf_status sf_reset_profile(sf_world *w) {
+    if (!w) return SF_ERR_ARG;
+    StepState *S = w->step;
+    for (int p = 0; p < SF_PHASES; p++) S->ph_ms[p] = 0.0;
+    S->ph_substeps = 0; S->solve_launches = 0; S->solve_contact_iters = 0; S->sub_nc.clear(); S->ev_used = 0;
+    w->launches = 0; S->wk.launches = 0; sor_reset_launches(w->sor);
+    return SF_OK;
+}
+
+sf_status sf_world_set_stream(sf_world *w, void *stream) {
+    if (!w) return SF_ERR_ARG;
+    SF_CUDA(cudaStreamSynchronize(w->stream));
+    w->stream = stream ? (cudaStream_t)stream : w->own_stream;
+    return SF_OK;
 }
 
 sf_status sf_read_contacts(sf_world *w, uint32_t scene, uint32_t *ids5, float *f7, float *s8, uint64_t cap, uint64_t *n) {

@@ -112,6 +112,7 @@ cudaError_t exclusive_scan_u32(const uint32_t *in, uint32_t *out, size_t n, uint
     while (m > (size_t)SCAN_TILE) { m = (m + SCAN_TILE - 1) / SCAN_TILE; need += m; }
     cudaError_t e = wk.scan_a.grow(need + 16);
     if (e != cudaSuccess) return e;
+    for (size_t q = n; ; q = (q + SCAN_TILE - 1) / SCAN_TILE) { wk.launches += q > (size_t)SCAN_TILE ? 2 : 1; if (q <= (size_t)SCAN_TILE) break; }
     return scan_rec(in, out, n, d_total, wk.scan_a.p, s);
 }
 
@@ -186,6 +187,7 @@ cudaError_t radix_sort_u64(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt, u
         e = exclusive_scan_u32(wk.hist.p, wk.hist.p, (size_t)256 * nblocks, nullptr, wk, s);
         if (e != cudaSuccess) return e;
         k_rs_scatter<<<nblocks, RS_BLOCK, 0, s>>>(ki, vi, ko, vo, n, shift, wk.hist.p, nblocks);
+        wk.launches += 2;
         std::swap(ki, ko);
         std::swap(vi, vo);
     }

@@ -138,6 +138,29 @@ __global__ void k_setup_bodies(uint32_t nb, const uint32_t *first, const uint32_
     }
 }
 
+__global__ void k_pack_bodies(uint32_t nb, const float4 *pos, const float4 *q, const float4 *v, const float4 *w,
+                              const uint8_t *alive, const uint8_t *asleep, float *out13, uint8_t *flags) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    float4 p = pos[b], qq = q[b], vv = v[b], ww = w[b];
+    float *o = out13 + (size_t)b * 13;
+    o[0] = p.x; o[1] = p.y; o[2] = p.z; o[3] = qq.x; o[4] = qq.y; o[5] = qq.z; o[6] = qq.w;
+    o[7] = vv.x; o[8] = vv.y; o[9] = vv.z; o[10] = ww.x; o[11] = ww.y; o[12] = ww.z;
+    flags[b] = (alive[b] ? 1 : 0) | (asleep[b] ? 2 : 0);
+}
+__global__ void k_unpack_bodies(uint32_t nb, const float *in13, const uint8_t *flags, float4 *pos, float4 *q, float4 *v,
+                                float4 *w, uint8_t *alive, uint8_t *asleep) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const float *o = in13 + (size_t)b * 13;
+    pos[b] = make_float4(o[0], o[1], o[2], 0.0f);
+    q[b] = make_float4(o[3], o[4], o[5], o[6]);
+    v[b] = make_float4(o[7], o[8], o[9], 0.0f);
+    w[b] = make_float4(o[10], o[11], o[12], 0.0f);
+    alive[b] = flags[b] & 1;
+    asleep[b] = (flags[b] >> 1) & 1;
+}
+
 __global__ void k_kill_marked(uint32_t nb, const uint8_t *alive, const uint32_t *first, const uint32_t *count, uint8_t *kmat) {
     uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb || alive[b]) return;
@@ -185,13 +208,14 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
     *out = nullptr;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { set_error("no CUDA device"); return SF_ERR_CUDA; }
-    std::unique_ptr<sf_world> w(new sf_world());
+    std::unique_ptr<sf_world, void (*)(sf_world *)> w(new sf_world(), sf_world_destroy);
     if (params) w->P = *params; else sf_params_default(&w->P);
     if (w->P.substeps == 0) w->P.substeps = 2;
     if (w->P.max_colors == 0 || w->P.max_colors > (uint32_t)MAXCOL) w->P.max_colors = MAXCOL;
     SF_CUDA(cudaGetDevice(&w->device));
     SF_CUDA(cudaDeviceGetAttribute(&w->sms, cudaDevAttrMultiProcessorCount, w->device));
-    SF_CUDA(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
+    SF_CUDA(cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking));
+    w->stream = w->own_stream;
     SF_CUDA(cudaEventCreate(&w->ev0));
     SF_CUDA(cudaEventCreate(&w->ev1));
     SF_CUDA(upload_mat_tables(w->stream));
@@ -350,12 +374,12 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
 
 void sf_world_destroy(sf_world *w) {
     if (!w) return;
-    cudaStreamSynchronize(w->stream);
+    if (w->stream) cudaStreamSynchronize(w->stream);
     sor_destroy(w);
     step_destroy(w);
     if (w->ev0) cudaEventDestroy(w->ev0);
     if (w->ev1) cudaEventDestroy(w->ev1);
-    cudaStream_t s = w->stream;
+    cudaStream_t s = w->own_stream;
     delete w;
     if (s) cudaStreamDestroy(s);
 }
@@ -373,55 +397,39 @@ sf_status sf_get_stats(const sf_world *w, sf_stats *st) {
     return SF_OK;
 }
 
+// Body state crosses the boundary as 13 floats per body (the layout a host engine keeps); the device keeps float4
+// columns. One copy of the packed block each way, packed and unpacked on the device.
 sf_status sf_read_bodies(sf_world *w, float *state13, float *sleep, uint8_t *flags) {
     if (!w) return SF_ERR_ARG;
     uint32_t nb = w->nb;
-    std::vector<float4> p(nb), q(nb), v(nb), om(nb);
+    if (nb == 0) return SF_OK;
     cudaStream_t s = w->stream;
-    SF_CUDA(cudaMemcpyAsync(p.data(), w->b_pos.p, nb * sizeof(float4), cudaMemcpyDeviceToHost, s));
-    SF_CUDA(cudaMemcpyAsync(q.data(), w->b_q.p, nb * sizeof(float4), cudaMemcpyDeviceToHost, s));
-    SF_CUDA(cudaMemcpyAsync(v.data(), w->b_v.p, nb * sizeof(float4), cudaMemcpyDeviceToHost, s));
-    SF_CUDA(cudaMemcpyAsync(om.data(), w->b_w.p, nb * sizeof(float4), cudaMemcpyDeviceToHost, s));
-    std::vector<uint8_t> al(nb), as(nb);
+    SF_CUDA(w->stage13.grow((size_t)nb * 13));
+    SF_CUDA(w->stage_flags.grow(nb));
+    k_pack_bodies<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_pos.p, w->b_q.p, w->b_v.p, w->b_w.p, w->b_alive.p,
+                                                    w->b_asleep.p, w->stage13.p, w->stage_flags.p);
+    w->launches++;
+    if (state13) SF_CUDA(cudaMemcpyAsync(state13, w->stage13.p, (size_t)nb * 13 * sizeof(float), cudaMemcpyDeviceToHost, s));
     if (sleep) SF_CUDA(cudaMemcpyAsync(sleep, w->b_sleep.p, nb * sizeof(float), cudaMemcpyDeviceToHost, s));
-    SF_CUDA(cudaMemcpyAsync(al.data(), w->b_alive.p, nb, cudaMemcpyDeviceToHost, s));
-    SF_CUDA(cudaMemcpyAsync(as.data(), w->b_asleep.p, nb, cudaMemcpyDeviceToHost, s));
+    if (flags) SF_CUDA(cudaMemcpyAsync(flags, w->stage_flags.p, nb, cudaMemcpyDeviceToHost, s));
     SF_CUDA(cudaStreamSynchronize(s));
-    for (uint32_t b = 0; b < nb; b++) {
-        if (state13) {
-            float *o = state13 + (size_t)b * 13;
-            o[0] = p[b].x; o[1] = p[b].y; o[2] = p[b].z;
-            o[3] = q[b].x; o[4] = q[b].y; o[5] = q[b].z; o[6] = q[b].w;
-            o[7] = v[b].x; o[8] = v[b].y; o[9] = v[b].z;
-            o[10] = om[b].x; o[11] = om[b].y; o[12] = om[b].z;
-        }
-        if (flags) flags[b] = (al[b] ? 1 : 0) | (as[b] ? 2 : 0);
-    }
     return SF_OK;
 }
 
 sf_status sf_write_bodies(sf_world *w, const float *state13, const float *sleep, const uint8_t *flags) {
     if (!w || !state13 || !sleep || !flags) return SF_ERR_ARG;
     uint32_t nb = w->nb;
-    std::vector<float4> p(nb), q(nb), v(nb), om(nb);
-    std::vector<uint8_t> al(nb), as(nb);
-    for (uint32_t b = 0; b < nb; b++) {
-        const float *o = state13 + (size_t)b * 13;
-        p[b] = make_float4(o[0], o[1], o[2], 0.0f);
-        q[b] = make_float4(o[3], o[4], o[5], o[6]);
-        v[b] = make_float4(o[7], o[8], o[9], 0.0f);
-        om[b] = make_float4(o[10], o[11], o[12], 0.0f);
-        al[b] = flags[b] & 1; as[b] = (flags[b] >> 1) & 1;
-    }
+    if (nb == 0) return SF_OK;
     cudaStream_t s = w->stream;
-    SF_CUDA(cudaMemcpyAsync(w->b_pos.p, p.data(), nb * sizeof(float4), cudaMemcpyHostToDevice, s));
-    SF_CUDA(cudaMemcpyAsync(w->b_q.p, q.data(), nb * sizeof(float4), cudaMemcpyHostToDevice, s));
-    SF_CUDA(cudaMemcpyAsync(w->b_v.p, v.data(), nb * sizeof(float4), cudaMemcpyHostToDevice, s));
-    SF_CUDA(cudaMemcpyAsync(w->b_w.p, om.data(), nb * sizeof(float4), cudaMemcpyHostToDevice, s));
+    SF_CUDA(w->stage13.grow((size_t)nb * 13));
+    SF_CUDA(w->stage_flags.grow(nb));
+    SF_CUDA(cudaMemcpyAsync(w->stage13.p, state13, (size_t)nb * 13 * sizeof(float), cudaMemcpyHostToDevice, s));
     SF_CUDA(cudaMemcpyAsync(w->b_sleep.p, sleep, nb * sizeof(float), cudaMemcpyHostToDevice, s));
-    SF_CUDA(cudaMemcpyAsync(w->b_alive.p, al.data(), nb, cudaMemcpyHostToDevice, s));
-    SF_CUDA(cudaMemcpyAsync(w->b_asleep.p, as.data(), nb, cudaMemcpyHostToDevice, s));
-    if (nb) k_kill_marked<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, w->b_first.p, w->b_count.p, w->k_mat.p);
+    SF_CUDA(cudaMemcpyAsync(w->stage_flags.p, flags, nb, cudaMemcpyHostToDevice, s));
+    k_unpack_bodies<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->stage13.p, w->stage_flags.p, w->b_pos.p, w->b_q.p, w->b_v.p,
+                                                      w->b_w.p, w->b_alive.p, w->b_asleep.p);
+    k_kill_marked<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, w->b_first.p, w->b_count.p, w->k_mat.p);
+    w->launches += 2;
     SF_CUDA(cudaGetLastError());
     SF_CUDA(cudaStreamSynchronize(s));
     return SF_OK;

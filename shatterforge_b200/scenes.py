@@ -219,6 +219,27 @@ class ClusterLibrary:
         lst = self.cache[k]
         return lst[pick % len(lst)]
 
+    def gather(self, ks: np.ndarray, picks: np.ndarray):
+        """Vectorised get() for many bodies: (concatenated cells, per-body extent in cells)."""
+        for k in sorted(set(int(k) for k in np.unique(ks))):
+            self.get(k, 0)
+        keys = sorted(self.cache)
+        flat, off, ext, vstart, vcount = [], [0], [], np.zeros(self.kmax + 2, np.int64), np.zeros(self.kmax + 2, np.int64)
+        for k in keys:
+            vstart[k] = len(ext)
+            vcount[k] = len(self.cache[k])
+            for c in self.cache[k]:
+                flat.append(c)
+                off.append(off[-1] + len(c))
+                ext.append(float(np.abs(c).max()))
+        flat = np.concatenate(flat, 0)
+        off = np.array(off[:-1], np.int64)
+        ext = np.array(ext)
+        lid = vstart[ks] + picks % vcount[ks]
+        first = np.concatenate([[0], np.cumsum(ks)])
+        idx = np.repeat(off[lid] - first[:-1], ks) + np.arange(first[-1])
+        return flat[idx], ext[lid]
+
 
 def debris_scene(n_bodies: int, seed: int, lib: ClusterLibrary | None = None, p_geom: float = 0.3, kmax: int = 256,
                  obstacles: tuple[int, int] = (4, 16), spacing: float = 2.5, v_sigma: float = 3.0,
@@ -230,10 +251,9 @@ def debris_scene(n_bodies: int, seed: int, lib: ClusterLibrary | None = None, p_
     lib = lib or ClusterLibrary(seed ^ 0x5F3759DF)
     ks = np.minimum(rng.geometric(p_geom, n_bodies), kmax).astype(np.int64)
     picks = rng.integers(0, 1 << 30, n_bodies)
-    clusters = [lib.get(int(k), int(p)) for k, p in zip(ks, picks)]
+    cl, ext_cells = lib.gather(ks, picks)
     first = np.zeros(n_bodies + 1, np.uint32)
     first[1:] = np.cumsum(ks)
-    cl = np.concatenate(clusters, 0)
     # spread bricks of a body over lattice cells about the origin cell
     bxyz = (cl + np.array(ORIGIN, np.int32)).astype(np.int32)
     bmat = np.array(mats, np.uint8)[rng.integers(0, len(mats), n_bodies)]
@@ -248,7 +268,7 @@ def debris_scene(n_bodies: int, seed: int, lib: ClusterLibrary | None = None, p_
     sy = slot // (side * side)
     jitter = rng.uniform(-0.25, 0.25, (n_bodies, 3))
     # big bodies take more room: shift by their extent in the layer above
-    ext = np.array([float(np.abs(c).max()) * 0.5 + 0.5 for c in clusters])
+    ext = ext_cells * 0.5 + 0.5
     half = (side - 1) * spacing * 0.5
     px = sx * spacing - half + jitter[:, 0]
     pz = sz * spacing - half + jitter[:, 2]
