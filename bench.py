@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--no-sor", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
 
@@ -163,31 +163,32 @@ def allreduce_sum(pg, x: float) -> float:
 
 
 # ---------------------------------------------------------------- CPU restatement (oracle) timing
-def cpu_body_steps(scenes, states, seconds: float, threads: int):
-    """Steps the oracle on the given scenes from the given states, one scene per thread, for about `seconds`."""
+def cpu_body_steps(scenes, warmup: int, steps: int, budget_s: float, threads: int):
+    """The oracle (CPU restatement) steps each scene from rest: `warmup` untimed steps, then up to `steps` timed
+    steps or until `budget_s`, one scene per thread. Returns (body-steps/s, timed steps in all)."""
     from oracle import binding as orc
     results = []
     lock = threading.Lock()
 
-    def work(sc, st):
+    def work(sc):
         ow = orc.OracleWorld(sc)
-        if st is not None:
-            ow.set_bodies(*st)
+        for _ in range(warmup):
+            ow.step(DT, iterations=ITERS, order=orc.ORDER_COLOR, pinch_kill=0)
         _, _, fl = ow.bodies()
         alive = int((fl & 1).sum())
         t0 = time.perf_counter()
         n = 0
-        while time.perf_counter() - t0 < seconds:
+        while n < steps and time.perf_counter() - t0 < budget_s:
             ow.step(DT, iterations=ITERS, order=orc.ORDER_COLOR, pinch_kill=0)
             n += 1
         el = time.perf_counter() - t0
         _, _, fl = ow.bodies()
-        # bodies only leave by falling out of the world (pinch removal is off): count the mean of start and end
-        bsteps = n * (alive + int((fl & 1).sum())) // 2
+        # bodies only leave by falling out of the world (pinch removal is off): the mean of start and end counts
+        bsteps = n * (alive + int((fl & 1).sum())) / 2.0
         with lock:
             results.append((bsteps, el, n))
 
-    ths = [threading.Thread(target=work, args=(sc, st)) for sc, st in zip(scenes, states)]
+    ths = [threading.Thread(target=work, args=(sc,)) for sc in scenes]
     for i in range(0, len(ths), threads):
         batch = ths[i:i + threads]
         for t in batch:
@@ -197,6 +198,14 @@ def cpu_body_steps(scenes, states, seconds: float, threads: int):
     bsteps = sum(r[0] for r in results)
     el = max(r[1] for r in results) if results else 1.0
     return bsteps / el, sum(r[2] for r in results)
+
+
+def cpu_sample(scenes, k: int):
+    """k scenes spread over the lower half of the size range (a bounded sample of the mix)."""
+    order = np.argsort([s.n_bodies for s in scenes])
+    half = order[: max(1, len(order) // 2)]
+    pick = half[np.linspace(0, len(half) - 1, min(k, len(half))).astype(int)]
+    return [scenes[i] for i in pick]
 
 
 def host_threads() -> int:
@@ -213,20 +222,19 @@ def reference_arm(args, rank, world, pg):
     from shatterforge_b200 import scenes as S
     scenes = S.config4_scenes(n_scenes=args.scenes, scale=args.scale)
     threads = host_threads()
-    # bounded sample: `threads` scenes spread over the size range, each stepped for the time budget from rest
-    order = np.argsort([s.n_bodies for s in scenes])
-    pick = order[np.linspace(0, len(order) - 1, min(threads, len(order))).astype(int)]
-    sample = [scenes[i] for i in pick]
+    sample = cpu_sample(scenes, threads)
     per = max(1.0, args.cpu_seconds)
-    rate, steps = cpu_body_steps(sample, [None] * len(sample), per, threads)
+    rate, steps = cpu_body_steps(sample, args.warmup, args.steps, per, threads)
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": 0, "steps": int(steps),
         "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded)",
         "config": {"workload": f"config4: {args.scenes} debris scenes, 1/60 s, {ITERS} iterations, 2 substeps",
-                   "sample": f"{len(sample)} scenes ({sum(s.n_bodies for s in sample)} bodies) stepped {per:.0f} s each from rest"},
+                   "sample": f"{len(sample)} scenes ({sum(s.n_bodies for s in sample)} bodies), steps {args.warmup}.."
+                             f"{args.warmup + args.steps} from rest, at most {per:.0f} s each"},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{len(sample)} of {args.scenes} scenes, one per thread, {per:.0f} s each"},
+                         "sample": f"{len(sample)} of {args.scenes} scenes (lower half of the sizes), one per thread, "
+                                   f"{steps} timed steps in all"},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -296,7 +304,6 @@ def our_arm(args, rank, world, local, pg):
                 "bytes_per_launch": solve_bytes / max(prof["solve_launches"], 1), "ms_per_launch": per_launch_ms,
                 "unit_bytes": f"{SOLVE_BYTES_PER_CONTACT_ITER} B per contact-iteration"}
     state_after = w.bodies()
-    sample_states = None
 
     # ---- plain path on the same simulated state: each scene alone, one launch sequence per scene
     plain = None
@@ -387,23 +394,18 @@ def our_arm(args, rank, world, local, pg):
                             "unit_bytes": f"{SOR_BYTES_PER_BRICK_SWEEP} B per brick-sweep"}}
         ws.close()
 
-    # ---- CPU baseline: the oracle on a bounded sample of the same workload, from the GPU's state
+    # ---- CPU baseline: the oracle on a bounded sample of the same workload and step window
     cpu = None
-    if not args.no_cpu and rank == 0 and world == 1:
-        st, sl, fl = state_after
-        order = np.argsort([s.n_bodies for s in scenes])
-        pick = order[np.linspace(0, len(order) - 1, 4).astype(int)]
-        samp = [scenes[i] for i in pick]
-        body_off = np.cumsum([0] + [s.n_bodies for s in scenes])
-        states = [(st[body_off[i]:body_off[i + 1]], sl[body_off[i]:body_off[i + 1]], fl[body_off[i]:body_off[i + 1]])
-                  for i in pick]
-        rate1, n1 = cpu_body_steps(samp[:1], states[:1], args.cpu_seconds / 2, 1)
+    if not args.no_cpu and rank == 0:
+        one = cpu_sample(scenes, 1)
+        rate1, n1 = cpu_body_steps(one, args.warmup, args.steps, args.cpu_seconds, 1)
         threads = host_threads()
-        rate_n, n_n = cpu_body_steps(samp, states, args.cpu_seconds / 2, threads)
+        many = cpu_sample(scenes, threads)
+        rate_n, n_n = cpu_body_steps(many, args.warmup, args.steps, args.cpu_seconds, threads)
         cpu = {"value": rate1, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"1 scene ({samp[0].n_bodies} bodies) from the GPU state after the timed run, {n1} steps",
-               "all_cores": {"value": rate_n, "cores": min(threads, len(samp)),
-                             "sample": f"{len(samp)} scenes, one per thread, {n_n} steps in all"}}
+               "sample": f"1 scene ({one[0].n_bodies} bodies), steps {args.warmup}..{args.warmup + n1} from rest",
+               "all_cores": {"value": rate_n, "cores": min(threads, len(many)),
+                             "sample": f"{len(many)} scenes of the lower half of the sizes, one per thread, {n_n} timed steps in all"}}
 
     if rank != 0:
         return

@@ -56,6 +56,7 @@ def load() -> C.CDLL:
     lib.ow_set_bodies.argtypes = [C.c_void_p, _f32p, _f32p, _u8p]
     lib.ow_get_setup.argtypes = [C.c_void_p, _f32p, _f32p]
     lib.ow_get_wpos.argtypes = [C.c_void_p, _f32p]
+    lib.ow_set_wpos.argtypes = [C.c_void_p, _f32p]
     lib.ow_get_bonds.argtypes = [C.c_void_p, _f32p, _u32p]
     lib.ow_step.argtypes = [C.c_void_p, C.c_float, C.POINTER(StepParams)]
     lib.ow_contacts_only.argtypes = [C.c_void_p, C.c_float, C.c_int]
@@ -133,6 +134,10 @@ class OracleWorld:
         p = np.zeros((self.nd, 3), np.float32)
         self.lib.ow_get_wpos(self.h, _p(p, C.c_float))
         return p
+
+    def set_brick_positions(self, wpos):
+        p = np.ascontiguousarray(wpos, np.float32)
+        self.lib.ow_set_wpos(self.h, _p(p, C.c_float))
 
     def bonds(self):
         b = np.zeros((self.ns, 4), np.float32)

@@ -1021,6 +1021,11 @@ void ow_get_wpos(void* h, float* wpos3) {
     World* w = (World*)h;
     for (uint32_t k = 0; k < w->nd; k++) for (int c = 0; c < 3; c++) wpos3[(size_t)k * 3 + c] = w->wpos[w->ns + k][c];
 }
+// brick world positions are part of the state: a sleeping body keeps the positions of its last awake substep
+void ow_set_wpos(void* h, const float* wpos3) {
+    World* w = (World*)h;
+    for (uint32_t k = 0; k < w->nd; k++) for (int c = 0; c < 3; c++) w->wpos[w->ns + k][c] = wpos3[(size_t)k * 3 + c];
+}
 void ow_get_bonds(void* h, float* bond4, uint32_t* nb6) {
     World* w = (World*)h;
     for (uint32_t i = 0; i < w->ns; i++) {

@@ -35,7 +35,11 @@ struct StepState {
     // hashed cell sort
     DBuf<uint64_t> ckey, ckey_alt;
     DBuf<uint32_t> cval, cval_alt;
-    DBuf<uint32_t> bstart, bend;
+    DBuf<uint2> brange;
+    DBuf<float4> srec;
+    DBuf<uint32_t> sinfo;
+    DBuf<uint4> slot_id;
+    DBuf<float4> slot_p, slot_n;
     // contacts, list order
     DBuf<uint32_t> ccount, coff;
     DBuf<uint32_t> L_a, L_b, L_bo, L_ba, L_bb;
@@ -136,50 +140,55 @@ __global__ void k_cell_keys(uint32_t nd, uint64_t none_key, const uint32_t *kbod
     val[i] = i;
 }
 
-__global__ void k_bucket_ranges(uint32_t nd, uint64_t none_key, const uint64_t *key, uint32_t *bstart, uint32_t *bend) {
+__global__ void k_bucket_ranges(uint32_t nd, uint64_t none_key, const uint64_t *key, uint2 *brange) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nd) return;
     uint64_t k = key[p];
     if (k >= none_key) return;
-    if (p == 0 || key[p - 1] != k) bstart[k] = p;
-    if (p == nd - 1 || key[p + 1] != k) bend[k] = p + 1;
+    if (p == 0 || key[p - 1] != k) brange[k].x = p;
+    if (p == nd - 1 || key[p + 1] != k) brange[k].y = p + 1;
+}
+
+// Packed bucket entries in sorted order: world position and brick id, then body id with the asleep bit (31) and the
+// removed-brick bit (30), so a bucket walk reads two contiguous arrays.
+__global__ void k_bucket_records(uint32_t nd, const uint32_t *cval, const uint32_t *kbody, const uint8_t *kmat,
+                                 const uint8_t *asleep, const float4 *wpos, float4 *srec, uint32_t *sinfo) {
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nd) return;
+    uint32_t j = cval[q];
+    uint32_t bj = kbody[j];
+    float4 p = wpos[j];
+    srec[q] = make_float4(p.x, p.y, p.z, __uint_as_float(j));
+    sinfo[q] = bj | (asleep[bj] ? 0x80000000u : 0u) | (kmat[j] == 0 ? 0x40000000u : 0u);
 }
 
 // ---------------------------------------------------------------- contacts
 struct ContactArgs {
     uint32_t nd;
     const uint32_t *kbody, *bscene, *ctab, *cpool;
-    const uint8_t *alive, *asleep, *kmat, *smat;
+    const uint8_t *alive, *asleep, *smat;
     const float4 *wpos, *v, *w;
     const float *rot, *rad;
-    const uint32_t *bstart, *bend, *cval;
+    const uint2 *brange;
+    const float4 *srec;
+    const uint32_t *sinfo;
     uint32_t *ccount;
     const uint32_t *coff;
     uint8_t *wake;
+    // slot scratch, slot-major: slot k of brick i at k * nd + i
+    uint4 *slot_id;
+    float4 *slot_p, *slot_n;
     uint32_t *L_a, *L_b, *L_bo, *L_ba, *L_bb;
     float4 *L_p, *L_n;
 };
+constexpr int CSLOTS = 12;
 
-template <bool FILL>
-__global__ void __launch_bounds__(128) k_contacts(ContactArgs A) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.nd) return;
-    uint32_t a = A.kbody[i];
-    if (!A.alive[a] || A.asleep[a]) { if (!FILL) A.ccount[i] = 0; return; }
+// gen_contacts for one brick of an awake body (src/lib.rs:1410-1468), contacts emitted in the reference's order.
+template <bool WAKE, class Emit>
+__device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint32_t a, Emit &&emit) {
     const uint32_t sc = A.bscene[a];
-    uint32_t n = 0;
-    const uint32_t base = FILL ? A.coff[i] : 0;
-    float4 p4 = A.wpos[i];
+    const float4 p4 = A.wpos[i];
     const V3 p = v3(p4.x, p4.y, p4.z);
-    auto emit = [&](uint32_t b, uint32_t bo, uint32_t bb, V3 cp, V3 nn, float depth) {
-        if (FILL) {
-            uint32_t o = base + n;
-            A.L_a[o] = a; A.L_b[o] = b; A.L_bo[o] = bo; A.L_ba[o] = i; A.L_bb[o] = bb;
-            A.L_p[o] = make_float4(cp.x, cp.y, cp.z, 0.0f);
-            A.L_n[o] = make_float4(nn.x, nn.y, nn.z, depth);
-        }
-        n++;
-    };
     // ground: the brick's 8 cube corners below y = 0 (src/lib.rs:1415-1421)
     if (p.y < 0.5f) {
         float r[9];
@@ -191,60 +200,75 @@ __global__ void __launch_bounds__(128) k_contacts(ContactArgs A) {
             if (cp.y < 0.0f) emit(STATIC, STATIC, NONE, cp, v3(0.0f, 1.0f, 0.0f), -cp.y);
         }
     }
-    // static cells of the 3^3 block (src/lib.rs:1422-1440)
+    // static cells of the 3^3 block (src/lib.rs:1422-1440): the block spans at most 2 x 2 x 2 chunks, read once
     {
         const int cx = floor_cell(p.x) + NX / 2, cy = floor_cell(p.y), cz = floor_cell(p.z) + NZ / 2;
-        for (int dz = -1; dz <= 1; dz++)
-            for (int dy = -1; dy <= 1; dy++)
-                for (int dx = -1; dx <= 1; dx++) {
-                    const int x = cx + dx, y = cy + dy, z = cz + dz;
-                    if (!inb(x, y, z)) continue;
-                    const uint32_t t = A.ctab[(size_t)sc * NCT + chunk_slot(x, y, z)];
-                    if (t == 0) continue;
-                    const uint32_t g = A.cpool[(size_t)(t - 1) * 512 + cell_in_chunk(x, y, z)];
-                    if (g == 0) continue;
-                    const uint32_t j = g - 1;
-                    if (A.smat[j] == 0) continue;
-                    const V3 c = lat_pos(x, y, z);
-                    const V3 qq = v3(clampf(p.x, c.x - H, c.x + H), clampf(p.y, c.y - H, c.y + H), clampf(p.z, c.z - H, c.z + H));
-                    const V3 d = sub(p, qq);
-                    const float dist = len(d);
-                    if (dist >= RB) continue;
-                    if (dist > 1e-4f) {
-                        emit(STATIC, STATIC, j, qq, mul(d, div_rn(1.0f, dist)), RB - dist);
-                    } else {
-                        const V3 r = sub(p, c);
-                        const float ar[3] = {r.x, r.y, r.z};
-                        int ax = 0;
-                        for (int k = 1; k < 3; k++) if (fabsf(ar[k]) > fabsf(ar[ax])) ax = k;
-                        float nv[3] = {0.0f, 0.0f, 0.0f};
-                        nv[ax] = ar[ax] >= 0.0f ? 1.0f : -1.0f;
-                        emit(STATIC, STATIC, j, p, v3(nv[0], nv[1], nv[2]), H + RB - fabsf(ar[ax]));
+        const int ox = (cx - 1) >> 3, oy = (cy - 1) >> 3, oz = (cz - 1) >> 3;
+        uint32_t ch[8];
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int qx = ((ox + (k & 1)) << 3), qy = ((oy + ((k >> 1) & 1)) << 3), qz = ((oz + (k >> 2)) << 3);
+            uint32_t t = 0;
+            if (inb(qx, qy, qz)) t = A.ctab[(size_t)sc * NCT + chunk_slot(qx, qy, qz)];
+            ch[k] = t;
+            any |= t != 0;
+        }
+        if (any) {
+            for (int dz = -1; dz <= 1; dz++)
+                for (int dy = -1; dy <= 1; dy++)
+                    for (int dx = -1; dx <= 1; dx++) {
+                        const int x = cx + dx, y = cy + dy, z = cz + dz;
+                        if (!inb(x, y, z)) continue;
+                        const int k = ((x >> 3) - ox) | (((y >> 3) - oy) << 1) | (((z >> 3) - oz) << 2);
+                        const uint32_t t = ch[k];
+                        if (t == 0) continue;
+                        const uint32_t g = A.cpool[(size_t)(t - 1) * 512 + cell_in_chunk(x, y, z)];
+                        if (g == 0) continue;
+                        const uint32_t j = g - 1;
+                        if (A.smat[j] == 0) continue;
+                        const V3 c = lat_pos(x, y, z);
+                        const V3 qq = v3(clampf(p.x, c.x - H, c.x + H), clampf(p.y, c.y - H, c.y + H), clampf(p.z, c.z - H, c.z + H));
+                        const V3 d = sub(p, qq);
+                        const float dist = len(d);
+                        if (dist >= RB) continue;
+                        if (dist > 1e-4f) {
+                            emit(STATIC, STATIC, j, qq, mul(d, div_rn(1.0f, dist)), RB - dist);
+                        } else {
+                            const V3 r = sub(p, c);
+                            const float ar[3] = {r.x, r.y, r.z};
+                            int ax = 0;
+                            for (int q = 1; q < 3; q++) if (fabsf(ar[q]) > fabsf(ar[ax])) ax = q;
+                            float nv[3] = {0.0f, 0.0f, 0.0f};
+                            nv[ax] = ar[ax] >= 0.0f ? 1.0f : -1.0f;
+                            emit(STATIC, STATIC, j, p, v3(nv[0], nv[1], nv[2]), H + RB - fabsf(ar[ax]));
+                        }
                     }
-                }
+        }
     }
-    // hashed neighbours in the 27 buckets around the brick (src/lib.rs:1441-1466)
+    // hashed neighbours in the 27 buckets around the brick (src/lib.rs:1441-1466); a bucket walked from its highest
+    // brick id down is the reference's chain order
     {
         const int hx = floor_cell(p.x), hy = floor_cell(p.y), hz = floor_cell(p.z);
         float speed = 0.0f;
-        if (FILL) {
-            float4 vv = A.v[a], ww = A.w[a];
+        if (WAKE) {
+            const float4 vv = A.v[a], ww = A.w[a];
             speed = len(v3(vv.x, vv.y, vv.z)) + len(v3(ww.x, ww.y, ww.z)) * A.rad[a] * 0.5f;
         }
         const float lim2 = 4.0f * RB * RB;
         for (int dz = -1; dz <= 1; dz++)
             for (int dy = -1; dy <= 1; dy++)
                 for (int dx = -1; dx <= 1; dx++) {
-                    const size_t hb = (size_t)sc * HSIZE + hkey(hx + dx, hy + dy, hz + dz);
-                    const uint32_t s0 = A.bstart[hb], s1 = A.bend[hb];
-                    for (uint32_t q = s1; q > s0; q--) {
-                        const uint32_t j = A.cval[q - 1];
-                        const uint32_t bj = A.kbody[j];
-                        if (bj == a || A.kmat[j] == 0) continue;
-                        const bool other_awake = !A.asleep[bj];
+                    const uint2 rg = A.brange[(size_t)sc * HSIZE + hkey(hx + dx, hy + dy, hz + dz)];
+                    for (uint32_t q = rg.y; q > rg.x; q--) {
+                        const uint32_t info = A.sinfo[q - 1];
+                        const uint32_t bj = info & 0x3FFFFFFFu;
+                        if (bj == a || (info & 0x40000000u)) continue;
+                        const float4 rec = A.srec[q - 1];
+                        const uint32_t j = __float_as_uint(rec.w);
+                        const bool other_awake = !(info & 0x80000000u);
                         if (other_awake && j < i) continue;
-                        const float4 pj4 = A.wpos[j];
-                        const V3 pj = v3(pj4.x, pj4.y, pj4.z);
+                        const V3 pj = v3(rec.x, rec.y, rec.z);
                         const V3 d = sub(p, pj);
                         const float dd = dot(d, d);
                         if (dd >= lim2 || dd < 1e-10f) continue;
@@ -253,13 +277,65 @@ __global__ void __launch_bounds__(128) k_contacts(ContactArgs A) {
                         const V3 cp = madd(pj, nn, dist * 0.5f);
                         if (other_awake) emit(bj, bj, j, cp, nn, 2.0f * RB - dist);
                         else {
-                            if (FILL && speed > 0.7f) A.wake[bj] = 1;
+                            if (WAKE && speed > 0.7f) A.wake[bj] = 1;
                             emit(STATIC, bj, j, cp, nn, 2.0f * RB - dist);
                         }
                     }
                 }
     }
-    if (!FILL) A.ccount[i] = n;
+}
+
+// pass 1: every contact of every awake brick counted; the first CSLOTS kept in the brick's slots
+__global__ void __launch_bounds__(128) k_contacts_gen(ContactArgs A) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.nd) return;
+    const uint32_t a = A.kbody[i];
+    if (!A.alive[a] || A.asleep[a]) { A.ccount[i] = 0; return; }
+    uint32_t n = 0;
+    const size_t nd = A.nd;
+    auto emit = [&](uint32_t b, uint32_t bo, uint32_t bb, V3 cp, V3 nn, float depth) {
+        if (n < CSLOTS) {
+            const size_t o = (size_t)n * nd + i;
+            A.slot_id[o] = make_uint4(b, bo, bb, 0u);
+            A.slot_p[o] = make_float4(cp.x, cp.y, cp.z, depth);
+            A.slot_n[o] = make_float4(nn.x, nn.y, nn.z, 0.0f);
+        }
+        n++;
+    };
+    gen_brick<true>(A, i, a, emit);
+    A.ccount[i] = n;
+}
+
+// pass 2: each brick's contacts to their place in the list; a brick with more than CSLOTS regenerates them
+__global__ void __launch_bounds__(128) k_contacts_place(ContactArgs A) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.nd) return;
+    const uint32_t n = A.ccount[i];
+    if (n == 0) return;
+    const uint32_t a = A.kbody[i];
+    const uint32_t base = A.coff[i];
+    const size_t nd = A.nd;
+    if (n <= CSLOTS) {
+        for (uint32_t k = 0; k < n; k++) {
+            const size_t o = (size_t)k * nd + i;
+            const uint4 id = A.slot_id[o];
+            const float4 pp = A.slot_p[o], nn = A.slot_n[o];
+            const uint32_t t = base + k;
+            A.L_a[t] = a; A.L_b[t] = id.x; A.L_bo[t] = id.y; A.L_ba[t] = i; A.L_bb[t] = id.z;
+            A.L_p[t] = make_float4(pp.x, pp.y, pp.z, 0.0f);
+            A.L_n[t] = make_float4(nn.x, nn.y, nn.z, pp.w);
+        }
+        return;
+    }
+    uint32_t k = 0;
+    auto emit = [&](uint32_t b, uint32_t bo, uint32_t bb, V3 cp, V3 nn, float depth) {
+        const uint32_t t = base + k;
+        A.L_a[t] = a; A.L_b[t] = b; A.L_bo[t] = bo; A.L_ba[t] = i; A.L_bb[t] = bb;
+        A.L_p[t] = make_float4(cp.x, cp.y, cp.z, 0.0f);
+        A.L_n[t] = make_float4(nn.x, nn.y, nn.z, depth);
+        k++;
+    };
+    gen_brick<false>(A, i, a, emit);
 }
 
 __global__ void k_body_nc(uint32_t nc, const uint32_t *L_a, const uint32_t *L_b, uint32_t *bnc) {
@@ -783,7 +859,9 @@ sf_status step_create(sf_world *w) {
     uint32_t nb = w->nb, nd = w->nd;
     cudaStream_t s = w->stream;
     SF_CUDA(S->ckey.alloc(nd)); SF_CUDA(S->ckey_alt.alloc(nd)); SF_CUDA(S->cval.alloc(nd)); SF_CUDA(S->cval_alt.alloc(nd));
-    SF_CUDA(S->bstart.alloc((size_t)w->n_scenes * HSIZE)); SF_CUDA(S->bend.alloc((size_t)w->n_scenes * HSIZE));
+    SF_CUDA(S->brange.alloc((size_t)w->n_scenes * HSIZE));
+    SF_CUDA(S->srec.alloc(nd)); SF_CUDA(S->sinfo.alloc(nd));
+    SF_CUDA(S->slot_id.alloc((size_t)nd * CSLOTS)); SF_CUDA(S->slot_p.alloc((size_t)nd * CSLOTS)); SF_CUDA(S->slot_n.alloc((size_t)nd * CSLOTS));
     SF_CUDA(S->ccount.alloc((size_t)nd + 1)); SF_CUDA(S->coff.alloc((size_t)nd + 1));
     SF_CUDA(S->bm_count.alloc((size_t)nb + 1)); SF_CUDA(S->bm_start.alloc((size_t)nb + 1)); SF_CUDA(S->bm_fill.alloc((size_t)nb + 1));
     SF_CUDA(S->masks.alloc((size_t)nb * 4 + 4)); SF_CUDA(S->vmasks.alloc((size_t)nb * 4 + 4));
@@ -831,19 +909,21 @@ static sf_status substep(sf_world *w, float h) {
     k_cell_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, w->k_body.p, w->b_scene.p, w->b_alive.p, w->k_wpos.p,
                                                   S->ckey.p, S->cval.p);
     SF_CUDA(radix_sort_u64(S->ckey.p, S->cval.p, S->ckey_alt.p, S->cval_alt.p, nd, bits_for(none_key), S->wk, s));
-    SF_CUDA(cudaMemsetAsync(S->bstart.p, 0, S->bstart.bytes(), s));
-    SF_CUDA(cudaMemsetAsync(S->bend.p, 0, S->bend.bytes(), s));
-    k_bucket_ranges<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, S->ckey.p, S->bstart.p, S->bend.p);
-    L += 2;
+    SF_CUDA(cudaMemsetAsync(S->brange.p, 0, S->brange.bytes(), s));
+    k_bucket_ranges<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, S->ckey.p, S->brange.p);
+    k_bucket_records<<<grid_for(nd, 256), 256, 0, s>>>(nd, S->cval.p, w->k_body.p, w->k_mat.p, w->b_asleep.p, w->k_wpos.p,
+                                                       S->srec.p, S->sinfo.p);
+    L += 3;
     prof_mark(w);
-    // contacts: count, scan, fill
+    // contacts: generate into slots and count, scan, place in list order
     ContactArgs C;
     C.nd = nd; C.kbody = w->k_body.p; C.bscene = w->b_scene.p; C.ctab = w->ctab.p; C.cpool = w->cpool.p;
-    C.alive = w->b_alive.p; C.asleep = w->b_asleep.p; C.kmat = w->k_mat.p; C.smat = w->s_mat.p; C.wpos = w->k_wpos.p;
-    C.v = w->b_v.p; C.w = w->b_w.p; C.rot = w->b_rot.p; C.rad = w->b_rad.p; C.bstart = S->bstart.p; C.bend = S->bend.p;
-    C.cval = S->cval.p; C.ccount = S->ccount.p; C.coff = S->coff.p; C.wake = w->b_wake.p;
+    C.alive = w->b_alive.p; C.asleep = w->b_asleep.p; C.smat = w->s_mat.p; C.wpos = w->k_wpos.p;
+    C.v = w->b_v.p; C.w = w->b_w.p; C.rot = w->b_rot.p; C.rad = w->b_rad.p; C.brange = S->brange.p; C.srec = S->srec.p;
+    C.sinfo = S->sinfo.p; C.ccount = S->ccount.p; C.coff = S->coff.p; C.wake = w->b_wake.p;
+    C.slot_id = S->slot_id.p; C.slot_p = S->slot_p.p; C.slot_n = S->slot_n.p;
     C.L_a = S->L_a.p; C.L_b = S->L_b.p; C.L_bo = S->L_bo.p; C.L_ba = S->L_ba.p; C.L_bb = S->L_bb.p; C.L_p = S->L_p.p; C.L_n = S->L_n.p;
-    k_contacts<false><<<grid_for(nd, 128), 128, 0, s>>>(C);
+    k_contacts_gen<<<grid_for(nd, 128), 128, 0, s>>>(C);
     SF_CUDA(exclusive_scan_u32(S->ccount.p, S->coff.p, nd, S->dev.p + DV_CONTACTS, S->wk, s));
     SF_CUDA(cudaMemcpyAsync(S->h_dev, S->dev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     SF_CUDA(cudaStreamSynchronize(s));
@@ -854,7 +934,7 @@ static sf_status substep(sf_world *w, float h) {
         SF_CUDA(grow_contacts(S, nc));
         C.L_a = S->L_a.p; C.L_b = S->L_b.p; C.L_bo = S->L_bo.p; C.L_ba = S->L_ba.p; C.L_bb = S->L_bb.p; C.L_p = S->L_p.p; C.L_n = S->L_n.p;
     }
-    k_contacts<true><<<grid_for(nd, 128), 128, 0, s>>>(C);
+    k_contacts_place<<<grid_for(nd, 128), 128, 0, s>>>(C);
     SF_CUDA(cudaMemsetAsync(w->b_nc.p, 0, w->b_nc.bytes(), s));
     SF_CUDA(cudaMemsetAsync(S->dev.p + DV_MANIFOLDS, 0, (DV_N - DV_MANIFOLDS) * sizeof(uint32_t), s));
     const uint32_t g_nc = grid_for(std::max<uint32_t>(nc, 1), 256);

@@ -165,6 +165,7 @@ def test_step_from_gpu_state(sf, oracle):
     st, sl, fl = w.bodies()
     ow = oracle.OracleWorld(sc)
     ow.set_bodies(st, sl, fl)
+    ow.set_brick_positions(w.brick_positions())
     w.step(1 / 60)
     ow.step(1 / 60, iterations=8, order=oracle.ORDER_COLOR)
     _compare_step_outputs(w, ow)
