@@ -181,6 +181,24 @@ sf_status sf_read_bonds(sf_world *w, float *bond4, uint32_t *nb6, uint8_t *mat);
  * decision (0 hold, 1 fatigue, 2 fail, 3 crush, 255 absent) with the crushed brick id for crushes */
 sf_status sf_read_joints(sf_world *w, float *ratio4, float *bond4, uint8_t *decision4, uint32_t *crushed4);
 
+/* ---- load-path solve without allocation
+ * No counterpart in the reference. Some callers cannot allocate GPU memory: a host engine that owns the device and
+ * gives this library no allocator of its own, or a frame loop that must not allocate once it is running. For them
+ * this entry point solves one structure (every brick given is structure 0, potentials start at 0, as a fresh world's
+ * first sf_structure_solve) with no cudaMalloc, no cudaFree and no allocating library call: all of its device
+ * scratch is one file-scope array of SF_STATIC_SCRATCH_BYTES (2.7 MB) that every GPU loading the library holds until
+ * the process exits. Inputs (lattice cells 3 per brick, material, infill, ext loads or NULL) and outputs (f64
+ * potentials per brick, sweeps, final residual) are host buffers of the caller. More than SF_STATIC_MAX_BRICKS
+ * bricks, or bricks spread over more than SF_STATIC_MAX_CHUNKS chunks of 8^3 cells, return SF_ERR_CAPACITY.
+ * The first call on a device looks up the array's device address (with that device current) and should come before
+ * any stream capture. Every call reuses the same array: calls whose work overlaps on the GPU race. */
+#define SF_STATIC_MAX_BRICKS 8192
+#define SF_STATIC_MAX_CHUNKS 128
+#define SF_STATIC_SCRATCH_BYTES 2815744
+sf_status sf_structure_solve_static(uint32_t n_bricks, const int32_t *xyz, const uint8_t *mat, const uint8_t *infill,
+                                    const float *ext, float omega, float tol, uint32_t max_sweeps, double *phi_out,
+                                    uint32_t *sweeps_out, double *resid_out, void *stream);
+
 /* ---- narrow phase entry points (batched) */
 /* Box-box SAT with face clipping and edge-edge, reduced to 4 points (engine/src/phys.rs:502-628). Boxes are
  * 10 floats: centre 3, quaternion 4, half extents 3. out per pair: count, normal 3, 4 x (point 3, separation). */

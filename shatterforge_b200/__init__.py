@@ -120,7 +120,32 @@ PROTOTYPES = {
     "sf_read_bonds": (C.c_int32, [C.c_void_p, _f32p, _u32p, _u8p]),
     "sf_read_joints": (C.c_int32, [C.c_void_p, _f32p, _f32p, _u8p, _u32p]),
     "sf_collide_boxes": (C.c_int32, [_f32p, _f32p, C.c_uint32, C.c_float, _f32p, _i32p]),
+    "sf_structure_solve_static": (C.c_int32, [C.c_uint32, _i32p, _u8p, _u8p, _f32p, C.c_float, C.c_float, C.c_uint32,
+                                              C.POINTER(C.c_double), _u32p, C.POINTER(C.c_double), C.c_void_p]),
 }
+
+STATIC_MAX_BRICKS = 8192
+STATIC_MAX_CHUNKS = 128
+
+
+def structure_solve_static(xyz, mat, infill=None, ext=None, omega: float = 1.7, tol: float = 1e-6,
+                           max_sweeps: int = 20000, stream_handle: int | None = None):
+    """Load-path solve of one structure with no GPU allocation (sf_structure_solve_static): for callers that
+    cannot allocate device memory. Returns (f64 potentials, sweeps, final residual)."""
+    lib = load()
+    x = np.ascontiguousarray(xyz, np.int32).reshape(-1, 3)
+    n = x.shape[0]
+    m = np.ascontiguousarray(mat, np.uint8)
+    inf = np.ascontiguousarray(infill if infill is not None else np.zeros(n, np.uint8), np.uint8)
+    e = None if ext is None else np.ascontiguousarray(ext, np.float32)
+    phi = np.zeros(n, np.float64)
+    sw = C.c_uint32()
+    rs = C.c_double()
+    _check(lib.sf_structure_solve_static(n, _ptr(x, C.c_int32), _ptr(m, C.c_uint8), _ptr(inf, C.c_uint8),
+                                         None if e is None else _ptr(e, C.c_float), float(omega), float(tol),
+                                         int(max_sweeps), _ptr(phi, C.c_double), C.byref(sw), C.byref(rs),
+                                         C.c_void_p(stream_handle or 0)), "sf_structure_solve_static")
+    return phi, sw.value, rs.value
 
 _lib = None
 

@@ -129,6 +129,34 @@ struct SorState;     // sf_sor.cu
 uint64_t sor_launches(const SorState *st);
 void sor_reset_launches(SorState *st);
 
+// Device buffers of one structure's load-path solve when the caller supplies every buffer (no allocation inside).
+struct SorBuffers {
+    const uint32_t *cell, *scene, *ctab;
+    const uint8_t *mat;
+    const int32_t *sid;
+    const uint32_t *nb6;
+    const float *bond, *ext;
+    double *phi64;
+    float *phi;
+    double *cphi;
+    float *crhs;
+    uint32_t *ccode;
+    int32_t *csid;
+    const int32_t *chunk_nbr, *chunk_sid;
+    const uint32_t *work, *active0;
+    unsigned long long *resid_buf;
+    uint32_t *sweeps;
+    double *resid;
+    GridBarrier *gb;
+    uint32_t *err;
+};
+cudaError_t sor_solve_on_buffers(const SorBuffers &B, uint32_t n_bricks, uint32_t n_chunks, float omega, float tol,
+                                 uint32_t max_sweeps, int sms, cudaStream_t s);
+// finalize_brick's links and bonds for bricks of one scene on caller-provided buffers (no allocation inside)
+cudaError_t finalize_on_buffers(uint32_t ns, const uint32_t *cell, const uint32_t *scene, const uint8_t *mat,
+                                const uint8_t *infill, const int32_t *sid, const uint32_t *ctab, const uint32_t *cpool,
+                                uint32_t *nb6, float *bond, float *bmax, cudaStream_t s);
+
 struct Scene {
     uint32_t static_off, n_static;
     uint32_t body_off, n_bodies;

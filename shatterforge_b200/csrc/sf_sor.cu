@@ -525,6 +525,33 @@ sf_status sor_create(sf_world *w) {
     return SF_OK;
 }
 
+// The red-black solve of one structure (id 0) on caller-provided chunk-layout buffers: no allocation, used by the
+// scratch-free entry point. Uploads this unit's material tables first (a copy to a constant symbol, no allocation).
+cudaError_t sor_solve_on_buffers(const SorBuffers &B, uint32_t n_bricks, uint32_t n_chunks, float omega, float tol,
+                                 uint32_t max_sweeps, int sms, cudaStream_t s) {
+    cudaError_t e = upload_mat_tables(s);
+    if (e != cudaSuccess) return e;
+    const uint32_t ncell = n_chunks * 512;
+    k_sor_clear<<<grid_for(ncell, 256), 256, 0, s>>>(ncell, B.ccode, B.csid);
+    k_sor_scatter<<<grid_for(n_bricks, 256), 256, 0, s>>>(n_bricks, B.cell, B.scene, B.mat, B.sid, B.nb6, B.bond, B.phi64,
+                                                          B.ext, B.ctab, B.cphi, B.crhs, B.ccode, B.csid);
+    k_sor_init<<<1, 32, 0, s>>>(1, B.resid_buf, B.sweeps, B.resid);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    int occ = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sor_redblack, SOR_BLOCK, 0)) != cudaSuccess) return e;
+    SorArgs A;
+    A.cphi = B.cphi; A.crhs = B.crhs; A.ccode = B.ccode; A.csid = B.csid; A.chunk_nbr = B.chunk_nbr; A.chunk_sid = B.chunk_sid;
+    A.work = B.work; A.n_work = n_chunks; A.n_struct = 1; A.active0 = B.active0; A.resid_buf = B.resid_buf;
+    A.sweeps = B.sweeps; A.resid = B.resid; A.omega = (double)omega; A.tol = (double)tol; A.max_sweeps = max_sweeps;
+    A.gb = B.gb; A.err = B.err;
+    unsigned grid = (unsigned)std::min<size_t>(n_chunks, (size_t)sms * std::max(occ, 1));
+    void *args[] = {&A};
+    if ((e = cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s)) != cudaSuccess) return e;
+    k_sor_gather<<<grid_for(n_bricks, 256), 256, 0, s>>>(n_bricks, B.cell, B.scene, B.mat, B.sid, B.active0, B.ctab, B.cphi,
+                                                         B.phi64, B.phi);
+    return cudaGetLastError();
+}
+
 uint64_t sor_launches(const SorState *st) { return st ? st->wk.launches + st->launches : 0; }
 void sor_reset_launches(SorState *st) { if (st) { st->wk.launches = 0; st->launches = 0; } }
 

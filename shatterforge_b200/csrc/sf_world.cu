@@ -167,6 +167,15 @@ __global__ void k_kill_marked(uint32_t nb, const uint8_t *alive, const uint32_t 
     for (uint32_t t = 0; t < count[b]; t++) kmat[first[b] + t] = 0;
 }
 
+cudaError_t finalize_on_buffers(uint32_t ns, const uint32_t *cell, const uint32_t *scene, const uint8_t *mat,
+                                const uint8_t *infill, const int32_t *sid, const uint32_t *ctab, const uint32_t *cpool,
+                                uint32_t *nb6, float *bond, float *bmax, cudaStream_t s) {
+    cudaError_t e = upload_mat_tables(s);
+    if (e != cudaSuccess || ns == 0) return e;
+    k_finalize_bricks<<<grid_for(ns, 256), 256, 0, s>>>(ns, cell, scene, mat, infill, sid, ctab, cpool, nb6, bond, bmax);
+    return cudaGetLastError();
+}
+
 sf_status read_error_word(sf_world *w) {
     uint32_t e = 0;
     SF_CUDA(cudaMemcpyAsync(&e, w->err.p, sizeof e, cudaMemcpyDeviceToHost, w->stream));
