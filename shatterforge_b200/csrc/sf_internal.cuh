@@ -177,6 +177,8 @@ struct sf_world {
     uint32_t n_scenes = 0, ns = 0, nd = 0, nb = 0, n_struct = 0, n_chunks = 0;
     uint32_t frame = 0;
     std::vector<sf::Scene> scenes;
+    std::vector<int4> h_sbox;            // per scene: static bricks' lattice bounding box (lo, hi)
+    sf::DBuf<int4> sbox;
 
     // static grid: per scene chunk table (NCT entries, global chunk index + 1) and chunk pool (static id + 1)
     sf::DBuf<uint32_t> ctab, cpool;

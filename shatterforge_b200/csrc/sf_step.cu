@@ -166,6 +166,7 @@ __global__ void k_bucket_records(uint32_t nd, const uint32_t *cval, const uint32
 struct ContactArgs {
     uint32_t nd;
     const uint32_t *kbody, *bscene, *ctab, *cpool;
+    const int4 *sbox;
     const uint8_t *alive, *asleep, *smat;
     const float4 *wpos, *v, *w;
     const float *rot, *rad;
@@ -201,8 +202,9 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
         }
     }
     // static cells of the 3^3 block (src/lib.rs:1422-1440): the block spans at most 2 x 2 x 2 chunks, read once
-    {
-        const int cx = floor_cell(p.x) + NX / 2, cy = floor_cell(p.y), cz = floor_cell(p.z) + NZ / 2;
+    const int cx = floor_cell(p.x) + NX / 2, cy = floor_cell(p.y), cz = floor_cell(p.z) + NZ / 2;
+    const int4 blo = A.sbox[2 * sc], bhi = A.sbox[2 * sc + 1];
+    if (cx + 1 >= blo.x && cx - 1 <= bhi.x && cy + 1 >= blo.y && cy - 1 <= bhi.y && cz + 1 >= blo.z && cz - 1 <= bhi.z) {
         const int ox = (cx - 1) >> 3, oy = (cy - 1) >> 3, oz = (cz - 1) >> 3;
         uint32_t ch[8];
         bool any = false;
@@ -286,7 +288,7 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
 }
 
 // pass 1: every contact of every awake brick counted; the first CSLOTS kept in the brick's slots
-__global__ void __launch_bounds__(128) k_contacts_gen(ContactArgs A) {
+__global__ void __launch_bounds__(128, 8) k_contacts_gen(ContactArgs A) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.nd) return;
     const uint32_t a = A.kbody[i];
@@ -593,9 +595,19 @@ __device__ __forceinline__ void solve_manifold(const SolveArgs &A, uint32_t m) {
 #pragma unroll
         for (int q = 0; q < 9; q++) ib[q] = A.iiw[(size_t)b * 9 + q];
     }
+    // the next contact's data is loaded while the current one is solved (the chain through the bodies is serial)
+    float4 nx_n = make_float4(0, 0, 0, 0), nx_t1 = nx_n, nx_t2 = nx_n, nx_ra = nx_n, nx_rb = nx_n, nx_j = nx_n;
+    if (cnt) {
+        nx_n = __ldg(&A.S_n[s0]); nx_t1 = __ldg(&A.S_t1[s0]); nx_t2 = __ldg(&A.S_t2[s0]);
+        nx_ra = __ldg(&A.S_ra[s0]); nx_rb = __ldg(&A.S_rb[s0]); nx_j = __ldcg(&A.S_j[s0]);
+    }
     for (uint32_t k = s0; k < s0 + cnt; k++) {
-        const float4 n4 = A.S_n[k], t14 = A.S_t1[k], t24 = A.S_t2[k], ra4 = A.S_ra[k], rb4 = A.S_rb[k];
-        float4 j4 = __ldcg(&A.S_j[k]);
+        const float4 n4 = nx_n, t14 = nx_t1, t24 = nx_t2, ra4 = nx_ra, rb4 = nx_rb;
+        float4 j4 = nx_j;
+        if (k + 1 < s0 + cnt) {
+            nx_n = __ldg(&A.S_n[k + 1]); nx_t1 = __ldg(&A.S_t1[k + 1]); nx_t2 = __ldg(&A.S_t2[k + 1]);
+            nx_ra = __ldg(&A.S_ra[k + 1]); nx_rb = __ldg(&A.S_rb[k + 1]); nx_j = __ldcg(&A.S_j[k + 1]);
+        }
         const V3 n = v3(n4.x, n4.y, n4.z), t1 = v3(t14.x, t14.y, t14.z), t2 = v3(t24.x, t24.y, t24.z);
         const V3 ra = v3(ra4.x, ra4.y, ra4.z), rb = v3(rb4.x, rb4.y, rb4.z);
         const float mn = n4.w, mt1 = t14.w, mt2 = t24.w, bias = ra4.w;
@@ -917,7 +929,7 @@ static sf_status substep(sf_world *w, float h) {
     prof_mark(w);
     // contacts: generate into slots and count, scan, place in list order
     ContactArgs C;
-    C.nd = nd; C.kbody = w->k_body.p; C.bscene = w->b_scene.p; C.ctab = w->ctab.p; C.cpool = w->cpool.p;
+    C.nd = nd; C.sbox = w->sbox.p; C.kbody = w->k_body.p; C.bscene = w->b_scene.p; C.ctab = w->ctab.p; C.cpool = w->cpool.p;
     C.alive = w->b_alive.p; C.asleep = w->b_asleep.p; C.smat = w->s_mat.p; C.wpos = w->k_wpos.p;
     C.v = w->b_v.p; C.w = w->b_w.p; C.rot = w->b_rot.p; C.rad = w->b_rad.p; C.brange = S->brange.p; C.srec = S->srec.p;
     C.sinfo = S->sinfo.p; C.ccount = S->ccount.p; C.coff = S->coff.p; C.wake = w->b_wake.p;

@@ -135,40 +135,51 @@ __global__ void k_rs_hist(const uint64_t *keys, size_t n, int shift, uint32_t *h
     hist[(size_t)threadIdx.x * nblocks + blockIdx.x] = cnt[threadIdx.x];
 }
 
-// Ranks keys of the tile in (item, thread) order, which is input order, so equal digits keep their order.
-__global__ void k_rs_scatter(const uint64_t *kin, const uint32_t *vin, uint64_t *kout, uint32_t *vout, size_t n, int shift,
-                             const uint32_t *offs, unsigned nblocks) {
-    __shared__ uint32_t base[256];
+// Stable ranking: warp w owns the tile's keys [w * 512, (w + 1) * 512), item k of lane l being key w*512 + k*32 + l,
+// so (warp, item, lane) is input order. Each warp counts its digits privately (the leader of each match group adds
+// the group's size), then one prefix over (warp, digit) places every key — two block barriers per tile.
+__global__ void __launch_bounds__(RS_BLOCK) k_rs_scatter(const uint64_t *kin, const uint32_t *vin, uint64_t *kout, uint32_t *vout,
+                                                         size_t n, int shift, const uint32_t *offs, unsigned nblocks) {
     __shared__ uint32_t wcnt[RS_WARPS][256];
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    base[threadIdx.x] = offs[(size_t)threadIdx.x * nblocks + blockIdx.x];
-    size_t tile = (size_t)blockIdx.x * RS_TILE;
-    unsigned lt = (1u << lane) - 1u;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; w++) wcnt[w][threadIdx.x] = 0;
+    const uint32_t gbase = offs[(size_t)threadIdx.x * nblocks + blockIdx.x];
+    __syncthreads();
+    const size_t wbase = (size_t)blockIdx.x * RS_TILE + (size_t)wid * (RS_ITEMS * 32);
+    const unsigned lt = (1u << lane) - 1u;
+    uint64_t key[RS_ITEMS];
+    uint32_t val[RS_ITEMS], rank[RS_ITEMS];
+#pragma unroll
     for (int k = 0; k < RS_ITEMS; k++) {
+        const size_t i = wbase + (size_t)k * 32 + lane;
+        const bool valid = i < n;
+        key[k] = valid ? kin[i] : 0ull;
+        val[k] = valid ? vin[i] : 0u;
+        const unsigned d = valid ? (unsigned)(key[k] >> shift) & 255u : 256u;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const int leader = __ffs(peers) - 1;
+        uint32_t prev = 0;
+        if (lane == leader && valid) { prev = wcnt[wid][d]; wcnt[wid][d] = prev + __popc(peers); }
+        prev = __shfl_sync(0xffffffffu, prev, leader);
+        rank[k] = prev + __popc(peers & lt);
+    }
+    __syncthreads();
+    {
+        uint32_t run = gbase;
 #pragma unroll
-        for (int w = 0; w < RS_WARPS; w++) wcnt[w][threadIdx.x] = 0;
-        __syncthreads();
-        size_t i = tile + (size_t)k * RS_BLOCK + threadIdx.x;
-        bool valid = i < n;
-        uint64_t key = valid ? kin[i] : 0ull;
-        uint32_t val = valid ? vin[i] : 0u;
-        unsigned d = valid ? (unsigned)(key >> shift) & 255u : 256u;
-        unsigned peers = __match_any_sync(0xffffffffu, d);
-        unsigned rank = __popc(peers & lt);
-        if (valid && rank == 0) wcnt[wid][d] = __popc(peers);
-        __syncthreads();
-        if (valid) {
-            uint32_t pos = base[d] + rank;
-            for (int w = 0; w < wid; w++) pos += wcnt[w][d];
-            kout[pos] = key;
-            vout[pos] = val;
+        for (int w = 0; w < RS_WARPS; w++) { const uint32_t c = wcnt[w][threadIdx.x]; wcnt[w][threadIdx.x] = run; run += c; }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; k++) {
+        const size_t i = wbase + (size_t)k * 32 + lane;
+        if (i < n) {
+            const unsigned d = (unsigned)(key[k] >> shift) & 255u;
+            const uint32_t pos = wcnt[wid][d] + rank[k];
+            kout[pos] = key[k];
+            vout[pos] = val[k];
         }
-        __syncthreads();
-        uint32_t add = 0;
-#pragma unroll
-        for (int w = 0; w < RS_WARPS; w++) add += wcnt[w][threadIdx.x];
-        base[threadIdx.x] += add;
-        __syncthreads();
     }
 }
 

@@ -294,12 +294,23 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
             s_sid[gi] = d.static_sid[k];
         }
         sc.n_chunks = nchunks - sc.chunk_off;
+        // the scene's static bricks' bounding box (empty: lo > hi), which lets a brick far from all of them skip
+        // the static-cell search
+        int4 lo = make_int4(1 << 20, 1 << 20, 1 << 20, 0), hi = make_int4(-(1 << 20), -(1 << 20), -(1 << 20), 0);
+        for (uint32_t k = 0; k < d.n_static; k++) {
+            int x = d.static_xyz[3 * k], y = d.static_xyz[3 * k + 1], z = d.static_xyz[3 * k + 2];
+            lo.x = std::min(lo.x, x); lo.y = std::min(lo.y, y); lo.z = std::min(lo.z, z);
+            hi.x = std::max(hi.x, x); hi.y = std::max(hi.y, y); hi.z = std::max(hi.z, z);
+        }
+        w->h_sbox.push_back(lo);
+        w->h_sbox.push_back(hi);
     }
     w->n_chunks = nchunks;
     w->h_sid = s_sid;
     w->h_s_cell = s_cell;
     cudaStream_t st = w->stream;
     SF_CUDA(upload(w->ctab, h_ctab, st));
+    SF_CUDA(upload(w->sbox, w->h_sbox, st));
     SF_CUDA(upload(w->cpool, h_cpool, st));
     SF_CUDA(upload(w->s_cell, s_cell, st));
     SF_CUDA(upload(w->s_scene, s_scene, st));
