@@ -205,6 +205,14 @@ sf_status sf_structure_solve_static(uint32_t n_bricks, const int32_t *xyz, const
 sf_status sf_collide_boxes(const float *boxes_a, const float *boxes_b, uint32_t n_pairs, float margin,
                            float *out20, int32_t *count);
 
+/* Convex-cell SAT (gpu/gpu_world.js:421-530 hull_ground / hull_hull, reduce4 :532-554): face axes of both cells,
+ * edge-direction crosses, reference-face clipping (up to 16 points, the deepest 8 kept) or edge-edge closest points.
+ * hull_data: n_hulls x 80 float4 in the reference's packed layout. Shapes are 11 floats: centre 3, quaternion 4,
+ * half extents 3, hull id; a b-shape with a negative hull id is the ground plane. out per pair: normal 3, 0, then
+ * 8 x (point 3, separation); reduce != 0 keeps at most 4 points. */
+sf_status sf_collide_hulls(const float *hull_data, uint32_t n_hulls, const float *shapes_a, const float *shapes_b,
+                           uint32_t n_pairs, float margin, int32_t reduce, float *out36, int32_t *count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -74,6 +74,8 @@ def load() -> C.CDLL:
     lib.ow_stress.restype = C.c_uint64
     lib.ow_stress.argtypes = [C.c_void_p, C.c_int32, C.c_float, C.c_int32, C.c_uint64, _u32p, _f32p, _f32p]
     lib.ow_remove_static.argtypes = [C.c_void_p, C.c_uint32]
+    lib.ow_collide_hulls.restype = C.c_int32
+    lib.ow_collide_hulls.argtypes = [_f32p, _f32p, _f32p, C.c_float, C.c_int32, _f32p]
     lib.ow_collide_boxes.restype = C.c_int32
     lib.ow_collide_boxes.argtypes = [_f32p, _f32p, C.c_float, C.c_int32, _f32p]
     _lib = lib
@@ -202,6 +204,17 @@ class OracleWorld:
 
     def remove_static(self, i):
         self.lib.ow_remove_static(self.h, int(i))
+
+
+def collide_hulls(hull_data, a, b, margin=0.02, reduce=False):
+    """hull_hull / hull_ground (gpu/gpu_world.js:421-530) for one pair; returns (count, normal, points[count, 4])."""
+    lib = load()
+    h = np.ascontiguousarray(hull_data, np.float32)
+    a = np.ascontiguousarray(a, np.float32); b = np.ascontiguousarray(b, np.float32)
+    out = np.zeros(36, np.float32)
+    n = lib.ow_collide_hulls(_p(h, C.c_float), _p(a, C.c_float), _p(b, C.c_float), float(margin), 1 if reduce else 0,
+                             _p(out, C.c_float))
+    return n, out[:3].copy(), out[4:4 + 4 * n].reshape(n, 4).copy()
 
 
 def collide_boxes(a, b, margin=0.02, reduce=True):

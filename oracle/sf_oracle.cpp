@@ -915,6 +915,168 @@ static int collide_boxes(P3 pa, const M3& ra, P3 ha, P3 pb, const M3& rb, P3 hb,
     return cnt;
 }
 
+
+// ---------------------------------------------------------------- convex-cell SAT (gpu/gpu_world.js:400-555)
+// Hull data: 80 float4 per hull (see shatterforge_b200/hulls.py). A shape is a cell in its box: p, rotation, half
+// extents h, hull id. Vector operations keep one fixed order (R*v = c0*v.x + c1*v.y + c2*v.z, normalize = v / |v|).
+struct HullShape { P3 p; M3 R; P3 h; const float* H; };
+static inline P3 hv4(const float* H, int k) { return p3(H[4 * k], H[4 * k + 1], H[4 * k + 2]); }
+static inline P3 rmul(const M3& R, P3 v) { return R.c[0] * v.x + R.c[1] * v.y + R.c[2] * v.z; }
+static inline P3 cmul(P3 a, P3 b) { return p3(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline P3 cdiv(P3 a, P3 b) { return p3(a.x / b.x, a.y / b.y, a.z / b.z); }
+static inline float plen(P3 a) { return std::sqrt(pdot(a, a)); }
+static inline P3 pnorm(P3 a) { float l = plen(a); return p3(a.x / l, a.y / l, a.z / l); }
+static inline int hnv(const float* H) { return (int)H[0]; }
+static inline int hnf(const float* H) { return (int)H[1]; }
+static inline int hns(const float* H) { return (int)H[2]; }
+static inline int hnd(const float* H) { return (int)H[3]; }
+static inline P3 hvert(const float* H, int k) { return hv4(H, 1 + k); }
+static inline int hfidx(const float* H, int f, int i) { return (int)H[4 * (29 + 2 * f + i / 4) + (i % 4)]; }
+static inline int hfcnt(const float* H, int f) { return (int)H[4 * (77 + f / 4) + (f % 4)]; }
+static inline void hseg(const float* H, int k, int& a, int& b) { const float* v = H + 4 * (53 + k / 2); if (k & 1) { a = (int)v[2]; b = (int)v[3]; } else { a = (int)v[0]; b = (int)v[1]; } }
+static inline P3 hdir(const float* H, int k) { return hv4(H, 65 + k); }
+static inline P3 hw(const HullShape& s, int k) { return s.p + rmul(s.R, cmul(s.h, hvert(s.H, k))); }
+static inline void hface(const HullShape& s, int f, P3& n, float& d) {
+    const float* pl = s.H + 4 * (17 + f);
+    P3 nw = rmul(s.R, cdiv(p3(pl[0], pl[1], pl[2]), s.h));
+    float l = plen(nw);
+    n = p3(nw.x / l, nw.y / l, nw.z / l);
+    d = pl[3] / l + pdot(n, s.p);
+}
+struct HC { P3 n; int cnt; float pt[8][4]; };
+static inline void hc_add(HC& c, P3 x, float w) {
+    if (c.cnt < 8) { c.pt[c.cnt][0] = x.x; c.pt[c.cnt][1] = x.y; c.pt[c.cnt][2] = x.z; c.pt[c.cnt][3] = w; c.cnt++; return; }
+    int hi = 0; for (int q = 1; q < 8; q++) if (c.pt[q][3] > c.pt[hi][3]) hi = q;
+    if (w < c.pt[hi][3]) { c.pt[hi][0] = x.x; c.pt[hi][1] = x.y; c.pt[hi][2] = x.z; c.pt[hi][3] = w; }
+}
+static HC hull_ground(const HullShape& s, float margin) {
+    HC c; c.cnt = 0; c.n = p3(0.0f, -1.0f, 0.0f);
+    for (int k = 0; k < hnv(s.H); k++) {
+        P3 x = hw(s, k);
+        if (x.y >= margin) continue;
+        hc_add(c, p3(x.x, 0.5f * x.y, x.z), x.y);
+    }
+    return c;
+}
+static HC hull_hull(const HullShape& A, const HullShape& B, float margin) {
+    HC c; c.cnt = 0; c.n = p3(0, 0, 0);
+    const int nfa = hnf(A.H), nfb = hnf(B.H), nva = hnv(A.H), nvb = hnv(B.H), nda = hnd(A.H), ndb = hnd(B.H);
+    P3 VA[16], VB[16], DA[12], DB[12];
+    for (int k = 0; k < nva; k++) VA[k] = hw(A, k);
+    for (int k = 0; k < nvb; k++) VB[k] = hw(B, k);
+    for (int k = 0; k < nda; k++) DA[k] = pnorm(rmul(A.R, cmul(A.h, hdir(A.H, k))));
+    for (int k = 0; k < ndb; k++) DB[k] = pnorm(rmul(B.R, cmul(B.h, hdir(B.H, k))));
+    float sa = -1e30f; int fa = 0;
+    for (int f = 0; f < nfa; f++) {
+        P3 n; float d; hface(A, f, n, d);
+        float lo = 1e30f; for (int k = 0; k < nvb; k++) lo = std::fmin(lo, pdot(VB[k], n));
+        float s = lo - d; if (s > margin) return c; if (s > sa) { sa = s; fa = f; }
+    }
+    float sb = -1e30f; int fb = 0;
+    for (int f = 0; f < nfb; f++) {
+        P3 n; float d; hface(B, f, n, d);
+        float lo = 1e30f; for (int k = 0; k < nva; k++) lo = std::fmin(lo, pdot(VA[k], n));
+        float s = lo - d; if (s > margin) return c; if (s > sb) { sb = s; fb = f; }
+    }
+    float se = -1e30f; P3 el = p3(0, 0, 0); int ei = 0, ej = 0;
+    for (int i = 0; i < nda; i++) for (int j = 0; j < ndb; j++) {
+        P3 l0 = pcross(DA[i], DB[j]); float l2 = pdot(l0, l0); if (l2 < 1e-6f) continue;
+        P3 l = l0 * (1.0f / std::sqrt(l2));
+        float alo = 1e30f, ahi = -1e30f, blo = 1e30f, bhi = -1e30f;
+        for (int k = 0; k < nva; k++) { float d = pdot(VA[k], l); alo = std::fmin(alo, d); ahi = std::fmax(ahi, d); }
+        for (int k = 0; k < nvb; k++) { float d = pdot(VB[k], l); blo = std::fmin(blo, d); bhi = std::fmax(bhi, d); }
+        float s1 = blo - ahi, s2 = alo - bhi;
+        float s = s1; if (s2 > s1) { s = s2; l = -l; }
+        if (s > margin) return c;
+        if (s > se) { se = s; el = l; ei = i; ej = j; }
+    }
+    bool use_b = sb > sa + 0.005f;
+    float fbest = use_b ? sb : sa;
+    if (se > fbest + 0.01f) {
+        P3 da = pnorm(rmul(A.R, cmul(A.h, hdir(A.H, ei)))), db = pnorm(rmul(B.R, cmul(B.h, hdir(B.H, ej))));
+        P3 a0 = A.p, a1 = A.p; float best = -1e30f;
+        for (int k = 0; k < hns(A.H); k++) {
+            int x, y; hseg(A.H, k, x, y); P3 q0 = hw(A, x), q1 = hw(A, y);
+            if (fabs_(pdot(pnorm(q1 - q0), da)) < 0.999f) continue;
+            float m = pdot(q0 + q1, el); if (m > best) { best = m; a0 = q0; a1 = q1; }
+        }
+        P3 b0 = B.p, b1 = B.p; best = 1e30f;
+        for (int k = 0; k < hns(B.H); k++) {
+            int x, y; hseg(B.H, k, x, y); P3 q0 = hw(B, x), q1 = hw(B, y);
+            if (fabs_(pdot(pnorm(q1 - q0), db)) < 0.999f) continue;
+            float m = pdot(q0 + q1, el); if (m < best) { best = m; b0 = q0; b1 = q1; }
+        }
+        P3 d1 = a1 - a0, d2 = b1 - b0, r = a0 - b0;
+        float aa = pdot(d1, d1), ee = pdot(d2, d2), ff = pdot(d2, r), cc = pdot(d1, r), bb = pdot(d1, d2);
+        float den = aa * ee - bb * bb;
+        float s1 = 0.0f; if (den > 1e-9f) s1 = std::fmin(std::fmax((bb * ff - cc * ee) / den, 0.0f), 1.0f);
+        float t1 = (bb * s1 + ff) / std::fmax(ee, 1e-9f);
+        if (t1 < 0.0f) { t1 = 0.0f; s1 = std::fmin(std::fmax(-cc / std::fmax(aa, 1e-9f), 0.0f), 1.0f); }
+        else if (t1 > 1.0f) { t1 = 1.0f; s1 = std::fmin(std::fmax((bb - cc) / std::fmax(aa, 1e-9f), 0.0f), 1.0f); }
+        P3 q1 = a0 + d1 * s1, q2 = b0 + d2 * t1;
+        c.n = el; c.cnt = 1;
+        P3 mid = (q1 + q2) * 0.5f;
+        c.pt[0][0] = mid.x; c.pt[0][1] = mid.y; c.pt[0][2] = mid.z; c.pt[0][3] = pdot(q2 - q1, el);
+        return c;
+    }
+    const HullShape& Rs = use_b ? B : A;
+    const HullShape& Is = use_b ? A : B;
+    const int fr = use_b ? fb : fa;
+    P3 n; float rw; hface(Rs, fr, n, rw);
+    const int nfi = use_b ? nfa : nfb;
+    int fi = 0; float bd = 1e30f;
+    for (int f = 0; f < nfi; f++) { P3 m; float d; hface(Is, f, m, d); float dd = pdot(m, n); if (dd < bd) { bd = dd; fi = f; } }
+    P3 poly[16], tmp[16];
+    int pn = hfcnt(Is.H, fi);
+    for (int q = 0; q < pn; q++) poly[q] = hw(Is, hfidx(Is.H, fi, q));
+    const int rn = hfcnt(Rs.H, fr);
+    P3 rc = p3(0, 0, 0);
+    for (int q = 0; q < rn; q++) rc = rc + hw(Rs, hfidx(Rs.H, fr, q));
+    rc = p3(rc.x / (float)rn, rc.y / (float)rn, rc.z / (float)rn);
+    for (int e = 0; e < rn; e++) {
+        P3 v0 = hw(Rs, hfidx(Rs.H, fr, e)), v1 = hw(Rs, hfidx(Rs.H, fr, (e + 1) % rn));
+        P3 sn = pnorm(pcross(v1 - v0, n)); if (pdot(sn, rc - v0) > 0.0f) sn = -sn;
+        int tn = 0;
+        for (int q = 0; q < pn; q++) {
+            P3 q0 = poly[q], q1 = poly[(q + 1) % pn];
+            float d0 = pdot(q0 - v0, sn), d1 = pdot(q1 - v0, sn);
+            if (d0 <= 0.0f && tn < 16) tmp[tn++] = q0;
+            if ((d0 <= 0.0f) != (d1 <= 0.0f) && tn < 16) tmp[tn++] = q0 + (q1 - q0) * (d0 / (d0 - d1));
+        }
+        pn = tn;
+        for (int q = 0; q < pn; q++) poly[q] = tmp[q];
+        if (pn == 0) return c;
+    }
+    for (int q = 0; q < pn; q++) {
+        P3 pp = poly[q]; float sep = pdot(pp, n) - rw;
+        if (sep > margin) continue;
+        hc_add(c, pp - n * (0.5f * sep), sep);
+    }
+    c.n = use_b ? -n : n;
+    return c;
+}
+// reduce4 as gpu/gpu_world.js:532-554
+static void hc_reduce4(HC& c) {
+    int cnt = c.cnt; if (cnt <= 4) return;
+    P3 n = c.n;
+    auto P = [&](int k) { return p3(c.pt[k][0], c.pt[k][1], c.pt[k][2]); };
+    int i0 = 0; for (int k = 1; k < cnt; k++) if (c.pt[k][3] < c.pt[i0][3]) i0 = k;
+    P3 q0 = P(i0);
+    int i1 = 0; float best = -1.0f;
+    for (int k = 0; k < cnt; k++) { P3 d = P(k) - q0; if (pdot(d, d) > best) { best = pdot(d, d); i1 = k; } }
+    P3 e = P(i1) - q0;
+    int i2 = 0, i3 = 0; float b2 = -1e30f, b3 = -1e30f;
+    for (int k = 0; k < cnt; k++) { float a = pdot(pcross(P(k) - q0, e), n); if (a > b2) { b2 = a; i2 = k; } if (-a > b3) { b3 = -a; i3 = k; } }
+    int sel[4] = {i0, i1, i2, i3};
+    float out[4][4]; int oc = 0;
+    for (int k = 0; k < 4; k++) {
+        bool dup = false; for (int q = 0; q < k; q++) if (sel[q] == sel[k]) dup = true;
+        if (!dup) { for (int t = 0; t < 4; t++) out[oc][t] = c.pt[sel[k]][t]; oc++; }
+    }
+    for (int k = 0; k < oc; k++) for (int t = 0; t < 4; t++) c.pt[k][t] = out[k][t];
+    c.cnt = oc;
+}
+
 }  // namespace
 
 // ============================================================================================================
@@ -1101,6 +1263,22 @@ void ow_remove_static(void* h, uint32_t i) {
     if (i >= w->ns || w->mat[i] == 0) return;
     w->gset(w->bx[i], w->by[i], w->bz[i], 0);
     w->mat[i] = 0;
+}
+
+
+// ---- hull SAT: shapes are p3 q4 h3 hull (11 floats); b's hull < 0 = the ground. Output: normal 3, pad, 8 x (p3, sep).
+int32_t ow_collide_hulls(const float* hulls, const float* A, const float* B, float margin, int32_t do_reduce, float* out36) {
+    HullShape a{p3(A[0], A[1], A[2]), quat_m3(A + 3), p3(A[7], A[8], A[9]), hulls + (size_t)(int)A[10] * 320};
+    HC c;
+    if (B[10] < 0.0f) c = hull_ground(a, margin);
+    else {
+        HullShape b{p3(B[0], B[1], B[2]), quat_m3(B + 3), p3(B[7], B[8], B[9]), hulls + (size_t)(int)B[10] * 320};
+        c = hull_hull(a, b, margin);
+    }
+    if (do_reduce) hc_reduce4(c);
+    out36[0] = c.n.x; out36[1] = c.n.y; out36[2] = c.n.z; out36[3] = 0.0f;
+    for (int k = 0; k < 8; k++) for (int t = 0; t < 4; t++) out36[4 + 4 * k + t] = k < c.cnt ? c.pt[k][t] : 0.0f;
+    return c.cnt;
 }
 
 // ---- box SAT: boxes are p3 q4 h3 (10 floats). Output: normal3 + up to 8 points (p3, sep), reduced to 4.

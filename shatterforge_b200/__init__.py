@@ -120,6 +120,7 @@ PROTOTYPES = {
     "sf_read_bonds": (C.c_int32, [C.c_void_p, _f32p, _u32p, _u8p]),
     "sf_read_joints": (C.c_int32, [C.c_void_p, _f32p, _f32p, _u8p, _u32p]),
     "sf_collide_boxes": (C.c_int32, [_f32p, _f32p, C.c_uint32, C.c_float, _f32p, _i32p]),
+    "sf_collide_hulls": (C.c_int32, [_f32p, C.c_uint32, _f32p, _f32p, C.c_uint32, C.c_float, C.c_int32, _f32p, _i32p]),
     "sf_structure_solve_static": (C.c_int32, [C.c_uint32, _i32p, _u8p, _u8p, _f32p, C.c_float, C.c_float, C.c_uint32,
                                               C.POINTER(C.c_double), _u32p, C.POINTER(C.c_double), C.c_void_p]),
 }
@@ -395,6 +396,23 @@ class World:
         _check(self._lib.sf_read_joints(self._h, _ptr(r, C.c_float), _ptr(b, C.c_float), _ptr(d, C.c_uint8), _ptr(k, C.c_uint32)),
                "sf_read_joints")
         return r, b, d, k
+
+
+def collide_hulls(hull_data: np.ndarray, shapes_a: np.ndarray, shapes_b: np.ndarray, margin: float = 0.02,
+                  reduce: bool = False):
+    """Batched convex-cell SAT (gpu/gpu_world.js:421-530). hull_data: [n_hulls, 80, 4] (shatterforge_b200.hulls);
+    shapes: [n, 11] (centre, quaternion, half extents, hull id; a b-shape hull id < 0 is the ground).
+    Returns (count[n], normal[n,3], points[n,8,4])."""
+    lib = load()
+    h = np.ascontiguousarray(hull_data, np.float32).reshape(-1, 80, 4)
+    a = np.ascontiguousarray(shapes_a, np.float32).reshape(-1, 11)
+    b = np.ascontiguousarray(shapes_b, np.float32).reshape(-1, 11)
+    n = a.shape[0]
+    out = np.zeros((n, 36), np.float32)
+    cnt = np.zeros(n, np.int32)
+    _check(lib.sf_collide_hulls(_ptr(h, C.c_float), h.shape[0], _ptr(a, C.c_float), _ptr(b, C.c_float), n, float(margin),
+                                1 if reduce else 0, _ptr(out, C.c_float), _ptr(cnt, C.c_int32)), "sf_collide_hulls")
+    return cnt, out[:, :3], out[:, 4:].reshape(n, 8, 4)
 
 
 def collide_boxes(boxes_a: np.ndarray, boxes_b: np.ndarray, margin: float = 0.02):

@@ -239,6 +239,36 @@ def test_config1_scene_runs(sf, oracle):
     np.testing.assert_array_equal(st, ost)
 
 
+# ---------------------------------------------------------------- hull SAT
+@pytest.mark.parametrize("reduce", [False, True])
+def test_hull_sat_bit_exact(sf, oracle, reduce):
+    from shatterforge_b200 import hulls
+    data = hulls.library().packed()
+    rng = np.random.default_rng(9)
+    n = 3000
+    def shapes(n, ground_frac=0.0):
+        s = np.zeros((n, 11), np.float32)
+        s[:, :3] = rng.uniform(-0.45, 0.45, (n, 3))
+        q = rng.normal(size=(n, 4))
+        s[:, 3:7] = q / np.linalg.norm(q, axis=1, keepdims=True)
+        s[:, 7:10] = rng.uniform(0.15, 0.5, (n, 3))
+        s[:, 10] = rng.integers(0, len(data), n)
+        return s
+    a, b = shapes(n), shapes(n)
+    b[: n // 10, 10] = -1.0                      # a tenth against the ground
+    a[: n // 10, 1] = rng.uniform(-0.2, 0.4, n // 10)
+    cnt, nrm, pts = sf.collide_hulls(data, a, b, margin=0.02, reduce=reduce)
+    hits = 0
+    for i in range(n):
+        on, onrm, opts = oracle.collide_hulls(data, a[i], b[i], margin=0.02, reduce=reduce)
+        assert cnt[i] == on, i
+        if on:
+            hits += 1
+            np.testing.assert_array_equal(nrm[i], onrm)
+            np.testing.assert_array_equal(pts[i, :on], opts)
+    assert hits > n // 4
+
+
 # ---------------------------------------------------------------- box SAT
 def test_box_sat_bit_exact(sf, oracle):
     rng = np.random.default_rng(5)
