@@ -75,7 +75,9 @@ typedef struct sf_params {
     uint32_t contact_capacity;  /* 0 = automatic (grows between steps) */
     uint32_t verify;            /* 1: check the colouring is proper every substep (SF_ERR_VERIFY on failure) */
     uint32_t solve_blocks;      /* persistent-kernel blocks per SM for the solve (0 = autotuned) */
-    uint32_t reserved[8];
+    uint32_t manifold_chunk;    /* a body pair's contacts are solved in chunks of at most this many (0 = whole pair);
+                                   chunks of one pair take different colours, bounding each colour's longest chain */
+    uint32_t reserved[7];
 } sf_params;
 
 typedef struct sf_stats {

@@ -28,7 +28,7 @@ _u64p = C.POINTER(C.c_uint64)
 
 class StepParams(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("substeps", C.c_uint32), ("order", C.c_uint32), ("sleep_mode", C.c_uint32),
-                ("pinch_kill", C.c_uint32)]
+                ("pinch_kill", C.c_uint32), ("chunk", C.c_uint32)]
 
 
 _lib = None
@@ -147,8 +147,8 @@ class OracleWorld:
         self.lib.ow_get_bonds(self.h, _p(b, C.c_float), _p(nb, C.c_uint32))
         return b, nb
 
-    def step(self, dt=1.0 / 60.0, iterations=10, substeps=2, order=ORDER_COLOR, sleep_mode=SLEEP_BODY, pinch_kill=1):
-        p = StepParams(iterations, substeps, order, sleep_mode, pinch_kill)
+    def step(self, dt=1.0 / 60.0, iterations=10, substeps=2, order=ORDER_COLOR, sleep_mode=SLEEP_BODY, pinch_kill=1, chunk=16):
+        p = StepParams(iterations, substeps, order, sleep_mode, pinch_kill, chunk)
         self.lib.ow_step(self.h, float(dt), C.byref(p))
 
     def contacts(self):

@@ -173,6 +173,7 @@ struct World {
     std::vector<uint32_t> island;    // per body, last substep
     std::vector<uint32_t> man_a, man_b, man_color, man_start, man_count, man_contacts;
     uint32_t ncolors = 0;
+    uint32_t chunk = 16;             // contacts per solve chunk of a body pair (0 = the whole pair)
     uint32_t frame = 0;
     uint64_t would_drop = 0;         // contacts the reference would have dropped past MAXC
     uint32_t crush_n = 0;
@@ -632,18 +633,25 @@ static void build_manifolds(World& w) {
     };
     std::stable_sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
     w.man_a.clear(); w.man_b.clear(); w.man_start.clear(); w.man_count.clear(); w.man_contacts = idx;
+    // a pair's contacts form chunks of at most K (K = 0: one chunk); the colouring and the solve see chunks
+    std::vector<uint32_t> prio;
+    size_t pair_start = 0;
     for (size_t t = 0; t < n; t++) {
-        if (t == 0 || key(idx[t]) != key(idx[t - 1])) {
+        bool new_pair = t == 0 || key(idx[t]) != key(idx[t - 1]);
+        if (new_pair) pair_start = t;
+        uint32_t j = w.chunk ? (uint32_t)((t - pair_start) / w.chunk) : 0u;
+        bool new_chunk = new_pair || (w.chunk && (t - pair_start) % w.chunk == 0);
+        if (new_chunk) {
             const Contact& c = w.cs[idx[t]];
             w.man_a.push_back(c.a); w.man_b.push_back(c.b); w.man_start.push_back((uint32_t)t); w.man_count.push_back(0);
+            uint32_t h = pair_priority(c.a, c.b == STATIC ? 0u : c.b + 1);
+            prio.push_back(j ? pair_priority(h, j) : h);
         }
         w.man_count.back()++;
     }
     size_t nm = w.man_a.size();
     std::vector<uint32_t> order(nm);
     std::iota(order.begin(), order.end(), 0u);
-    std::vector<uint32_t> prio(nm);
-    for (size_t k = 0; k < nm; k++) prio[k] = pair_priority(w.man_a[k], w.man_b[k] == STATIC ? 0u : w.man_b[k] + 1);
     std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return prio[x] != prio[y] ? prio[x] > prio[y] : x < y; });
     std::vector<std::vector<uint64_t>> used(w.nbody, std::vector<uint64_t>(4, 0));
     w.man_color.assign(nm, 0);
@@ -1084,7 +1092,7 @@ static void hc_reduce4(HC& c) {
 // ============================================================================================================
 extern "C" {
 
-struct ow_step_params { uint32_t iterations, substeps, order, sleep_mode, pinch_kill; };
+struct ow_step_params { uint32_t iterations, substeps, order, sleep_mode, pinch_kill, chunk; };
 
 void* ow_create(uint32_t n_static, const int32_t* static_xyz, const uint8_t* static_mat, const int32_t* static_sid,
                 const uint8_t* static_infill, uint32_t n_bodies, const uint32_t* body_first, const int32_t* body_brick_xyz,
@@ -1198,6 +1206,7 @@ void ow_get_bonds(void* h, float* bond4, uint32_t* nb6) {
 
 void ow_step(void* h, float dt, const ow_step_params* p) {
     StepParams P{p->iterations, p->substeps, p->order, p->sleep_mode, p->pinch_kill};
+    ((World*)h)->chunk = p->chunk;
     step(*(World*)h, dt, P);
 }
 // substep pieces for per-phase parity: update_cache + gravity + hash + contacts (+ prep)

@@ -53,7 +53,8 @@ class WorldDesc(C.Structure):
 class Params(C.Structure):
     _fields_ = [("substeps", C.c_uint32), ("iterations", C.c_uint32), ("sleep_mode", C.c_uint32),
                 ("pinch_kill", C.c_uint32), ("max_colors", C.c_uint32), ("contact_capacity", C.c_uint32),
-                ("verify", C.c_uint32), ("solve_blocks", C.c_uint32), ("reserved", C.c_uint32 * 8)]
+                ("verify", C.c_uint32), ("solve_blocks", C.c_uint32), ("manifold_chunk", C.c_uint32),
+                ("reserved", C.c_uint32 * 7)]
 
 
 class Stats(C.Structure):

@@ -618,7 +618,7 @@ sf_status sf_structure_solve(sf_world *w, int32_t structure, float omega, float 
     A.chunk_sid = st->chunk_sid.p; A.work = st->work.p; A.n_work = (uint32_t)chunks.size(); A.n_struct = nst;
     A.active0 = st->active0.p; A.resid_buf = st->resid_buf.p; A.sweeps = st->sweeps.p; A.resid = st->resid.p;
     A.omega = (double)omega; A.tol = (double)tol; A.max_sweeps = max_sweeps; A.gb = w->barrier.p; A.err = w->err.p;
-    unsigned grid = (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * st->occ);
+    unsigned grid = (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * std::min(st->occ, 2));
     void *args[] = {&A};
     SF_CUDA(cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s));
     k_sor_gather<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p,

@@ -47,7 +47,7 @@ struct StepState {
     // manifold order
     DBuf<uint64_t> mkey, mkey_alt;
     DBuf<uint32_t> perm, perm_alt, invperm;
-    DBuf<uint32_t> mflag, mpos;
+    DBuf<uint32_t> mflag, mpos, pair_start, cflag, cpos;
     DBuf<uint32_t> man_a, man_b, man_start, man_count, man_prio, man_color, man_round;
     DBuf<float4> S_n, S_t1, S_t2, S_ra, S_rb, S_j;
     // colouring
@@ -88,7 +88,7 @@ static void prof_mark(sf_world *w) {
 }
 
 enum { DV_CONTACTS = 0, DV_MANIFOLDS = 1, DV_COLORS = 2, DV_ROUNDS = 3, DV_WL0 = 4, DV_WL1 = 5, DV_WL2 = 6,
-       DV_ALIVE = 7, DV_AWAKE = 8, DV_ISLANDS = 9, DV_N = 16 };
+       DV_ALIVE = 7, DV_AWAKE = 8, DV_ISLANDS = 9, DV_PAIRS = 10, DV_N = 16 };
 
 // ---------------------------------------------------------------- pose cache
 __global__ void k_update_cache(uint32_t nb, float h, const uint8_t *alive, const uint8_t *asleep, const float4 *q,
@@ -362,17 +362,33 @@ __global__ void k_man_flags(uint32_t nc, const uint64_t *key, uint32_t *flag) {
     if (t >= nc) return;
     flag[t] = (t == 0 || key[t] != key[t - 1]) ? 1u : 0u;
 }
-__global__ void k_man_write(uint32_t nc, const uint32_t *flag, const uint32_t *pos, const uint32_t *perm, const uint32_t *L_a,
-                            const uint32_t *L_b, const uint32_t *bscene, const uint32_t *body_off_of_body,
-                            uint32_t *man_a, uint32_t *man_b, uint32_t *man_start, uint32_t *man_prio) {
+__global__ void k_pair_start(uint32_t nc, const uint32_t *flag, const uint32_t *pos, uint32_t *pair_start) {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nc || !flag[t]) return;
-    uint32_t m = pos[t];
+    if (t < nc && flag[t]) pair_start[pos[t]] = t;
+}
+// A body pair's contacts are solved in chunks of at most K (K = 0: the whole pair at once). Chunks of one pair share
+// its bodies, so they conflict and take different colours; a chunk is the unit the colouring and the solve see.
+__global__ void k_chunk_flags(uint32_t nc, uint32_t K, const uint32_t *flag, const uint32_t *pos, const uint32_t *pair_start,
+                              uint32_t *cflag) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nc) return;
+    const uint32_t mid = pos[t] + flag[t] - 1;
+    cflag[t] = K ? ((t - pair_start[mid]) % K == 0 ? 1u : 0u) : flag[t];
+}
+__global__ void k_man_write(uint32_t nc, uint32_t K, const uint32_t *cflag, const uint32_t *cpos, const uint32_t *flag,
+                            const uint32_t *pos, const uint32_t *pair_start, const uint32_t *perm, const uint32_t *L_a,
+                            const uint32_t *L_b, const uint32_t *body_off_of_body, uint32_t *man_a, uint32_t *man_b,
+                            uint32_t *man_start, uint32_t *man_prio) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nc || !cflag[t]) return;
+    uint32_t m = cpos[t];
     uint32_t k = perm[t];
     uint32_t a = L_a[k], b = L_b[k];
     man_a[m] = a; man_b[m] = b; man_start[m] = t;
     uint32_t off = body_off_of_body[a];
-    man_prio[m] = pair_priority(a - off, b == STATIC ? 0u : b - off + 1u);
+    uint32_t h = pair_priority(a - off, b == STATIC ? 0u : b - off + 1u);
+    const uint32_t j = K ? (t - pair_start[pos[t] + flag[t] - 1]) / K : 0u;
+    man_prio[m] = j ? pair_priority(h, j) : h;
 }
 __global__ void k_man_count(const uint32_t *nm_p, uint32_t nc, const uint32_t *man_start, uint32_t *man_count) {
     uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -855,7 +871,7 @@ static cudaError_t grow_contacts(StepState *S, uint64_t need) {
     cudaError_t e;
 #define G(buf) if ((e = S->buf.alloc(cap)) != cudaSuccess) return e
     G(L_a); G(L_b); G(L_bo); G(L_ba); G(L_bb); G(L_p); G(L_n);
-    G(mkey); G(mkey_alt); G(perm); G(perm_alt); G(invperm); G(mflag); G(mpos);
+    G(mkey); G(mkey_alt); G(perm); G(perm_alt); G(invperm); G(mflag); G(mpos); G(pair_start); G(cflag); G(cpos);
     G(man_a); G(man_b); G(man_start); G(man_count); G(man_prio); G(man_color); G(man_round);
     G(S_n); G(S_t1); G(S_t2); G(S_ra); G(S_rb); G(S_j);
     G(wl0); G(wl1); G(col_list);
@@ -959,12 +975,17 @@ static sf_status substep(sf_world *w, float h) {
     if (nc) {
         k_man_keys<<<g_nc, 256, 0, s>>>(nc, nb1, S->L_a.p, S->L_b.p, S->mkey.p, S->perm.p);
         SF_CUDA(radix_sort_u64(S->mkey.p, S->perm.p, S->mkey_alt.p, S->perm_alt.p, nc, bits_for((uint64_t)nb * nb1 + nb1), S->wk, s));
+        const uint32_t K = w->P.manifold_chunk;
         k_man_flags<<<g_nc, 256, 0, s>>>(nc, S->mkey.p, S->mflag.p);
-        SF_CUDA(exclusive_scan_u32(S->mflag.p, S->mpos.p, nc, S->dev.p + DV_MANIFOLDS, S->wk, s));
-        k_man_write<<<g_nc, 256, 0, s>>>(nc, S->mflag.p, S->mpos.p, S->perm.p, S->L_a.p, S->L_b.p, w->b_scene.p,
-                                         S->body_off_of_body.p, S->man_a.p, S->man_b.p, S->man_start.p, S->man_prio.p);
+        SF_CUDA(exclusive_scan_u32(S->mflag.p, S->mpos.p, nc, S->dev.p + DV_PAIRS, S->wk, s));
+        k_pair_start<<<g_nc, 256, 0, s>>>(nc, S->mflag.p, S->mpos.p, S->pair_start.p);
+        k_chunk_flags<<<g_nc, 256, 0, s>>>(nc, K, S->mflag.p, S->mpos.p, S->pair_start.p, S->cflag.p);
+        SF_CUDA(exclusive_scan_u32(S->cflag.p, S->cpos.p, nc, S->dev.p + DV_MANIFOLDS, S->wk, s));
+        k_man_write<<<g_nc, 256, 0, s>>>(nc, K, S->cflag.p, S->cpos.p, S->mflag.p, S->mpos.p, S->pair_start.p, S->perm.p,
+                                         S->L_a.p, S->L_b.p, S->body_off_of_body.p, S->man_a.p, S->man_b.p, S->man_start.p,
+                                         S->man_prio.p);
         k_man_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, nc, S->man_start.p, S->man_count.p);
-        L += 4;
+        L += 6;
         prof_mark(w);
         PrepArgs PA;
         PA.nc = nc; PA.h = h; PA.perm = S->perm.p; PA.L_a = S->L_a.p; PA.L_b = S->L_b.p; PA.L_p = S->L_p.p; PA.L_n = S->L_n.p;
@@ -988,7 +1009,7 @@ static sf_status substep(sf_world *w, float h) {
         J.bm_start = S->bm_start.p; J.bm_list = S->bm_list.p; J.man_round = S->man_round.p; J.man_color = S->man_color.p;
         J.masks = S->masks.p; J.wl0 = S->wl0.p; J.wl1 = S->wl1.p; J.dev = S->dev.p; J.max_colors = w->P.max_colors;
         J.max_rounds = 1u << 16; J.gb = w->barrier.p; J.err = w->err.p;
-        unsigned jgrid = (unsigned)std::min<uint64_t>((uint64_t)w->sms * S->jp_occ, (nc + 255) / 256 + 1);
+        unsigned jgrid = (unsigned)std::min<uint64_t>((uint64_t)w->sms * std::min(S->jp_occ, 2), (nc + 255) / 256 + 1);
         void *jargs[] = {&J};
         SF_CUDA(cudaLaunchCooperativeKernel((void *)k_jp, dim3(jgrid), dim3(256), jargs, 0, s));
         SF_CUDA(cudaMemsetAsync(S->col_count.p, 0, S->col_count.bytes(), s));
@@ -1016,7 +1037,7 @@ static sf_status substep(sf_world *w, float h) {
         A.man_a = S->man_a.p; A.man_b = S->man_b.p; A.man_start = S->man_start.p; A.man_count = S->man_count.p;
         A.S_n = S->S_n.p; A.S_t1 = S->S_t1.p; A.S_t2 = S->S_t2.p; A.S_ra = S->S_ra.p; A.S_rb = S->S_rb.p; A.S_j = S->S_j.p;
         A.v = w->b_v.p; A.w = w->b_w.p; A.im = w->b_im.p; A.iiw = w->b_iiw.p; A.gb = w->barrier.p; A.err = w->err.p;
-        unsigned per_sm = w->P.solve_blocks ? std::min<unsigned>(w->P.solve_blocks, S->solve_occ) : S->solve_occ;
+        unsigned per_sm = w->P.solve_blocks ? std::min<unsigned>(w->P.solve_blocks, S->solve_occ) : std::min(S->solve_occ, 2);
         unsigned sgrid = (unsigned)std::min<uint64_t>((uint64_t)w->sms * per_sm, (nc + SOLVE_BLOCK - 1) / SOLVE_BLOCK + 1);
         void *sargs[] = {&A};
         SF_CUDA(cudaLaunchCooperativeKernel((void *)k_solve, dim3(sgrid), dim3(SOLVE_BLOCK), sargs, 0, s));
