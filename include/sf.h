@@ -147,6 +147,10 @@ sf_status sf_structure_solve(sf_world *w, int32_t structure, float omega, float 
 /* Joint checks of one structure (or -1 = all) on the current potentials; live != 0 applies fatigue, failures and
  * crushes as stress_brick does. */
 sf_status sf_structure_check(sf_world *w, int32_t structure, float dt, int32_t live, sf_check_report *report);
+/* Resting-body loads of `structural` (src/lib.rs:1233-1259) for the listed structures: brick positions refreshed as
+ * update_cache does, each body's weight shared over the listed structures' bricks under it and the ground, summed
+ * per brick in body-then-brick order into extn, then ext = 0.8 ext + 0.2 extn. */
+sf_status sf_structure_loads(sf_world *w, const int32_t *structures, uint32_t n_structures);
 /* Per-structure sweeps and final residuals of the last sf_structure_solve (n_structures entries each). */
 sf_status sf_read_solve_detail(sf_world *w, uint32_t *sweeps, double *resid);
 

@@ -74,6 +74,8 @@ def load() -> C.CDLL:
     lib.ow_stress.restype = C.c_uint64
     lib.ow_stress.argtypes = [C.c_void_p, C.c_int32, C.c_float, C.c_int32, C.c_uint64, _u32p, _f32p, _f32p]
     lib.ow_remove_static.argtypes = [C.c_void_p, C.c_uint32]
+    lib.ow_structure_loads.argtypes = [C.c_void_p, _i32p, C.c_uint32]
+    lib.ow_get_ext.argtypes = [C.c_void_p, _f32p]
     lib.ow_collide_hulls.restype = C.c_int32
     lib.ow_collide_hulls.argtypes = [_f32p, _f32p, _f32p, C.c_float, C.c_int32, _f32p]
     lib.ow_collide_boxes.restype = C.c_int32
@@ -201,6 +203,15 @@ class OracleWorld:
         n = self.lib.ow_stress(self.h, int(structure), float(dt), 1 if live else 0, cap, _p(ids, C.c_uint32),
                                _p(vals, C.c_float), C.byref(mr))
         return ids[:n], vals[:n], mr.value
+
+    def structure_loads(self, structures):
+        s = np.ascontiguousarray(structures, np.int32)
+        self.lib.ow_structure_loads(self.h, _p(s, C.c_int32), len(s))
+
+    def ext(self):
+        e = np.zeros(self.ns, np.float32)
+        self.lib.ow_get_ext(self.h, _p(e, C.c_float))
+        return e
 
     def remove_static(self, i):
         self.lib.ow_remove_static(self.h, int(i))

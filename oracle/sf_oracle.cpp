@@ -1267,6 +1267,38 @@ uint64_t ow_stress(void* h, int32_t s, float dt, int32_t live, uint64_t cap, uin
     }
     return out.size();
 }
+// structural's resting-body loads (src/lib.rs:1233-1259) for the listed structures, after update_cache as step does
+void ow_structure_loads(void* h, const int32_t* listed, uint32_t n) {
+    World* w = (World*)h;
+    std::vector<uint8_t> act(4096, 0);
+    for (uint32_t k = 0; k < n; k++) if (listed[k] >= 0 && listed[k] < 4096) act[listed[k]] = 1;
+    update_cache(*w);
+    std::vector<float> extn(w->ns, 0.0f);
+    auto target = [&](V p) -> uint32_t {
+        int cx = (int)std::floor(p[0] / S) + NX / 2, cy = (int)std::floor((p[1] - RB - 0.02f) / S), cz = (int)std::floor(p[2] / S) + NZ / 2;
+        uint32_t j = w->static_brick(cx, cy, cz);
+        if (j == NONE || w->sid[j] < 0 || !act[w->sid[j]]) return NONE;
+        return j;
+    };
+    for (uint32_t b = 0; b < w->nbody; b++) {
+        if (!w->alive[b]) continue;
+        uint32_t ns = 0, nground = 0;
+        for (uint32_t k = w->first[b]; k != NONE; k = w->next[k]) {
+            V p = w->wpos[k];
+            if (p[1] < RB + 0.05f) nground++;
+            if (target(p) != NONE) ns++;
+        }
+        if (ns == 0) continue;
+        float share = w->m[b] / (float)(ns + nground);
+        for (uint32_t k = w->first[b]; k != NONE; k = w->next[k]) {
+            uint32_t j = target(w->wpos[k]);
+            if (j != NONE) extn[j] += share;
+        }
+    }
+    for (uint32_t i = 0; i < w->ns; i++) if (w->sid[i] >= 0 && act[w->sid[i]]) w->ext[i] = w->ext[i] * 0.8f + extn[i] * 0.2f;
+}
+void ow_get_ext(void* h, float* ext) { World* w = (World*)h; for (uint32_t i = 0; i < w->ns; i++) ext[i] = w->ext[i]; }
+
 void ow_remove_static(void* h, uint32_t i) {
     World* w = (World*)h;
     if (i >= w->ns || w->mat[i] == 0) return;

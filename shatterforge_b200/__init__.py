@@ -104,6 +104,7 @@ PROTOTYPES = {
     "sf_structure_solve": (C.c_int32, [C.c_void_p, C.c_int32, C.c_float, C.c_float, C.c_uint32, C.POINTER(SolveReport)]),
     "sf_structure_check": (C.c_int32, [C.c_void_p, C.c_int32, C.c_float, C.c_int32, C.POINTER(CheckReport)]),
     "sf_read_solve_detail": (C.c_int32, [C.c_void_p, _u32p, C.POINTER(C.c_double)]),
+    "sf_structure_loads": (C.c_int32, [C.c_void_p, _i32p, C.c_uint32]),
     "sf_world_get_info": (C.c_int32, [C.c_void_p, C.POINTER(WorldInfo)]),
     "sf_get_stats": (C.c_int32, [C.c_void_p, C.POINTER(Stats)]),
     "sf_read_bodies": (C.c_int32, [C.c_void_p, _f32p, _f32p, _u8p]),
@@ -289,6 +290,11 @@ class World:
         _check(self._lib.sf_structure_solve(self._h, int(structure), float(omega), float(tol), int(max_sweeps), C.byref(r)),
                "sf_structure_solve")
         return r
+
+    def structure_loads(self, structures):
+        """Resting-body loads onto the listed structures (src/lib.rs:1233-1259); updates ext."""
+        s = np.ascontiguousarray(structures, np.int32)
+        _check(self._lib.sf_structure_loads(self._h, _ptr(s, C.c_int32), len(s)), "sf_structure_loads")
 
     def solve_detail(self):
         n = self.info.n_structures

@@ -290,5 +290,7 @@ sf_status sor_create(sf_world *w);
 void sor_destroy(sf_world *w);
 sf_status step_create(sf_world *w);
 void step_destroy(sf_world *w);
+// update_cache without gravity: rotation, world inverse inertia and brick positions of awake bodies
+cudaError_t refresh_poses(sf_world *w);
 sf_status read_error_word(sf_world *w);
 }  // namespace sf

@@ -47,6 +47,10 @@ struct SorState {
     DBuf<uint32_t> cand_flag, cand_pos, cand_list;
     DBuf<uint32_t> counters;        // joints, over, failed, crushed, maxr bits, ncand
     DBuf<uint32_t> st_req;          // requested structures list for the apply pass
+    // resting-body loads
+    DBuf<float> extn, share;
+    DBuf<uint64_t> lkey, lkey_alt;
+    DBuf<uint32_t> lval, lval_alt;
     Work wk;
     uint64_t launches = 0;
     int occ = 1;
@@ -443,6 +447,81 @@ __global__ void k_stress_zero(uint32_t ns, const int32_t *sid, const uint8_t *ma
     if (s >= 0 && mat[i] != 0 && active[s]) stress[i] = 0.0f;
 }
 
+// ---------------------------------------------------------------- resting-body loads (src/lib.rs:1233-1259)
+// A body resting on bricks of listed structures spreads its weight over those bricks and the ground: each brick of
+// the body whose cell 0.29 m below holds a static brick of a listed structure counts once (ns), each brick within
+// RB + 0.05 of the ground once (nground), and every such static brick receives m / (ns + nground).
+__device__ __forceinline__ uint32_t load_target(const float4 p, uint32_t sc, const uint32_t *ctab, const uint32_t *cpool,
+                                                const uint8_t *smat, const int32_t *sid, const uint32_t *listed) {
+    const float yy = p.y - RB - 0.02f;
+    const int x = __float2int_rz(floorf(p.x / S)) + NX / 2, y = __float2int_rz(floorf(yy / S)), z = __float2int_rz(floorf(p.z / S)) + NZ / 2;
+    if (!inb(x, y, z)) return NONE;
+    const uint32_t t = ctab[(size_t)sc * NCT + chunk_slot(x, y, z)];
+    if (t == 0) return NONE;
+    const uint32_t g = cpool[(size_t)(t - 1) * 512 + cell_in_chunk(x, y, z)];
+    if (g == 0) return NONE;
+    const uint32_t j = g - 1;
+    if (smat[j] == 0) return NONE;
+    const int32_t s = sid[j];
+    return (s >= 0 && listed[s]) ? j : NONE;
+}
+
+__global__ void k_loads_share(uint32_t nb, const uint32_t *first, const uint32_t *count, const uint8_t *alive,
+                              const uint32_t *bscene, const float4 *wpos, const float *m, const uint32_t *ctab,
+                              const uint32_t *cpool, const uint8_t *smat, const int32_t *sid, const uint32_t *listed,
+                              float *share) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    float sh = 0.0f;
+    if (alive[b]) {
+        uint32_t ns = 0, ng = 0;
+        const uint32_t sc = bscene[b];
+        for (uint32_t t = 0; t < count[b]; t++) {
+            const float4 p = wpos[first[b] + t];
+            if (p.y < RB + 0.05f) ng++;
+            if (load_target(p, sc, ctab, cpool, smat, sid, listed) != NONE) ns++;
+        }
+        if (ns) sh = div_rn(m[b], (float)(ns + ng));
+    }
+    share[b] = sh;
+}
+
+__global__ void k_loads_keys(uint32_t nd, uint64_t none_key, const uint32_t *kbody, const uint32_t *bscene, const float4 *wpos,
+                             const float *share, const uint32_t *ctab, const uint32_t *cpool, const uint8_t *smat,
+                             const int32_t *sid, const uint32_t *listed, uint64_t *key, uint32_t *val) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nd) return;
+    const uint32_t b = kbody[i];
+    uint64_t k = none_key;
+    if (share[b] > 0.0f) {
+        const uint32_t j = load_target(wpos[i], bscene[b], ctab, cpool, smat, sid, listed);
+        if (j != NONE) k = j;
+    }
+    key[i] = k;
+    val[i] = i;
+}
+
+// each static brick sums its shares in body order, then brick order (the keys were sorted stably by brick id)
+__global__ void k_loads_sum(uint32_t nd, uint64_t none_key, const uint64_t *key, const uint32_t *val, const uint32_t *kbody,
+                            const float *share, float *extn) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nd) return;
+    const uint64_t k = key[p];
+    if (k >= none_key || (p > 0 && key[p - 1] == k)) return;
+    float s = 0.0f;
+    for (uint32_t q = p; q < nd && key[q] == k; q++) s += share[kbody[val[q]]];
+    extn[k] = s;
+}
+
+__global__ void k_loads_apply(uint32_t ns, const int32_t *sid, const uint8_t *mat, const uint32_t *listed, const float *extn,
+                              float *ext) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    const int32_t s = sid[i];
+    if (s < 0 || !listed[s]) return;
+    ext[i] = ext[i] * 0.8f + extn[i] * 0.2f;
+}
+
 // ---------------------------------------------------------------- host side
 sf_status sor_create(sf_world *w) {
     SorState *st = new SorState();
@@ -618,7 +697,7 @@ sf_status sf_structure_solve(sf_world *w, int32_t structure, float omega, float 
     A.chunk_sid = st->chunk_sid.p; A.work = st->work.p; A.n_work = (uint32_t)chunks.size(); A.n_struct = nst;
     A.active0 = st->active0.p; A.resid_buf = st->resid_buf.p; A.sweeps = st->sweeps.p; A.resid = st->resid.p;
     A.omega = (double)omega; A.tol = (double)tol; A.max_sweeps = max_sweeps; A.gb = w->barrier.p; A.err = w->err.p;
-    unsigned grid = (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * std::min(st->occ, 2));
+    unsigned grid = (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * st->occ);
     void *args[] = {&A};
     SF_CUDA(cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s));
     k_sor_gather<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p,
@@ -694,6 +773,46 @@ sf_status sf_structure_check(sf_world *w, int32_t structure, float dt, int32_t l
     std::memcpy(&rep.max_ratio, &c[4], 4);
     rep.ms = ms;
     if (report) *report = rep;
+    return SF_OK;
+}
+
+sf_status sf_structure_loads(sf_world *w, const int32_t *structures, uint32_t n_structures) {
+    if (!w || (n_structures && !structures)) return SF_ERR_ARG;
+    SorState *st = w->sor;
+    const uint32_t nst = w->n_struct, ns = w->ns, nd = w->nd, nb = w->nb;
+    std::vector<uint32_t> listed(std::max<uint32_t>(nst, 1), 0);
+    for (uint32_t k = 0; k < n_structures; k++) {
+        if (structures[k] < 0 || (uint32_t)structures[k] >= nst) { set_error("structure %d does not exist", structures[k]); return SF_ERR_ARG; }
+        listed[structures[k]] = 1;
+    }
+    if (ns == 0 || n_structures == 0) return SF_OK;
+    cudaStream_t s = w->stream;
+    SF_CUDA(st->active0.grow(listed.size()));
+    SF_CUDA(cudaMemcpyAsync(st->active0.p, listed.data(), listed.size() * 4, cudaMemcpyHostToDevice, s));
+    SF_CUDA(st->extn.grow(ns));
+    SF_CUDA(cudaMemsetAsync(st->extn.p, 0, (size_t)ns * 4, s));
+    if (nb && nd) {
+        // the brick positions after the last integrate (update_cache before structural, src/lib.rs:3654)
+        SF_CUDA(refresh_poses(w));
+        SF_CUDA(st->share.grow(nb));
+        SF_CUDA(st->lkey.grow(nd)); SF_CUDA(st->lkey_alt.grow(nd)); SF_CUDA(st->lval.grow(nd)); SF_CUDA(st->lval_alt.grow(nd));
+        const uint64_t none_key = ns;
+        int bits = 0;
+        while (bits < 64 && (none_key >> bits)) bits++;
+        k_loads_share<<<grid_for(nb, 128), 128, 0, s>>>(nb, w->b_first.p, w->b_count.p, w->b_alive.p, w->b_scene.p, w->k_wpos.p,
+                                                        w->b_m.p, w->ctab.p, w->cpool.p, w->s_mat.p, w->s_sid.p, st->active0.p,
+                                                        st->share.p);
+        k_loads_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, w->k_body.p, w->b_scene.p, w->k_wpos.p, st->share.p,
+                                                       w->ctab.p, w->cpool.p, w->s_mat.p, w->s_sid.p, st->active0.p,
+                                                       st->lkey.p, st->lval.p);
+        SF_CUDA(radix_sort_u64(st->lkey.p, st->lval.p, st->lkey_alt.p, st->lval_alt.p, nd, bits, st->wk, s));
+        k_loads_sum<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, st->lkey.p, st->lval.p, w->k_body.p, st->share.p, st->extn.p);
+        st->launches += 3;
+    }
+    k_loads_apply<<<grid_for(ns, 256), 256, 0, s>>>(ns, w->s_sid.p, w->s_mat.p, st->active0.p, st->extn.p, w->s_ext.p);
+    st->launches++;
+    SF_CUDA(cudaGetLastError());
+    SF_CUDA(cudaStreamSynchronize(s));
     return SF_OK;
 }
 

@@ -912,6 +912,19 @@ sf_status step_create(sf_world *w) {
     return SF_OK;
 }
 
+cudaError_t refresh_poses(sf_world *w) {
+    const uint32_t nb = w->nb, nd = w->nd;
+    if (nb == 0 || nd == 0) return cudaSuccess;
+    cudaStream_t s = w->stream;
+    // h = 0: v.y - 0 leaves every velocity bit unchanged
+    k_update_cache<<<grid_for(nb, 128), 128, 0, s>>>(nb, 0.0f, w->b_alive.p, w->b_asleep.p, w->b_q.p, w->b_iil.p, w->b_rot.p,
+                                                     w->b_iiw.p, w->b_v.p);
+    k_brick_pos<<<grid_for(nd, 256), 256, 0, s>>>(nd, w->k_body.p, w->b_alive.p, w->b_asleep.p, w->b_pos.p, w->b_rot.p,
+                                                  w->k_local.p, w->k_wpos.p);
+    w->launches += 2;
+    return cudaGetLastError();
+}
+
 void step_destroy(sf_world *w) {
     if (w->step && w->step->h_dev) cudaFreeHost(w->step->h_dev);
     delete w->step;

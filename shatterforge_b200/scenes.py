@@ -185,6 +185,81 @@ def config1_scene(seed: int = 1, n_debris: int = 1024, removed: bool = False) ->
     return frame.contiguous()
 
 
+def config2_tower(seed: int = 2, remove_columns: int = 8):
+    """Config 2: a 16-storey tower on 48 x 48 cells, storeys of 7 cells. Per storey: 6-cell concrete columns on a
+    5 x 5 grid at 12-cell spacing, glass infill panels (6 cells high, non-bearing) in alternate 2-cell bays of the
+    perimeter, and a 48 x 48 slab whose outer ring is masonry (the 1-brick perimeter) and whose inside is concrete.
+    16 * (25 * 6 + 534 + 2304) = 47,808 bricks, structure 0. Returns (scene, removed_mask) where removed_mask marks
+    the bricks of `remove_columns` seed-chosen ground-storey columns."""
+    rng = XorShift32(seed)
+    W, H, storeys = 48, 7, 16
+    x0, z0 = ORIGIN[0] - W // 2, ORIGIN[2] - W // 2
+    cols = [0, 12, 24, 36, 47]
+    ring = [(x, 0) for x in range(W)] + [(W - 1, z) for z in range(1, W)] + \
+           [(x, W - 1) for x in range(W - 2, -1, -1)] + [(0, z) for z in range(W - 2, 0, -1)]
+    colset = {(cx, cz) for cx in cols for cz in cols}
+    bays = [c for k, c in enumerate(ring) if (k // 2) % 2 == 1 and c not in colset]
+    xyz, mat = [], []
+    for s in range(storeys):
+        yb = s * H
+        for cx in cols:
+            for cz in cols:
+                for y in range(yb, yb + H - 1):
+                    xyz.append((x0 + cx, y, z0 + cz)); mat.append(CONC)
+        for (bx, bz) in bays:
+            for y in range(yb, yb + H - 1):
+                xyz.append((x0 + bx, y, z0 + bz)); mat.append(GLASS)
+        ys = yb + H - 1
+        for x in range(W):
+            for z in range(W):
+                edge = x == 0 or z == 0 or x == W - 1 or z == W - 1
+                xyz.append((x0 + x, ys, z0 + z)); mat.append(MASON if edge else CONC)
+    xyz = np.array(xyz, np.int32)
+    mat = np.array(mat, np.uint8)
+    inf = (mat == GLASS).astype(np.uint8)
+    sc = Scene(xyz, mat, np.zeros(len(mat), np.int32), inf, name="tower16").contiguous()
+    ground_cols = [(x0 + cx, z0 + cz) for cx in cols for cz in cols]
+    chosen = []
+    while len(chosen) < remove_columns:
+        k = int(rng.rnd() * len(ground_cols)) % len(ground_cols)
+        if k not in chosen:
+            chosen.append(k)
+    removed = np.zeros(sc.n_static, bool)
+    for k in chosen:
+        cx, cz = ground_cols[k]
+        removed |= (xyz[:, 0] == cx) & (xyz[:, 2] == cz) & (xyz[:, 1] < H - 1)
+    return sc, removed
+
+
+def config2_scene(seed: int = 2, n_bodies: int = 30000, removed: bool = True, kmax: int = 512,
+                  lift: float = 60.0) -> Scene:
+    """Config 2 with its debris: the tower (ground columns removed) plus a pre-fragmented body set of n compound
+    bodies of 1-512 bricks (k ~ Geometric(0.3), a few large slabs) falling beside and onto it from `lift` m above
+    the config-4 spawn layers (the roof is at 56 m)."""
+    tower, rm = config2_tower(seed)
+    if removed:
+        tower = tower.without_static(rm)
+    lib = ClusterLibrary(seed ^ 0x1B873593, kmax=kmax)
+    deb = debris_scene(n_bodies, seed * 7919 + 1, lib=lib, kmax=kmax, obstacles=(0, 0), spacing=2.0)
+    big = max(1, n_bodies // 500)
+    ks = np.diff(deb.body_first.astype(np.int64))
+    # a few large fragments (slab pieces of up to kmax bricks) stand for the bodies a collapse sheds
+    rng = np.random.default_rng(seed + 17)
+    sel = rng.choice(n_bodies, big, replace=False)
+    ks[sel] = rng.integers(kmax // 4, kmax + 1, big)
+    picks = rng.integers(0, 1 << 30, n_bodies)
+    cl, _ = lib.gather(ks, picks)
+    first = np.zeros(n_bodies + 1, np.uint32)
+    first[1:] = np.cumsum(ks)
+    bmat = np.repeat(np.array((CONC, MASON, WOOD), np.uint8)[rng.integers(0, 3, n_bodies)], ks)
+    pose = deb.body_pose.copy()
+    pose[:, 1] += lift
+    tower.body_first, tower.body_brick_xyz = first, (cl + np.array(ORIGIN, np.int32)).astype(np.int32)
+    tower.body_brick_mat, tower.body_pose = bmat, pose
+    tower.name = "config2"
+    return tower.contiguous()
+
+
 # ---------------------------------------------------------------- compound debris (config 4)
 _NBR = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]], np.int32)
 

@@ -66,6 +66,14 @@ def test_generators_config_shapes():
     d = S.debris_scene(500, seed=7)
     assert d.n_bodies == 500 and d.body_first[-1] == d.n_body_bricks
     assert d.n_static > 0 and (d.static_sid == -1).all()
+    t, trm = S.config2_tower()
+    assert t.n_static == 47808 and trm.sum() == 48
+    assert (t.static_infill == (t.static_mat == S.GLASS)).all() and t.static_infill.sum() == 16 * 534
+    t2 = t.without_static(trm)
+    assert S.grounded_mask(t2.static_xyz, t2.static_mat, t2.static_sid, t2.static_infill).all()
+    c2 = S.config2_scene(n_bodies=600)
+    ks = np.diff(c2.body_first.astype(np.int64))
+    assert c2.n_bodies == 600 and ks.min() >= 1 and ks.max() <= 512 and ks.max() >= 128
 
 
 def test_xorshift_matches_reference_stream():

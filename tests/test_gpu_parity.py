@@ -125,6 +125,27 @@ def test_joint_decisions_bit_exact(sf, oracle, case):
         assert rep.over > 0
 
 
+def test_resting_loads_bit_exact(sf, oracle):
+    """Debris falls on the 5-storey frame's roof; the loads it puts on the structure match the oracle's, computed
+    from the same state (bodies and brick positions)."""
+    frame, _ = S.config1_frame()
+    bf, bxyz, bmat, pose = S.loose_debris(300, seed=17, box_lo=(-5.0, 19.0, -5.0), box_hi=(5.0, 23.0, 5.0))
+    frame.body_first, frame.body_brick_xyz, frame.body_brick_mat, frame.body_pose = bf, bxyz, bmat, pose
+    sc = frame.contiguous()
+    w = sf.World(sc, iterations=8)
+    w.step(1 / 60, nsteps=100)
+    st, sl, fl = w.bodies()
+    ow = oracle.OracleWorld(sc)
+    ow.set_bodies(st, sl, fl)
+    ow.set_brick_positions(w.brick_positions())
+    for _ in range(3):
+        w.structure_loads([0])
+        ow.structure_loads([0])
+    e, oe = w.ext(), ow.ext()
+    assert (oe > 0).sum() > 20
+    np.testing.assert_array_equal(e, oe)
+
+
 # ---------------------------------------------------------------- rigid step
 def _compare_step_outputs(w, ow, scene=0):
     ids, f, s = w.contacts(scene)
@@ -291,3 +312,56 @@ def test_box_sat_bit_exact(sf, oracle):
             np.testing.assert_array_equal(nrm[i], onrm)
             np.testing.assert_array_equal(pts[i, :on], opts)
     assert hits > n // 4
+
+
+# ---------------------------------------------------------------- config 2: 16-storey tower with glass infill
+def test_config2_tower_sor_bit_exact(sf, oracle):
+    """The tower with 8 ground columns removed (47,760 bricks, infill panels that bond only downwards): the same
+    red-black FP64 sweeps on both sides, stopped at the same sweep count."""
+    sc, rm = S.config2_tower()
+    sc = sc.without_static(rm)
+    w = sf.World(sc)
+    rep = w.structure_solve(0, omega=1.7, tol=1e-9, max_sweeps=3000)
+    sw, rs = w.solve_detail()
+    ow = oracle.OracleWorld(sc)
+    osw, ors = ow.sor(0, 1.7, 1e-9, 3000, mode=oracle.MODE_REDBLACK_F64)
+    assert sw[0] == osw == 3000 and rep.max_sweeps_done == 3000
+    assert rs[0] == ors
+    np.testing.assert_array_equal(w.phi64(), ow.phi64())
+
+
+def test_config2_tower_joints_bit_exact(sf, oracle):
+    sc, rm = S.config2_tower()
+    sc = sc.without_static(rm)
+    w = sf.World(sc)
+    rep = w.structure_solve(0, omega=1.7, tol=1e-6, max_sweeps=200000)
+    assert rep.max_residual < 1e-6
+    ow = oracle.OracleWorld(sc)
+    ow.set_phi(w.phi())
+    ids, vals, mr = ow.stress(0, dt=1 / 60, live=True)
+    rep = w.structure_check(0, dt=1 / 60, live=True)
+    r, b, d, k = w.joints()
+    odec, orat, obnd, ocr = _joint_table(ids, vals, sc.n_static)
+    np.testing.assert_array_equal(d, odec)
+    present = odec != 255
+    np.testing.assert_array_equal(r[present], orat[present])
+    np.testing.assert_array_equal(b[present], obnd[present])
+    np.testing.assert_array_equal(k[odec == 3], ocr[odec == 3])
+    assert rep.max_ratio == mr
+
+
+def test_config2_compound_bodies_bit_exact(sf, oracle):
+    """Compound fragments of 1-512 bricks land on the tower's roof and around it: 100 steps, bit-exact."""
+    sc = S.config2_scene(n_bodies=1500, lift=54.0)
+    w = sf.World(sc, iterations=8)
+    ow = oracle.OracleWorld(sc)
+    for _ in range(100):
+        w.step(1 / 60)
+        ow.step(1 / 60, iterations=8, order=oracle.ORDER_COLOR)
+    st, sl, fl = w.bodies()
+    ost, osl, ofl = ow.bodies()
+    np.testing.assert_array_equal(fl, ofl)
+    np.testing.assert_array_equal(st, ost)
+    np.testing.assert_array_equal(sl, osl)
+    _compare_step_outputs(w, ow)
+    assert w.stats().contacts > 100

@@ -83,6 +83,22 @@ def test_reference_f32_sweeps_reach_residual(oracle):
         assert np.abs(w.phi() - exact).max() / exact.max() < 1e-3
 
 
+def test_resting_load_closed_form(oracle):
+    """structural's body loads (src/lib.rs:1233-1259): a 300 kg brick resting on one structure brick, clear of the
+    ground, puts its whole weight share on that brick: ext = 0.8 * 0 + 0.2 * 300."""
+    xyz = np.array([[S.ORIGIN[0], 0, S.ORIGIN[2]]], np.int32)
+    pose = np.zeros((1, 13), np.float32)
+    pose[0, :3] = [0.0, 0.5, 0.0]          # brick centre (0.25, 0.75, 0.25): the cell 0.29 m below is the static one
+    pose[0, 6] = 1.0
+    sc = S.Scene(xyz, np.array([S.CONC], np.uint8), np.zeros(1, np.int32), np.zeros(1, np.uint8),
+                 np.array([0, 1], np.uint32), np.array([S.ORIGIN], np.int32), np.array([S.CONC], np.uint8), pose).contiguous()
+    w = oracle.OracleWorld(sc)
+    w.structure_loads([0])
+    assert w.ext()[0] == np.float32(0.2) * np.float32(300.0)
+    w.structure_loads([0])
+    assert w.ext()[0] == np.float32(np.float32(0.2) * np.float32(300.0) * np.float32(0.8) + np.float32(0.2) * np.float32(300.0))
+
+
 def test_oracle_rest_contacts(oracle):
     """A single brick resting on the ground: its 4 lower cube corners touch, normal +y (src/lib.rs:1415-1421)."""
     pose = np.zeros((1, 13), np.float32)
