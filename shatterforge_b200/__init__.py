@@ -97,6 +97,7 @@ PROTOTYPES = {
     "sf_last_error": (C.c_char_p, []),
     "sf_version": (C.c_int32, []),
     "sf_world_step": (C.c_int32, [C.c_void_p, C.c_float, C.c_uint32]),
+    "sf_world_step_scenes": (C.c_int32, [C.c_void_p, C.c_float, C.c_uint32, C.POINTER(C.c_uint8)]),
     "sf_world_set_stream": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "sf_set_profiling": (C.c_int32, [C.c_void_p, C.c_int32]),
     "sf_read_profile": (C.c_int32, [C.c_void_p, C.POINTER(Profile)]),
@@ -283,6 +284,14 @@ class World:
     # -- hot path
     def step(self, dt: float = 1.0 / 60.0, nsteps: int = 1) -> "Stats":
         _check(self._lib.sf_world_step(self._h, float(dt), int(nsteps)), "sf_world_step")
+        return self.stats()
+
+    def step_scenes(self, mask, dt: float = 1.0 / 60.0, nsteps: int = 1) -> "Stats":
+        """Step only the scenes whose mask entry is non-zero; the others stay exactly as they are."""
+        m = np.ascontiguousarray(mask, np.uint8)
+        if m.shape != (len(self.scenes),):
+            raise ValueError(f"mask has shape {m.shape}, the world has {len(self.scenes)} scenes")
+        _check(self._lib.sf_world_step_scenes(self._h, float(dt), int(nsteps), _ptr(m, C.c_uint8)), "sf_world_step_scenes")
         return self.stats()
 
     def structure_solve(self, structure: int = -1, omega: float = 1.7, tol: float = 1e-6, max_sweeps: int = 20000) -> SolveReport:

@@ -59,6 +59,16 @@ struct StepState {
     DBuf<uint32_t> parent, label, mint;
     // per-scene body offsets (for scene-local priorities)
     DBuf<uint32_t> body_off_of_body;
+    // the active set of the current step
+    DBuf<uint32_t> act_body, act_brick, cidx, scene_act, man_ca, man_cb;
+    DBuf<uint4> seg;
+    DBuf<uint8_t> live_dev;
+    uint8_t *h_live_pin = nullptr;          // pinned mirror of live_dev
+    std::vector<uint8_t> live;              // per scene: an awake body at the end of the last step
+    std::vector<uint32_t> act;              // active scenes, ascending
+    std::vector<uint32_t> act_brick_base;   // per scene: first active-list brick of the last substep, NONE if idle
+    uint32_t nb_act = 0, nd_act = 0;
+    bool act_valid = false;
     // device scalars: [0] contacts, [1] manifolds, [2] colours, [3] rounds, [4..6] jp counts, [7] alive, [8] awake,
     // [9] islands
     DBuf<uint32_t> dev;
@@ -91,10 +101,17 @@ enum { DV_CONTACTS = 0, DV_MANIFOLDS = 1, DV_COLORS = 2, DV_ROUNDS = 3, DV_WL0 =
        DV_ALIVE = 7, DV_AWAKE = 8, DV_ISLANDS = 9, DV_PAIRS = 10, DV_N = 16 };
 
 // ---------------------------------------------------------------- pose cache
-__global__ void k_update_cache(uint32_t nb, float h, const uint8_t *alive, const uint8_t *asleep, const float4 *q,
-                               const float *iil, float *rot, float *iiw, float4 *v) {
-    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb || !alive[b] || asleep[b]) return;
+// Kernels over bodies or bricks take the substep's active list (global ids of the bodies / bricks of the scenes
+// that step); a null list means every body / brick of the world.
+__device__ __forceinline__ uint32_t pick(const uint32_t *list, uint32_t t) { return list ? list[t] : t; }
+
+__global__ void k_update_cache(uint32_t nb, const uint32_t *list, float h, const uint8_t *alive, const uint8_t *asleep,
+                               const float4 *q, const float *iil, float *rot, float *iiw, float4 *v, uint32_t *bnc) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    const uint32_t b = pick(list, t);
+    if (bnc) bnc[b] = 0;
+    if (!alive[b] || asleep[b]) return;
     float4 qq = q[b];
     float r[9], il[9], t1[9], t2[9], t3[9];
     q_to_m(qq.x, qq.y, qq.z, qq.w, r);
@@ -110,10 +127,11 @@ __global__ void k_update_cache(uint32_t nb, float h, const uint8_t *alive, const
     v[b] = vv;
 }
 
-__global__ void k_brick_pos(uint32_t nd, const uint32_t *kbody, const uint8_t *alive, const uint8_t *asleep,
-                            const float4 *pos, const float *rot, const float4 *local, float4 *wpos) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nd) return;
+__global__ void k_brick_pos(uint32_t nd, const uint32_t *list, const uint32_t *kbody, const uint8_t *alive,
+                            const uint8_t *asleep, const float4 *pos, const float *rot, const float4 *local, float4 *wpos) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nd) return;
+    const uint32_t i = pick(list, t);
     uint32_t b = kbody[i];
     if (!alive[b] || asleep[b]) return;
     float r[9];
@@ -126,18 +144,21 @@ __global__ void k_brick_pos(uint32_t nd, const uint32_t *kbody, const uint8_t *a
 
 __device__ __forceinline__ int floor_cell(float x) { return __float2int_rz(floorf(x / S)); }
 
-__global__ void k_cell_keys(uint32_t nd, uint64_t none_key, const uint32_t *kbody, const uint32_t *bscene,
-                            const uint8_t *alive, const float4 *wpos, uint64_t *key, uint32_t *val) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nd) return;
+// key = (the scene's index in the active set, hashed cell); bricks of dead bodies sort last
+__global__ void k_cell_keys(uint32_t nd, const uint32_t *list, uint64_t none_key, const uint32_t *kbody,
+                            const uint32_t *bscene, const uint32_t *scene_act, const uint8_t *alive, const float4 *wpos,
+                            uint64_t *key, uint32_t *val) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nd) return;
+    const uint32_t i = pick(list, t);
     uint32_t b = kbody[i];
     uint64_t k = none_key;
     if (alive[b]) {
         float4 p = wpos[i];
-        k = (uint64_t)bscene[b] * HSIZE + hkey(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z));
+        k = (uint64_t)scene_act[bscene[b]] * HSIZE + hkey(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z));
     }
-    key[i] = k;
-    val[i] = i;
+    key[t] = k;
+    val[t] = i;
 }
 
 __global__ void k_bucket_ranges(uint32_t nd, uint64_t none_key, const uint64_t *key, uint2 *brange) {
@@ -164,7 +185,8 @@ __global__ void k_bucket_records(uint32_t nd, const uint32_t *cval, const uint32
 
 // ---------------------------------------------------------------- contacts
 struct ContactArgs {
-    uint32_t nd;
+    uint32_t nd;                       // active bricks
+    const uint32_t *list, *scene_act;  // active brick -> global brick; scene -> index in the active set
     const uint32_t *kbody, *bscene, *ctab, *cpool;
     const int4 *sbox;
     const uint8_t *alive, *asleep, *smat;
@@ -176,7 +198,7 @@ struct ContactArgs {
     uint32_t *ccount;
     const uint32_t *coff;
     uint8_t *wake;
-    // slot scratch, slot-major: slot k of brick i at k * nd + i
+    // slot scratch, slot-major: slot k of active brick t at k * nd + t
     uint4 *slot_id;
     float4 *slot_p, *slot_n;
     uint32_t *L_a, *L_b, *L_bo, *L_ba, *L_bb;
@@ -252,6 +274,7 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
     // brick id down is the reference's chain order
     {
         const int hx = floor_cell(p.x), hy = floor_cell(p.y), hz = floor_cell(p.z);
+        const uint32_t sk = A.scene_act[sc];
         float speed = 0.0f;
         if (WAKE) {
             const float4 vv = A.v[a], ww = A.w[a];
@@ -261,7 +284,7 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
         for (int dz = -1; dz <= 1; dz++)
             for (int dy = -1; dy <= 1; dy++)
                 for (int dx = -1; dx <= 1; dx++) {
-                    const uint2 rg = A.brange[(size_t)sc * HSIZE + hkey(hx + dx, hy + dy, hz + dz)];
+                    const uint2 rg = A.brange[(size_t)sk * HSIZE + hkey(hx + dx, hy + dy, hz + dz)];
                     for (uint32_t q = rg.y; q > rg.x; q--) {
                         const uint32_t info = A.sinfo[q - 1];
                         const uint32_t bj = info & 0x3FFFFFFFu;
@@ -289,15 +312,16 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
 
 // pass 1: every contact of every awake brick counted; the first CSLOTS kept in the brick's slots
 __global__ void __launch_bounds__(128, 8) k_contacts_gen(ContactArgs A) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.nd) return;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= A.nd) return;
+    const uint32_t i = pick(A.list, t);
     const uint32_t a = A.kbody[i];
-    if (!A.alive[a] || A.asleep[a]) { A.ccount[i] = 0; return; }
+    if (!A.alive[a] || A.asleep[a]) { A.ccount[t] = 0; return; }
     uint32_t n = 0;
     const size_t nd = A.nd;
     auto emit = [&](uint32_t b, uint32_t bo, uint32_t bb, V3 cp, V3 nn, float depth) {
         if (n < CSLOTS) {
-            const size_t o = (size_t)n * nd + i;
+            const size_t o = (size_t)n * nd + t;
             A.slot_id[o] = make_uint4(b, bo, bb, 0u);
             A.slot_p[o] = make_float4(cp.x, cp.y, cp.z, depth);
             A.slot_n[o] = make_float4(nn.x, nn.y, nn.z, 0.0f);
@@ -305,21 +329,22 @@ __global__ void __launch_bounds__(128, 8) k_contacts_gen(ContactArgs A) {
         n++;
     };
     gen_brick<true>(A, i, a, emit);
-    A.ccount[i] = n;
+    A.ccount[t] = n;
 }
 
 // pass 2: each brick's contacts to their place in the list; a brick with more than CSLOTS regenerates them
 __global__ void __launch_bounds__(128) k_contacts_place(ContactArgs A) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.nd) return;
-    const uint32_t n = A.ccount[i];
+    const uint32_t ta = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ta >= A.nd) return;
+    const uint32_t n = A.ccount[ta];
     if (n == 0) return;
+    const uint32_t i = pick(A.list, ta);
     const uint32_t a = A.kbody[i];
-    const uint32_t base = A.coff[i];
+    const uint32_t base = A.coff[ta];
     const size_t nd = A.nd;
     if (n <= CSLOTS) {
         for (uint32_t k = 0; k < n; k++) {
-            const size_t o = (size_t)k * nd + i;
+            const size_t o = (size_t)k * nd + ta;
             const uint4 id = A.slot_id[o];
             const float4 pp = A.slot_p[o], nn = A.slot_n[o];
             const uint32_t t = base + k;
@@ -377,14 +402,16 @@ __global__ void k_chunk_flags(uint32_t nc, uint32_t K, const uint32_t *flag, con
 }
 __global__ void k_man_write(uint32_t nc, uint32_t K, const uint32_t *cflag, const uint32_t *cpos, const uint32_t *flag,
                             const uint32_t *pos, const uint32_t *pair_start, const uint32_t *perm, const uint32_t *L_a,
-                            const uint32_t *L_b, const uint32_t *body_off_of_body, uint32_t *man_a, uint32_t *man_b,
-                            uint32_t *man_start, uint32_t *man_prio) {
+                            const uint32_t *L_b, const uint32_t *body_off_of_body, const uint32_t *cidx,
+                            uint32_t *man_a, uint32_t *man_b, uint32_t *man_ca, uint32_t *man_cb, uint32_t *man_start,
+                            uint32_t *man_prio) {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nc || !cflag[t]) return;
     uint32_t m = cpos[t];
     uint32_t k = perm[t];
     uint32_t a = L_a[k], b = L_b[k];
     man_a[m] = a; man_b[m] = b; man_start[m] = t;
+    man_ca[m] = cidx[a]; man_cb[m] = b == STATIC ? STATIC : cidx[b];
     uint32_t off = body_off_of_body[a];
     uint32_t h = pair_priority(a - off, b == STATIC ? 0u : b - off + 1u);
     const uint32_t j = K ? (t - pair_start[pos[t] + flag[t] - 1]) / K : 0u;
@@ -472,6 +499,8 @@ __global__ void k_prep(PrepArgs A) {
 }
 
 // ---------------------------------------------------------------- colouring
+// The body-to-manifold lists and the colour masks are indexed by the body's place in the substep's active list
+// (man_ca / man_cb), so their size and clearing follow the active bodies only.
 __global__ void k_bm_count(const uint32_t *nm_p, const uint32_t *man_a, const uint32_t *man_b, uint32_t *bm_count) {
     uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= *nm_p) return;
@@ -491,7 +520,7 @@ __global__ void k_bm_fill(const uint32_t *nm_p, const uint32_t *man_a, const uin
 
 struct JpArgs {
     const uint32_t *nm_p;
-    const uint32_t *man_a, *man_b, *prio, *bm_start, *bm_list;
+    const uint32_t *man_a, *man_b, *prio, *bm_start, *bm_list;   // man_a / man_b: active-list body ids
     uint32_t *man_round, *man_color, *masks;
     uint32_t *wl0, *wl1, *dev;
     uint32_t max_colors, max_rounds;
@@ -680,9 +709,10 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) k_solve(SolveArgs A) {
 }
 
 // ---------------------------------------------------------------- islands
-__global__ void k_uf_init(uint32_t nb, uint32_t *parent, uint32_t *mint) {
-    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
+__global__ void k_uf_init(uint32_t nb, const uint32_t *list, uint32_t *parent, uint32_t *mint) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    const uint32_t b = pick(list, t);
     parent[b] = b;
     mint[b] = 0x7f7fffffu;
 }
@@ -710,10 +740,11 @@ __global__ void k_uf_union(const uint32_t *nm_p, const uint32_t *man_a, const ui
         if (atomicCAS(&parent[x], x, y) == x) return;
     }
 }
-__global__ void k_uf_label(uint32_t nb, const uint8_t *alive, const uint8_t *asleep, uint32_t *parent, uint32_t *label,
-                           uint32_t *dev) {
-    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
+__global__ void k_uf_label(uint32_t nb, const uint32_t *list, const uint8_t *alive, const uint8_t *asleep, uint32_t *parent,
+                           uint32_t *label, uint32_t *dev) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    const uint32_t b = pick(list, t);
     if (!alive[b] || asleep[b]) { label[b] = NONE; return; }
     uint32_t r = uf_find(parent, b);
     label[b] = r;
@@ -723,6 +754,7 @@ __global__ void k_uf_label(uint32_t nb, const uint8_t *alive, const uint8_t *asl
 // ---------------------------------------------------------------- pinch clamps + integrate
 struct IntArgs {
     uint32_t nb;
+    const uint32_t *list;
     float h;
     int pinch_kill, island_mode;
     uint8_t *alive, *asleep;
@@ -738,8 +770,10 @@ struct IntArgs {
 __device__ __forceinline__ void kill_mark(const IntArgs &A, uint32_t b) { A.alive[b] = 0; }
 
 __global__ void k_integrate(IntArgs A) {
-    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= A.nb || !A.alive[b] || A.asleep[b]) return;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= A.nb) return;
+    const uint32_t b = pick(A.list, t);
+    if (!A.alive[b] || A.asleep[b]) return;
     float4 t4 = A.v[b];
     V3 v = v3(t4.x, t4.y, t4.z);
     t4 = A.w[b];
@@ -813,17 +847,20 @@ __global__ void k_integrate(IntArgs A) {
     if (p.y < -15.0f || fabsf(p.x) > 190.0f || fabsf(p.z) > 190.0f || p.y > 120.0f) A.alive[b] = 0;
 }
 
-__global__ void k_island_min(uint32_t nb, const uint8_t *alive, const uint32_t *label, const float *sleep, uint32_t *mint) {
-    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
+__global__ void k_island_min(uint32_t nb, const uint32_t *list, const uint8_t *alive, const uint32_t *label,
+                             const float *sleep, uint32_t *mint) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    const uint32_t b = pick(list, t);
     uint32_t r = label[b];
     if (r == NONE || !alive[b]) return;
     atomicMin(&mint[r], __float_as_uint(sleep[b]));
 }
-__global__ void k_island_sleep(uint32_t nb, const uint8_t *alive, uint8_t *asleep, const uint32_t *label, const float *sleep,
-                               const uint32_t *mint, float4 *v, float4 *w) {
-    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
+__global__ void k_island_sleep(uint32_t nb, const uint32_t *list, const uint8_t *alive, uint8_t *asleep,
+                               const uint32_t *label, const float *sleep, const uint32_t *mint, float4 *v, float4 *w) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    const uint32_t b = pick(list, t);
     uint32_t r = label[b];
     if (r == NONE || !alive[b] || asleep[b]) return;
     if (__uint_as_float(mint[r]) > 0.45f || sleep[b] > 0.9f) {
@@ -832,15 +869,21 @@ __global__ void k_island_sleep(uint32_t nb, const uint8_t *alive, uint8_t *aslee
         w[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
 }
-__global__ void k_wake(uint32_t nb, uint8_t *wake, const uint8_t *alive, uint8_t *asleep, float *sleep) {
-    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb || !wake[b]) return;
+__global__ void k_wake(uint32_t nb, const uint32_t *list, uint8_t *wake, const uint8_t *alive, uint8_t *asleep,
+                       float *sleep) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    const uint32_t b = pick(list, t);
+    if (!wake[b]) return;
     wake[b] = 0;
     if (alive[b]) { asleep[b] = 0; sleep[b] = 0.0f; }
 }
-__global__ void k_save_pre(uint32_t nb, const uint8_t *alive, const float4 *v, const float4 *w, float4 *vpre, float4 *wpre) {
-    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb || !alive[b]) return;
+__global__ void k_save_pre(uint32_t nb, const uint32_t *list, const uint8_t *alive, const float4 *v, const float4 *w,
+                           float4 *vpre, float4 *wpre) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    const uint32_t b = pick(list, t);
+    if (!alive[b]) return;
     vpre[b] = v[b];
     wpre[b] = w[b];
 }
@@ -856,10 +899,47 @@ __global__ void k_count_bodies(uint32_t nb, const uint8_t *alive, const uint8_t 
     }
 }
 // the kill of a body also removes its bricks (kill_body, src/lib.rs:826-843)
-__global__ void k_kill_bricks(uint32_t nd, const uint32_t *kbody, const uint8_t *alive, uint8_t *kmat) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nd) return;
+__global__ void k_kill_bricks(uint32_t nd, const uint32_t *list, const uint32_t *kbody, const uint8_t *alive, uint8_t *kmat) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nd) return;
+    const uint32_t i = pick(list, t);
     if (!alive[kbody[i]]) kmat[i] = 0;
+}
+
+// ---------------------------------------------------------------- the active set
+// Scenes step only while one of their bodies is awake: a scene whose bodies all sleep (or are dead) is left
+// unchanged by a substep (gen_contacts, integrate and the islands all skip sleeping bodies), so leaving it out is
+// exact. A caller may also hold scenes out (a served pool steps only the scenes with work). The active scenes'
+// bodies and bricks are listed in scene order; seg[k] = (body_off, body_base, brick_off, brick_base) of the k-th.
+__device__ __forceinline__ uint32_t seg_of(const uint4 *seg, uint32_t K, uint32_t t, bool bricks) {
+    uint32_t lo = 0, hi = K;   // last k with base <= t
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t base = bricks ? seg[mid].w : seg[mid].y;
+        if (base <= t) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+__global__ void k_build_lists(uint32_t K, const uint4 *seg, uint32_t nb_act, uint32_t nd_act, uint32_t *act_body,
+                              uint32_t *cidx, uint32_t *act_brick) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nb_act) {
+        const uint4 g = seg[seg_of(seg, K, t, false)];
+        const uint32_t b = g.x + (t - g.y);
+        act_body[t] = b;
+        cidx[b] = t;
+    }
+    if (t < nd_act) {
+        const uint4 g = seg[seg_of(seg, K, t, true)];
+        act_brick[t] = g.z + (t - g.w);
+    }
+}
+__global__ void k_scene_live(uint32_t nb, const uint32_t *list, const uint8_t *alive, const uint8_t *asleep,
+                             const uint32_t *bscene, uint8_t *live) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    const uint32_t b = pick(list, t);
+    if (alive[b] && !asleep[b]) live[bscene[b]] = 1;
 }
 
 // ---------------------------------------------------------------- host side
@@ -872,7 +952,7 @@ static cudaError_t grow_contacts(StepState *S, uint64_t need) {
 #define G(buf) if ((e = S->buf.alloc(cap)) != cudaSuccess) return e
     G(L_a); G(L_b); G(L_bo); G(L_ba); G(L_bb); G(L_p); G(L_n);
     G(mkey); G(mkey_alt); G(perm); G(perm_alt); G(invperm); G(mflag); G(mpos); G(pair_start); G(cflag); G(cpos);
-    G(man_a); G(man_b); G(man_start); G(man_count); G(man_prio); G(man_color); G(man_round);
+    G(man_a); G(man_b); G(man_ca); G(man_cb); G(man_start); G(man_count); G(man_prio); G(man_color); G(man_round);
     G(S_n); G(S_t1); G(S_t2); G(S_ra); G(S_rb); G(S_j);
     G(wl0); G(wl1); G(col_list);
 #undef G
@@ -885,9 +965,10 @@ sf_status step_create(sf_world *w) {
     StepState *S = new StepState();
     w->step = S;
     uint32_t nb = w->nb, nd = w->nd;
+    const uint32_t nsc = std::max<uint32_t>(w->n_scenes, 1);
     cudaStream_t s = w->stream;
     SF_CUDA(S->ckey.alloc(nd)); SF_CUDA(S->ckey_alt.alloc(nd)); SF_CUDA(S->cval.alloc(nd)); SF_CUDA(S->cval_alt.alloc(nd));
-    SF_CUDA(S->brange.alloc((size_t)w->n_scenes * HSIZE));
+    SF_CUDA(S->brange.alloc((size_t)nsc * HSIZE));
     SF_CUDA(S->srec.alloc(nd)); SF_CUDA(S->sinfo.alloc(nd));
     SF_CUDA(S->slot_id.alloc((size_t)nd * CSLOTS)); SF_CUDA(S->slot_p.alloc((size_t)nd * CSLOTS)); SF_CUDA(S->slot_n.alloc((size_t)nd * CSLOTS));
     SF_CUDA(S->ccount.alloc((size_t)nd + 1)); SF_CUDA(S->coff.alloc((size_t)nd + 1));
@@ -896,7 +977,13 @@ sf_status step_create(sf_world *w) {
     SF_CUDA(S->col_count.alloc(MAXCOL + 2)); SF_CUDA(S->col_start.alloc(MAXCOL + 2)); SF_CUDA(S->col_fill.alloc(MAXCOL + 2));
     SF_CUDA(S->parent.alloc(nb)); SF_CUDA(S->label.alloc(nb)); SF_CUDA(S->mint.alloc(nb));
     SF_CUDA(cudaMemsetAsync(S->label.p, 0xFF, S->label.bytes(), s));
+    SF_CUDA(S->act_body.alloc(nb)); SF_CUDA(S->cidx.alloc(nb)); SF_CUDA(S->act_brick.alloc(nd));
+    SF_CUDA(S->scene_act.alloc(nsc)); SF_CUDA(S->seg.alloc(nsc)); SF_CUDA(S->live_dev.alloc(nsc));
+    SF_CUDA(cudaMallocHost((void **)&S->h_live_pin, nsc));
+    S->live.assign(w->n_scenes, 1);   // every scene steps until a step shows it asleep
+    S->act_brick_base.assign(w->n_scenes, NONE);
     SF_CUDA(S->dev.alloc(DV_N));
+    SF_CUDA(cudaMemsetAsync(S->dev.p, 0, S->dev.bytes(), s));
     SF_CUDA(cudaMallocHost((void **)&S->h_dev, DV_N * sizeof(uint32_t)));
     std::vector<uint32_t> off(nb);
     for (const Scene &sc : w->scenes) for (uint32_t b = 0; b < sc.n_bodies; b++) off[sc.body_off + b] = sc.body_off;
@@ -909,6 +996,7 @@ sf_status step_create(sf_world *w) {
     S->solve_occ = std::max(1, occ);
     SF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jp, 256, 0));
     S->jp_occ = std::max(1, occ);
+    SF_CUDA(cudaStreamSynchronize(s));   // the host vector `off` is the copy's source
     return SF_OK;
 }
 
@@ -917,40 +1005,109 @@ cudaError_t refresh_poses(sf_world *w) {
     if (nb == 0 || nd == 0) return cudaSuccess;
     cudaStream_t s = w->stream;
     // h = 0: v.y - 0 leaves every velocity bit unchanged
-    k_update_cache<<<grid_for(nb, 128), 128, 0, s>>>(nb, 0.0f, w->b_alive.p, w->b_asleep.p, w->b_q.p, w->b_iil.p, w->b_rot.p,
-                                                     w->b_iiw.p, w->b_v.p);
-    k_brick_pos<<<grid_for(nd, 256), 256, 0, s>>>(nd, w->k_body.p, w->b_alive.p, w->b_asleep.p, w->b_pos.p, w->b_rot.p,
-                                                  w->k_local.p, w->k_wpos.p);
+    k_update_cache<<<grid_for(nb, 128), 128, 0, s>>>(nb, nullptr, 0.0f, w->b_alive.p, w->b_asleep.p, w->b_q.p, w->b_iil.p,
+                                                     w->b_rot.p, w->b_iiw.p, w->b_v.p, nullptr);
+    k_brick_pos<<<grid_for(nd, 256), 256, 0, s>>>(nd, nullptr, w->k_body.p, w->b_alive.p, w->b_asleep.p, w->b_pos.p,
+                                                  w->b_rot.p, w->k_local.p, w->k_wpos.p);
     w->launches += 2;
     return cudaGetLastError();
 }
 
 void step_destroy(sf_world *w) {
     if (w->step && w->step->h_dev) cudaFreeHost(w->step->h_dev);
+    if (w->step && w->step->h_live_pin) cudaFreeHost(w->step->h_live_pin);
     delete w->step;
     w->step = nullptr;
+}
+
+void step_mark_live(sf_world *w, uint32_t scene) {
+    if (w->step && scene < w->step->live.size()) w->step->live[scene] = 1;
+}
+void step_mark_all_live(sf_world *w) {
+    if (w->step) std::fill(w->step->live.begin(), w->step->live.end(), (uint8_t)1);
+}
+void step_set_live(sf_world *w, uint32_t scene, bool live) {
+    if (w->step && scene < w->step->live.size()) w->step->live[scene] = live ? 1 : 0;
+}
+cudaError_t step_reset_labels(sf_world *w, uint32_t first_body, uint32_t n) {
+    if (!w->step || n == 0) return cudaSuccess;
+    return cudaMemsetAsync(w->step->label.p + first_body, 0xFF, (size_t)n * 4, w->stream);
+}
+
+// The active set of the next step: live scenes the caller lets step. Lists are rebuilt only when the set changes.
+static sf_status set_active(sf_world *w, const uint8_t *mask) {
+    StepState *S = w->step;
+    cudaStream_t s = w->stream;
+    std::vector<uint32_t> act;
+    for (uint32_t q = 0; q < w->n_scenes; q++)
+        if (S->live[q] && (!mask || mask[q]) && w->scenes[q].n_bodies) act.push_back(q);
+    if (S->act_valid && act == S->act) return SF_OK;
+    // scenes that fell asleep leave the set: their bodies' island labels are those of sleeping bodies
+    for (uint32_t q : S->act)
+        if (!S->live[q] && !std::binary_search(act.begin(), act.end(), q)) {
+            const Scene &sc = w->scenes[q];
+            SF_CUDA(cudaMemsetAsync(S->label.p + sc.body_off, 0xFF, (size_t)sc.n_bodies * 4, s));
+        }
+    std::vector<uint32_t> scene_act(std::max<uint32_t>(w->n_scenes, 1), NONE);
+    std::vector<uint4> seg(std::max<size_t>(act.size(), 1));
+    uint32_t nb_act = 0, nd_act = 0;
+    for (size_t k = 0; k < act.size(); k++) {
+        const Scene &sc = w->scenes[act[k]];
+        scene_act[act[k]] = (uint32_t)k;
+        seg[k] = make_uint4(sc.body_off, nb_act, sc.brick_off, nd_act);
+        nb_act += sc.n_bodies;
+        nd_act += sc.n_bricks;
+    }
+    SF_CUDA(cudaMemcpyAsync(S->scene_act.p, scene_act.data(), scene_act.size() * 4, cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemcpyAsync(S->seg.p, seg.data(), seg.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
+    const uint32_t n = std::max(nb_act, nd_act);
+    if (n) {
+        k_build_lists<<<grid_for(n, 256), 256, 0, s>>>((uint32_t)act.size(), S->seg.p, nb_act, nd_act, S->act_body.p,
+                                                       S->cidx.p, S->act_brick.p);
+        w->launches++;
+    }
+    SF_CUDA(cudaGetLastError());
+    SF_CUDA(cudaStreamSynchronize(s));   // the host vectors above are the copies' sources
+    S->act = std::move(act);
+    S->nb_act = nb_act;
+    S->nd_act = nd_act;
+    S->act_valid = true;
+    return SF_OK;
 }
 
 static sf_status substep(sf_world *w, float h) {
     StepState *S = w->step;
     cudaStream_t s = w->stream;
-    const uint32_t nb = w->nb, nd = w->nd;
-    const uint64_t none_key = (uint64_t)w->n_scenes * HSIZE;
-    if (nb == 0 || nd == 0) return SF_OK;
+    const uint32_t nb = S->nb_act, nd = S->nd_act;
+    const uint32_t *blist = S->act_body.p, *klist = S->act_brick.p;
+    const uint64_t none_key = (uint64_t)S->act.size() * HSIZE;
+    std::fill(S->act_brick_base.begin(), S->act_brick_base.end(), NONE);
+    if (nb == 0 || nd == 0) {
+        SF_CUDA(cudaMemsetAsync(S->dev.p, 0, DV_ALIVE * sizeof(uint32_t), s));
+        SF_CUDA(cudaMemsetAsync(S->dev.p + DV_ISLANDS, 0, (DV_N - DV_ISLANDS) * sizeof(uint32_t), s));
+        for (int p = 0; p <= SF_PHASES; p++) prof_mark(w);
+        if (S->profile) S->sub_nc.push_back(0);
+        S->have_contacts = true;
+        return SF_OK;
+    }
+    {
+        uint32_t base = 0;
+        for (uint32_t q : S->act) { S->act_brick_base[q] = base; base += w->scenes[q].n_bricks; }
+    }
     uint64_t &L = w->launches;
     // pose cache + gravity, brick positions
     prof_mark(w);
-    k_update_cache<<<grid_for(nb, 128), 128, 0, s>>>(nb, h, w->b_alive.p, w->b_asleep.p, w->b_q.p, w->b_iil.p, w->b_rot.p,
-                                                     w->b_iiw.p, w->b_v.p);
-    k_brick_pos<<<grid_for(nd, 256), 256, 0, s>>>(nd, w->k_body.p, w->b_alive.p, w->b_asleep.p, w->b_pos.p, w->b_rot.p,
-                                                  w->k_local.p, w->k_wpos.p);
+    k_update_cache<<<grid_for(nb, 128), 128, 0, s>>>(nb, blist, h, w->b_alive.p, w->b_asleep.p, w->b_q.p, w->b_iil.p,
+                                                     w->b_rot.p, w->b_iiw.p, w->b_v.p, w->b_nc.p);
+    k_brick_pos<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, w->k_body.p, w->b_alive.p, w->b_asleep.p, w->b_pos.p,
+                                                  w->b_rot.p, w->k_local.p, w->k_wpos.p);
     L += 2;
     prof_mark(w);
     // hashed cells
-    k_cell_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, w->k_body.p, w->b_scene.p, w->b_alive.p, w->k_wpos.p,
-                                                  S->ckey.p, S->cval.p);
+    k_cell_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, none_key, w->k_body.p, w->b_scene.p, S->scene_act.p,
+                                                  w->b_alive.p, w->k_wpos.p, S->ckey.p, S->cval.p);
     SF_CUDA(radix_sort_u64(S->ckey.p, S->cval.p, S->ckey_alt.p, S->cval_alt.p, nd, bits_for(none_key), S->wk, s));
-    SF_CUDA(cudaMemsetAsync(S->brange.p, 0, S->brange.bytes(), s));
+    SF_CUDA(cudaMemsetAsync(S->brange.p, 0, (size_t)S->act.size() * HSIZE * sizeof(uint2), s));
     k_bucket_ranges<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, S->ckey.p, S->brange.p);
     k_bucket_records<<<grid_for(nd, 256), 256, 0, s>>>(nd, S->cval.p, w->k_body.p, w->k_mat.p, w->b_asleep.p, w->k_wpos.p,
                                                        S->srec.p, S->sinfo.p);
@@ -958,7 +1115,8 @@ static sf_status substep(sf_world *w, float h) {
     prof_mark(w);
     // contacts: generate into slots and count, scan, place in list order
     ContactArgs C;
-    C.nd = nd; C.sbox = w->sbox.p; C.kbody = w->k_body.p; C.bscene = w->b_scene.p; C.ctab = w->ctab.p; C.cpool = w->cpool.p;
+    C.nd = nd; C.list = klist; C.scene_act = S->scene_act.p;
+    C.sbox = w->sbox.p; C.kbody = w->k_body.p; C.bscene = w->b_scene.p; C.ctab = w->ctab.p; C.cpool = w->cpool.p;
     C.alive = w->b_alive.p; C.asleep = w->b_asleep.p; C.smat = w->s_mat.p; C.wpos = w->k_wpos.p;
     C.v = w->b_v.p; C.w = w->b_w.p; C.rot = w->b_rot.p; C.rad = w->b_rad.p; C.brange = S->brange.p; C.srec = S->srec.p;
     C.sinfo = S->sinfo.p; C.ccount = S->ccount.p; C.coff = S->coff.p; C.wake = w->b_wake.p;
@@ -976,18 +1134,17 @@ static sf_status substep(sf_world *w, float h) {
         C.L_a = S->L_a.p; C.L_b = S->L_b.p; C.L_bo = S->L_bo.p; C.L_ba = S->L_ba.p; C.L_bb = S->L_bb.p; C.L_p = S->L_p.p; C.L_n = S->L_n.p;
     }
     k_contacts_place<<<grid_for(nd, 128), 128, 0, s>>>(C);
-    SF_CUDA(cudaMemsetAsync(w->b_nc.p, 0, w->b_nc.bytes(), s));
     SF_CUDA(cudaMemsetAsync(S->dev.p + DV_MANIFOLDS, 0, (DV_N - DV_MANIFOLDS) * sizeof(uint32_t), s));
     const uint32_t g_nc = grid_for(std::max<uint32_t>(nc, 1), 256);
     if (nc) { k_body_nc<<<g_nc, 256, 0, s>>>(nc, S->L_a.p, S->L_b.p, w->b_nc.p); L++; }
-    L += 2;
+    L += 1;
     if (S->profile) S->sub_nc.push_back(nc);
     prof_mark(w);
     // manifolds
-    const uint64_t nb1 = (uint64_t)nb + 1;
+    const uint64_t nb1 = (uint64_t)w->nb + 1;
     if (nc) {
         k_man_keys<<<g_nc, 256, 0, s>>>(nc, nb1, S->L_a.p, S->L_b.p, S->mkey.p, S->perm.p);
-        SF_CUDA(radix_sort_u64(S->mkey.p, S->perm.p, S->mkey_alt.p, S->perm_alt.p, nc, bits_for((uint64_t)nb * nb1 + nb1), S->wk, s));
+        SF_CUDA(radix_sort_u64(S->mkey.p, S->perm.p, S->mkey_alt.p, S->perm_alt.p, nc, bits_for((uint64_t)w->nb * nb1 + nb1), S->wk, s));
         const uint32_t K = w->P.manifold_chunk;
         k_man_flags<<<g_nc, 256, 0, s>>>(nc, S->mkey.p, S->mflag.p);
         SF_CUDA(exclusive_scan_u32(S->mflag.p, S->mpos.p, nc, S->dev.p + DV_PAIRS, S->wk, s));
@@ -995,8 +1152,8 @@ static sf_status substep(sf_world *w, float h) {
         k_chunk_flags<<<g_nc, 256, 0, s>>>(nc, K, S->mflag.p, S->mpos.p, S->pair_start.p, S->cflag.p);
         SF_CUDA(exclusive_scan_u32(S->cflag.p, S->cpos.p, nc, S->dev.p + DV_MANIFOLDS, S->wk, s));
         k_man_write<<<g_nc, 256, 0, s>>>(nc, K, S->cflag.p, S->cpos.p, S->mflag.p, S->mpos.p, S->pair_start.p, S->perm.p,
-                                         S->L_a.p, S->L_b.p, S->body_off_of_body.p, S->man_a.p, S->man_b.p, S->man_start.p,
-                                         S->man_prio.p);
+                                         S->L_a.p, S->L_b.p, S->body_off_of_body.p, S->cidx.p, S->man_a.p, S->man_b.p,
+                                         S->man_ca.p, S->man_cb.p, S->man_start.p, S->man_prio.p);
         k_man_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, nc, S->man_start.p, S->man_count.p);
         L += 6;
         prof_mark(w);
@@ -1008,17 +1165,17 @@ static sf_status substep(sf_world *w, float h) {
         k_prep<<<g_nc, 256, 0, s>>>(PA);
         L++;
         prof_mark(w);
-        // colouring
-        SF_CUDA(cudaMemsetAsync(S->bm_count.p, 0, S->bm_count.bytes(), s));
-        SF_CUDA(cudaMemsetAsync(S->bm_fill.p, 0, S->bm_fill.bytes(), s));
-        SF_CUDA(cudaMemsetAsync(S->masks.p, 0, S->masks.bytes(), s));
+        // colouring, on the active list's body ids
+        SF_CUDA(cudaMemsetAsync(S->bm_count.p, 0, ((size_t)nb + 1) * 4, s));
+        SF_CUDA(cudaMemsetAsync(S->bm_fill.p, 0, ((size_t)nb + 1) * 4, s));
+        SF_CUDA(cudaMemsetAsync(S->masks.p, 0, (size_t)nb * 16, s));
         SF_CUDA(cudaMemsetAsync(S->man_round.p, 0xFF, (size_t)nc * 4, s));
-        k_bm_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_a.p, S->man_b.p, S->bm_count.p);
+        k_bm_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_ca.p, S->man_cb.p, S->bm_count.p);
         SF_CUDA(exclusive_scan_u32(S->bm_count.p, S->bm_start.p, (size_t)nb + 1, nullptr, S->wk, s));
-        k_bm_fill<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_a.p, S->man_b.p, S->bm_start.p, S->bm_fill.p, S->bm_list.p);
+        k_bm_fill<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_ca.p, S->man_cb.p, S->bm_start.p, S->bm_fill.p, S->bm_list.p);
         SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s));
         JpArgs J;
-        J.nm_p = S->dev.p + DV_MANIFOLDS; J.man_a = S->man_a.p; J.man_b = S->man_b.p; J.prio = S->man_prio.p;
+        J.nm_p = S->dev.p + DV_MANIFOLDS; J.man_a = S->man_ca.p; J.man_b = S->man_cb.p; J.prio = S->man_prio.p;
         J.bm_start = S->bm_start.p; J.bm_list = S->bm_list.p; J.man_round = S->man_round.p; J.man_color = S->man_color.p;
         J.masks = S->masks.p; J.wl0 = S->wl0.p; J.wl1 = S->wl1.p; J.dev = S->dev.p; J.max_colors = w->P.max_colors;
         J.max_rounds = 1u << 16; J.gb = w->barrier.p; J.err = w->err.p;
@@ -1032,15 +1189,15 @@ static sf_status substep(sf_world *w, float h) {
         k_col_fill<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_color.p, S->col_start.p, S->col_fill.p, S->col_list.p);
         L += 6;
         if (w->P.verify) {
-            SF_CUDA(cudaMemsetAsync(S->vmasks.p, 0, S->vmasks.bytes(), s));
-            k_col_verify<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_a.p, S->man_b.p, S->man_color.p, S->vmasks.p, w->err.p);
+            SF_CUDA(cudaMemsetAsync(S->vmasks.p, 0, (size_t)nb * 16, s));
+            k_col_verify<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_ca.p, S->man_cb.p, S->man_color.p, S->vmasks.p, w->err.p);
             L++;
         }
     } else {
         prof_mark(w);
         prof_mark(w);
     }
-    k_save_pre<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, w->b_v.p, w->b_w.p, w->b_vpre.p, w->b_wpre.p);
+    k_save_pre<<<grid_for(nb, 256), 256, 0, s>>>(nb, blist, w->b_alive.p, w->b_v.p, w->b_w.p, w->b_vpre.p, w->b_wpre.p);
     L++;
     SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s));
     prof_mark(w);
@@ -1060,24 +1217,24 @@ static sf_status substep(sf_world *w, float h) {
     }
     prof_mark(w);
     // islands over the manifolds of this substep
-    k_uf_init<<<grid_for(nb, 256), 256, 0, s>>>(nb, S->parent.p, S->mint.p);
+    k_uf_init<<<grid_for(nb, 256), 256, 0, s>>>(nb, blist, S->parent.p, S->mint.p);
     if (nc) { k_uf_union<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_a.p, S->man_b.p, S->parent.p); L++; }
-    k_uf_label<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, w->b_asleep.p, S->parent.p, S->label.p, S->dev.p);
+    k_uf_label<<<grid_for(nb, 256), 256, 0, s>>>(nb, blist, w->b_alive.p, w->b_asleep.p, S->parent.p, S->label.p, S->dev.p);
     L += 2;
     prof_mark(w);
     IntArgs I;
-    I.nb = nb; I.h = h; I.pinch_kill = w->P.pinch_kill ? 1 : 0; I.island_mode = w->P.sleep_mode == SF_SLEEP_ISLAND;
+    I.nb = nb; I.list = blist; I.h = h; I.pinch_kill = w->P.pinch_kill ? 1 : 0; I.island_mode = w->P.sleep_mode == SF_SLEEP_ISLAND;
     I.alive = w->b_alive.p; I.asleep = w->b_asleep.p; I.pos = w->b_pos.p; I.q = w->b_q.p; I.v = w->b_v.p; I.w = w->b_w.p;
     I.vpre = w->b_vpre.p; I.wpre = w->b_wpre.p; I.rad = w->b_rad.p; I.sleep = w->b_sleep.p; I.maxr = w->b_maxr.p;
     I.nc = w->b_nc.p; I.count = w->b_count.p; I.first = w->b_first.p; I.kmat = w->k_mat.p;
     k_integrate<<<grid_for(nb, 128), 128, 0, s>>>(I);
     if (I.island_mode) {
-        k_island_min<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, S->label.p, w->b_sleep.p, S->mint.p);
-        k_island_sleep<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, w->b_asleep.p, S->label.p, w->b_sleep.p, S->mint.p,
-                                                         w->b_v.p, w->b_w.p);
+        k_island_min<<<grid_for(nb, 256), 256, 0, s>>>(nb, blist, w->b_alive.p, S->label.p, w->b_sleep.p, S->mint.p);
+        k_island_sleep<<<grid_for(nb, 256), 256, 0, s>>>(nb, blist, w->b_alive.p, w->b_asleep.p, S->label.p, w->b_sleep.p,
+                                                         S->mint.p, w->b_v.p, w->b_w.p);
     }
-    k_wake<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_wake.p, w->b_alive.p, w->b_asleep.p, w->b_sleep.p);
-    k_kill_bricks<<<grid_for(nd, 256), 256, 0, s>>>(nd, w->k_body.p, w->b_alive.p, w->k_mat.p);
+    k_wake<<<grid_for(nb, 256), 256, 0, s>>>(nb, blist, w->b_wake.p, w->b_alive.p, w->b_asleep.p, w->b_sleep.p);
+    k_kill_bricks<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, w->k_body.p, w->b_alive.p, w->k_mat.p);
     L += I.island_mode ? 5 : 3;
     prof_mark(w);
     SF_CUDA(cudaGetLastError());
@@ -1085,13 +1242,26 @@ static sf_status substep(sf_world *w, float h) {
     return SF_OK;
 }
 
-}  // namespace sf
+// after a step: which active scenes still have an awake body (read back with the step's counters)
+static sf_status queue_live_readback(sf_world *w) {
+    StepState *S = w->step;
+    cudaStream_t s = w->stream;
+    if (S->act.empty()) return SF_OK;
+    SF_CUDA(cudaMemsetAsync(S->live_dev.p, 0, w->n_scenes, s));
+    if (S->nb_act) {
+        k_scene_live<<<grid_for(S->nb_act, 256), 256, 0, s>>>(S->nb_act, S->act_body.p, w->b_alive.p, w->b_asleep.p,
+                                                             w->b_scene.p, S->live_dev.p);
+        w->launches++;
+    }
+    SF_CUDA(cudaMemcpyAsync(S->h_live_pin, S->live_dev.p, w->n_scenes, cudaMemcpyDeviceToHost, s));
+    return SF_OK;
+}
+static void apply_live_readback(sf_world *w) {
+    StepState *S = w->step;
+    for (uint32_t q : S->act) S->live[q] = S->h_live_pin[q];
+}
 
-using namespace sf;
-
-extern "C" {
-
-sf_status sf_world_step(sf_world *w, float dt, uint32_t nsteps) {
+static sf_status step_impl(sf_world *w, float dt, uint32_t nsteps, const uint8_t *mask) {
     if (!w) return SF_ERR_ARG;
     if (!(dt == dt)) { set_error("dt is NaN"); return SF_ERR_ARG; }
     StepState *S = w->step;
@@ -1103,16 +1273,25 @@ sf_status sf_world_step(sf_world *w, float dt, uint32_t nsteps) {
     SF_CUDA(cudaEventRecord(w->ev0, s));
     for (uint32_t k = 0; k < nsteps; k++) {
         w->frame++;
+        sf_status r = set_active(w, mask);
+        if (r != SF_OK) return r;
         for (uint32_t q = 0; q < ns; q++) {
-            sf_status r = substep(w, h);
+            r = substep(w, h);
             if (r != SF_OK) return r;
+        }
+        r = queue_live_readback(w);
+        if (r != SF_OK) return r;
+        if (k + 1 < nsteps) {
+            SF_CUDA(cudaStreamSynchronize(s));
+            apply_live_readback(w);
         }
     }
     SF_CUDA(cudaMemsetAsync(S->dev.p + DV_ALIVE, 0, 2 * sizeof(uint32_t), s));
     if (w->nb) k_count_bodies<<<grid_for(w->nb, 256), 256, 0, s>>>(w->nb, w->b_alive.p, w->b_asleep.p, S->dev.p);
     SF_CUDA(cudaEventRecord(w->ev1, s));
     SF_CUDA(cudaMemcpyAsync(S->h_dev, S->dev.p, DV_N * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    sf_status r = read_error_word(w);
+    sf_status r = read_error_word(w);   // synchronises the stream
+    if (nsteps) apply_live_readback(w);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, w->ev0, w->ev1);
     sf_stats &st = w->stats;
@@ -1139,6 +1318,19 @@ sf_status sf_world_step(sf_world *w, float dt, uint32_t nsteps) {
         S->ev_used = 0;
     }
     return r;
+}
+
+}  // namespace sf
+
+using namespace sf;
+
+extern "C" {
+
+sf_status sf_world_step(sf_world *w, float dt, uint32_t nsteps) { return step_impl(w, dt, nsteps, nullptr); }
+
+sf_status sf_world_step_scenes(sf_world *w, float dt, uint32_t nsteps, const uint8_t *scene_mask) {
+    if (!w || !scene_mask) { set_error("null argument"); return SF_ERR_ARG; }
+    return step_impl(w, dt, nsteps, scene_mask);
 }
 
 sf_status sf_set_profiling(sf_world *w, int32_t on) {
@@ -1186,13 +1378,14 @@ sf_status sf_read_contacts(sf_world *w, uint32_t scene, uint32_t *ids5, float *f
     const Scene &sc = w->scenes[scene];
     uint32_t nc = (uint32_t)S->last_contacts;
     cudaStream_t s = w->stream;
-    // the scene's contacts are the list range of its bricks
+    // the scene's contacts are the list range of its bricks in the last substep's active list (none if it was idle)
     uint32_t lo = 0, hi = 0;
-    if (sc.n_bricks) {
-        SF_CUDA(cudaMemcpyAsync(&lo, S->coff.p + sc.brick_off, 4, cudaMemcpyDeviceToHost, s));
-        if (sc.brick_off + sc.n_bricks < w->nd) SF_CUDA(cudaMemcpyAsync(&hi, S->coff.p + sc.brick_off + sc.n_bricks, 4, cudaMemcpyDeviceToHost, s));
+    const uint32_t kb = S->act_brick_base[scene];
+    if (sc.n_bricks && kb != NONE) {
+        SF_CUDA(cudaMemcpyAsync(&lo, S->coff.p + kb, 4, cudaMemcpyDeviceToHost, s));
+        if (kb + sc.n_bricks < S->nd_act) SF_CUDA(cudaMemcpyAsync(&hi, S->coff.p + kb + sc.n_bricks, 4, cudaMemcpyDeviceToHost, s));
         SF_CUDA(cudaStreamSynchronize(s));
-        if (sc.brick_off + sc.n_bricks >= w->nd) hi = nc;
+        if (kb + sc.n_bricks >= S->nd_act) hi = nc;
     }
     uint64_t cnt = hi - lo;
     if (n) *n = cnt;

@@ -365,3 +365,49 @@ def test_config2_compound_bodies_bit_exact(sf, oracle):
     np.testing.assert_array_equal(sl, osl)
     _compare_step_outputs(w, ow)
     assert w.stats().contacts > 100
+
+
+# ---------------------------------------------------------------- scene subsets and the active set
+def test_masked_steps_equal_alone(sf):
+    """Scenes stepped on different subsets of the world's steps (sf_world_step_scenes) end exactly where the same
+    number of steps takes each scene alone; a held scene is left untouched."""
+    scenes = [small_debris(seed=40 + k, n=80 + 50 * k) for k in range(4)]
+    big = sf.World(scenes, iterations=8)
+    rng = np.random.default_rng(5)
+    counts = np.zeros(4, int)
+    for _ in range(45):
+        m = (rng.random(4) < 0.6).astype(np.uint8)
+        before = big.bodies()[0].copy()
+        big.step_scenes(m, 1 / 60)
+        after = big.bodies()[0]
+        for k in range(4):
+            if not m[k]:
+                sl = slice(big.body_off[k], big.body_off[k + 1])
+                np.testing.assert_array_equal(after[sl], before[sl])
+        counts += m
+    bst, bsl, bfl = big.bodies()
+    for k, sc in enumerate(scenes):
+        w = sf.World(sc, iterations=8)
+        w.step(1 / 60, nsteps=int(counts[k]))
+        st, sl, fl = w.bodies()
+        sl_ = slice(big.body_off[k], big.body_off[k + 1])
+        np.testing.assert_array_equal(st, bst[sl_])
+        np.testing.assert_array_equal(sl, bsl[sl_])
+        np.testing.assert_array_equal(fl, bfl[sl_])
+
+
+def test_sleeping_scenes_leave_the_active_set(sf, oracle):
+    """A long run where scenes fall asleep one by one (and so stop stepping) stays bit-exact, islands included."""
+    sc = small_debris(seed=14, n=60)
+    w = sf.World(sc, iterations=8)
+    ow = oracle.OracleWorld(sc)
+    for _ in range(260):
+        w.step(1 / 60)
+        ow.step(1 / 60, iterations=8, order=oracle.ORDER_COLOR)
+    st, sl, fl = w.bodies()
+    ost, osl, ofl = ow.bodies()
+    np.testing.assert_array_equal(fl, ofl)
+    np.testing.assert_array_equal(st, ost)
+    np.testing.assert_array_equal(sl, osl)
+    np.testing.assert_array_equal(w.islands(), ow.islands())
+    assert w.stats().awake < sc.n_bodies
