@@ -59,6 +59,12 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=3.0, help="length of the served arrival stream")
+    ap.add_argument("--serve-plain-seconds", type=float, default=1.0, help="length of the stream the plain path serves")
+    ap.add_argument("--serve-rate", type=float, default=2000.0)
+    ap.add_argument("--serve-worlds", type=int, default=96)
+    ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     return ap.parse_args()
 
 
@@ -252,6 +258,92 @@ def run_steps(w, k: int):
     return alive, ms
 
 
+# ---------------------------------------------------------------- serving (config 5)
+def _latency(res, kind=None):
+    lat = np.array([(r["t_done"] - r["t_arrival"]) * 1e3 for r in res if kind is None or r["kind"] == kind])
+    if len(lat) == 0:
+        return None
+    return {"n": int(len(lat)), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "p999_ms": float(np.percentile(lat, 99.9)), "mean_ms": float(lat.mean())}
+
+
+def serve_run(args, worlds, structs, slots, batching: bool, seconds: float, seed: int):
+    """One server on the population, fed a Poisson stream of `seconds` at --serve-rate; returns the summary."""
+    import shatterforge_b200 as sf
+    from shatterforge_b200 import serving as SV
+
+    srv = SV.Server(slots=slots, structures=structs, budget_bytes=int(args.serve_budget_gb * 2**30), batching=batching,
+                    sweeps_per_tick=128, iterations=ITERS, pinch_kill=0)
+    ids = [srv.add_scene(w) for w in worlds]
+    sids = structs.structure_ids()
+    srv.start()
+    # resident structures start solved (their potentials are part of the resident state)
+    for q in sids:
+        srv.submit_solve(q, omega=1.7, tol=1e-6, max_sweeps=200000)
+    srv.drain(600000)
+    srv.poll(cap=len(sids) + 8)
+    rng = np.random.default_rng(seed)
+    n = int(args.serve_rate * seconds)
+    t0 = srv.stats()["now_s"] + 0.05
+    t = t0 + np.cumsum(rng.exponential(1.0 / args.serve_rate, n))
+    steps_of = {}
+    bricks_of = {q: np.nonzero(structs.static_sid == q)[0] for q in sids}
+    for k in range(n):
+        if rng.random() < 0.7:
+            wid = int(rng.integers(len(ids)))
+            ns = int(rng.integers(1, 9))
+            steps_of[srv.submit_step(ids[wid], ns, t_arrival=float(t[k]))] = ns * worlds[wid].n_bodies
+        else:
+            q = int(sids[int(rng.integers(len(sids)))])
+            lb = rng.choice(bricks_of[q], 3)
+            lv = rng.uniform(50.0, 400.0, 3).astype(np.float32)
+            srv.submit_solve(q, omega=1.7, tol=1e-6, max_sweeps=20000, loads=(lb, lv), t_arrival=float(t[k]))
+    unfinished = 0
+    try:
+        srv.drain(int(max(60.0, 20 * seconds) * 1000))
+    except sf.SfError:
+        unfinished = srv.stats()["pending"]
+    res = srv.poll(cap=n + 16)
+    st = srv.stats()
+    srv.close()
+    done = [r for r in res if r["status"] == 0]
+    span = max(r["t_done"] for r in done) - t0 if done else float("nan")
+    body_steps = sum(steps_of.get(r["ticket"], 0) for r in done)
+    return {"requests": n, "completed": len(done), "unfinished": int(unfinished), "seconds_of_arrivals": seconds,
+            "throughput_req_s": len(done) / span, "served_body_steps_per_s": body_steps / span,
+            "all": _latency(done), "step": _latency(done, 1), "solve": _latency(done, 2),
+            "ticks": {"step": int(st["step_ticks"]), "solve": int(st["solve_ticks"])},
+            "loads": int(st["loads"]), "restores": int(st["restores"]), "evictions": int(st["evictions"]),
+            "resident_gb": st["pool_bytes"] / 2**30}
+
+
+def serve_section(args):
+    from shatterforge_b200 import scenes as S
+    from shatterforge_b200 import serving as SV
+
+    rng = np.random.default_rng(17)
+    sizes = np.exp(rng.uniform(math.log(1000), math.log(100000), args.serve_worlds)).astype(np.int64)
+    lib = S.ClusterLibrary(0x51ED)
+    worlds = [S.debris_scene(int(nb), seed=5000 + k, lib=lib, name=f"served{k}") for k, nb in enumerate(sizes)]
+    structs = S.config3_world(seed=7)
+    # one slot per world while the budget holds them all; otherwise fewer slots of the largest size (LRU eviction)
+    slots = [SV.slot_for(w_) for w_ in worlds]
+    budget = int(args.serve_budget_gb * 2**30) - 4 * 2**30      # headroom for the structures world and scratch
+    if SV.pool_bytes(slots) > budget:
+        big = tuple(max(c[i] for c in slots) for i in range(4))
+        k = max(1, budget // SV.pool_bytes([big]))
+        slots = [big] * int(min(k, len(worlds)))
+    batched = serve_run(args, worlds, structs, slots, True, args.serve_seconds, seed=23)
+    plain = serve_run(args, worlds, structs, slots, False, args.serve_plain_seconds, seed=23)
+    return {"rate_req_s": args.serve_rate, "worlds": len(worlds), "world_bodies": int(sizes.sum()),
+            "structures": len(structs.structure_ids()), "structure_bricks": structs.n_static,
+            "slots": len(slots), "budget_gb": args.serve_budget_gb, "mix": "70% scene steps (1-8 steps), 30% structure "
+            "solves (3 random loads of 50-400 kg, omega 1.7 to 1e-6, from resident potentials)",
+            "batched": batched, "plain": plain,
+            "note": "latency = completion - arrival on the server clock; plain = one request at a time with its own "
+                    "launches, on the same population and the first seconds of the same stream"}
+
+
 def our_arm(args, rank, world, local, pg):
     import torch
 
@@ -396,6 +488,10 @@ def our_arm(args, rank, world, local, pg):
 
     # ---- CPU baseline: the oracle on a bounded sample of the same workload and step window
     cpu = None
+    serve = None
+    if not args.no_serve and rank == 0:
+        serve = serve_section(args)
+
     if not args.no_cpu and rank == 0:
         one = cpu_sample(scenes, 1)
         rate1, n1 = cpu_body_steps(one, args.warmup, args.steps, args.cpu_seconds, 1)
@@ -430,6 +526,7 @@ def our_arm(args, rank, world, local, pg):
         "plain": plain,
         "sor": sor,
         "cpu_baseline": cpu,
+        "serve": serve,
     }
     print(json.dumps(line), flush=True)
 

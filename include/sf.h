@@ -138,12 +138,26 @@ sf_status sf_read_profile(sf_world *w, sf_profile *out);
 sf_status sf_reset_profile(sf_world *w);
 
 /* ---- hot path */
-/* nsteps world steps of dt each (dt clamped to [0, 1/30] as src/lib.rs:3642 does), all scenes at once. */
+/* nsteps world steps of dt each (dt clamped to [0, 1/30] as src/lib.rs:3642 does), all scenes at once. Scenes
+ * whose bodies all sleep are skipped (a step leaves them unchanged), so the cost follows the awake scenes. */
 sf_status sf_world_step(sf_world *w, float dt, uint32_t nsteps);
+/* As sf_world_step, but only the scenes with scene_mask[scene] != 0 step (host array of n_scenes bytes); the others
+ * are left exactly as they are. No counterpart in the reference (one world per wasm instance there): this is the
+ * batched form's way to step a chosen subset of resident scenes in one set of launches. */
+sf_status sf_world_step_scenes(sf_world *w, float dt, uint32_t nsteps, const uint8_t *scene_mask);
 /* Load-path solve of one structure (>= 0) or of every structure (-1): red-black SOR with relaxation omega until
  * the reference's residual max|dphi| / max(phi, 1) < tol or max_sweeps. */
 sf_status sf_structure_solve(sf_world *w, int32_t structure, float omega, float tol, uint32_t max_sweeps,
                              sf_solve_report *report);
+/* The same solve for a list of structures in one persistent launch (each structure stops at its own residual).
+ * Every solve starts from the stored potentials, so a solve split over several calls of k sweeps each takes the
+ * same sweeps as one call. No counterpart in the reference (its structures are solved one per `structural` call);
+ * this is the batched form's entry point. */
+sf_status sf_structure_solve_set(sf_world *w, const int32_t *structures, uint32_t n, float omega, float tol,
+                                 uint32_t max_sweeps, sf_solve_report *report);
+/* ext[brick[k]] += value[k] for k in order: external loads on static bricks (the body-load term of `structural`
+ * folds into ext the same way, src/lib.rs:1257-1258). */
+sf_status sf_structure_add_loads(sf_world *w, uint32_t n, const uint32_t *brick, const float *value);
 /* Joint checks of one structure (or -1 = all) on the current potentials; live != 0 applies fatigue, failures and
  * crushes as stress_brick does. */
 sf_status sf_structure_check(sf_world *w, int32_t structure, float dt, int32_t live, sf_check_report *report);
@@ -218,6 +232,89 @@ sf_status sf_collide_boxes(const float *boxes_a, const float *boxes_b, uint32_t 
  * 8 x (point 3, separation); reduce != 0 keeps at most 4 points. */
 sf_status sf_collide_hulls(const float *hull_data, uint32_t n_hulls, const float *shapes_a, const float *shapes_b,
                            uint32_t n_pairs, float margin, int32_t reduce, float *out36, int32_t *count);
+
+/* ---- scene pools: the batched and served forms (no counterpart in the reference, which runs one world per wasm
+ * instance). A pool is a world of fixed-capacity scene slots; a rigid scene (bodies plus loose static geometry, no
+ * load-path structures) is loaded into a slot, stepped with the other slots by sf_world_step / sf_world_step_scenes
+ * (slot index = scene index), saved to host memory and restored, bit for bit, into any slot large enough. */
+typedef struct sf_pool_slot {
+    uint32_t bodies, bricks;    /* body and body-brick capacity */
+    uint32_t statics, chunks;   /* static-brick capacity and the 8^3 chunks they may occupy */
+} sf_pool_slot;
+/* Device bytes a pool of these slots takes (an estimate from the per-element sizes, initial contact capacity of 4
+ * per brick included). */
+sf_status sf_pool_bytes(uint32_t n_slots, const sf_pool_slot *slots, uint64_t *bytes);
+sf_status sf_pool_create(uint32_t n_slots, const sf_pool_slot *slots, const sf_params *params, sf_world **out);
+/* Load a scene into a slot (replacing what it held); SF_ERR_CAPACITY if it does not fit. */
+sf_status sf_pool_load(sf_world *w, uint32_t slot, const sf_scene_desc *scene);
+sf_status sf_pool_clear(sf_world *w, uint32_t slot);
+/* Host bytes of a snapshot of a scene with these counts, and the snapshot calls: save writes the slot's mutable
+ * state (body poses, velocities, rotation caches, sleep state; brick positions and removals) to host memory;
+ * restore loads the scene's fixed parts from its description and then that state. */
+uint64_t sf_pool_snapshot_bytes(uint32_t n_bodies, uint32_t n_bricks);
+sf_status sf_pool_save(sf_world *w, uint32_t slot, void *host, uint64_t cap, uint64_t *bytes);
+sf_status sf_pool_restore(sf_world *w, uint32_t slot, const sf_scene_desc *scene, const void *host, uint64_t bytes);
+/* The loaded scene's bodies, as sf_read_bodies. */
+sf_status sf_pool_read_bodies(sf_world *w, uint32_t slot, float *state13, float *sleep, uint8_t *flags);
+
+/* ---- serving (no counterpart in the reference): a request loop over resident worlds with continuous batching.
+ * Scene-step requests run on a scene pool (one step of every scene with work per tick, in one set of launches;
+ * a scene without a slot takes a free one or evicts the least recently used idle scene to pinned host memory);
+ * structure-solve requests run on a resident structures world (every structure with work solved in one persistent
+ * launch of up to sweeps_per_tick sweeps per tick). The two kinds run on their own threads and streams, so their
+ * device work overlaps. With batching = 0 one thread runs the requests one at a time in arrival order, each with
+ * its own launches (the plain path). Requests arrive at t_arrival on the server clock (seconds since
+ * sf_server_start), so an arrival process can be submitted up front. */
+#define SF_REQ_STEP 1
+#define SF_REQ_SOLVE 2
+typedef struct sf_server sf_server;
+typedef struct sf_server_desc {
+    uint32_t n_slots;
+    const sf_pool_slot *slots;           /* the scene pool (n_slots = 0: no scene requests) */
+    const sf_world_desc *structures;     /* the resident structures (NULL: no solve requests) */
+    uint64_t budget_bytes;               /* device bytes the resident state may take (0 = no limit): SF_ERR_BUDGET above */
+    float dt;                            /* step length of scene requests */
+    uint32_t sweeps_per_tick;            /* SOR sweeps per tick of the solve batch (0 = 128) */
+    uint32_t batching;                   /* 1 = continuous batching, 0 = one request at a time */
+    sf_params params;
+} sf_server_desc;
+typedef struct sf_request {
+    uint32_t kind;                       /* SF_REQ_STEP or SF_REQ_SOLVE */
+    uint32_t world;                      /* a scene id from sf_server_add_scene, or a structure id */
+    uint32_t nsteps;                     /* STEP */
+    float omega, tol;                    /* SOLVE */
+    uint32_t max_sweeps;                 /* SOLVE */
+    uint32_t n_loads, reserved;          /* SOLVE: ext[load_brick[k]] += load_value[k] before the solve (copied) */
+    const uint32_t *load_brick;
+    const float *load_value;
+    double t_arrival;
+    float *out_state13;                  /* STEP, optional: the scene's bodies after the request (13 floats each) */
+} sf_request;
+typedef struct sf_result {
+    uint64_t ticket;
+    uint32_t kind, world, status, steps, sweeps, reserved;
+    double residual;
+    double t_arrival, t_start, t_done;   /* server clock, seconds */
+} sf_result;
+typedef struct sf_server_stats {
+    uint64_t completed, pending, step_ticks, solve_ticks, loads, restores, evictions;
+    uint64_t pool_bytes;                 /* device bytes the resident state took at creation */
+    double busy_s, now_s;
+} sf_server_stats;
+sf_status sf_server_create(const sf_server_desc *desc, sf_server **out);
+/* Register a scene (deep copy) before sf_server_start; it is loaded into a slot when a request needs it. */
+sf_status sf_server_add_scene(sf_server *s, const sf_scene_desc *scene, uint32_t *id);
+sf_status sf_server_start(sf_server *s);
+/* Thread-safe. */
+sf_status sf_server_submit(sf_server *s, const sf_request *req, uint64_t *ticket);
+/* Finished requests (up to cap), waiting up to wait_ms for the first. */
+sf_status sf_server_poll(sf_server *s, sf_result *out, uint32_t cap, uint32_t *n, uint32_t wait_ms);
+/* Wait until every submitted request has finished. */
+sf_status sf_server_drain(sf_server *s, uint32_t timeout_ms);
+sf_status sf_server_get_stats(sf_server *s, sf_server_stats *out);
+/* The structures' potentials (FP64), when no request is open. */
+sf_status sf_server_read_phi64(sf_server *s, double *phi);
+void sf_server_destroy(sf_server *s);
 
 #ifdef __cplusplus
 }

@@ -88,6 +88,39 @@ class WorldInfo(C.Structure):
                 ("n_body_bricks", C.c_uint32), ("n_structures", C.c_uint32), ("n_chunks", C.c_uint32)]
 
 
+class PoolSlot(C.Structure):
+    _fields_ = [("bodies", C.c_uint32), ("bricks", C.c_uint32), ("statics", C.c_uint32), ("chunks", C.c_uint32)]
+
+
+class ServerDesc(C.Structure):
+    _fields_ = [("n_slots", C.c_uint32), ("slots", C.POINTER(PoolSlot)), ("structures", C.POINTER(WorldDesc)),
+                ("budget_bytes", C.c_uint64), ("dt", C.c_float), ("sweeps_per_tick", C.c_uint32),
+                ("batching", C.c_uint32), ("params", Params)]
+
+
+class Request(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("world", C.c_uint32), ("nsteps", C.c_uint32), ("omega", C.c_float),
+                ("tol", C.c_float), ("max_sweeps", C.c_uint32), ("n_loads", C.c_uint32), ("reserved", C.c_uint32),
+                ("load_brick", C.POINTER(C.c_uint32)), ("load_value", C.POINTER(C.c_float)),
+                ("t_arrival", C.c_double), ("out_state13", C.POINTER(C.c_float))]
+
+
+class Result(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("kind", C.c_uint32), ("world", C.c_uint32), ("status", C.c_uint32),
+                ("steps", C.c_uint32), ("sweeps", C.c_uint32), ("reserved", C.c_uint32), ("residual", C.c_double),
+                ("t_arrival", C.c_double), ("t_start", C.c_double), ("t_done", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("pending", C.c_uint64), ("step_ticks", C.c_uint64),
+                ("solve_ticks", C.c_uint64), ("loads", C.c_uint64), ("restores", C.c_uint64),
+                ("evictions", C.c_uint64), ("pool_bytes", C.c_uint64), ("busy_s", C.c_double), ("now_s", C.c_double)]
+
+
+SF_REQ_STEP, SF_REQ_SOLVE = 1, 2
+_vp = C.c_void_p
+_u64p = C.POINTER(C.c_uint64)
+
 # every exported function: name -> (restype, argtypes)
 PROTOTYPES = {
     "sf_params_default": (None, [C.POINTER(Params)]),
@@ -126,6 +159,25 @@ PROTOTYPES = {
     "sf_collide_hulls": (C.c_int32, [_f32p, C.c_uint32, _f32p, _f32p, C.c_uint32, C.c_float, C.c_int32, _f32p, _i32p]),
     "sf_structure_solve_static": (C.c_int32, [C.c_uint32, _i32p, _u8p, _u8p, _f32p, C.c_float, C.c_float, C.c_uint32,
                                               C.POINTER(C.c_double), _u32p, C.POINTER(C.c_double), C.c_void_p]),
+    "sf_structure_solve_set": (C.c_int32, [_vp, _i32p, C.c_uint32, C.c_float, C.c_float, C.c_uint32, C.POINTER(SolveReport)]),
+    "sf_structure_add_loads": (C.c_int32, [_vp, C.c_uint32, _u32p, _f32p]),
+    "sf_pool_bytes": (C.c_int32, [C.c_uint32, C.POINTER(PoolSlot), _u64p]),
+    "sf_pool_create": (C.c_int32, [C.c_uint32, C.POINTER(PoolSlot), C.POINTER(Params), C.POINTER(_vp)]),
+    "sf_pool_load": (C.c_int32, [_vp, C.c_uint32, C.POINTER(SceneDesc)]),
+    "sf_pool_clear": (C.c_int32, [_vp, C.c_uint32]),
+    "sf_pool_snapshot_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32]),
+    "sf_pool_save": (C.c_int32, [_vp, C.c_uint32, _vp, C.c_uint64, _u64p]),
+    "sf_pool_restore": (C.c_int32, [_vp, C.c_uint32, C.POINTER(SceneDesc), _vp, C.c_uint64]),
+    "sf_pool_read_bodies": (C.c_int32, [_vp, C.c_uint32, _f32p, _f32p, _u8p]),
+    "sf_server_create": (C.c_int32, [C.POINTER(ServerDesc), C.POINTER(_vp)]),
+    "sf_server_add_scene": (C.c_int32, [_vp, C.POINTER(SceneDesc), _u32p]),
+    "sf_server_start": (C.c_int32, [_vp]),
+    "sf_server_submit": (C.c_int32, [_vp, C.POINTER(Request), _u64p]),
+    "sf_server_poll": (C.c_int32, [_vp, C.POINTER(Result), C.c_uint32, _u32p, C.c_uint32]),
+    "sf_server_drain": (C.c_int32, [_vp, C.c_uint32]),
+    "sf_server_get_stats": (C.c_int32, [_vp, C.POINTER(ServerStats)]),
+    "sf_server_read_phi64": (C.c_int32, [_vp, C.POINTER(C.c_double)]),
+    "sf_server_destroy": (None, [_vp]),
 }
 
 STATIC_MAX_BRICKS = 8192
@@ -213,6 +265,30 @@ def default_params(**kw) -> Params:
     return p
 
 
+def fill_scene_desc(d: SceneDesc, s: Scene) -> SceneDesc:
+    """Point a SceneDesc at a (contiguous) scene's arrays; the scene must outlive the calls that read it."""
+    d.n_static = s.n_static
+    d.static_xyz = _ptr(s.static_xyz, C.c_int32)
+    d.static_mat = _ptr(s.static_mat, C.c_uint8)
+    d.static_sid = _ptr(s.static_sid, C.c_int32)
+    d.static_infill = _ptr(s.static_infill, C.c_uint8)
+    d.n_bodies = s.n_bodies
+    d.body_first = _ptr(s.body_first, C.c_uint32)
+    d.body_brick_xyz = _ptr(s.body_brick_xyz, C.c_int32)
+    d.body_brick_mat = _ptr(s.body_brick_mat, C.c_uint8)
+    d.body_pose = _ptr(s.body_pose, C.c_float)
+    return d
+
+
+def world_desc(scenes):
+    """(WorldDesc, keep-alive) for a list of scenes."""
+    scenes = [s.contiguous() for s in scenes]
+    descs = (SceneDesc * len(scenes))()
+    for d, s in zip(descs, scenes):
+        fill_scene_desc(d, s)
+    return WorldDesc(len(scenes), descs, 0), (scenes, descs)
+
+
 class World:
     """A set of independent scenes resident on the GPU, stepped together (one launch per phase for all)."""
 
@@ -222,19 +298,7 @@ class World:
         if isinstance(scenes, Scene):
             scenes = [scenes]
         self.scenes = [s.contiguous() for s in scenes]
-        descs = (SceneDesc * len(self.scenes))()
-        for d, s in zip(descs, self.scenes):
-            d.n_static = s.n_static
-            d.static_xyz = _ptr(s.static_xyz, C.c_int32)
-            d.static_mat = _ptr(s.static_mat, C.c_uint8)
-            d.static_sid = _ptr(s.static_sid, C.c_int32)
-            d.static_infill = _ptr(s.static_infill, C.c_uint8)
-            d.n_bodies = s.n_bodies
-            d.body_first = _ptr(s.body_first, C.c_uint32)
-            d.body_brick_xyz = _ptr(s.body_brick_xyz, C.c_int32)
-            d.body_brick_mat = _ptr(s.body_brick_mat, C.c_uint8)
-            d.body_pose = _ptr(s.body_pose, C.c_float)
-        wd = WorldDesc(len(self.scenes), descs, 0)
+        wd, _keep = world_desc(self.scenes)
         self.params = params if params is not None else default_params(**param_kw)
         h = C.c_void_p()
         _check(lib.sf_world_create(C.byref(wd), C.byref(self.params), C.byref(h)), "sf_world_create")

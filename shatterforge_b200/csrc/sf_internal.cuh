@@ -164,6 +164,13 @@ struct Scene {
     uint32_t chunk_off, n_chunks;
 };
 
+// A scene pool keeps fixed-capacity scene slots (the Scene ranges above are the capacities); a slot holds one
+// loaded scene or nothing. Bodies past the loaded count are dead, bricks past it belong to the sentinel body.
+struct PoolSlot {
+    uint32_t bodies = 0, bricks = 0, statics = 0, chunks = 0;   // loaded counts
+    bool loaded = false;
+};
+
 }  // namespace sf
 
 struct sf_world {
@@ -210,6 +217,8 @@ struct sf_world {
 
     sf::SorState *sor = nullptr;
     sf::StepState *step = nullptr;
+    std::vector<sf::PoolSlot> pool;      // non-empty for a scene pool
+    uint32_t sentinel = 0xFFFFFFFFu;     // a scene pool's always-dead body
     sf_stats stats{};
 };
 
@@ -292,5 +301,10 @@ sf_status step_create(sf_world *w);
 void step_destroy(sf_world *w);
 // update_cache without gravity: rotation, world inverse inertia and brick positions of awake bodies
 cudaError_t refresh_poses(sf_world *w);
+// the step's active set: a scene marked live steps at the next step even if its bodies were asleep
+void step_mark_live(sf_world *w, uint32_t scene);
+void step_mark_all_live(sf_world *w);
+void step_set_live(sf_world *w, uint32_t scene, bool live);
+cudaError_t step_reset_labels(sf_world *w, uint32_t first_body, uint32_t n);
 sf_status read_error_word(sf_world *w);
 }  // namespace sf

@@ -132,6 +132,12 @@ __global__ void k_sor_init(uint32_t nst, unsigned long long *resid_buf, uint32_t
     resid[s] = 0.0;
 }
 
+// ext += value, in list order (a brick listed twice gets both, in order)
+__global__ void k_add_loads(uint32_t n, const uint32_t *brick, const float *value, float *ext) {
+    if (blockIdx.x * blockDim.x + threadIdx.x != 0) return;
+    for (uint32_t k = 0; k < n; k++) ext[brick[k]] += value[k];
+}
+
 // ---------------------------------------------------------------- the persistent red-black kernel
 constexpr int SOR_BLOCK = 256;
 constexpr int SOR_MAX_LOCAL_STRUCT = 8192;   // active flags kept in shared memory as bits
@@ -662,19 +668,35 @@ static sf_status sor_select(sf_world *w, int32_t structure, std::vector<uint32_t
     return SF_OK;
 }
 
-}  // namespace sf
+// a list of structures (each at most once)
+static sf_status sor_select_set(sf_world *w, const int32_t *ids, uint32_t n, std::vector<uint32_t> &act,
+                                std::vector<uint32_t> &chunks, std::vector<uint32_t> &req) {
+    SorState *st = w->sor;
+    uint32_t nst = w->n_struct;
+    act.assign(std::max<uint32_t>(nst, 1), 0);
+    chunks.clear();
+    req.clear();
+    for (uint32_t k = 0; k < n; k++) {
+        const int32_t q = ids[k];
+        if (q < 0 || (uint32_t)q >= nst) { set_error("structure %d does not exist", q); return SF_ERR_ARG; }
+        if (act[q]) { set_error("structure %d listed twice", q); return SF_ERR_ARG; }
+        if (!st->h_st_count[q]) continue;
+        act[q] = 1;
+        req.push_back((uint32_t)q);
+        chunks.insert(chunks.end(), st->st_chunk_list.begin() + st->st_chunk_start[q],
+                      st->st_chunk_list.begin() + st->st_chunk_start[q + 1]);
+    }
+    return SF_OK;
+}
 
-using namespace sf;
-
-extern "C" {
-
-sf_status sf_structure_solve(sf_world *w, int32_t structure, float omega, float tol, uint32_t max_sweeps,
-                             sf_solve_report *report) {
+static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, uint32_t n_ids, float omega, float tol,
+                            uint32_t max_sweeps, sf_solve_report *report) {
     if (!w) return SF_ERR_ARG;
+    if (!w->sor) { set_error("this world holds no load-path state (a scene pool)"); return SF_ERR_STATE; }
     if (!(omega > 0.0f && omega < 2.0f)) { set_error("omega %g outside (0, 2)", (double)omega); return SF_ERR_ARG; }
     SorState *st = w->sor;
     std::vector<uint32_t> act, chunks, req;
-    sf_status r = sor_select(w, structure, act, chunks, req);
+    sf_status r = ids ? sor_select_set(w, ids, n_ids, act, chunks, req) : sor_select(w, structure, act, chunks, req);
     if (r != SF_OK) return r;
     sf_solve_report rep{};
     if (chunks.empty() || max_sweeps == 0) { if (report) *report = rep; return SF_OK; }
@@ -723,9 +745,47 @@ sf_status sf_structure_solve(sf_world *w, int32_t structure, float omega, float 
     return e;
 }
 
+}  // namespace sf
+
+using namespace sf;
+
+extern "C" {
+
+sf_status sf_structure_solve(sf_world *w, int32_t structure, float omega, float tol, uint32_t max_sweeps,
+                             sf_solve_report *report) {
+    return solve_impl(w, structure, nullptr, 0, omega, tol, max_sweeps, report);
+}
+
+sf_status sf_structure_solve_set(sf_world *w, const int32_t *structures, uint32_t n, float omega, float tol,
+                                 uint32_t max_sweeps, sf_solve_report *report) {
+    if (!w || (n && !structures)) { set_error("null argument"); return SF_ERR_ARG; }
+    if (n == 0) { if (report) *report = sf_solve_report{}; return SF_OK; }
+    return solve_impl(w, -1, structures, n, omega, tol, max_sweeps, report);
+}
+
+sf_status sf_structure_add_loads(sf_world *w, uint32_t n, const uint32_t *brick, const float *value) {
+    if (!w || (n && (!brick || !value))) { set_error("null argument"); return SF_ERR_ARG; }
+    if (!w->sor) { set_error("this world holds no load-path state (a scene pool)"); return SF_ERR_STATE; }
+    if (n == 0) return SF_OK;
+    for (uint32_t k = 0; k < n; k++)
+        if (brick[k] >= w->ns) { set_error("static brick %u does not exist", brick[k]); return SF_ERR_ARG; }
+    DBuf<uint32_t> d_b;
+    DBuf<float> d_v;
+    cudaStream_t s = w->stream;
+    SF_CUDA(d_b.alloc(n)); SF_CUDA(d_v.alloc(n));
+    SF_CUDA(cudaMemcpyAsync(d_b.p, brick, (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemcpyAsync(d_v.p, value, (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    k_add_loads<<<grid_for(n, 256), 256, 0, s>>>(n, d_b.p, d_v.p, w->s_ext.p);
+    w->sor->launches++;
+    SF_CUDA(cudaGetLastError());
+    SF_CUDA(cudaStreamSynchronize(s));
+    return SF_OK;
+}
+
 // per-structure sweeps and residuals of the last solve (n_struct entries each)
 sf_status sf_read_solve_detail(sf_world *w, uint32_t *sweeps, double *resid) {
     if (!w) return SF_ERR_ARG;
+    if (!w->sor) { set_error("this world holds no load-path state (a scene pool)"); return SF_ERR_STATE; }
     uint32_t nst = w->n_struct;
     if (sweeps) SF_CUDA(cudaMemcpyAsync(sweeps, w->sor->sweeps.p, nst * 4, cudaMemcpyDeviceToHost, w->stream));
     if (resid) SF_CUDA(cudaMemcpyAsync(resid, w->sor->resid.p, nst * 8, cudaMemcpyDeviceToHost, w->stream));
@@ -735,6 +795,7 @@ sf_status sf_read_solve_detail(sf_world *w, uint32_t *sweeps, double *resid) {
 
 sf_status sf_structure_check(sf_world *w, int32_t structure, float dt, int32_t live, sf_check_report *report) {
     if (!w) return SF_ERR_ARG;
+    if (!w->sor) { set_error("this world holds no load-path state (a scene pool)"); return SF_ERR_STATE; }
     SorState *st = w->sor;
     std::vector<uint32_t> act, chunks, req;
     sf_status r = sor_select(w, structure, act, chunks, req);
@@ -778,6 +839,7 @@ sf_status sf_structure_check(sf_world *w, int32_t structure, float dt, int32_t l
 
 sf_status sf_structure_loads(sf_world *w, const int32_t *structures, uint32_t n_structures) {
     if (!w || (n_structures && !structures)) return SF_ERR_ARG;
+    if (!w->sor) { set_error("this world holds no load-path state (a scene pool)"); return SF_ERR_STATE; }
     SorState *st = w->sor;
     const uint32_t nst = w->n_struct, ns = w->ns, nd = w->nd, nb = w->nb;
     std::vector<uint32_t> listed(std::max<uint32_t>(nst, 1), 0);
@@ -818,6 +880,7 @@ sf_status sf_structure_loads(sf_world *w, const int32_t *structures, uint32_t n_
 
 sf_status sf_read_joints(sf_world *w, float *ratio4, float *bond4, uint8_t *decision4, uint32_t *crushed4) {
     if (!w) return SF_ERR_ARG;
+    if (!w->sor) { set_error("this world holds no load-path state (a scene pool)"); return SF_ERR_STATE; }
     SorState *st = w->sor;
     size_t nj = (size_t)w->ns * 4;
     cudaStream_t s = w->stream;

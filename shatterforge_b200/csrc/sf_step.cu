@@ -35,6 +35,8 @@ struct StepState {
     // hashed cell sort
     DBuf<uint64_t> ckey, ckey_alt;
     DBuf<uint32_t> cval, cval_alt;
+    DBuf<uint32_t> aw_flag, awk_pos, awk_list, inc_flag, inc_pos, bucket_bits, scene_awake, scene_bricks;
+    uint32_t n_awk = 0, n_inc = 0;
     DBuf<uint2> brange;
     DBuf<float4> srec;
     DBuf<uint32_t> sinfo;
@@ -98,7 +100,7 @@ static void prof_mark(sf_world *w) {
 }
 
 enum { DV_CONTACTS = 0, DV_MANIFOLDS = 1, DV_COLORS = 2, DV_ROUNDS = 3, DV_WL0 = 4, DV_WL1 = 5, DV_WL2 = 6,
-       DV_ALIVE = 7, DV_AWAKE = 8, DV_ISLANDS = 9, DV_PAIRS = 10, DV_N = 16 };
+       DV_ALIVE = 7, DV_AWAKE = 8, DV_ISLANDS = 9, DV_PAIRS = 10, DV_AWK = 11, DV_INC = 12, DV_N = 16 };
 
 // ---------------------------------------------------------------- pose cache
 // Kernels over bodies or bricks take the substep's active list (global ids of the bodies / bricks of the scenes
@@ -144,21 +146,80 @@ __global__ void k_brick_pos(uint32_t nd, const uint32_t *list, const uint32_t *k
 
 __device__ __forceinline__ int floor_cell(float x) { return __float2int_rz(floorf(x / S)); }
 
-// key = (the scene's index in the active set, hashed cell); bricks of dead bodies sort last
-__global__ void k_cell_keys(uint32_t nd, const uint32_t *list, uint64_t none_key, const uint32_t *kbody,
-                            const uint32_t *bscene, const uint32_t *scene_act, const uint8_t *alive, const float4 *wpos,
-                            uint64_t *key, uint32_t *val) {
+// The hash holds the bricks a bucket walk can meet: every awake brick, and each other live brick whose bucket is one
+// of the 27 around an awake brick (gen_contacts walks only those buckets, so a brick outside them is never read; the
+// walk's order inside a bucket, by brick index, is unchanged by leaving it out). A scene with more than 1/8 of its
+// bricks awake simply puts every live brick in (marking would cost more than it saves).
+__global__ void k_awake_flags(uint32_t nd, const uint32_t *list, const uint32_t *kbody, const uint32_t *bscene,
+                              const uint32_t *scene_act, const uint8_t *alive, const uint8_t *asleep, uint32_t *flag,
+                              uint32_t *scene_awake) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t aw = 0, sk = NONE;
+    if (t < nd) {
+        const uint32_t b = kbody[pick(list, t)];
+        aw = (alive[b] && !asleep[b]) ? 1u : 0u;
+        flag[t] = aw;
+        if (aw) sk = scene_act[bscene[b]];
+    }
+    // one atomic per (warp, scene) group
+    const unsigned peers = __match_any_sync(0xffffffffu, sk);
+    if (sk != NONE && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&scene_awake[sk], __popc(peers));
+}
+__device__ __forceinline__ bool scene_full(const uint32_t *scene_awake, const uint32_t *scene_bricks, uint32_t sk) {
+    return (uint64_t)scene_awake[sk] * 8 > scene_bricks[sk];
+}
+__global__ void k_compact_list(uint32_t nd, const uint32_t *list, const uint32_t *flag, const uint32_t *pos, uint32_t *out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nd && flag[t]) out[pos[t]] = pick(list, t);
+}
+// each awake brick marks the 27 buckets around it in its scene's bitmap (32768 bits per active scene)
+__global__ void k_mark_buckets(const uint32_t *n_p, const uint32_t *awk, const uint32_t *kbody, const uint32_t *bscene,
+                               const uint32_t *scene_act, const uint32_t *scene_awake, const uint32_t *scene_bricks,
+                               const float4 *wpos, uint32_t *bits) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= *n_p) return;
+    const uint32_t i = awk[u];
+    const uint32_t sk = scene_act[bscene[kbody[i]]];
+    if (scene_full(scene_awake, scene_bricks, sk)) return;
+    const float4 p = wpos[i];
+    const int hx = floor_cell(p.x), hy = floor_cell(p.y), hz = floor_cell(p.z);
+    uint32_t *sb = bits + (size_t)sk * (HSIZE / 32);
+    for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+                const uint32_t h = hkey(hx + dx, hy + dy, hz + dz);
+                const uint32_t m = 1u << (h & 31);
+                if (!(__ldcg(&sb[h >> 5]) & m)) atomicOr(&sb[h >> 5], m);
+            }
+}
+// key = (the scene's index in the active set, hashed cell), flagged when the brick goes into the hash
+__global__ void k_cell_keys(uint32_t nd, const uint32_t *list, const uint32_t *kbody, const uint32_t *bscene,
+                            const uint32_t *scene_act, const uint32_t *scene_awake, const uint32_t *scene_bricks,
+                            const uint8_t *alive, const uint8_t *asleep, const float4 *wpos, const uint32_t *bits,
+                            uint64_t *key, uint32_t *val, uint32_t *inc) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nd) return;
     const uint32_t i = pick(list, t);
-    uint32_t b = kbody[i];
-    uint64_t k = none_key;
+    const uint32_t b = kbody[i];
+    uint32_t in = 0;
     if (alive[b]) {
-        float4 p = wpos[i];
-        k = (uint64_t)scene_act[bscene[b]] * HSIZE + hkey(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z));
+        const float4 p = wpos[i];
+        const uint32_t sk = scene_act[bscene[b]];
+        const uint32_t h = hkey(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z));
+        in = !asleep[b] || scene_full(scene_awake, scene_bricks, sk) ||
+             ((bits[(size_t)sk * (HSIZE / 32) + (h >> 5)] >> (h & 31)) & 1u);
+        key[t] = (uint64_t)sk * HSIZE + h;
+        val[t] = i;
     }
-    key[t] = k;
-    val[t] = i;
+    inc[t] = in;
+}
+__global__ void k_compact_keys(uint32_t nd, const uint32_t *inc, const uint32_t *pos, const uint64_t *key_in,
+                               const uint32_t *val_in, uint64_t *key, uint32_t *val) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nd || !inc[t]) return;
+    const uint32_t o = pos[t];
+    key[o] = key_in[t];
+    val[o] = val_in[t];
 }
 
 __global__ void k_bucket_ranges(uint32_t nd, uint64_t none_key, const uint64_t *key, uint2 *brange) {
@@ -619,13 +680,21 @@ struct SolveArgs {
     uint32_t *err;
 };
 
+// Body velocities and impulses written by other blocks are read through L2 (__ldcg) in the grid-wide solve; in the
+// one-block solve every write is the block's own, ordered by __syncthreads, so plain (L1-cached) loads are exact.
+template <bool ONE_BLOCK> __device__ __forceinline__ float4 ld_rw(const float4 *p) {
+    if (ONE_BLOCK) return *p;
+    return __ldcg(p);
+}
+
+template <bool ONE_BLOCK>
 __device__ __forceinline__ void solve_manifold(const SolveArgs &A, uint32_t m) {
     const uint32_t a = A.man_a[m], b = A.man_b[m];
     const bool hasb = b != STATIC;
     const uint32_t s0 = A.man_start[m], cnt = A.man_count[m];
-    float4 t4 = __ldcg(&A.v[a]);
+    float4 t4 = ld_rw<ONE_BLOCK>(&A.v[a]);
     V3 va = v3(t4.x, t4.y, t4.z);
-    t4 = __ldcg(&A.w[a]);
+    t4 = ld_rw<ONE_BLOCK>(&A.w[a]);
     V3 wa = v3(t4.x, t4.y, t4.z);
     const float ima = A.im[a];
     float ia[9], ib[9];
@@ -634,8 +703,8 @@ __device__ __forceinline__ void solve_manifold(const SolveArgs &A, uint32_t m) {
     V3 vb = v3(0.0f, 0.0f, 0.0f), wb = v3(0.0f, 0.0f, 0.0f);
     float imb = 0.0f;
     if (hasb) {
-        t4 = __ldcg(&A.v[b]); vb = v3(t4.x, t4.y, t4.z);
-        t4 = __ldcg(&A.w[b]); wb = v3(t4.x, t4.y, t4.z);
+        t4 = ld_rw<ONE_BLOCK>(&A.v[b]); vb = v3(t4.x, t4.y, t4.z);
+        t4 = ld_rw<ONE_BLOCK>(&A.w[b]); wb = v3(t4.x, t4.y, t4.z);
         imb = A.im[b];
 #pragma unroll
         for (int q = 0; q < 9; q++) ib[q] = A.iiw[(size_t)b * 9 + q];
@@ -644,14 +713,14 @@ __device__ __forceinline__ void solve_manifold(const SolveArgs &A, uint32_t m) {
     float4 nx_n = make_float4(0, 0, 0, 0), nx_t1 = nx_n, nx_t2 = nx_n, nx_ra = nx_n, nx_rb = nx_n, nx_j = nx_n;
     if (cnt) {
         nx_n = __ldg(&A.S_n[s0]); nx_t1 = __ldg(&A.S_t1[s0]); nx_t2 = __ldg(&A.S_t2[s0]);
-        nx_ra = __ldg(&A.S_ra[s0]); nx_rb = __ldg(&A.S_rb[s0]); nx_j = __ldcg(&A.S_j[s0]);
+        nx_ra = __ldg(&A.S_ra[s0]); nx_rb = __ldg(&A.S_rb[s0]); nx_j = ld_rw<ONE_BLOCK>(&A.S_j[s0]);
     }
     for (uint32_t k = s0; k < s0 + cnt; k++) {
         const float4 n4 = nx_n, t14 = nx_t1, t24 = nx_t2, ra4 = nx_ra, rb4 = nx_rb;
         float4 j4 = nx_j;
         if (k + 1 < s0 + cnt) {
             nx_n = __ldg(&A.S_n[k + 1]); nx_t1 = __ldg(&A.S_t1[k + 1]); nx_t2 = __ldg(&A.S_t2[k + 1]);
-            nx_ra = __ldg(&A.S_ra[k + 1]); nx_rb = __ldg(&A.S_rb[k + 1]); nx_j = __ldcg(&A.S_j[k + 1]);
+            nx_ra = __ldg(&A.S_ra[k + 1]); nx_rb = __ldg(&A.S_rb[k + 1]); nx_j = ld_rw<ONE_BLOCK>(&A.S_j[k + 1]);
         }
         const V3 n = v3(n4.x, n4.y, n4.z), t1 = v3(t14.x, t14.y, t14.z), t2 = v3(t24.x, t24.y, t24.z);
         const V3 ra = v3(ra4.x, ra4.y, ra4.z), rb = v3(rb4.x, rb4.y, rb4.z);
@@ -702,8 +771,22 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) k_solve(SolveArgs A) {
     for (uint32_t it = 0; it < A.iterations; it++) {
         for (uint32_t c = 0; c < ncol; c++) {
             const uint32_t s0 = A.col_start[c], s1 = A.col_start[c + 1];
-            for (uint32_t t = s0 + blockIdx.x * blockDim.x + threadIdx.x; t < s1; t += stride) solve_manifold(A, A.col_list[t]);
+            for (uint32_t t = s0 + blockIdx.x * blockDim.x + threadIdx.x; t < s1; t += stride) solve_manifold<false>(A, A.col_list[t]);
             if (!grid_sync(A.gb, gridDim.x, A.err)) return;
+        }
+    }
+}
+
+// small substeps: one block, colours separated by __syncthreads instead of a grid barrier
+constexpr int SOLVE_ONE_BLOCK = 512;
+constexpr uint32_t SOLVE_ONE_BLOCK_MAX_CONTACTS = 8192;
+__global__ void __launch_bounds__(SOLVE_ONE_BLOCK) k_solve_one_block(SolveArgs A) {
+    const uint32_t ncol = A.dev[DV_COLORS];
+    for (uint32_t it = 0; it < A.iterations; it++) {
+        for (uint32_t c = 0; c < ncol; c++) {
+            const uint32_t s0 = A.col_start[c], s1 = A.col_start[c + 1];
+            for (uint32_t t = s0 + threadIdx.x; t < s1; t += blockDim.x) solve_manifold<true>(A, A.col_list[t]);
+            __syncthreads();
         }
     }
 }
@@ -968,6 +1051,10 @@ sf_status step_create(sf_world *w) {
     const uint32_t nsc = std::max<uint32_t>(w->n_scenes, 1);
     cudaStream_t s = w->stream;
     SF_CUDA(S->ckey.alloc(nd)); SF_CUDA(S->ckey_alt.alloc(nd)); SF_CUDA(S->cval.alloc(nd)); SF_CUDA(S->cval_alt.alloc(nd));
+    SF_CUDA(S->aw_flag.alloc(nd)); SF_CUDA(S->awk_pos.alloc(nd)); SF_CUDA(S->awk_list.alloc(nd));
+    SF_CUDA(S->inc_flag.alloc(nd)); SF_CUDA(S->inc_pos.alloc(nd));
+    SF_CUDA(S->bucket_bits.alloc((size_t)nsc * (HSIZE / 32)));
+    SF_CUDA(S->scene_awake.alloc(nsc)); SF_CUDA(S->scene_bricks.alloc(nsc));
     SF_CUDA(S->brange.alloc((size_t)nsc * HSIZE));
     SF_CUDA(S->srec.alloc(nd)); SF_CUDA(S->sinfo.alloc(nd));
     SF_CUDA(S->slot_id.alloc((size_t)nd * CSLOTS)); SF_CUDA(S->slot_p.alloc((size_t)nd * CSLOTS)); SF_CUDA(S->slot_n.alloc((size_t)nd * CSLOTS));
@@ -1050,14 +1137,17 @@ static sf_status set_active(sf_world *w, const uint8_t *mask) {
         }
     std::vector<uint32_t> scene_act(std::max<uint32_t>(w->n_scenes, 1), NONE);
     std::vector<uint4> seg(std::max<size_t>(act.size(), 1));
+    std::vector<uint32_t> nbr(std::max<size_t>(act.size(), 1), 0);
     uint32_t nb_act = 0, nd_act = 0;
     for (size_t k = 0; k < act.size(); k++) {
         const Scene &sc = w->scenes[act[k]];
         scene_act[act[k]] = (uint32_t)k;
         seg[k] = make_uint4(sc.body_off, nb_act, sc.brick_off, nd_act);
+        nbr[k] = sc.n_bricks;
         nb_act += sc.n_bodies;
         nd_act += sc.n_bricks;
     }
+    SF_CUDA(cudaMemcpyAsync(S->scene_bricks.p, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice, s));
     SF_CUDA(cudaMemcpyAsync(S->scene_act.p, scene_act.data(), scene_act.size() * 4, cudaMemcpyHostToDevice, s));
     SF_CUDA(cudaMemcpyAsync(S->seg.p, seg.data(), seg.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
     const uint32_t n = std::max(nb_act, nd_act);
@@ -1103,27 +1193,48 @@ static sf_status substep(sf_world *w, float h) {
                                                   w->b_rot.p, w->k_local.p, w->k_wpos.p);
     L += 2;
     prof_mark(w);
-    // hashed cells
-    k_cell_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, none_key, w->k_body.p, w->b_scene.p, S->scene_act.p,
-                                                  w->b_alive.p, w->k_wpos.p, S->ckey.p, S->cval.p);
-    SF_CUDA(radix_sort_u64(S->ckey.p, S->cval.p, S->ckey_alt.p, S->cval_alt.p, nd, bits_for(none_key), S->wk, s));
+    // awake bricks (in active-list order) and the hashed cells they can reach
+    SF_CUDA(cudaMemsetAsync(S->scene_awake.p, 0, S->act.size() * 4, s));
+    k_awake_flags<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, w->k_body.p, w->b_scene.p, S->scene_act.p, w->b_alive.p,
+                                                    w->b_asleep.p, S->aw_flag.p, S->scene_awake.p);
+    SF_CUDA(exclusive_scan_u32(S->aw_flag.p, S->awk_pos.p, nd, S->dev.p + DV_AWK, S->wk, s));
+    k_compact_list<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, S->aw_flag.p, S->awk_pos.p, S->awk_list.p);
+    SF_CUDA(cudaMemsetAsync(S->bucket_bits.p, 0, (size_t)S->act.size() * (HSIZE / 32) * 4, s));
+    k_mark_buckets<<<grid_for(nd, 128), 128, 0, s>>>(S->dev.p + DV_AWK, S->awk_list.p, w->k_body.p, w->b_scene.p,
+                                                     S->scene_act.p, S->scene_awake.p, S->scene_bricks.p, w->k_wpos.p,
+                                                     S->bucket_bits.p);
+    k_cell_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, w->k_body.p, w->b_scene.p, S->scene_act.p, S->scene_awake.p,
+                                                  S->scene_bricks.p, w->b_alive.p, w->b_asleep.p, w->k_wpos.p,
+                                                  S->bucket_bits.p, S->ckey_alt.p, S->cval_alt.p, S->inc_flag.p);
+    SF_CUDA(exclusive_scan_u32(S->inc_flag.p, S->inc_pos.p, nd, S->dev.p + DV_INC, S->wk, s));
+    k_compact_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, S->inc_flag.p, S->inc_pos.p, S->ckey_alt.p, S->cval_alt.p,
+                                                     S->ckey.p, S->cval.p);
+    L += 5;
+    SF_CUDA(cudaMemcpyAsync(S->h_dev + DV_AWK, S->dev.p + DV_AWK, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    const uint32_t n_awk = S->h_dev[DV_AWK], n_inc = S->h_dev[DV_INC];
+    S->n_awk = n_awk;
+    S->n_inc = n_inc;
+    SF_CUDA(radix_sort_u64(S->ckey.p, S->cval.p, S->ckey_alt.p, S->cval_alt.p, n_inc, bits_for(none_key), S->wk, s));
     SF_CUDA(cudaMemsetAsync(S->brange.p, 0, (size_t)S->act.size() * HSIZE * sizeof(uint2), s));
-    k_bucket_ranges<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, S->ckey.p, S->brange.p);
-    k_bucket_records<<<grid_for(nd, 256), 256, 0, s>>>(nd, S->cval.p, w->k_body.p, w->k_mat.p, w->b_asleep.p, w->k_wpos.p,
-                                                       S->srec.p, S->sinfo.p);
-    L += 3;
+    if (n_inc) {
+        k_bucket_ranges<<<grid_for(n_inc, 256), 256, 0, s>>>(n_inc, none_key, S->ckey.p, S->brange.p);
+        k_bucket_records<<<grid_for(n_inc, 256), 256, 0, s>>>(n_inc, S->cval.p, w->k_body.p, w->k_mat.p, w->b_asleep.p,
+                                                              w->k_wpos.p, S->srec.p, S->sinfo.p);
+        L += 2;
+    }
     prof_mark(w);
     // contacts: generate into slots and count, scan, place in list order
     ContactArgs C;
-    C.nd = nd; C.list = klist; C.scene_act = S->scene_act.p;
+    C.nd = n_awk; C.list = S->awk_list.p; C.scene_act = S->scene_act.p;
     C.sbox = w->sbox.p; C.kbody = w->k_body.p; C.bscene = w->b_scene.p; C.ctab = w->ctab.p; C.cpool = w->cpool.p;
     C.alive = w->b_alive.p; C.asleep = w->b_asleep.p; C.smat = w->s_mat.p; C.wpos = w->k_wpos.p;
     C.v = w->b_v.p; C.w = w->b_w.p; C.rot = w->b_rot.p; C.rad = w->b_rad.p; C.brange = S->brange.p; C.srec = S->srec.p;
     C.sinfo = S->sinfo.p; C.ccount = S->ccount.p; C.coff = S->coff.p; C.wake = w->b_wake.p;
     C.slot_id = S->slot_id.p; C.slot_p = S->slot_p.p; C.slot_n = S->slot_n.p;
     C.L_a = S->L_a.p; C.L_b = S->L_b.p; C.L_bo = S->L_bo.p; C.L_ba = S->L_ba.p; C.L_bb = S->L_bb.p; C.L_p = S->L_p.p; C.L_n = S->L_n.p;
-    k_contacts_gen<<<grid_for(nd, 128), 128, 0, s>>>(C);
-    SF_CUDA(exclusive_scan_u32(S->ccount.p, S->coff.p, nd, S->dev.p + DV_CONTACTS, S->wk, s));
+    if (n_awk) k_contacts_gen<<<grid_for(n_awk, 128), 128, 0, s>>>(C);
+    SF_CUDA(exclusive_scan_u32(S->ccount.p, S->coff.p, n_awk, S->dev.p + DV_CONTACTS, S->wk, s));
     SF_CUDA(cudaMemcpyAsync(S->h_dev, S->dev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     SF_CUDA(cudaStreamSynchronize(s));
     const uint32_t nc = S->h_dev[DV_CONTACTS];
@@ -1133,7 +1244,7 @@ static sf_status substep(sf_world *w, float h) {
         SF_CUDA(grow_contacts(S, nc));
         C.L_a = S->L_a.p; C.L_b = S->L_b.p; C.L_bo = S->L_bo.p; C.L_ba = S->L_ba.p; C.L_bb = S->L_bb.p; C.L_p = S->L_p.p; C.L_n = S->L_n.p;
     }
-    k_contacts_place<<<grid_for(nd, 128), 128, 0, s>>>(C);
+    if (n_awk) k_contacts_place<<<grid_for(n_awk, 128), 128, 0, s>>>(C);
     SF_CUDA(cudaMemsetAsync(S->dev.p + DV_MANIFOLDS, 0, (DV_N - DV_MANIFOLDS) * sizeof(uint32_t), s));
     const uint32_t g_nc = grid_for(std::max<uint32_t>(nc, 1), 256);
     if (nc) { k_body_nc<<<g_nc, 256, 0, s>>>(nc, S->L_a.p, S->L_b.p, w->b_nc.p); L++; }
@@ -1207,10 +1318,14 @@ static sf_status substep(sf_world *w, float h) {
         A.man_a = S->man_a.p; A.man_b = S->man_b.p; A.man_start = S->man_start.p; A.man_count = S->man_count.p;
         A.S_n = S->S_n.p; A.S_t1 = S->S_t1.p; A.S_t2 = S->S_t2.p; A.S_ra = S->S_ra.p; A.S_rb = S->S_rb.p; A.S_j = S->S_j.p;
         A.v = w->b_v.p; A.w = w->b_w.p; A.im = w->b_im.p; A.iiw = w->b_iiw.p; A.gb = w->barrier.p; A.err = w->err.p;
-        unsigned per_sm = w->P.solve_blocks ? std::min<unsigned>(w->P.solve_blocks, S->solve_occ) : std::min(S->solve_occ, 2);
-        unsigned sgrid = (unsigned)std::min<uint64_t>((uint64_t)w->sms * per_sm, (nc + SOLVE_BLOCK - 1) / SOLVE_BLOCK + 1);
-        void *sargs[] = {&A};
-        SF_CUDA(cudaLaunchCooperativeKernel((void *)k_solve, dim3(sgrid), dim3(SOLVE_BLOCK), sargs, 0, s));
+        if (nc <= SOLVE_ONE_BLOCK_MAX_CONTACTS) {
+            k_solve_one_block<<<1, SOLVE_ONE_BLOCK, 0, s>>>(A);
+        } else {
+            unsigned per_sm = w->P.solve_blocks ? std::min<unsigned>(w->P.solve_blocks, S->solve_occ) : std::min(S->solve_occ, 2);
+            unsigned sgrid = (unsigned)std::min<uint64_t>((uint64_t)w->sms * per_sm, (nc + SOLVE_BLOCK - 1) / SOLVE_BLOCK + 1);
+            void *sargs[] = {&A};
+            SF_CUDA(cudaLaunchCooperativeKernel((void *)k_solve, dim3(sgrid), dim3(SOLVE_BLOCK), sargs, 0, s));
+        }
         L++;
         S->solve_launches++;
         S->solve_contact_iters += (uint64_t)nc * w->P.iterations;
@@ -1378,14 +1493,19 @@ sf_status sf_read_contacts(sf_world *w, uint32_t scene, uint32_t *ids5, float *f
     const Scene &sc = w->scenes[scene];
     uint32_t nc = (uint32_t)S->last_contacts;
     cudaStream_t s = w->stream;
-    // the scene's contacts are the list range of its bricks in the last substep's active list (none if it was idle)
+    // the scene's contacts are the list range of its awake bricks in the last substep (none if it was idle): the
+    // awake list is the active list's awake bricks in order, so the scene's bricks map to one run of it
     uint32_t lo = 0, hi = 0;
     const uint32_t kb = S->act_brick_base[scene];
-    if (sc.n_bricks && kb != NONE) {
-        SF_CUDA(cudaMemcpyAsync(&lo, S->coff.p + kb, 4, cudaMemcpyDeviceToHost, s));
-        if (kb + sc.n_bricks < S->nd_act) SF_CUDA(cudaMemcpyAsync(&hi, S->coff.p + kb + sc.n_bricks, 4, cudaMemcpyDeviceToHost, s));
+    if (sc.n_bricks && kb != NONE && S->n_awk) {
+        uint32_t a0 = 0, a1 = S->n_awk;
+        SF_CUDA(cudaMemcpyAsync(&a0, S->awk_pos.p + kb, 4, cudaMemcpyDeviceToHost, s));
+        if (kb + sc.n_bricks < S->nd_act) SF_CUDA(cudaMemcpyAsync(&a1, S->awk_pos.p + kb + sc.n_bricks, 4, cudaMemcpyDeviceToHost, s));
         SF_CUDA(cudaStreamSynchronize(s));
-        if (kb + sc.n_bricks >= S->nd_act) hi = nc;
+        lo = nc; hi = nc;
+        if (a0 < S->n_awk) SF_CUDA(cudaMemcpyAsync(&lo, S->coff.p + a0, 4, cudaMemcpyDeviceToHost, s));
+        if (a1 < S->n_awk) SF_CUDA(cudaMemcpyAsync(&hi, S->coff.p + a1, 4, cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaStreamSynchronize(s));
     }
     uint64_t cnt = hi - lo;
     if (n) *n = cnt;

@@ -22,10 +22,9 @@ void host_mat_tables(MatTables &t) {
     }
 }
 
-static std::mutex g_err_mu;
-static char g_err[512] = "";
+// the last error of the calling thread (the server's worker threads report their own)
+static thread_local char g_err[512] = "";
 void set_error(const char *fmt, ...) {
-    std::lock_guard<std::mutex> lk(g_err_mu);
     va_list ap;
     va_start(ap, fmt);
     vsnprintf(g_err, sizeof g_err, fmt, ap);

@@ -21,11 +21,13 @@ __device__ __forceinline__ uint32_t grid_get(const uint32_t *ctab, const uint32_
     return cpool[(size_t)(t - 1) * 512 + cell_in_chunk(x, y, z)];
 }
 
-__global__ void k_finalize_bricks(uint32_t ns, const uint32_t *cell, const uint32_t *scene, const uint8_t *mat,
+// static bricks base .. base + ns - 1
+__global__ void k_finalize_bricks(uint32_t ns, uint32_t base, const uint32_t *cell, const uint32_t *scene, const uint8_t *mat,
                                   const uint8_t *infill, const int32_t *sid, const uint32_t *ctab, const uint32_t *cpool,
                                   uint32_t *nb6, float *bond, float *bmax) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ns) return;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ns) return;
+    const uint32_t i = base + t;
     int x, y, z;
     unpack_cell(cell[i], x, y, z);
     uint32_t sc = scene[i];
@@ -59,14 +61,16 @@ __global__ void k_finalize_bricks(uint32_t ns, const uint32_t *cell, const uint3
     bmax[(size_t)i * 4 + 3] = f;
 }
 
-// one thread per body, its bricks in list order (the sums must round in the reference's order)
-__global__ void k_setup_bodies(uint32_t nb, const uint32_t *first, const uint32_t *count, const int32_t *xyz,
+// one thread per body, its bricks in list order (the sums must round in the reference's order); bodies
+// base .. base + nb - 1, their poses at pose13[0 ..]
+__global__ void k_setup_bodies(uint32_t nb, uint32_t base, const uint32_t *first, const uint32_t *count, const int32_t *xyz,
                                const uint8_t *kmat, const float *pose13, float4 *local, float4 *wpos, uint32_t *kbody,
                                float4 *pos, float4 *q, float4 *v, float4 *w, float *rot, float *iil, float *iiw,
                                float *m, float *im, float *rad, float *sleep, float *maxr, uint8_t *alive, uint8_t *asleep,
                                uint8_t *wake) {
-    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
+    const uint32_t lb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lb >= nb) return;
+    const uint32_t b = base + lb;
     uint32_t s = first[b], n = count[b];
     float mass = 0.0f;
     V3 cl = v3(0.0f, 0.0f, 0.0f);
@@ -111,7 +115,7 @@ __global__ void k_setup_bodies(uint32_t nb, const uint32_t *first, const uint32_
             inv[6] = c2 * id; inv[7] = (a[1] * a[6] - a[0] * a[7]) * id; inv[8] = (a[0] * a[4] - a[1] * a[3]) * id;
         }
     }
-    const float *ps = pose13 + (size_t)b * 13;
+    const float *ps = pose13 + (size_t)lb * 13;
     float prot[9];
     q_to_m(ps[3], ps[4], ps[5], ps[6], prot);
     V3 off = mv(prot, cl);
@@ -172,7 +176,7 @@ cudaError_t finalize_on_buffers(uint32_t ns, const uint32_t *cell, const uint32_
                                 uint32_t *nb6, float *bond, float *bmax, cudaStream_t s) {
     cudaError_t e = upload_mat_tables(s);
     if (e != cudaSuccess || ns == 0) return e;
-    k_finalize_bricks<<<grid_for(ns, 256), 256, 0, s>>>(ns, cell, scene, mat, infill, sid, ctab, cpool, nb6, bond, bmax);
+    k_finalize_bricks<<<grid_for(ns, 256), 256, 0, s>>>(ns, 0u, cell, scene, mat, infill, sid, ctab, cpool, nb6, bond, bmax);
     return cudaGetLastError();
 }
 
@@ -330,7 +334,7 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
     SF_CUDA(cudaMemsetAsync(w->s_ext.p, 0, w->s_ext.bytes(), st));
     SF_CUDA(cudaMemsetAsync(w->s_stress.p, 0, w->s_stress.bytes(), st));
     if (ns) {
-        k_finalize_bricks<<<grid_for(ns, 256), 256, 0, st>>>((uint32_t)ns, w->s_cell.p, w->s_scene.p, w->s_mat.p,
+        k_finalize_bricks<<<grid_for(ns, 256), 256, 0, st>>>((uint32_t)ns, 0u, w->s_cell.p, w->s_scene.p, w->s_mat.p,
                                                            w->s_infill.p, w->s_sid.p, w->ctab.p, w->cpool.p, w->s_nb6.p,
                                                            w->s_bond.p, w->s_bmax.p);
         SF_CUDA(cudaGetLastError());
@@ -373,7 +377,7 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
     SF_CUDA(cudaMemsetAsync(w->b_nc.p, 0, w->b_nc.bytes(), st));
     SF_CUDA(w->k_local.alloc(nd)); SF_CUDA(w->k_wpos.alloc(nd)); SF_CUDA(w->k_body.alloc(nd));
     if (nb) {
-        k_setup_bodies<<<grid_for(nb, 128), 128, 0, st>>>((uint32_t)nb, w->b_first.p, w->b_count.p, w->k_xyz.p, w->k_mat.p,
+        k_setup_bodies<<<grid_for(nb, 128), 128, 0, st>>>((uint32_t)nb, 0u, w->b_first.p, w->b_count.p, w->k_xyz.p, w->k_mat.p,
                                                         d_pose.p, w->k_local.p, w->k_wpos.p, w->k_body.p, w->b_pos.p,
                                                         w->b_q.p, w->b_v.p, w->b_w.p, w->b_rot.p, w->b_iil.p, w->b_iiw.p,
                                                         w->b_m.p, w->b_im.p, w->b_rad.p, w->b_sleep.p, w->b_maxr.p,
@@ -451,6 +455,7 @@ sf_status sf_write_bodies(sf_world *w, const float *state13, const float *sleep,
                                                       w->b_w.p, w->b_alive.p, w->b_asleep.p);
     k_kill_marked<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, w->b_first.p, w->b_count.p, w->k_mat.p);
     w->launches += 2;
+    step_mark_all_live(w);
     SF_CUDA(cudaGetLastError());
     SF_CUDA(cudaStreamSynchronize(s));
     return SF_OK;
@@ -524,6 +529,328 @@ sf_status sf_read_bonds(sf_world *w, float *bond4, uint32_t *nb6, uint8_t *mat) 
     if (bond4) SF_CUDA(cudaMemcpyAsync(bond4, w->s_bond.p, (size_t)w->ns * 16, cudaMemcpyDeviceToHost, s));
     if (nb6) SF_CUDA(cudaMemcpyAsync(nb6, w->s_nb6.p, (size_t)w->ns * 24, cudaMemcpyDeviceToHost, s));
     if (mat) SF_CUDA(cudaMemcpyAsync(mat, w->s_mat.p, (size_t)w->ns, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    return SF_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- scene pools
+// A pool is a world laid out by capacity: slot s owns fixed ranges of bodies, bricks, static bricks and chunks,
+// and a scene is loaded into a slot, saved out of it and restored into it without touching the other slots. The
+// step's active set never includes an empty slot, so the pool's cost follows the loaded, awake scenes.
+namespace sf {
+
+// device bytes per unit of capacity (the arrays of sf_world, StepState and an initial 4 contacts per brick)
+constexpr uint64_t POOL_BYTES_BODY = 320, POOL_BYTES_BRICK = 1560, POOL_BYTES_STATIC = 96, POOL_BYTES_CHUNK = 2048;
+constexpr uint64_t POOL_BYTES_SLOT = (uint64_t)NCT * 4 + (uint64_t)HSIZE * 8 + 64;
+
+static uint64_t slot_bytes(const sf_pool_slot &c) {
+    return POOL_BYTES_SLOT + c.bodies * POOL_BYTES_BODY + c.bricks * POOL_BYTES_BRICK + c.statics * POOL_BYTES_STATIC +
+           c.chunks * POOL_BYTES_CHUNK;
+}
+
+// mutable state of a loaded scene, in this order: per body pos, q, v, w (float4), rot, iiw (9 floats), sleep
+// (float), alive, asleep (bytes); per brick world position (float4) and material (byte; 0 = removed)
+static uint64_t snapshot_bytes(uint64_t nb, uint64_t nd) { return nb * (64 + 72 + 4 + 2) + nd * (16 + 1); }
+
+struct SnapPart { void *dev; size_t elem; };
+
+static void snapshot_parts(sf_world *w, const Scene &sc, SnapPart parts[11]) {
+    const uint32_t b = sc.body_off, k = sc.brick_off;
+    parts[0] = {w->b_pos.p + b, 16}; parts[1] = {w->b_q.p + b, 16}; parts[2] = {w->b_v.p + b, 16};
+    parts[3] = {w->b_w.p + b, 16}; parts[4] = {w->b_rot.p + (size_t)b * 9, 36}; parts[5] = {w->b_iiw.p + (size_t)b * 9, 36};
+    parts[6] = {w->b_sleep.p + b, 4}; parts[7] = {w->b_alive.p + b, 1}; parts[8] = {w->b_asleep.p + b, 1};
+    parts[9] = {w->k_wpos.p + k, 16}; parts[10] = {w->k_mat.p + k, 1};
+}
+
+// validates a scene against a slot's capacity; a pool serves rigid scenes, so static bricks must not belong to a
+// structure
+static sf_status check_slot_scene(const sf_world *w, uint32_t slot, const sf_scene_desc *d) {
+    if (w->pool.empty()) { set_error("not a scene pool"); return SF_ERR_ARG; }
+    if (!d || slot >= w->pool.size()) { set_error("bad slot %u or null scene", slot); return SF_ERR_ARG; }
+    const Scene &sc = w->scenes[slot];
+    if (d->n_static && (!d->static_xyz || !d->static_mat || !d->static_sid || !d->static_infill)) { set_error("null static array"); return SF_ERR_ARG; }
+    if (d->n_bodies && (!d->body_first || !d->body_brick_xyz || !d->body_brick_mat || !d->body_pose)) { set_error("null body array"); return SF_ERR_ARG; }
+    const uint32_t nbr = d->n_bodies ? d->body_first[d->n_bodies] : 0;
+    if (d->n_bodies > sc.n_bodies || nbr > sc.n_bricks || d->n_static > sc.n_static) {
+        set_error("scene (%u bodies, %u bricks, %u static) exceeds slot %u (%u, %u, %u)", d->n_bodies, nbr, d->n_static,
+                  slot, sc.n_bodies, sc.n_bricks, sc.n_static);
+        return SF_ERR_CAPACITY;
+    }
+    if (d->n_bodies && d->body_first[0] != 0) { set_error("body_first[0] must be 0"); return SF_ERR_ARG; }
+    for (uint32_t b = 0; b < d->n_bodies; b++) {
+        if (d->body_first[b + 1] <= d->body_first[b]) { set_error("body %u: no bricks", b); return SF_ERR_ARG; }
+        for (int k = 0; k < 13; k++)
+            if (!std::isfinite(d->body_pose[(size_t)b * 13 + k])) { set_error("body %u: non-finite pose", b); return SF_ERR_ARG; }
+    }
+    for (uint32_t k = 0; k < nbr; k++)
+        if (d->body_brick_mat[k] == 0 || d->body_brick_mat[k] > 8) { set_error("body brick %u: material %u", k, d->body_brick_mat[k]); return SF_ERR_ARG; }
+    for (uint32_t k = 0; k < d->n_static; k++) {
+        const int x = d->static_xyz[3 * k], y = d->static_xyz[3 * k + 1], z = d->static_xyz[3 * k + 2];
+        if (!inb(x, y, z)) { set_error("static %u: cell (%d,%d,%d) outside the lattice", k, x, y, z); return SF_ERR_ARG; }
+        if (d->static_mat[k] == 0 || d->static_mat[k] > 8) { set_error("static %u: material %u", k, d->static_mat[k]); return SF_ERR_ARG; }
+        if (d->static_sid[k] != -1) { set_error("static %u: structure %d; a scene pool holds no load-path structures", k, d->static_sid[k]); return SF_ERR_ARG; }
+    }
+    return SF_OK;
+}
+
+}  // namespace sf
+
+extern "C" {
+
+sf_status sf_pool_bytes(uint32_t n_slots, const sf_pool_slot *slots, uint64_t *bytes) {
+    if (!bytes || (n_slots && !slots)) { set_error("null argument"); return SF_ERR_ARG; }
+    uint64_t t = 0;
+    for (uint32_t s = 0; s < n_slots; s++) t += slot_bytes(slots[s]);
+    *bytes = t;
+    return SF_OK;
+}
+
+uint64_t sf_pool_snapshot_bytes(uint32_t n_bodies, uint32_t n_bricks) { return snapshot_bytes(n_bodies, n_bricks); }
+
+sf_status sf_pool_create(uint32_t n_slots, const sf_pool_slot *slots, const sf_params *params, sf_world **out) {
+    if (!out || !n_slots || !slots) { set_error("null argument or no slots"); return SF_ERR_ARG; }
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { set_error("no CUDA device"); return SF_ERR_CUDA; }
+    std::unique_ptr<sf_world, void (*)(sf_world *)> w(new sf_world(), sf_world_destroy);
+    if (params) w->P = *params; else sf_params_default(&w->P);
+    if (w->P.substeps == 0) w->P.substeps = 2;
+    if (w->P.max_colors == 0 || w->P.max_colors > (uint32_t)MAXCOL) w->P.max_colors = MAXCOL;
+    SF_CUDA(cudaGetDevice(&w->device));
+    SF_CUDA(cudaDeviceGetAttribute(&w->sms, cudaDevAttrMultiProcessorCount, w->device));
+    SF_CUDA(cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking));
+    w->stream = w->own_stream;
+    SF_CUDA(cudaEventCreate(&w->ev0));
+    SF_CUDA(cudaEventCreate(&w->ev1));
+    SF_CUDA(upload_mat_tables(w->stream));
+    cudaStream_t st = w->stream;
+    w->n_scenes = n_slots;
+    w->scenes.resize(n_slots);
+    w->pool.assign(n_slots, PoolSlot{});
+    uint64_t ns = 0, nd = 0, nb = 0, nch = 0;
+    for (uint32_t s = 0; s < n_slots; s++) {
+        const sf_pool_slot &c = slots[s];
+        if (c.bodies == 0 || c.bricks < c.bodies) { set_error("slot %u: %u bodies, %u bricks", s, c.bodies, c.bricks); return SF_ERR_ARG; }
+        Scene &sc = w->scenes[s];
+        sc.static_off = (uint32_t)ns; sc.n_static = c.statics;
+        sc.body_off = (uint32_t)nb; sc.n_bodies = c.bodies;
+        sc.brick_off = (uint32_t)nd; sc.n_bricks = c.bricks;
+        sc.chunk_off = (uint32_t)nch; sc.n_chunks = c.chunks;
+        ns += c.statics; nd += c.bricks; nb += c.bodies; nch += c.chunks;
+    }
+    nb += 1;   // the sentinel body: never alive, owner of every unused brick
+    if (ns >= 0x7fffffffu || nd >= 0x7fffffffu || nb >= 0x7fffffffu || nch >= (1u << 24)) { set_error("pool too large"); return SF_ERR_CAPACITY; }
+    w->ns = (uint32_t)ns; w->nd = (uint32_t)nd; w->nb = (uint32_t)nb; w->n_chunks = (uint32_t)nch; w->n_struct = 0;
+    w->sentinel = (uint32_t)nb - 1;
+    // static grid: empty tables, static bricks absent (material 0, no structure)
+    SF_CUDA(w->ctab.alloc((size_t)n_slots * NCT)); SF_CUDA(cudaMemsetAsync(w->ctab.p, 0, w->ctab.bytes(), st));
+    SF_CUDA(w->cpool.alloc(std::max<uint64_t>(nch, 1) * 512)); SF_CUDA(cudaMemsetAsync(w->cpool.p, 0, w->cpool.bytes(), st));
+    w->h_sbox.assign((size_t)n_slots * 2, make_int4(0, 0, 0, 0));
+    for (uint32_t s = 0; s < n_slots; s++) {
+        w->h_sbox[2 * s] = make_int4(1 << 20, 1 << 20, 1 << 20, 0);
+        w->h_sbox[2 * s + 1] = make_int4(-(1 << 20), -(1 << 20), -(1 << 20), 0);
+    }
+    SF_CUDA(upload(w->sbox, w->h_sbox, st));
+    std::vector<uint32_t> s_scene(ns);
+    for (uint32_t s = 0; s < n_slots; s++)
+        std::fill(s_scene.begin() + w->scenes[s].static_off, s_scene.begin() + w->scenes[s].static_off + w->scenes[s].n_static, s);
+    SF_CUDA(upload(w->s_scene, s_scene, st));
+    std::vector<int32_t> s_sid(ns, -1);
+    SF_CUDA(upload(w->s_sid, s_sid, st));
+    SF_CUDA(w->s_cell.alloc(ns)); SF_CUDA(w->s_mat.alloc(ns)); SF_CUDA(w->s_infill.alloc(ns));
+    SF_CUDA(cudaMemsetAsync(w->s_mat.p, 0, w->s_mat.bytes(), st));
+    SF_CUDA(w->s_nb6.alloc((size_t)ns * 6)); SF_CUDA(w->s_bond.alloc((size_t)ns * 4)); SF_CUDA(w->s_bmax.alloc((size_t)ns * 4));
+    SF_CUDA(w->s_phi.alloc(ns)); SF_CUDA(w->s_phi64.alloc(ns)); SF_CUDA(w->s_ext.alloc(ns)); SF_CUDA(w->s_stress.alloc(ns));
+    // bodies: all dead; every brick belongs to the sentinel
+    std::vector<uint32_t> b_scene(nb, 0);
+    for (uint32_t s = 0; s < n_slots; s++)
+        std::fill(b_scene.begin() + w->scenes[s].body_off, b_scene.begin() + w->scenes[s].body_off + w->scenes[s].n_bodies, s);
+    SF_CUDA(upload(w->b_scene, b_scene, st));
+    SF_CUDA(w->b_first.alloc(nb)); SF_CUDA(w->b_count.alloc(nb));
+    SF_CUDA(cudaMemsetAsync(w->b_first.p, 0, w->b_first.bytes(), st));
+    SF_CUDA(cudaMemsetAsync(w->b_count.p, 0, w->b_count.bytes(), st));
+    SF_CUDA(w->k_xyz.alloc((size_t)nd * 3)); SF_CUDA(w->k_mat.alloc(nd));
+    SF_CUDA(cudaMemsetAsync(w->k_mat.p, 0, w->k_mat.bytes(), st));
+    std::vector<uint32_t> k_body(nd, w->sentinel);
+    SF_CUDA(upload(w->k_body, k_body, st));
+    SF_CUDA(w->b_pos.alloc(nb)); SF_CUDA(w->b_q.alloc(nb)); SF_CUDA(w->b_v.alloc(nb)); SF_CUDA(w->b_w.alloc(nb));
+    SF_CUDA(w->b_vpre.alloc(nb)); SF_CUDA(w->b_wpre.alloc(nb));
+    SF_CUDA(w->b_rot.alloc((size_t)nb * 9)); SF_CUDA(w->b_iil.alloc((size_t)nb * 9)); SF_CUDA(w->b_iiw.alloc((size_t)nb * 9));
+    SF_CUDA(w->b_m.alloc(nb)); SF_CUDA(w->b_im.alloc(nb)); SF_CUDA(w->b_rad.alloc(nb)); SF_CUDA(w->b_sleep.alloc(nb));
+    SF_CUDA(w->b_maxr.alloc(nb));
+    SF_CUDA(w->b_alive.alloc(nb)); SF_CUDA(w->b_asleep.alloc(nb)); SF_CUDA(w->b_wake.alloc(nb)); SF_CUDA(w->b_nc.alloc(nb));
+    SF_CUDA(cudaMemsetAsync(w->b_alive.p, 0, w->b_alive.bytes(), st));
+    SF_CUDA(cudaMemsetAsync(w->b_asleep.p, 0, w->b_asleep.bytes(), st));
+    SF_CUDA(cudaMemsetAsync(w->b_wake.p, 0, w->b_wake.bytes(), st));
+    SF_CUDA(cudaMemsetAsync(w->b_nc.p, 0, w->b_nc.bytes(), st));
+    SF_CUDA(w->k_local.alloc(nd)); SF_CUDA(w->k_wpos.alloc(nd));
+    SF_CUDA(w->err.alloc(64));
+    SF_CUDA(cudaMemsetAsync(w->err.p, 0, w->err.bytes(), st));
+    SF_CUDA(w->barrier.alloc(4));
+    SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, w->barrier.bytes(), st));
+    sf_status r = step_create(w.get());   // no load-path state: a pool holds rigid scenes only
+    if (r != SF_OK) return r;
+    for (uint32_t s = 0; s < n_slots; s++) step_set_live(w.get(), s, false);
+    SF_CUDA(cudaStreamSynchronize(st));
+    *out = w.release();
+    return SF_OK;
+}
+
+sf_status sf_pool_load(sf_world *w, uint32_t slot, const sf_scene_desc *d) {
+    if (!w) { set_error("null world"); return SF_ERR_ARG; }
+    sf_status r = check_slot_scene(w, slot, d);
+    if (r != SF_OK) return r;
+    const Scene &sc = w->scenes[slot];
+    cudaStream_t st = w->stream;
+    const uint32_t nbr = d->n_bodies ? d->body_first[d->n_bodies] : 0;
+    // static part: the slot's chunk table, its chunks and its static bricks
+    std::vector<uint32_t> ctab(NCT, 0), cpool((size_t)sc.n_chunks * 512, 0);
+    std::vector<uint32_t> s_cell(sc.n_static, 0);
+    std::vector<uint8_t> s_mat(sc.n_static, 0), s_inf(sc.n_static, 0);
+    uint32_t used = 0;
+    int4 lo = make_int4(1 << 20, 1 << 20, 1 << 20, 0), hi = make_int4(-(1 << 20), -(1 << 20), -(1 << 20), 0);
+    for (uint32_t k = 0; k < d->n_static; k++) {
+        const int x = d->static_xyz[3 * k], y = d->static_xyz[3 * k + 1], z = d->static_xyz[3 * k + 2];
+        uint32_t &t = ctab[chunk_slot(x, y, z)];
+        if (t == 0) {
+            if (used == sc.n_chunks) { set_error("scene needs more than the slot's %u chunks", sc.n_chunks); return SF_ERR_CAPACITY; }
+            t = sc.chunk_off + (++used);
+        }
+        uint32_t &cell = cpool[(size_t)(t - 1 - sc.chunk_off) * 512 + cell_in_chunk(x, y, z)];
+        if (cell) { set_error("static %u: cell (%d,%d,%d) already holds a brick", k, x, y, z); return SF_ERR_ARG; }
+        cell = sc.static_off + k + 1;
+        s_cell[k] = pack_cell(x, y, z);
+        s_mat[k] = d->static_mat[k];
+        s_inf[k] = (d->static_mat[k] == GLASS || d->static_infill[k]) ? 1 : 0;
+        lo.x = std::min(lo.x, x); lo.y = std::min(lo.y, y); lo.z = std::min(lo.z, z);
+        hi.x = std::max(hi.x, x); hi.y = std::max(hi.y, y); hi.z = std::max(hi.z, z);
+    }
+    w->h_sbox[2 * slot] = lo;
+    w->h_sbox[2 * slot + 1] = hi;
+    // bodies and bricks; unused bodies dead, unused bricks owned by the sentinel
+    std::vector<uint32_t> b_first(sc.n_bodies, 0), b_count(sc.n_bodies, 0), k_body(sc.n_bricks, w->sentinel);
+    std::vector<int32_t> k_xyz((size_t)sc.n_bricks * 3, 0);
+    std::vector<uint8_t> k_mat(sc.n_bricks, 0);
+    for (uint32_t b = 0; b < d->n_bodies; b++) {
+        b_first[b] = sc.brick_off + d->body_first[b];
+        b_count[b] = d->body_first[b + 1] - d->body_first[b];
+    }
+    if (nbr) {
+        std::memcpy(k_xyz.data(), d->body_brick_xyz, (size_t)nbr * 12);
+        std::memcpy(k_mat.data(), d->body_brick_mat, nbr);
+    }
+    DBuf<float> d_pose;
+    SF_CUDA(d_pose.alloc(std::max<size_t>((size_t)d->n_bodies * 13, 1)));
+    SF_CUDA(cudaMemcpyAsync(w->ctab.p + (size_t)slot * NCT, ctab.data(), ctab.size() * 4, cudaMemcpyHostToDevice, st));
+    if (!cpool.empty()) SF_CUDA(cudaMemcpyAsync(w->cpool.p + (size_t)sc.chunk_off * 512, cpool.data(), cpool.size() * 4, cudaMemcpyHostToDevice, st));
+    SF_CUDA(cudaMemcpyAsync(w->sbox.p + 2 * slot, &w->h_sbox[2 * slot], 2 * sizeof(int4), cudaMemcpyHostToDevice, st));
+    if (sc.n_static) {
+        SF_CUDA(cudaMemcpyAsync(w->s_cell.p + sc.static_off, s_cell.data(), s_cell.size() * 4, cudaMemcpyHostToDevice, st));
+        SF_CUDA(cudaMemcpyAsync(w->s_mat.p + sc.static_off, s_mat.data(), s_mat.size(), cudaMemcpyHostToDevice, st));
+        SF_CUDA(cudaMemcpyAsync(w->s_infill.p + sc.static_off, s_inf.data(), s_inf.size(), cudaMemcpyHostToDevice, st));
+    }
+    SF_CUDA(cudaMemcpyAsync(w->b_first.p + sc.body_off, b_first.data(), b_first.size() * 4, cudaMemcpyHostToDevice, st));
+    SF_CUDA(cudaMemcpyAsync(w->b_count.p + sc.body_off, b_count.data(), b_count.size() * 4, cudaMemcpyHostToDevice, st));
+    SF_CUDA(cudaMemcpyAsync(w->k_body.p + sc.brick_off, k_body.data(), k_body.size() * 4, cudaMemcpyHostToDevice, st));
+    SF_CUDA(cudaMemcpyAsync(w->k_xyz.p + (size_t)sc.brick_off * 3, k_xyz.data(), k_xyz.size() * 4, cudaMemcpyHostToDevice, st));
+    SF_CUDA(cudaMemcpyAsync(w->k_mat.p + sc.brick_off, k_mat.data(), k_mat.size(), cudaMemcpyHostToDevice, st));
+    if (d->n_bodies) SF_CUDA(cudaMemcpyAsync(d_pose.p, d->body_pose, (size_t)d->n_bodies * 52, cudaMemcpyHostToDevice, st));
+    SF_CUDA(cudaMemsetAsync(w->b_alive.p + sc.body_off, 0, sc.n_bodies, st));
+    SF_CUDA(cudaMemsetAsync(w->b_asleep.p + sc.body_off, 0, sc.n_bodies, st));
+    SF_CUDA(cudaMemsetAsync(w->b_wake.p + sc.body_off, 0, sc.n_bodies, st));
+    if (d->n_static)
+        k_finalize_bricks<<<grid_for(d->n_static, 256), 256, 0, st>>>(d->n_static, sc.static_off, w->s_cell.p,
+                                                                      w->s_scene.p, w->s_mat.p, w->s_infill.p,
+                                                                      w->s_sid.p, w->ctab.p, w->cpool.p, w->s_nb6.p,
+                                                                      w->s_bond.p, w->s_bmax.p);
+    if (d->n_bodies)
+        k_setup_bodies<<<grid_for(d->n_bodies, 128), 128, 0, st>>>(d->n_bodies, sc.body_off, w->b_first.p, w->b_count.p,
+                                                                 w->k_xyz.p, w->k_mat.p, d_pose.p, w->k_local.p,
+                                                                 w->k_wpos.p, w->k_body.p, w->b_pos.p, w->b_q.p, w->b_v.p,
+                                                                 w->b_w.p, w->b_rot.p, w->b_iil.p, w->b_iiw.p, w->b_m.p,
+                                                                 w->b_im.p, w->b_rad.p, w->b_sleep.p, w->b_maxr.p,
+                                                                 w->b_alive.p, w->b_asleep.p, w->b_wake.p);
+    w->launches += 2;
+    SF_CUDA(cudaGetLastError());
+    SF_CUDA(step_reset_labels(w, sc.body_off, sc.n_bodies));
+    SF_CUDA(cudaStreamSynchronize(st));   // host vectors and the pose buffer are the copies' sources
+    PoolSlot &ps = w->pool[slot];
+    ps.bodies = d->n_bodies; ps.bricks = nbr; ps.statics = d->n_static; ps.chunks = used; ps.loaded = true;
+    step_set_live(w, slot, d->n_bodies > 0);
+    return SF_OK;
+}
+
+sf_status sf_pool_clear(sf_world *w, uint32_t slot) {
+    if (!w || w->pool.empty() || slot >= w->pool.size()) { set_error("not a pool slot"); return SF_ERR_ARG; }
+    const Scene &sc = w->scenes[slot];
+    cudaStream_t st = w->stream;
+    SF_CUDA(cudaMemsetAsync(w->b_alive.p + sc.body_off, 0, sc.n_bodies, st));
+    SF_CUDA(cudaMemsetAsync(w->k_mat.p + sc.brick_off, 0, sc.n_bricks, st));
+    SF_CUDA(cudaMemsetAsync(w->ctab.p + (size_t)slot * NCT, 0, (size_t)NCT * 4, st));
+    if (sc.n_static) SF_CUDA(cudaMemsetAsync(w->s_mat.p + sc.static_off, 0, sc.n_static, st));
+    SF_CUDA(step_reset_labels(w, sc.body_off, sc.n_bodies));
+    SF_CUDA(cudaStreamSynchronize(st));
+    w->pool[slot] = PoolSlot{};
+    step_set_live(w, slot, false);
+    return SF_OK;
+}
+
+sf_status sf_pool_save(sf_world *w, uint32_t slot, void *host, uint64_t cap, uint64_t *bytes) {
+    if (!w || w->pool.empty() || slot >= w->pool.size() || !w->pool[slot].loaded) { set_error("no scene in that slot"); return SF_ERR_ARG; }
+    const PoolSlot &ps = w->pool[slot];
+    const uint64_t need = snapshot_bytes(ps.bodies, ps.bricks);
+    if (bytes) *bytes = need;
+    if (!host) return SF_OK;
+    if (cap < need) { set_error("snapshot needs %llu bytes, buffer holds %llu", (unsigned long long)need, (unsigned long long)cap); return SF_ERR_CAPACITY; }
+    SnapPart parts[11];
+    snapshot_parts(w, w->scenes[slot], parts);
+    uint8_t *o = (uint8_t *)host;
+    for (int k = 0; k < 11; k++) {
+        const size_t n = (k < 9 ? ps.bodies : ps.bricks) * parts[k].elem;
+        if (n) SF_CUDA(cudaMemcpyAsync(o, parts[k].dev, n, cudaMemcpyDeviceToHost, w->stream));
+        o += n;
+    }
+    SF_CUDA(cudaStreamSynchronize(w->stream));
+    return SF_OK;
+}
+
+sf_status sf_pool_restore(sf_world *w, uint32_t slot, const sf_scene_desc *d, const void *host, uint64_t bytes) {
+    if (!w || !host) { set_error("null argument"); return SF_ERR_ARG; }
+    const uint32_t nbr = d && d->n_bodies ? d->body_first[d->n_bodies] : 0;
+    if (!d || bytes != snapshot_bytes(d->n_bodies, nbr)) { set_error("snapshot size does not match the scene"); return SF_ERR_ARG; }
+    sf_status r = sf_pool_load(w, slot, d);   // the scene's fixed parts (mass, inertia, offsets, static grid)
+    if (r != SF_OK) return r;
+    SnapPart parts[11];
+    snapshot_parts(w, w->scenes[slot], parts);
+    const uint8_t *o = (const uint8_t *)host;
+    for (int k = 0; k < 11; k++) {
+        const size_t n = (k < 9 ? d->n_bodies : nbr) * parts[k].elem;
+        if (n) SF_CUDA(cudaMemcpyAsync(parts[k].dev, o, n, cudaMemcpyHostToDevice, w->stream));
+        o += n;
+    }
+    SF_CUDA(cudaStreamSynchronize(w->stream));
+    step_set_live(w, slot, true);
+    return SF_OK;
+}
+
+sf_status sf_pool_read_bodies(sf_world *w, uint32_t slot, float *state13, float *sleep, uint8_t *flags) {
+    if (!w || w->pool.empty() || slot >= w->pool.size()) { set_error("not a pool slot"); return SF_ERR_ARG; }
+    const PoolSlot &ps = w->pool[slot];
+    const Scene &sc = w->scenes[slot];
+    const uint32_t nb = ps.bodies;
+    if (nb == 0) return SF_OK;
+    cudaStream_t s = w->stream;
+    SF_CUDA(w->stage13.grow((size_t)nb * 13));
+    SF_CUDA(w->stage_flags.grow(nb));
+    const uint32_t b = sc.body_off;
+    k_pack_bodies<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_pos.p + b, w->b_q.p + b, w->b_v.p + b, w->b_w.p + b,
+                                                    w->b_alive.p + b, w->b_asleep.p + b, w->stage13.p, w->stage_flags.p);
+    w->launches++;
+    if (state13) SF_CUDA(cudaMemcpyAsync(state13, w->stage13.p, (size_t)nb * 52, cudaMemcpyDeviceToHost, s));
+    if (sleep) SF_CUDA(cudaMemcpyAsync(sleep, w->b_sleep.p + b, (size_t)nb * 4, cudaMemcpyDeviceToHost, s));
+    if (flags) SF_CUDA(cudaMemcpyAsync(flags, w->stage_flags.p, nb, cudaMemcpyDeviceToHost, s));
     SF_CUDA(cudaStreamSynchronize(s));
     return SF_OK;
 }
