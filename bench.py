@@ -376,6 +376,7 @@ def our_arm(args, rank, world, local, pg):
     ms = e0.elapsed_time(e1)
     clocks = clk.summary()
     prof = w.profile()
+    tuning = w.tuning()
     stats = w.stats()
     ms_max = allreduce_max(pg, ms)
     alive_total = allreduce_sum(pg, alive_sum)
@@ -520,6 +521,8 @@ def our_arm(args, rank, world, local, pg):
         "roofline": roofline,
         "phases_ms": {k: round(v, 3) for k, v in phase_ms.items()},
         "top_phase": top,
+        "autotune": {"blocks_per_sm_by_log2_size": tuning, "note": "launch shapes picked online per size bucket; "
+                     "they do not change results"},
         "last_step": {"contacts": int(stats.contacts), "manifolds": int(stats.manifolds), "colors": int(stats.colors),
                       "color_rounds": int(stats.color_rounds), "islands": int(stats.islands), "alive": int(stats.alive),
                       "awake": int(stats.awake)},

@@ -75,8 +75,9 @@ typedef struct sf_params {
     uint32_t contact_capacity;  /* 0 = automatic (grows between steps) */
     uint32_t verify;            /* 1: check the colouring is proper every substep (SF_ERR_VERIFY on failure) */
     uint32_t solve_blocks;      /* persistent-kernel blocks per SM for the solve (0 = autotuned) */
-    uint32_t manifold_chunk;    /* a body pair's contacts are solved in chunks of at most this many (0 = whole pair);
-                                   chunks of one pair take different colours, bounding each colour's longest chain */
+    uint32_t manifold_chunk;    /* a body pair's contacts are solved in chunks of at most this many, 1..32 (0 or more
+                                   than 32 mean 32); chunks of one pair take different colours, bounding each
+                                   colour's longest chain and the contact layout's depth */
     uint32_t reserved[7];
 } sf_params;
 
@@ -95,7 +96,7 @@ typedef struct sf_stats {
 } sf_stats;
 
 /* Per-phase device time of the rigid step, from CUDA events around each phase of each substep (profiling on). */
-#define SF_PHASES 9             /* pose, hash, contacts, manifolds, prep, colour, solve, islands, integrate */
+#define SF_PHASES 9             /* pose, hash, contacts, manifolds, colour, prep, solve, islands, integrate */
 typedef struct sf_profile {
     double ms[SF_PHASES];
     uint64_t substeps;
@@ -136,6 +137,14 @@ sf_status sf_world_set_stream(sf_world *w, void *stream);
 sf_status sf_set_profiling(sf_world *w, int32_t on);
 sf_status sf_read_profile(sf_world *w, sf_profile *out);
 sf_status sf_reset_profile(sf_world *w);
+/* The launch-shape autotuner: persistent kernels' blocks per SM, chosen per size bucket (bucket b holds launches of
+ * 2^b .. 2^(b+1) - 1 work items: contacts for the solve and the colouring, chunks for the load solve) by timing each
+ * candidate on the bucket's first launches. These shapes never change results. Writes the chosen value per bucket
+ * (-1 = not settled yet) for the first n buckets. */
+#define SF_TUNE_SOLVE 0
+#define SF_TUNE_COLOR 1
+#define SF_TUNE_SOR 2
+sf_status sf_read_tuning(sf_world *w, uint32_t which, int32_t *blocks_per_sm, uint32_t n);
 
 /* ---- hot path */
 /* nsteps world steps of dt each (dt clamped to [0, 1/30] as src/lib.rs:3642 does), all scenes at once. Scenes

@@ -65,7 +65,7 @@ class Stats(C.Structure):
 
 
 SF_PHASES = 9
-PHASE_NAMES = ["pose", "hash", "contacts", "manifolds", "prep", "colour", "solve", "islands", "integrate"]
+PHASE_NAMES = ["pose", "hash", "contacts", "manifolds", "colour", "prep", "solve", "islands", "integrate"]
 
 
 class Profile(C.Structure):
@@ -135,6 +135,7 @@ PROTOTYPES = {
     "sf_set_profiling": (C.c_int32, [C.c_void_p, C.c_int32]),
     "sf_read_profile": (C.c_int32, [C.c_void_p, C.POINTER(Profile)]),
     "sf_reset_profile": (C.c_int32, [C.c_void_p]),
+    "sf_read_tuning": (C.c_int32, [C.c_void_p, C.c_uint32, _i32p, C.c_uint32]),
     "sf_structure_solve": (C.c_int32, [C.c_void_p, C.c_int32, C.c_float, C.c_float, C.c_uint32, C.POINTER(SolveReport)]),
     "sf_structure_check": (C.c_int32, [C.c_void_p, C.c_int32, C.c_float, C.c_int32, C.POINTER(CheckReport)]),
     "sf_read_solve_detail": (C.c_int32, [C.c_void_p, _u32p, C.POINTER(C.c_double)]),
@@ -341,6 +342,15 @@ class World:
         _check(self._lib.sf_read_profile(self._h, C.byref(p)), "sf_read_profile")
         return {"ms": dict(zip(PHASE_NAMES, list(p.ms))), "substeps": p.substeps, "solve_launches": p.solve_launches,
                 "solve_contact_iters": p.solve_contact_iters, "contacts_sum": p.contacts_sum, "launches": p.launches}
+
+    def tuning(self) -> dict:
+        """Blocks per SM the autotuner settled on, per size bucket (log2 of work items), for each tuned kernel."""
+        out = {}
+        for name, which in (("solve", 0), ("colour", 1), ("sor", 2)):
+            a = np.full(40, -1, np.int32)
+            _check(self._lib.sf_read_tuning(self._h, which, _ptr(a, C.c_int32), 40), "sf_read_tuning")
+            out[name] = {int(b): int(v) for b, v in enumerate(a) if v >= 0}
+        return out
 
     def reset_profile(self):
         _check(self._lib.sf_reset_profile(self._h), "sf_reset_profile")

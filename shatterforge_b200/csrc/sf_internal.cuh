@@ -121,12 +121,45 @@ struct DBuf {
     size_t bytes() const { return n * sizeof(T); }
 };
 
+// Online autotuner for launch shapes that do not change results (blocks per SM of the persistent kernels: the
+// order of work inside a colour or a red-black half-sweep does not change any value). Keyed on a size bucket
+// (log2 of the launch's work items); the first launches of a bucket try each candidate twice, timed with CUDA
+// events, and the bucket then keeps the fastest.
+struct Tuner {
+    static constexpr int NB = 40, NC = 4, TRIES = 2;
+    int cand[NC] = {1, 2, 3, 4};
+    int ncand = 0;
+    struct Entry { int best = -1; float sum[NC] = {}; int n[NC] = {}; } e[NB];
+    void init(const int *c, int n) { ncand = 0; for (int k = 0; k < n && ncand < NC; k++) if (c[k] > 0) cand[ncand++] = c[k]; }
+    static int bucket(uint64_t work) { int b = 0; while (b < NB - 1 && (work >> (b + 1))) b++; return b; }
+    // the value to launch with, and the candidate index to record (-1 once the bucket is settled)
+    int choose(int b, int &ci) const {
+        const Entry &x = e[b];
+        ci = -1;
+        if (x.best >= 0 || ncand == 0) return ncand ? cand[x.best] : 1;
+        for (int k = 0; k < ncand; k++) if (x.n[k] < TRIES) { ci = k; return cand[k]; }
+        return cand[0];
+    }
+    void record(int b, int ci, float ms) {
+        Entry &x = e[b];
+        if (ci < 0 || x.best >= 0) return;
+        x.sum[ci] += ms;
+        x.n[ci]++;
+        for (int k = 0; k < ncand; k++) if (x.n[k] < TRIES) return;
+        int best = 0;
+        for (int k = 1; k < ncand; k++) if (x.sum[k] < x.sum[best]) best = k;
+        x.best = best;
+    }
+    int settled(int b) const { return e[b].best >= 0 ? cand[e[b].best] : -1; }
+};
+
 // persistent-kernel grid barrier state (bounded spin, see grid_sync)
 struct GridBarrier { unsigned count; unsigned gen; };
 
 struct StepState;    // sf_step.cu
 struct SorState;     // sf_sor.cu
 uint64_t sor_launches(const SorState *st);
+const Tuner *sor_tuner(const SorState *st);
 void sor_reset_launches(SorState *st);
 
 // Device buffers of one structure's load-path solve when the caller supplies every buffer (no allocation inside).

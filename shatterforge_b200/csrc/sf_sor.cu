@@ -54,7 +54,10 @@ struct SorState {
     Work wk;
     uint64_t launches = 0;
     int occ = 1;
+    Tuner tune;   // blocks per SM of the red-black kernel, keyed on log2(chunks of the solve)
 };
+
+const Tuner *sor_tuner(const SorState *st) { return st ? &st->tune : nullptr; }
 
 enum : uint8_t { J_HOLD = 0, J_FATIGUE = 1, J_FAIL = 2, J_CRUSH = 3, J_ABSENT = 255 };
 
@@ -606,6 +609,12 @@ sf_status sor_create(sf_world *w) {
     int occ = 0;
     SF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sor_redblack, SOR_BLOCK, 0));
     st->occ = std::max(1, occ);
+    {
+        int c[4], n = 0;
+        for (int v : {1, 2, 4, 8}) if (v <= st->occ) c[n++] = v;
+        if (n == 0 || c[n - 1] != st->occ) { if (n == 4) n = 3; c[n++] = st->occ; }
+        st->tune.init(c, n);
+    }
     if (nst > (uint32_t)SOR_MAX_LOCAL_STRUCT) { set_error("more than %d structures", SOR_MAX_LOCAL_STRUCT); return SF_ERR_CAPACITY; }
     return SF_OK;
 }
@@ -719,7 +728,10 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     A.chunk_sid = st->chunk_sid.p; A.work = st->work.p; A.n_work = (uint32_t)chunks.size(); A.n_struct = nst;
     A.active0 = st->active0.p; A.resid_buf = st->resid_buf.p; A.sweeps = st->sweeps.p; A.resid = st->resid.p;
     A.omega = (double)omega; A.tol = (double)tol; A.max_sweeps = max_sweeps; A.gb = w->barrier.p; A.err = w->err.p;
-    unsigned grid = (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * st->occ);
+    int tci = -1;
+    const int tb = Tuner::bucket(chunks.size());
+    const unsigned per_sm = (unsigned)st->tune.choose(tb, tci);
+    unsigned grid = (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * per_sm);
     void *args[] = {&A};
     SF_CUDA(cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s));
     k_sor_gather<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p,
@@ -740,6 +752,8 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
         rep.brick_sweeps += (uint64_t)sw[q] * st->h_st_count[q];
         rep.max_residual = std::max(rep.max_residual, (double)rs[q]);
     }
+    // per sweep, since solves of one bucket converge in different sweep counts
+    if (e == SF_OK) st->tune.record(tb, tci, ms / (float)std::max<uint32_t>(rep.max_sweeps_done, 1));
     if (report) *report = rep;
     if (e == SF_OK && (w->stats.error_word & ERR_SOR_NONFINITE)) { set_error("non-finite potential (ungrounded piece?)"); return SF_ERR_VERIFY; }
     return e;

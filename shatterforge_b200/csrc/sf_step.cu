@@ -37,6 +37,7 @@ struct StepState {
     DBuf<uint32_t> cval, cval_alt;
     DBuf<uint32_t> aw_flag, awk_pos, awk_list, inc_flag, inc_pos, bucket_bits, scene_awake, scene_bricks;
     uint32_t n_awk = 0, n_inc = 0;
+    bool use_sparse = false, last_sparse = false;
     DBuf<uint2> brange;
     DBuf<float4> srec;
     DBuf<uint32_t> sinfo;
@@ -56,7 +57,7 @@ struct StepState {
     DBuf<uint32_t> bm_count, bm_start, bm_fill, bm_list;
     DBuf<uint32_t> masks, vmasks;
     DBuf<uint32_t> wl0, wl1;
-    DBuf<uint32_t> col_count, col_start, col_fill, col_list;
+    DBuf<uint32_t> col_count, col_hstart, col_start, col_fill, col_list, jds_off;
     // islands
     DBuf<uint32_t> parent, label, mint;
     // per-scene body offsets (for scene-local priorities)
@@ -78,6 +79,12 @@ struct StepState {
     uint64_t capacity = 0;
     uint64_t last_contacts = 0;
     int solve_occ = 1, jp_occ = 1;
+    // launch-shape tuning: pending timings of this step's tuned launches
+    Tuner solve_t, jp_t;
+    struct Pending { Tuner *t; int bucket, ci; cudaEvent_t e0, e1; };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> tev;
+    size_t tev_used = 0;
     bool have_contacts = false;
     // profiling: PH_N + 1 events per substep, elapsed times folded in after each sf_world_step
     bool profile = false;
@@ -101,6 +108,7 @@ static void prof_mark(sf_world *w) {
 
 enum { DV_CONTACTS = 0, DV_MANIFOLDS = 1, DV_COLORS = 2, DV_ROUNDS = 3, DV_WL0 = 4, DV_WL1 = 5, DV_WL2 = 6,
        DV_ALIVE = 7, DV_AWAKE = 8, DV_ISLANDS = 9, DV_PAIRS = 10, DV_AWK = 11, DV_INC = 12, DV_N = 16 };
+constexpr int JDS_K = 32;   // the largest manifold chunk: the depth of the solve's contact layout
 
 // ---------------------------------------------------------------- pose cache
 // Kernels over bodies or bricks take the substep's active list (global ids of the bodies / bricks of the scenes
@@ -192,15 +200,26 @@ __global__ void k_mark_buckets(const uint32_t *n_p, const uint32_t *awk, const u
                 if (!(__ldcg(&sb[h >> 5]) & m)) atomicOr(&sb[h >> 5], m);
             }
 }
-// key = (the scene's index in the active set, hashed cell), flagged when the brick goes into the hash
-__global__ void k_cell_keys(uint32_t nd, const uint32_t *list, const uint32_t *kbody, const uint32_t *bscene,
-                            const uint32_t *scene_act, const uint32_t *scene_awake, const uint32_t *scene_bricks,
-                            const uint8_t *alive, const uint8_t *asleep, const float4 *wpos, const uint32_t *bits,
-                            uint64_t *key, uint32_t *val, uint32_t *inc) {
+// key = (the scene's index in the active set, hashed cell), flagged when the brick goes into the hash. Dense form
+// (inc == null, most bricks awake): every live brick goes in, dead ones get none_key and sort last.
+__global__ void k_cell_keys(uint32_t nd, const uint32_t *list, uint64_t none_key, const uint32_t *kbody,
+                            const uint32_t *bscene, const uint32_t *scene_act, const uint32_t *scene_awake,
+                            const uint32_t *scene_bricks, const uint8_t *alive, const uint8_t *asleep, const float4 *wpos,
+                            const uint32_t *bits, uint64_t *key, uint32_t *val, uint32_t *inc) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nd) return;
     const uint32_t i = pick(list, t);
     const uint32_t b = kbody[i];
+    if (!inc) {
+        uint64_t k = none_key;
+        if (alive[b]) {
+            const float4 p = wpos[i];
+            k = (uint64_t)scene_act[bscene[b]] * HSIZE + hkey(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z));
+        }
+        key[t] = k;
+        val[t] = i;
+        return;
+    }
     uint32_t in = 0;
     if (alive[b]) {
         const float4 p = wpos[i];
@@ -496,15 +515,26 @@ struct PrepArgs {
     uint32_t nc;
     float h;
     const uint32_t *perm, *L_a, *L_b;
+    const uint32_t *man_start, *col_start, *col_list, *jds_off;
     const float4 *L_p, *L_n, *pos, *v, *w;
     const float *im, *iiw;
     float4 *S_n, *S_t1, *S_t2, *S_ra, *S_rb, *S_j;
     uint32_t *invperm;
 };
 
+// One thread per slot d of the solve's contact layout (so the writes are coalesced): the slot's colour and depth come
+// from the layout table, its manifold from the colour list, its contact from the manifold's first contact.
 __global__ void k_prep(PrepArgs A) {
-    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= A.nc) return;
+    const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= A.nc) return;
+    uint32_t lo = 0, hi = MAXCOL * JDS_K;   // last table entry <= d
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (A.jds_off[mid] <= d) lo = mid; else hi = mid;
+    }
+    const uint32_t c = lo / JDS_K, kk = lo % JDS_K;
+    const uint32_t m = A.col_list[A.col_start[c] + (d - A.jds_off[lo])];
+    const uint32_t t = A.man_start[m] + kk;
     uint32_t k = A.perm[t];
     uint32_t a = A.L_a[k], b = A.L_b[k];
     bool hasb = b != STATIC;
@@ -550,13 +580,13 @@ __global__ void k_prep(PrepArgs A) {
     float mt2 = eff_mass(ima, iia, hasb, imb, iib, ra, rb, t2);
     float bias = minf(div_rn(0.2f, A.h) * maxf(depth - 0.01f, 0.0f), 1.0f);
     if (vn < -2.0f) bias = maxf(bias, -0.12f * vn);
-    A.S_n[t] = make_float4(n.x, n.y, n.z, mn);
-    A.S_t1[t] = make_float4(t1.x, t1.y, t1.z, mt1);
-    A.S_t2[t] = make_float4(t2.x, t2.y, t2.z, mt2);
-    A.S_ra[t] = make_float4(ra.x, ra.y, ra.z, bias);
-    A.S_rb[t] = make_float4(rb.x, rb.y, rb.z, vn0);
-    A.S_j[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    A.invperm[k] = t;
+    A.S_n[d] = make_float4(n.x, n.y, n.z, mn);
+    A.S_t1[d] = make_float4(t1.x, t1.y, t1.z, mt1);
+    A.S_t2[d] = make_float4(t2.x, t2.y, t2.z, mt2);
+    A.S_ra[d] = make_float4(ra.x, ra.y, ra.z, bias);
+    A.S_rb[d] = make_float4(rb.x, rb.y, rb.z, vn0);
+    A.S_j[d] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    A.invperm[k] = d;
 }
 
 // ---------------------------------------------------------------- colouring
@@ -640,20 +670,45 @@ __global__ void __launch_bounds__(256) k_jp(JpArgs A) {
     }
 }
 
-__global__ void k_col_count(const uint32_t *nm_p, const uint32_t *man_color, uint32_t *col_count, uint32_t *dev) {
+// manifolds counted by (colour, contact count), count descending: bucket c * (JDS_K + 1) + (JDS_K - count)
+constexpr int JDS_ROW = JDS_K + 1;
+__global__ void k_col_count(const uint32_t *nm_p, const uint32_t *man_color, const uint32_t *man_count, uint32_t *hist,
+                            uint32_t *dev) {
     uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= *nm_p) return;
     uint32_t c = man_color[m];
-    atomicAdd(&col_count[c], 1u);
+    atomicAdd(&hist[c * JDS_ROW + (JDS_K - man_count[m])], 1u);
     atomicMax(&dev[DV_COLORS], c + 1);
 }
-__global__ void k_col_fill(const uint32_t *nm_p, const uint32_t *man_color, const uint32_t *col_start, uint32_t *col_fill,
-                           uint32_t *col_list) {
+__global__ void k_col_fill(const uint32_t *nm_p, const uint32_t *man_color, const uint32_t *man_count,
+                           const uint32_t *hstart, uint32_t *hfill, uint32_t *col_list) {
     uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= *nm_p) return;
-    uint32_t c = man_color[m];
-    col_list[col_start[c] + atomicAdd(&col_fill[c], 1u)] = m;
+    const uint32_t bkt = man_color[m] * JDS_ROW + (JDS_K - man_count[m]);
+    col_list[hstart[bkt] + atomicAdd(&hfill[bkt], 1u)] = m;
 }
+// one thread per colour: colour starts in col_list and the JDS offsets (contacts of colour c before c come first)
+__global__ void __launch_bounds__(MAXCOL) k_jds_table(const uint32_t *hist, const uint32_t *hstart, const uint32_t *nm_p,
+                                                      uint32_t *col_start, uint32_t *jds_off) {
+    __shared__ uint32_t tot[MAXCOL];
+    const uint32_t c = threadIdx.x;
+    uint32_t n[JDS_K];
+    uint32_t run = 0, total = 0;
+    // n[k] = manifolds of colour c with more than k contacts = those in buckets j <= JDS_K - 1 - k
+#pragma unroll
+    for (int j = 0; j < JDS_K; j++) { run += hist[c * JDS_ROW + j]; n[JDS_K - 1 - j] = run; }
+#pragma unroll
+    for (int k = 0; k < JDS_K; k++) total += n[k];
+    tot[c] = total;
+    __syncthreads();
+    uint32_t base = 0;
+    for (uint32_t q = 0; q < c; q++) base += tot[q];
+    col_start[c] = hstart[c * JDS_ROW];
+    if (c == MAXCOL - 1) col_start[MAXCOL] = *nm_p;
+#pragma unroll
+    for (int k = 0; k < JDS_K; k++) { jds_off[c * JDS_K + k] = base; base += n[k]; }
+}
+
 // proper-colouring check: no two manifolds of one colour at one awake body
 __global__ void k_col_verify(const uint32_t *nm_p, const uint32_t *man_a, const uint32_t *man_b, const uint32_t *man_color,
                              uint32_t *vmasks, uint32_t *err) {
@@ -667,11 +722,14 @@ __global__ void k_col_verify(const uint32_t *nm_p, const uint32_t *man_a, const 
 }
 
 // ---------------------------------------------------------------- the coloured sequential-impulse solve
+// Contact layout (jagged diagonal, per colour): a colour's manifolds are listed by contact count, most first, and
+// contact k of the colour's p-th manifold sits at jds_off[colour * JDS_K + k] + p. The k-th contacts of a colour's
+// manifolds are therefore contiguous, so the threads of a warp (consecutive p) read them coalesced.
 struct SolveArgs {
     uint32_t iterations;
     const uint32_t *dev;           // DV_COLORS
-    const uint32_t *col_start, *col_list;
-    const uint32_t *man_a, *man_b, *man_start, *man_count;
+    const uint32_t *col_start, *col_list, *jds_off;
+    const uint32_t *man_a, *man_b, *man_count;
     const float4 *S_n, *S_t1, *S_t2, *S_ra, *S_rb;
     float4 *S_j;
     float4 *v, *w;
@@ -688,10 +746,10 @@ template <bool ONE_BLOCK> __device__ __forceinline__ float4 ld_rw(const float4 *
 }
 
 template <bool ONE_BLOCK>
-__device__ __forceinline__ void solve_manifold(const SolveArgs &A, uint32_t m) {
+__device__ __forceinline__ void solve_manifold(const SolveArgs &A, uint32_t m, uint32_t p, const uint32_t *off) {
     const uint32_t a = A.man_a[m], b = A.man_b[m];
     const bool hasb = b != STATIC;
-    const uint32_t s0 = A.man_start[m], cnt = A.man_count[m];
+    const uint32_t cnt = A.man_count[m];
     float4 t4 = ld_rw<ONE_BLOCK>(&A.v[a]);
     V3 va = v3(t4.x, t4.y, t4.z);
     t4 = ld_rw<ONE_BLOCK>(&A.w[a]);
@@ -711,16 +769,19 @@ __device__ __forceinline__ void solve_manifold(const SolveArgs &A, uint32_t m) {
     }
     // the next contact's data is loaded while the current one is solved (the chain through the bodies is serial)
     float4 nx_n = make_float4(0, 0, 0, 0), nx_t1 = nx_n, nx_t2 = nx_n, nx_ra = nx_n, nx_rb = nx_n, nx_j = nx_n;
+    uint32_t at = off[0] + p;
     if (cnt) {
-        nx_n = __ldg(&A.S_n[s0]); nx_t1 = __ldg(&A.S_t1[s0]); nx_t2 = __ldg(&A.S_t2[s0]);
-        nx_ra = __ldg(&A.S_ra[s0]); nx_rb = __ldg(&A.S_rb[s0]); nx_j = ld_rw<ONE_BLOCK>(&A.S_j[s0]);
+        nx_n = __ldg(&A.S_n[at]); nx_t1 = __ldg(&A.S_t1[at]); nx_t2 = __ldg(&A.S_t2[at]);
+        nx_ra = __ldg(&A.S_ra[at]); nx_rb = __ldg(&A.S_rb[at]); nx_j = ld_rw<ONE_BLOCK>(&A.S_j[at]);
     }
-    for (uint32_t k = s0; k < s0 + cnt; k++) {
+    for (uint32_t k = 0; k < cnt; k++) {
         const float4 n4 = nx_n, t14 = nx_t1, t24 = nx_t2, ra4 = nx_ra, rb4 = nx_rb;
         float4 j4 = nx_j;
-        if (k + 1 < s0 + cnt) {
-            nx_n = __ldg(&A.S_n[k + 1]); nx_t1 = __ldg(&A.S_t1[k + 1]); nx_t2 = __ldg(&A.S_t2[k + 1]);
-            nx_ra = __ldg(&A.S_ra[k + 1]); nx_rb = __ldg(&A.S_rb[k + 1]); nx_j = ld_rw<ONE_BLOCK>(&A.S_j[k + 1]);
+        const uint32_t cur = at;
+        if (k + 1 < cnt) {
+            at = off[k + 1] + p;
+            nx_n = __ldg(&A.S_n[at]); nx_t1 = __ldg(&A.S_t1[at]); nx_t2 = __ldg(&A.S_t2[at]);
+            nx_ra = __ldg(&A.S_ra[at]); nx_rb = __ldg(&A.S_rb[at]); nx_j = ld_rw<ONE_BLOCK>(&A.S_j[at]);
         }
         const V3 n = v3(n4.x, n4.y, n4.z), t1 = v3(t14.x, t14.y, t14.z), t2 = v3(t24.x, t24.y, t24.z);
         const V3 ra = v3(ra4.x, ra4.y, ra4.z), rb = v3(rb4.x, rb4.y, rb4.z);
@@ -753,7 +814,7 @@ __device__ __forceinline__ void solve_manifold(const SolveArgs &A, uint32_t m) {
             wa = add(wa, mv(ia, cross(ra, P)));
             if (hasb) { vb = madd(vb, P, -imb); wb = sub(wb, mv(ib, cross(rb, P))); }
         }
-        A.S_j[k] = j4;
+        A.S_j[cur] = j4;
     }
     A.v[a] = make_float4(va.x, va.y, va.z, 0.0f);
     A.w[a] = make_float4(wa.x, wa.y, wa.z, 0.0f);
@@ -766,12 +827,15 @@ __device__ __forceinline__ void solve_manifold(const SolveArgs &A, uint32_t m) {
 constexpr int SOLVE_BLOCK = 128;
 
 __global__ void __launch_bounds__(SOLVE_BLOCK) k_solve(SolveArgs A) {
+    __shared__ uint32_t off[JDS_K];
     const uint32_t ncol = A.dev[DV_COLORS];
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t it = 0; it < A.iterations; it++) {
         for (uint32_t c = 0; c < ncol; c++) {
-            const uint32_t s0 = A.col_start[c], s1 = A.col_start[c + 1];
-            for (uint32_t t = s0 + blockIdx.x * blockDim.x + threadIdx.x; t < s1; t += stride) solve_manifold<false>(A, A.col_list[t]);
+            if (threadIdx.x < JDS_K) off[threadIdx.x] = A.jds_off[c * JDS_K + threadIdx.x];
+            __syncthreads();
+            const uint32_t s0 = A.col_start[c], n = A.col_start[c + 1] - s0;
+            for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) solve_manifold<false>(A, A.col_list[s0 + p], p, off);
             if (!grid_sync(A.gb, gridDim.x, A.err)) return;
         }
     }
@@ -781,11 +845,14 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) k_solve(SolveArgs A) {
 constexpr int SOLVE_ONE_BLOCK = 512;
 constexpr uint32_t SOLVE_ONE_BLOCK_MAX_CONTACTS = 8192;
 __global__ void __launch_bounds__(SOLVE_ONE_BLOCK) k_solve_one_block(SolveArgs A) {
+    __shared__ uint32_t off[JDS_K];
     const uint32_t ncol = A.dev[DV_COLORS];
     for (uint32_t it = 0; it < A.iterations; it++) {
         for (uint32_t c = 0; c < ncol; c++) {
-            const uint32_t s0 = A.col_start[c], s1 = A.col_start[c + 1];
-            for (uint32_t t = s0 + threadIdx.x; t < s1; t += blockDim.x) solve_manifold<true>(A, A.col_list[t]);
+            if (threadIdx.x < JDS_K) off[threadIdx.x] = A.jds_off[c * JDS_K + threadIdx.x];
+            __syncthreads();
+            const uint32_t s0 = A.col_start[c], n = A.col_start[c + 1] - s0;
+            for (uint32_t p = threadIdx.x; p < n; p += blockDim.x) solve_manifold<true>(A, A.col_list[s0 + p], p, off);
             __syncthreads();
         }
     }
@@ -1061,7 +1128,10 @@ sf_status step_create(sf_world *w) {
     SF_CUDA(S->ccount.alloc((size_t)nd + 1)); SF_CUDA(S->coff.alloc((size_t)nd + 1));
     SF_CUDA(S->bm_count.alloc((size_t)nb + 1)); SF_CUDA(S->bm_start.alloc((size_t)nb + 1)); SF_CUDA(S->bm_fill.alloc((size_t)nb + 1));
     SF_CUDA(S->masks.alloc((size_t)nb * 4 + 4)); SF_CUDA(S->vmasks.alloc((size_t)nb * 4 + 4));
-    SF_CUDA(S->col_count.alloc(MAXCOL + 2)); SF_CUDA(S->col_start.alloc(MAXCOL + 2)); SF_CUDA(S->col_fill.alloc(MAXCOL + 2));
+    SF_CUDA(S->col_count.alloc(MAXCOL * JDS_ROW + 1)); SF_CUDA(S->col_start.alloc(MAXCOL + 2));
+    SF_CUDA(S->col_fill.alloc(MAXCOL * JDS_ROW + 1)); SF_CUDA(S->jds_off.alloc(MAXCOL * JDS_K));
+    SF_CUDA(S->col_hstart.alloc(MAXCOL * JDS_ROW + 1));
+    if (w->P.manifold_chunk == 0 || w->P.manifold_chunk > (uint32_t)JDS_K) w->P.manifold_chunk = JDS_K;
     SF_CUDA(S->parent.alloc(nb)); SF_CUDA(S->label.alloc(nb)); SF_CUDA(S->mint.alloc(nb));
     SF_CUDA(cudaMemsetAsync(S->label.p, 0xFF, S->label.bytes(), s));
     SF_CUDA(S->act_body.alloc(nb)); SF_CUDA(S->cidx.alloc(nb)); SF_CUDA(S->act_brick.alloc(nd));
@@ -1083,6 +1153,14 @@ sf_status step_create(sf_world *w) {
     S->solve_occ = std::max(1, occ);
     SF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jp, 256, 0));
     S->jp_occ = std::max(1, occ);
+    {
+        int c[4], n = 0;
+        for (int v = 1; v <= 4; v++) if (v <= S->solve_occ) c[n++] = v;
+        S->solve_t.init(c, n);
+        n = 0;
+        for (int v : {1, 2, 4}) if (v <= S->jp_occ) c[n++] = v;
+        S->jp_t.init(c, n);
+    }
     SF_CUDA(cudaStreamSynchronize(s));   // the host vector `off` is the copy's source
     return SF_OK;
 }
@@ -1100,7 +1178,37 @@ cudaError_t refresh_poses(sf_world *w) {
     return cudaGetLastError();
 }
 
+static cudaEvent_t tune_event(StepState *S) {
+    if (S->tev_used == S->tev.size()) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        S->tev.push_back(e);
+    }
+    return S->tev[S->tev_used++];
+}
+// time a tuned launch: events around it, resolved after the step
+static void tune_begin(StepState *S, Tuner *t, int bucket, int ci, cudaStream_t s) {
+    if (ci < 0) return;
+    cudaEvent_t e0 = tune_event(S), e1 = tune_event(S);
+    if (!e0 || !e1) return;
+    cudaEventRecord(e0, s);
+    S->pending.push_back({t, bucket, ci, e0, e1});
+}
+static void tune_end(StepState *S, int ci, cudaStream_t s) {
+    if (ci < 0 || S->pending.empty()) return;
+    cudaEventRecord(S->pending.back().e1, s);
+}
+static void tune_resolve(StepState *S) {
+    for (const StepState::Pending &p : S->pending) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, p.e0, p.e1) == cudaSuccess) p.t->record(p.bucket, p.ci, ms);
+    }
+    S->pending.clear();
+    S->tev_used = 0;
+}
+
 void step_destroy(sf_world *w) {
+    if (w->step) for (cudaEvent_t e : w->step->tev) cudaEventDestroy(e);
     if (w->step && w->step->h_dev) cudaFreeHost(w->step->h_dev);
     if (w->step && w->step->h_live_pin) cudaFreeHost(w->step->h_live_pin);
     delete w->step;
@@ -1193,7 +1301,19 @@ static sf_status substep(sf_world *w, float h) {
                                                   w->b_rot.p, w->k_local.p, w->k_wpos.p);
     L += 2;
     prof_mark(w);
-    // awake bricks (in active-list order) and the hashed cells they can reach
+    // Sparse form (most bricks asleep): the awake bricks, in active-list order, and the hashed cells they can reach.
+    // Dense form: every live brick hashed, every active brick a contact thread. Both give the same contacts.
+    const bool sparse = S->use_sparse;
+    S->last_sparse = sparse;
+    uint32_t n_awk = nd, n_inc = nd;
+    const uint32_t *clist = klist;
+    if (!sparse) {
+        k_cell_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, none_key, w->k_body.p, w->b_scene.p, S->scene_act.p,
+                                                      nullptr, nullptr, w->b_alive.p, w->b_asleep.p, w->k_wpos.p, nullptr,
+                                                      S->ckey.p, S->cval.p, nullptr);
+        L++;
+    } else {
+    clist = S->awk_list.p;
     SF_CUDA(cudaMemsetAsync(S->scene_awake.p, 0, S->act.size() * 4, s));
     k_awake_flags<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, w->k_body.p, w->b_scene.p, S->scene_act.p, w->b_alive.p,
                                                     w->b_asleep.p, S->aw_flag.p, S->scene_awake.p);
@@ -1203,16 +1323,19 @@ static sf_status substep(sf_world *w, float h) {
     k_mark_buckets<<<grid_for(nd, 128), 128, 0, s>>>(S->dev.p + DV_AWK, S->awk_list.p, w->k_body.p, w->b_scene.p,
                                                      S->scene_act.p, S->scene_awake.p, S->scene_bricks.p, w->k_wpos.p,
                                                      S->bucket_bits.p);
-    k_cell_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, w->k_body.p, w->b_scene.p, S->scene_act.p, S->scene_awake.p,
-                                                  S->scene_bricks.p, w->b_alive.p, w->b_asleep.p, w->k_wpos.p,
-                                                  S->bucket_bits.p, S->ckey_alt.p, S->cval_alt.p, S->inc_flag.p);
+    k_cell_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, none_key, w->k_body.p, w->b_scene.p, S->scene_act.p,
+                                                  S->scene_awake.p, S->scene_bricks.p, w->b_alive.p, w->b_asleep.p,
+                                                  w->k_wpos.p, S->bucket_bits.p, S->ckey_alt.p, S->cval_alt.p,
+                                                  S->inc_flag.p);
     SF_CUDA(exclusive_scan_u32(S->inc_flag.p, S->inc_pos.p, nd, S->dev.p + DV_INC, S->wk, s));
     k_compact_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, S->inc_flag.p, S->inc_pos.p, S->ckey_alt.p, S->cval_alt.p,
                                                      S->ckey.p, S->cval.p);
     L += 5;
     SF_CUDA(cudaMemcpyAsync(S->h_dev + DV_AWK, S->dev.p + DV_AWK, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     SF_CUDA(cudaStreamSynchronize(s));
-    const uint32_t n_awk = S->h_dev[DV_AWK], n_inc = S->h_dev[DV_INC];
+    n_awk = S->h_dev[DV_AWK];
+    n_inc = S->h_dev[DV_INC];
+    }
     S->n_awk = n_awk;
     S->n_inc = n_inc;
     SF_CUDA(radix_sort_u64(S->ckey.p, S->cval.p, S->ckey_alt.p, S->cval_alt.p, n_inc, bits_for(none_key), S->wk, s));
@@ -1226,7 +1349,7 @@ static sf_status substep(sf_world *w, float h) {
     prof_mark(w);
     // contacts: generate into slots and count, scan, place in list order
     ContactArgs C;
-    C.nd = n_awk; C.list = S->awk_list.p; C.scene_act = S->scene_act.p;
+    C.nd = n_awk; C.list = clist; C.scene_act = S->scene_act.p;
     C.sbox = w->sbox.p; C.kbody = w->k_body.p; C.bscene = w->b_scene.p; C.ctab = w->ctab.p; C.cpool = w->cpool.p;
     C.alive = w->b_alive.p; C.asleep = w->b_asleep.p; C.smat = w->s_mat.p; C.wpos = w->k_wpos.p;
     C.v = w->b_v.p; C.w = w->b_w.p; C.rot = w->b_rot.p; C.rad = w->b_rad.p; C.brange = S->brange.p; C.srec = S->srec.p;
@@ -1268,14 +1391,6 @@ static sf_status substep(sf_world *w, float h) {
         k_man_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, nc, S->man_start.p, S->man_count.p);
         L += 6;
         prof_mark(w);
-        PrepArgs PA;
-        PA.nc = nc; PA.h = h; PA.perm = S->perm.p; PA.L_a = S->L_a.p; PA.L_b = S->L_b.p; PA.L_p = S->L_p.p; PA.L_n = S->L_n.p;
-        PA.pos = w->b_pos.p; PA.v = w->b_v.p; PA.w = w->b_w.p; PA.im = w->b_im.p; PA.iiw = w->b_iiw.p;
-        PA.S_n = S->S_n.p; PA.S_t1 = S->S_t1.p; PA.S_t2 = S->S_t2.p; PA.S_ra = S->S_ra.p; PA.S_rb = S->S_rb.p; PA.S_j = S->S_j.p;
-        PA.invperm = S->invperm.p;
-        k_prep<<<g_nc, 256, 0, s>>>(PA);
-        L++;
-        prof_mark(w);
         // colouring, on the active list's body ids
         SF_CUDA(cudaMemsetAsync(S->bm_count.p, 0, ((size_t)nb + 1) * 4, s));
         SF_CUDA(cudaMemsetAsync(S->bm_fill.p, 0, ((size_t)nb + 1) * 4, s));
@@ -1290,20 +1405,38 @@ static sf_status substep(sf_world *w, float h) {
         J.bm_start = S->bm_start.p; J.bm_list = S->bm_list.p; J.man_round = S->man_round.p; J.man_color = S->man_color.p;
         J.masks = S->masks.p; J.wl0 = S->wl0.p; J.wl1 = S->wl1.p; J.dev = S->dev.p; J.max_colors = w->P.max_colors;
         J.max_rounds = 1u << 16; J.gb = w->barrier.p; J.err = w->err.p;
-        unsigned jgrid = (unsigned)std::min<uint64_t>((uint64_t)w->sms * std::min(S->jp_occ, 2), (nc + 255) / 256 + 1);
+        int jci = -1;
+        const int jb = Tuner::bucket(nc);
+        const unsigned jper = (unsigned)S->jp_t.choose(jb, jci);
+        unsigned jgrid = (unsigned)std::min<uint64_t>((uint64_t)w->sms * jper, (nc + 255) / 256 + 1);
         void *jargs[] = {&J};
+        tune_begin(S, &S->jp_t, jb, jci, s);
         SF_CUDA(cudaLaunchCooperativeKernel((void *)k_jp, dim3(jgrid), dim3(256), jargs, 0, s));
+        tune_end(S, jci, s);
+        // colour lists with each colour's manifolds by contact count (most first), and the contact layout
         SF_CUDA(cudaMemsetAsync(S->col_count.p, 0, S->col_count.bytes(), s));
         SF_CUDA(cudaMemsetAsync(S->col_fill.p, 0, S->col_fill.bytes(), s));
-        k_col_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_color.p, S->col_count.p, S->dev.p);
-        SF_CUDA(exclusive_scan_u32(S->col_count.p, S->col_start.p, MAXCOL + 1, nullptr, S->wk, s));
-        k_col_fill<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_color.p, S->col_start.p, S->col_fill.p, S->col_list.p);
-        L += 6;
+        k_col_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_color.p, S->man_count.p, S->col_count.p, S->dev.p);
+        SF_CUDA(exclusive_scan_u32(S->col_count.p, S->col_hstart.p, MAXCOL * JDS_ROW, nullptr, S->wk, s));
+        k_col_fill<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_color.p, S->man_count.p, S->col_hstart.p,
+                                        S->col_fill.p, S->col_list.p);
+        k_jds_table<<<1, MAXCOL, 0, s>>>(S->col_count.p, S->col_hstart.p, S->dev.p + DV_MANIFOLDS, S->col_start.p, S->jds_off.p);
+        L += 7;
         if (w->P.verify) {
             SF_CUDA(cudaMemsetAsync(S->vmasks.p, 0, (size_t)nb * 16, s));
             k_col_verify<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_ca.p, S->man_cb.p, S->man_color.p, S->vmasks.p, w->err.p);
             L++;
         }
+        prof_mark(w);
+        PrepArgs PA;
+        PA.nc = nc; PA.h = h; PA.perm = S->perm.p; PA.L_a = S->L_a.p; PA.L_b = S->L_b.p; PA.L_p = S->L_p.p; PA.L_n = S->L_n.p;
+        PA.man_start = S->man_start.p; PA.col_start = S->col_start.p; PA.col_list = S->col_list.p;
+        PA.jds_off = S->jds_off.p;
+        PA.pos = w->b_pos.p; PA.v = w->b_v.p; PA.w = w->b_w.p; PA.im = w->b_im.p; PA.iiw = w->b_iiw.p;
+        PA.S_n = S->S_n.p; PA.S_t1 = S->S_t1.p; PA.S_t2 = S->S_t2.p; PA.S_ra = S->S_ra.p; PA.S_rb = S->S_rb.p; PA.S_j = S->S_j.p;
+        PA.invperm = S->invperm.p;
+        k_prep<<<g_nc, 256, 0, s>>>(PA);
+        L++;
     } else {
         prof_mark(w);
         prof_mark(w);
@@ -1315,16 +1448,21 @@ static sf_status substep(sf_world *w, float h) {
     if (nc && w->P.iterations) {
         SolveArgs A;
         A.iterations = w->P.iterations; A.dev = S->dev.p; A.col_start = S->col_start.p; A.col_list = S->col_list.p;
-        A.man_a = S->man_a.p; A.man_b = S->man_b.p; A.man_start = S->man_start.p; A.man_count = S->man_count.p;
+        A.jds_off = S->jds_off.p; A.man_a = S->man_a.p; A.man_b = S->man_b.p; A.man_count = S->man_count.p;
         A.S_n = S->S_n.p; A.S_t1 = S->S_t1.p; A.S_t2 = S->S_t2.p; A.S_ra = S->S_ra.p; A.S_rb = S->S_rb.p; A.S_j = S->S_j.p;
         A.v = w->b_v.p; A.w = w->b_w.p; A.im = w->b_im.p; A.iiw = w->b_iiw.p; A.gb = w->barrier.p; A.err = w->err.p;
         if (nc <= SOLVE_ONE_BLOCK_MAX_CONTACTS) {
             k_solve_one_block<<<1, SOLVE_ONE_BLOCK, 0, s>>>(A);
         } else {
-            unsigned per_sm = w->P.solve_blocks ? std::min<unsigned>(w->P.solve_blocks, S->solve_occ) : std::min(S->solve_occ, 2);
+            int sci = -1;
+            const int sb = Tuner::bucket(nc);
+            unsigned per_sm = w->P.solve_blocks ? std::min<unsigned>(w->P.solve_blocks, S->solve_occ)
+                                                : (unsigned)S->solve_t.choose(sb, sci);
             unsigned sgrid = (unsigned)std::min<uint64_t>((uint64_t)w->sms * per_sm, (nc + SOLVE_BLOCK - 1) / SOLVE_BLOCK + 1);
             void *sargs[] = {&A};
+            tune_begin(S, &S->solve_t, sb, sci, s);
             SF_CUDA(cudaLaunchCooperativeKernel((void *)k_solve, dim3(sgrid), dim3(SOLVE_BLOCK), sargs, 0, s));
+            tune_end(S, sci, s);
         }
         L++;
         S->solve_launches++;
@@ -1399,6 +1537,7 @@ static sf_status step_impl(sf_world *w, float dt, uint32_t nsteps, const uint8_t
         if (k + 1 < nsteps) {
             SF_CUDA(cudaStreamSynchronize(s));
             apply_live_readback(w);
+            tune_resolve(S);
         }
     }
     SF_CUDA(cudaMemsetAsync(S->dev.p + DV_ALIVE, 0, 2 * sizeof(uint32_t), s));
@@ -1407,9 +1546,14 @@ static sf_status step_impl(sf_world *w, float dt, uint32_t nsteps, const uint8_t
     SF_CUDA(cudaMemcpyAsync(S->h_dev, S->dev.p, DV_N * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     sf_status r = read_error_word(w);   // synchronises the stream
     if (nsteps) apply_live_readback(w);
+    tune_resolve(S);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, w->ev0, w->ev1);
     sf_stats &st = w->stats;
+    // the next step hashes sparsely once at most half the active scenes' bodies are awake (below that the smaller
+    // sort and the contact pass over awake bricks only pay for the extra passes and the count read-back; measured on
+    // the 256-scene mix)
+    S->use_sparse = nsteps && (uint64_t)S->h_dev[DV_AWAKE] * 2 <= (uint64_t)S->nb_act;
     st.contacts = S->h_dev[DV_CONTACTS];
     st.manifolds = S->h_dev[DV_MANIFOLDS];
     st.colors = S->h_dev[DV_COLORS];
@@ -1442,6 +1586,15 @@ using namespace sf;
 extern "C" {
 
 sf_status sf_world_step(sf_world *w, float dt, uint32_t nsteps) { return step_impl(w, dt, nsteps, nullptr); }
+
+sf_status sf_read_tuning(sf_world *w, uint32_t which, int32_t *blocks_per_sm, uint32_t n) {
+    if (!w || !blocks_per_sm) { set_error("null argument"); return SF_ERR_ARG; }
+    const Tuner *t = which == SF_TUNE_SOLVE ? &w->step->solve_t : which == SF_TUNE_COLOR ? &w->step->jp_t
+                                                                                      : sor_tuner(w->sor);
+    if (!t) { set_error("no such tuner"); return SF_ERR_ARG; }
+    for (uint32_t b = 0; b < n; b++) blocks_per_sm[b] = b < (uint32_t)Tuner::NB ? t->settled((int)b) : -1;
+    return SF_OK;
+}
 
 sf_status sf_world_step_scenes(sf_world *w, float dt, uint32_t nsteps, const uint8_t *scene_mask) {
     if (!w || !scene_mask) { set_error("null argument"); return SF_ERR_ARG; }
@@ -1498,10 +1651,13 @@ sf_status sf_read_contacts(sf_world *w, uint32_t scene, uint32_t *ids5, float *f
     uint32_t lo = 0, hi = 0;
     const uint32_t kb = S->act_brick_base[scene];
     if (sc.n_bricks && kb != NONE && S->n_awk) {
-        uint32_t a0 = 0, a1 = S->n_awk;
-        SF_CUDA(cudaMemcpyAsync(&a0, S->awk_pos.p + kb, 4, cudaMemcpyDeviceToHost, s));
-        if (kb + sc.n_bricks < S->nd_act) SF_CUDA(cudaMemcpyAsync(&a1, S->awk_pos.p + kb + sc.n_bricks, 4, cudaMemcpyDeviceToHost, s));
-        SF_CUDA(cudaStreamSynchronize(s));
+        uint32_t a0 = kb, a1 = std::min(kb + sc.n_bricks, S->n_awk);
+        if (S->last_sparse) {
+            a1 = S->n_awk;
+            SF_CUDA(cudaMemcpyAsync(&a0, S->awk_pos.p + kb, 4, cudaMemcpyDeviceToHost, s));
+            if (kb + sc.n_bricks < S->nd_act) SF_CUDA(cudaMemcpyAsync(&a1, S->awk_pos.p + kb + sc.n_bricks, 4, cudaMemcpyDeviceToHost, s));
+            SF_CUDA(cudaStreamSynchronize(s));
+        }
         lo = nc; hi = nc;
         if (a0 < S->n_awk) SF_CUDA(cudaMemcpyAsync(&lo, S->coff.p + a0, 4, cudaMemcpyDeviceToHost, s));
         if (a1 < S->n_awk) SF_CUDA(cudaMemcpyAsync(&hi, S->coff.p + a1, 4, cudaMemcpyDeviceToHost, s));
