@@ -93,6 +93,7 @@ typedef struct sf_stats {
     uint64_t contact_capacity;
     double ms_last_step;        /* device time of the last sf_world_step call (CUDA events) */
     uint64_t launches;          /* kernels this world has launched (all entry points) */
+    uint64_t graph_launches;    /* load-path solves replayed from a captured CUDA graph */
 } sf_stats;
 
 /* Per-phase device time of the rigid step, from CUDA events around each phase of each substep (profiling on). */

@@ -160,6 +160,7 @@ struct StepState;    // sf_step.cu
 struct SorState;     // sf_sor.cu
 uint64_t sor_launches(const SorState *st);
 const Tuner *sor_tuner(const SorState *st);
+uint64_t sor_graph_launches(const SorState *st);
 void sor_reset_launches(SorState *st);
 
 // Device buffers of one structure's load-path solve when the caller supplies every buffer (no allocation inside).

@@ -25,6 +25,8 @@
 
 namespace sf {
 
+struct SorParams { double omega, tol; uint32_t max_sweeps, pad; };
+
 struct SorState {
     DBuf<double> cphi;
     DBuf<float> crhs;
@@ -55,6 +57,13 @@ struct SorState {
     uint64_t launches = 0;
     int occ = 1;
     Tuner tune;   // blocks per SM of the red-black kernel, keyed on log2(chunks of the solve)
+    // The solve's launch sequence captured in CUDA graphs, one per launch shape (the chunk list and the active
+    // flags live in device buffers the graph reads, so a graph serves every solve of its shape).
+    struct Graph { uint32_t n_work, grid; cudaGraphExec_t exec; };
+    DBuf<SorParams> prm;
+    std::vector<Graph> graphs;
+    bool graphs_ok = true;
+    uint64_t graph_launches = 0;
 };
 
 const Tuner *sor_tuner(const SorState *st) { return st ? &st->tune : nullptr; }
@@ -161,6 +170,8 @@ struct SorArgs {
     double *resid;
     double omega, tol;
     uint32_t max_sweeps;
+    const SorParams *prm;          // when set, omega / tol / max_sweeps are read from here (a captured graph's launch
+                                   // then serves every parameter set)
     GridBarrier *gb;
     uint32_t *err;
 };
@@ -207,7 +218,9 @@ __global__ void __launch_bounds__(SOR_BLOCK) k_sor_redblack(SorArgs A) {
     const uint32_t per = (A.n_work + gridDim.x - 1) / gridDim.x;
     const uint32_t w0 = min(A.n_work, blockIdx.x * per), w1 = min(A.n_work, w0 + per);
     const unsigned long long one = (unsigned long long)__double_as_longlong(1.0);
-    for (uint32_t sweep = 0; sweep < A.max_sweeps; sweep++) {
+    const double omega = A.prm ? A.prm->omega : A.omega, tol = A.prm ? A.prm->tol : A.tol;
+    const uint32_t max_sweeps = A.prm ? A.prm->max_sweeps : A.max_sweeps;
+    for (uint32_t sweep = 0; sweep < max_sweeps; sweep++) {
         unsigned long long *md = A.resid_buf + (size_t)((sweep % 3) * 2) * nst;
         unsigned long long *mp = md + nst;
         if (blockIdx.x == 0) {
@@ -259,7 +272,7 @@ __global__ void __launch_bounds__(SOR_BLOCK) k_sor_redblack(SorArgs A) {
                 double dabs = 0.0;
                 if (sk > 0.0) {
                     const double target = ((double)A.crhs[at] + skp) / sk;
-                    const double dd = A.omega * (target - p);
+                    const double dd = omega * (target - p);
                     p += dd;
                     A.cphi[at] = p;
                     dabs = fabs(dd);
@@ -280,7 +293,7 @@ __global__ void __launch_bounds__(SOR_BLOCK) k_sor_redblack(SorArgs A) {
             if (!is_active(act, (int32_t)s)) continue;
             const double r = __longlong_as_double((long long)__ldcg(&md[s])) / __longlong_as_double((long long)__ldcg(&mp[s]));
             if (blockIdx.x == 0) { A.sweeps[s] = sweep + 1; A.resid[s] = r; }
-            if (r < A.tol || sweep + 1 >= A.max_sweeps) atomicAnd(&act[s >> 5], ~(1u << (s & 31)));
+            if (r < tol || sweep + 1 >= max_sweeps) atomicAnd(&act[s >> 5], ~(1u << (s & 31)));
             else s_any = 1;
         }
         __syncthreads();
@@ -558,6 +571,7 @@ sf_status sor_create(sf_world *w) {
             if (t) nbr[(size_t)c * 6 + d] = (int32_t)(t - 1);
         }
     }
+    SF_CUDA(st->prm.alloc(1));
     SF_CUDA(st->chunk_nbr.alloc(nbr.size()));
     if (!nbr.empty()) SF_CUDA(cudaMemcpyAsync(st->chunk_nbr.p, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice, s));
     // chunks of each structure
@@ -637,7 +651,7 @@ cudaError_t sor_solve_on_buffers(const SorBuffers &B, uint32_t n_bricks, uint32_
     A.cphi = B.cphi; A.crhs = B.crhs; A.ccode = B.ccode; A.csid = B.csid; A.chunk_nbr = B.chunk_nbr; A.chunk_sid = B.chunk_sid;
     A.work = B.work; A.n_work = n_chunks; A.n_struct = 1; A.active0 = B.active0; A.resid_buf = B.resid_buf;
     A.sweeps = B.sweeps; A.resid = B.resid; A.omega = (double)omega; A.tol = (double)tol; A.max_sweeps = max_sweeps;
-    A.gb = B.gb; A.err = B.err;
+    A.prm = nullptr; A.gb = B.gb; A.err = B.err;
     unsigned grid = (unsigned)std::min<size_t>(n_chunks, (size_t)sms * std::max(occ, 1));
     void *args[] = {&A};
     if ((e = cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s)) != cudaSuccess) return e;
@@ -647,9 +661,11 @@ cudaError_t sor_solve_on_buffers(const SorBuffers &B, uint32_t n_bricks, uint32_
 }
 
 uint64_t sor_launches(const SorState *st) { return st ? st->wk.launches + st->launches : 0; }
+uint64_t sor_graph_launches(const SorState *st) { return st ? st->graph_launches : 0; }
 void sor_reset_launches(SorState *st) { if (st) { st->wk.launches = 0; st->launches = 0; } }
 
 void sor_destroy(sf_world *w) {
+    if (w->sor) for (auto &g : w->sor->graphs) cudaGraphExecDestroy(g.exec);
     delete w->sor;
     w->sor = nullptr;
 }
@@ -715,27 +731,58 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     SF_CUDA(cudaMemcpyAsync(st->work.p, chunks.data(), chunks.size() * 4, cudaMemcpyHostToDevice, s));
     SF_CUDA(cudaEventRecord(w->ev0, s));
     size_t ncell = (size_t)w->n_chunks * 512;
-    k_sor_clear<<<grid_for(ncell, 256), 256, 0, s>>>((uint32_t)ncell, st->ccode.p, st->csid.p);
     st->launches += 5;   // clear, scatter, init, red-black, gather
-    k_sor_scatter<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p, w->s_nb6.p,
-                                                       w->s_bond.p, w->s_phi64.p, w->s_ext.p, w->ctab.p, st->cphi.p,
-                                                       st->crhs.p, st->ccode.p, st->csid.p);
-    k_sor_init<<<grid_for(nst, 256), 256, 0, s>>>(nst, st->resid_buf.p, st->sweeps.p, st->resid.p);
-    SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s));
-    SF_CUDA(cudaMemsetAsync(w->err.p, 0, sizeof(uint32_t), s));
     SorArgs A;
     A.cphi = st->cphi.p; A.crhs = st->crhs.p; A.ccode = st->ccode.p; A.csid = st->csid.p; A.chunk_nbr = st->chunk_nbr.p;
     A.chunk_sid = st->chunk_sid.p; A.work = st->work.p; A.n_work = (uint32_t)chunks.size(); A.n_struct = nst;
     A.active0 = st->active0.p; A.resid_buf = st->resid_buf.p; A.sweeps = st->sweeps.p; A.resid = st->resid.p;
     A.omega = (double)omega; A.tol = (double)tol; A.max_sweeps = max_sweeps; A.gb = w->barrier.p; A.err = w->err.p;
+    A.prm = st->prm.p;
+    const SorParams hp{(double)omega, (double)tol, max_sweeps, 0u};
+    SF_CUDA(cudaMemcpyAsync(st->prm.p, &hp, sizeof hp, cudaMemcpyHostToDevice, s));
     int tci = -1;
     const int tb = Tuner::bucket(chunks.size());
     const unsigned per_sm = (unsigned)st->tune.choose(tb, tci);
     unsigned grid = (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * per_sm);
     void *args[] = {&A};
-    SF_CUDA(cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s));
-    k_sor_gather<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p,
-                                                      st->active0.p, w->ctab.p, st->cphi.p, w->s_phi64.p, w->s_phi.p);
+    auto enqueue = [&]() -> cudaError_t {
+        k_sor_clear<<<grid_for(ncell, 256), 256, 0, s>>>((uint32_t)ncell, st->ccode.p, st->csid.p);
+        k_sor_scatter<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p,
+                                                           w->s_nb6.p, w->s_bond.p, w->s_phi64.p, w->s_ext.p, w->ctab.p,
+                                                           st->cphi.p, st->crhs.p, st->ccode.p, st->csid.p);
+        k_sor_init<<<grid_for(nst, 256), 256, 0, s>>>(nst, st->resid_buf.p, st->sweeps.p, st->resid.p);
+        cudaError_t e = cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(w->err.p, 0, sizeof(uint32_t), s);
+        if (e == cudaSuccess) e = cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s);
+        if (e != cudaSuccess) return e;
+        k_sor_gather<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p,
+                                                          st->active0.p, w->ctab.p, st->cphi.p, w->s_phi64.p, w->s_phi.p);
+        return cudaGetLastError();
+    };
+    // replay the captured sequence for this launch shape, capturing it the first time; if the runtime refuses to
+    // capture (a cooperative launch in a graph), the solve launches directly from then on
+    cudaGraphExec_t ex = nullptr;
+    for (auto &g : st->graphs)
+        if (g.n_work == A.n_work && g.grid == grid) ex = g.exec;
+    if (!ex && st->graphs_ok) {
+        cudaGraph_t gr = nullptr;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const cudaError_t e1 = enqueue();
+            const cudaError_t e2 = cudaStreamEndCapture(s, &gr);
+            if ((e1 != cudaSuccess || e2 != cudaSuccess) && gr) { cudaGraphDestroy(gr); gr = nullptr; }
+        }
+        if (gr) {
+            if (cudaGraphInstantiate(&ex, gr, 0) != cudaSuccess) ex = nullptr;
+            cudaGraphDestroy(gr);
+        }
+        if (!ex) { st->graphs_ok = false; cudaGetLastError(); }
+        else {
+            if (st->graphs.size() >= 8) { cudaGraphExecDestroy(st->graphs.front().exec); st->graphs.erase(st->graphs.begin()); }
+            st->graphs.push_back({A.n_work, grid, ex});
+        }
+    }
+    if (ex) { SF_CUDA(cudaGraphLaunch(ex, s)); st->graph_launches++; }
+    else SF_CUDA(enqueue());
     SF_CUDA(cudaEventRecord(w->ev1, s));
     SF_CUDA(cudaGetLastError());
     std::vector<uint32_t> sw(nst);
@@ -752,6 +799,7 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
         rep.brick_sweeps += (uint64_t)sw[q] * st->h_st_count[q];
         rep.max_residual = std::max(rep.max_residual, (double)rs[q]);
     }
+    w->stats.graph_launches = st->graph_launches;
     // per sweep, since solves of one bucket converge in different sweep counts
     if (e == SF_OK) st->tune.record(tb, tci, ms / (float)std::max<uint32_t>(rep.max_sweeps_done, 1));
     if (report) *report = rep;

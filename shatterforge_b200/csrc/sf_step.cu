@@ -1564,6 +1564,7 @@ static sf_status step_impl(sf_world *w, float dt, uint32_t nsteps, const uint8_t
     st.contact_capacity = S->capacity;
     st.ms_last_step = ms;
     st.launches = w->launches + S->wk.launches + sor_launches(w->sor);
+    st.graph_launches = sor_graph_launches(w->sor);
     if (S->profile) {
         // each substep recorded SF_PHASES + 1 events
         const size_t per = SF_PHASES + 1;
