@@ -361,15 +361,23 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
             speed = len(v3(vv.x, vv.y, vv.z)) + len(v3(ww.x, ww.y, ww.z)) * A.rad[a] * 0.5f;
         }
         const float lim2 = 4.0f * RB * RB;
-        for (int dz = -1; dz <= 1; dz++)
-            for (int dy = -1; dy <= 1; dy++)
-                for (int dx = -1; dx <= 1; dx++) {
-                    const uint2 rg = A.brange[(size_t)sk * HSIZE + hkey(hx + dx, hy + dy, hz + dz)];
+        const uint2 *br = A.brange + (size_t)sk * HSIZE;
+        for (int dz = -1; dz <= 1; dz++) {
+            // the layer's nine bucket ranges are fetched together (independent loads in flight), then walked in the
+            // reference's dy, dx order
+            uint2 rgs[9];
+#pragma unroll
+            for (int c = 0; c < 9; c++) rgs[c] = br[hkey(hx + (c % 3) - 1, hy + (c / 3) - 1, hz + dz)];
+#pragma unroll 1
+            for (int c = 0; c < 9; c++) {
+                    uint2 rg = rgs[0];   // register select, not a dynamically indexed (local memory) array
+#pragma unroll
+                    for (int k = 1; k < 9; k++) if (c == k) rg = rgs[k];
                     for (uint32_t q = rg.y; q > rg.x; q--) {
                         const uint32_t info = A.sinfo[q - 1];
+                        const float4 rec = A.srec[q - 1];
                         const uint32_t bj = info & 0x3FFFFFFFu;
                         if (bj == a || (info & 0x40000000u)) continue;
-                        const float4 rec = A.srec[q - 1];
                         const uint32_t j = __float_as_uint(rec.w);
                         const bool other_awake = !(info & 0x80000000u);
                         if (other_awake && j < i) continue;
@@ -386,12 +394,13 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
                             emit(STATIC, bj, j, cp, nn, 2.0f * RB - dist);
                         }
                     }
-                }
+            }
+        }
     }
 }
 
 // pass 1: every contact of every awake brick counted; the first CSLOTS kept in the brick's slots
-__global__ void __launch_bounds__(128, 8) k_contacts_gen(ContactArgs A) {
+__global__ void __launch_bounds__(128, 6) k_contacts_gen(ContactArgs A) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= A.nd) return;
     const uint32_t i = pick(A.list, t);
