@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-worlds", type=int, default=96)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
+    ap.add_argument("--serve-age-steps", type=int, default=300,
+                    help="steps the population has run before the aged stream (0 = skip the aged runs)")
     return ap.parse_args()
 
 
@@ -267,7 +269,7 @@ def _latency(res, kind=None):
             "p999_ms": float(np.percentile(lat, 99.9)), "mean_ms": float(lat.mean())}
 
 
-def serve_run(args, worlds, structs, slots, batching: bool, seconds: float, seed: int):
+def serve_run(args, worlds, structs, slots, batching: bool, seconds: float, seed: int, states=None):
     """One server on the population, fed a Poisson stream of `seconds` at --serve-rate; returns the summary."""
     import shatterforge_b200 as sf
     from shatterforge_b200 import serving as SV
@@ -275,6 +277,9 @@ def serve_run(args, worlds, structs, slots, batching: bool, seconds: float, seed
     srv = SV.Server(slots=slots, structures=structs, budget_bytes=int(args.serve_budget_gb * 2**30), batching=batching,
                     sweeps_per_tick=128, iterations=ITERS, pinch_kill=0)
     ids = [srv.add_scene(w) for w in worlds]
+    if states is not None:
+        for i, st in zip(ids, states):
+            srv.set_scene_state(i, *st)
     sids = structs.structure_ids()
     srv.start()
     # resident structures start solved (their potentials are part of the resident state)
@@ -335,11 +340,25 @@ def serve_section(args):
         slots = [big] * int(min(k, len(worlds)))
     batched = serve_run(args, worlds, structs, slots, True, args.serve_seconds, seed=23)
     plain = serve_run(args, worlds, structs, slots, False, args.serve_plain_seconds, seed=23)
+    aged = None
+    if args.serve_age_steps > 0:
+        # the same population after it has run a while (most debris settled): the worlds a server keeps resident
+        import shatterforge_b200 as sf
+        wa = sf.World(worlds, iterations=ITERS, pinch_kill=0)
+        wa.step(DT, nsteps=args.serve_age_steps)
+        st, sl, fl = wa.bodies()
+        awake = int(wa.stats().awake)
+        off = wa.body_off
+        states = [(st[off[k]:off[k + 1]], sl[off[k]:off[k + 1]], fl[off[k]:off[k + 1]]) for k in range(len(worlds))]
+        wa.close()
+        aged = {"age_steps": args.serve_age_steps, "awake_bodies": awake,
+                "batched": serve_run(args, worlds, structs, slots, True, args.serve_seconds, seed=29, states=states),
+                "plain": serve_run(args, worlds, structs, slots, False, args.serve_plain_seconds, seed=29, states=states)}
     return {"rate_req_s": args.serve_rate, "worlds": len(worlds), "world_bodies": int(sizes.sum()),
             "structures": len(structs.structure_ids()), "structure_bricks": structs.n_static,
             "slots": len(slots), "budget_gb": args.serve_budget_gb, "mix": "70% scene steps (1-8 steps), 30% structure "
             "solves (3 random loads of 50-400 kg, omega 1.7 to 1e-6, from resident potentials)",
-            "batched": batched, "plain": plain,
+            "batched": batched, "plain": plain, "aged": aged,
             "note": "latency = completion - arrival on the server clock; plain = one request at a time with its own "
                     "launches, on the same population and the first seconds of the same stream"}
 

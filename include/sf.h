@@ -184,7 +184,9 @@ typedef struct sf_world_info {
 } sf_world_info;
 sf_status sf_world_get_info(const sf_world *w, sf_world_info *info);
 sf_status sf_get_stats(const sf_world *w, sf_stats *stats);
-/* 13 floats per body (pos 3, quat 4, v 3, spin 3); sleep timer; flags bit0 alive, bit1 asleep */
+/* 13 floats per body (pos 3, quat 4, v 3, spin 3); sleep timer; flags bit0 alive, bit1 asleep. A write refreshes
+ * the rotation cache and brick positions of every body whose pose it changes (sleeping ones included); bodies
+ * written with their current pose keep their caches, so reading and writing back the state changes nothing. */
 sf_status sf_read_bodies(sf_world *w, float *state13, float *sleep, uint8_t *flags);
 sf_status sf_write_bodies(sf_world *w, const float *state13, const float *sleep, const uint8_t *flags);
 /* per body: mass, 1/mass, radius, local inverse inertia 9; per body brick: local offset 3 */
@@ -264,8 +266,9 @@ sf_status sf_pool_clear(sf_world *w, uint32_t slot);
 uint64_t sf_pool_snapshot_bytes(uint32_t n_bodies, uint32_t n_bricks);
 sf_status sf_pool_save(sf_world *w, uint32_t slot, void *host, uint64_t cap, uint64_t *bytes);
 sf_status sf_pool_restore(sf_world *w, uint32_t slot, const sf_scene_desc *scene, const void *host, uint64_t bytes);
-/* The loaded scene's bodies, as sf_read_bodies. */
+/* The loaded scene's bodies, as sf_read_bodies / sf_write_bodies. */
 sf_status sf_pool_read_bodies(sf_world *w, uint32_t slot, float *state13, float *sleep, uint8_t *flags);
+sf_status sf_pool_write_bodies(sf_world *w, uint32_t slot, const float *state13, const float *sleep, const uint8_t *flags);
 
 /* ---- serving (no counterpart in the reference): a request loop over resident worlds with continuous batching.
  * Scene-step requests run on a scene pool (one step of every scene with work per tick, in one set of launches;
@@ -314,6 +317,10 @@ typedef struct sf_server_stats {
 sf_status sf_server_create(const sf_server_desc *desc, sf_server **out);
 /* Register a scene (deep copy) before sf_server_start; it is loaded into a slot when a request needs it. */
 sf_status sf_server_add_scene(sf_server *s, const sf_scene_desc *scene, uint32_t *id);
+/* Optional, before sf_server_start: the registered scene's body state (as sf_write_bodies) at its first load, e.g.
+ * a world that has already been running (copied). */
+sf_status sf_server_set_scene_state(sf_server *s, uint32_t id, const float *state13, const float *sleep,
+                                    const uint8_t *flags);
 sf_status sf_server_start(sf_server *s);
 /* Thread-safe. */
 sf_status sf_server_submit(sf_server *s, const sf_request *req, uint64_t *ticket);

@@ -170,6 +170,8 @@ PROTOTYPES = {
     "sf_pool_save": (C.c_int32, [_vp, C.c_uint32, _vp, C.c_uint64, _u64p]),
     "sf_pool_restore": (C.c_int32, [_vp, C.c_uint32, C.POINTER(SceneDesc), _vp, C.c_uint64]),
     "sf_pool_read_bodies": (C.c_int32, [_vp, C.c_uint32, _f32p, _f32p, _u8p]),
+    "sf_pool_write_bodies": (C.c_int32, [_vp, C.c_uint32, _f32p, _f32p, _u8p]),
+    "sf_server_set_scene_state": (C.c_int32, [_vp, C.c_uint32, _f32p, _f32p, _u8p]),
     "sf_server_create": (C.c_int32, [C.POINTER(ServerDesc), C.POINTER(_vp)]),
     "sf_server_add_scene": (C.c_int32, [_vp, C.POINTER(SceneDesc), _u32p]),
     "sf_server_start": (C.c_int32, [_vp]),

@@ -245,7 +245,7 @@ struct sf_world {
     sf::DBuf<int32_t> k_xyz;
 
     sf::DBuf<float> stage13;     // packed body state for the read/write calls
-    sf::DBuf<uint8_t> stage_flags;
+    sf::DBuf<uint8_t> stage_flags, stage_dirty;
     sf::DBuf<uint32_t> err;      // [0] error bits, [1..] counters
     sf::DBuf<sf::GridBarrier> barrier;
 

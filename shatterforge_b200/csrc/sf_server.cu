@@ -68,6 +68,8 @@ struct SceneRec {
     uint8_t *snap = nullptr;     // pinned snapshot of an evicted scene
     uint64_t snap_bytes = 0;
     bool has_snap = false;
+    std::vector<float> init13, init_sleep;   // optional body state at the first load
+    std::vector<uint8_t> init_flags;
 };
 
 }  // namespace sf
@@ -181,6 +183,8 @@ sf_status admit(sf_server *S, uint32_t id, bool &ok) {
     const sf_scene_desc d = R.sc.desc();
     sf_status r = R.has_snap ? sf_pool_restore(S->pool, (uint32_t)best, &d, R.snap, R.snap_bytes)
                              : sf_pool_load(S->pool, (uint32_t)best, &d);
+    if (r == SF_OK && !R.has_snap && !R.init13.empty())
+        r = sf_pool_write_bodies(S->pool, (uint32_t)best, R.init13.data(), R.init_sleep.data(), R.init_flags.data());
     if (r != SF_OK) return r;
     const bool restored = R.has_snap;
     bump(S, [&](sf_server_stats &t) { if (restored) t.restores++; else t.loads++; });
@@ -448,6 +452,19 @@ sf_status sf_server_add_scene(sf_server *S, const sf_scene_desc *d, uint32_t *id
     if (!any) { set_error("no slot of the pool fits a scene of %u bodies, %u bricks", c.n_bodies, c.n_bricks); return SF_ERR_BUDGET; }
     *id = (uint32_t)S->scenes.size();
     S->scenes.push_back(std::move(R));
+    return SF_OK;
+}
+
+sf_status sf_server_set_scene_state(sf_server *S, uint32_t id, const float *state13, const float *sleep,
+                                    const uint8_t *flags) {
+    if (!S || !state13 || !sleep || !flags) { set_error("null argument"); return SF_ERR_ARG; }
+    if (S->started) { set_error("scene states are set before sf_server_start"); return SF_ERR_STATE; }
+    if (id >= S->scenes.size()) { set_error("scene %u is not registered", id); return SF_ERR_ARG; }
+    SceneRec &R = *S->scenes[id];
+    const uint32_t n = R.sc.n_bodies;
+    R.init13.assign(state13, state13 + (size_t)n * 13);
+    R.init_sleep.assign(sleep, sleep + n);
+    R.init_flags.assign(flags, flags + n);
     return SF_OK;
 }
 

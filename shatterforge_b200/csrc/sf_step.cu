@@ -79,6 +79,7 @@ struct StepState {
     uint64_t capacity = 0;
     uint64_t last_contacts = 0;
     int solve_occ = 1, jp_occ = 1;
+    uint32_t max_scene_bodies = 0;
     // launch-shape tuning: pending timings of this step's tuned launches
     Tuner solve_t, jp_t;
     struct Pending { Tuner *t; int bucket, ci; cudaEvent_t e0, e1; };
@@ -463,12 +464,15 @@ __global__ void k_body_nc(uint32_t nc, const uint32_t *L_a, const uint32_t *L_b,
 }
 
 // ---------------------------------------------------------------- manifolds
-__global__ void k_man_keys(uint32_t nc, uint64_t nb1, const uint32_t *L_a, const uint32_t *L_b, uint64_t *key, uint32_t *val) {
+// key = (a, b') with b' = 0 for the static side, else b's index in its scene + 1 (both bodies are in one scene, so
+// the pair order is the same as with global ids, in fewer key bits)
+__global__ void k_man_keys(uint32_t nc, uint64_t span, const uint32_t *L_a, const uint32_t *L_b, const uint32_t *body_off,
+                           uint64_t *key, uint32_t *val) {
     uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nc) return;
     uint32_t b = L_b[k];
-    uint64_t bp = b == STATIC ? 0 : (uint64_t)b + 1;
-    key[k] = (uint64_t)L_a[k] * nb1 + bp;
+    uint64_t bp = b == STATIC ? 0 : (uint64_t)(b - body_off[b]) + 1;
+    key[k] = (uint64_t)L_a[k] * span + bp;
     val[k] = k;
 }
 __global__ void k_man_flags(uint32_t nc, const uint64_t *key, uint32_t *flag) {
@@ -640,17 +644,27 @@ __device__ __forceinline__ bool jp_blocked(const JpArgs &A, uint32_t body, uint3
     return false;
 }
 
+// Once a round's worklist is short, block 0 runs the remaining rounds alone with block barriers (the other blocks
+// leave): every round still sees the colours of all earlier rounds, so the colouring is the same.
+constexpr uint32_t JP_SOLO = 4096;
 __global__ void __launch_bounds__(256) k_jp(JpArgs A) {
     const uint32_t nm = *A.nm_p;
     uint32_t r = 0;
+    bool solo = gridDim.x == 1;
     for (; r < A.max_rounds; r++) {
         const uint32_t n_in = r == 0 ? nm : __ldcg(&A.dev[DV_WL0 + (r % 3)]);
         if (n_in == 0) break;
+        if (!solo && n_in <= JP_SOLO) {
+            solo = true;
+            if (blockIdx.x != 0) return;
+        }
+        const uint32_t t0 = solo ? threadIdx.x : blockIdx.x * blockDim.x + threadIdx.x;
+        const uint32_t step = solo ? blockDim.x : gridDim.x * blockDim.x;
         const uint32_t *wl_in = (r & 1) ? A.wl1 : A.wl0;
         uint32_t *wl_out = (r & 1) ? A.wl0 : A.wl1;
         uint32_t *cnt_out = &A.dev[DV_WL0 + ((r + 1) % 3)];
         if (blockIdx.x == 0 && threadIdx.x == 0) A.dev[DV_WL0 + ((r + 2) % 3)] = 0;
-        for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_in; t += gridDim.x * blockDim.x) {
+        for (uint32_t t = t0; t < n_in; t += step) {
             const uint32_t m = r == 0 ? t : __ldcg(&wl_in[t]);
             const uint32_t a = A.man_a[m], b = A.man_b[m], pm = A.prio[m];
             bool blocked = jp_blocked(A, a, m, pm, r);
@@ -671,7 +685,10 @@ __global__ void __launch_bounds__(256) k_jp(JpArgs A) {
             atomicOr(&A.masks[(size_t)a * 4 + (c >> 5)], 1u << (c & 31));
             if (b != STATIC) atomicOr(&A.masks[(size_t)b * 4 + (c >> 5)], 1u << (c & 31));
         }
-        if (!grid_sync(A.gb, gridDim.x, A.err)) return;
+        if (solo) {
+            __threadfence();
+            __syncthreads();
+        } else if (!grid_sync(A.gb, gridDim.x, A.err)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         A.dev[DV_ROUNDS] = r;
@@ -1152,7 +1169,10 @@ sf_status step_create(sf_world *w) {
     SF_CUDA(cudaMemsetAsync(S->dev.p, 0, S->dev.bytes(), s));
     SF_CUDA(cudaMallocHost((void **)&S->h_dev, DV_N * sizeof(uint32_t)));
     std::vector<uint32_t> off(nb);
-    for (const Scene &sc : w->scenes) for (uint32_t b = 0; b < sc.n_bodies; b++) off[sc.body_off + b] = sc.body_off;
+    for (const Scene &sc : w->scenes) {
+        for (uint32_t b = 0; b < sc.n_bodies; b++) off[sc.body_off + b] = sc.body_off;
+        S->max_scene_bodies = std::max(S->max_scene_bodies, sc.n_bodies);
+    }
     SF_CUDA(S->body_off_of_body.alloc(nb));
     if (nb) SF_CUDA(cudaMemcpyAsync(S->body_off_of_body.p, off.data(), nb * 4, cudaMemcpyHostToDevice, s));
     uint64_t initial = w->P.contact_capacity ? w->P.contact_capacity : (uint64_t)std::max<uint32_t>(nd, 1) * 4;
@@ -1384,10 +1404,10 @@ static sf_status substep(sf_world *w, float h) {
     if (S->profile) S->sub_nc.push_back(nc);
     prof_mark(w);
     // manifolds
-    const uint64_t nb1 = (uint64_t)w->nb + 1;
     if (nc) {
-        k_man_keys<<<g_nc, 256, 0, s>>>(nc, nb1, S->L_a.p, S->L_b.p, S->mkey.p, S->perm.p);
-        SF_CUDA(radix_sort_u64(S->mkey.p, S->perm.p, S->mkey_alt.p, S->perm_alt.p, nc, bits_for((uint64_t)w->nb * nb1 + nb1), S->wk, s));
+        const uint64_t span = (uint64_t)S->max_scene_bodies + 1;
+        k_man_keys<<<g_nc, 256, 0, s>>>(nc, span, S->L_a.p, S->L_b.p, S->body_off_of_body.p, S->mkey.p, S->perm.p);
+        SF_CUDA(radix_sort_u64(S->mkey.p, S->perm.p, S->mkey_alt.p, S->perm_alt.p, nc, bits_for((uint64_t)w->nb * span + span), S->wk, s));
         const uint32_t K = w->P.manifold_chunk;
         k_man_flags<<<g_nc, 256, 0, s>>>(nc, S->mkey.p, S->mflag.p);
         SF_CUDA(exclusive_scan_u32(S->mflag.p, S->mpos.p, nc, S->dev.p + DV_PAIRS, S->wk, s));

@@ -152,17 +152,50 @@ __global__ void k_pack_bodies(uint32_t nb, const float4 *pos, const float4 *q, c
     o[7] = vv.x; o[8] = vv.y; o[9] = vv.z; o[10] = ww.x; o[11] = ww.y; o[12] = ww.z;
     flags[b] = (alive[b] ? 1 : 0) | (asleep[b] ? 2 : 0);
 }
+// dirty[b] = the body's pose changed (or it came back to life): its rotation cache and brick positions are refreshed
 __global__ void k_unpack_bodies(uint32_t nb, const float *in13, const uint8_t *flags, float4 *pos, float4 *q, float4 *v,
-                                float4 *w, uint8_t *alive, uint8_t *asleep) {
+                                float4 *w, uint8_t *alive, uint8_t *asleep, uint8_t *dirty) {
     uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
     const float *o = in13 + (size_t)b * 13;
-    pos[b] = make_float4(o[0], o[1], o[2], 0.0f);
-    q[b] = make_float4(o[3], o[4], o[5], o[6]);
+    const float4 np = make_float4(o[0], o[1], o[2], 0.0f), nq = make_float4(o[3], o[4], o[5], o[6]);
+    const float4 op = pos[b], oq = q[b];
+    auto same = [](float x, float y) { return __float_as_uint(x) == __float_as_uint(y); };
+    const bool moved = !(same(np.x, op.x) && same(np.y, op.y) && same(np.z, op.z) && same(nq.x, oq.x) &&
+                         same(nq.y, oq.y) && same(nq.z, oq.z) && same(nq.w, oq.w));
+    dirty[b] = (moved || ((flags[b] & 1) && !alive[b])) ? 1 : 0;
+    pos[b] = np;
+    q[b] = nq;
     v[b] = make_float4(o[7], o[8], o[9], 0.0f);
     w[b] = make_float4(o[10], o[11], o[12], 0.0f);
     alive[b] = flags[b] & 1;
     asleep[b] = (flags[b] >> 1) & 1;
+}
+
+// rotation, world inverse inertia and brick positions of the dirty bodies base .. base + nb - 1 (sleeping ones too:
+// the step refreshes only awake bodies)
+__global__ void k_refresh_bodies(uint32_t nb, uint32_t base, const uint8_t *dirty, const uint8_t *alive, const float4 *q,
+                                 const float *iil, float *rot, float *iiw, const float4 *pos, const uint32_t *first,
+                                 const uint32_t *count, const float4 *local, float4 *wpos) {
+    const uint32_t lb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lb >= nb || !dirty[lb]) return;
+    const uint32_t b = base + lb;
+    if (!alive[b]) return;
+    const float4 qq = q[b];
+    float r[9], il[9], t1[9], t2[9], t3[9];
+    q_to_m(qq.x, qq.y, qq.z, qq.w, r);
+    for (int k = 0; k < 9; k++) il[k] = iil[(size_t)b * 9 + k];
+    mmul(r, il, t1);
+    mtr(r, t2);
+    mmul(t1, t2, t3);
+    for (int k = 0; k < 9; k++) { rot[(size_t)b * 9 + k] = r[k]; iiw[(size_t)b * 9 + k] = t3[k]; }
+    const float4 p = pos[b];
+    for (uint32_t t = 0; t < count[b]; t++) {
+        const uint32_t i = first[b] + t;
+        const float4 l = local[i];
+        const V3 wp = add(v3(p.x, p.y, p.z), mv(r, v3(l.x, l.y, l.z)));
+        wpos[i] = make_float4(wp.x, wp.y, wp.z, 0.0f);
+    }
 }
 
 __global__ void k_kill_marked(uint32_t nb, const uint8_t *alive, const uint32_t *first, const uint32_t *count, uint8_t *kmat) {
@@ -178,6 +211,31 @@ cudaError_t finalize_on_buffers(uint32_t ns, const uint32_t *cell, const uint32_
     if (e != cudaSuccess || ns == 0) return e;
     k_finalize_bricks<<<grid_for(ns, 256), 256, 0, s>>>(ns, 0u, cell, scene, mat, infill, sid, ctab, cpool, nb6, bond, bmax);
     return cudaGetLastError();
+}
+
+// host-written body state for bodies base .. base + nb - 1
+sf_status write_bodies_range(sf_world *w, uint32_t base, uint32_t nb, const float *state13, const float *sleep,
+                             const uint8_t *flags) {
+    if (nb == 0) return SF_OK;
+    cudaStream_t s = w->stream;
+    SF_CUDA(w->stage13.grow((size_t)nb * 13));
+    SF_CUDA(w->stage_flags.grow(nb));
+    SF_CUDA(w->stage_dirty.grow(nb));
+    SF_CUDA(cudaMemcpyAsync(w->stage13.p, state13, (size_t)nb * 13 * sizeof(float), cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemcpyAsync(w->b_sleep.p + base, sleep, nb * sizeof(float), cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemcpyAsync(w->stage_flags.p, flags, nb, cudaMemcpyHostToDevice, s));
+    k_unpack_bodies<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->stage13.p, w->stage_flags.p, w->b_pos.p + base,
+                                                      w->b_q.p + base, w->b_v.p + base, w->b_w.p + base,
+                                                      w->b_alive.p + base, w->b_asleep.p + base, w->stage_dirty.p);
+    k_refresh_bodies<<<grid_for(nb, 128), 128, 0, s>>>(nb, base, w->stage_dirty.p, w->b_alive.p, w->b_q.p, w->b_iil.p,
+                                                       w->b_rot.p, w->b_iiw.p, w->b_pos.p, w->b_first.p, w->b_count.p,
+                                                       w->k_local.p, w->k_wpos.p);
+    k_kill_marked<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p + base, w->b_first.p + base, w->b_count.p + base,
+                                                    w->k_mat.p);
+    w->launches += 3;
+    SF_CUDA(cudaGetLastError());
+    SF_CUDA(cudaStreamSynchronize(s));
+    return SF_OK;
 }
 
 sf_status read_error_word(sf_world *w) {
@@ -443,22 +501,9 @@ sf_status sf_read_bodies(sf_world *w, float *state13, float *sleep, uint8_t *fla
 
 sf_status sf_write_bodies(sf_world *w, const float *state13, const float *sleep, const uint8_t *flags) {
     if (!w || !state13 || !sleep || !flags) return SF_ERR_ARG;
-    uint32_t nb = w->nb;
-    if (nb == 0) return SF_OK;
-    cudaStream_t s = w->stream;
-    SF_CUDA(w->stage13.grow((size_t)nb * 13));
-    SF_CUDA(w->stage_flags.grow(nb));
-    SF_CUDA(cudaMemcpyAsync(w->stage13.p, state13, (size_t)nb * 13 * sizeof(float), cudaMemcpyHostToDevice, s));
-    SF_CUDA(cudaMemcpyAsync(w->b_sleep.p, sleep, nb * sizeof(float), cudaMemcpyHostToDevice, s));
-    SF_CUDA(cudaMemcpyAsync(w->stage_flags.p, flags, nb, cudaMemcpyHostToDevice, s));
-    k_unpack_bodies<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->stage13.p, w->stage_flags.p, w->b_pos.p, w->b_q.p, w->b_v.p,
-                                                      w->b_w.p, w->b_alive.p, w->b_asleep.p);
-    k_kill_marked<<<grid_for(nb, 256), 256, 0, s>>>(nb, w->b_alive.p, w->b_first.p, w->b_count.p, w->k_mat.p);
-    w->launches += 2;
+    sf_status r = write_bodies_range(w, 0, w->nb, state13, sleep, flags);
     step_mark_all_live(w);
-    SF_CUDA(cudaGetLastError());
-    SF_CUDA(cudaStreamSynchronize(s));
-    return SF_OK;
+    return r;
 }
 
 sf_status sf_read_body_setup(sf_world *w, float *body12, float *local3) {
@@ -833,6 +878,14 @@ sf_status sf_pool_restore(sf_world *w, uint32_t slot, const sf_scene_desc *d, co
     SF_CUDA(cudaStreamSynchronize(w->stream));
     step_set_live(w, slot, true);
     return SF_OK;
+}
+
+sf_status sf_pool_write_bodies(sf_world *w, uint32_t slot, const float *state13, const float *sleep, const uint8_t *flags) {
+    if (!w || w->pool.empty() || slot >= w->pool.size() || !w->pool[slot].loaded) { set_error("no scene in that slot"); return SF_ERR_ARG; }
+    if (!state13 || !sleep || !flags) { set_error("null argument"); return SF_ERR_ARG; }
+    sf_status r = write_bodies_range(w, w->scenes[slot].body_off, w->pool[slot].bodies, state13, sleep, flags);
+    step_set_live(w, slot, true);
+    return r;
 }
 
 sf_status sf_pool_read_bodies(sf_world *w, uint32_t slot, float *state13, float *sleep, uint8_t *flags) {

@@ -93,6 +93,13 @@ class ScenePool:
                                              _ptr(fl, C.c_uint8)), "sf_pool_read_bodies")
         return st, sl, fl
 
+    def write_bodies(self, slot: int, state13, sleep, flags):
+        st = np.ascontiguousarray(state13, np.float32)
+        sl = np.ascontiguousarray(sleep, np.float32)
+        fl = np.ascontiguousarray(flags, np.uint8)
+        _check(self._lib.sf_pool_write_bodies(self._h, int(slot), _ptr(st, C.c_float), _ptr(sl, C.c_float),
+                                              _ptr(fl, C.c_uint8)), "sf_pool_write_bodies")
+
     def step(self, dt: float = 1.0 / 60.0, nsteps: int = 1) -> Stats:
         _check(self._lib.sf_world_step(self._h, float(dt), int(nsteps)), "sf_world_step")
         return self.stats()
@@ -156,6 +163,14 @@ class Server:
         _check(self._lib.sf_server_add_scene(self._h, C.byref(d), C.byref(i)), "sf_server_add_scene")
         self.scenes.append(scene)
         return int(i.value)
+
+    def set_scene_state(self, scene: int, state13, sleep, flags):
+        """Body state the scene starts from at its first load (a world that has already been running)."""
+        st = np.ascontiguousarray(state13, np.float32)
+        sl = np.ascontiguousarray(sleep, np.float32)
+        fl = np.ascontiguousarray(flags, np.uint8)
+        _check(self._lib.sf_server_set_scene_state(self._h, int(scene), _ptr(st, C.c_float), _ptr(sl, C.c_float),
+                                                   _ptr(fl, C.c_uint8)), "sf_server_set_scene_state")
 
     def start(self):
         _check(self._lib.sf_server_start(self._h), "sf_server_start")

@@ -411,3 +411,37 @@ def test_sleeping_scenes_leave_the_active_set(sf, oracle):
     np.testing.assert_array_equal(sl, osl)
     np.testing.assert_array_equal(w.islands(), ow.islands())
     assert w.stats().awake < sc.n_bodies
+
+
+# ---------------------------------------------------------------- host-written state
+def test_write_back_same_state_changes_nothing(sf):
+    sc = small_debris(seed=15, n=200)
+    a, b = sf.World(sc, iterations=8), sf.World(sc, iterations=8)
+    a.step(1 / 60, nsteps=120)
+    b.step(1 / 60, nsteps=120)
+    a.set_bodies(*a.bodies())
+    a.step(1 / 60, nsteps=40)
+    b.step(1 / 60, nsteps=40)
+    for x, y in zip(a.bodies(), b.bodies()):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_write_moves_sleeping_bodies_bricks(sf):
+    """A host write that moves a sleeping body refreshes its brick positions (the step refreshes awake bodies only)."""
+    sc = small_debris(seed=16, n=120)
+    w = sf.World(sc, iterations=8)
+    w.step(1 / 60, nsteps=300)
+    st, sl, fl = w.bodies()
+    asleep = np.nonzero((fl & 3) == 3)[0]
+    assert len(asleep) > 0
+    b = int(asleep[0])
+    before = w.brick_positions()
+    st2 = st.copy()
+    st2[b, 1] += 5.0
+    w.set_bodies(st2, sl, fl)
+    after = w.brick_positions()
+    first = sc.body_first
+    mine = np.arange(first[b], first[b + 1])
+    np.testing.assert_allclose(after[mine, 1] - before[mine, 1], 5.0, atol=1e-5)
+    others = np.setdiff1d(np.arange(sc.n_body_bricks), mine)
+    np.testing.assert_array_equal(after[others], before[others])

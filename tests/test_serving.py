@@ -147,3 +147,24 @@ def test_server_budget_is_enforced(sf, sv):
     need = sv.pool_bytes([sv.slot_for(sc)] * 4)
     with pytest.raises(sf.SfError):
         sv.Server(slots=[sv.slot_for(sc)] * 4, budget_bytes=need // 2)
+
+
+def test_server_scene_initial_state_equals_alone(sf, sv):
+    """A scene registered with a running world's state is served from that state: the result equals the same steps
+    on a world given the same state."""
+    sc = scene(95, 150)
+    src = sf.World(sc, iterations=8)
+    src.step(1 / 60, nsteps=90)
+    state = src.bodies()
+    srv = sv.Server(slots=[sv.slot_for(sc)], iterations=8)
+    i = srv.add_scene(sc)
+    srv.set_scene_state(i, *state)
+    srv.start()
+    t = srv.submit_step(i, 7, want_state=True)
+    srv.drain(60000)
+    r = {x["ticket"]: x for x in srv.poll()}[t]
+    w = sf.World(sc, iterations=8)
+    w.set_bodies(*state)
+    w.step(1 / 60, nsteps=7)
+    np.testing.assert_array_equal(r["state"], w.bodies()[0])
+    srv.close()
