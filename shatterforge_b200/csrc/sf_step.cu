@@ -644,27 +644,17 @@ __device__ __forceinline__ bool jp_blocked(const JpArgs &A, uint32_t body, uint3
     return false;
 }
 
-// Once a round's worklist is short, block 0 runs the remaining rounds alone with block barriers (the other blocks
-// leave): every round still sees the colours of all earlier rounds, so the colouring is the same.
-constexpr uint32_t JP_SOLO = 4096;
 __global__ void __launch_bounds__(256) k_jp(JpArgs A) {
     const uint32_t nm = *A.nm_p;
     uint32_t r = 0;
-    bool solo = gridDim.x == 1;
     for (; r < A.max_rounds; r++) {
         const uint32_t n_in = r == 0 ? nm : __ldcg(&A.dev[DV_WL0 + (r % 3)]);
         if (n_in == 0) break;
-        if (!solo && n_in <= JP_SOLO) {
-            solo = true;
-            if (blockIdx.x != 0) return;
-        }
-        const uint32_t t0 = solo ? threadIdx.x : blockIdx.x * blockDim.x + threadIdx.x;
-        const uint32_t step = solo ? blockDim.x : gridDim.x * blockDim.x;
         const uint32_t *wl_in = (r & 1) ? A.wl1 : A.wl0;
         uint32_t *wl_out = (r & 1) ? A.wl0 : A.wl1;
         uint32_t *cnt_out = &A.dev[DV_WL0 + ((r + 1) % 3)];
         if (blockIdx.x == 0 && threadIdx.x == 0) A.dev[DV_WL0 + ((r + 2) % 3)] = 0;
-        for (uint32_t t = t0; t < n_in; t += step) {
+        for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_in; t += gridDim.x * blockDim.x) {
             const uint32_t m = r == 0 ? t : __ldcg(&wl_in[t]);
             const uint32_t a = A.man_a[m], b = A.man_b[m], pm = A.prio[m];
             bool blocked = jp_blocked(A, a, m, pm, r);
@@ -685,10 +675,7 @@ __global__ void __launch_bounds__(256) k_jp(JpArgs A) {
             atomicOr(&A.masks[(size_t)a * 4 + (c >> 5)], 1u << (c & 31));
             if (b != STATIC) atomicOr(&A.masks[(size_t)b * 4 + (c >> 5)], 1u << (c & 31));
         }
-        if (solo) {
-            __threadfence();
-            __syncthreads();
-        } else if (!grid_sync(A.gb, gridDim.x, A.err)) return;
+        if (!grid_sync(A.gb, gridDim.x, A.err)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         A.dev[DV_ROUNDS] = r;
