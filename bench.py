@@ -42,6 +42,10 @@ UNIT = "body-steps/s"
 DT = 1.0 / 60.0
 ITERS = 8
 SOLVE_BYTES_PER_CONTACT_ITER = 184     # contact 64 + impulse r/w 24 + both bodies' v, w r/w 96
+# DRAM bytes (read + write) per contact-iteration of k_solve, from one ncu capture at the peak of contacts on the
+# half-size mix (DRAM bytes of that launch / (its contacts x 8 iterations)); the roofline's `traffic` scales it to this
+# run's average launch
+SOLVE_DRAM_BYTES_PER_CONTACT_ITER = 89.7
 SOR_BYTES_PER_BRICK_SWEEP = 24         # f64 potential r/w 16 + rhs 4 + link word 4
 
 
@@ -414,7 +418,9 @@ def our_arm(args, rank, world, local, pg):
     achieved = solve_bytes / max(solve_ms * 1e-3, 1e-12) / 1e9
     roofline = {"kernel": "k_solve (coloured sequential-impulse solve, persistent)", "bound": "hbm", "achieved": achieved,
                 "peak": hbm, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback", "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None,
+                "frac": achieved / hbm,
+                "traffic": (SOLVE_DRAM_BYTES_PER_CONTACT_ITER * prof["solve_contact_iters"] / max(prof["solve_launches"], 1)
+                            if SOLVE_DRAM_BYTES_PER_CONTACT_ITER else None),
                 "bytes_per_launch": solve_bytes / max(prof["solve_launches"], 1), "ms_per_launch": per_launch_ms,
                 "unit_bytes": f"{SOLVE_BYTES_PER_CONTACT_ITER} B per contact-iteration"}
     state_after = w.bodies()
