@@ -156,11 +156,16 @@ def barrier(pg, args):
         pg.barrier()
 
 
+def _reduce_device(pg) -> str:
+    """NCCL reduces device tensors, gloo host tensors."""
+    return "cuda" if pg.get_backend() == "nccl" else "cpu"
+
+
 def allreduce_max(pg, x: float) -> float:
     if pg is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device(pg))
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
@@ -169,9 +174,21 @@ def allreduce_sum(pg, x: float) -> float:
     if pg is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device(pg))
     pg.all_reduce(t, op=pg.ReduceOp.SUM)
     return float(t.item())
+
+
+def combine(pg, ms: float, body_steps: float) -> tuple[float, float, float]:
+    """Whole-job figures of a weak-scaling run: (slowest rank's ms, all ranks' body-steps, body-steps / s of the job)."""
+    ms_max = allreduce_max(pg, ms)
+    total = allreduce_sum(pg, body_steps)
+    return ms_max, total, total / (ms_max * 1e-3)
+
+
+def rank_seed(rank: int) -> int:
+    """Each rank steps its own 256-scene mix (independent units, no data-path collective)."""
+    return 3 + 7919 * rank
 
 
 # ---------------------------------------------------------------- CPU restatement (oracle) timing
@@ -374,7 +391,7 @@ def our_arm(args, rank, world, local, pg):
     from shatterforge_b200 import scenes as S
 
     dev = torch.cuda.current_device()
-    seed = 3 + 7919 * rank
+    seed = rank_seed(rank)
     scenes = S.config4_scenes(seed=seed, n_scenes=args.scenes, scale=args.scale)
     n_bodies = sum(s.n_bodies for s in scenes)
     n_bricks = sum(s.n_body_bricks for s in scenes)
@@ -403,8 +420,7 @@ def our_arm(args, rank, world, local, pg):
     prof = w.profile()
     tuning = w.tuning()
     stats = w.stats()
-    ms_max = allreduce_max(pg, ms)
-    alive_total = allreduce_sum(pg, alive_sum)
+    ms_max, alive_total, _ = combine(pg, ms, alive_sum)
     value = alive_total / (ms_max * 1e-3)
 
     # roofline of the dominant phase
