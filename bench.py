@@ -496,8 +496,7 @@ def our_arm(args, rank, world, local, pg):
     for _ in range(e2e_steps):
         we.set_bodies(h_state, h_sleep, h_flags)
         e_alive += we.step(DT, 1).alive
-        a, b, c = we.bodies()
-        h_state[:] = a; h_sleep[:] = b; h_flags[:] = c
+        we.bodies(out=(h_state, h_sleep, h_flags))
     torch.cuda.synchronize()
     e_s = time.perf_counter() - t0
     barrier(pg, args)

@@ -146,6 +146,10 @@ sf_status sf_reset_profile(sf_world *w);
 #define SF_TUNE_COLOR 1
 #define SF_TUNE_SOR 2
 sf_status sf_read_tuning(sf_world *w, uint32_t which, int32_t *blocks_per_sm, uint32_t n);
+/* Self-check of the device-side waits (no counterpart in the reference): one kernel waits on a flag that nothing
+ * sets, through the same bounded wait the persistent kernels' grid barriers use, with a limit of limit_ms (1..2000).
+ * Returns SF_ERR_TIMEOUT when the wait gave up as it should (the context stays usable), and the device time waited. */
+sf_status sf_check_wait_timeout(uint32_t limit_ms, double *waited_ms);
 
 /* ---- hot path */
 /* nsteps world steps of dt each (dt clamped to [0, 1/30] as src/lib.rs:3642 does), all scenes at once. Scenes

@@ -136,6 +136,7 @@ PROTOTYPES = {
     "sf_read_profile": (C.c_int32, [C.c_void_p, C.POINTER(Profile)]),
     "sf_reset_profile": (C.c_int32, [C.c_void_p]),
     "sf_read_tuning": (C.c_int32, [C.c_void_p, C.c_uint32, _i32p, C.c_uint32]),
+    "sf_check_wait_timeout": (C.c_int32, [C.c_uint32, C.POINTER(C.c_double)]),
     "sf_structure_solve": (C.c_int32, [C.c_void_p, C.c_int32, C.c_float, C.c_float, C.c_uint32, C.POINTER(SolveReport)]),
     "sf_structure_check": (C.c_int32, [C.c_void_p, C.c_int32, C.c_float, C.c_int32, C.POINTER(CheckReport)]),
     "sf_read_solve_detail": (C.c_int32, [C.c_void_p, _u32p, C.POINTER(C.c_double)]),
@@ -400,11 +401,19 @@ class World:
         _check(self._lib.sf_get_stats(self._h, C.byref(s)), "sf_get_stats")
         return s
 
-    def bodies(self):
+    def bodies(self, out=None):
+        """(state13, sleep, flags); `out` = three C-contiguous arrays of those shapes and types to fill instead (e.g.
+        pinned host buffers, which the device writes directly)."""
         nb = self.info.n_bodies
-        st = np.zeros((nb, 13), np.float32)
-        sl = np.zeros(nb, np.float32)
-        fl = np.zeros(nb, np.uint8)
+        if out is not None:
+            st, sl, fl = out
+            if st.shape != (nb, 13) or st.dtype != np.float32 or sl.shape != (nb,) or sl.dtype != np.float32 or \
+                    fl.shape != (nb,) or fl.dtype != np.uint8 or not all(a.flags.c_contiguous for a in out):
+                raise ValueError("out arrays must be C-contiguous float32 [nb, 13], float32 [nb], uint8 [nb]")
+        else:
+            st = np.zeros((nb, 13), np.float32)
+            sl = np.zeros(nb, np.float32)
+            fl = np.zeros(nb, np.uint8)
         _check(self._lib.sf_read_bodies(self._h, _ptr(st, C.c_float), _ptr(sl, C.c_float), _ptr(fl, C.c_uint8)), "sf_read_bodies")
         return st, sl, fl
 
@@ -488,6 +497,13 @@ class World:
         _check(self._lib.sf_read_joints(self._h, _ptr(r, C.c_float), _ptr(b, C.c_float), _ptr(d, C.c_uint8), _ptr(k, C.c_uint32)),
                "sf_read_joints")
         return r, b, d, k
+
+
+def check_wait_timeout(limit_ms: int = 200) -> tuple[int, float]:
+    """Run the device-wait self-check: returns (status, device ms waited); SF_ERR_TIMEOUT is the expected status."""
+    ms = C.c_double()
+    st = load().sf_check_wait_timeout(int(limit_ms), C.byref(ms))
+    return int(st), float(ms.value)
 
 
 def collide_hulls(hull_data: np.ndarray, shapes_a: np.ndarray, shapes_b: np.ndarray, margin: float = 0.02,

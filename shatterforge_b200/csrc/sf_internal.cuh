@@ -297,6 +297,22 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
     return t;
 }
 constexpr unsigned long long BARRIER_LIMIT_NS = 4000000000ull;   // 4 s
+// Every device-side wait in this library: spin while *p == v for at most limit_ns of wall time (and at most 2^30
+// polls, a backstop should the clock misbehave); on running out, set ERR_TIMEOUT in *err and return false.
+__device__ __forceinline__ bool bounded_wait_while_equal(const unsigned *p, unsigned v, unsigned long long limit_ns,
+                                                         unsigned *err) {
+    const unsigned long long t0 = globaltimer_ns();
+    unsigned spins = 0;
+    while (ld_acquire_u32(p) == v) {
+        ++spins;
+        if (((spins & 255u) == 0 && globaltimer_ns() - t0 > limit_ns) || spins >= (1u << 30)) {
+            atomicOr(err, (unsigned)ERR_TIMEOUT);
+            return false;
+        }
+        __nanosleep(20);
+    }
+    return true;
+}
 __device__ __forceinline__ bool grid_sync(GridBarrier *gb, unsigned nblocks, unsigned *err) {
     __shared__ int s_ok;
     __syncthreads();
@@ -310,16 +326,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *gb, unsigned nblocks, uns
             __threadfence();
             atomicAdd(&gb->gen, 1u);
         } else {
-            unsigned long long t0 = globaltimer_ns();
-            unsigned spins = 0;
-            while (ld_acquire_u32(&gb->gen) == gen) {
-                if ((++spins & 255u) == 0 && globaltimer_ns() - t0 > BARRIER_LIMIT_NS) {
-                    atomicOr(err, (unsigned)ERR_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(20);
-            }
+            ok = bounded_wait_while_equal(&gb->gen, gen, BARRIER_LIMIT_NS, err) ? 1 : 0;
         }
         __threadfence();
         if (ld_acquire_u32(err) & ERR_TIMEOUT) ok = 0;

@@ -117,7 +117,10 @@ cudaError_t exclusive_scan_u32(const uint32_t *in, uint32_t *out, size_t n, uint
 
 // ---------------------------------------------------------------- stable LSD radix sort, 8-bit digits
 constexpr int RS_BLOCK = 256;
-constexpr int RS_ITEMS = 16;
+#ifndef SF_RS_ITEMS
+#define SF_RS_ITEMS 16   // keys per thread of a radix-sort tile (a build-time choice: registers against tiles)
+#endif
+constexpr int RS_ITEMS = SF_RS_ITEMS;
 constexpr int RS_TILE = RS_BLOCK * RS_ITEMS;
 constexpr int RS_WARPS = RS_BLOCK / 32;
 
@@ -208,9 +211,41 @@ cudaError_t radix_sort_u64(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt, u
     return cudaGetLastError();
 }
 
+// a wait on a flag that nothing sets: it must give up after its limit and report it
+__global__ void k_wait_flag(const unsigned *flag, unsigned long long limit_ns, unsigned *err) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) bounded_wait_while_equal(flag, 0u, limit_ns, err);
+}
+
 }  // namespace sf
 
 extern "C" {
+
+sf_status sf_check_wait_timeout(uint32_t limit_ms, double *waited_ms) {
+    if (limit_ms == 0 || limit_ms > 2000) { sf::set_error("limit_ms %u outside 1..2000", limit_ms); return SF_ERR_ARG; }
+    unsigned *d = nullptr;
+    if (cudaMalloc((void **)&d, 2 * sizeof(unsigned)) != cudaSuccess) { sf::set_error("cudaMalloc failed"); return SF_ERR_CUDA; }
+    unsigned err = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMemset(d, 0, 2 * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, 0);
+    if (e == cudaSuccess) {
+        sf::k_wait_flag<<<1, 32>>>(d, (unsigned long long)limit_ms * 1000000ull, d + 1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(e1, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(&err, d + 1, sizeof err, cudaMemcpyDeviceToHost);
+    float ms = 0.0f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    if (waited_ms) *waited_ms = ms;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(d);
+    if (e != cudaSuccess) { sf::set_error("%s", cudaGetErrorString(e)); return SF_ERR_CUDA; }
+    if (err & sf::ERR_TIMEOUT) { sf::set_error("the wait gave up after %.1f ms", (double)ms); return SF_ERR_TIMEOUT; }
+    return SF_OK;
+}
 const char *sf_last_error(void) { return sf::g_err; }
 int32_t sf_version(void) { return 100; }
 const char *sf_status_string(sf_status s) {

@@ -445,3 +445,15 @@ def test_write_moves_sleeping_bodies_bricks(sf):
     np.testing.assert_allclose(after[mine, 1] - before[mine, 1], 5.0, atol=1e-5)
     others = np.setdiff1d(np.arange(sc.n_body_bricks), mine)
     np.testing.assert_array_equal(after[others], before[others])
+
+
+# ---------------------------------------------------------------- failure detection without a GPU fault
+def test_bounded_wait_gives_up_and_context_stays_usable(sf):
+    """A device wait on a flag nothing sets (the grid barriers' wait) gives up after its limit with SF_ERR_TIMEOUT;
+    the next world step on the same context runs normally."""
+    st, ms = sf.check_wait_timeout(300)
+    assert st == sf.SF_ERR_TIMEOUT
+    assert 250.0 <= ms < 3000.0
+    w = sf.World(small_debris(seed=17, n=40), iterations=8)
+    w.step(1 / 60, nsteps=5)
+    assert w.stats().error_word == 0
