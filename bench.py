@@ -290,6 +290,28 @@ def _latency(res, kind=None):
             "p999_ms": float(np.percentile(lat, 99.9)), "mean_ms": float(lat.mean())}
 
 
+def colour_comparison(scenes, params):
+    """The GPU colouring's colour count beside the reference's round-based colouring (gpu/gpu_world.js:922-1038,
+    restated in the CPU oracle) on the same manifolds, 100 steps into 16 scenes of the mix (near their contact peak)."""
+    import shatterforge_b200 as sf
+    from oracle import binding as orc
+    w = sf.World(scenes, **params)
+    w.step(DT, nsteps=100)
+    ref_max, ovf, n = 0, 0, 0
+    for k, sc in enumerate(scenes):
+        m = w.manifolds(k)
+        if len(m) == 0:
+            continue
+        b = m[:, 1]
+        _, used, o = orc.ref_colouring(m[:, 0], b, np.ones(len(m), np.uint8), (b != 0xFFFFFFFF).astype(np.uint8), sc.n_bodies)
+        ref_max, ovf, n = max(ref_max, used), ovf + o, n + len(m)
+    out = {"gpu": int(w.stats().colors), "gpu_overflow": 0, "reference_algorithm": ref_max, "reference_overflow": ovf,
+           "manifolds": n, "note": "greedy colouring by priority (Jones-Plassmann rounds) vs the reference's 16 colours "
+                                   "in 2 + 4 claim rounds with an overflow pass, on the same manifolds"}
+    w.close()
+    return out
+
+
 def serve_run(args, worlds, structs, slots, batching: bool, seconds: float, seed: int, states=None):
     """One server on the population, fed a Poisson stream of `seconds` at --serve-rate; returns the summary."""
     import shatterforge_b200 as sf
@@ -551,6 +573,7 @@ def our_arm(args, rank, world, local, pg):
                "sample": f"1 scene ({one[0].n_bodies} bodies), steps {args.warmup}..{args.warmup + n1} from rest",
                "all_cores": {"value": rate_n, "cores": min(threads, len(many)),
                              "sample": f"{len(many)} scenes of the lower half of the sizes, one per thread, {n_n} timed steps in all"}}
+        cpu["colours"] = colour_comparison(scenes[:16], params)
 
     if rank != 0:
         return

@@ -78,6 +78,8 @@ def load() -> C.CDLL:
     lib.ow_get_ext.argtypes = [C.c_void_p, _f32p]
     lib.ow_collide_hulls.restype = C.c_int32
     lib.ow_collide_hulls.argtypes = [_f32p, _f32p, _f32p, C.c_float, C.c_int32, _f32p]
+    lib.ow_ref_colouring.argtypes = [C.c_uint32, _u32p, _u32p, _u32p, _u8p, _u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                     _u32p, _u32p]
     lib.ow_collide_boxes.restype = C.c_int32
     lib.ow_collide_boxes.argtypes = [_f32p, _f32p, C.c_float, C.c_int32, _f32p]
     _lib = lib
@@ -234,3 +236,24 @@ def collide_boxes(a, b, margin=0.02, reduce=True):
     a = np.ascontiguousarray(a, np.float32); b = np.ascontiguousarray(b, np.float32)
     n = lib.ow_collide_boxes(_p(a, C.c_float), _p(b, C.c_float), float(margin), 1 if reduce else 0, _p(out, C.c_float))
     return n, out[:3].copy(), out[3:3 + 4 * n].reshape(n, 4).copy()
+
+
+def ref_colouring(a, b, a_awake, b_awake, n_bodies, color_limit=16, rounds_s=2, rounds_a=4):
+    """The reference's round-based manifold colouring (gpu/gpu_world.js:922-1038) on a manifold graph; returns
+    (colour per manifold, colours used, overflow manifolds). b = 0xFFFFFFFF marks the static side."""
+    lib = load()
+    a = np.ascontiguousarray(a, np.uint32); b = np.ascontiguousarray(b, np.uint32)
+    aa = np.ascontiguousarray(a_awake, np.uint8); bb = np.ascontiguousarray(b_awake, np.uint8)
+    # salt = the manifold's index among the manifolds of the same body pair (chunks of one pair)
+    pair = a.astype(np.uint64) << np.uint64(32) | b.astype(np.uint64)
+    order = np.argsort(pair, kind="stable")
+    sp = pair[order]
+    start = np.r_[0, np.nonzero(sp[1:] != sp[:-1])[0] + 1]
+    run = np.repeat(start, np.diff(np.r_[start, len(sp)]))
+    salt = np.zeros(len(a), np.uint32)
+    salt[order] = (np.arange(len(sp)) - run).astype(np.uint32)
+    col = np.zeros(len(a), np.uint32)
+    st = np.zeros(2, np.uint32)
+    lib.ow_ref_colouring(len(a), _p(a, C.c_uint32), _p(b, C.c_uint32), _p(salt, C.c_uint32), _p(aa, C.c_uint8), _p(bb, C.c_uint8), int(n_bodies),
+                         int(color_limit), int(rounds_s), int(rounds_a), _p(col, C.c_uint32), _p(st, C.c_uint32))
+    return col, int(st[0]), int(st[1])

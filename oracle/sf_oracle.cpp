@@ -1335,4 +1335,107 @@ int32_t ow_collide_boxes(const float* A, const float* B, float margin, int32_t d
     return cnt;
 }
 
+
+// The reference's manifold colouring (gpu/gpu_world.js:922-1038, rounds scheduled at :2576-2577), restated on a
+// manifold graph given as endpoint pairs: each round every uncoloured manifold picks one of the four lowest colours
+// free at both its awake bodies (by its key and its own round), claims it at each with its priority (supports, i.e.
+// manifolds with a static or sleeping side, first; then by key), breaks priority ties with a second hash, and keeps
+// the colour where its claim is the strongest at both bodies. The first rounds_s rounds let only supports claim.
+// What is uncoloured after rounds_s + rounds_a rounds, or finds no free colour, goes to the overflow pass
+// (colour = color_limit). Shape ids for the keys are (a + 1 + salt * 2^20, b + 1) with b = 0 for the static side;
+// the salt (the chunk's index within its body pair) keeps the keys of one pair's chunks distinct, as the reference's
+// shape pairs are. Stats out: [0] colours used (highest colour + 1 among coloured), [1] overflow manifolds.
+static uint32_t ref_mkey(uint32_t sa, uint32_t sb) {   // gpu/gpu_world.js:245-250
+    uint32_t h = (sa * 0x9E3779B1u) ^ ((sb + 0x7F4A7C15u) * 0x85EBCA77u);
+    h ^= h >> 15; h *= 0x2C1B3C6Du; h ^= h >> 12;
+    return h | 1u;
+}
+static uint32_t ref_mkey2(uint32_t sa, uint32_t sb) {  // gpu/gpu_world.js:979-984
+    uint32_t h = (sb * 0x2545F491u) ^ ((sa + 0x68E31DA4u) * 0xB5297A4Du);
+    h ^= h >> 13; h *= 0x1B873593u; h ^= h >> 16;
+    return h;
+}
+
+void ow_ref_colouring(uint32_t n, const uint32_t* a, const uint32_t* b, const uint32_t* salt, const uint8_t* a_awake,
+                      const uint8_t* b_awake, uint32_t n_bodies, uint32_t color_limit, uint32_t rounds_s, uint32_t rounds_a, uint32_t* colour,
+                      uint32_t* stats) {
+    const uint32_t UNC = 0xfffffffeu, COL_ROUNDS = 12;
+    if (color_limit > 31) color_limit = 31;
+    std::vector<uint32_t> mask(n_bodies, 0), claim((size_t)n_bodies * 32, 0), claim2((size_t)n_bodies * 32, 0);
+    std::vector<uint32_t> mtry(n, 0), key(n), key2(n), pri(n);
+    for (uint32_t m = 0; m < n; m++) {
+        colour[m] = UNC;
+        const uint32_t sa = a[m] + 1 + (salt ? salt[m] << 20 : 0u), sb = b[m] == 0xFFFFFFFFu ? 0u : b[m] + 1;
+        key[m] = ref_mkey(sa, sb);
+        key2[m] = ref_mkey2(sa, sb);
+        const bool support = !a_awake[m] || !b_awake[m];
+        pri[m] = (support ? 0u : 0x2000000u) | (key[m] >> 7);
+    }
+    const uint32_t all = color_limit >= 32 ? 0xffffffffu : ((1u << color_limit) - 1u);
+    uint32_t gr = 0;
+    for (uint32_t r = 0; r < rounds_s + rounds_a; r++) {
+        const bool support_only = r < rounds_s;
+        // claim
+        for (uint32_t m = 0; m < n; m++) {
+            if (colour[m] != UNC) continue;
+            const bool da = a_awake[m], db = b_awake[m];
+            if (support_only && da && db) continue;
+            const uint32_t round = mtry[m] & 0xffffu;
+            uint32_t used = 0;
+            if (da) used |= mask[a[m]];
+            if (db) used |= mask[b[m]];
+            uint32_t free = all & ~used;
+            if (free == 0 || round >= COL_ROUNDS) { colour[m] = color_limit; continue; }
+            const uint32_t nf = (uint32_t)__builtin_popcount(free);
+            const uint32_t pick = ((key[m] >> 3) + round * 0x9E37u) % (nf < 4 ? nf : 4);
+            for (uint32_t k = 0; k < pick; k++) free &= free - 1;
+            const uint32_t c = (uint32_t)__builtin_ctz(free);
+            const uint32_t v = ((gr + 1) << 27) | (0x3ffffffu - pri[m]);
+            if (da) claim[(size_t)a[m] * 32 + c] = std::max(claim[(size_t)a[m] * 32 + c], v);
+            if (db) claim[(size_t)b[m] * 32 + c] = std::max(claim[(size_t)b[m] * 32 + c], v);
+            mtry[m] = (round + 1) | (c << 16) | 0x80000000u;
+        }
+        const uint32_t tag = (gr + 1) << 27;
+        auto claimed = [&](uint32_t m, bool stage2) {
+            const uint32_t c = (mtry[m] >> 16) & 0x7fffu;
+            const bool da = a_awake[m], db = b_awake[m];
+            const uint32_t v = tag | (0x3ffffffu - pri[m]);
+            if (da && claim[(size_t)a[m] * 32 + c] != v) return false;
+            if (db && claim[(size_t)b[m] * 32 + c] != v) return false;
+            const uint32_t v2 = tag | (key2[m] >> 5);
+            if (!stage2) {
+                if (da) claim2[(size_t)a[m] * 32 + c] = std::max(claim2[(size_t)a[m] * 32 + c], v2);
+                if (db) claim2[(size_t)b[m] * 32 + c] = std::max(claim2[(size_t)b[m] * 32 + c], v2);
+                return true;
+            }
+            if (da && claim2[(size_t)a[m] * 32 + c] != v2) return false;
+            if (db && claim2[(size_t)b[m] * 32 + c] != v2) return false;
+            return true;
+        };
+        // tie
+        for (uint32_t m = 0; m < n; m++)
+            if (colour[m] == UNC && (mtry[m] & 0x80000000u)) claimed(m, false);
+        // resolve
+        for (uint32_t m = 0; m < n; m++) {
+            if (colour[m] != UNC || !(mtry[m] & 0x80000000u)) continue;
+            const bool won = claimed(m, true);
+            mtry[m] &= 0x7fffffffu;
+            if (!won) continue;
+            const uint32_t c = (mtry[m] >> 16) & 0x7fffu;
+            colour[m] = c;
+            if (a_awake[m]) mask[a[m]] |= 1u << c;
+            if (b_awake[m]) mask[b[m]] |= 1u << c;
+        }
+        gr++;
+    }
+    uint32_t used = 0, ovf = 0;
+    for (uint32_t m = 0; m < n; m++) {
+        if (colour[m] == UNC) colour[m] = color_limit;
+        if (colour[m] >= color_limit) ovf++;
+        else used = std::max(used, colour[m] + 1);
+    }
+    stats[0] = used;
+    stats[1] = ovf;
+}
+
 }  // extern "C"

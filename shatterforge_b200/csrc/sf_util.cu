@@ -118,7 +118,7 @@ cudaError_t exclusive_scan_u32(const uint32_t *in, uint32_t *out, size_t n, uint
 // ---------------------------------------------------------------- stable LSD radix sort, 8-bit digits
 constexpr int RS_BLOCK = 256;
 #ifndef SF_RS_ITEMS
-#define SF_RS_ITEMS 16   // keys per thread of a radix-sort tile (a build-time choice: registers against tiles)
+#define SF_RS_ITEMS 8    // keys per thread of a radix-sort tile (a build-time choice: registers against tiles)
 #endif
 constexpr int RS_ITEMS = SF_RS_ITEMS;
 constexpr int RS_TILE = RS_BLOCK * RS_ITEMS;

@@ -151,3 +151,35 @@ def test_box_sat_edge_contact(oracle):
     assert n == 1
     assert nrm[1] > 0.99
     assert pts[0, 3] < 0
+
+
+def _proper(a, b, col, limit):
+    seen = set()
+    for x, y, c in zip(a, b, col):
+        if c >= limit:
+            continue
+        for body in (x, y):
+            if body == 0xFFFFFFFF:
+                continue
+            assert (body, c) not in seen
+            seen.add((body, c))
+
+
+def test_reference_colouring_restatement(oracle):
+    """gpu/gpu_world.js:922-1038 restated: a proper colouring of the coloured manifolds; supports (a static side)
+    claim in the first rounds; a body with more manifolds than colours sends the rest to the overflow pass."""
+    rng = np.random.default_rng(3)
+    n_bodies = 300
+    a = rng.integers(0, n_bodies, 1500).astype(np.uint32)
+    b = rng.integers(0, n_bodies, 1500).astype(np.uint32)
+    b[b == a] = (b[b == a] + 1) % n_bodies
+    b[rng.random(1500) < 0.3] = 0xFFFFFFFF
+    col, used, ovf = oracle.ref_colouring(a, b, np.ones(1500, np.uint8), (b != 0xFFFFFFFF).astype(np.uint8), n_bodies)
+    _proper(a, b, col, 16)
+    assert used <= 16 and ovf == int((col >= 16).sum())
+    # a star of 20 awake manifolds at body 0 with 4 colours: at most 4 coloured
+    a2 = np.zeros(20, np.uint32)
+    b2 = np.arange(1, 21, dtype=np.uint32)
+    col2, used2, ovf2 = oracle.ref_colouring(a2, b2, np.ones(20, np.uint8), np.ones(20, np.uint8), 21, color_limit=4)
+    _proper(a2, b2, col2, 4)
+    assert used2 <= 4 and ovf2 >= 16
