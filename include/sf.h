@@ -78,7 +78,10 @@ typedef struct sf_params {
     uint32_t manifold_chunk;    /* a body pair's contacts are solved in chunks of at most this many, 1..32 (0 or more
                                    than 32 mean 32); chunks of one pair take different colours, bounding each
                                    colour's longest chain and the contact layout's depth */
-    uint32_t reserved[7];
+    uint32_t sor_cluster;       /* 1: a structure of at most 65,536 bricks is solved by one thread-block cluster that
+                                   keeps its cells in shared memory (same potentials and sweeps); 0: always the
+                                   grid-wide kernel */
+    uint32_t reserved[6];
 } sf_params;
 
 typedef struct sf_stats {
@@ -94,6 +97,7 @@ typedef struct sf_stats {
     double ms_last_step;        /* device time of the last sf_world_step call (CUDA events) */
     uint64_t launches;          /* kernels this world has launched (all entry points) */
     uint64_t graph_launches;    /* load-path solves replayed from a captured CUDA graph */
+    uint64_t cluster_solves;    /* load-path solves run by one thread-block cluster per structure */
 } sf_stats;
 
 /* Per-phase device time of the rigid step, from CUDA events around each phase of each substep (profiling on). */

@@ -54,14 +54,15 @@ class Params(C.Structure):
     _fields_ = [("substeps", C.c_uint32), ("iterations", C.c_uint32), ("sleep_mode", C.c_uint32),
                 ("pinch_kill", C.c_uint32), ("max_colors", C.c_uint32), ("contact_capacity", C.c_uint32),
                 ("verify", C.c_uint32), ("solve_blocks", C.c_uint32), ("manifold_chunk", C.c_uint32),
-                ("reserved", C.c_uint32 * 7)]
+                ("sor_cluster", C.c_uint32), ("reserved", C.c_uint32 * 6)]
 
 
 class Stats(C.Structure):
     _fields_ = [("contacts", C.c_uint64), ("manifolds", C.c_uint64), ("ref_would_drop", C.c_uint64),
                 ("colors", C.c_uint32), ("color_rounds", C.c_uint32), ("islands", C.c_uint32), ("alive", C.c_uint32),
                 ("awake", C.c_uint32), ("error_word", C.c_uint32), ("contact_capacity", C.c_uint64),
-                ("ms_last_step", C.c_double), ("launches", C.c_uint64), ("graph_launches", C.c_uint64)]
+                ("ms_last_step", C.c_double), ("launches", C.c_uint64), ("graph_launches", C.c_uint64),
+                ("cluster_solves", C.c_uint64)]
 
 
 SF_PHASES = 9

@@ -21,6 +21,8 @@
 #include <algorithm>
 #include <cstring>
 
+#include <cooperative_groups.h>
+
 #include "sf_internal.cuh"
 
 namespace sf {
@@ -59,7 +61,13 @@ struct SorState {
     Tuner tune;   // blocks per SM of the red-black kernel, keyed on log2(chunks of the solve)
     // The solve's launch sequence captured in CUDA graphs, one per launch shape (the chunk list and the active
     // flags live in device buffers the graph reads, so a graph serves every solve of its shape).
-    struct Graph { uint32_t n_work, grid; cudaGraphExec_t exec; };
+    struct Graph { uint32_t n_work, grid, mode; cudaGraphExec_t exec; };
+    // the cluster path: one thread-block cluster per structure, the structure's cells in the cluster's shared memory
+    bool cl_ready = false;
+    std::vector<uint32_t> h_cl_n, h_cl_per;
+    DBuf<uint32_t> cl_cpos, cl_off, cl_n, cl_per, cl_even, cl_list;
+    DBuf<uint16_t> cl_nbr;
+    uint64_t cluster_solves = 0;
     DBuf<SorParams> prm;
     std::vector<Graph> graphs;
     bool graphs_ok = true;
@@ -299,6 +307,159 @@ __global__ void __launch_bounds__(SOR_BLOCK) k_sor_redblack(SorArgs A) {
         __syncthreads();
         if (!s_any) break;
     }
+}
+
+// ---------------------------------------------------------------- one cluster per structure
+// A structure of up to SOR_CL x SOR_CL_CAP bricks is solved by one cluster of SOR_CL blocks that hold its cells in
+// shared memory for the whole solve: cells listed in space order, split in SOR_CL contiguous ranges (one per
+// block), each range with its even-parity cells first. A half-sweep updates one parity; a neighbour in another block
+// of the cluster is read from that block's shared memory; a cluster barrier (hardware, no spin) separates the
+// halves, and the one that ends a sweep also publishes each block's residual maxima (two barriers per sweep). The
+// largest structures' clusters are listed first. Each update is the grid kernel's arithmetic on the same values in the same order, and the residual and
+// stopping rule are the same, so the potentials and sweep counts are identical to the grid kernel's.
+constexpr int SOR_CL = 8;
+constexpr int SOR_CL_MAX_THREADS = 1024;         // threads per block: 256, 512 or 1024, picked per launch
+constexpr uint32_t SOR_CL_CAP = 8192;            // cells per block: 28 B each (phi 8, rhs 4, code 4, 6 neighbours 12)
+constexpr uint32_t SOR_CL_BYTES_PER_CELL = 28;
+constexpr uint32_t CELL_ACTIVE = 1u << 31;
+constexpr uint16_t NO_CELL = 0xFFFFu;
+
+struct SorClusterArgs {
+    const uint32_t *list;                        // the structure of each cluster
+    const uint32_t *off, *n, *per, *even;        // per structure; even: per (structure, block)
+    const uint32_t *cpos;                        // per listed cell: its place in the chunk layout
+    const uint16_t *nbr;                         // per listed cell: 6 neighbours as block rank << 13 | index in block
+    double *cphi;
+    const float *crhs;
+    const uint32_t *ccode;
+    const int32_t *csid;
+    uint32_t per_max;
+    const SorParams *prm;
+    uint32_t *sweeps;
+    double *resid;
+    uint32_t *err;
+};
+
+// threads per block for a launch whose largest block range holds per_max cells: about two cells per thread and sweep
+static unsigned sor_cl_threads(uint32_t per_max) {
+    const uint32_t half = per_max / 2;
+    return half > 512 ? 1024u : half > 256 ? 512u : 256u;
+}
+
+__global__ void __launch_bounds__(SOR_CL_MAX_THREADS) k_sor_cluster(SorClusterArgs A) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char sm[];
+    const uint32_t P = A.per_max;
+    double *phi = (double *)sm;
+    float *rhs = (float *)(phi + P);
+    uint32_t *code = (uint32_t *)(rhs + P);
+    uint16_t *nbr = (uint16_t *)(code + P);
+    // this block's maxima of sweep s in slot s & 1, published before the barrier that ends the sweep; after it,
+    // thread 0 of every block reads all SOR_CL blocks' slots and takes the stop decision (the same in every block)
+    __shared__ unsigned long long blk_d[2], blk_p[2];
+    __shared__ unsigned long long wd[SOR_CL_MAX_THREADS / 32], wp[SOR_CL_MAX_THREADS / 32];
+    __shared__ int s_stop;
+    // conductances as f64: kt[2 lm + (axis is y)] = STIFF[lm] x axis factor (the f32 product, promoted), kt[32 + m]
+    // = the foundation conductance of material m
+    __shared__ double kt[48];
+    for (uint32_t k = threadIdx.x; k < 16; k += blockDim.x) {
+        const float st = k < 9 ? c_mat.stiff[k] : 0.0f;
+        kt[2 * k] = (double)(st * 0.3f);
+        kt[2 * k + 1] = (double)(st * 1.0f);
+        kt[32 + k] = k < 9 ? (double)c_mat.gk[k] : 0.0;
+    }
+    const unsigned long long one = (unsigned long long)__double_as_longlong(1.0);
+    const uint32_t rank = cl.block_rank(), tid = threadIdx.x;
+    const uint32_t q = A.list[blockIdx.x / SOR_CL];
+    const uint32_t off = A.off[q], n = A.n[q], per = A.per[q];
+    const uint32_t b0 = min(n, rank * per), b1 = min(n, b0 + per), my = b1 - b0;
+    const uint32_t ev = A.even[q * SOR_CL + rank];
+    for (uint32_t i = tid; i < my; i += blockDim.x) {
+        const uint32_t g = off + b0 + i;
+        const uint32_t at = A.cpos[g];
+        phi[i] = A.cphi[at];
+        rhs[i] = A.crhs[at];
+        code[i] = A.csid[at] == (int32_t)q ? (A.ccode[at] | CELL_ACTIVE) : 0u;
+#pragma unroll
+        for (int d = 0; d < 6; d++) nbr[i * 6 + d] = A.nbr[(size_t)g * 6 + d];
+    }
+    const double omega = A.prm->omega, tol = A.prm->tol;
+    const uint32_t max_sweeps = A.prm->max_sweeps;
+    double r_last = 0.0;
+    uint32_t done = 0;
+    cl.sync();
+    for (uint32_t sweep = 0; sweep < max_sweeps; sweep++) {
+        unsigned long long accd = 0ull, accp = 0ull;
+        for (int colour = 0; colour < 2; colour++) {
+            const uint32_t c0 = colour ? ev : 0u, c1 = colour ? my : ev;
+            for (uint32_t i = c0 + tid; i < c1; i += blockDim.x) {
+                const uint32_t cd = code[i];
+                if (!(cd & CELL_ACTIVE)) continue;
+                double sk = 0.0, skp = 0.0;
+#pragma unroll
+                for (int d = 0; d < 6; d++) {
+                    const uint32_t lm = (cd >> (4 * d)) & 15u;
+                    if (lm == 0) continue;
+                    const uint32_t g = nbr[i * 6 + d];
+                    if (g == NO_CELL) { atomicOr(A.err, (unsigned)ERR_SOR_NONFINITE); continue; }
+                    const uint32_t r = g >> 13, l = g & 8191u;
+                    const double pj = r == rank ? phi[l] : cl.map_shared_rank(phi, r)[l];
+                    const double k = kt[2 * lm + ((d >> 1) == 1 ? 1 : 0)];
+                    sk += k;
+                    skp += k * pj;
+                }
+                if (cd & (1u << 28)) sk += kt[32 + ((cd >> 24) & 15u)];
+                double p = phi[i];
+                double dabs = 0.0;
+                if (sk > 0.0) {
+                    const double target = ((double)rhs[i] + skp) / sk;
+                    const double dd = omega * (target - p);
+                    p += dd;
+                    phi[i] = p;
+                    dabs = fabs(dd);
+                    if (!isfinite(p)) atomicOr(A.err, (unsigned)ERR_SOR_NONFINITE);
+                }
+                accd = max(accd, (unsigned long long)__double_as_longlong(dabs));
+                if (p > 0.0) accp = max(accp, (unsigned long long)__double_as_longlong(p));
+            }
+            if (colour == 0) cl.sync();
+        }
+        // the cluster's maxima of this sweep. Slot sweep & 1 is next written two sweeps later, after the next
+        // sweep's first barrier, which no block passes before it has read the slot.
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            accd = max(accd, __shfl_xor_sync(0xffffffffu, accd, o));
+            accp = max(accp, __shfl_xor_sync(0xffffffffu, accp, o));
+        }
+        if ((tid & 31) == 0) { wd[tid >> 5] = accd; wp[tid >> 5] = accp; }
+        __syncthreads();
+        const uint32_t slot = sweep & 1u;
+        if (tid == 0) {
+            unsigned long long dm = 0ull, pm = one;
+            for (uint32_t k = 0; k < blockDim.x / 32; k++) { dm = max(dm, wd[k]); pm = max(pm, wp[k]); }
+            blk_d[slot] = dm;
+            blk_p[slot] = pm;
+        }
+        cl.sync();
+        if (tid == 0) {
+            unsigned long long dm = 0ull, pm = one;
+#pragma unroll
+            for (uint32_t b = 0; b < (uint32_t)SOR_CL; b++) {
+                dm = max(dm, cl.map_shared_rank(blk_d, b)[slot]);
+                pm = max(pm, cl.map_shared_rank(blk_p, b)[slot]);
+            }
+            r_last = __longlong_as_double((long long)dm) / __longlong_as_double((long long)pm);
+            s_stop = (r_last < tol || sweep + 1 >= max_sweeps) ? 1 : 0;
+        }
+        done = sweep + 1;
+        __syncthreads();
+        if (s_stop) break;
+    }
+    for (uint32_t i = tid; i < my; i += blockDim.x)
+        if (code[i] & CELL_ACTIVE) A.cphi[A.cpos[off + b0 + i]] = phi[i];
+    if (rank == 0 && tid == 0 && done) { A.sweeps[q] = done; A.resid[q] = r_last; }
+    cl.sync();   // every block's shared memory outlives the other blocks' reads of it
 }
 
 // ---------------------------------------------------------------- joint checks
@@ -714,6 +875,102 @@ static sf_status sor_select_set(sf_world *w, const int32_t *ids, uint32_t n, std
     return SF_OK;
 }
 
+// The cluster path's tables, built on its first use: each structure's bricks in lattice order (chunk slot, cell in
+// chunk), cut into SOR_CL ranges with each range's even-parity cells first; every listed cell's place in the chunk
+// layout and its six neighbours' indices in the list (NO_CELL for none, or a brick of another structure). A structure
+// with more than 65,535 bricks takes the grid kernel.
+static sf_status sor_cluster_tables(sf_world *w) {
+    SorState *st = w->sor;
+    const uint32_t nst = w->n_struct, ns = w->ns;
+    std::vector<uint32_t> h_ctab((size_t)w->n_scenes * NCT), h_cpool((size_t)std::max<uint32_t>(w->n_chunks, 1) * 512);
+    SF_CUDA(cudaStreamSynchronize(w->stream));
+    SF_CUDA(cudaMemcpy(h_ctab.data(), w->ctab.p, h_ctab.size() * 4, cudaMemcpyDeviceToHost));
+    if (w->n_chunks) SF_CUDA(cudaMemcpy(h_cpool.data(), w->cpool.p, (size_t)w->n_chunks * 512 * 4, cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> scene_of(ns, 0);
+    for (uint32_t q = 0; q < w->n_scenes; q++)
+        for (uint32_t i = 0; i < w->scenes[q].n_static; i++) scene_of[w->scenes[q].static_off + i] = q;
+    std::vector<std::vector<uint32_t>> bricks(nst);
+    for (uint32_t i = 0; i < ns; i++) if (w->h_sid[i] >= 0) bricks[w->h_sid[i]].push_back(i);
+    auto key = [&](uint32_t i) {
+        int x, y, z;
+        unpack_cell(w->h_s_cell[i], x, y, z);
+        return (uint64_t)chunk_slot(x, y, z) * 512 + cell_in_chunk(x, y, z);
+    };
+    auto cpos_of = [&](uint32_t sc, int x, int y, int z) -> uint32_t {   // (chunk << 9 | cell) or NONE
+        if (!inb(x, y, z)) return NONE;
+        const uint32_t t = h_ctab[(size_t)sc * NCT + chunk_slot(x, y, z)];
+        return t ? ((t - 1) << 9) | cell_in_chunk(x, y, z) : NONE;
+    };
+    std::vector<uint32_t> idx(ns, NONE), cpos, even(std::max<size_t>((size_t)nst * SOR_CL, 1), 0);
+    std::vector<uint16_t> nbr;
+    st->h_cl_n.assign(nst, 0);
+    st->h_cl_per.assign(nst, 0);
+    std::vector<uint32_t> off(std::max<uint32_t>(nst, 1), 0), cnt(std::max<uint32_t>(nst, 1), 0), per(std::max<uint32_t>(nst, 1), 0);
+    const int D[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    for (uint32_t q = 0; q < nst; q++) {
+        // links join bricks of one structure only (a bond needs equal structure ids), so every link of a listed
+        // cell ends at a listed cell
+        std::vector<uint32_t> &b = bricks[q];
+        if (b.empty() || b.size() >= NO_CELL) continue;
+        std::sort(b.begin(), b.end(), [&](uint32_t u, uint32_t v) { return key(u) < key(v); });
+        const uint32_t n = (uint32_t)b.size(), pr = (n + SOR_CL - 1) / SOR_CL;
+        for (uint32_t r = 0; r < SOR_CL; r++) {
+            auto lo = b.begin() + std::min(n, r * pr), hi = b.begin() + std::min(n, (r + 1) * pr);
+            auto mid = std::stable_partition(lo, hi, [&](uint32_t i) {
+                int x, y, z;
+                unpack_cell(w->h_s_cell[i], x, y, z);
+                return ((x + y + z) & 1) == 0;
+            });
+            even[(size_t)q * SOR_CL + r] = (uint32_t)(mid - lo);
+        }
+        off[q] = (uint32_t)cpos.size();
+        cnt[q] = n;
+        per[q] = pr;
+        for (uint32_t k = 0; k < n; k++) idx[b[k]] = k;
+        for (uint32_t k = 0; k < n; k++) {
+            const uint32_t i = b[k], sc = scene_of[i];
+            int x, y, z;
+            unpack_cell(w->h_s_cell[i], x, y, z);
+            cpos.push_back(cpos_of(sc, x, y, z));
+            for (int d = 0; d < 6; d++) {
+                const uint32_t c = cpos_of(sc, x + D[d][0], y + D[d][1], z + D[d][2]);
+                uint16_t g = NO_CELL;
+                if (c != NONE) {
+                    const uint32_t j1 = h_cpool[(size_t)(c >> 9) * 512 + (c & 511)];
+                    if (j1 && w->h_sid[j1 - 1] == (int32_t)q) {
+                        const uint32_t t = idx[j1 - 1];
+                        g = (uint16_t)(((t / pr) << 13) | (t % pr));   // pr <= 8192: the index fits 13 bits
+                    }
+                }
+                nbr.push_back(g);
+            }
+        }
+        st->h_cl_n[q] = n;
+        st->h_cl_per[q] = pr;
+    }
+    // places in the chunk layout as chunk * 512 + cell
+    for (uint32_t &c : cpos) c = (c >> 9) * 512 + (c & 511);
+    cudaStream_t s = w->stream;
+    auto up32 = [&](DBuf<uint32_t> &d, const std::vector<uint32_t> &h) -> cudaError_t {
+        cudaError_t e = d.alloc(std::max<size_t>(h.size(), 1));
+        if (e == cudaSuccess && !h.empty()) e = cudaMemcpyAsync(d.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice, s);
+        return e;
+    };
+    SF_CUDA(up32(st->cl_cpos, cpos));
+    SF_CUDA(up32(st->cl_off, off));
+    SF_CUDA(up32(st->cl_n, cnt));
+    SF_CUDA(up32(st->cl_per, per));
+    SF_CUDA(up32(st->cl_even, even));
+    SF_CUDA(st->cl_list.alloc(std::max<uint32_t>(nst, 1)));
+    SF_CUDA(st->cl_nbr.alloc(std::max<size_t>(nbr.size(), 1)));
+    if (!nbr.empty()) SF_CUDA(cudaMemcpyAsync(st->cl_nbr.p, nbr.data(), nbr.size() * 2, cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(SOR_CL_CAP * SOR_CL_BYTES_PER_CELL)));
+    SF_CUDA(cudaStreamSynchronize(s));
+    st->cl_ready = true;
+    return SF_OK;
+}
+
 static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, uint32_t n_ids, float omega, float tol,
                             uint32_t max_sweeps, sf_solve_report *report) {
     if (!w) return SF_ERR_ARG;
@@ -727,8 +984,24 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     if (chunks.empty() || max_sweeps == 0) { if (report) *report = rep; return SF_OK; }
     cudaStream_t s = w->stream;
     uint32_t nst = w->n_struct;
+    // the cluster path when every requested structure fits one cluster's shared memory
+    bool use_cl = w->P.sor_cluster != 0;
+    if (use_cl && !st->cl_ready) { sf_status e = sor_cluster_tables(w); if (e != SF_OK) return e; }
+    uint32_t per_max = 0;
+    for (uint32_t q : req) {
+        if (!use_cl) break;
+        if (st->h_cl_n[q] == 0 || st->h_cl_per[q] > SOR_CL_CAP) use_cl = false;
+        per_max = std::max(per_max, st->h_cl_per[q]);
+    }
     SF_CUDA(cudaMemcpyAsync(st->active0.p, act.data(), nst * 4, cudaMemcpyHostToDevice, s));
-    SF_CUDA(cudaMemcpyAsync(st->work.p, chunks.data(), chunks.size() * 4, cudaMemcpyHostToDevice, s));
+    std::vector<uint32_t> cl_order;
+    if (use_cl) {
+        // largest structures first: their clusters start before the small ones when not all fit at once
+        cl_order = req;
+        std::stable_sort(cl_order.begin(), cl_order.end(), [&](uint32_t a, uint32_t b) { return st->h_cl_n[a] > st->h_cl_n[b]; });
+        SF_CUDA(cudaMemcpyAsync(st->cl_list.p, cl_order.data(), cl_order.size() * 4, cudaMemcpyHostToDevice, s));
+    }
+    else SF_CUDA(cudaMemcpyAsync(st->work.p, chunks.data(), chunks.size() * 4, cudaMemcpyHostToDevice, s));
     SF_CUDA(cudaEventRecord(w->ev0, s));
     size_t ncell = (size_t)w->n_chunks * 512;
     st->launches += 5;   // clear, scatter, init, red-black, gather
@@ -742,9 +1015,26 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     SF_CUDA(cudaMemcpyAsync(st->prm.p, &hp, sizeof hp, cudaMemcpyHostToDevice, s));
     int tci = -1;
     const int tb = Tuner::bucket(chunks.size());
-    const unsigned per_sm = (unsigned)st->tune.choose(tb, tci);
-    unsigned grid = (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * per_sm);
+    const unsigned per_sm = use_cl ? 1u : (unsigned)st->tune.choose(tb, tci);
+    if (use_cl) tci = -1;
+    unsigned grid = use_cl ? per_max : (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * per_sm);
+    const uint32_t n_launch = use_cl ? (uint32_t)req.size() : A.n_work;
     void *args[] = {&A};
+    SorClusterArgs CA;
+    CA.list = st->cl_list.p; CA.off = st->cl_off.p; CA.n = st->cl_n.p; CA.per = st->cl_per.p; CA.even = st->cl_even.p;
+    CA.cpos = st->cl_cpos.p; CA.nbr = st->cl_nbr.p; CA.cphi = st->cphi.p; CA.crhs = st->crhs.p; CA.ccode = st->ccode.p;
+    CA.csid = st->csid.p; CA.per_max = per_max; CA.prm = st->prm.p; CA.sweeps = st->sweeps.p; CA.resid = st->resid.p;
+    CA.err = w->err.p;
+    cudaLaunchConfig_t ccfg = {};
+    cudaLaunchAttribute cattr[1];
+    ccfg.gridDim = dim3((unsigned)(req.size() * SOR_CL));
+    ccfg.blockDim = dim3(sor_cl_threads(per_max));
+    ccfg.dynamicSmemBytes = (size_t)per_max * SOR_CL_BYTES_PER_CELL;
+    ccfg.stream = s;
+    cattr[0].id = cudaLaunchAttributeClusterDimension;
+    cattr[0].val.clusterDim.x = SOR_CL; cattr[0].val.clusterDim.y = 1; cattr[0].val.clusterDim.z = 1;
+    ccfg.attrs = cattr;
+    ccfg.numAttrs = 1;
     auto enqueue = [&]() -> cudaError_t {
         k_sor_clear<<<grid_for(ncell, 256), 256, 0, s>>>((uint32_t)ncell, st->ccode.p, st->csid.p);
         k_sor_scatter<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p,
@@ -753,7 +1043,8 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
         k_sor_init<<<grid_for(nst, 256), 256, 0, s>>>(nst, st->resid_buf.p, st->sweeps.p, st->resid.p);
         cudaError_t e = cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s);
         if (e == cudaSuccess) e = cudaMemsetAsync(w->err.p, 0, sizeof(uint32_t), s);
-        if (e == cudaSuccess) e = cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s);
+        if (e == cudaSuccess) e = use_cl ? cudaLaunchKernelEx(&ccfg, k_sor_cluster, CA)
+                                         : cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s);
         if (e != cudaSuccess) return e;
         k_sor_gather<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p,
                                                           st->active0.p, w->ctab.p, st->cphi.p, w->s_phi64.p, w->s_phi.p);
@@ -763,7 +1054,7 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     // capture (a cooperative launch in a graph), the solve launches directly from then on
     cudaGraphExec_t ex = nullptr;
     for (auto &g : st->graphs)
-        if (g.n_work == A.n_work && g.grid == grid) ex = g.exec;
+        if (g.n_work == n_launch && g.grid == grid && g.mode == (use_cl ? 1u : 0u)) ex = g.exec;
     if (!ex && st->graphs_ok) {
         cudaGraph_t gr = nullptr;
         if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
@@ -778,11 +1069,12 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
         if (!ex) { st->graphs_ok = false; cudaGetLastError(); }
         else {
             if (st->graphs.size() >= 8) { cudaGraphExecDestroy(st->graphs.front().exec); st->graphs.erase(st->graphs.begin()); }
-            st->graphs.push_back({A.n_work, grid, ex});
+            st->graphs.push_back({n_launch, grid, use_cl ? 1u : 0u, ex});
         }
     }
     if (ex) { SF_CUDA(cudaGraphLaunch(ex, s)); st->graph_launches++; }
     else SF_CUDA(enqueue());
+    if (use_cl) st->cluster_solves++;
     SF_CUDA(cudaEventRecord(w->ev1, s));
     SF_CUDA(cudaGetLastError());
     std::vector<uint32_t> sw(nst);
@@ -800,6 +1092,7 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
         rep.max_residual = std::max(rep.max_residual, (double)rs[q]);
     }
     w->stats.graph_launches = st->graph_launches;
+    w->stats.cluster_solves = st->cluster_solves;
     // per sweep, since solves of one bucket converge in different sweep counts
     if (e == SF_OK) st->tune.record(tb, tci, ms / (float)std::max<uint32_t>(rep.max_sweeps_done, 1));
     if (report) *report = rep;

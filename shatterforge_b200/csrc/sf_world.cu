@@ -273,6 +273,7 @@ void sf_params_default(sf_params *p) {
     p->verify = 1;
     p->solve_blocks = 0;
     p->manifold_chunk = 16;
+    p->sor_cluster = 1;
 }
 
 sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf_world **out) {

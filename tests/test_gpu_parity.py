@@ -457,3 +457,38 @@ def test_bounded_wait_gives_up_and_context_stays_usable(sf):
     w = sf.World(small_debris(seed=17, n=40), iterations=8)
     w.step(1 / 60, nsteps=5)
     assert w.stats().error_word == 0
+
+
+def test_colour_count_beside_the_references(sf, oracle):
+    """The GPU colouring (greedy in priority order, by Jones-Plassmann rounds) is proper, and its colour count is
+    reported beside that of the reference's round-based colouring (gpu/gpu_world.js:922-1038) run on the same
+    manifolds with its defaults (16 colours, 2 + 4 rounds): the reference sends what it cannot colour in its rounds
+    to an overflow pass, the GPU colouring colours every manifold."""
+    sc = S.debris_scene(1500, seed=22, spacing=1.0)
+    w = sf.World(sc, iterations=8)
+    w.step(1 / 60, nsteps=60)
+    m = w.manifolds()
+    assert len(m) > 500
+    a, b, col = m[:, 0], m[:, 1], m[:, 2]
+    ours = int(col.max()) + 1
+    assert ours == w.stats().colors
+    rcol, used, ovf = oracle.ref_colouring(a, b, np.ones(len(m), np.uint8), (b != STATIC).astype(np.uint8), sc.n_bodies)
+    print(f"colours: gpu {ours} (no overflow); reference algorithm {used} + {ovf} overflow of {len(m)} manifolds")
+    assert used >= 1 and ovf + int((rcol < 16).sum()) == len(m)
+
+
+def test_sor_cluster_path_equals_grid_path(sf):
+    """One thread-block cluster per structure (cells in shared memory) gives the grid-wide kernel's potentials, sweep
+    counts and residuals bit for bit, on many structures at once and on the 16-storey tower."""
+    for sc in (S.config3_world(scale=0.05, n_struct=8), S.config2_tower()[0]):
+        a = sf.World(sc, sor_cluster=1)
+        b = sf.World(sc, sor_cluster=0)
+        ra = a.structure_solve(-1, omega=1.7, tol=1e-7, max_sweeps=40000)
+        rb = b.structure_solve(-1, omega=1.7, tol=1e-7, max_sweeps=40000)
+        assert a.stats().cluster_solves == 1 and b.stats().cluster_solves == 0
+        np.testing.assert_array_equal(a.phi64(), b.phi64())
+        sa, xa = a.solve_detail()
+        sb, xb = b.solve_detail()
+        np.testing.assert_array_equal(sa, sb)
+        np.testing.assert_array_equal(xa, xb)
+        assert ra.max_sweeps_done == rb.max_sweeps_done
