@@ -61,13 +61,17 @@ struct SorState {
     Tuner tune;   // blocks per SM of the red-black kernel, keyed on log2(chunks of the solve)
     // The solve's launch sequence captured in CUDA graphs, one per launch shape (the chunk list and the active
     // flags live in device buffers the graph reads, so a graph serves every solve of its shape).
-    struct Graph { uint32_t n_work, grid, mode; cudaGraphExec_t exec; };
+    struct Graph { uint32_t n_work, grid, mode, n_big, grid_small; cudaGraphExec_t exec; };
     // the cluster path: one thread-block cluster per structure, the structure's cells in the cluster's shared memory
     bool cl_ready = false;
     std::vector<uint32_t> h_cl_n, h_cl_per;
     DBuf<uint32_t> cl_cpos, cl_off, cl_n, cl_per, cl_even, cl_list;
     DBuf<uint16_t> cl_nbr;
     uint64_t cluster_solves = 0;
+    // the small structures' clusters run beside the large ones', on a second stream forked from and joined to the
+    // world's stream (inside the captured graph too)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     DBuf<SorParams> prm;
     std::vector<Graph> graphs;
     bool graphs_ok = true;
@@ -321,6 +325,7 @@ constexpr int SOR_CL = 8;
 constexpr int SOR_CL_MAX_THREADS = 1024;         // threads per block: 256, 512 or 1024, picked per launch
 constexpr uint32_t SOR_CL_CAP = 8192;            // cells per block: 28 B each (phi 8, rhs 4, code 4, 6 neighbours 12)
 constexpr uint32_t SOR_CL_BYTES_PER_CELL = 28;
+constexpr uint32_t SOR_CL_SPLIT = 1024;          // cells per block above which a structure counts as large
 constexpr uint32_t CELL_ACTIVE = 1u << 31;
 constexpr uint16_t NO_CELL = 0xFFFFu;
 
@@ -826,7 +831,12 @@ uint64_t sor_graph_launches(const SorState *st) { return st ? st->graph_launches
 void sor_reset_launches(SorState *st) { if (st) { st->wk.launches = 0; st->launches = 0; } }
 
 void sor_destroy(sf_world *w) {
-    if (w->sor) for (auto &g : w->sor->graphs) cudaGraphExecDestroy(g.exec);
+    if (w->sor) {
+        for (auto &g : w->sor->graphs) cudaGraphExecDestroy(g.exec);
+        if (w->sor->fork) cudaEventDestroy(w->sor->fork);
+        if (w->sor->join) cudaEventDestroy(w->sor->join);
+        if (w->sor->aux) cudaStreamDestroy(w->sor->aux);
+    }
     delete w->sor;
     w->sor = nullptr;
 }
@@ -966,6 +976,8 @@ static sf_status sor_cluster_tables(sf_world *w) {
     if (!nbr.empty()) SF_CUDA(cudaMemcpyAsync(st->cl_nbr.p, nbr.data(), nbr.size() * 2, cudaMemcpyHostToDevice, s));
     SF_CUDA(cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(SOR_CL_CAP * SOR_CL_BYTES_PER_CELL)));
+    SF_CUDA(cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared));
     SF_CUDA(cudaStreamSynchronize(s));
     st->cl_ready = true;
     return SF_OK;
@@ -995,11 +1007,25 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     }
     SF_CUDA(cudaMemcpyAsync(st->active0.p, act.data(), nst * 4, cudaMemcpyHostToDevice, s));
     std::vector<uint32_t> cl_order;
+    // two launches when the structures are of both sizes: the large ones' clusters with SOR_CL_MAX_THREADS threads a
+    // block (one block an SM), the small ones' with 256 threads and their own, smaller shared memory (several blocks
+    // an SM), side by side, so that all clusters are resident at once
+    uint32_t n_big = 0, per_big = 0, per_small = 0;
     if (use_cl) {
         // largest structures first: their clusters start before the small ones when not all fit at once
         cl_order = req;
         std::stable_sort(cl_order.begin(), cl_order.end(), [&](uint32_t a, uint32_t b) { return st->h_cl_n[a] > st->h_cl_n[b]; });
+        for (uint32_t q : cl_order) {
+            if (st->h_cl_per[q] > SOR_CL_SPLIT) { n_big++; per_big = std::max(per_big, st->h_cl_per[q]); }
+            else per_small = std::max(per_small, st->h_cl_per[q]);
+        }
+        if (n_big == 0 || n_big == cl_order.size()) { n_big = 0; per_small = 0; }   // one launch
         SF_CUDA(cudaMemcpyAsync(st->cl_list.p, cl_order.data(), cl_order.size() * 4, cudaMemcpyHostToDevice, s));
+        if (n_big && !st->aux) {
+            SF_CUDA(cudaStreamCreateWithFlags(&st->aux, cudaStreamNonBlocking));
+            SF_CUDA(cudaEventCreateWithFlags(&st->fork, cudaEventDisableTiming));
+            SF_CUDA(cudaEventCreateWithFlags(&st->join, cudaEventDisableTiming));
+        }
     }
     else SF_CUDA(cudaMemcpyAsync(st->work.p, chunks.data(), chunks.size() * 4, cudaMemcpyHostToDevice, s));
     SF_CUDA(cudaEventRecord(w->ev0, s));
@@ -1017,24 +1043,32 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     const int tb = Tuner::bucket(chunks.size());
     const unsigned per_sm = use_cl ? 1u : (unsigned)st->tune.choose(tb, tci);
     if (use_cl) tci = -1;
-    unsigned grid = use_cl ? per_max : (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * per_sm);
+    unsigned grid = use_cl ? (n_big ? per_big : per_max) : (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * per_sm);
     const uint32_t n_launch = use_cl ? (uint32_t)req.size() : A.n_work;
     void *args[] = {&A};
     SorClusterArgs CA;
     CA.list = st->cl_list.p; CA.off = st->cl_off.p; CA.n = st->cl_n.p; CA.per = st->cl_per.p; CA.even = st->cl_even.p;
     CA.cpos = st->cl_cpos.p; CA.nbr = st->cl_nbr.p; CA.cphi = st->cphi.p; CA.crhs = st->crhs.p; CA.ccode = st->ccode.p;
-    CA.csid = st->csid.p; CA.per_max = per_max; CA.prm = st->prm.p; CA.sweeps = st->sweeps.p; CA.resid = st->resid.p;
-    CA.err = w->err.p;
-    cudaLaunchConfig_t ccfg = {};
+    CA.csid = st->csid.p; CA.per_max = n_big ? per_big : per_max; CA.prm = st->prm.p; CA.sweeps = st->sweeps.p;
+    CA.resid = st->resid.p; CA.err = w->err.p;
+    SorClusterArgs CS = CA;   // the small structures' launch: the list after the large ones
+    CS.list = st->cl_list.p + n_big;
+    CS.per_max = per_small;
     cudaLaunchAttribute cattr[1];
-    ccfg.gridDim = dim3((unsigned)(req.size() * SOR_CL));
-    ccfg.blockDim = dim3(sor_cl_threads(per_max));
-    ccfg.dynamicSmemBytes = (size_t)per_max * SOR_CL_BYTES_PER_CELL;
-    ccfg.stream = s;
     cattr[0].id = cudaLaunchAttributeClusterDimension;
     cattr[0].val.clusterDim.x = SOR_CL; cattr[0].val.clusterDim.y = 1; cattr[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t ccfg = {}, scfg = {};
+    ccfg.gridDim = dim3((unsigned)((n_big ? n_big : req.size()) * SOR_CL));
+    ccfg.blockDim = dim3(sor_cl_threads(CA.per_max));
+    ccfg.dynamicSmemBytes = (size_t)CA.per_max * SOR_CL_BYTES_PER_CELL;
+    ccfg.stream = s;
     ccfg.attrs = cattr;
     ccfg.numAttrs = 1;
+    scfg = ccfg;
+    scfg.gridDim = dim3((unsigned)((req.size() - n_big) * SOR_CL));
+    scfg.blockDim = dim3(256);
+    scfg.dynamicSmemBytes = (size_t)per_small * SOR_CL_BYTES_PER_CELL;
+    scfg.stream = st->aux;
     auto enqueue = [&]() -> cudaError_t {
         k_sor_clear<<<grid_for(ncell, 256), 256, 0, s>>>((uint32_t)ncell, st->ccode.p, st->csid.p);
         k_sor_scatter<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p,
@@ -1043,8 +1077,17 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
         k_sor_init<<<grid_for(nst, 256), 256, 0, s>>>(nst, st->resid_buf.p, st->sweeps.p, st->resid.p);
         cudaError_t e = cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s);
         if (e == cudaSuccess) e = cudaMemsetAsync(w->err.p, 0, sizeof(uint32_t), s);
-        if (e == cudaSuccess) e = use_cl ? cudaLaunchKernelEx(&ccfg, k_sor_cluster, CA)
-                                         : cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s);
+        if (use_cl && n_big) {
+            if (e == cudaSuccess) e = cudaEventRecord(st->fork, s);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(st->aux, st->fork, 0);
+            if (e == cudaSuccess) e = cudaLaunchKernelEx(&scfg, k_sor_cluster, CS);
+            if (e == cudaSuccess) e = cudaEventRecord(st->join, st->aux);
+            if (e == cudaSuccess) e = cudaLaunchKernelEx(&ccfg, k_sor_cluster, CA);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, st->join, 0);
+        } else if (e == cudaSuccess) {
+            e = use_cl ? cudaLaunchKernelEx(&ccfg, k_sor_cluster, CA)
+                       : cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s);
+        }
         if (e != cudaSuccess) return e;
         k_sor_gather<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p,
                                                           st->active0.p, w->ctab.p, st->cphi.p, w->s_phi64.p, w->s_phi.p);
@@ -1054,7 +1097,9 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     // capture (a cooperative launch in a graph), the solve launches directly from then on
     cudaGraphExec_t ex = nullptr;
     for (auto &g : st->graphs)
-        if (g.n_work == n_launch && g.grid == grid && g.mode == (use_cl ? 1u : 0u)) ex = g.exec;
+        if (g.n_work == n_launch && g.grid == grid && g.mode == (use_cl ? 1u : 0u) && g.n_big == n_big &&
+            g.grid_small == per_small)
+            ex = g.exec;
     if (!ex && st->graphs_ok) {
         cudaGraph_t gr = nullptr;
         if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
@@ -1069,7 +1114,7 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
         if (!ex) { st->graphs_ok = false; cudaGetLastError(); }
         else {
             if (st->graphs.size() >= 8) { cudaGraphExecDestroy(st->graphs.front().exec); st->graphs.erase(st->graphs.begin()); }
-            st->graphs.push_back({n_launch, grid, use_cl ? 1u : 0u, ex});
+            st->graphs.push_back({n_launch, grid, use_cl ? 1u : 0u, n_big, per_small, ex});
         }
     }
     if (ex) { SF_CUDA(cudaGraphLaunch(ex, s)); st->graph_launches++; }

@@ -479,12 +479,15 @@ def test_colour_count_beside_the_references(sf, oracle):
 
 def test_sor_cluster_path_equals_grid_path(sf):
     """One thread-block cluster per structure (cells in shared memory) gives the grid-wide kernel's potentials, sweep
-    counts and residuals bit for bit, on many structures at once and on the 16-storey tower."""
-    for sc in (S.config3_world(scale=0.05, n_struct=8), S.config2_tower()[0]):
+    counts and residuals bit for bit: on many small structures at once, on the 16-storey tower, and on the 37-structure
+    lattice of 275,618 bricks, whose large and small structures run as two launches side by side."""
+    cases = ((S.config3_world(scale=0.05, n_struct=8), 1e-7, 40000), (S.config2_tower()[0], 1e-7, 40000),
+             (S.config3_world(seed=2), 1e-6, 3000))
+    for sc, tol, cap in cases:
         a = sf.World(sc, sor_cluster=1)
         b = sf.World(sc, sor_cluster=0)
-        ra = a.structure_solve(-1, omega=1.7, tol=1e-7, max_sweeps=40000)
-        rb = b.structure_solve(-1, omega=1.7, tol=1e-7, max_sweeps=40000)
+        ra = a.structure_solve(-1, omega=1.7, tol=tol, max_sweeps=cap)
+        rb = b.structure_solve(-1, omega=1.7, tol=tol, max_sweeps=cap)
         assert a.stats().cluster_solves == 1 and b.stats().cluster_solves == 0
         np.testing.assert_array_equal(a.phi64(), b.phi64())
         sa, xa = a.solve_detail()
