@@ -78,7 +78,7 @@ typedef struct sf_params {
     uint32_t manifold_chunk;    /* a body pair's contacts are solved in chunks of at most this many, 1..32 (0 or more
                                    than 32 mean 32); chunks of one pair take different colours, bounding each
                                    colour's longest chain and the contact layout's depth */
-    uint32_t sor_cluster;       /* 1: a structure of at most 65,536 bricks is solved by one thread-block cluster that
+    uint32_t sor_cluster;       /* 1: a structure of at most 65,534 bricks is solved by one thread-block cluster that
                                    keeps its cells in shared memory (same potentials and sweeps); 0: always the
                                    grid-wide kernel */
     uint32_t reserved[6];

@@ -297,21 +297,31 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
     return t;
 }
 constexpr unsigned long long BARRIER_LIMIT_NS = 4000000000ull;   // 4 s
-// Every device-side wait in this library: spin while *p == v for at most limit_ns of wall time (and at most 2^30
-// polls, a backstop should the clock misbehave); on running out, set ERR_TIMEOUT in *err and return false.
-__device__ __forceinline__ bool bounded_wait_while_equal(const unsigned *p, unsigned v, unsigned long long limit_ns,
-                                                         unsigned *err) {
+// Every device-side wait in this library goes through bounded_wait: spin until done() holds, for at most limit_ns of
+// wall time (and at most 2^30 polls, a backstop should the clock misbehave); on running out, set ERR_TIMEOUT in *err
+// and return false. A wait also gives up (returns false) once another wait has set ERR_TIMEOUT, so that waits on work
+// that will now never finish end promptly instead of each running out its own limit.
+template <class Done>
+__device__ __forceinline__ bool bounded_wait(Done done, unsigned long long limit_ns, unsigned *err) {
     const unsigned long long t0 = globaltimer_ns();
     unsigned spins = 0;
-    while (ld_acquire_u32(p) == v) {
+    while (!done()) {
         ++spins;
-        if (((spins & 255u) == 0 && globaltimer_ns() - t0 > limit_ns) || spins >= (1u << 30)) {
-            atomicOr(err, (unsigned)ERR_TIMEOUT);
-            return false;
+        if ((spins & 255u) == 0) {
+            if (globaltimer_ns() - t0 > limit_ns || spins >= (1u << 30)) {
+                atomicOr(err, (unsigned)ERR_TIMEOUT);
+                return false;
+            }
+            if (ld_acquire_u32(err) & ERR_TIMEOUT) return false;
         }
         __nanosleep(20);
     }
     return true;
+}
+// spin while *p == v
+__device__ __forceinline__ bool bounded_wait_while_equal(const unsigned *p, unsigned v, unsigned long long limit_ns,
+                                                         unsigned *err) {
+    return bounded_wait([&] { return ld_acquire_u32(p) != v; }, limit_ns, err);
 }
 __device__ __forceinline__ bool grid_sync(GridBarrier *gb, unsigned nblocks, unsigned *err) {
     __shared__ int s_ok;
