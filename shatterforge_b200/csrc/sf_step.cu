@@ -839,6 +839,13 @@ __device__ __forceinline__ void solve_manifold(const SolveArgs &A, uint32_t m, u
 
 constexpr int SOLVE_BLOCK = 128;
 
+// A colour's manifolds are listed by contact count, most first. Thread g takes position g of even rounds and the
+// mirrored position of odd rounds (2 stride - 1 - g, ...), so the threads that get a round's largest manifolds get
+// the next round's smallest; consecutive threads still take consecutive positions (coalesced contact loads).
+__device__ __forceinline__ uint32_t snake_pos(uint32_t r, uint32_t g, uint32_t stride) {
+    return (r & 1u) ? (r + 1) * stride - 1 - g : r * stride + g;
+}
+
 __global__ void __launch_bounds__(SOLVE_BLOCK) k_solve(SolveArgs A) {
     __shared__ uint32_t off[JDS_K];
     const uint32_t ncol = A.dev[DV_COLORS];
@@ -848,7 +855,11 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) k_solve(SolveArgs A) {
             if (threadIdx.x < JDS_K) off[threadIdx.x] = A.jds_off[c * JDS_K + threadIdx.x];
             __syncthreads();
             const uint32_t s0 = A.col_start[c], n = A.col_start[c + 1] - s0;
-            for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) solve_manifold<false>(A, A.col_list[s0 + p], p, off);
+            const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+            for (uint32_t r = 0; r * stride < n; r++) {
+                const uint32_t p = snake_pos(r, g, stride);
+                if (p < n) solve_manifold<false>(A, A.col_list[s0 + p], p, off);
+            }
             if (!grid_sync(A.gb, gridDim.x, A.err)) return;
         }
     }
@@ -865,7 +876,10 @@ __global__ void __launch_bounds__(SOLVE_ONE_BLOCK) k_solve_one_block(SolveArgs A
             if (threadIdx.x < JDS_K) off[threadIdx.x] = A.jds_off[c * JDS_K + threadIdx.x];
             __syncthreads();
             const uint32_t s0 = A.col_start[c], n = A.col_start[c + 1] - s0;
-            for (uint32_t p = threadIdx.x; p < n; p += blockDim.x) solve_manifold<true>(A, A.col_list[s0 + p], p, off);
+            for (uint32_t r = 0; r * blockDim.x < n; r++) {
+                const uint32_t p = snake_pos(r, threadIdx.x, blockDim.x);
+                if (p < n) solve_manifold<true>(A, A.col_list[s0 + p], p, off);
+            }
             __syncthreads();
         }
     }
