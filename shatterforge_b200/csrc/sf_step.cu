@@ -527,7 +527,8 @@ __device__ __forceinline__ float eff_mass(float ima, const float *iia, bool hasb
 struct PrepArgs {
     uint32_t nc;
     float h;
-    const uint32_t *perm, *L_a, *L_b;
+    const uint32_t *nm_p, *ncol_p;           // manifolds and colours of the substep (device counts)
+    const uint32_t *perm, *man_a, *man_b, *man_count;
     const uint32_t *man_start, *col_start, *col_list, *jds_off;
     const float4 *L_p, *L_n, *pos, *v, *w;
     const float *im, *iiw;
@@ -535,71 +536,75 @@ struct PrepArgs {
     uint32_t *invperm;
 };
 
-// One thread per slot d of the solve's contact layout (so the writes are coalesced): the slot's colour and depth come
-// from the layout table, its manifold from the colour list, its contact from the manifold's first contact.
+// One thread per manifold, in colour-list order (position p of colour c): the two bodies are read once, then each of
+// the manifold's contacts is prepared into its slot of the contact layout, jds_off[c][kk] + p (consecutive threads
+// write consecutive slots). The per-contact arithmetic is prep_contacts' (src/lib.rs:1553-1580).
 __global__ void k_prep(PrepArgs A) {
-    const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= A.nc) return;
-    uint32_t lo = 0, hi = MAXCOL * JDS_K;   // last table entry <= d
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *A.nm_p) return;
+    uint32_t lo = 0, hi = *A.ncol_p;   // colour c: col_start[c] <= i < col_start[c + 1]
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (A.jds_off[mid] <= d) lo = mid; else hi = mid;
+        if (A.col_start[mid] <= i) lo = mid; else hi = mid;
     }
-    const uint32_t c = lo / JDS_K, kk = lo % JDS_K;
-    const uint32_t m = A.col_list[A.col_start[c] + (d - A.jds_off[lo])];
-    const uint32_t t = A.man_start[m] + kk;
-    uint32_t k = A.perm[t];
-    uint32_t a = A.L_a[k], b = A.L_b[k];
-    bool hasb = b != STATIC;
-    float4 p4 = A.L_p[k], n4 = A.L_n[k];
-    V3 p = v3(p4.x, p4.y, p4.z), n = v3(n4.x, n4.y, n4.z);
-    float depth = n4.w;
-    float4 pa = A.pos[a];
-    V3 ra = sub(p, v3(pa.x, pa.y, pa.z));
-    V3 rb = v3(0.0f, 0.0f, 0.0f);
+    const uint32_t c = lo, p = i - A.col_start[c];
+    const uint32_t m = A.col_list[i];
+    const uint32_t a = A.man_a[m], b = A.man_b[m], cnt = A.man_count[m], t0 = A.man_start[m];
+    const bool hasb = b != STATIC;
+    const float4 pa = A.pos[a], va = A.v[a], wa = A.w[a];
     float iia[9], iib[9];
 #pragma unroll
     for (int q = 0; q < 9; q++) iia[q] = A.iiw[(size_t)a * 9 + q];
-    float ima = A.im[a], imb = 0.0f;
-    V3 vela, velb = v3(0.0f, 0.0f, 0.0f);
-    {
-        float4 va = A.v[a], wa = A.w[a];
-        vela = add(v3(va.x, va.y, va.z), cross(v3(wa.x, wa.y, wa.z), ra));
-    }
+    const float ima = A.im[a];
+    float imb = 0.0f;
+    float4 pb = make_float4(0, 0, 0, 0), vb = pb, wb = pb;
     if (hasb) {
-        float4 pb = A.pos[b];
-        rb = sub(p, v3(pb.x, pb.y, pb.z));
+        pb = A.pos[b]; vb = A.v[b]; wb = A.w[b];
 #pragma unroll
         for (int q = 0; q < 9; q++) iib[q] = A.iiw[(size_t)b * 9 + q];
         imb = A.im[b];
-        float4 vb = A.v[b], wb = A.w[b];
-        velb = add(v3(vb.x, vb.y, vb.z), cross(v3(wb.x, wb.y, wb.z), rb));
     }
-    float mn = eff_mass(ima, iia, hasb, imb, iib, ra, rb, n);
-    V3 dv = sub(vela, velb);
-    float vn = dot(dv, n);
-    float vn0 = maxf(-vn, 0.0f);
-    V3 vt = sub(dv, mul(n, vn));
-    float lt = len(vt);
-    V3 t1;
-    if (lt > 1e-4f) t1 = mul(vt, div_rn(1.0f, lt));
-    else {
-        V3 tt = fabsf(n.x) < 0.9f ? v3(1.0f, 0.0f, 0.0f) : v3(0.0f, 1.0f, 0.0f);
-        V3 x = cross(n, tt);
-        t1 = mul(x, div_rn(1.0f, len(x)));
+    const uint32_t *off = A.jds_off + c * JDS_K;
+    for (uint32_t kk = 0; kk < cnt; kk++) {
+        const uint32_t d = off[kk] + p;
+        const uint32_t k = A.perm[t0 + kk];
+        const float4 p4 = A.L_p[k], n4 = A.L_n[k];
+        const V3 pt = v3(p4.x, p4.y, p4.z), n = v3(n4.x, n4.y, n4.z);
+        const float depth = n4.w;
+        const V3 ra = sub(pt, v3(pa.x, pa.y, pa.z));
+        V3 rb = v3(0.0f, 0.0f, 0.0f);
+        const V3 vela = add(v3(va.x, va.y, va.z), cross(v3(wa.x, wa.y, wa.z), ra));
+        V3 velb = v3(0.0f, 0.0f, 0.0f);
+        if (hasb) {
+            rb = sub(pt, v3(pb.x, pb.y, pb.z));
+            velb = add(v3(vb.x, vb.y, vb.z), cross(v3(wb.x, wb.y, wb.z), rb));
+        }
+        const float mn = eff_mass(ima, iia, hasb, imb, iib, ra, rb, n);
+        const V3 dv = sub(vela, velb);
+        const float vn = dot(dv, n);
+        const float vn0 = maxf(-vn, 0.0f);
+        const V3 vt = sub(dv, mul(n, vn));
+        const float lt = len(vt);
+        V3 t1;
+        if (lt > 1e-4f) t1 = mul(vt, div_rn(1.0f, lt));
+        else {
+            V3 tt = fabsf(n.x) < 0.9f ? v3(1.0f, 0.0f, 0.0f) : v3(0.0f, 1.0f, 0.0f);
+            V3 x = cross(n, tt);
+            t1 = mul(x, div_rn(1.0f, len(x)));
+        }
+        const V3 t2 = cross(n, t1);
+        const float mt1 = eff_mass(ima, iia, hasb, imb, iib, ra, rb, t1);
+        const float mt2 = eff_mass(ima, iia, hasb, imb, iib, ra, rb, t2);
+        float bias = minf(div_rn(0.2f, A.h) * maxf(depth - 0.01f, 0.0f), 1.0f);
+        if (vn < -2.0f) bias = maxf(bias, -0.12f * vn);
+        A.S_n[d] = make_float4(n.x, n.y, n.z, mn);
+        A.S_t1[d] = make_float4(t1.x, t1.y, t1.z, mt1);
+        A.S_t2[d] = make_float4(t2.x, t2.y, t2.z, mt2);
+        A.S_ra[d] = make_float4(ra.x, ra.y, ra.z, bias);
+        A.S_rb[d] = make_float4(rb.x, rb.y, rb.z, vn0);
+        A.S_j[d] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        A.invperm[k] = d;
     }
-    V3 t2 = cross(n, t1);
-    float mt1 = eff_mass(ima, iia, hasb, imb, iib, ra, rb, t1);
-    float mt2 = eff_mass(ima, iia, hasb, imb, iib, ra, rb, t2);
-    float bias = minf(div_rn(0.2f, A.h) * maxf(depth - 0.01f, 0.0f), 1.0f);
-    if (vn < -2.0f) bias = maxf(bias, -0.12f * vn);
-    A.S_n[d] = make_float4(n.x, n.y, n.z, mn);
-    A.S_t1[d] = make_float4(t1.x, t1.y, t1.z, mt1);
-    A.S_t2[d] = make_float4(t2.x, t2.y, t2.z, mt2);
-    A.S_ra[d] = make_float4(ra.x, ra.y, ra.z, bias);
-    A.S_rb[d] = make_float4(rb.x, rb.y, rb.z, vn0);
-    A.S_j[d] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    A.invperm[k] = d;
 }
 
 // ---------------------------------------------------------------- colouring
@@ -1459,7 +1464,8 @@ static sf_status substep(sf_world *w, float h) {
         }
         prof_mark(w);
         PrepArgs PA;
-        PA.nc = nc; PA.h = h; PA.perm = S->perm.p; PA.L_a = S->L_a.p; PA.L_b = S->L_b.p; PA.L_p = S->L_p.p; PA.L_n = S->L_n.p;
+        PA.nc = nc; PA.h = h; PA.nm_p = S->dev.p + DV_MANIFOLDS; PA.ncol_p = S->dev.p + DV_COLORS; PA.perm = S->perm.p;
+        PA.man_a = S->man_a.p; PA.man_b = S->man_b.p; PA.man_count = S->man_count.p; PA.L_p = S->L_p.p; PA.L_n = S->L_n.p;
         PA.man_start = S->man_start.p; PA.col_start = S->col_start.p; PA.col_list = S->col_list.p;
         PA.jds_off = S->jds_off.p;
         PA.pos = w->b_pos.p; PA.v = w->b_v.p; PA.w = w->b_w.p; PA.im = w->b_im.p; PA.iiw = w->b_iiw.p;
