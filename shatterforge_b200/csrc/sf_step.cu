@@ -659,15 +659,28 @@ __global__ void __launch_bounds__(256) k_jp(JpArgs A) {
         uint32_t *wl_out = (r & 1) ? A.wl0 : A.wl1;
         uint32_t *cnt_out = &A.dev[DV_WL0 + ((r + 1) % 3)];
         if (blockIdx.x == 0 && threadIdx.x == 0) A.dev[DV_WL0 + ((r + 2) % 3)] = 0;
-        for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_in; t += gridDim.x * blockDim.x) {
-            const uint32_t m = r == 0 ? t : __ldcg(&wl_in[t]);
-            const uint32_t a = A.man_a[m], b = A.man_b[m], pm = A.prio[m];
-            bool blocked = jp_blocked(A, a, m, pm, r);
-            if (!blocked && b != STATIC) blocked = jp_blocked(A, b, m, pm, r);
-            if (blocked) {
-                wl_out[atomicAdd(cnt_out, 1u)] = m;
-                continue;
+        // a warp walks 32 consecutive entries at a time (the same entries per thread as a plain grid-stride loop),
+        // so that it can append its blocked manifolds to the next worklist with one atomic
+        const uint32_t lane = threadIdx.x & 31u;
+        for (uint32_t t0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); t0 < n_in; t0 += gridDim.x * blockDim.x) {
+            const uint32_t t = t0 + lane;
+            const bool valid = t < n_in;
+            uint32_t m = 0, a = 0, b = STATIC, pm = 0;
+            bool blocked = false;
+            if (valid) {
+                m = r == 0 ? t : __ldcg(&wl_in[t]);
+                a = A.man_a[m]; b = A.man_b[m]; pm = A.prio[m];
+                blocked = jp_blocked(A, a, m, pm, r);
+                if (!blocked && b != STATIC) blocked = jp_blocked(A, b, m, pm, r);
             }
+            const uint32_t bal = __ballot_sync(0xffffffffu, valid && blocked);
+            if (bal) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(cnt_out, (uint32_t)__popc(bal));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (valid && blocked) wl_out[base + __popc(bal & ((1u << lane) - 1u))] = m;
+            }
+            if (!valid || blocked) continue;
             uint32_t used[4];
 #pragma unroll
             for (int k = 0; k < 4; k++) used[k] = __ldcg(&A.masks[(size_t)a * 4 + k]) | (b != STATIC ? __ldcg(&A.masks[(size_t)b * 4 + k]) : 0u);
@@ -688,22 +701,39 @@ __global__ void __launch_bounds__(256) k_jp(JpArgs A) {
     }
 }
 
+// Warp-aggregated counter increment: the lanes that share a key take one atomicAdd on ctr[key] between them; each
+// gets old value + its rank among those lanes. Every lane of the warp must call it; invalid lanes take nothing.
+__device__ __forceinline__ uint32_t warp_add1(uint32_t *ctr, uint32_t key, bool valid) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t peers = __match_any_sync(0xffffffffu, valid ? key : 0xFFFFFFFFu);
+    const uint32_t leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (valid && lane == leader) base = atomicAdd(&ctr[key], (uint32_t)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + __popc(peers & ((1u << lane) - 1u));
+}
+
 // manifolds counted by (colour, contact count), count descending: bucket c * (JDS_K + 1) + (JDS_K - count)
 constexpr int JDS_ROW = JDS_K + 1;
+// Most manifolds fall in a few (colour, count) buckets: the lanes of a warp that share a bucket take one atomic
+// between them (warp_add1), and the colour count is reduced over the warp first. (The order of a bucket's
+// manifolds is arbitrary either way; a colour's manifolds are independent.)
 __global__ void k_col_count(const uint32_t *nm_p, const uint32_t *man_color, const uint32_t *man_count, uint32_t *hist,
                             uint32_t *dev) {
-    uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= *nm_p) return;
-    uint32_t c = man_color[m];
-    atomicAdd(&hist[c * JDS_ROW + (JDS_K - man_count[m])], 1u);
-    atomicMax(&dev[DV_COLORS], c + 1);
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = m < *nm_p;
+    const uint32_t c = valid ? man_color[m] : 0u;
+    warp_add1(hist, valid ? c * JDS_ROW + (JDS_K - man_count[m]) : 0u, valid);
+    const uint32_t cm = __reduce_max_sync(0xffffffffu, valid ? c + 1 : 0u);
+    if ((threadIdx.x & 31u) == 0 && cm) atomicMax(&dev[DV_COLORS], cm);
 }
 __global__ void k_col_fill(const uint32_t *nm_p, const uint32_t *man_color, const uint32_t *man_count,
                            const uint32_t *hstart, uint32_t *hfill, uint32_t *col_list) {
-    uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= *nm_p) return;
-    const uint32_t bkt = man_color[m] * JDS_ROW + (JDS_K - man_count[m]);
-    col_list[hstart[bkt] + atomicAdd(&hfill[bkt], 1u)] = m;
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = m < *nm_p;
+    const uint32_t bkt = valid ? man_color[m] * JDS_ROW + (JDS_K - man_count[m]) : 0u;
+    const uint32_t slot = warp_add1(hfill, bkt, valid);
+    if (valid) col_list[hstart[bkt] + slot] = m;
 }
 // one thread per colour: colour starts in col_list and the JDS offsets (contacts of colour c before c come first)
 __global__ void __launch_bounds__(MAXCOL) k_jds_table(const uint32_t *hist, const uint32_t *hstart, const uint32_t *nm_p,
@@ -925,12 +955,18 @@ __global__ void k_uf_union(const uint32_t *nm_p, const uint32_t *man_a, const ui
 __global__ void k_uf_label(uint32_t nb, const uint32_t *list, const uint8_t *alive, const uint8_t *asleep, uint32_t *parent,
                            uint32_t *label, uint32_t *dev) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nb) return;
-    const uint32_t b = pick(list, t);
-    if (!alive[b] || asleep[b]) { label[b] = NONE; return; }
-    uint32_t r = uf_find(parent, b);
-    label[b] = r;
-    if (r == b) atomicAdd(&dev[DV_ISLANDS], 1u);
+    bool root = false;
+    if (t < nb) {
+        const uint32_t b = pick(list, t);
+        if (!alive[b] || asleep[b]) label[b] = NONE;
+        else {
+            const uint32_t r = uf_find(parent, b);
+            label[b] = r;
+            root = r == b;
+        }
+    }
+    const uint32_t n = __popc(__ballot_sync(0xffffffffu, root));   // one atomic per warp
+    if ((threadIdx.x & 31u) == 0 && n) atomicAdd(&dev[DV_ISLANDS], n);
 }
 
 // ---------------------------------------------------------------- pinch clamps + integrate
