@@ -43,9 +43,9 @@ DT = 1.0 / 60.0
 ITERS = 8
 SOLVE_BYTES_PER_CONTACT_ITER = 184     # contact 64 + impulse r/w 24 + both bodies' v, w r/w 96
 # DRAM bytes (read + write) per contact-iteration of k_solve, from one ncu capture at the peak of contacts on the
-# half-size mix (DRAM bytes of that launch / (its contacts x 8 iterations)); the roofline's `traffic` scales it to this
-# run's average launch
-SOLVE_DRAM_BYTES_PER_CONTACT_ITER = 89.7
+# half-size mix: 722.7 MB for that launch / (≈847,700 contacts, from the same substep's k_prep grid, x 8 iterations);
+# the roofline's `traffic` scales it to this run's average launch
+SOLVE_DRAM_BYTES_PER_CONTACT_ITER = 106.6
 SOR_BYTES_PER_BRICK_SWEEP = 24         # grid path: f64 potential r/w 16 + rhs 4 + link word 4
 SOR_CLUSTER_BYTES_PER_BRICK = 52       # cluster path, once per solve: staging reads (phi 8, rhs 4, code 4, sid 4,
                                        # place 4, neighbours 12) + the potential written back 8 + gather 8
