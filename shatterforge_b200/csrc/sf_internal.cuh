@@ -119,6 +119,8 @@ struct DBuf {
     }
     cudaError_t grow(size_t count) { return count <= n && p ? cudaSuccess : alloc(count + count / 4 + 1024); }
     size_t bytes() const { return n * sizeof(T); }
+    // exchange the buffers of two DBufs (ping-pong pairs whose roles a pass swaps)
+    void swap(DBuf &o) { T *tp = p; p = o.p; o.p = tp; size_t tn = n; n = o.n; o.n = tn; }
 };
 
 // Online autotuner for launch shapes that do not change results (blocks per SM of the persistent kernels: the
@@ -277,10 +279,13 @@ struct Work {
 };
 // exclusive scan of n uint32 values (in place allowed); the total is written to *d_total if non-null
 cudaError_t exclusive_scan_u32(const uint32_t *in, uint32_t *out, size_t n, uint32_t *d_total, Work &wk, cudaStream_t s);
-// stable LSD radix sort of (key, value) pairs on key bits [0, bits); the result ends in keys/vals (the alt buffers,
-// n entries each, are scratch)
+// stable LSD radix sort of (key, value) pairs on key bits [0, bits). With in_alt null the result ends in keys/vals
+// (the alt buffers, n entries each, are scratch); otherwise it stays where the last pass left it and *in_alt says
+// whether that is the alt pair (the caller then swaps the buffers' roles instead of copying back)
 cudaError_t radix_sort_u64(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt, uint32_t *vals_alt, size_t n, int bits,
-                           Work &wk, cudaStream_t s);
+                           Work &wk, cudaStream_t s, bool *in_alt = nullptr);
+cudaError_t radix_sort_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt, uint32_t *vals_alt, size_t n, int bits,
+                           Work &wk, cudaStream_t s, bool *in_alt = nullptr);
 
 // ---------------------------------------------------------------- bounded grid barrier for persistent kernels
 // Every block of a cooperative launch calls it; a wait that outlasts the limit sets ERR_TIMEOUT and returns false

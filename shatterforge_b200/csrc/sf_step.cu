@@ -33,7 +33,7 @@ namespace sf {
 struct StepState {
     Work wk;
     // hashed cell sort
-    DBuf<uint64_t> ckey, ckey_alt;
+    DBuf<uint32_t> ckey, ckey_alt;   // (active scene index x HSIZE + bucket) fits 32 bits (checked per step)
     DBuf<uint32_t> cval, cval_alt;
     DBuf<uint32_t> aw_flag, awk_pos, awk_list, inc_flag, inc_pos, bucket_bits, scene_awake, scene_bricks;
     uint32_t n_awk = 0, n_inc = 0;
@@ -203,19 +203,19 @@ __global__ void k_mark_buckets(const uint32_t *n_p, const uint32_t *awk, const u
 }
 // key = (the scene's index in the active set, hashed cell), flagged when the brick goes into the hash. Dense form
 // (inc == null, most bricks awake): every live brick goes in, dead ones get none_key and sort last.
-__global__ void k_cell_keys(uint32_t nd, const uint32_t *list, uint64_t none_key, const uint32_t *kbody,
+__global__ void k_cell_keys(uint32_t nd, const uint32_t *list, uint32_t none_key, const uint32_t *kbody,
                             const uint32_t *bscene, const uint32_t *scene_act, const uint32_t *scene_awake,
                             const uint32_t *scene_bricks, const uint8_t *alive, const uint8_t *asleep, const float4 *wpos,
-                            const uint32_t *bits, uint64_t *key, uint32_t *val, uint32_t *inc) {
+                            const uint32_t *bits, uint32_t *key, uint32_t *val, uint32_t *inc) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nd) return;
     const uint32_t i = pick(list, t);
     const uint32_t b = kbody[i];
     if (!inc) {
-        uint64_t k = none_key;
+        uint32_t k = none_key;
         if (alive[b]) {
             const float4 p = wpos[i];
-            k = (uint64_t)scene_act[bscene[b]] * HSIZE + hkey(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z));
+            k = scene_act[bscene[b]] * HSIZE + hkey(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z));
         }
         key[t] = k;
         val[t] = i;
@@ -228,13 +228,13 @@ __global__ void k_cell_keys(uint32_t nd, const uint32_t *list, uint64_t none_key
         const uint32_t h = hkey(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z));
         in = !asleep[b] || scene_full(scene_awake, scene_bricks, sk) ||
              ((bits[(size_t)sk * (HSIZE / 32) + (h >> 5)] >> (h & 31)) & 1u);
-        key[t] = (uint64_t)sk * HSIZE + h;
+        key[t] = sk * HSIZE + h;
         val[t] = i;
     }
     inc[t] = in;
 }
-__global__ void k_compact_keys(uint32_t nd, const uint32_t *inc, const uint32_t *pos, const uint64_t *key_in,
-                               const uint32_t *val_in, uint64_t *key, uint32_t *val) {
+__global__ void k_compact_keys(uint32_t nd, const uint32_t *inc, const uint32_t *pos, const uint32_t *key_in,
+                               const uint32_t *val_in, uint32_t *key, uint32_t *val) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nd || !inc[t]) return;
     const uint32_t o = pos[t];
@@ -242,10 +242,10 @@ __global__ void k_compact_keys(uint32_t nd, const uint32_t *inc, const uint32_t 
     val[o] = val_in[t];
 }
 
-__global__ void k_bucket_ranges(uint32_t nd, uint64_t none_key, const uint64_t *key, uint2 *brange) {
+__global__ void k_bucket_ranges(uint32_t nd, uint32_t none_key, const uint32_t *key, uint2 *brange) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nd) return;
-    uint64_t k = key[p];
+    uint32_t k = key[p];
     if (k >= none_key) return;
     if (p == 0 || key[p - 1] != k) brange[k].x = p;
     if (p == nd - 1 || key[p + 1] != k) brange[k].y = p + 1;
@@ -1349,7 +1349,11 @@ static sf_status substep(sf_world *w, float h) {
     cudaStream_t s = w->stream;
     const uint32_t nb = S->nb_act, nd = S->nd_act;
     const uint32_t *blist = S->act_body.p, *klist = S->act_brick.p;
-    const uint64_t none_key = (uint64_t)S->act.size() * HSIZE;
+    if ((uint64_t)S->act.size() * HSIZE >= 0xFFFFFFFFull) {
+        set_error("%zu active scenes exceed the hash key range", S->act.size());
+        return SF_ERR_CAPACITY;
+    }
+    const uint32_t none_key = (uint32_t)S->act.size() * HSIZE;
     std::fill(S->act_brick_base.begin(), S->act_brick_base.end(), NONE);
     if (nb == 0 || nd == 0) {
         SF_CUDA(cudaMemsetAsync(S->dev.p, 0, DV_ALIVE * sizeof(uint32_t), s));
@@ -1409,7 +1413,11 @@ static sf_status substep(sf_world *w, float h) {
     }
     S->n_awk = n_awk;
     S->n_inc = n_inc;
-    SF_CUDA(radix_sort_u64(S->ckey.p, S->cval.p, S->ckey_alt.p, S->cval_alt.p, n_inc, bits_for(none_key), S->wk, s));
+    {
+        bool alt = false;   // the sorted keys stay where the last pass left them
+        SF_CUDA(radix_sort_u32(S->ckey.p, S->cval.p, S->ckey_alt.p, S->cval_alt.p, n_inc, bits_for(none_key), S->wk, s, &alt));
+        if (alt) { S->ckey.swap(S->ckey_alt); S->cval.swap(S->cval_alt); }
+    }
     SF_CUDA(cudaMemsetAsync(S->brange.p, 0, (size_t)S->act.size() * HSIZE * sizeof(uint2), s));
     if (n_inc) {
         k_bucket_ranges<<<grid_for(n_inc, 256), 256, 0, s>>>(n_inc, none_key, S->ckey.p, S->brange.p);
@@ -1449,7 +1457,9 @@ static sf_status substep(sf_world *w, float h) {
     if (nc) {
         const uint64_t span = (uint64_t)S->max_scene_bodies + 1;
         k_man_keys<<<g_nc, 256, 0, s>>>(nc, span, S->L_a.p, S->L_b.p, S->body_off_of_body.p, S->mkey.p, S->perm.p);
-        SF_CUDA(radix_sort_u64(S->mkey.p, S->perm.p, S->mkey_alt.p, S->perm_alt.p, nc, bits_for((uint64_t)w->nb * span + span), S->wk, s));
+        bool alt = false;
+        SF_CUDA(radix_sort_u64(S->mkey.p, S->perm.p, S->mkey_alt.p, S->perm_alt.p, nc, bits_for((uint64_t)w->nb * span + span), S->wk, s, &alt));
+        if (alt) { S->mkey.swap(S->mkey_alt); S->perm.swap(S->perm_alt); }
         const uint32_t K = w->P.manifold_chunk;
         k_man_flags<<<g_nc, 256, 0, s>>>(nc, S->mkey.p, S->mflag.p);
         SF_CUDA(exclusive_scan_u32(S->mflag.p, S->mpos.p, nc, S->dev.p + DV_PAIRS, S->wk, s));

@@ -124,7 +124,8 @@ constexpr int RS_ITEMS = SF_RS_ITEMS;
 constexpr int RS_TILE = RS_BLOCK * RS_ITEMS;
 constexpr int RS_WARPS = RS_BLOCK / 32;
 
-__global__ void k_rs_hist(const uint64_t *keys, size_t n, int shift, uint32_t *hist, unsigned nblocks) {
+template <class K>
+__global__ void k_rs_hist(const K *keys, size_t n, int shift, uint32_t *hist, unsigned nblocks) {
     __shared__ uint32_t cnt[256];
     cnt[threadIdx.x] = 0;
     __syncthreads();
@@ -140,7 +141,8 @@ __global__ void k_rs_hist(const uint64_t *keys, size_t n, int shift, uint32_t *h
 // Stable ranking: warp w owns the tile's keys [w * 512, (w + 1) * 512), item k of lane l being key w*512 + k*32 + l,
 // so (warp, item, lane) is input order. Each warp counts its digits privately (the leader of each match group adds
 // the group's size), then one prefix over (warp, digit) places every key — two block barriers per tile.
-__global__ void __launch_bounds__(RS_BLOCK) k_rs_scatter(const uint64_t *kin, const uint32_t *vin, uint64_t *kout, uint32_t *vout,
+template <class K>
+__global__ void __launch_bounds__(RS_BLOCK) k_rs_scatter(const K *kin, const uint32_t *vin, K *kout, uint32_t *vout,
                                                          size_t n, int shift, const uint32_t *offs, unsigned nblocks) {
     __shared__ uint32_t wcnt[RS_WARPS][256];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -150,13 +152,13 @@ __global__ void __launch_bounds__(RS_BLOCK) k_rs_scatter(const uint64_t *kin, co
     __syncthreads();
     const size_t wbase = (size_t)blockIdx.x * RS_TILE + (size_t)wid * (RS_ITEMS * 32);
     const unsigned lt = (1u << lane) - 1u;
-    uint64_t key[RS_ITEMS];
+    K key[RS_ITEMS];
     uint32_t val[RS_ITEMS], rank[RS_ITEMS];
 #pragma unroll
     for (int k = 0; k < RS_ITEMS; k++) {
         const size_t i = wbase + (size_t)k * 32 + lane;
         const bool valid = i < n;
-        key[k] = valid ? kin[i] : 0ull;
+        key[k] = valid ? kin[i] : (K)0;
         val[k] = valid ? vin[i] : 0u;
         const unsigned d = valid ? (unsigned)(key[k] >> shift) & 255u : 256u;
         const unsigned peers = __match_any_sync(0xffffffffu, d);
@@ -185,30 +187,44 @@ __global__ void __launch_bounds__(RS_BLOCK) k_rs_scatter(const uint64_t *kin, co
     }
 }
 
-cudaError_t radix_sort_u64(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt, uint32_t *vals_alt, size_t n, int bits,
-                           Work &wk, cudaStream_t s) {
+template <class K>
+static cudaError_t radix_sort_impl(K *keys, uint32_t *vals, K *keys_alt, uint32_t *vals_alt, size_t n, int bits, Work &wk,
+                                   cudaStream_t s, bool *in_alt) {
+    if (in_alt) *in_alt = false;
     if (n <= 1 || bits <= 0) return cudaSuccess;
     unsigned nblocks = (unsigned)((n + RS_TILE - 1) / RS_TILE);
     cudaError_t e = wk.hist.grow((size_t)256 * nblocks);
     if (e != cudaSuccess) return e;
     int passes = (bits + 7) / 8;
-    uint64_t *ki = keys, *ko = keys_alt;
+    K *ki = keys, *ko = keys_alt;
     uint32_t *vi = vals, *vo = vals_alt;
     for (int p = 0; p < passes; p++) {
         int shift = p * 8;
-        k_rs_hist<<<nblocks, RS_BLOCK, 0, s>>>(ki, n, shift, wk.hist.p, nblocks);
+        k_rs_hist<K><<<nblocks, RS_BLOCK, 0, s>>>(ki, n, shift, wk.hist.p, nblocks);
         e = exclusive_scan_u32(wk.hist.p, wk.hist.p, (size_t)256 * nblocks, nullptr, wk, s);
         if (e != cudaSuccess) return e;
-        k_rs_scatter<<<nblocks, RS_BLOCK, 0, s>>>(ki, vi, ko, vo, n, shift, wk.hist.p, nblocks);
+        k_rs_scatter<K><<<nblocks, RS_BLOCK, 0, s>>>(ki, vi, ko, vo, n, shift, wk.hist.p, nblocks);
         wk.launches += 2;
         std::swap(ki, ko);
         std::swap(vi, vo);
     }
     if (ki != keys) {
-        cudaMemcpyAsync(keys, ki, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(vals, vi, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+        if (in_alt) *in_alt = true;
+        else {
+            cudaMemcpyAsync(keys, ki, n * sizeof(K), cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(vals, vi, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+        }
     }
     return cudaGetLastError();
+}
+
+cudaError_t radix_sort_u64(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt, uint32_t *vals_alt, size_t n, int bits,
+                           Work &wk, cudaStream_t s, bool *in_alt) {
+    return radix_sort_impl(keys, vals, keys_alt, vals_alt, n, bits, wk, s, in_alt);
+}
+cudaError_t radix_sort_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt, uint32_t *vals_alt, size_t n, int bits,
+                           Work &wk, cudaStream_t s, bool *in_alt) {
+    return radix_sort_impl(keys, vals, keys_alt, vals_alt, n, bits < 32 ? bits : 32, wk, s, in_alt);
 }
 
 // a wait on a flag that nothing sets: it must give up after its limit and report it
