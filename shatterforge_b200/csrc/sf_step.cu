@@ -401,7 +401,7 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
 }
 
 // pass 1: every contact of every awake brick counted; the first CSLOTS kept in the brick's slots
-__global__ void __launch_bounds__(128, 6) k_contacts_gen(ContactArgs A) {
+__global__ void __launch_bounds__(128, 7) k_contacts_gen(ContactArgs A) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= A.nd) return;
     const uint32_t i = pick(A.list, t);
