@@ -34,6 +34,9 @@ class StepParams(C.Structure):
 _lib = None
 
 
+NATIVE_LIB = HERE / "_build" / "native" / "libsf_oracle.so"
+
+
 def build() -> Path:
     src = HERE / "sf_oracle.cpp"
     if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
@@ -41,13 +44,32 @@ def build() -> Path:
     return LIB
 
 
+def build_native() -> Path:
+    """The same oracle compiled with -march=native for the host this runs on (always rebuilt: the file may have been
+    made on another machine). Used only to time the CPU baseline."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "native"], check=True)
+    return NATIVE_LIB
+
+
+_native = None
+
+
+def use_native() -> None:
+    """Route every later OracleWorld through the -march=native build (call before the first OracleWorld)."""
+    global _lib, _native
+    path = build_native()
+    _native = path
+    _lib = None
+
+
 def load() -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    if not LIB.exists():
+    path = _native or LIB
+    if not path.exists():
         build()
-    lib = C.CDLL(str(LIB))
+    lib = C.CDLL(str(path))
     lib.ow_create.restype = C.c_void_p
     lib.ow_create.argtypes = [C.c_uint32, _i32p, _u8p, _i32p, _u8p, C.c_uint32, _u32p, _i32p, _u8p, _f32p]
     lib.ow_destroy.argtypes = [C.c_void_p]

@@ -199,6 +199,10 @@ def structure_solve_static(xyz, mat, infill=None, ext=None, omega: float = 1.7, 
     m = np.ascontiguousarray(mat, np.uint8)
     inf = np.ascontiguousarray(infill if infill is not None else np.zeros(n, np.uint8), np.uint8)
     e = None if ext is None else np.ascontiguousarray(ext, np.float32)
+    # the library copies n entries from each array: a shorter one would be read past its end
+    for name, a in (("mat", m), ("infill", inf), ("ext", e)):
+        if a is not None and a.shape != (n,):
+            raise ValueError(f"{name} has shape {a.shape}; {n} bricks need shape ({n},)")
     phi = np.zeros(n, np.float64)
     sw = C.c_uint32()
     rs = C.c_double()

@@ -44,6 +44,7 @@ enum : uint32_t {
     ERR_VERIFY_COLOR = 1u << 3,
     ERR_JP_ROUNDS = 1u << 4,
     ERR_SOR_NONFINITE = 1u << 5,
+    ERR_ISLANDS = 1u << 6,         // a union-find walk or link ran past its bound (corrupt or cyclic parents)
 };
 
 // ---------------------------------------------------------------- f32 helpers (src/lib.rs:25-108 order)

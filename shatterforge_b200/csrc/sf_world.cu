@@ -245,7 +245,7 @@ sf_status read_error_word(sf_world *w) {
     w->stats.error_word = e;
     if (e & ERR_TIMEOUT) { set_error("a device barrier wait timed out"); return SF_ERR_TIMEOUT; }
     if (e & (ERR_CAPACITY_CONTACTS | ERR_CAPACITY_COLORS)) { set_error("device capacity exceeded (error bits 0x%x)", e); return SF_ERR_CAPACITY; }
-    if (e & (ERR_VERIFY_COLOR | ERR_JP_ROUNDS)) { set_error("device self-check failed (error bits 0x%x)", e); return SF_ERR_VERIFY; }
+    if (e & (ERR_VERIFY_COLOR | ERR_JP_ROUNDS | ERR_ISLANDS)) { set_error("device self-check failed (error bits 0x%x)", e); return SF_ERR_VERIFY; }
     return SF_OK;
 }
 

@@ -387,41 +387,69 @@ def config4_scenes(seed: int = 3, n_scenes: int = 256, lo: int = 500, hi: int = 
 
 # ---------------------------------------------------------------- structures (config 3)
 def config3_world(seed: int = 2, n_struct: int = 37, lo: int = 1000, hi: int = 40000, cap: int = 500000,
-                  scale: float = 1.0) -> Scene:
-    """Config 3: n_struct column/slab frames in one 640 x 136 x 640 lattice; brick counts log-uniform in [lo, hi]
-    (total capped at `cap`), storey height 6-8 cells, footprints 8-60 cells a side, materials 50 % concrete,
-    25 % masonry, 10 % steel, 10 % timber, 5 % glass (glass is infill, non-bearing)."""
+                  scale: float = 1.0, total: float = 378000.0) -> Scene:
+    """Config 3: n_struct column/slab frames in one 640 x 136 x 640 lattice; brick counts log-uniform in [lo, hi],
+    scaled together so that 37 structures hold `total` bricks (capped at `cap`), storey height 6-8 cells, footprints
+    8-60 cells a side, materials 50 % concrete, 25 % masonry, 10 % steel, 10 % timber, 5 % glass.
+
+    Glass is non-bearing infill: under finalize_brick's rules (src/lib.rs:668-690) an infill brick bonds to nothing
+    sideways and to no structural brick above it, so glass can only stand on a structural brick. It is placed as
+    window panels standing on a slab's perimeter (storey height - 1 cells tall, under the next slab, which they do
+    not bond to), never inside a column or a slab, where it would cut a load path. Each footprint is drawn wide
+    enough that the target fits under the lattice's 136-cell height."""
     rng = np.random.default_rng(seed)
-    targets = np.exp(rng.uniform(math.log(lo), math.log(hi), n_struct)) * scale
+    targets = np.exp(rng.uniform(math.log(lo), math.log(hi), n_struct))
+    targets *= total * n_struct / 37.0 / targets.sum()
     if targets.sum() > cap:
         targets *= cap / targets.sum()
+    targets *= scale
     slots_x, slots_z = 7, 6
     parts = []
     for s in range(n_struct):
         target = float(targets[s])
         h = int(rng.integers(6, 9))
-        wmax = int(min(60, max(8, math.sqrt(target / 2.0))))
-        wx = int(rng.integers(8, wmax + 1))
-        wz = int(rng.integers(8, wmax + 1))
+        max_storeys = (NY - 1) // h
+        # the smallest square footprint that holds the target in max_storeys slabs, and the largest the target allows
+        wmin = int(min(60, max(8, math.ceil(math.sqrt(target / max_storeys)))))
+        wmax = int(min(60, max(wmin, math.sqrt(target / 2.0))))
+        wx = int(rng.integers(wmin, wmax + 1))
+        wz = int(rng.integers(wmin, wmax + 1))
         spacing = int(rng.integers(5, 13))
         col_xs = sorted(set(list(range(0, wx, spacing)) + [wx - 1]))
         col_zs = sorted(set(list(range(0, wz, spacing)) + [wz - 1]))
-        per = wx * wz + len(col_xs) * len(col_zs) * (h - 1)
-        storeys = int(max(1, min((NY - 1) // h, round(target / per))))
+        structural = wx * wz + len(col_xs) * len(col_zs) * (h - 1)
+        panels = int(round(0.05 / 0.95 * structural / (h - 1)))     # glass panels per storey
+        per = structural + panels * (h - 1)
+        storeys = int(max(1, min(max_storeys, round(target / per))))
         gx, gz = s % slots_x, s // slots_x
         x0 = 8 + gx * (NX - 16) // slots_x
         z0 = 8 + gz * (NZ - 16) // slots_z
 
         def mat_of(xyz, _rng=rng):
-            u = _rng.random(len(xyz))
+            # structural bricks: 50 / 25 / 10 / 10 of the structure's 95 % that is not glass
+            u = _rng.random(len(xyz)) * 0.95
             m = np.full(len(xyz), CONC, np.uint8)
             m[u >= 0.50] = MASON
             m[u >= 0.75] = STEEL
             m[u >= 0.85] = WOOD
-            m[u >= 0.95] = GLASS
             return m
 
         parts.append(frame_structure(x0, z0, wx, wz, storeys, h, col_xs, col_zs, s, mat_of))
+        # window panels on the perimeter of each slab that has a storey above it, away from the columns
+        ring = [(x, 0) for x in range(wx)] + [(x, wz - 1) for x in range(wx)] + \
+               [(0, z) for z in range(1, wz - 1)] + [(wx - 1, z) for z in range(1, wz - 1)]
+        ring = [c for c in ring if not (c[0] in col_xs and c[1] in col_zs)]
+        cells = []
+        for st in range(storeys - 1):
+            ys = st * h + h - 1
+            pick = rng.choice(len(ring), min(panels, len(ring)), replace=False)
+            for k in pick:
+                cx, cz = ring[int(k)]
+                for y in range(ys + 1, ys + h):
+                    cells.append((x0 + cx, y, z0 + cz))
+        if cells:
+            g = np.array(cells, np.int32)
+            parts.append((g, np.full(len(g), GLASS, np.uint8), np.full(len(g), s, np.int32), np.ones(len(g), np.uint8)))
     xyz, mat, sid, inf = _concat_static(parts)
     keep = grounded_mask(xyz, mat, sid, inf)
     return Scene(xyz[keep], mat[keep], sid[keep], inf[keep], name="structures").contiguous()
@@ -462,3 +490,49 @@ def grounded_mask(xyz, mat, sid, infill):
     good = np.zeros(lab.max() + 1, bool)
     good[lab[xyz[:, 1] == 0]] = True
     return good[lab]
+
+
+# ---------------------------------------------------------------- long-horizon statistics
+HEIGHT_BINS = (-1e9, 0.5, 1.0, 1.5, 2.0, 3.0, 5.0, 1e9)
+SIZE_BINS = (1, 2, 4, 8, 16, 1 << 30)      # fragment size classes in bricks: 1, 2-3, 4-7, 8-15, 16+
+
+
+def horizon_stats(scene: Scene, state13: np.ndarray, flags: np.ndarray) -> dict:
+    """Statistics by which trajectories of a chaotic pile are compared after many steps, when bit-level agreement of
+    different impulse orders is lost: the centre-of-mass height of the surviving bodies; per material, the
+    histogram of their heights (HEIGHT_BINS, metres) and the surviving fraction of each fragment size class
+    (SIZE_BINS, bricks per body; bodies leave by pinch removal or by falling out of the world)."""
+    first = scene.body_first.astype(np.int64)
+    size = np.diff(first)
+    mat = scene.body_brick_mat[first[:-1]] if len(size) else np.zeros(0, np.uint8)
+    alive = (flags & 1) == 1
+    y = state13[:, 1].astype(np.float64)
+    out = {"com_y": float(y[alive].mean()) if alive.any() else float("nan"), "alive": int(alive.sum()),
+           "asleep": int(((flags & 3) == 3).sum()), "materials": {}}
+    cls = np.searchsorted(np.array(SIZE_BINS), size, side="right") - 1
+    for m in np.unique(mat):
+        sel = mat == m
+        live = sel & alive
+        hist, _ = np.histogram(y[live], bins=HEIGHT_BINS)
+        surv = []
+        for c in range(len(SIZE_BINS) - 1):
+            n0 = int((sel & (cls == c)).sum())
+            surv.append((n0, int((live & (cls == c)).sum())))
+        out["materials"][int(m)] = {"alive": int(live.sum()), "mean_y": float(y[live].mean()) if live.any() else float("nan"),
+                                    "height_hist": (hist / max(int(live.sum()), 1)).tolist(), "survivors": surv}
+    return out
+
+
+def horizon_distance(a: dict, b: dict, min_class: int = 20) -> dict:
+    """Largest differences between two horizon_stats: COM height (m), a material's mean height (m), the total
+    variation distance of a material's height histograms, and a size class's surviving fraction (classes of at
+    least min_class bodies)."""
+    d = {"com_y": abs(a["com_y"] - b["com_y"]), "mean_y": 0.0, "height_tv": 0.0, "survival": 0.0}
+    for m, x in a["materials"].items():
+        y = b["materials"][m]
+        d["mean_y"] = max(d["mean_y"], abs(x["mean_y"] - y["mean_y"]))
+        d["height_tv"] = max(d["height_tv"], 0.5 * float(np.abs(np.array(x["height_hist"]) - np.array(y["height_hist"])).sum()))
+        for (n0, s0), (_, s1) in zip(x["survivors"], y["survivors"]):
+            if n0 >= min_class:
+                d["survival"] = max(d["survival"], abs(s0 - s1) / n0)
+    return d

@@ -74,3 +74,38 @@ def test_static_solve_rejects_oversize(sf):
     ref_phi, ref_sweeps, _, _ = solve_in_world(sf, sc, ext, 1.7, 1e-6)
     assert sweeps == ref_sweeps
     np.testing.assert_array_equal(phi, ref_phi)
+
+
+def test_static_solve_equals_fp64_oracle(sf, oracle):
+    """On its own: the scratch-free solve equals the FP64 red-black oracle at the same residual, bit for bit."""
+    sc, ext = frame(4, 3, 12)
+    phi, sweeps, resid = sf.structure_solve_static(sc.static_xyz, sc.static_mat, sc.static_infill, ext,
+                                                   omega=1.7, tol=1e-6, max_sweeps=50000)
+    ow = oracle.OracleWorld(sc)
+    ow.set_ext(ext)
+    osw, ors = ow.sor(0, 1.7, 1e-6, 50000, mode=oracle.MODE_REDBLACK_F64)
+    assert sweeps == osw and resid == ors
+    np.testing.assert_array_equal(phi, ow.phi64())
+
+
+@pytest.mark.parametrize("bad", ["outside", "duplicate", "material"])
+def test_static_solve_rejects_bad_bricks_then_works(sf, bad):
+    """The device-side input checks: a brick outside the lattice, two bricks in one cell, a material outside 1..8
+    each return SF_ERR_ARG; the next call with good bricks gives the regular solve's result."""
+    sc, ext = frame(5, 2, 10)
+    xyz, mat = sc.static_xyz.copy(), sc.static_mat.copy()
+    if bad == "outside":
+        xyz[7] = [640, 3, 300]
+    elif bad == "duplicate":
+        xyz[9] = xyz[4]
+    else:
+        mat[11] = 9
+    with pytest.raises(sf.SfError) as e:
+        sf.structure_solve_static(xyz, mat, sc.static_infill, ext)
+    assert e.value.status == sf.SF_ERR_ARG
+    with pytest.raises(ValueError):
+        sf.structure_solve_static(sc.static_xyz, sc.static_mat[:-1], sc.static_infill, ext)
+    phi, sweeps, resid = sf.structure_solve_static(sc.static_xyz, sc.static_mat, sc.static_infill, ext)
+    ref_phi, ref_sweeps, ref_resid, _ = solve_in_world(sf, sc, ext, 1.7, 1e-6)
+    assert sweeps == ref_sweeps and resid == ref_resid
+    np.testing.assert_array_equal(phi, ref_phi)
