@@ -46,6 +46,11 @@ SOLVE_BYTES_PER_CONTACT_ITER = 184     # contact 64 + impulse r/w 24 + both bodi
 # half-size mix: 722.7 MB for that launch / (≈847,700 contacts, from the same substep's k_prep grid, x 8 iterations);
 # the roofline's `traffic` scales it to this run's average launch
 SOLVE_DRAM_BYTES_PER_CONTACT_ITER = 106.6
+GEN_BYTES_PER_BRICK = 40               # local offset 12 + body id 4 read, world position 12 written and re-read
+GEN_BYTES_PER_CONTACT = 64             # one contact's setup written
+# DRAM bytes (read + write) of k_contacts_gen per algorithmic byte, from the ncu capture at the peak of contacts on
+# the half-size mix: 199 MB against 40 B x 2.19M bricks + 64 B x 0.85M contacts
+GEN_DRAM_PER_ALGORITHMIC_BYTE = 1.40
 SOR_BYTES_PER_BRICK_SWEEP = 24         # grid path: f64 potential r/w 16 + rhs 4 + link word 4
 SOR_CLUSTER_BYTES_PER_BRICK = 52       # cluster path, once per solve: staging reads (phi 8, rhs 4, code 4, sid 4,
                                        # place 4, neighbours 12) + the potential written back 8 + gather 8
@@ -59,7 +64,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scenes", type=int, default=256)
     ap.add_argument("--scale", type=float, default=1.0, help="body-count scale of the debris mix (1.0 = as specified)")
-    ap.add_argument("--plain-steps", type=int, default=5)
+    ap.add_argument("--plain-steps", type=int, default=5, help="steps of the plain/batched comparison at the contact peak")
+    ap.add_argument("--plain-steps-window", type=int, default=20, help="at most this many steps of the headline window")
+    ap.add_argument("--peak-step", type=int, default=110, help="the step at which the mix has its peak of contacts")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = as --steps")
     ap.add_argument("--no-sor", action="store_true")
     ap.add_argument("--sor-max-sweeps", type=int, default=200000, help="sweep limit of the timed load-path solve")
@@ -195,49 +202,61 @@ def rank_seed(rank: int) -> int:
 
 
 # ---------------------------------------------------------------- CPU restatement (oracle) timing
-def cpu_body_steps(scenes, warmup: int, steps: int, budget_s: float, threads: int):
-    """The oracle (CPU restatement) steps each scene from rest: `warmup` untimed steps, then up to `steps` timed
-    steps or until `budget_s`, one scene per thread. Returns (body-steps/s, timed steps in all)."""
+def cpu_body_steps(scenes, warmup: int, steps: int, budget_s: float, threads: int, order=None):
+    """The oracle (the reference's CPU path, restated; built -march=native on this host) steps each scene from rest in
+    the reference's own list order: `warmup` untimed steps, then up to `steps` timed steps or until `budget_s` per
+    scene. Scenes are taken largest first by `threads` worker threads (the oracle releases the GIL). Returns
+    (body-steps/s, timed steps in all, scenes that ran every step): body-steps over the slowest thread's summed
+    timed seconds."""
+    import queue
+
     from oracle import binding as orc
+    order = orc.ORDER_LIST if order is None else order
+    work = queue.Queue()
+    for sc in sorted(scenes, key=lambda x: -x.n_bodies):
+        work.put(sc)
+    per_thread = [0.0] * threads
     results = []
     lock = threading.Lock()
 
-    def work(sc):
-        ow = orc.OracleWorld(sc)
-        for _ in range(warmup):
-            ow.step(DT, iterations=ITERS, order=orc.ORDER_COLOR, pinch_kill=0)
-        _, _, fl = ow.bodies()
-        alive = int((fl & 1).sum())
-        t0 = time.perf_counter()
-        n = 0
-        while n < steps and time.perf_counter() - t0 < budget_s:
-            ow.step(DT, iterations=ITERS, order=orc.ORDER_COLOR, pinch_kill=0)
-            n += 1
-        el = time.perf_counter() - t0
-        _, _, fl = ow.bodies()
-        # bodies only leave by falling out of the world (pinch removal is off): the mean of start and end counts
-        bsteps = n * (alive + int((fl & 1).sum())) / 2.0
-        with lock:
-            results.append((bsteps, el, n))
+    def worker(t):
+        while True:
+            try:
+                sc = work.get_nowait()
+            except queue.Empty:
+                return
+            ow = orc.OracleWorld(sc)
+            for _ in range(warmup):
+                ow.step(DT, iterations=ITERS, order=order, pinch_kill=0)
+            _, _, fl = ow.bodies()
+            alive = int((fl & 1).sum())
+            t0 = time.perf_counter()
+            n = 0
+            while n < steps and time.perf_counter() - t0 < budget_s:
+                ow.step(DT, iterations=ITERS, order=order, pinch_kill=0)
+                n += 1
+            el = time.perf_counter() - t0
+            _, _, fl = ow.bodies()
+            ow.close()
+            # bodies only leave by falling out of the world (pinch removal is off): the mean of start and end counts
+            bsteps = n * (alive + int((fl & 1).sum())) / 2.0
+            with lock:
+                per_thread[t] += el
+                results.append((bsteps, n, n == steps))
 
-    ths = [threading.Thread(target=work, args=(sc,)) for sc in scenes]
-    for i in range(0, len(ths), threads):
-        batch = ths[i:i + threads]
-        for t in batch:
-            t.start()
-        for t in batch:
-            t.join()
+    ths = [threading.Thread(target=worker, args=(t,)) for t in range(threads)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
     bsteps = sum(r[0] for r in results)
-    el = max(r[1] for r in results) if results else 1.0
-    return bsteps / el, sum(r[2] for r in results)
+    el = max(per_thread) if results else 1.0
+    return bsteps / max(el, 1e-9), sum(r[1] for r in results), sum(1 for r in results if r[2])
 
 
-def cpu_sample(scenes, k: int):
-    """k scenes spread over the lower half of the size range (a bounded sample of the mix)."""
+def median_scene(scenes):
     order = np.argsort([s.n_bodies for s in scenes])
-    half = order[: max(1, len(order) // 2)]
-    pick = half[np.linspace(0, len(half) - 1, min(k, len(half))).astype(int)]
-    return [scenes[i] for i in pick]
+    return scenes[int(order[len(order) // 2])]
 
 
 def host_threads() -> int:
@@ -247,40 +266,58 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
+def cpu_name() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def reference_arm(args, rank, world, pg):
-    """The reference's CPU path, restated (the Rust/wasm reference cannot be built here), on every host thread."""
+    """The reference's CPU path, restated (the Rust/wasm reference cannot be built here), on every host thread: the
+    whole 256-scene mix, each scene stepped from rest over the same window as our arm (warm-up untimed)."""
     if rank != 0:
         return
+    from oracle import binding as orc
     from shatterforge_b200 import scenes as S
+    orc.use_native()
     scenes = S.config4_scenes(n_scenes=args.scenes, scale=args.scale)
     threads = host_threads()
-    sample = cpu_sample(scenes, threads)
     per = max(1.0, args.cpu_seconds)
-    rate, steps = cpu_body_steps(sample, args.warmup, args.steps, per, threads)
+    rate, steps, complete = cpu_body_steps(scenes, args.warmup, args.steps, per, threads)
     line = {
-        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": 0, "steps": int(steps),
-        "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded)",
         "config": {"workload": f"config4: {args.scenes} debris scenes, 1/60 s, {ITERS} iterations, 2 substeps",
-                   "sample": f"{len(sample)} scenes ({sum(s.n_bodies for s in sample)} bodies), steps {args.warmup}.."
-                             f"{args.warmup + args.steps} from rest, at most {per:.0f} s each"},
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{len(sample)} of {args.scenes} scenes (lower half of the sizes), one per thread, "
-                                   f"{steps} timed steps in all"},
+                   "sample": f"all {len(scenes)} scenes ({sum(s.n_bodies for s in scenes)} bodies), steps {args.warmup}.."
+                             f"{args.warmup + args.steps} from rest; {complete} scenes ran every step (at most "
+                             f"{per:.0f} s of timed stepping each)"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "cpu": cpu_name(),
+                         "order": "reference list order (src/lib.rs:1579-1601)", "build": "-O2 -march=native -ffp-contract=off",
+                         "sample": f"{len(scenes)} scenes over {threads} threads, largest first; {steps} timed scene-steps"},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------- our arm
-def run_steps(w, k: int):
-    """k world steps, one call each; returns (summed alive bodies, device ms from the library's events)."""
+def run_steps(w, k: int, awake_out: list | None = None):
+    """k world steps, one call each; returns (summed alive bodies, device ms from the library's events). The summed
+    awake bodies (after each step) go to awake_out[0] when given."""
     alive = 0
+    awake = 0
     ms = 0.0
     for _ in range(k):
         st = w.step(DT, 1)
         alive += st.alive
+        awake += st.awake
         ms += st.ms_last_step
+    if awake_out is not None:
+        awake_out.append(awake)
     return alive, ms
 
 
@@ -409,6 +446,72 @@ def serve_section(args):
                     "launches, on the same population and the first seconds of the same stream"}
 
 
+def plain_compare(sf, scenes, params, stream, args):
+    """The plain path (every scene its own world, stepped one scene per launch sequence) against the batched path over
+    the same steps from the same state: (a) the headline's window, steps warmup..warmup+K from rest (K at most
+    --plain-steps-window); (b) --plain-steps steps at the mix's contact peak (after --peak-step steps)."""
+    import torch
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        out = fn()
+        t1.record(stream); torch.cuda.synchronize()
+        return out, t0.elapsed_time(t1)
+
+    def window(wb, worlds, k):
+        acc = []
+        b_alive, _ = run_steps(wb, k, acc)
+        return b_alive, acc[0]
+
+    def plain_steps(worlds, k):
+        alive = awake = 0
+        for _ in range(k):
+            for pw in worlds:
+                st = pw.step(DT, 1)
+                alive += st.alive
+                awake += st.awake
+        return alive, awake
+
+    out = {}
+    wb = sf.World(scenes, **params)
+    wb.set_stream(stream.cuda_stream)
+    worlds = []
+    for sc in scenes:
+        pw = sf.World(sc, **params)
+        pw.set_stream(stream.cuda_stream)
+        worlds.append(pw)
+    # (a) from rest, the headline's window
+    run_steps(wb, args.warmup)
+    for pw in worlds:
+        run_steps(pw, args.warmup)
+    k = min(args.steps, args.plain_steps_window)
+    (b_alive, b_awake), b_ms = timed(lambda: window(wb, worlds, k))
+    (p_alive, p_awake), p_ms = timed(lambda: plain_steps(worlds, k))
+    out["window"] = {"steps": f"{args.warmup}..{args.warmup + k} from rest", "plain": p_alive / (p_ms * 1e-3),
+                     "batched": b_alive / (b_ms * 1e-3), "batched_over_plain": (b_alive / b_ms) / max(p_alive / p_ms, 1e-30),
+                     "awake_fraction": b_awake / max(b_alive, 1)}
+    # (b) at the contact peak, from the batched world's state
+    run_steps(wb, max(0, args.peak_step - args.warmup - k))
+    st, sl, fl = wb.bodies()
+    for j, pw in enumerate(worlds):
+        a, b = wb.body_off[j], wb.body_off[j + 1]
+        pw.set_bodies(st[a:b], sl[a:b], fl[a:b])
+    (b_alive, b_awake), b_ms = timed(lambda: window(wb, worlds, args.plain_steps))
+    (p_alive, p_awake), p_ms = timed(lambda: plain_steps(worlds, args.plain_steps))
+    out["peak"] = {"steps": f"{args.peak_step}..{args.peak_step + args.plain_steps}", "plain": p_alive / (p_ms * 1e-3),
+                   "batched": b_alive / (b_ms * 1e-3), "batched_over_plain": (b_alive / b_ms) / max(p_alive / p_ms, 1e-30),
+                   "awake_fraction": b_awake / max(b_alive, 1), "contacts": int(wb.stats().contacts)}
+    out["value"] = out["window"]["plain"]
+    out["unit"] = UNIT
+    out["note"] = "plain = each scene its own world and launches; batched = all scenes in one world, same steps, same state"
+    for pw in worlds:
+        pw.close()
+    wb.close()
+    return out
+
+
 def our_arm(args, rank, world, local, pg):
     import torch
 
@@ -434,9 +537,10 @@ def our_arm(args, rank, world, local, pg):
     barrier(pg, args)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    awake_acc = []
     with Clocks(dev) as clk:
         e0.record(stream)
-        alive_sum, _ = run_steps(w, args.steps)
+        alive_sum, _ = run_steps(w, args.steps, awake_acc)
         e1.record(stream)
         torch.cuda.synchronize()
     barrier(pg, args)
@@ -446,62 +550,43 @@ def our_arm(args, rank, world, local, pg):
     tuning = w.tuning()
     stats = w.stats()
     ms_max, alive_total, _ = combine(pg, ms, alive_sum)
+    awake_total = allreduce_sum(pg, float(awake_acc[0]))
     value = alive_total / (ms_max * 1e-3)
 
-    # roofline of the dominant phase
+    # roofline of the dominant phase's kernel: contact generation or the solve, whichever phase took longer;
+    # both are printed
     phase_ms = prof["ms"]
     top = max(phase_ms, key=phase_ms.get)
-    solve_ms = phase_ms["solve"]
-    solve_bytes = SOLVE_BYTES_PER_CONTACT_ITER * prof["solve_contact_iters"]
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     hbm = float(peaks.get("hbm_gbs", 6650.0))
-    per_launch_ms = solve_ms / max(prof["solve_launches"], 1)
-    achieved = solve_bytes / max(solve_ms * 1e-3, 1e-12) / 1e9
-    roofline = {"kernel": "k_solve (coloured sequential-impulse solve, persistent)", "bound": "hbm", "achieved": achieved,
-                "peak": hbm, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback", "unit": "GB/s",
-                "frac": achieved / hbm,
-                "traffic": (SOLVE_DRAM_BYTES_PER_CONTACT_ITER * prof["solve_contact_iters"] / max(prof["solve_launches"], 1)
-                            if SOLVE_DRAM_BYTES_PER_CONTACT_ITER else None),
-                "bytes_per_launch": solve_bytes / max(prof["solve_launches"], 1), "ms_per_launch": per_launch_ms,
-                "unit_bytes": f"{SOLVE_BYTES_PER_CONTACT_ITER} B per contact-iteration"}
-    state_after = w.bodies()
+    peak_source = "measured" if "hbm_gbs" in peaks else "fallback"
+    launches = max(int(prof["substeps"]), 1)
+    solve_ms = phase_ms["solve"]
+    solve_bytes = SOLVE_BYTES_PER_CONTACT_ITER * prof["solve_contact_iters"]
+    nsl = max(prof["solve_launches"], 1)
+    roof_solve = {"kernel": "k_solve (coloured sequential-impulse solve)", "bound": "hbm",
+                  "achieved": solve_bytes / max(solve_ms * 1e-3, 1e-12) / 1e9, "peak": hbm, "peak_source": peak_source,
+                  "unit": "GB/s", "traffic": SOLVE_DRAM_BYTES_PER_CONTACT_ITER * prof["solve_contact_iters"] / nsl,
+                  "bytes_per_launch": solve_bytes / nsl, "ms_per_launch": solve_ms / nsl, "launches": int(prof["solve_launches"]),
+                  "unit_bytes": f"{SOLVE_BYTES_PER_CONTACT_ITER} B per contact-iteration"}
+    roof_solve["frac"] = roof_solve["achieved"] / hbm
+    gen_bytes = GEN_BYTES_PER_BRICK * prof["gen_bricks"] + GEN_BYTES_PER_CONTACT * prof["contacts_sum"]
+    roof_gen = {"kernel": "k_contacts_gen (broad and narrow phase, one thread per awake brick)", "bound": "hbm",
+                "achieved": gen_bytes / max(prof["gen_ms"] * 1e-3, 1e-12) / 1e9, "peak": hbm, "peak_source": peak_source,
+                "unit": "GB/s", "traffic": GEN_DRAM_PER_ALGORITHMIC_BYTE * gen_bytes / launches,
+                "bytes_per_launch": gen_bytes / launches, "ms_per_launch": prof["gen_ms"] / launches, "launches": launches,
+                "unit_bytes": f"{GEN_BYTES_PER_BRICK} B per awake brick + {GEN_BYTES_PER_CONTACT} B per contact"}
+    roof_gen["frac"] = roof_gen["achieved"] / hbm
+    roofline = dict(roof_gen if phase_ms["contacts"] >= phase_ms["solve"] else roof_solve)
+    roofline["phase_share"] = max(phase_ms["contacts"], phase_ms["solve"]) / max(sum(phase_ms.values()), 1e-12)
+    rooflines = {"k_contacts_gen": roof_gen, "k_solve": roof_solve}
+    w.close()
 
-    # ---- plain path on the same simulated state: each scene alone, one launch sequence per scene
+    # ---- plain path: each scene alone, stepped by its own launches; over the headline's step window from rest, and
+    # for a few steps at the mix's contact peak, against the batched path over the same steps from the same state
     plain = None
     if not args.no_plain and rank == 0 and args.plain_steps > 0:
-        st, sl, fl = state_after
-        worlds = []
-        for k, sc in enumerate(scenes):
-            pw = sf.World(sc, **params)
-            pw.set_stream(stream.cuda_stream)
-            a, b = w.body_off[k], w.body_off[k + 1]
-            pw.set_bodies(st[a:b], sl[a:b], fl[a:b])
-            worlds.append(pw)
-        # the batched path over the same steps from the same state
-        wb = sf.World(scenes, **params)
-        wb.set_stream(stream.cuda_stream)
-        wb.set_bodies(st, sl, fl)
-        torch.cuda.synchronize()
-        t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
-        t0.record(stream)
-        b_alive, _ = run_steps(wb, args.plain_steps)
-        t1.record(stream); torch.cuda.synchronize()
-        b_ms = t0.elapsed_time(t1)
-        t0.record(stream)
-        p_alive = 0
-        for _ in range(args.plain_steps):
-            for pw in worlds:
-                p_alive += pw.step(DT, 1).alive
-        t1.record(stream); torch.cuda.synchronize()
-        p_ms = t0.elapsed_time(t1)
-        plain = {"value": p_alive / (p_ms * 1e-3), "unit": UNIT, "steps": args.plain_steps,
-                 "batched_same_steps": b_alive / (b_ms * 1e-3),
-                 "batched_over_plain": (b_alive / b_ms) / max(p_alive / p_ms, 1e-30),
-                 "note": "steps after the timed run, from the same state, each scene stepped by its own launches"}
-        for pw in worlds:
-            pw.close()
-        wb.close()
-    w.close()
+        plain = plain_compare(sf, scenes, params, stream, args)
 
     # ---- end to end through the C ABI with pinned host buffers
     e2e_steps = args.e2e_steps or args.steps
@@ -579,16 +664,21 @@ def our_arm(args, rank, world, local, pg):
         serve = serve_section(args)
 
     if not args.no_cpu and rank == 0:
-        one = cpu_sample(scenes, 1)
-        rate1, n1 = cpu_body_steps(one, args.warmup, args.steps, args.cpu_seconds, 1)
+        from oracle import binding as orc
+        cpu_colours = colour_comparison(scenes[:16], params)
+        orc.use_native()
+        med = median_scene(scenes)
+        rate1, n1, _ = cpu_body_steps([med], args.warmup, args.steps, args.cpu_seconds, 1)
         threads = host_threads()
-        many = cpu_sample(scenes, threads)
-        rate_n, n_n = cpu_body_steps(many, args.warmup, args.steps, args.cpu_seconds, threads)
-        cpu = {"value": rate1, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"1 scene ({one[0].n_bodies} bodies), steps {args.warmup}..{args.warmup + n1} from rest",
-               "all_cores": {"value": rate_n, "cores": min(threads, len(many)),
-                             "sample": f"{len(many)} scenes of the lower half of the sizes, one per thread, {n_n} timed steps in all"}}
-        cpu["colours"] = colour_comparison(scenes[:16], params)
+        rate_n, n_n, complete = cpu_body_steps(scenes, args.warmup, args.steps, args.cpu_seconds, threads)
+        cpu = {"value": rate1, "unit": UNIT, "cores": 1, "kind": "port", "cpu": cpu_name(),
+               "order": "reference list order (src/lib.rs:1579-1601)", "build": "-O2 -march=native -ffp-contract=off",
+               "sample": f"the median scene ({med.n_bodies} bodies), steps {args.warmup}..{args.warmup + n1} from rest",
+               "all_cores": {"value": rate_n, "cores": threads,
+                             "sample": f"all {len(scenes)} scenes, largest first over {threads} threads, steps "
+                                       f"{args.warmup}..{args.warmup + args.steps} from rest ({complete} scenes ran "
+                                       f"every step; {n_n} timed scene-steps)"},
+               "colours": cpu_colours}
 
     if rank != 0:
         return
@@ -604,7 +694,10 @@ def our_arm(args, rank, world, local, pg):
         "clocks": clocks,
         "e2e": e2e,
         "gpu_launches": int(prof["launches"]),
+        "awake_fraction": awake_total / max(alive_total, 1),
+        "awake_body_steps_per_s": awake_total / (ms_max * 1e-3),
         "roofline": roofline,
+        "rooflines": rooflines,
         "phases_ms": {k: round(v, 3) for k, v in phase_ms.items()},
         "top_phase": top,
         "autotune": {"blocks_per_sm_by_log2_size": tuning, "note": "launch shapes picked online per size bucket; "

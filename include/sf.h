@@ -109,6 +109,8 @@ typedef struct sf_profile {
     uint64_t solve_contact_iters;   /* sum over solve launches of contacts x iterations */
     uint64_t contacts_sum;          /* sum over substeps of contacts */
     uint64_t launches;
+    double gen_ms;                  /* device time of the contact-generation kernel alone (inside the contacts phase) */
+    uint64_t gen_bricks;            /* sum over its launches of the bricks it visited */
 } sf_profile;
 
 typedef struct sf_solve_report {
@@ -183,6 +185,30 @@ sf_status sf_structure_check(sf_world *w, int32_t structure, float dt, int32_t l
  * update_cache does, each body's weight shared over the listed structures' bricks under it and the ground, summed
  * per brick in body-then-brick order into extn, then ext = 0.8 ext + 0.2 extn. */
 sf_status sf_structure_loads(sf_world *w, const int32_t *structures, uint32_t n_structures);
+/* The reference's per-frame load-path schedule, with this library's red-black FP64 sweeps in place of its
+ * lexicographic f32 ones (the schedule's residual tests then see FP64 residuals):
+ *   sf_structure_warm    warm_struct (src/lib.rs:1061-1066): a structure not yet solved gets 560 warm-up sweeps pending
+ *                        and a settle timer that starts when they are done (once per structure)
+ *   sf_structure_frame   one frame: the sweep loop of `structural` (src/lib.rs:1268-1281) over the listed active
+ *                        structures, in order (omega 1.85; nmin sweeps by the residual of the structure's last sweep:
+ *                        below 1e-4 one on every third frame, counted by (frame + structure) % 3 == 0, else none;
+ *                        otherwise 1 for more than 15,000 bricks and 6 for fewer; then more while its residual is at
+ *                        least 4e-4, it has done fewer than 90 and a budget of 160,000 brick-updates shared in order
+ *                        is left), the settle timers (src/lib.rs:1334), then warm_step (src/lib.rs:1068-1079: pending
+ *                        warm-up sweeps in structure order from a budget of 120,000 brick-updates, omega 1.9 while
+ *                        more than 60 remain, then 1.0). Only structures passed to sf_structure_warm are swept.
+ * Joints are judged live (the `live` of sf_structure_check) once a structure's settle timer is <= 0 and its residual
+ * is below 1.5e-3 (src/lib.rs:1328); sf_read_structure_state returns both (n_structures entries each, any NULL). */
+typedef struct sf_frame_report {
+    uint32_t sweeps;            /* structural sweeps this frame, summed over structures */
+    uint32_t warm_sweeps;       /* warm-up sweeps this frame, summed over structures */
+    uint64_t brick_updates;     /* bricks x sweeps, both kinds */
+    double ms;                  /* device time of the frame's solves */
+} sf_frame_report;
+sf_status sf_structure_warm(sf_world *w, int32_t structure);
+sf_status sf_structure_frame(sf_world *w, uint32_t frame, float dt, const int32_t *active, uint32_t n_active,
+                             sf_frame_report *report);
+sf_status sf_read_structure_state(sf_world *w, int32_t *warm, uint8_t *solved, float *settle, double *resid);
 /* Per-structure sweeps and final residuals of the last sf_structure_solve (n_structures entries each). */
 sf_status sf_read_solve_detail(sf_world *w, uint32_t *sweeps, double *resid);
 

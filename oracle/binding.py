@@ -92,6 +92,9 @@ def load() -> C.CDLL:
     lib.ow_get_phi.argtypes = [C.c_void_p, _f32p]
     lib.ow_get_phi64.argtypes = [C.c_void_p, _f64p]
     lib.ow_set_phi.argtypes = [C.c_void_p, _f32p]
+    lib.ow_structure_warm.argtypes = [C.c_void_p, C.c_int32]
+    lib.ow_structure_frame.argtypes = [C.c_void_p, C.c_uint32, C.c_float, _i32p, C.c_uint32, _u32p]
+    lib.ow_structure_state.argtypes = [C.c_void_p, _i32p, _u8p, _f32p, C.POINTER(C.c_double)]
     lib.ow_set_ext.argtypes = [C.c_void_p, _f32p]
     lib.ow_stress.restype = C.c_uint64
     lib.ow_stress.argtypes = [C.c_void_p, C.c_int32, C.c_float, C.c_int32, C.c_uint64, _u32p, _f32p, _f32p]
@@ -200,6 +203,22 @@ class OracleWorld:
         sw = C.c_uint32()
         r = self.lib.ow_sor(self.h, int(structure), float(omega), float(tol), int(max_sweeps), int(mode), C.byref(sw))
         return sw.value, r
+
+    def structure_warm(self, s):
+        self.lib.ow_structure_warm(self.h, int(s))
+
+    def structure_frame(self, frame, dt, active):
+        a = np.ascontiguousarray(active, np.int32)
+        out = np.zeros(2, np.uint32)
+        self.lib.ow_structure_frame(self.h, int(frame), float(dt), _p(a, C.c_int32), len(a), _p(out, C.c_uint32))
+        return int(out[0]), int(out[1])
+
+    def structure_state(self, n):
+        warm = np.zeros(n, np.int32); solved = np.zeros(n, np.uint8); settle = np.zeros(n, np.float32)
+        resid = np.zeros(n, np.float64)
+        self.lib.ow_structure_state(self.h, _p(warm, C.c_int32), _p(solved, C.c_uint8), _p(settle, C.c_float),
+                                    resid.ctypes.data_as(C.POINTER(C.c_double)))
+        return warm, solved, settle, resid
 
     def phi(self):
         p = np.zeros(self.ns, np.float32)

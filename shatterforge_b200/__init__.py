@@ -71,7 +71,8 @@ PHASE_NAMES = ["pose", "hash", "contacts", "manifolds", "colour", "prep", "solve
 
 class Profile(C.Structure):
     _fields_ = [("ms", C.c_double * SF_PHASES), ("substeps", C.c_uint64), ("solve_launches", C.c_uint64),
-                ("solve_contact_iters", C.c_uint64), ("contacts_sum", C.c_uint64), ("launches", C.c_uint64)]
+                ("solve_contact_iters", C.c_uint64), ("contacts_sum", C.c_uint64), ("launches", C.c_uint64),
+                ("gen_ms", C.c_double), ("gen_bricks", C.c_uint64)]
 
 
 class SolveReport(C.Structure):
@@ -82,6 +83,10 @@ class SolveReport(C.Structure):
 class CheckReport(C.Structure):
     _fields_ = [("joints", C.c_uint64), ("over", C.c_uint64), ("failed", C.c_uint64), ("crushed", C.c_uint64),
                 ("max_ratio", C.c_float), ("ms", C.c_double)]
+
+
+class FrameReport(C.Structure):
+    _fields_ = [("sweeps", C.c_uint32), ("warm_sweeps", C.c_uint32), ("brick_updates", C.c_uint64), ("ms", C.c_double)]
 
 
 class WorldInfo(C.Structure):
@@ -141,6 +146,9 @@ PROTOTYPES = {
     "sf_structure_solve": (C.c_int32, [C.c_void_p, C.c_int32, C.c_float, C.c_float, C.c_uint32, C.POINTER(SolveReport)]),
     "sf_structure_check": (C.c_int32, [C.c_void_p, C.c_int32, C.c_float, C.c_int32, C.POINTER(CheckReport)]),
     "sf_read_solve_detail": (C.c_int32, [C.c_void_p, _u32p, C.POINTER(C.c_double)]),
+    "sf_structure_warm": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "sf_structure_frame": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_float, _i32p, C.c_uint32, C.POINTER(FrameReport)]),
+    "sf_read_structure_state": (C.c_int32, [C.c_void_p, _i32p, _u8p, _f32p, C.POINTER(C.c_double)]),
     "sf_structure_loads": (C.c_int32, [C.c_void_p, _i32p, C.c_uint32]),
     "sf_world_get_info": (C.c_int32, [C.c_void_p, C.POINTER(WorldInfo)]),
     "sf_get_stats": (C.c_int32, [C.c_void_p, C.POINTER(Stats)]),
@@ -349,7 +357,8 @@ class World:
         p = Profile()
         _check(self._lib.sf_read_profile(self._h, C.byref(p)), "sf_read_profile")
         return {"ms": dict(zip(PHASE_NAMES, list(p.ms))), "substeps": p.substeps, "solve_launches": p.solve_launches,
-                "solve_contact_iters": p.solve_contact_iters, "contacts_sum": p.contacts_sum, "launches": p.launches}
+                "solve_contact_iters": p.solve_contact_iters, "contacts_sum": p.contacts_sum, "launches": p.launches,
+                "gen_ms": p.gen_ms, "gen_bricks": p.gen_bricks}
 
     def tuning(self) -> dict:
         """Blocks per SM the autotuner settled on, per size bucket (log2 of work items), for each tuned kernel."""
@@ -393,6 +402,28 @@ class World:
         rs = np.zeros(max(n, 1), np.float64)
         _check(self._lib.sf_read_solve_detail(self._h, _ptr(sw, C.c_uint32), _ptr(rs, C.c_double)), "sf_read_solve_detail")
         return sw[:n], rs[:n]
+
+    def structure_warm(self, structure: int):
+        """warm_struct: 560 warm-up sweeps pending for a structure not yet solved (once)."""
+        _check(self._lib.sf_structure_warm(self._h, int(structure)), "sf_structure_warm")
+
+    def structure_frame(self, frame: int, active, dt: float = 1.0 / 60.0) -> FrameReport:
+        """One frame of the reference's load-path schedule over the listed active structures (sf_structure_frame)."""
+        a = np.ascontiguousarray(active, np.int32)
+        r = FrameReport()
+        _check(self._lib.sf_structure_frame(self._h, int(frame), float(dt), _ptr(a, C.c_int32), len(a), C.byref(r)),
+               "sf_structure_frame")
+        return r
+
+    def structure_state(self):
+        """Per structure: pending warm-up sweeps, solved flag, settle timer, residual of its last sweep."""
+        n = max(self.info.n_structures, 1)
+        warm = np.zeros(n, np.int32); solved = np.zeros(n, np.uint8); settle = np.zeros(n, np.float32)
+        resid = np.zeros(n, np.float64)
+        _check(self._lib.sf_read_structure_state(self._h, _ptr(warm, C.c_int32), _ptr(solved, C.c_uint8),
+                                                 _ptr(settle, C.c_float), _ptr(resid, C.c_double)), "sf_read_structure_state")
+        k = self.info.n_structures
+        return warm[:k], solved[:k], settle[:k], resid[:k]
 
     def structure_check(self, structure: int = -1, dt: float = 1.0 / 60.0, live: bool = True) -> CheckReport:
         r = CheckReport()

@@ -27,7 +27,10 @@
 
 namespace sf {
 
-struct SorParams { double omega, tol; uint32_t max_sweeps, pad; };
+// omega, tolerance and sweep limit of a solve, read from device memory (so a captured graph serves every solve of its
+// shape); use_cap != 0: structure q also stops after cap[q] sweeps (the per-frame schedules give each structure
+// its own count)
+struct SorParams { double omega, tol; uint32_t max_sweeps, use_cap; };
 
 struct SorState {
     DBuf<double> cphi;
@@ -65,6 +68,9 @@ struct SorState {
     // the cluster path: one thread-block cluster per structure, the structure's cells in the cluster's shared memory
     bool cl_ready = false;
     std::vector<uint32_t> h_cl_n, h_cl_per;
+    // per structure: its height in cells, and the sweeps its last solve took (0 = none yet); the launch split puts
+    // the structures expected to take longest on the larger blocks
+    std::vector<uint32_t> h_st_height, h_last_sweeps;
     DBuf<uint32_t> cl_cpos, cl_off, cl_n, cl_per, cl_even, cl_list;
     DBuf<uint16_t> cl_nbr;
     uint64_t cluster_solves = 0;
@@ -73,6 +79,13 @@ struct SorState {
     cudaStream_t aux = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
     DBuf<SorParams> prm;
+    DBuf<uint32_t> cap;             // per structure: its own sweep limit when SorParams::use_cap is set
+    // the reference's per-frame schedule (src/lib.rs:1061-1079, 1268-1281): per structure its pending warm-up
+    // sweeps, whether it has been solved (warmed), its settle timer and the residual of its last sweep
+    std::vector<int32_t> h_warm;
+    std::vector<uint8_t> h_solved;
+    std::vector<float> h_settle;
+    std::vector<double> h_resid;
     std::vector<Graph> graphs;
     bool graphs_ok = true;
     uint64_t graph_launches = 0;
@@ -167,6 +180,7 @@ constexpr int SOR_BLOCK = 256;
 constexpr int SOR_MAX_LOCAL_STRUCT = 8192;   // active flags kept in shared memory as bits
 
 struct SorArgs {
+    const uint32_t *cap;
     double *cphi;
     const float *crhs;
     const uint32_t *ccode;
@@ -305,7 +319,8 @@ __global__ void __launch_bounds__(SOR_BLOCK) k_sor_redblack(SorArgs A) {
             if (!is_active(act, (int32_t)s)) continue;
             const double r = __longlong_as_double((long long)__ldcg(&md[s])) / __longlong_as_double((long long)__ldcg(&mp[s]));
             if (blockIdx.x == 0) { A.sweeps[s] = sweep + 1; A.resid[s] = r; }
-            if (r < tol || sweep + 1 >= max_sweeps) atomicAnd(&act[s >> 5], ~(1u << (s & 31)));
+            const uint32_t lim = (A.prm && A.prm->use_cap && A.cap) ? min(max_sweeps, A.cap[s]) : max_sweeps;
+            if (r < tol || sweep + 1 >= lim) atomicAnd(&act[s >> 5], ~(1u << (s & 31)));
             else s_any = 1;
         }
         __syncthreads();
@@ -330,6 +345,7 @@ constexpr uint32_t CELL_ACTIVE = 1u << 31;
 constexpr uint16_t NO_CELL = 0xFFFFu;
 
 struct SorClusterArgs {
+    const uint32_t *cap;                         // per structure sweep limits (when prm->use_cap)
     const uint32_t *list;                        // the structure of each cluster
     const uint32_t *off, *n, *per, *even;        // per structure; even: per (structure, block)
     const uint32_t *cpos;                        // per listed cell: its place in the chunk layout
@@ -390,7 +406,7 @@ __global__ void __launch_bounds__(SOR_CL_MAX_THREADS) k_sor_cluster(SorClusterAr
         for (int d = 0; d < 6; d++) nbr[i * 6 + d] = A.nbr[(size_t)g * 6 + d];
     }
     const double omega = A.prm->omega, tol = A.prm->tol;
-    const uint32_t max_sweeps = A.prm->max_sweeps;
+    const uint32_t max_sweeps = A.prm->use_cap ? min(A.prm->max_sweeps, A.cap[q]) : A.prm->max_sweeps;
     double r_last = 0.0;
     uint32_t done = 0;
     cl.sync();
@@ -440,22 +456,34 @@ __global__ void __launch_bounds__(SOR_CL_MAX_THREADS) k_sor_cluster(SorClusterAr
         if ((tid & 31) == 0) { wd[tid >> 5] = accd; wp[tid >> 5] = accp; }
         __syncthreads();
         const uint32_t slot = sweep & 1u;
-        if (tid == 0) {
-            unsigned long long dm = 0ull, pm = one;
-            for (uint32_t k = 0; k < blockDim.x / 32; k++) { dm = max(dm, wd[k]); pm = max(pm, wp[k]); }
-            blk_d[slot] = dm;
-            blk_p[slot] = pm;
+        // the block's maxima: warp 0 reduces the warps' values with shuffles (max is exact in any order)
+        if (tid < 32) {
+            const uint32_t nw = blockDim.x / 32;
+            unsigned long long dm = tid < nw ? wd[tid] : 0ull, pm = tid < nw ? wp[tid] : one;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                dm = max(dm, __shfl_xor_sync(0xffffffffu, dm, o));
+                pm = max(pm, __shfl_xor_sync(0xffffffffu, pm, o));
+            }
+            if (tid == 0) { blk_d[slot] = dm; blk_p[slot] = pm; }
         }
         cl.sync();
-        if (tid == 0) {
+        // the cluster's maxima: lane b of warp 0 reads block b's slot (the eight remote reads in flight together)
+        if (tid < 32) {
             unsigned long long dm = 0ull, pm = one;
-#pragma unroll
-            for (uint32_t b = 0; b < (uint32_t)SOR_CL; b++) {
-                dm = max(dm, cl.map_shared_rank(blk_d, b)[slot]);
-                pm = max(pm, cl.map_shared_rank(blk_p, b)[slot]);
+            if (tid < (uint32_t)SOR_CL) {
+                dm = cl.map_shared_rank(blk_d, tid)[slot];
+                pm = cl.map_shared_rank(blk_p, tid)[slot];
             }
-            r_last = __longlong_as_double((long long)dm) / __longlong_as_double((long long)pm);
-            s_stop = (r_last < tol || sweep + 1 >= max_sweeps) ? 1 : 0;
+#pragma unroll
+            for (int o = 4; o > 0; o >>= 1) {
+                dm = max(dm, __shfl_xor_sync(0xffffffffu, dm, o));
+                pm = max(pm, __shfl_xor_sync(0xffffffffu, pm, o));
+            }
+            if (tid == 0) {
+                r_last = __longlong_as_double((long long)dm) / __longlong_as_double((long long)pm);
+                s_stop = (r_last < tol || sweep + 1 >= max_sweeps) ? 1 : 0;
+            }
         }
         done = sweep + 1;
         __syncthreads();
@@ -738,6 +766,11 @@ sf_status sor_create(sf_world *w) {
         }
     }
     SF_CUDA(st->prm.alloc(1));
+    SF_CUDA(st->cap.alloc(std::max<uint32_t>(nst, 1)));
+    st->h_warm.assign(nst, 0);
+    st->h_solved.assign(nst, 0);
+    st->h_settle.assign(nst, 0.0f);
+    st->h_resid.assign(nst, 0.0);
     SF_CUDA(st->chunk_nbr.alloc(nbr.size()));
     if (!nbr.empty()) SF_CUDA(cudaMemcpyAsync(st->chunk_nbr.p, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice, s));
     // chunks of each structure
@@ -817,7 +850,7 @@ cudaError_t sor_solve_on_buffers(const SorBuffers &B, uint32_t n_bricks, uint32_
     A.cphi = B.cphi; A.crhs = B.crhs; A.ccode = B.ccode; A.csid = B.csid; A.chunk_nbr = B.chunk_nbr; A.chunk_sid = B.chunk_sid;
     A.work = B.work; A.n_work = n_chunks; A.n_struct = 1; A.active0 = B.active0; A.resid_buf = B.resid_buf;
     A.sweeps = B.sweeps; A.resid = B.resid; A.omega = (double)omega; A.tol = (double)tol; A.max_sweeps = max_sweeps;
-    A.prm = nullptr; A.gb = B.gb; A.err = B.err;
+    A.prm = nullptr; A.cap = nullptr; A.gb = B.gb; A.err = B.err;
     unsigned grid = (unsigned)std::min<size_t>(n_chunks, (size_t)sms * std::max(occ, 1));
     void *args[] = {&A};
     if ((e = cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s)) != cudaSuccess) return e;
@@ -915,6 +948,8 @@ static sf_status sor_cluster_tables(sf_world *w) {
     std::vector<uint16_t> nbr;
     st->h_cl_n.assign(nst, 0);
     st->h_cl_per.assign(nst, 0);
+    st->h_st_height.assign(nst, 0);
+    st->h_last_sweeps.assign(nst, 0);
     std::vector<uint32_t> off(std::max<uint32_t>(nst, 1), 0), cnt(std::max<uint32_t>(nst, 1), 0), per(std::max<uint32_t>(nst, 1), 0);
     const int D[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
     for (uint32_t q = 0; q < nst; q++) {
@@ -957,6 +992,13 @@ static sf_status sor_cluster_tables(sf_world *w) {
         }
         st->h_cl_n[q] = n;
         st->h_cl_per[q] = pr;
+        int ylo = NY, yhi = -1;
+        for (uint32_t k = 0; k < n; k++) {
+            int x, y, z;
+            unpack_cell(w->h_s_cell[b[k]], x, y, z);
+            ylo = std::min(ylo, y); yhi = std::max(yhi, y);
+        }
+        st->h_st_height[q] = (uint32_t)(yhi - ylo + 1);
     }
     // places in the chunk layout as chunk * 512 + cell
     for (uint32_t &c : cpos) c = (c >> 9) * 512 + (c & 511);
@@ -983,8 +1025,9 @@ static sf_status sor_cluster_tables(sf_world *w) {
     return SF_OK;
 }
 
+// caps (optional, n_struct entries): structure q stops after at most caps[q] sweeps (max_sweeps bounds them all)
 static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, uint32_t n_ids, float omega, float tol,
-                            uint32_t max_sweeps, sf_solve_report *report) {
+                            uint32_t max_sweeps, sf_solve_report *report, const uint32_t *caps = nullptr) {
     if (!w) return SF_ERR_ARG;
     if (!w->sor) { set_error("this world holds no load-path state (a scene pool)"); return SF_ERR_STATE; }
     if (!(omega > 0.0f && omega < 2.0f)) { set_error("omega %g outside (0, 2)", (double)omega); return SF_ERR_ARG; }
@@ -1012,13 +1055,30 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     // an SM), side by side, so that all clusters are resident at once
     uint32_t n_big = 0, per_big = 0, per_small = 0;
     if (use_cl) {
-        // largest structures first: their clusters start before the small ones when not all fit at once
-        cl_order = req;
-        std::stable_sort(cl_order.begin(), cl_order.end(), [&](uint32_t a, uint32_t b) { return st->h_cl_n[a] > st->h_cl_n[b]; });
-        for (uint32_t q : cl_order) {
-            if (st->h_cl_per[q] > SOR_CL_SPLIT) { n_big++; per_big = std::max(per_big, st->h_cl_per[q]); }
-            else per_small = std::max(per_small, st->h_cl_per[q]);
+        // Critical path first. A structure's solve takes its sweeps times its time per sweep, and the sweeps are
+        // known from its last solve (a first solve guesses them from its height). The large blocks (1,024 threads)
+        // take every structure of more than SOR_CL_SPLIT cells a block, and also each small one that would be
+        // among the slowest on 256 threads; within each launch the slowest clusters are listed first, so they
+        // start first when not all are resident at once.
+        auto expect = [&](uint32_t q) -> double {
+            return st->h_last_sweeps[q] ? (double)st->h_last_sweeps[q] : 60.0 * std::max<uint32_t>(st->h_st_height[q], 1);
+        };
+        auto cost_small = [&](uint32_t q) { return expect(q) * (1.0 + std::ceil(st->h_cl_per[q] / 512.0)); };
+        auto cost_large = [&](uint32_t q) { return expect(q) * (1.0 + std::ceil(st->h_cl_per[q] / 2048.0)); };
+        double worst = 0.0;
+        for (uint32_t q : req) worst = std::max(worst, st->h_cl_per[q] > SOR_CL_SPLIT ? cost_large(q) : cost_small(q));
+        std::vector<uint32_t> big, small;
+        for (uint32_t q : req) {
+            const bool large = st->h_cl_per[q] > SOR_CL_SPLIT || cost_small(q) >= 0.5 * worst;
+            (large ? big : small).push_back(q);
         }
+        std::stable_sort(big.begin(), big.end(), [&](uint32_t a, uint32_t b) { return cost_large(a) > cost_large(b); });
+        std::stable_sort(small.begin(), small.end(), [&](uint32_t a, uint32_t b) { return cost_small(a) > cost_small(b); });
+        cl_order = big;
+        cl_order.insert(cl_order.end(), small.begin(), small.end());
+        n_big = (uint32_t)big.size();
+        for (uint32_t q : big) per_big = std::max(per_big, st->h_cl_per[q]);
+        for (uint32_t q : small) per_small = std::max(per_small, st->h_cl_per[q]);
         if (n_big == 0 || n_big == cl_order.size()) { n_big = 0; per_small = 0; }   // one launch
         SF_CUDA(cudaMemcpyAsync(st->cl_list.p, cl_order.data(), cl_order.size() * 4, cudaMemcpyHostToDevice, s));
         if (n_big && !st->aux) {
@@ -1037,7 +1097,9 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     A.active0 = st->active0.p; A.resid_buf = st->resid_buf.p; A.sweeps = st->sweeps.p; A.resid = st->resid.p;
     A.omega = (double)omega; A.tol = (double)tol; A.max_sweeps = max_sweeps; A.gb = w->barrier.p; A.err = w->err.p;
     A.prm = st->prm.p;
-    const SorParams hp{(double)omega, (double)tol, max_sweeps, 0u};
+    A.cap = st->cap.p;
+    if (caps) SF_CUDA(cudaMemcpyAsync(st->cap.p, caps, (size_t)nst * 4, cudaMemcpyHostToDevice, s));
+    const SorParams hp{(double)omega, (double)tol, max_sweeps, caps ? 1u : 0u};
     SF_CUDA(cudaMemcpyAsync(st->prm.p, &hp, sizeof hp, cudaMemcpyHostToDevice, s));
     int tci = -1;
     const int tb = Tuner::bucket(chunks.size());
@@ -1047,6 +1109,7 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     const uint32_t n_launch = use_cl ? (uint32_t)req.size() : A.n_work;
     void *args[] = {&A};
     SorClusterArgs CA;
+    CA.cap = st->cap.p;
     CA.list = st->cl_list.p; CA.off = st->cl_off.p; CA.n = st->cl_n.p; CA.per = st->cl_per.p; CA.even = st->cl_even.p;
     CA.cpos = st->cl_cpos.p; CA.nbr = st->cl_nbr.p; CA.cphi = st->cphi.p; CA.crhs = st->crhs.p; CA.ccode = st->ccode.p;
     CA.csid = st->csid.p; CA.per_max = n_big ? per_big : per_max; CA.prm = st->prm.p; CA.sweeps = st->sweeps.p;
@@ -1059,7 +1122,7 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     cattr[0].val.clusterDim.x = SOR_CL; cattr[0].val.clusterDim.y = 1; cattr[0].val.clusterDim.z = 1;
     cudaLaunchConfig_t ccfg = {}, scfg = {};
     ccfg.gridDim = dim3((unsigned)((n_big ? n_big : req.size()) * SOR_CL));
-    ccfg.blockDim = dim3(sor_cl_threads(CA.per_max));
+    ccfg.blockDim = dim3(n_big ? (unsigned)SOR_CL_MAX_THREADS : sor_cl_threads(CA.per_max));
     ccfg.dynamicSmemBytes = (size_t)CA.per_max * SOR_CL_BYTES_PER_CELL;
     ccfg.stream = s;
     ccfg.attrs = cattr;
@@ -1132,6 +1195,8 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     rep.ms = ms;
     for (uint32_t q : req) {
         rep.structures++;
+        if (!caps && q < st->h_last_sweeps.size() && e == SF_OK) st->h_last_sweeps[q] = sw[q];
+        if (e == SF_OK && sw[q]) st->h_resid[q] = rs[q];
         rep.max_sweeps_done = std::max(rep.max_sweeps_done, sw[q]);
         rep.brick_sweeps += (uint64_t)sw[q] * st->h_st_count[q];
         rep.max_residual = std::max(rep.max_residual, (double)rs[q]);
@@ -1154,6 +1219,126 @@ extern "C" {
 sf_status sf_structure_solve(sf_world *w, int32_t structure, float omega, float tol, uint32_t max_sweeps,
                              sf_solve_report *report) {
     return solve_impl(w, structure, nullptr, 0, omega, tol, max_sweeps, report);
+}
+
+sf_status sf_structure_warm(sf_world *w, int32_t structure) {
+    if (!w || !w->sor) { set_error("no load-path state"); return SF_ERR_ARG; }
+    SorState *st = w->sor;
+    if (structure < 0 || (uint32_t)structure >= w->n_struct) { set_error("structure %d out of range", structure); return SF_ERR_ARG; }
+    // warm_struct (src/lib.rs:1061-1066): 560 warm-up sweeps pending, once per structure
+    if (st->h_solved[structure]) return SF_OK;
+    st->h_solved[structure] = 1;
+    st->h_warm[structure] = 560;
+    st->h_settle[structure] = 1e9f;
+    return SF_OK;
+}
+
+sf_status sf_structure_frame(sf_world *w, uint32_t frame, float dt, const int32_t *active, uint32_t n_active,
+                             sf_frame_report *report) {
+    if (!w || !w->sor || (n_active && !active)) { set_error("null argument"); return SF_ERR_ARG; }
+    SorState *st = w->sor;
+    const uint32_t nst = w->n_struct;
+    sf_frame_report rep{};
+    float ms_total = 0.0f;
+    auto size_of = [&](uint32_t q) -> int64_t { return (int64_t)st->h_st_count[q]; };
+    // one solve of the listed structures, structure q stopping after caps[q] sweeps (or at tol)
+    auto run = [&](std::vector<uint32_t> &caps, const std::vector<int32_t> &ids, float omega, float tol) -> sf_status {
+        if (ids.empty()) return SF_OK;
+        uint32_t mx = 0;
+        for (int32_t q : ids) mx = std::max(mx, caps[q]);
+        if (mx == 0) return SF_OK;
+        sf_solve_report r{};
+        sf_status e = solve_impl(w, -1, ids.data(), (uint32_t)ids.size(), omega, tol, mx, &r, caps.data());
+        if (e != SF_OK) return e;
+        rep.brick_updates += r.brick_sweeps;
+        ms_total += (float)r.ms;
+        return SF_OK;
+    };
+    std::vector<uint32_t> caps(std::max<uint32_t>(nst, 1), 0);
+    std::vector<uint32_t> sw(std::max<uint32_t>(nst, 1));
+    std::vector<double> rs(std::max<uint32_t>(nst, 1));
+    // structural's sweep loop (src/lib.rs:1268-1281) over the active, solved structures in the given order: every
+    // structure takes its nmin sweeps at omega 1.85 (nmin from the residual of its last sweep: 1 or 0 every third
+    // frame once below 1e-4, else 1 for more than 15,000 bricks, else 6), then, in order, continues while its
+    // residual is at least 4e-4, it has done fewer than 90 sweeps and the shared budget of 160,000 brick-updates
+    // is not spent. The nmin sweeps of all structures run in one launch (their order cannot change them); each
+    // continuation runs alone, because the budget it may use depends on the structures before it.
+    std::vector<int32_t> act;
+    for (uint32_t k = 0; k < n_active; k++) {
+        const int32_t q = active[k];
+        if (q < 0 || (uint32_t)q >= nst) { set_error("structure %d out of range", q); return SF_ERR_ARG; }
+        if (st->h_solved[q] && st->h_st_count[q]) act.push_back(q);
+    }
+    std::vector<uint32_t> nmin(std::max<uint32_t>(nst, 1), 0);
+    std::vector<int32_t> first;
+    for (int32_t q : act) {
+        const double r = st->h_resid[q];
+        nmin[q] = r < 1e-4 ? (((frame + (uint32_t)q) % 3 == 0) ? 1u : 0u) : (size_of(q) > 15000 ? 1u : 6u);
+        if (nmin[q]) { caps[q] = nmin[q]; first.push_back(q); }
+    }
+    sf_status e = run(caps, first, 1.85f, 0.0f);
+    if (e != SF_OK) return e;
+    for (int32_t q : first) rep.sweeps += nmin[q];
+    int64_t budget = 160000;
+    for (int32_t q : act) {
+        if (!nmin[q]) continue;
+        const int64_t size = size_of(q);
+        budget -= (int64_t)nmin[q] * size;
+        uint32_t n = nmin[q];
+        if (st->h_resid[q] < (double)4e-4f || n >= 90 || budget <= 0) continue;
+        const uint32_t more = (uint32_t)std::min<int64_t>(90 - n, (budget + size - 1) / size);
+        std::fill(caps.begin(), caps.end(), 0u);
+        caps[q] = more;
+        const uint64_t before = rep.brick_updates;
+        e = run(caps, std::vector<int32_t>{q}, 1.85f, 4e-4f);
+        if (e != SF_OK) return e;
+        const uint32_t done = (uint32_t)((rep.brick_updates - before) / (uint64_t)std::max<int64_t>(size, 1));
+        rep.sweeps += done;
+        budget -= (int64_t)done * size;
+    }
+    // structural's settle timers (src/lib.rs:1334): a structure whose warm-up is over settles for 0.3 s; its joints
+    // are judged live once settled with a residual below 1.5e-3 (src/lib.rs:1328; sf_read_structure_state)
+    for (int32_t q : act)
+        if (st->h_settle[q] > 0.0f && st->h_warm[q] == 0) st->h_settle[q] -= dt;
+    // warm_step (src/lib.rs:1068-1079): the pending warm-up sweeps of every structure in structure order, from a
+    // budget of 120,000 brick-updates: omega 1.9 while more than 60 remain, then 1.0; no residual test. The counts
+    // follow from the sizes alone, so every structure's 1.9-sweeps run in one launch and its 1.0-sweeps in another.
+    std::vector<uint32_t> c19(std::max<uint32_t>(nst, 1), 0), c10(std::max<uint32_t>(nst, 1), 0);
+    std::vector<int32_t> w19, w10;
+    int64_t wb = 120000;
+    for (uint32_t q = 0; q < nst; q++) {
+        if (st->h_warm[q] <= 0 || wb <= 0 || !st->h_st_count[q]) continue;
+        const int64_t size = size_of(q);
+        const uint32_t k = (uint32_t)std::min<int64_t>(st->h_warm[q], (wb + size - 1) / size);
+        const uint32_t hi = (uint32_t)std::max<int32_t>(0, st->h_warm[q] - 60);
+        c19[q] = std::min(k, hi);
+        c10[q] = k - c19[q];
+        if (c19[q]) w19.push_back((int32_t)q);
+        if (c10[q]) w10.push_back((int32_t)q);
+        wb -= (int64_t)k * size;
+        st->h_warm[q] -= (int32_t)k;
+        rep.warm_sweeps += k;
+        if (st->h_warm[q] == 0) st->h_settle[q] = 0.3f;
+    }
+    e = run(c19, w19, 1.9f, 0.0f);
+    if (e != SF_OK) return e;
+    e = run(c10, w10, 1.0f, 0.0f);
+    if (e != SF_OK) return e;
+    rep.ms = ms_total;
+    if (report) *report = rep;
+    return SF_OK;
+}
+
+sf_status sf_read_structure_state(sf_world *w, int32_t *warm, uint8_t *solved, float *settle, double *resid) {
+    if (!w || !w->sor) { set_error("no load-path state"); return SF_ERR_ARG; }
+    SorState *st = w->sor;
+    for (uint32_t q = 0; q < w->n_struct; q++) {
+        if (warm) warm[q] = st->h_warm[q];
+        if (solved) solved[q] = st->h_solved[q];
+        if (settle) settle[q] = st->h_settle[q];
+        if (resid) resid[q] = st->h_resid[q];
+    }
+    return SF_OK;
 }
 
 sf_status sf_structure_solve_set(sf_world *w, const int32_t *structures, uint32_t n, float omega, float tol,

@@ -40,7 +40,7 @@ struct StepState {
     bool use_sparse = false, last_sparse = false;
     DBuf<uint2> brange;
     DBuf<float4> srec;
-    DBuf<uint32_t> sinfo;
+    DBuf<uint32_t> sinfo, scell;
     DBuf<uint4> slot_id;
     DBuf<float4> slot_p, slot_n;
     // contacts, list order
@@ -57,7 +57,16 @@ struct StepState {
     DBuf<uint32_t> bm_count, bm_start, bm_fill, bm_list;
     DBuf<uint32_t> masks, vmasks;
     DBuf<uint32_t> wl0, wl1;
-    DBuf<uint32_t> col_count, col_hstart, col_start, col_fill, col_list, jds_off;
+    DBuf<uint32_t> col_count, col_hstart, col_start, col_fill, col_list, jds_off, seg_tot, seg_base;
+    // sync domains: contiguous runs of active scenes, each coloured and solved by its own blocks with its own barrier
+    // (scenes never share a body, so no colour or round of one domain waits for another's)
+    DBuf<uint32_t> dom_of_act, man_dom, dom_m0, dom_m1, dom_ncol, dom_cnt;
+    DBuf<uint4> blk_dom;           // per block of the colouring / solve launch: domain, rank in it, its block count
+    DBuf<GridBarrier> dom_gb;
+    struct Partition { unsigned R = 0; uint32_t D = 0; std::vector<uint4> blk; std::vector<uint32_t> dom_of_act; };
+    std::vector<Partition> parts;  // by launch size, for the current active set
+    uint32_t part_D = 1;           // domains of the partition in use this substep
+    int part_in_use = -1;          // which of `parts` the device tables hold
     // islands
     DBuf<uint32_t> parent, label, mint;
     // per-scene body offsets (for scene-local priorities)
@@ -81,7 +90,7 @@ struct StepState {
     int solve_occ = 1, jp_occ = 1;
     uint32_t max_scene_bodies = 0;
     // launch-shape tuning: pending timings of this step's tuned launches
-    Tuner solve_t, jp_t;
+    Tuner solve_t;
     struct Pending { Tuner *t; int bucket, ci; cudaEvent_t e0, e1; };
     std::vector<Pending> pending;
     std::vector<cudaEvent_t> tev;
@@ -94,6 +103,11 @@ struct StepState {
     std::vector<uint32_t> sub_nc;
     double ph_ms[SF_PHASES] = {};
     uint64_t ph_substeps = 0, solve_contact_iters = 0, solve_launches = 0;
+    // contact generation alone: an event pair per launch, folded in with the phases
+    std::vector<cudaEvent_t> gen_ev;
+    size_t gen_used = 0;
+    double gen_ms = 0.0;
+    uint64_t gen_bricks = 0;
 };
 
 static void prof_mark(sf_world *w) {
@@ -251,10 +265,27 @@ __global__ void k_bucket_ranges(uint32_t nd, uint32_t none_key, const uint32_t *
     if (p == nd - 1 || key[p + 1] != k) brange[k].y = p + 1;
 }
 
+// A brick's world cell packed in 32 bits (x 11, y 10, z 11 bits about offsets 1024, 512, 1024), each coordinate
+// clamped to its field. Clamping never separates two cells: cells within 2 of each other per axis stay within 2.
+__device__ __forceinline__ uint32_t pack_wcell(int x, int y, int z) {
+    x = min(max(x + 1024, 0), 2047); y = min(max(y + 512, 0), 1023); z = min(max(z + 1024, 0), 2047);
+    return (uint32_t)x | ((uint32_t)y << 11) | ((uint32_t)z << 21);
+}
+// true when the packed cells differ by at most 2 in every coordinate: two brick centres closer than 2 RB = 0.54 m
+// (1.08 cells) always are, so a bucket entry that fails this cannot touch the brick and is skipped unread
+__device__ __forceinline__ bool wcell_near(uint32_t a, uint32_t b) {
+    const int dx = (int)(a & 2047u) - (int)(b & 2047u);
+    const int dy = (int)((a >> 11) & 1023u) - (int)((b >> 11) & 1023u);
+    const int dz = (int)(a >> 21) - (int)(b >> 21);
+    return (uint32_t)(dx + 2) <= 4u && (uint32_t)(dy + 2) <= 4u && (uint32_t)(dz + 2) <= 4u;
+}
+
 // Packed bucket entries in sorted order: world position and brick id, then body id with the asleep bit (31) and the
-// removed-brick bit (30), so a bucket walk reads two contiguous arrays.
+// removed-brick bit (30), and the packed world cell, so a bucket walk reads contiguous arrays: the cells first, the
+// rest only for entries near enough to touch (a full bucket holds mostly other cells that share its hash).
 __global__ void k_bucket_records(uint32_t nd, const uint32_t *cval, const uint32_t *kbody, const uint8_t *kmat,
-                                 const uint8_t *asleep, const float4 *wpos, float4 *srec, uint32_t *sinfo) {
+                                 const uint8_t *asleep, const float4 *wpos, float4 *srec, uint32_t *sinfo,
+                                 uint32_t *scell) {
     uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nd) return;
     uint32_t j = cval[q];
@@ -262,6 +293,7 @@ __global__ void k_bucket_records(uint32_t nd, const uint32_t *cval, const uint32
     float4 p = wpos[j];
     srec[q] = make_float4(p.x, p.y, p.z, __uint_as_float(j));
     sinfo[q] = bj | (asleep[bj] ? 0x80000000u : 0u) | (kmat[j] == 0 ? 0x40000000u : 0u);
+    scell[q] = pack_wcell(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z));
 }
 
 // ---------------------------------------------------------------- contacts
@@ -275,7 +307,7 @@ struct ContactArgs {
     const float *rot, *rad;
     const uint2 *brange;
     const float4 *srec;
-    const uint32_t *sinfo;
+    const uint32_t *sinfo, *scell;
     uint32_t *ccount;
     const uint32_t *coff;
     uint8_t *wake;
@@ -362,6 +394,7 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
             speed = len(v3(vv.x, vv.y, vv.z)) + len(v3(ww.x, ww.y, ww.z)) * A.rad[a] * 0.5f;
         }
         const float lim2 = 4.0f * RB * RB;
+        const uint32_t mycell = pack_wcell(hx, hy, hz);
         const uint2 *br = A.brange + (size_t)sk * HSIZE;
         for (int dz = -1; dz <= 1; dz++) {
             // the layer's nine bucket ranges are fetched together (independent loads in flight), then walked in the
@@ -375,6 +408,7 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
 #pragma unroll
                     for (int k = 1; k < 9; k++) if (c == k) rg = rgs[k];
                     for (uint32_t q = rg.y; q > rg.x; q--) {
+                        if (!wcell_near(mycell, A.scell[q - 1])) continue;
                         const uint32_t info = A.sinfo[q - 1];
                         const float4 rec = A.srec[q - 1];
                         const uint32_t bj = info & 0x3FFFFFFFu;
@@ -496,14 +530,16 @@ __global__ void k_chunk_flags(uint32_t nc, uint32_t K, const uint32_t *flag, con
 __global__ void k_man_write(uint32_t nc, uint32_t K, const uint32_t *cflag, const uint32_t *cpos, const uint32_t *flag,
                             const uint32_t *pos, const uint32_t *pair_start, const uint32_t *perm, const uint32_t *L_a,
                             const uint32_t *L_b, const uint32_t *body_off_of_body, const uint32_t *cidx,
+                            const uint32_t *bscene, const uint32_t *scene_act, const uint32_t *dom_of_act,
                             uint32_t *man_a, uint32_t *man_b, uint32_t *man_ca, uint32_t *man_cb, uint32_t *man_start,
-                            uint32_t *man_prio) {
+                            uint32_t *man_prio, uint32_t *man_dom) {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nc || !cflag[t]) return;
     uint32_t m = cpos[t];
     uint32_t k = perm[t];
     uint32_t a = L_a[k], b = L_b[k];
     man_a[m] = a; man_b[m] = b; man_start[m] = t;
+    man_dom[m] = dom_of_act[scene_act[bscene[a]]];
     man_ca[m] = cidx[a]; man_cb[m] = b == STATIC ? STATIC : cidx[b];
     uint32_t off = body_off_of_body[a];
     uint32_t h = pair_priority(a - off, b == STATIC ? 0u : b - off + 1u);
@@ -518,6 +554,16 @@ __global__ void k_man_count(const uint32_t *nm_p, uint32_t nc, const uint32_t *m
     man_count[m] = e - man_start[m];
 }
 
+// each domain's manifolds form one run (manifolds are ordered by body, bodies by scene, domains are runs of scenes)
+__global__ void k_dom_ranges(const uint32_t *nm_p, const uint32_t *man_dom, uint32_t *m0, uint32_t *m1) {
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nm = *nm_p;
+    if (m >= nm) return;
+    const uint32_t d = man_dom[m];
+    if (m == 0 || man_dom[m - 1] != d) m0[d] = m;
+    if (m + 1 == nm || man_dom[m + 1] != d) m1[d] = m + 1;
+}
+
 __device__ __forceinline__ float eff_mass(float ima, const float *iia, bool hasb, float imb, const float *iib, V3 ra, V3 rb, V3 n) {
     float k = ima + dot(n, cross(mv(iia, cross(ra, n)), ra));
     if (hasb) k += imb + dot(n, cross(mv(iib, cross(rb, n)), rb));
@@ -527,7 +573,8 @@ __device__ __forceinline__ float eff_mass(float ima, const float *iia, bool hasb
 struct PrepArgs {
     uint32_t nc;
     float h;
-    const uint32_t *nm_p, *ncol_p;           // manifolds and colours of the substep (device counts)
+    uint32_t nseg;                           // (domain, colour) segments of the colour lists
+    const uint32_t *nm_p;                    // manifolds of the substep (device count)
     const uint32_t *perm, *man_a, *man_b, *man_count;
     const uint32_t *man_start, *col_start, *col_list, *jds_off;
     const float4 *L_p, *L_n, *pos, *v, *w;
@@ -536,13 +583,14 @@ struct PrepArgs {
     uint32_t *invperm;
 };
 
-// One thread per manifold, in colour-list order (position p of colour c): the two bodies are read once, then each of
-// the manifold's contacts is prepared into its slot of the contact layout, jds_off[c][kk] + p (consecutive threads
-// write consecutive slots). The per-contact arithmetic is prep_contacts' (src/lib.rs:1553-1580).
+// One thread per manifold, in colour-list order (position p of segment c, a (domain, colour) pair): the two bodies
+// are read once, then each of the manifold's contacts is prepared into its slot of the contact layout,
+// jds_off[c][kk] + p (consecutive threads write consecutive slots). The per-contact arithmetic is prep_contacts'
+// (src/lib.rs:1553-1580).
 __global__ void k_prep(PrepArgs A) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= *A.nm_p) return;
-    uint32_t lo = 0, hi = *A.ncol_p;   // colour c: col_start[c] <= i < col_start[c + 1]
+    uint32_t lo = 0, hi = A.nseg;   // the last segment c with col_start[c] <= i (empty segments start where it does)
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
         if (A.col_start[mid] <= i) lo = mid; else hi = mid;
@@ -628,12 +676,14 @@ __global__ void k_bm_fill(const uint32_t *nm_p, const uint32_t *man_a, const uin
 }
 
 struct JpArgs {
-    const uint32_t *nm_p;
     const uint32_t *man_a, *man_b, *prio, *bm_start, *bm_list;   // man_a / man_b: active-list body ids
     uint32_t *man_round, *man_color, *masks;
     uint32_t *wl0, *wl1, *dev;
+    const uint4 *blk_dom;             // per block: domain, rank in the domain, blocks of the domain
+    const uint32_t *dom_m0, *dom_m1;  // per domain: its manifolds [m0, m1)
+    uint32_t *dom_cnt;                // per domain: three rotating worklist counters
     uint32_t max_colors, max_rounds;
-    GridBarrier *gb;
+    GridBarrier *gb;                  // per domain
     uint32_t *err;
 };
 
@@ -649,26 +699,41 @@ __device__ __forceinline__ bool jp_blocked(const JpArgs &A, uint32_t body, uint3
     return false;
 }
 
-__global__ void __launch_bounds__(256) k_jp(JpArgs A) {
-    const uint32_t nm = *A.nm_p;
+// The barrier of one sync domain: a block alone needs only __syncthreads; several blocks meet at the domain's own
+// bounded grid barrier (false once a wait timed out).
+__device__ __forceinline__ bool dom_sync(GridBarrier *gb, uint32_t nblk, uint32_t *err) {
+    if (nblk == 1) { __syncthreads(); return true; }
+    return grid_sync(gb, nblk, err);
+}
+
+// Jones-Plassmann rounds, each domain on its own blocks: a round colours every manifold of the domain's worklist whose
+// higher-priority neighbours are all coloured (the smallest colour free at both bodies) and passes the others on.
+// Neighbouring manifolds share a body, hence a scene, hence a domain, so each domain's result is the greedy
+// colouring in priority order whatever the other domains do.
+__global__ void __launch_bounds__(128) k_jp(JpArgs A) {
+    const uint4 bd = A.blk_dom[blockIdx.x];
+    const uint32_t d = bd.x, rank = bd.y, nblk = bd.z;
+    const uint32_t m0 = A.dom_m0[d], nm = A.dom_m1[d] - m0;
+    uint32_t *cnt = A.dom_cnt + 3 * d;
+    const uint32_t stride = nblk * blockDim.x;
     uint32_t r = 0;
     for (; r < A.max_rounds; r++) {
-        const uint32_t n_in = r == 0 ? nm : __ldcg(&A.dev[DV_WL0 + (r % 3)]);
+        const uint32_t n_in = r == 0 ? nm : __ldcg(&cnt[r % 3]);
         if (n_in == 0) break;
-        const uint32_t *wl_in = (r & 1) ? A.wl1 : A.wl0;
-        uint32_t *wl_out = (r & 1) ? A.wl0 : A.wl1;
-        uint32_t *cnt_out = &A.dev[DV_WL0 + ((r + 1) % 3)];
-        if (blockIdx.x == 0 && threadIdx.x == 0) A.dev[DV_WL0 + ((r + 2) % 3)] = 0;
-        // a warp walks 32 consecutive entries at a time (the same entries per thread as a plain grid-stride loop),
-        // so that it can append its blocked manifolds to the next worklist with one atomic
+        const uint32_t *wl_in = ((r & 1) ? A.wl1 : A.wl0) + m0;
+        uint32_t *wl_out = ((r & 1) ? A.wl0 : A.wl1) + m0;
+        uint32_t *cnt_out = &cnt[(r + 1) % 3];
+        if (rank == 0 && threadIdx.x == 0) cnt[(r + 2) % 3] = 0;
+        // a warp walks 32 consecutive entries at a time, so that it can append its blocked manifolds to the next
+        // worklist with one atomic
         const uint32_t lane = threadIdx.x & 31u;
-        for (uint32_t t0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); t0 < n_in; t0 += gridDim.x * blockDim.x) {
+        for (uint32_t t0 = rank * blockDim.x + (threadIdx.x & ~31u); t0 < n_in; t0 += stride) {
             const uint32_t t = t0 + lane;
             const bool valid = t < n_in;
             uint32_t m = 0, a = 0, b = STATIC, pm = 0;
             bool blocked = false;
             if (valid) {
-                m = r == 0 ? t : __ldcg(&wl_in[t]);
+                m = r == 0 ? m0 + t : __ldcg(&wl_in[t]);
                 a = A.man_a[m]; b = A.man_b[m]; pm = A.prio[m];
                 blocked = jp_blocked(A, a, m, pm, r);
                 if (!blocked && b != STATIC) blocked = jp_blocked(A, b, m, pm, r);
@@ -693,10 +758,10 @@ __global__ void __launch_bounds__(256) k_jp(JpArgs A) {
             atomicOr(&A.masks[(size_t)a * 4 + (c >> 5)], 1u << (c & 31));
             if (b != STATIC) atomicOr(&A.masks[(size_t)b * 4 + (c >> 5)], 1u << (c & 31));
         }
-        if (!grid_sync(A.gb, gridDim.x, A.err)) return;
+        if (!dom_sync(A.gb + d, nblk, A.err)) return;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        A.dev[DV_ROUNDS] = r;
+    if (rank == 0 && threadIdx.x == 0) {
+        atomicMax(&A.dev[DV_ROUNDS], r);
         if (r >= A.max_rounds) atomicOr(A.err, (unsigned)ERR_JP_ROUNDS);
     }
 }
@@ -713,48 +778,57 @@ __device__ __forceinline__ uint32_t warp_add1(uint32_t *ctr, uint32_t key, bool 
     return base + __popc(peers & ((1u << lane) - 1u));
 }
 
-// manifolds counted by (colour, contact count), count descending: bucket c * (JDS_K + 1) + (JDS_K - count)
+// manifolds counted by (segment, contact count), count descending, where segment = domain * cstride + colour:
+// bucket segment * (JDS_K + 1) + (JDS_K - count)
 constexpr int JDS_ROW = JDS_K + 1;
-// Most manifolds fall in a few (colour, count) buckets: the lanes of a warp that share a bucket take one atomic
-// between them (warp_add1), and the colour count is reduced over the warp first. (The order of a bucket's
-// manifolds is arbitrary either way; a colour's manifolds are independent.)
-__global__ void k_col_count(const uint32_t *nm_p, const uint32_t *man_color, const uint32_t *man_count, uint32_t *hist,
-                            uint32_t *dev) {
+// Most manifolds fall in a few buckets: the lanes of a warp that share a bucket take one atomic between them
+// (warp_add1), and the colour counts (per domain and overall) are reduced over the warp first. (The order of a
+// bucket's manifolds is arbitrary either way; a colour's manifolds are independent.)
+__global__ void k_col_count(const uint32_t *nm_p, const uint32_t *man_color, const uint32_t *man_count,
+                            const uint32_t *man_dom, uint32_t cstride, uint32_t *hist, uint32_t *dom_ncol, uint32_t *dev) {
     const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = m < *nm_p;
     const uint32_t c = valid ? man_color[m] : 0u;
-    warp_add1(hist, valid ? c * JDS_ROW + (JDS_K - man_count[m]) : 0u, valid);
+    const uint32_t d = valid ? man_dom[m] : 0u;
+    warp_add1(hist, valid ? (d * cstride + c) * JDS_ROW + (JDS_K - man_count[m]) : 0u, valid);
+    const uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : 0xFFFFFFFFu);
+    const uint32_t dm = __reduce_max_sync(peers, valid ? c + 1 : 0u);
+    if (valid && (threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1)) atomicMax(&dom_ncol[d], dm);
     const uint32_t cm = __reduce_max_sync(0xffffffffu, valid ? c + 1 : 0u);
     if ((threadIdx.x & 31u) == 0 && cm) atomicMax(&dev[DV_COLORS], cm);
 }
 __global__ void k_col_fill(const uint32_t *nm_p, const uint32_t *man_color, const uint32_t *man_count,
-                           const uint32_t *hstart, uint32_t *hfill, uint32_t *col_list) {
+                           const uint32_t *man_dom, uint32_t cstride, const uint32_t *hstart, uint32_t *hfill,
+                           uint32_t *col_list) {
     const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = m < *nm_p;
-    const uint32_t bkt = valid ? man_color[m] * JDS_ROW + (JDS_K - man_count[m]) : 0u;
+    const uint32_t bkt = valid ? (man_dom[m] * cstride + man_color[m]) * JDS_ROW + (JDS_K - man_count[m]) : 0u;
     const uint32_t slot = warp_add1(hfill, bkt, valid);
     if (valid) col_list[hstart[bkt] + slot] = m;
 }
-// one thread per colour: colour starts in col_list and the JDS offsets (contacts of colour c before c come first)
-__global__ void __launch_bounds__(MAXCOL) k_jds_table(const uint32_t *hist, const uint32_t *hstart, const uint32_t *nm_p,
-                                                      uint32_t *col_start, uint32_t *jds_off) {
-    __shared__ uint32_t tot[MAXCOL];
-    const uint32_t c = threadIdx.x;
-    uint32_t n[JDS_K];
+// per segment: the contacts it holds (its contact-layout size)
+__global__ void k_seg_totals(uint32_t nseg, const uint32_t *hist, uint32_t *tot) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nseg) return;
+    // n[k] = manifolds with more than k contacts = those in buckets j <= JDS_K - 1 - k; contacts = sum of n[k]
     uint32_t run = 0, total = 0;
-    // n[k] = manifolds of colour c with more than k contacts = those in buckets j <= JDS_K - 1 - k
-#pragma unroll
-    for (int j = 0; j < JDS_K; j++) { run += hist[c * JDS_ROW + j]; n[JDS_K - 1 - j] = run; }
-#pragma unroll
-    for (int k = 0; k < JDS_K; k++) total += n[k];
+    for (int j = 0; j < JDS_K; j++) { run += hist[(size_t)c * JDS_ROW + j]; total += run; }
     tot[c] = total;
-    __syncthreads();
-    uint32_t base = 0;
-    for (uint32_t q = 0; q < c; q++) base += tot[q];
-    col_start[c] = hstart[c * JDS_ROW];
-    if (c == MAXCOL - 1) col_start[MAXCOL] = *nm_p;
+}
+// per segment: its start in col_list and the JDS offsets of its contact layout (segments' contacts in segment order)
+__global__ void k_seg_table(uint32_t nseg, const uint32_t *hist, const uint32_t *hstart, const uint32_t *base,
+                            const uint32_t *nm_p, uint32_t *col_start, uint32_t *jds_off) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nseg) return;
+    uint32_t n[JDS_K];
+    uint32_t run = 0;
 #pragma unroll
-    for (int k = 0; k < JDS_K; k++) { jds_off[c * JDS_K + k] = base; base += n[k]; }
+    for (int j = 0; j < JDS_K; j++) { run += hist[(size_t)c * JDS_ROW + j]; n[JDS_K - 1 - j] = run; }
+    uint32_t b = base[c];
+    col_start[c] = hstart[(size_t)c * JDS_ROW];
+    if (c == nseg - 1) col_start[nseg] = *nm_p;
+#pragma unroll
+    for (int k = 0; k < JDS_K; k++) { jds_off[(size_t)c * JDS_K + k] = b; b += n[k]; }
 }
 
 // proper-colouring check: no two manifolds of one colour at one awake body
@@ -776,6 +850,9 @@ __global__ void k_col_verify(const uint32_t *nm_p, const uint32_t *man_a, const 
 struct SolveArgs {
     uint32_t iterations;
     const uint32_t *dev;           // DV_COLORS
+    const uint4 *blk_dom;          // per block: domain, rank in the domain, blocks of the domain
+    const uint32_t *dom_ncol;      // per domain: colours used
+    uint32_t cstride;              // segment of (domain d, colour c) = d * cstride + c
     const uint32_t *col_start, *col_list, *jds_off;
     const uint32_t *man_a, *man_b, *man_count;
     const float4 *S_n, *S_t1, *S_t2, *S_ra, *S_rb;
@@ -881,21 +958,26 @@ __device__ __forceinline__ uint32_t snake_pos(uint32_t r, uint32_t g, uint32_t s
     return (r & 1u) ? (r + 1) * stride - 1 - g : r * stride + g;
 }
 
+// Each sync domain runs its own iterations and colours on its own blocks, meeting at its own barrier after each
+// colour: scenes never share a body, so no domain waits for another's colours.
 __global__ void __launch_bounds__(SOLVE_BLOCK) k_solve(SolveArgs A) {
     __shared__ uint32_t off[JDS_K];
-    const uint32_t ncol = A.dev[DV_COLORS];
-    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint4 bd = A.blk_dom[blockIdx.x];
+    const uint32_t d = bd.x, nblk = bd.z;
+    const uint32_t ncol = A.dom_ncol[d];
+    const uint32_t stride = nblk * blockDim.x;
+    const uint32_t g = bd.y * blockDim.x + threadIdx.x;
     for (uint32_t it = 0; it < A.iterations; it++) {
         for (uint32_t c = 0; c < ncol; c++) {
-            if (threadIdx.x < JDS_K) off[threadIdx.x] = A.jds_off[c * JDS_K + threadIdx.x];
+            const uint32_t seg = d * A.cstride + c;
+            if (threadIdx.x < JDS_K) off[threadIdx.x] = A.jds_off[(size_t)seg * JDS_K + threadIdx.x];
             __syncthreads();
-            const uint32_t s0 = A.col_start[c], n = A.col_start[c + 1] - s0;
-            const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+            const uint32_t s0 = A.col_start[seg], n = A.col_start[seg + 1] - s0;
             for (uint32_t r = 0; r * stride < n; r++) {
                 const uint32_t p = snake_pos(r, g, stride);
                 if (p < n) solve_manifold<false>(A, A.col_list[s0 + p], p, off);
             }
-            if (!grid_sync(A.gb, gridDim.x, A.err)) return;
+            if (!dom_sync(A.gb + d, nblk, A.err)) return;
         }
     }
 }
@@ -1169,6 +1251,97 @@ __global__ void k_scene_live(uint32_t nb, const uint32_t *list, const uint8_t *a
 // ---------------------------------------------------------------- host side
 static int bits_for(uint64_t v) { int b = 0; while (b < 64 && (v >> b) != 0) b++; return b; }
 
+// Sync domains for the colouring and the solve: the active scenes are cut into contiguous runs and every run gets
+// blocks in proportion to its bricks (a stand-in for its contacts). A scene with at least 1 / DOM_MAX of the
+// active bricks is a domain of its own; smaller ones are gathered until a run reaches that share. A run of one block
+// needs only __syncthreads between colours; larger runs meet at their own grid barrier.
+constexpr uint32_t DOM_MAX = 256;
+
+static void make_partition(const sf_world *w, const StepState *S, unsigned R, bool single, StepState::Partition &P) {
+    const size_t K = S->act.size();
+    P.R = R;
+    P.dom_of_act.assign(std::max<size_t>(K, 1), 0);
+    P.blk.assign(R, make_uint4(0, 0, R, 0));
+    P.D = 1;
+    for (unsigned b = 0; b < R; b++) P.blk[b] = make_uint4(0, b, R, 0);
+    if (single || K <= 1 || R <= 1) return;
+    std::vector<double> load(K);
+    double total = 0.0;
+    for (size_t k = 0; k < K; k++) { load[k] = std::max(1.0, (double)w->scenes[S->act[k]].n_bricks); total += load[k]; }
+    const uint32_t dmax = std::min<uint32_t>(R, DOM_MAX);
+    const double target = total / dmax;
+    std::vector<std::pair<size_t, size_t>> runs;
+    std::vector<double> rl;
+    size_t a = 0;
+    double acc = 0.0;
+    for (size_t k = 0; k < K; k++) {
+        if (load[k] >= target) {
+            if (k > a) { runs.push_back({a, k}); rl.push_back(acc); }
+            runs.push_back({k, k + 1}); rl.push_back(load[k]);
+            a = k + 1; acc = 0.0;
+            continue;
+        }
+        acc += load[k];
+        if (acc >= target) { runs.push_back({a, k + 1}); rl.push_back(acc); a = k + 1; acc = 0.0; }
+    }
+    if (a < K) { runs.push_back({a, K}); rl.push_back(acc); }
+    // a large scene can split a gathering run in two: merge the lightest neighbouring pair until dmax runs remain
+    while (runs.size() > dmax) {
+        size_t best = 0;
+        for (size_t i = 1; i + 1 < runs.size(); i++) if (rl[i] + rl[i + 1] < rl[best] + rl[best + 1]) best = i;
+        runs[best].second = runs[best + 1].second;
+        rl[best] += rl[best + 1];
+        runs.erase(runs.begin() + best + 1);
+        rl.erase(rl.begin() + best + 1);
+    }
+    const size_t D = runs.size();
+    std::vector<unsigned> nb(D);
+    unsigned sum = 0;
+    for (size_t d = 0; d < D; d++) { nb[d] = std::max(1u, (unsigned)(rl[d] * R / total)); sum += nb[d]; }
+    while (sum > R) {   // take a block from the run that has the most blocks per load
+        size_t best = D;
+        for (size_t d = 0; d < D; d++)
+            if (nb[d] > 1 && (best == D || nb[d] / rl[d] > nb[best] / rl[best])) best = d;
+        nb[best]--; sum--;
+    }
+    while (sum < R) {   // give a block to the run with the most load per block
+        size_t best = 0;
+        for (size_t d = 1; d < D; d++) if (rl[d] / nb[d] > rl[best] / nb[best]) best = d;
+        nb[best]++; sum++;
+    }
+    P.D = (uint32_t)D;
+    unsigned b = 0;
+    for (size_t d = 0; d < D; d++) {
+        for (size_t k = runs[d].first; k < runs[d].second; k++) P.dom_of_act[k] = (uint32_t)d;
+        for (unsigned r = 0; r < nb[d]; r++) P.blk[b++] = make_uint4((uint32_t)d, r, nb[d], 0);
+    }
+}
+
+// the partition for a launch of R blocks over the current active set (built once per active set and launch size)
+static sf_status use_partition(sf_world *w, unsigned R, bool single) {
+    StepState *S = w->step;
+    const unsigned key = single ? 0x80000000u | R : R;
+    size_t at = S->parts.size();
+    for (size_t k = 0; k < S->parts.size(); k++) if (S->parts[k].R == key) at = k;
+    if (at == S->parts.size()) {
+        S->parts.emplace_back();
+        make_partition(w, S, R, single, S->parts.back());
+        S->parts.back().R = key;
+    }
+    StepState::Partition &P = S->parts[at];
+    // the blocks' table and the scenes' domains, uploaded when the partition in use changes
+    if (S->part_in_use != (int)at) {
+        cudaStream_t s = w->stream;
+        SF_CUDA(S->blk_dom.grow(P.blk.size()));
+        SF_CUDA(S->dom_of_act.grow(P.dom_of_act.size()));
+        SF_CUDA(cudaMemcpyAsync(S->blk_dom.p, P.blk.data(), P.blk.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
+        SF_CUDA(cudaMemcpyAsync(S->dom_of_act.p, P.dom_of_act.data(), P.dom_of_act.size() * 4, cudaMemcpyHostToDevice, s));
+        S->part_in_use = (int)at;
+    }
+    S->part_D = P.D;
+    return SF_OK;
+}
+
 static cudaError_t grow_contacts(StepState *S, uint64_t need) {
     if (need <= S->capacity) return cudaSuccess;
     uint64_t cap = std::max<uint64_t>(need + need / 2, 4096);
@@ -1176,7 +1349,7 @@ static cudaError_t grow_contacts(StepState *S, uint64_t need) {
 #define G(buf) if ((e = S->buf.alloc(cap)) != cudaSuccess) return e
     G(L_a); G(L_b); G(L_bo); G(L_ba); G(L_bb); G(L_p); G(L_n);
     G(mkey); G(mkey_alt); G(perm); G(perm_alt); G(invperm); G(mflag); G(mpos); G(pair_start); G(cflag); G(cpos);
-    G(man_a); G(man_b); G(man_ca); G(man_cb); G(man_start); G(man_count); G(man_prio); G(man_color); G(man_round);
+    G(man_a); G(man_b); G(man_ca); G(man_cb); G(man_start); G(man_count); G(man_prio); G(man_color); G(man_round); G(man_dom);
     G(S_n); G(S_t1); G(S_t2); G(S_ra); G(S_rb); G(S_j);
     G(wl0); G(wl1); G(col_list);
 #undef G
@@ -1197,14 +1370,19 @@ sf_status step_create(sf_world *w) {
     SF_CUDA(S->bucket_bits.alloc((size_t)nsc * (HSIZE / 32)));
     SF_CUDA(S->scene_awake.alloc(nsc)); SF_CUDA(S->scene_bricks.alloc(nsc));
     SF_CUDA(S->brange.alloc((size_t)nsc * HSIZE));
-    SF_CUDA(S->srec.alloc(nd)); SF_CUDA(S->sinfo.alloc(nd));
+    SF_CUDA(S->srec.alloc(nd)); SF_CUDA(S->sinfo.alloc(nd)); SF_CUDA(S->scell.alloc(nd));
     SF_CUDA(S->slot_id.alloc((size_t)nd * CSLOTS)); SF_CUDA(S->slot_p.alloc((size_t)nd * CSLOTS)); SF_CUDA(S->slot_n.alloc((size_t)nd * CSLOTS));
     SF_CUDA(S->ccount.alloc((size_t)nd + 1)); SF_CUDA(S->coff.alloc((size_t)nd + 1));
     SF_CUDA(S->bm_count.alloc((size_t)nb + 1)); SF_CUDA(S->bm_start.alloc((size_t)nb + 1)); SF_CUDA(S->bm_fill.alloc((size_t)nb + 1));
     SF_CUDA(S->masks.alloc((size_t)nb * 4 + 4)); SF_CUDA(S->vmasks.alloc((size_t)nb * 4 + 4));
-    SF_CUDA(S->col_count.alloc(MAXCOL * JDS_ROW + 1)); SF_CUDA(S->col_start.alloc(MAXCOL + 2));
-    SF_CUDA(S->col_fill.alloc(MAXCOL * JDS_ROW + 1)); SF_CUDA(S->jds_off.alloc(MAXCOL * JDS_K));
-    SF_CUDA(S->col_hstart.alloc(MAXCOL * JDS_ROW + 1));
+    {
+        const size_t nseg = (size_t)DOM_MAX * w->P.max_colors;
+        SF_CUDA(S->col_count.alloc(nseg * JDS_ROW + 1)); SF_CUDA(S->col_start.alloc(nseg + 2));
+        SF_CUDA(S->col_fill.alloc(nseg * JDS_ROW + 1)); SF_CUDA(S->jds_off.alloc(nseg * JDS_K));
+        SF_CUDA(S->col_hstart.alloc(nseg * JDS_ROW + 1)); SF_CUDA(S->seg_tot.alloc(nseg)); SF_CUDA(S->seg_base.alloc(nseg));
+        SF_CUDA(S->dom_m0.alloc(DOM_MAX)); SF_CUDA(S->dom_m1.alloc(DOM_MAX)); SF_CUDA(S->dom_ncol.alloc(DOM_MAX));
+        SF_CUDA(S->dom_cnt.alloc(3 * DOM_MAX)); SF_CUDA(S->dom_gb.alloc(DOM_MAX));
+    }
     if (w->P.manifold_chunk == 0 || w->P.manifold_chunk > (uint32_t)JDS_K) w->P.manifold_chunk = JDS_K;
     SF_CUDA(S->parent.alloc(nb)); SF_CUDA(S->label.alloc(nb)); SF_CUDA(S->mint.alloc(nb));
     SF_CUDA(cudaMemsetAsync(S->label.p, 0xFF, S->label.bytes(), s));
@@ -1228,15 +1406,14 @@ sf_status step_create(sf_world *w) {
     int occ = 0;
     SF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve, SOLVE_BLOCK, 0));
     S->solve_occ = std::max(1, occ);
-    SF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jp, 256, 0));
+    SF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jp, SOLVE_BLOCK, 0));
     S->jp_occ = std::max(1, occ);
     {
+        // the colouring and the solve run on the same blocks (one partition into sync domains serves both)
+        const int top = std::min(S->solve_occ, S->jp_occ);
         int c[4], n = 0;
-        for (int v = 1; v <= 4; v++) if (v <= S->solve_occ) c[n++] = v;
+        for (int v = 1; v <= 4; v++) if (v <= top) c[n++] = v;
         S->solve_t.init(c, n);
-        n = 0;
-        for (int v : {1, 2, 4}) if (v <= S->jp_occ) c[n++] = v;
-        S->jp_t.init(c, n);
     }
     SF_CUDA(cudaStreamSynchronize(s));   // the host vector `off` is the copy's source
     return SF_OK;
@@ -1286,6 +1463,8 @@ static void tune_resolve(StepState *S) {
 
 void step_destroy(sf_world *w) {
     if (w->step) for (cudaEvent_t e : w->step->tev) cudaEventDestroy(e);
+    if (w->step) for (cudaEvent_t e : w->step->gen_ev) cudaEventDestroy(e);
+    if (w->step) for (cudaEvent_t e : w->step->ev_pool) cudaEventDestroy(e);
     if (w->step && w->step->h_dev) cudaFreeHost(w->step->h_dev);
     if (w->step && w->step->h_live_pin) cudaFreeHost(w->step->h_live_pin);
     delete w->step;
@@ -1347,6 +1526,8 @@ static sf_status set_active(sf_world *w, const uint8_t *mask) {
     S->nb_act = nb_act;
     S->nd_act = nd_act;
     S->act_valid = true;
+    S->parts.clear();
+    S->part_in_use = -1;
     return SF_OK;
 }
 
@@ -1428,7 +1609,7 @@ static sf_status substep(sf_world *w, float h) {
     if (n_inc) {
         k_bucket_ranges<<<grid_for(n_inc, 256), 256, 0, s>>>(n_inc, none_key, S->ckey.p, S->brange.p);
         k_bucket_records<<<grid_for(n_inc, 256), 256, 0, s>>>(n_inc, S->cval.p, w->k_body.p, w->k_mat.p, w->b_asleep.p,
-                                                              w->k_wpos.p, S->srec.p, S->sinfo.p);
+                                                              w->k_wpos.p, S->srec.p, S->sinfo.p, S->scell.p);
         L += 2;
     }
     prof_mark(w);
@@ -1438,10 +1619,25 @@ static sf_status substep(sf_world *w, float h) {
     C.sbox = w->sbox.p; C.kbody = w->k_body.p; C.bscene = w->b_scene.p; C.ctab = w->ctab.p; C.cpool = w->cpool.p;
     C.alive = w->b_alive.p; C.asleep = w->b_asleep.p; C.smat = w->s_mat.p; C.wpos = w->k_wpos.p;
     C.v = w->b_v.p; C.w = w->b_w.p; C.rot = w->b_rot.p; C.rad = w->b_rad.p; C.brange = S->brange.p; C.srec = S->srec.p;
-    C.sinfo = S->sinfo.p; C.ccount = S->ccount.p; C.coff = S->coff.p; C.wake = w->b_wake.p;
+    C.sinfo = S->sinfo.p; C.scell = S->scell.p; C.ccount = S->ccount.p; C.coff = S->coff.p; C.wake = w->b_wake.p;
     C.slot_id = S->slot_id.p; C.slot_p = S->slot_p.p; C.slot_n = S->slot_n.p;
     C.L_a = S->L_a.p; C.L_b = S->L_b.p; C.L_bo = S->L_bo.p; C.L_ba = S->L_ba.p; C.L_bb = S->L_bb.p; C.L_p = S->L_p.p; C.L_n = S->L_n.p;
+    cudaEvent_t g0 = nullptr, g1 = nullptr;
+    if (S->profile && n_awk) {
+        while (S->gen_ev.size() < S->gen_used + 2) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) break;
+            S->gen_ev.push_back(e);
+        }
+        if (S->gen_ev.size() >= S->gen_used + 2) {
+            g0 = S->gen_ev[S->gen_used]; g1 = S->gen_ev[S->gen_used + 1];
+            S->gen_used += 2;
+            S->gen_bricks += n_awk;
+        }
+    }
+    if (g0) cudaEventRecord(g0, s);
     if (n_awk) k_contacts_gen<<<grid_for(n_awk, 128), 128, 0, s>>>(C);
+    if (g1) cudaEventRecord(g1, s);
     SF_CUDA(exclusive_scan_u32(S->ccount.p, S->coff.p, n_awk, S->dev.p + DV_CONTACTS, S->wk, s));
     SF_CUDA(cudaMemcpyAsync(S->h_dev, S->dev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     SF_CUDA(cudaStreamSynchronize(s));
@@ -1459,8 +1655,23 @@ static sf_status substep(sf_world *w, float h) {
     L += 1;
     if (S->profile) S->sub_nc.push_back(nc);
     prof_mark(w);
+    // The launch size of the colouring and the solve, and its partition into sync domains. A substep with few contacts
+    // is solved by one block (k_solve_one_block); its colouring then runs as a single domain.
+    const bool one_block = nc <= SOLVE_ONE_BLOCK_MAX_CONTACTS;
+    int sci = -1;
+    const int sb = Tuner::bucket(nc);
+    const unsigned top_occ = (unsigned)std::min(S->solve_occ, S->jp_occ);
+    unsigned per_sm = w->P.solve_blocks ? std::min<unsigned>(w->P.solve_blocks, top_occ)
+                                        : (unsigned)S->solve_t.choose(sb, sci);
+    if (one_block) sci = -1;
+    const unsigned R = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)w->sms * per_sm,
+                                                                         (nc + SOLVE_BLOCK - 1) / SOLVE_BLOCK + 1));
+    const uint32_t cstride = w->P.max_colors;
     // manifolds
     if (nc) {
+        sf_status pst = use_partition(w, R, one_block);
+        if (pst != SF_OK) return pst;
+        const uint32_t D = S->part_D;
         const uint64_t span = (uint64_t)S->max_scene_bodies + 1;
         k_man_keys<<<g_nc, 256, 0, s>>>(nc, span, S->L_a.p, S->L_b.p, S->body_off_of_body.p, S->mkey.p, S->perm.p);
         bool alt = false;
@@ -1473,12 +1684,16 @@ static sf_status substep(sf_world *w, float h) {
         k_chunk_flags<<<g_nc, 256, 0, s>>>(nc, K, S->mflag.p, S->mpos.p, S->pair_start.p, S->cflag.p);
         SF_CUDA(exclusive_scan_u32(S->cflag.p, S->cpos.p, nc, S->dev.p + DV_MANIFOLDS, S->wk, s));
         k_man_write<<<g_nc, 256, 0, s>>>(nc, K, S->cflag.p, S->cpos.p, S->mflag.p, S->mpos.p, S->pair_start.p, S->perm.p,
-                                         S->L_a.p, S->L_b.p, S->body_off_of_body.p, S->cidx.p, S->man_a.p, S->man_b.p,
-                                         S->man_ca.p, S->man_cb.p, S->man_start.p, S->man_prio.p);
+                                         S->L_a.p, S->L_b.p, S->body_off_of_body.p, S->cidx.p, w->b_scene.p, S->scene_act.p,
+                                         S->dom_of_act.p, S->man_a.p, S->man_b.p, S->man_ca.p, S->man_cb.p, S->man_start.p,
+                                         S->man_prio.p, S->man_dom.p);
         k_man_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, nc, S->man_start.p, S->man_count.p);
-        L += 6;
+        SF_CUDA(cudaMemsetAsync(S->dom_m0.p, 0, (size_t)D * 4, s));
+        SF_CUDA(cudaMemsetAsync(S->dom_m1.p, 0, (size_t)D * 4, s));
+        k_dom_ranges<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_dom.p, S->dom_m0.p, S->dom_m1.p);
+        L += 7;
         prof_mark(w);
-        // colouring, on the active list's body ids
+        // colouring, on the active list's body ids, each domain on its own blocks
         SF_CUDA(cudaMemsetAsync(S->bm_count.p, 0, ((size_t)nb + 1) * 4, s));
         SF_CUDA(cudaMemsetAsync(S->bm_fill.p, 0, ((size_t)nb + 1) * 4, s));
         SF_CUDA(cudaMemsetAsync(S->masks.p, 0, (size_t)nb * 16, s));
@@ -1486,29 +1701,31 @@ static sf_status substep(sf_world *w, float h) {
         k_bm_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_ca.p, S->man_cb.p, S->bm_count.p);
         SF_CUDA(exclusive_scan_u32(S->bm_count.p, S->bm_start.p, (size_t)nb + 1, nullptr, S->wk, s));
         k_bm_fill<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_ca.p, S->man_cb.p, S->bm_start.p, S->bm_fill.p, S->bm_list.p);
-        SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s));
+        SF_CUDA(cudaMemsetAsync(S->dom_gb.p, 0, (size_t)D * sizeof(GridBarrier), s));
+        SF_CUDA(cudaMemsetAsync(S->dom_cnt.p, 0, (size_t)D * 3 * 4, s));
         JpArgs J;
-        J.nm_p = S->dev.p + DV_MANIFOLDS; J.man_a = S->man_ca.p; J.man_b = S->man_cb.p; J.prio = S->man_prio.p;
+        J.man_a = S->man_ca.p; J.man_b = S->man_cb.p; J.prio = S->man_prio.p;
         J.bm_start = S->bm_start.p; J.bm_list = S->bm_list.p; J.man_round = S->man_round.p; J.man_color = S->man_color.p;
-        J.masks = S->masks.p; J.wl0 = S->wl0.p; J.wl1 = S->wl1.p; J.dev = S->dev.p; J.max_colors = w->P.max_colors;
-        J.max_rounds = 1u << 16; J.gb = w->barrier.p; J.err = w->err.p;
-        int jci = -1;
-        const int jb = Tuner::bucket(nc);
-        const unsigned jper = (unsigned)S->jp_t.choose(jb, jci);
-        unsigned jgrid = (unsigned)std::min<uint64_t>((uint64_t)w->sms * jper, (nc + 255) / 256 + 1);
+        J.masks = S->masks.p; J.wl0 = S->wl0.p; J.wl1 = S->wl1.p; J.dev = S->dev.p; J.blk_dom = S->blk_dom.p;
+        J.dom_m0 = S->dom_m0.p; J.dom_m1 = S->dom_m1.p; J.dom_cnt = S->dom_cnt.p; J.max_colors = w->P.max_colors;
+        J.max_rounds = 1u << 16; J.gb = S->dom_gb.p; J.err = w->err.p;
         void *jargs[] = {&J};
-        tune_begin(S, &S->jp_t, jb, jci, s);
-        SF_CUDA(cudaLaunchCooperativeKernel((void *)k_jp, dim3(jgrid), dim3(256), jargs, 0, s));
-        tune_end(S, jci, s);
-        // colour lists with each colour's manifolds by contact count (most first), and the contact layout
-        SF_CUDA(cudaMemsetAsync(S->col_count.p, 0, S->col_count.bytes(), s));
-        SF_CUDA(cudaMemsetAsync(S->col_fill.p, 0, S->col_fill.bytes(), s));
-        k_col_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_color.p, S->man_count.p, S->col_count.p, S->dev.p);
-        SF_CUDA(exclusive_scan_u32(S->col_count.p, S->col_hstart.p, MAXCOL * JDS_ROW, nullptr, S->wk, s));
-        k_col_fill<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_color.p, S->man_count.p, S->col_hstart.p,
-                                        S->col_fill.p, S->col_list.p);
-        k_jds_table<<<1, MAXCOL, 0, s>>>(S->col_count.p, S->col_hstart.p, S->dev.p + DV_MANIFOLDS, S->col_start.p, S->jds_off.p);
-        L += 7;
+        SF_CUDA(cudaLaunchCooperativeKernel((void *)k_jp, dim3(R), dim3(SOLVE_BLOCK), jargs, 0, s));
+        // colour lists: each (domain, colour) segment's manifolds by contact count (most first), and the contact layout
+        const uint32_t nseg = D * cstride;
+        SF_CUDA(cudaMemsetAsync(S->col_count.p, 0, (size_t)nseg * JDS_ROW * 4, s));
+        SF_CUDA(cudaMemsetAsync(S->col_fill.p, 0, (size_t)nseg * JDS_ROW * 4, s));
+        SF_CUDA(cudaMemsetAsync(S->dom_ncol.p, 0, (size_t)D * 4, s));
+        k_col_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_color.p, S->man_count.p, S->man_dom.p, cstride,
+                                         S->col_count.p, S->dom_ncol.p, S->dev.p);
+        SF_CUDA(exclusive_scan_u32(S->col_count.p, S->col_hstart.p, (size_t)nseg * JDS_ROW, nullptr, S->wk, s));
+        k_col_fill<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_color.p, S->man_count.p, S->man_dom.p, cstride,
+                                        S->col_hstart.p, S->col_fill.p, S->col_list.p);
+        k_seg_totals<<<grid_for(nseg, 128), 128, 0, s>>>(nseg, S->col_count.p, S->seg_tot.p);
+        SF_CUDA(exclusive_scan_u32(S->seg_tot.p, S->seg_base.p, nseg, nullptr, S->wk, s));
+        k_seg_table<<<grid_for(nseg, 128), 128, 0, s>>>(nseg, S->col_count.p, S->col_hstart.p, S->seg_base.p,
+                                                        S->dev.p + DV_MANIFOLDS, S->col_start.p, S->jds_off.p);
+        L += 6;
         if (w->P.verify) {
             SF_CUDA(cudaMemsetAsync(S->vmasks.p, 0, (size_t)nb * 16, s));
             k_col_verify<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_ca.p, S->man_cb.p, S->man_color.p, S->vmasks.p, w->err.p);
@@ -1516,7 +1733,7 @@ static sf_status substep(sf_world *w, float h) {
         }
         prof_mark(w);
         PrepArgs PA;
-        PA.nc = nc; PA.h = h; PA.nm_p = S->dev.p + DV_MANIFOLDS; PA.ncol_p = S->dev.p + DV_COLORS; PA.perm = S->perm.p;
+        PA.nc = nc; PA.h = h; PA.nseg = nseg; PA.nm_p = S->dev.p + DV_MANIFOLDS; PA.perm = S->perm.p;
         PA.man_a = S->man_a.p; PA.man_b = S->man_b.p; PA.man_count = S->man_count.p; PA.L_p = S->L_p.p; PA.L_n = S->L_n.p;
         PA.man_start = S->man_start.p; PA.col_start = S->col_start.p; PA.col_list = S->col_list.p;
         PA.jds_off = S->jds_off.p;
@@ -1531,25 +1748,21 @@ static sf_status substep(sf_world *w, float h) {
     }
     k_save_pre<<<grid_for(nb, 256), 256, 0, s>>>(nb, blist, w->b_alive.p, w->b_v.p, w->b_w.p, w->b_vpre.p, w->b_wpre.p);
     L++;
-    SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s));
     prof_mark(w);
     if (nc && w->P.iterations) {
         SolveArgs A;
         A.iterations = w->P.iterations; A.dev = S->dev.p; A.col_start = S->col_start.p; A.col_list = S->col_list.p;
+        A.blk_dom = S->blk_dom.p; A.dom_ncol = S->dom_ncol.p; A.cstride = cstride;
         A.jds_off = S->jds_off.p; A.man_a = S->man_a.p; A.man_b = S->man_b.p; A.man_count = S->man_count.p;
         A.S_n = S->S_n.p; A.S_t1 = S->S_t1.p; A.S_t2 = S->S_t2.p; A.S_ra = S->S_ra.p; A.S_rb = S->S_rb.p; A.S_j = S->S_j.p;
-        A.v = w->b_v.p; A.w = w->b_w.p; A.im = w->b_im.p; A.iiw = w->b_iiw.p; A.gb = w->barrier.p; A.err = w->err.p;
-        if (nc <= SOLVE_ONE_BLOCK_MAX_CONTACTS) {
+        A.v = w->b_v.p; A.w = w->b_w.p; A.im = w->b_im.p; A.iiw = w->b_iiw.p; A.gb = S->dom_gb.p; A.err = w->err.p;
+        if (one_block) {
             k_solve_one_block<<<1, SOLVE_ONE_BLOCK, 0, s>>>(A);
         } else {
-            int sci = -1;
-            const int sb = Tuner::bucket(nc);
-            unsigned per_sm = w->P.solve_blocks ? std::min<unsigned>(w->P.solve_blocks, S->solve_occ)
-                                                : (unsigned)S->solve_t.choose(sb, sci);
-            unsigned sgrid = (unsigned)std::min<uint64_t>((uint64_t)w->sms * per_sm, (nc + SOLVE_BLOCK - 1) / SOLVE_BLOCK + 1);
+            SF_CUDA(cudaMemsetAsync(S->dom_gb.p, 0, (size_t)S->part_D * sizeof(GridBarrier), s));
             void *sargs[] = {&A};
             tune_begin(S, &S->solve_t, sb, sci, s);
-            SF_CUDA(cudaLaunchCooperativeKernel((void *)k_solve, dim3(sgrid), dim3(SOLVE_BLOCK), sargs, 0, s));
+            SF_CUDA(cudaLaunchCooperativeKernel((void *)k_solve, dim3(R), dim3(SOLVE_BLOCK), sargs, 0, s));
             tune_end(S, sci, s);
         }
         L++;
@@ -1665,6 +1878,11 @@ static sf_status step_impl(sf_world *w, float dt, uint32_t nsteps, const uint8_t
             S->ph_substeps++;
         }
         S->ev_used = 0;
+        for (size_t k = 0; k + 1 < S->gen_used; k += 2) {
+            float e = 0.0f;
+            if (cudaEventElapsedTime(&e, S->gen_ev[k], S->gen_ev[k + 1]) == cudaSuccess) S->gen_ms += e;
+        }
+        S->gen_used = 0;
     }
     return r;
 }
@@ -1679,8 +1897,8 @@ sf_status sf_world_step(sf_world *w, float dt, uint32_t nsteps) { return step_im
 
 sf_status sf_read_tuning(sf_world *w, uint32_t which, int32_t *blocks_per_sm, uint32_t n) {
     if (!w || !blocks_per_sm) { set_error("null argument"); return SF_ERR_ARG; }
-    const Tuner *t = which == SF_TUNE_SOLVE ? &w->step->solve_t : which == SF_TUNE_COLOR ? &w->step->jp_t
-                                                                                      : sor_tuner(w->sor);
+    // the colouring runs on the solve's blocks, so both read the solve's tuner
+    const Tuner *t = (which == SF_TUNE_SOLVE || which == SF_TUNE_COLOR) ? &w->step->solve_t : sor_tuner(w->sor);
     if (!t) { set_error("no such tuner"); return SF_ERR_ARG; }
     for (uint32_t b = 0; b < n; b++) blocks_per_sm[b] = b < (uint32_t)Tuner::NB ? t->settled((int)b) : -1;
     return SF_OK;
@@ -1710,6 +1928,8 @@ sf_status sf_read_profile(sf_world *w, sf_profile *out) {
     for (uint32_t n : S->sub_nc) sum += n;
     out->contacts_sum = sum;
     out->launches = w->launches + S->wk.launches + sor_launches(w->sor);
+    out->gen_ms = S->gen_ms;
+    out->gen_bricks = S->gen_bricks;
     return SF_OK;
 }
 
@@ -1718,6 +1938,7 @@ sf_status sf_reset_profile(sf_world *w) {
     StepState *S = w->step;
     for (int p = 0; p < SF_PHASES; p++) S->ph_ms[p] = 0.0;
     S->ph_substeps = 0; S->solve_launches = 0; S->solve_contact_iters = 0; S->sub_nc.clear(); S->ev_used = 0;
+    S->gen_ms = 0.0; S->gen_bricks = 0; S->gen_used = 0;
     w->launches = 0; S->wk.launches = 0; sor_reset_launches(w->sor);
     return SF_OK;
 }
