@@ -46,7 +46,7 @@ def _scene_state(w, k):
 def _local_labels(lab, off):
     out = lab.copy()
     live = lab != STATIC
-    out[live] -= off
+    out[live] -= np.uint32(off)
     return out
 
 
