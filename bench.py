@@ -623,11 +623,11 @@ def our_arm(args, rank, world, local, pg):
         c3 = S.config3_world(seed=2 + rank)
         ws = sf.World(c3)
         ws.set_stream(stream.cuda_stream)
-        # warm-up: short solves from zero let the autotuner try each launch shape and capture the graph the timed
-        # solve replays (the shape is independent of the sweep limit)
-        for _ in range(10):
+        # warm-up: two full solves from zero. The first teaches the launch split each structure's sweep count (the
+        # structures that take longest get the large blocks); the second captures the graph the timed solve replays
+        for _ in range(2):
             ws.set_phi(np.zeros(c3.n_static, np.float32))
-            ws.structure_solve(-1, omega=1.7, tol=1e-6, max_sweeps=1500)
+            ws.structure_solve(-1, omega=1.7, tol=1e-6, max_sweeps=args.sor_max_sweeps)
         ws.set_phi(np.zeros(c3.n_static, np.float32))
         torch.cuda.synchronize()
         t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
@@ -650,7 +650,12 @@ def our_arm(args, rank, world, local, pg):
             roof = {"bound": "hbm", "unit": "GB/s", "achieved": SOR_BYTES_PER_BRICK_SWEEP * bs / (s_ms * 1e-3) / 1e9,
                     "peak": hbm, "frac": SOR_BYTES_PER_BRICK_SWEEP * bs / (s_ms * 1e-3) / 1e9 / hbm,
                     "unit_bytes": f"{SOR_BYTES_PER_BRICK_SWEEP} B per brick-sweep"}
+        sw, _ = ws.solve_detail()
+        counts = np.bincount(c3.static_sid, minlength=len(sw))
+        slow = np.argsort(-sw.astype(np.int64))[:5]
+        sor_slowest = [{"structure": int(q), "bricks": int(counts[q]), "sweeps": int(sw[q])} for q in slow]
         sor = {"brick_sweeps_per_s": bs / (s_ms * 1e-3), "bricks": c3.n_static, "structures": rep.structures,
+               "slowest": sor_slowest,
                "path": "one thread-block cluster per structure" if cluster else "grid-wide persistent kernel",
                "cuda_graph_replays": graphs, "autotune_blocks_per_sm": ws.tuning()["sor"],
                "max_sweeps": rep.max_sweeps_done, "brick_sweeps": bs, "ms": s_ms, "max_residual": rep.max_residual,

@@ -194,16 +194,22 @@ sf_status sf_structure_loads(sf_world *w, const int32_t *structures, uint32_t n_
  *                        below 1e-4 one on every third frame, counted by (frame + structure) % 3 == 0, else none;
  *                        otherwise 1 for more than 15,000 bricks and 6 for fewer; then more while its residual is at
  *                        least 4e-4, it has done fewer than 90 and a budget of 160,000 brick-updates shared in order
- *                        is left), the settle timers (src/lib.rs:1334), then warm_step (src/lib.rs:1068-1079: pending
- *                        warm-up sweeps in structure order from a budget of 120,000 brick-updates, omega 1.9 while
- *                        more than 60 remain, then 1.0). Only structures passed to sf_structure_warm are swept.
- * Joints are judged live (the `live` of sf_structure_check) once a structure's settle timer is <= 0 and its residual
- * is below 1.5e-3 (src/lib.rs:1328); sf_read_structure_state returns both (n_structures entries each, any NULL). */
+ *                        is left); the joint pass of the structures that are live (settle timer <= 0 and residual
+ *                        below 1.5e-3, src/lib.rs:1323-1339: fatigue, failures and crushes applied, one crush budget
+ *                        of 300 for the frame); the settle timers (src/lib.rs:1334); then warm_step
+ *                        (src/lib.rs:1068-1079: pending warm-up sweeps in structure order from a budget of 120,000
+ *                        brick-updates, omega 1.9 while more than 60 remain, then 1.0). Only structures passed to
+ *                        sf_structure_warm are swept.
+ * sf_read_structure_state returns per structure its pending warm-up, solved flag, settle timer and last residual
+ * (n_structures entries each, any NULL). */
 typedef struct sf_frame_report {
     uint32_t sweeps;            /* structural sweeps this frame, summed over structures */
     uint32_t warm_sweeps;       /* warm-up sweeps this frame, summed over structures */
     uint64_t brick_updates;     /* bricks x sweeps, both kinds */
     double ms;                  /* device time of the frame's solves */
+    uint32_t live;              /* structures whose joints were judged live this frame */
+    float max_ratio;            /* the live joints' largest ratio */
+    uint64_t joints, over, failed, crushed;   /* the live joint pass, as sf_check_report */
 } sf_frame_report;
 sf_status sf_structure_warm(sf_world *w, int32_t structure);
 sf_status sf_structure_frame(sf_world *w, uint32_t frame, float dt, const int32_t *active, uint32_t n_active,

@@ -208,10 +208,12 @@ class OracleWorld:
         self.lib.ow_structure_warm(self.h, int(s))
 
     def structure_frame(self, frame, dt, active):
+        """One frame of the load-path schedule; returns (sweeps, warm_sweeps, live, joints, over, failed, crushed,
+        max_ratio) of the frame."""
         a = np.ascontiguousarray(active, np.int32)
-        out = np.zeros(2, np.uint32)
+        out = np.zeros(8, np.uint32)
         self.lib.ow_structure_frame(self.h, int(frame), float(dt), _p(a, C.c_int32), len(a), _p(out, C.c_uint32))
-        return int(out[0]), int(out[1])
+        return tuple(int(x) for x in out[:7]) + (float(out[7:8].view(np.float32)[0]),)
 
     def structure_state(self, n):
         warm = np.zeros(n, np.int32); solved = np.zeros(n, np.uint8); settle = np.zeros(n, np.float32)

@@ -397,79 +397,6 @@ static SorResult sor_solve(World& w, int s, float omega, double tol, uint32_t ma
     return r;
 }
 
-// ---------------------------------------------------------------- the per-frame schedule (src/lib.rs:1061-1079, 1268-1281)
-// Restated with red-black FP64 sweeps that continue from the stored f64 potentials (the GPU path's arithmetic):
-// the schedule (which structures sweep, how often, with which omega, from which budget) is the reference's.
-static double rb64_sweep(World& w, const std::vector<uint32_t>& list, double omega) {
-    double md = 0.0, mp = 1.0;
-    for (int colour = 0; colour < 2; colour++)
-        for (uint32_t i : list) {
-            if (((w.bx[i] + w.by[i] + w.bz[i]) & 1) != colour) continue;
-            double d = sor_brick64(w, i, omega);
-            if (d > md) md = d;
-        }
-    for (uint32_t i : list) if (w.phi64[i] > mp) mp = w.phi64[i];
-    return md / mp;
-}
-static void sched_size(World& w) {
-    int32_t n = 0;
-    for (uint32_t i = 0; i < w.ns; i++) n = std::max(n, w.sid[i] + 1);
-    if ((int32_t)w.st_warm.size() < n) {
-        w.st_warm.resize(n, 0); w.st_solved.resize(n, 0); w.st_settle.resize(n, 0.0f); w.st_resid.resize(n, 0.0);
-    }
-}
-static void warm_struct(World& w, int32_t s) {   // src/lib.rs:1061-1066
-    sched_size(w);
-    if (s < 0 || s >= (int32_t)w.st_warm.size() || w.st_solved[s]) return;
-    w.st_solved[s] = 1;
-    w.st_warm[s] = 560;
-    w.st_settle[s] = 1e9f;
-}
-static void structure_frame(World& w, uint32_t frame, float dt, const int32_t* active, uint32_t n_active, uint32_t* counts) {
-    sched_size(w);
-    const int32_t nst = (int32_t)w.st_warm.size();
-    std::vector<std::vector<uint32_t>> lists(nst);
-    for (uint32_t i = 0; i < w.ns; i++) if (w.sid[i] >= 0 && w.in_struct(i, w.sid[i])) lists[w.sid[i]].push_back(i);
-    uint32_t sweeps = 0, warm_sweeps = 0;
-    std::vector<int32_t> act;
-    for (uint32_t t = 0; t < n_active; t++) {
-        int32_t s = active[t];
-        if (s >= 0 && s < nst && w.st_solved[s] && !lists[s].empty()) act.push_back(s);
-    }
-    // the sweep loop of structural (src/lib.rs:1268-1281)
-    int64_t budget = 160000;
-    for (int32_t s : act) {
-        const int64_t size = (int64_t)lists[s].size();
-        const uint32_t nmin = w.st_resid[s] < 1e-4 ? (((frame + (uint32_t)s) % 3 == 0) ? 1u : 0u) : (size > 15000 ? 1u : 6u);
-        if (nmin == 0) continue;
-        uint32_t n = 0;
-        for (;;) {
-            w.st_resid[s] = rb64_sweep(w, lists[s], (double)1.85f);
-            n++; budget -= size;
-            if (n >= nmin && (w.st_resid[s] < (double)4e-4f || n >= 90 || budget <= 0)) break;
-        }
-        sweeps += n;
-    }
-    // the settle timers (src/lib.rs:1334)
-    for (int32_t s : act) if (w.st_settle[s] > 0.0f && w.st_warm[s] == 0) w.st_settle[s] -= dt;
-    // warm_step (src/lib.rs:1068-1079)
-    int64_t wb = 120000;
-    for (int32_t s = 0; s < nst; s++) {
-        const int64_t size = (int64_t)lists[s].size();
-        if (size == 0) continue;
-        while (w.st_warm[s] > 0 && wb > 0) {
-            const float om = w.st_warm[s] > 60 ? 1.9f : 1.0f;
-            w.st_resid[s] = rb64_sweep(w, lists[s], (double)om);
-            w.st_warm[s] -= 1;
-            wb -= size;
-            warm_sweeps++;
-            if (w.st_warm[s] == 0) w.st_settle[s] = 0.3f;
-        }
-    }
-    for (int32_t s = 0; s < nst; s++) for (uint32_t i : lists[s]) w.phi[i] = (float)w.phi64[i];
-    if (counts) { counts[0] = sweeps; counts[1] = warm_sweeps; }
-}
-
 // ---------------------------------------------------------------- joint checks (src/lib.rs:1153-1227)
 enum { J_HOLD = 0, J_FATIGUE = 1, J_FAIL = 2, J_CRUSH = 3 };
 struct Joint { uint32_t i, axis, j, decision, crushed; float ratio, bond_after; };
@@ -535,6 +462,103 @@ static float stress_brick(World& w, uint32_t i, float dt, bool live, std::vector
         out.push_back(jr);
     }
     return maxr;
+}
+
+// ---------------------------------------------------------------- the per-frame schedule (src/lib.rs:1061-1079, 1268-1281)
+// Restated with red-black FP64 sweeps that continue from the stored f64 potentials (the GPU path's arithmetic):
+// the schedule (which structures sweep, how often, with which omega, from which budget) is the reference's.
+static double rb64_sweep(World& w, const std::vector<uint32_t>& list, double omega) {
+    double md = 0.0, mp = 1.0;
+    for (int colour = 0; colour < 2; colour++)
+        for (uint32_t i : list) {
+            if (((w.bx[i] + w.by[i] + w.bz[i]) & 1) != colour) continue;
+            double d = sor_brick64(w, i, omega);
+            if (d > md) md = d;
+        }
+    for (uint32_t i : list) if (w.phi64[i] > mp) mp = w.phi64[i];
+    return md / mp;
+}
+static void sched_size(World& w) {
+    int32_t n = 0;
+    for (uint32_t i = 0; i < w.ns; i++) n = std::max(n, w.sid[i] + 1);
+    if ((int32_t)w.st_warm.size() < n) {
+        w.st_warm.resize(n, 0); w.st_solved.resize(n, 0); w.st_settle.resize(n, 0.0f); w.st_resid.resize(n, 0.0);
+    }
+}
+static void warm_struct(World& w, int32_t s) {   // src/lib.rs:1061-1066
+    sched_size(w);
+    if (s < 0 || s >= (int32_t)w.st_warm.size() || w.st_solved[s]) return;
+    w.st_solved[s] = 1;
+    w.st_warm[s] = 560;
+    w.st_settle[s] = 1e9f;
+}
+static void structure_frame(World& w, uint32_t frame, float dt, const int32_t* active, uint32_t n_active, uint32_t* counts) {
+    sched_size(w);
+    const int32_t nst = (int32_t)w.st_warm.size();
+    std::vector<std::vector<uint32_t>> lists(nst);
+    for (uint32_t i = 0; i < w.ns; i++) if (w.sid[i] >= 0 && w.in_struct(i, w.sid[i])) lists[w.sid[i]].push_back(i);
+    uint32_t sweeps = 0, warm_sweeps = 0;
+    std::vector<int32_t> act;
+    for (uint32_t t = 0; t < n_active; t++) {
+        int32_t s = active[t];
+        if (s >= 0 && s < nst && w.st_solved[s] && !lists[s].empty()) act.push_back(s);
+    }
+    // the sweep loop of structural (src/lib.rs:1268-1281)
+    int64_t budget = 160000;
+    for (int32_t s : act) {
+        const int64_t size = (int64_t)lists[s].size();
+        const uint32_t nmin = w.st_resid[s] < 1e-4 ? (((frame + (uint32_t)s) % 3 == 0) ? 1u : 0u) : (size > 15000 ? 1u : 6u);
+        if (nmin == 0) continue;
+        uint32_t n = 0;
+        for (;;) {
+            w.st_resid[s] = rb64_sweep(w, lists[s], (double)1.85f);
+            n++; budget -= size;
+            if (n >= nmin && (w.st_resid[s] < (double)4e-4f || n >= 90 || budget <= 0)) break;
+        }
+        sweeps += n;
+    }
+    for (int32_t s : act) for (uint32_t i : lists[s]) w.phi[i] = (float)w.phi64[i];
+    // the joint pass (src/lib.rs:1323-1339) of the live structures, in structure order, one crush budget a frame
+    // (src/lib.rs:3645); structures that are not live only shade their stress display there and are left out
+    std::vector<int32_t> live;
+    for (int32_t s : act) if (w.st_settle[s] <= 0.0f && w.st_resid[s] < (double)1.5e-3f) live.push_back(s);
+    std::sort(live.begin(), live.end());
+    w.crush_n = 0;
+    uint32_t joints = 0, over = 0, failed = 0, crushed = 0;
+    float mr = 0.0f;
+    for (int32_t s : live) {
+        std::vector<Joint> out;
+        for (uint32_t i : lists[s]) if (w.in_struct(i, s)) w.stress[i] = 0.0f;
+        for (uint32_t i : lists[s]) if (w.in_struct(i, s)) { float r = stress_brick(w, i, dt, true, out); if (r > mr) mr = r; }
+        for (const Joint& j : out) {
+            joints++;
+            if (j.ratio > 1.0f) over++;
+            if (j.decision == J_FAIL) failed++;
+            if (j.decision == J_CRUSH) crushed++;
+        }
+    }
+    // the settle timers (src/lib.rs:1334)
+    for (int32_t s : act) if (w.st_settle[s] > 0.0f && w.st_warm[s] == 0) w.st_settle[s] -= dt;
+    // warm_step (src/lib.rs:1068-1079)
+    int64_t wb = 120000;
+    for (int32_t s = 0; s < nst; s++) {
+        const int64_t size = (int64_t)lists[s].size();
+        if (size == 0) continue;
+        while (w.st_warm[s] > 0 && wb > 0) {
+            const float om = w.st_warm[s] > 60 ? 1.9f : 1.0f;
+            w.st_resid[s] = rb64_sweep(w, lists[s], (double)om);
+            w.st_warm[s] -= 1;
+            wb -= size;
+            warm_sweeps++;
+            if (w.st_warm[s] == 0) w.st_settle[s] = 0.3f;
+        }
+    }
+    for (int32_t s = 0; s < nst; s++) for (uint32_t i : lists[s]) w.phi[i] = (float)w.phi64[i];
+    if (counts) {
+        counts[0] = sweeps; counts[1] = warm_sweeps; counts[2] = (uint32_t)live.size(); counts[3] = joints;
+        counts[4] = over; counts[5] = failed; counts[6] = crushed;
+        std::memcpy(&counts[7], &mr, 4);
+    }
 }
 
 // ---------------------------------------------------------------- rigid step (src/lib.rs:1367-1783)

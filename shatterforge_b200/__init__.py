@@ -86,7 +86,9 @@ class CheckReport(C.Structure):
 
 
 class FrameReport(C.Structure):
-    _fields_ = [("sweeps", C.c_uint32), ("warm_sweeps", C.c_uint32), ("brick_updates", C.c_uint64), ("ms", C.c_double)]
+    _fields_ = [("sweeps", C.c_uint32), ("warm_sweeps", C.c_uint32), ("brick_updates", C.c_uint64), ("ms", C.c_double),
+                ("live", C.c_uint32), ("max_ratio", C.c_float), ("joints", C.c_uint64), ("over", C.c_uint64),
+                ("failed", C.c_uint64), ("crushed", C.c_uint64)]
 
 
 class WorldInfo(C.Structure):

@@ -412,37 +412,54 @@ __global__ void __launch_bounds__(SOR_CL_MAX_THREADS) k_sor_cluster(SorClusterAr
     cl.sync();
     for (uint32_t sweep = 0; sweep < max_sweeps; sweep++) {
         unsigned long long accd = 0ull, accp = 0ull;
+        // One cell's update: the new potential (unchanged when it has no conductance) and |dphi|. Cells of one
+        // colour never read each other, so a thread computes two of them before it stores either: the two
+        // dependent f64 chains (neighbour loads, divide) overlap.
+        auto update = [&](uint32_t i, double &p, double &dabs) -> bool {
+            const uint32_t cd = code[i];
+            if (!(cd & CELL_ACTIVE)) return false;
+            double sk = 0.0, skp = 0.0;
+#pragma unroll
+            for (int d = 0; d < 6; d++) {
+                const uint32_t lm = (cd >> (4 * d)) & 15u;
+                if (lm == 0) continue;
+                const uint32_t g = nbr[i * 6 + d];
+                if (g == NO_CELL) { atomicOr(A.err, (unsigned)ERR_SOR_NONFINITE); continue; }
+                const uint32_t r = g >> 13, l = g & 8191u;
+                const double pj = r == rank ? phi[l] : cl.map_shared_rank(phi, r)[l];
+                const double k = kt[2 * lm + ((d >> 1) == 1 ? 1 : 0)];
+                sk += k;
+                skp += k * pj;
+            }
+            if (cd & (1u << 28)) sk += kt[32 + ((cd >> 24) & 15u)];
+            p = phi[i];
+            dabs = 0.0;
+            if (sk > 0.0) {
+                const double target = ((double)rhs[i] + skp) / sk;
+                const double dd = omega * (target - p);
+                p += dd;
+                dabs = fabs(dd);
+                if (!isfinite(p)) atomicOr(A.err, (unsigned)ERR_SOR_NONFINITE);
+            }
+            return true;
+        };
         for (int colour = 0; colour < 2; colour++) {
             const uint32_t c0 = colour ? ev : 0u, c1 = colour ? my : ev;
-            for (uint32_t i = c0 + tid; i < c1; i += blockDim.x) {
-                const uint32_t cd = code[i];
-                if (!(cd & CELL_ACTIVE)) continue;
-                double sk = 0.0, skp = 0.0;
-#pragma unroll
-                for (int d = 0; d < 6; d++) {
-                    const uint32_t lm = (cd >> (4 * d)) & 15u;
-                    if (lm == 0) continue;
-                    const uint32_t g = nbr[i * 6 + d];
-                    if (g == NO_CELL) { atomicOr(A.err, (unsigned)ERR_SOR_NONFINITE); continue; }
-                    const uint32_t r = g >> 13, l = g & 8191u;
-                    const double pj = r == rank ? phi[l] : cl.map_shared_rank(phi, r)[l];
-                    const double k = kt[2 * lm + ((d >> 1) == 1 ? 1 : 0)];
-                    sk += k;
-                    skp += k * pj;
+            for (uint32_t i = c0 + tid; i < c1; i += 2 * blockDim.x) {
+                const uint32_t i2 = i + blockDim.x;
+                double p1 = 0.0, d1 = 0.0, p2 = 0.0, d2 = 0.0;
+                const bool a1 = update(i, p1, d1);
+                const bool a2 = i2 < c1 && update(i2, p2, d2);
+                if (a1) {
+                    phi[i] = p1;
+                    accd = max(accd, (unsigned long long)__double_as_longlong(d1));
+                    if (p1 > 0.0) accp = max(accp, (unsigned long long)__double_as_longlong(p1));
                 }
-                if (cd & (1u << 28)) sk += kt[32 + ((cd >> 24) & 15u)];
-                double p = phi[i];
-                double dabs = 0.0;
-                if (sk > 0.0) {
-                    const double target = ((double)rhs[i] + skp) / sk;
-                    const double dd = omega * (target - p);
-                    p += dd;
-                    phi[i] = p;
-                    dabs = fabs(dd);
-                    if (!isfinite(p)) atomicOr(A.err, (unsigned)ERR_SOR_NONFINITE);
+                if (a2) {
+                    phi[i2] = p2;
+                    accd = max(accd, (unsigned long long)__double_as_longlong(d2));
+                    if (p2 > 0.0) accp = max(accp, (unsigned long long)__double_as_longlong(p2));
                 }
-                accd = max(accd, (unsigned long long)__double_as_longlong(dabs));
-                if (p > 0.0) accp = max(accp, (unsigned long long)__double_as_longlong(p));
             }
             if (colour == 0) cl.sync();
         }
@@ -1195,7 +1212,9 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     rep.ms = ms;
     for (uint32_t q : req) {
         rep.structures++;
-        if (!caps && q < st->h_last_sweeps.size() && e == SF_OK) st->h_last_sweeps[q] = sw[q];
+        // a solve that converged gives the structure's sweep count; one stopped by the sweep limit a lower bound
+        if (!caps && q < st->h_last_sweeps.size() && e == SF_OK)
+            st->h_last_sweeps[q] = rs[q] < (double)tol ? sw[q] : std::max(st->h_last_sweeps[q], sw[q]);
         if (e == SF_OK && sw[q]) st->h_resid[q] = rs[q];
         rep.max_sweeps_done = std::max(rep.max_sweeps_done, sw[q]);
         rep.brick_sweeps += (uint64_t)sw[q] * st->h_st_count[q];
@@ -1210,6 +1229,8 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     return e;
 }
 
+static sf_status check_impl(sf_world *w, int32_t structure, const int32_t *ids, uint32_t n_ids, float dt, int32_t live,
+                            sf_check_report *report);
 }  // namespace sf
 
 using namespace sf;
@@ -1296,8 +1317,25 @@ sf_status sf_structure_frame(sf_world *w, uint32_t frame, float dt, const int32_
         rep.sweeps += done;
         budget -= (int64_t)done * size;
     }
-    // structural's settle timers (src/lib.rs:1334): a structure whose warm-up is over settles for 0.3 s; its joints
-    // are judged live once settled with a residual below 1.5e-3 (src/lib.rs:1328; sf_read_structure_state)
+    // structural's joint pass (src/lib.rs:1323-1339): a structure's joints are judged live once it has settled and
+    // its residual is below 1.5e-3; the live structures' joints are checked in structure order with one crush budget
+    // (the reference's budget of 300 crushes a frame). A structure that is not live only shades its stress display in
+    // the reference (no joint changes), which is left out here.
+    {
+        std::vector<int32_t> live_ids;
+        for (int32_t q : act)
+            if (st->h_settle[q] <= 0.0f && st->h_resid[q] < (double)1.5e-3f) live_ids.push_back(q);
+        std::sort(live_ids.begin(), live_ids.end());
+        if (!live_ids.empty()) {
+            sf_check_report cr{};
+            e = check_impl(w, -1, live_ids.data(), (uint32_t)live_ids.size(), dt, 1, &cr);
+            if (e != SF_OK) return e;
+            rep.live = (uint32_t)live_ids.size();
+            rep.joints = cr.joints; rep.over = cr.over; rep.failed = cr.failed; rep.crushed = cr.crushed;
+            rep.max_ratio = cr.max_ratio;
+        }
+    }
+    // the settle timers (src/lib.rs:1334): a structure whose warm-up is over settles for 0.3 s
     for (int32_t q : act)
         if (st->h_settle[q] > 0.0f && st->h_warm[q] == 0) st->h_settle[q] -= dt;
     // warm_step (src/lib.rs:1068-1079): the pending warm-up sweeps of every structure in structure order, from a
@@ -1379,11 +1417,22 @@ sf_status sf_read_solve_detail(sf_world *w, uint32_t *sweeps, double *resid) {
 }
 
 sf_status sf_structure_check(sf_world *w, int32_t structure, float dt, int32_t live, sf_check_report *report) {
+    return check_impl(w, structure, nullptr, 0, dt, live, report);
+}
+
+sf_status sf_structure_loads(sf_world *w, const int32_t *structures, uint32_t n_structures);
+
+}  // extern "C"
+
+namespace sf {
+// joint checks of one structure, of all (structure -1), or of a list (ids), in structure order with one crush budget
+static sf_status check_impl(sf_world *w, int32_t structure, const int32_t *ids, uint32_t n_ids, float dt, int32_t live,
+                            sf_check_report *report) {
     if (!w) return SF_ERR_ARG;
     if (!w->sor) { set_error("this world holds no load-path state (a scene pool)"); return SF_ERR_STATE; }
     SorState *st = w->sor;
     std::vector<uint32_t> act, chunks, req;
-    sf_status r = sor_select(w, structure, act, chunks, req);
+    sf_status r = ids ? sor_select_set(w, ids, n_ids, act, chunks, req) : sor_select(w, structure, act, chunks, req);
     if (r != SF_OK) return r;
     cudaStream_t s = w->stream;
     uint32_t ns = w->ns, nst = w->n_struct;
@@ -1421,6 +1470,9 @@ sf_status sf_structure_check(sf_world *w, int32_t structure, float dt, int32_t l
     if (report) *report = rep;
     return SF_OK;
 }
+}  // namespace sf
+
+extern "C" {
 
 sf_status sf_structure_loads(sf_world *w, const int32_t *structures, uint32_t n_structures) {
     if (!w || (n_structures && !structures)) return SF_ERR_ARG;

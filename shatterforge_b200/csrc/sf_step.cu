@@ -33,14 +33,14 @@ namespace sf {
 struct StepState {
     Work wk;
     // hashed cell sort
-    DBuf<uint32_t> ckey, ckey_alt;   // (active scene index x HSIZE + bucket) fits 32 bits (checked per step)
-    DBuf<uint32_t> cval, cval_alt;
-    DBuf<uint32_t> aw_flag, awk_pos, awk_list, inc_flag, inc_pos, bucket_bits, scene_awake, scene_bricks;
-    uint32_t n_awk = 0, n_inc = 0;
+    DBuf<uint32_t> ckey, ckey_alt;   // per active brick: its hash key (active scene index x HSIZE + bucket) and rank
+    DBuf<uint32_t> cval;             // the hash table's entries: brick ids, bucket by bucket
+    DBuf<uint32_t> aw_flag, awk_pos, awk_list, bucket_bits, scene_awake, scene_bricks;
+    uint32_t n_awk = 0;
     bool use_sparse = false, last_sparse = false;
-    DBuf<uint2> brange;
+    DBuf<uint32_t> bstart;          // the hash table: per (active scene, bucket) count, then start (+1 for the end)
     DBuf<float4> srec;
-    DBuf<uint32_t> sinfo, scell;
+    DBuf<uint2> sent;
     DBuf<uint4> slot_id;
     DBuf<float4> slot_p, slot_n;
     // contacts, list order
@@ -215,54 +215,55 @@ __global__ void k_mark_buckets(const uint32_t *n_p, const uint32_t *awk, const u
                 if (!(__ldcg(&sb[h >> 5]) & m)) atomicOr(&sb[h >> 5], m);
             }
 }
-// key = (the scene's index in the active set, hashed cell), flagged when the brick goes into the hash. Dense form
-// (inc == null, most bricks awake): every live brick goes in, dead ones get none_key and sort last.
-__global__ void k_cell_keys(uint32_t nd, const uint32_t *list, uint32_t none_key, const uint32_t *kbody,
-                            const uint32_t *bscene, const uint32_t *scene_act, const uint32_t *scene_awake,
-                            const uint32_t *scene_bricks, const uint8_t *alive, const uint8_t *asleep, const float4 *wpos,
-                            const uint32_t *bits, uint32_t *key, uint32_t *val, uint32_t *inc) {
+// The spatial hash as a counting sort into the reference's 32768 buckets per active scene (build_hash,
+// src/lib.rs:1379-1395): each hashed brick takes an arrival rank in its bucket (k_hash_count), an exclusive scan of
+// the counts gives every bucket's start (the table is then CSR: bucket k holds [start[k], start[k + 1])), the bricks
+// are placed by start + rank (k_hash_place), and each bucket's few entries are put in ascending brick-id order
+// (k_hash_order), which is the order a walk from the highest id down needs (the reference's chain order).
+// A brick goes in when it is alive; in the sparse form (most bricks asleep) only when it is awake, its scene has more
+// than 1/8 of its bricks awake, or its bucket is one a walk can reach (gen_contacts walks only the 27 buckets around
+// an awake brick, so leaving other bricks out changes no walk).
+__global__ void k_hash_count(uint32_t nd, const uint32_t *list, const uint32_t *kbody, const uint32_t *bscene,
+                             const uint32_t *scene_act, const uint32_t *scene_awake, const uint32_t *scene_bricks,
+                             const uint8_t *alive, const uint8_t *asleep, const float4 *wpos, const uint32_t *bits,
+                             uint32_t *cnt, uint32_t *tkey, uint32_t *trank) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nd) return;
     const uint32_t i = pick(list, t);
     const uint32_t b = kbody[i];
-    if (!inc) {
-        uint32_t k = none_key;
-        if (alive[b]) {
-            const float4 p = wpos[i];
-            k = scene_act[bscene[b]] * HSIZE + hkey(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z));
-        }
-        key[t] = k;
-        val[t] = i;
-        return;
-    }
-    uint32_t in = 0;
+    uint32_t key = NONE, rank = 0;
     if (alive[b]) {
         const float4 p = wpos[i];
         const uint32_t sk = scene_act[bscene[b]];
         const uint32_t h = hkey(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z));
-        in = !asleep[b] || scene_full(scene_awake, scene_bricks, sk) ||
-             ((bits[(size_t)sk * (HSIZE / 32) + (h >> 5)] >> (h & 31)) & 1u);
-        key[t] = sk * HSIZE + h;
-        val[t] = i;
+        const bool in = !bits || !asleep[b] || scene_full(scene_awake, scene_bricks, sk) ||
+                        ((bits[(size_t)sk * (HSIZE / 32) + (h >> 5)] >> (h & 31)) & 1u);
+        if (in) {
+            key = sk * HSIZE + h;
+            rank = atomicAdd(&cnt[key], 1u);
+        }
     }
-    inc[t] = in;
+    tkey[t] = key;
+    trank[t] = rank;
 }
-__global__ void k_compact_keys(uint32_t nd, const uint32_t *inc, const uint32_t *pos, const uint32_t *key_in,
-                               const uint32_t *val_in, uint32_t *key, uint32_t *val) {
+__global__ void k_hash_place(uint32_t nd, const uint32_t *list, const uint32_t *tkey, const uint32_t *trank,
+                             const uint32_t *start, uint32_t *cval) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nd || !inc[t]) return;
-    const uint32_t o = pos[t];
-    key[o] = key_in[t];
-    val[o] = val_in[t];
+    if (t >= nd) return;
+    const uint32_t key = tkey[t];
+    if (key != NONE) cval[start[key] + trank[t]] = pick(list, t);
 }
-
-__global__ void k_bucket_ranges(uint32_t nd, uint32_t none_key, const uint32_t *key, uint2 *brange) {
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= nd) return;
-    uint32_t k = key[p];
-    if (k >= none_key) return;
-    if (p == 0 || key[p - 1] != k) brange[k].x = p;
-    if (p == nd - 1 || key[p + 1] != k) brange[k].y = p + 1;
+// a bucket holds a few bricks (the table has 32768 buckets a scene): insertion sort by brick id
+__global__ void k_hash_order(uint32_t nbk, const uint32_t *start, uint32_t *cval) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nbk) return;
+    const uint32_t lo = start[k], hi = start[k + 1];
+    for (uint32_t a = lo + 1; a < hi; a++) {
+        const uint32_t v = cval[a];
+        uint32_t b = a;
+        while (b > lo && cval[b - 1] > v) { cval[b] = cval[b - 1]; b--; }
+        cval[b] = v;
+    }
 }
 
 // A brick's world cell packed in 32 bits (x 11, y 10, z 11 bits about offsets 1024, 512, 1024), each coordinate
@@ -280,20 +281,20 @@ __device__ __forceinline__ bool wcell_near(uint32_t a, uint32_t b) {
     return (uint32_t)(dx + 2) <= 4u && (uint32_t)(dy + 2) <= 4u && (uint32_t)(dz + 2) <= 4u;
 }
 
-// Packed bucket entries in sorted order: world position and brick id, then body id with the asleep bit (31) and the
-// removed-brick bit (30), and the packed world cell, so a bucket walk reads contiguous arrays: the cells first, the
-// rest only for entries near enough to touch (a full bucket holds mostly other cells that share its hash).
-__global__ void k_bucket_records(uint32_t nd, const uint32_t *cval, const uint32_t *kbody, const uint8_t *kmat,
-                                 const uint8_t *asleep, const float4 *wpos, float4 *srec, uint32_t *sinfo,
-                                 uint32_t *scell) {
+// Packed bucket entries in sorted order: world position and brick id (srec), and the packed world cell with the body
+// id, its asleep bit (31) and the removed-brick bit (30) (sent), so a bucket walk reads contiguous arrays: the 8-byte
+// words first, the position only for entries near enough to touch (a full bucket holds mostly other cells that
+// share its hash).
+__global__ void k_bucket_records(const uint32_t *n_p, const uint32_t *cval, const uint32_t *kbody, const uint8_t *kmat,
+                                 const uint8_t *asleep, const float4 *wpos, float4 *srec, uint2 *sent) {
     uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nd) return;
+    if (q >= *n_p) return;
     uint32_t j = cval[q];
     uint32_t bj = kbody[j];
     float4 p = wpos[j];
     srec[q] = make_float4(p.x, p.y, p.z, __uint_as_float(j));
-    sinfo[q] = bj | (asleep[bj] ? 0x80000000u : 0u) | (kmat[j] == 0 ? 0x40000000u : 0u);
-    scell[q] = pack_wcell(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z));
+    sent[q] = make_uint2(pack_wcell(floor_cell(p.x), floor_cell(p.y), floor_cell(p.z)),
+                         bj | (asleep[bj] ? 0x80000000u : 0u) | (kmat[j] == 0 ? 0x40000000u : 0u));
 }
 
 // ---------------------------------------------------------------- contacts
@@ -305,9 +306,9 @@ struct ContactArgs {
     const uint8_t *alive, *asleep, *smat;
     const float4 *wpos, *v, *w;
     const float *rot, *rad;
-    const uint2 *brange;
+    const uint32_t *bstart;            // per (active scene, bucket): first entry; the next bucket's start ends it
     const float4 *srec;
-    const uint32_t *sinfo, *scell;
+    const uint2 *sent;
     uint32_t *ccount;
     const uint32_t *coff;
     uint8_t *wake;
@@ -318,6 +319,7 @@ struct ContactArgs {
     float4 *L_p, *L_n;
 };
 constexpr int CSLOTS = 12;
+constexpr int WALK = 8;        // bucket entries whose packed words one brick loads together
 
 // gen_contacts for one brick of an awake body (src/lib.rs:1410-1468), contacts emitted in the reference's order.
 template <bool WAKE, class Emit>
@@ -395,47 +397,69 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
         }
         const float lim2 = 4.0f * RB * RB;
         const uint32_t mycell = pack_wcell(hx, hy, hz);
-        const uint2 *br = A.brange + (size_t)sk * HSIZE;
+        const uint32_t *bst = A.bstart + (size_t)sk * HSIZE;
         for (int dz = -1; dz <= 1; dz++) {
-            // the layer's nine bucket ranges are fetched together (independent loads in flight), then walked in the
-            // reference's dy, dx order
-            uint2 rgs[9];
+            // The layer's nine buckets are walked as one sequence: bucket c (the reference's dy, dx order) from its
+            // highest brick id down; entry t of the sequence lies in bucket c with pre[c] <= t < pre[c + 1]. The
+            // nine buckets' bounds are fetched together, then the packed (cell, body) words of WALK entries at a time, so a
+            // brick waits on a few rounds of loads per layer instead of one per entry; only entries near enough to
+            // touch (a full bucket holds mostly other cells that share its hash) go on to the position record.
+            uint32_t hi[9], pre[10];
+            pre[0] = 0;
 #pragma unroll
-            for (int c = 0; c < 9; c++) rgs[c] = br[hkey(hx + (c % 3) - 1, hy + (c / 3) - 1, hz + dz)];
-#pragma unroll 1
             for (int c = 0; c < 9; c++) {
-                    uint2 rg = rgs[0];   // register select, not a dynamically indexed (local memory) array
+                const uint32_t h = hkey(hx + (c % 3) - 1, hy + (c / 3) - 1, hz + dz);
+                const uint32_t lo = bst[h];
+                hi[c] = bst[h + 1];
+                pre[c + 1] = pre[c] + (hi[c] - lo);
+            }
+            const uint32_t n = pre[9];
+            for (uint32_t b0 = 0; b0 < n; b0 += WALK) {
+                uint2 e[WALK];
+                uint32_t qq[WALK];
 #pragma unroll
-                    for (int k = 1; k < 9; k++) if (c == k) rg = rgs[k];
-                    for (uint32_t q = rg.y; q > rg.x; q--) {
-                        if (!wcell_near(mycell, A.scell[q - 1])) continue;
-                        const uint32_t info = A.sinfo[q - 1];
-                        const float4 rec = A.srec[q - 1];
-                        const uint32_t bj = info & 0x3FFFFFFFu;
-                        if (bj == a || (info & 0x40000000u)) continue;
-                        const uint32_t j = __float_as_uint(rec.w);
-                        const bool other_awake = !(info & 0x80000000u);
-                        if (other_awake && j < i) continue;
-                        const V3 pj = v3(rec.x, rec.y, rec.z);
-                        const V3 d = sub(p, pj);
-                        const float dd = dot(d, d);
-                        if (dd >= lim2 || dd < 1e-10f) continue;
-                        const float dist = sqrt_rn(dd);
-                        const V3 nn = mul(d, div_rn(1.0f, dist));
-                        const V3 cp = madd(pj, nn, dist * 0.5f);
-                        if (other_awake) emit(bj, bj, j, cp, nn, 2.0f * RB - dist);
-                        else {
-                            if (WAKE && speed > 0.7f) A.wake[bj] = 1;
-                            emit(STATIC, bj, j, cp, nn, 2.0f * RB - dist);
-                        }
+                for (int u = 0; u < WALK; u++) {
+                    const uint32_t t = b0 + u;
+                    uint32_t h = hi[0], p0 = pre[0];
+#pragma unroll
+                    for (int k = 1; k < 9; k++) if (t >= pre[k]) { h = hi[k]; p0 = pre[k]; }
+                    qq[u] = h - 1u - (t - p0);
+                    e[u] = t < n ? A.sent[qq[u]] : make_uint2(0u, 0u);
+                }
+#pragma unroll
+                for (int u = 0; u < WALK; u++) {
+                    if (b0 + u >= n) break;
+                    if (!wcell_near(mycell, e[u].x)) continue;
+                    const uint32_t info = e[u].y;
+                    const uint32_t bj = info & 0x3FFFFFFFu;
+                    if (bj == a || (info & 0x40000000u)) continue;
+                    const float4 rec = A.srec[qq[u]];
+                    const uint32_t j = __float_as_uint(rec.w);
+                    const bool other_awake = !(info & 0x80000000u);
+                    if (other_awake && j < i) continue;
+                    const V3 pj = v3(rec.x, rec.y, rec.z);
+                    const V3 d = sub(p, pj);
+                    const float dd = dot(d, d);
+                    if (dd >= lim2 || dd < 1e-10f) continue;
+                    const float dist = sqrt_rn(dd);
+                    const V3 nn = mul(d, div_rn(1.0f, dist));
+                    const V3 cp = madd(pj, nn, dist * 0.5f);
+                    if (other_awake) emit(bj, bj, j, cp, nn, 2.0f * RB - dist);
+                    else {
+                        if (WAKE && speed > 0.7f) A.wake[bj] = 1;
+                        emit(STATIC, bj, j, cp, nn, 2.0f * RB - dist);
                     }
+                }
             }
         }
     }
 }
 
 // pass 1: every contact of every awake brick counted; the first CSLOTS kept in the brick's slots
-__global__ void __launch_bounds__(128, 7) k_contacts_gen(ContactArgs A) {
+#ifndef SF_GEN_BLOCKS_PER_SM
+#define SF_GEN_BLOCKS_PER_SM 6   // 80 registers (a few spilled): measured faster than 4 or 5 blocks an SM
+#endif
+__global__ void __launch_bounds__(128, SF_GEN_BLOCKS_PER_SM) k_contacts_gen(ContactArgs A) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= A.nd) return;
     const uint32_t i = pick(A.list, t);
@@ -1364,13 +1388,12 @@ sf_status step_create(sf_world *w) {
     uint32_t nb = w->nb, nd = w->nd;
     const uint32_t nsc = std::max<uint32_t>(w->n_scenes, 1);
     cudaStream_t s = w->stream;
-    SF_CUDA(S->ckey.alloc(nd)); SF_CUDA(S->ckey_alt.alloc(nd)); SF_CUDA(S->cval.alloc(nd)); SF_CUDA(S->cval_alt.alloc(nd));
+    SF_CUDA(S->ckey.alloc(nd)); SF_CUDA(S->ckey_alt.alloc(nd)); SF_CUDA(S->cval.alloc(nd));
     SF_CUDA(S->aw_flag.alloc(nd)); SF_CUDA(S->awk_pos.alloc(nd)); SF_CUDA(S->awk_list.alloc(nd));
-    SF_CUDA(S->inc_flag.alloc(nd)); SF_CUDA(S->inc_pos.alloc(nd));
     SF_CUDA(S->bucket_bits.alloc((size_t)nsc * (HSIZE / 32)));
     SF_CUDA(S->scene_awake.alloc(nsc)); SF_CUDA(S->scene_bricks.alloc(nsc));
-    SF_CUDA(S->brange.alloc((size_t)nsc * HSIZE));
-    SF_CUDA(S->srec.alloc(nd)); SF_CUDA(S->sinfo.alloc(nd)); SF_CUDA(S->scell.alloc(nd));
+    SF_CUDA(S->bstart.alloc((size_t)nsc * HSIZE + 1));
+    SF_CUDA(S->srec.alloc(nd)); SF_CUDA(S->sent.alloc(nd));
     SF_CUDA(S->slot_id.alloc((size_t)nd * CSLOTS)); SF_CUDA(S->slot_p.alloc((size_t)nd * CSLOTS)); SF_CUDA(S->slot_n.alloc((size_t)nd * CSLOTS));
     SF_CUDA(S->ccount.alloc((size_t)nd + 1)); SF_CUDA(S->coff.alloc((size_t)nd + 1));
     SF_CUDA(S->bm_count.alloc((size_t)nb + 1)); SF_CUDA(S->bm_start.alloc((size_t)nb + 1)); SF_CUDA(S->bm_fill.alloc((size_t)nb + 1));
@@ -1540,7 +1563,6 @@ static sf_status substep(sf_world *w, float h) {
         set_error("%zu active scenes exceed the hash key range", S->act.size());
         return SF_ERR_CAPACITY;
     }
-    const uint32_t none_key = (uint32_t)S->act.size() * HSIZE;
     std::fill(S->act_brick_base.begin(), S->act_brick_base.end(), NONE);
     if (nb == 0 || nd == 0) {
         SF_CUDA(cudaMemsetAsync(S->dev.p, 0, DV_ALIVE * sizeof(uint32_t), s));
@@ -1567,59 +1589,48 @@ static sf_status substep(sf_world *w, float h) {
     // Dense form: every live brick hashed, every active brick a contact thread. Both give the same contacts.
     const bool sparse = S->use_sparse;
     S->last_sparse = sparse;
-    uint32_t n_awk = nd, n_inc = nd;
+    uint32_t n_awk = nd;
     const uint32_t *clist = klist;
-    if (!sparse) {
-        k_cell_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, none_key, w->k_body.p, w->b_scene.p, S->scene_act.p,
-                                                      nullptr, nullptr, w->b_alive.p, w->b_asleep.p, w->k_wpos.p, nullptr,
-                                                      S->ckey.p, S->cval.p, nullptr);
-        L++;
-    } else {
-    clist = S->awk_list.p;
-    SF_CUDA(cudaMemsetAsync(S->scene_awake.p, 0, S->act.size() * 4, s));
-    k_awake_flags<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, w->k_body.p, w->b_scene.p, S->scene_act.p, w->b_alive.p,
-                                                    w->b_asleep.p, S->aw_flag.p, S->scene_awake.p);
-    SF_CUDA(exclusive_scan_u32(S->aw_flag.p, S->awk_pos.p, nd, S->dev.p + DV_AWK, S->wk, s));
-    k_compact_list<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, S->aw_flag.p, S->awk_pos.p, S->awk_list.p);
-    SF_CUDA(cudaMemsetAsync(S->bucket_bits.p, 0, (size_t)S->act.size() * (HSIZE / 32) * 4, s));
-    k_mark_buckets<<<grid_for(nd, 128), 128, 0, s>>>(S->dev.p + DV_AWK, S->awk_list.p, w->k_body.p, w->b_scene.p,
-                                                     S->scene_act.p, S->scene_awake.p, S->scene_bricks.p, w->k_wpos.p,
-                                                     S->bucket_bits.p);
-    k_cell_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, none_key, w->k_body.p, w->b_scene.p, S->scene_act.p,
-                                                  S->scene_awake.p, S->scene_bricks.p, w->b_alive.p, w->b_asleep.p,
-                                                  w->k_wpos.p, S->bucket_bits.p, S->ckey_alt.p, S->cval_alt.p,
-                                                  S->inc_flag.p);
-    SF_CUDA(exclusive_scan_u32(S->inc_flag.p, S->inc_pos.p, nd, S->dev.p + DV_INC, S->wk, s));
-    k_compact_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, S->inc_flag.p, S->inc_pos.p, S->ckey_alt.p, S->cval_alt.p,
-                                                     S->ckey.p, S->cval.p);
-    L += 5;
-    SF_CUDA(cudaMemcpyAsync(S->h_dev + DV_AWK, S->dev.p + DV_AWK, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    SF_CUDA(cudaStreamSynchronize(s));
-    n_awk = S->h_dev[DV_AWK];
-    n_inc = S->h_dev[DV_INC];
+    const size_t nbk = S->act.size() * (size_t)HSIZE;
+    if (sparse) {
+        clist = S->awk_list.p;
+        SF_CUDA(cudaMemsetAsync(S->scene_awake.p, 0, S->act.size() * 4, s));
+        k_awake_flags<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, w->k_body.p, w->b_scene.p, S->scene_act.p, w->b_alive.p,
+                                                        w->b_asleep.p, S->aw_flag.p, S->scene_awake.p);
+        SF_CUDA(exclusive_scan_u32(S->aw_flag.p, S->awk_pos.p, nd, S->dev.p + DV_AWK, S->wk, s));
+        k_compact_list<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, S->aw_flag.p, S->awk_pos.p, S->awk_list.p);
+        SF_CUDA(cudaMemsetAsync(S->bucket_bits.p, 0, (size_t)S->act.size() * (HSIZE / 32) * 4, s));
+        k_mark_buckets<<<grid_for(nd, 128), 128, 0, s>>>(S->dev.p + DV_AWK, S->awk_list.p, w->k_body.p, w->b_scene.p,
+                                                         S->scene_act.p, S->scene_awake.p, S->scene_bricks.p, w->k_wpos.p,
+                                                         S->bucket_bits.p);
+        L += 3;
+    }
+    // the hash table (counting sort into the buckets; see k_hash_count)
+    SF_CUDA(cudaMemsetAsync(S->bstart.p, 0, nbk * 4, s));
+    k_hash_count<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, w->k_body.p, w->b_scene.p, S->scene_act.p,
+                                                   sparse ? S->scene_awake.p : nullptr, S->scene_bricks.p, w->b_alive.p,
+                                                   w->b_asleep.p, w->k_wpos.p, sparse ? S->bucket_bits.p : nullptr,
+                                                   S->bstart.p, S->ckey.p, S->ckey_alt.p);
+    SF_CUDA(exclusive_scan_u32(S->bstart.p, S->bstart.p, nbk, S->bstart.p + nbk, S->wk, s));
+    k_hash_place<<<grid_for(nd, 256), 256, 0, s>>>(nd, klist, S->ckey.p, S->ckey_alt.p, S->bstart.p, S->cval.p);
+    k_hash_order<<<grid_for(nbk, 256), 256, 0, s>>>((uint32_t)nbk, S->bstart.p, S->cval.p);
+    k_bucket_records<<<grid_for(nd, 256), 256, 0, s>>>(S->bstart.p + nbk, S->cval.p, w->k_body.p, w->k_mat.p, w->b_asleep.p,
+                                                       w->k_wpos.p, S->srec.p, S->sent.p);
+    L += 4;
+    if (sparse) {
+        SF_CUDA(cudaMemcpyAsync(S->h_dev + DV_AWK, S->dev.p + DV_AWK, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        SF_CUDA(cudaStreamSynchronize(s));
+        n_awk = S->h_dev[DV_AWK];
     }
     S->n_awk = n_awk;
-    S->n_inc = n_inc;
-    {
-        bool alt = false;   // the sorted keys stay where the last pass left them
-        SF_CUDA(radix_sort_u32(S->ckey.p, S->cval.p, S->ckey_alt.p, S->cval_alt.p, n_inc, bits_for(none_key), S->wk, s, &alt));
-        if (alt) { S->ckey.swap(S->ckey_alt); S->cval.swap(S->cval_alt); }
-    }
-    SF_CUDA(cudaMemsetAsync(S->brange.p, 0, (size_t)S->act.size() * HSIZE * sizeof(uint2), s));
-    if (n_inc) {
-        k_bucket_ranges<<<grid_for(n_inc, 256), 256, 0, s>>>(n_inc, none_key, S->ckey.p, S->brange.p);
-        k_bucket_records<<<grid_for(n_inc, 256), 256, 0, s>>>(n_inc, S->cval.p, w->k_body.p, w->k_mat.p, w->b_asleep.p,
-                                                              w->k_wpos.p, S->srec.p, S->sinfo.p, S->scell.p);
-        L += 2;
-    }
     prof_mark(w);
     // contacts: generate into slots and count, scan, place in list order
     ContactArgs C;
     C.nd = n_awk; C.list = clist; C.scene_act = S->scene_act.p;
     C.sbox = w->sbox.p; C.kbody = w->k_body.p; C.bscene = w->b_scene.p; C.ctab = w->ctab.p; C.cpool = w->cpool.p;
     C.alive = w->b_alive.p; C.asleep = w->b_asleep.p; C.smat = w->s_mat.p; C.wpos = w->k_wpos.p;
-    C.v = w->b_v.p; C.w = w->b_w.p; C.rot = w->b_rot.p; C.rad = w->b_rad.p; C.brange = S->brange.p; C.srec = S->srec.p;
-    C.sinfo = S->sinfo.p; C.scell = S->scell.p; C.ccount = S->ccount.p; C.coff = S->coff.p; C.wake = w->b_wake.p;
+    C.v = w->b_v.p; C.w = w->b_w.p; C.rot = w->b_rot.p; C.rad = w->b_rad.p; C.bstart = S->bstart.p; C.srec = S->srec.p;
+    C.sent = S->sent.p; C.ccount = S->ccount.p; C.coff = S->coff.p; C.wake = w->b_wake.p;
     C.slot_id = S->slot_id.p; C.slot_p = S->slot_p.p; C.slot_n = S->slot_n.p;
     C.L_a = S->L_a.p; C.L_b = S->L_b.p; C.L_bo = S->L_bo.p; C.L_ba = S->L_ba.p; C.L_bb = S->L_bb.p; C.L_p = S->L_p.p; C.L_n = S->L_n.p;
     cudaEvent_t g0 = nullptr, g1 = nullptr;

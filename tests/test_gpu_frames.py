@@ -3,8 +3,9 @@ src/lib.rs:1061-1079, 1268-1281) on the GPU, through the C ABI, against the orac
 
 Both sides sweep red-black in FP64; the schedule decides per frame which structures sweep, how many times, with
 which relaxation and from which brick-update budget (160,000 for the structural loop, shared in order; 120,000 for
-the warm-up). Per frame the sweep counts, every structure's pending warm-up, settle timer and last residual, and
-the potentials must be identical.
+the warm-up), and which structures' joints are live. Per frame the sweep counts, the live joint pass's counts and
+largest ratio, every structure's pending warm-up, settle timer and last residual must be identical, and every ten
+frames the potentials and the bonds (after fatigue and failures).
 """
 import numpy as np
 import pytest
@@ -22,17 +23,20 @@ def run_frames(sf, oracle, sc, frames, warm_at=None, active=None):
     warm_at = warm_at or {s: 1 for s in ids}
     w = sf.World(sc)
     ow = oracle.OracleWorld(sc)
-    totals = [0, 0]
+    totals = [0, 0, 0]
     for f in range(1, frames + 1):
         for s, at in warm_at.items():
             if at == f:
                 w.structure_warm(s)
                 ow.structure_warm(s)
         rep = w.structure_frame(f, active, dt=DT)
-        osw, ows = ow.structure_frame(f, DT, active)
+        osw, ows, olive, oj, oover, ofail, ocrush, omr = ow.structure_frame(f, DT, active)
         assert (rep.sweeps, rep.warm_sweeps) == (osw, ows), f
+        assert (rep.live, rep.joints, rep.over, rep.failed, rep.crushed) == (olive, oj, oover, ofail, ocrush), f
+        assert rep.max_ratio == omr, f
         totals[0] += osw
         totals[1] += ows
+        totals[2] += olive
         gw, gs, gt, gr = w.structure_state()
         n = len(gw)
         owarm, osol, oset, ores = ow.structure_state(n)
@@ -42,6 +46,9 @@ def run_frames(sf, oracle, sc, frames, warm_at=None, active=None):
         np.testing.assert_array_equal(gr, ores, err_msg=f"frame {f}")
         if f % 10 == 0 or f == frames:
             np.testing.assert_array_equal(w.phi64(), ow.phi64(), err_msg=f"frame {f}")
+            b, _, _ = w.bonds()
+            ob, _ = ow.bonds()
+            np.testing.assert_array_equal(b, ob, err_msg=f"frame {f}")
     w.close()
     return totals
 
@@ -52,8 +59,8 @@ def test_frames_many_structures(sf, oracle):
     sc = S.config3_world(scale=0.05, n_struct=8)
     ids = sc.structure_ids()
     warm_at = {s: 1 + 3 * k for k, s in enumerate(ids)}
-    sw, ws = run_frames(sf, oracle, sc, 60, warm_at=warm_at)
-    assert ws == 560 * len(ids) and sw > 0
+    sw, ws, live = run_frames(sf, oracle, sc, 60, warm_at=warm_at)
+    assert ws == 560 * len(ids) and sw > 0 and live > 0
 
 
 def test_frames_frame_and_tower(sf, oracle):
@@ -67,5 +74,5 @@ def test_frames_frame_and_tower(sf, oracle):
     sc = S.Scene(xyz, np.concatenate([frame.static_mat, tower.static_mat]),
                  np.concatenate([frame.static_sid, tower.static_sid + 1]).astype(np.int32),
                  np.concatenate([frame.static_infill, tower.static_infill])).contiguous()
-    sw, ws = run_frames(sf, oracle, sc, 40)
+    sw, ws, live = run_frames(sf, oracle, sc, 40)
     assert ws > 0 and sw > 0
