@@ -46,11 +46,11 @@ SOLVE_BYTES_PER_CONTACT_ITER = 184     # contact 64 + impulse r/w 24 + both bodi
 # half-size mix: 722.7 MB for that launch / (≈847,700 contacts, from the same substep's k_prep grid, x 8 iterations);
 # the roofline's `traffic` scales it to this run's average launch
 SOLVE_DRAM_BYTES_PER_CONTACT_ITER = 106.6
-GEN_BYTES_PER_BRICK = 40               # SURVEY 8d: local offset 12 + body id 4 read, world position 12 written and re-read
+GEN_BYTES_PER_BRICK = 40               # local offset 12 + body id 4 read, world position 12 written and re-read
 GEN_BYTES_PER_CONTACT = 64             # one contact's setup written
-# DRAM bytes (read + write) of k_contacts_gen per algorithmic byte, from the ncu capture at the peak of contacts on
-# the half-size mix: 199 MB against 40 B x 2.19M bricks + 64 B x 0.85M contacts
-GEN_DRAM_PER_ALGORITHMIC_BYTE = 1.40
+# DRAM bytes (read + write) of k_contacts_gen per algorithmic byte, from the ncu capture in free fall on the half-size
+# mix (the benchmark window's regime): 77.2 MB against 40 B x 1.11M bricks + 64 B x ~4,000 contacts
+GEN_DRAM_PER_ALGORITHMIC_BYTE = 1.73
 SOR_BYTES_PER_BRICK_SWEEP = 24         # grid path: f64 potential r/w 16 + rhs 4 + link word 4
 SOR_CLUSTER_BYTES_PER_BRICK = 52       # cluster path, once per solve: staging reads (phi 8, rhs 4, code 4, sid 4,
                                        # place 4, neighbours 12) + the potential written back 8 + gather 8
@@ -284,7 +284,7 @@ def reference_arm(args, rank, world, pg):
     from oracle import binding as orc
     from shatterforge_b200 import scenes as S
     orc.use_native()
-    scenes = S.config4_scenes(n_scenes=args.scenes, scale=args.scale)
+    scenes = S.debris_mix(n_scenes=args.scenes, scale=args.scale)
     threads = host_threads()
     per = max(1.0, args.cpu_seconds)
     rate, steps, complete = cpu_body_steps(scenes, args.warmup, args.steps, per, threads)
@@ -292,7 +292,7 @@ def reference_arm(args, rank, world, pg):
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded)",
-        "config": {"workload": f"config4: {args.scenes} debris scenes, 1/60 s, {ITERS} iterations, 2 substeps",
+        "config": {"workload": f"debris mix: {args.scenes} scenes, 1/60 s, {ITERS} iterations, 2 substeps",
                    "sample": f"all {len(scenes)} scenes ({sum(s.n_bodies for s in scenes)} bodies), steps {args.warmup}.."
                              f"{args.warmup + args.steps} from rest; {complete} scenes ran every step (at most "
                              f"{per:.0f} s of timed stepping each)"},
@@ -321,7 +321,7 @@ def run_steps(w, k: int, awake_out: list | None = None):
     return alive, ms
 
 
-# ---------------------------------------------------------------- serving (config 5)
+# ---------------------------------------------------------------- serving
 def _latency(res, kind=None):
     lat = np.array([(r["t_done"] - r["t_arrival"]) * 1e3 for r in res if kind is None or r["kind"] == kind])
     if len(lat) == 0:
@@ -413,7 +413,7 @@ def serve_section(args):
     sizes = np.exp(rng.uniform(math.log(1000), math.log(100000), args.serve_worlds)).astype(np.int64)
     lib = S.ClusterLibrary(0x51ED)
     worlds = [S.debris_scene(int(nb), seed=5000 + k, lib=lib, name=f"served{k}") for k, nb in enumerate(sizes)]
-    structs = S.config3_world(seed=7)
+    structs = S.structure_lattice(seed=7)
     # one slot per world while the budget holds them all; otherwise fewer slots of the largest size (LRU eviction)
     slots = [SV.slot_for(w_) for w_ in worlds]
     budget = int(args.serve_budget_gb * 2**30) - 4 * 2**30      # headroom for the structures world and scratch
@@ -520,7 +520,7 @@ def our_arm(args, rank, world, local, pg):
 
     dev = torch.cuda.current_device()
     seed = rank_seed(rank)
-    scenes = S.config4_scenes(seed=seed, n_scenes=args.scenes, scale=args.scale)
+    scenes = S.debris_mix(seed=seed, n_scenes=args.scenes, scale=args.scale)
     n_bodies = sum(s.n_bodies for s in scenes)
     n_bricks = sum(s.n_body_bricks for s in scenes)
     # a stream of its own (not the legacy default stream), so the library may capture its launch sequences in graphs
@@ -620,7 +620,7 @@ def our_arm(args, rank, world, local, pg):
     # ---- load path: 37 structures in one lattice, one persistent launch to residual 1e-6
     sor = None
     if not args.no_sor:
-        c3 = S.config3_world(seed=2 + rank)
+        c3 = S.structure_lattice(seed=2 + rank)
         ws = sf.World(c3)
         ws.set_stream(stream.cuda_stream)
         # warm-up: two full solves from zero. The first teaches the launch split each structure's sweep count (the
@@ -691,7 +691,7 @@ def our_arm(args, rank, world, local, pg):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded generators of the configured shapes)",
-        "config": {"workload": f"config4: {args.scenes} debris scenes in one batch, {n_bodies} bodies, {n_bricks} brick spheres"
+        "config": {"workload": f"debris mix: {args.scenes} scenes in one batch, {n_bodies} bodies, {n_bricks} brick spheres"
                                f" per GPU, dt 1/60 s, {ITERS} iterations, 2 substeps",
                    "scenes": args.scenes, "bodies_per_gpu": n_bodies, "bricks_per_gpu": n_bricks, "iterations": ITERS,
                    "substeps": 2, "pinch_kill": 0, "l2": "inputs larger than L2 (world state several hundred MB)",

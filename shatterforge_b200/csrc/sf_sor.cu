@@ -1158,11 +1158,13 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
         cudaError_t e = cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s);
         if (e == cudaSuccess) e = cudaMemsetAsync(w->err.p, 0, sizeof(uint32_t), s);
         if (use_cl && n_big) {
+            // the large clusters are submitted first: each of their blocks needs most of an SM (1,024 threads and
+            // up to 229 KB of shared memory), and the small blocks fill what the large ones leave
             if (e == cudaSuccess) e = cudaEventRecord(st->fork, s);
+            if (e == cudaSuccess) e = cudaLaunchKernelEx(&ccfg, k_sor_cluster, CA);
             if (e == cudaSuccess) e = cudaStreamWaitEvent(st->aux, st->fork, 0);
             if (e == cudaSuccess) e = cudaLaunchKernelEx(&scfg, k_sor_cluster, CS);
             if (e == cudaSuccess) e = cudaEventRecord(st->join, st->aux);
-            if (e == cudaSuccess) e = cudaLaunchKernelEx(&ccfg, k_sor_cluster, CA);
             if (e == cudaSuccess) e = cudaStreamWaitEvent(s, st->join, 0);
         } else if (e == cudaSuccess) {
             e = use_cl ? cudaLaunchKernelEx(&ccfg, k_sor_cluster, CA)

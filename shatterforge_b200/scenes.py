@@ -136,7 +136,7 @@ def _quat_uniform(u1, u2, u3):
     return np.stack([a * np.sin(t1), a * np.cos(t1), b * np.sin(t2), b * np.cos(t2)], -1)
 
 
-def config1_frame(seed: int = 1, remove_columns: int = 2):
+def frame5_structure(seed: int = 1, remove_columns: int = 2):
     """5-storey concrete frame on 24 x 24 cells; storeys of 7 cells (6-cell 1 x 1 columns on a 3 x 3 grid, then a
     full 24 x 24 slab): 5 * (9 * 6 + 576) = 3150 bricks, structure 0, centred on the lattice origin.
     Returns (scene, removed_mask) where removed_mask marks the bricks of `remove_columns` seed-chosen ground columns."""
@@ -160,7 +160,7 @@ def config1_frame(seed: int = 1, remove_columns: int = 2):
 
 def loose_debris(n: int, seed: int, box_lo=(8.0, 2.0, -5.0), box_hi=(18.0, 12.0, 5.0),
                  mats=(CONC, MASON, WOOD)):
-    """n single-brick bodies at xorshift32-uniform positions in an axis-aligned box, at rest (config 1 debris)."""
+    """n single-brick bodies at xorshift32-uniform positions in an axis-aligned box, at rest (the debris beside the 5-storey frame)."""
     rng = XorShift32(seed)
     pose = np.zeros((n, 13), np.float32)
     mat = np.zeros(n, np.uint8)
@@ -174,19 +174,19 @@ def loose_debris(n: int, seed: int, box_lo=(8.0, 2.0, -5.0), box_hi=(18.0, 12.0,
     return np.arange(n + 1, dtype=np.uint32), xyz, mat, pose
 
 
-def config1_scene(seed: int = 1, n_debris: int = 1024, removed: bool = False) -> Scene:
-    """Config 1: the 5-storey frame plus 1,024 loose single-brick bodies 2 m above the ground beside it."""
-    frame, rm = config1_frame(seed)
+def frame5_debris_scene(seed: int = 1, n_debris: int = 1024, removed: bool = False) -> Scene:
+    """The 5-storey frame plus 1,024 loose single-brick bodies 2 m above the ground beside it."""
+    frame, rm = frame5_structure(seed)
     if removed:
         frame = frame.without_static(rm)
     bf, bxyz, bmat, pose = loose_debris(n_debris, seed + 101)
     frame.body_first, frame.body_brick_xyz, frame.body_brick_mat, frame.body_pose = bf, bxyz, bmat, pose
-    frame.name = "config1"
+    frame.name = "frame5_debris"
     return frame.contiguous()
 
 
-def config2_tower(seed: int = 2, remove_columns: int = 8):
-    """Config 2: a 16-storey tower on 48 x 48 cells, storeys of 7 cells. Per storey: 6-cell concrete columns on a
+def tower16_structure(seed: int = 2, remove_columns: int = 8):
+    """A 16-storey tower on 48 x 48 cells, storeys of 7 cells. Per storey: 6-cell concrete columns on a
     5 x 5 grid at 12-cell spacing, glass infill panels (6 cells high, non-bearing) in alternate 2-cell bays of the
     perimeter, and a 48 x 48 slab whose outer ring is masonry (the 1-brick perimeter) and whose inside is concrete.
     16 * (25 * 6 + 534 + 2304) = 47,808 bricks, structure 0. Returns (scene, removed_mask) where removed_mask marks
@@ -231,12 +231,12 @@ def config2_tower(seed: int = 2, remove_columns: int = 8):
     return sc, removed
 
 
-def config2_scene(seed: int = 2, n_bodies: int = 30000, removed: bool = True, kmax: int = 512,
+def tower16_debris_scene(seed: int = 2, n_bodies: int = 30000, removed: bool = True, kmax: int = 512,
                   lift: float = 60.0) -> Scene:
-    """Config 2 with its debris: the tower (ground columns removed) plus a pre-fragmented body set of n compound
+    """The 16-storey tower with its debris: the tower (ground columns removed) plus a pre-fragmented body set of n compound
     bodies of 1-512 bricks (k ~ Geometric(0.3), a few large slabs) falling beside and onto it from `lift` m above
-    the config-4 spawn layers (the roof is at 56 m)."""
-    tower, rm = config2_tower(seed)
+    the debris mix's spawn layers (the roof is at 56 m)."""
+    tower, rm = tower16_structure(seed)
     if removed:
         tower = tower.without_static(rm)
     lib = ClusterLibrary(seed ^ 0x1B873593, kmax=kmax)
@@ -256,11 +256,11 @@ def config2_scene(seed: int = 2, n_bodies: int = 30000, removed: bool = True, km
     pose[:, 1] += lift
     tower.body_first, tower.body_brick_xyz = first, (cl + np.array(ORIGIN, np.int32)).astype(np.int32)
     tower.body_brick_mat, tower.body_pose = bmat, pose
-    tower.name = "config2"
+    tower.name = "tower16_debris"
     return tower.contiguous()
 
 
-# ---------------------------------------------------------------- compound debris (config 4)
+# ---------------------------------------------------------------- compound debris
 _NBR = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]], np.int32)
 
 
@@ -319,7 +319,7 @@ class ClusterLibrary:
 def debris_scene(n_bodies: int, seed: int, lib: ClusterLibrary | None = None, p_geom: float = 0.3, kmax: int = 256,
                  obstacles: tuple[int, int] = (4, 16), spacing: float = 2.5, v_sigma: float = 3.0,
                  mats=(CONC, MASON, WOOD), name: str = "debris") -> Scene:
-    """Config 4 scene: n compound bodies of k ~ Geometric(p) bricks (capped at kmax) in connected random lattice
+    """A debris scene: n compound bodies of k ~ Geometric(p) bricks (capped at kmax) in connected random lattice
     clusters, uniform random orientation, N(0, v_sigma) velocities, falling onto the ground plane among 4-16
     static box obstacles (static bricks, no structure)."""
     rng = np.random.default_rng(seed)
@@ -375,9 +375,9 @@ def debris_scene(n_bodies: int, seed: int, lib: ClusterLibrary | None = None, p_
     return Scene(sxyz, smat, ssid, sinf, first, bxyz, bmat, pose, name).contiguous()
 
 
-def config4_scenes(seed: int = 3, n_scenes: int = 256, lo: int = 500, hi: int = 20000, scale: float = 1.0,
+def debris_mix(seed: int = 3, n_scenes: int = 256, lo: int = 500, hi: int = 20000, scale: float = 1.0,
                    **kw) -> list[Scene]:
-    """Config 4: n_scenes independent debris scenes, body counts log-uniform in [lo, hi] (times `scale`)."""
+    """The debris mix: n_scenes independent debris scenes, body counts log-uniform in [lo, hi] (times `scale`)."""
     rng = np.random.default_rng(seed)
     counts = np.exp(rng.uniform(math.log(lo), math.log(hi), n_scenes)) * scale
     counts = np.maximum(1, counts.astype(np.int64))
@@ -385,10 +385,10 @@ def config4_scenes(seed: int = 3, n_scenes: int = 256, lo: int = 500, hi: int = 
     return [debris_scene(int(c), seed * 1000003 + s, lib=lib, name=f"debris{s}", **kw) for s, c in enumerate(counts)]
 
 
-# ---------------------------------------------------------------- structures (config 3)
-def config3_world(seed: int = 2, n_struct: int = 37, lo: int = 1000, hi: int = 40000, cap: int = 500000,
+# ---------------------------------------------------------------- the structure lattice
+def structure_lattice(seed: int = 2, n_struct: int = 37, lo: int = 1000, hi: int = 40000, cap: int = 500000,
                   scale: float = 1.0, total: float = 378000.0) -> Scene:
-    """Config 3: n_struct column/slab frames in one 640 x 136 x 640 lattice; brick counts log-uniform in [lo, hi],
+    """The structure lattice: n_struct column/slab frames in one 640 x 136 x 640 lattice; brick counts log-uniform in [lo, hi],
     scaled together so that 37 structures hold `total` bricks (capped at `cap`), storey height 6-8 cells, footprints
     8-60 cells a side, materials 50 % concrete, 25 % masonry, 10 % steel, 10 % timber, 5 % glass.
 

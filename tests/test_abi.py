@@ -51,29 +51,35 @@ def test_no_device_fails_loudly(sf):
     if torch.cuda.is_available():
         pytest.skip("a device is present")
     from shatterforge_b200 import scenes as S
-    sc, _ = S.config1_frame()
+    sc, _ = S.frame5_structure()
     with pytest.raises(sf.SfError) as e:
         sf.World(sc)
     assert e.value.status == sf.SF_ERR_CUDA
 
 
-def test_generators_config_shapes():
+def test_generators_shapes():
     from shatterforge_b200 import scenes as S
-    sc, rm = S.config1_frame()
+    sc, rm = S.frame5_structure()
     assert sc.n_static == 3150 and rm.sum() == 12
-    c1 = S.config1_scene()
+    c1 = S.frame5_debris_scene()
     assert c1.n_bodies == 1024 and c1.n_body_bricks == 1024
     d = S.debris_scene(500, seed=7)
     assert d.n_bodies == 500 and d.body_first[-1] == d.n_body_bricks
     assert d.n_static > 0 and (d.static_sid == -1).all()
-    t, trm = S.config2_tower()
+    t, trm = S.tower16_structure()
     assert t.n_static == 47808 and trm.sum() == 48
     assert (t.static_infill == (t.static_mat == S.GLASS)).all() and t.static_infill.sum() == 16 * 534
     t2 = t.without_static(trm)
     assert S.grounded_mask(t2.static_xyz, t2.static_mat, t2.static_sid, t2.static_infill).all()
-    c2 = S.config2_scene(n_bodies=600)
+    c2 = S.tower16_debris_scene(n_bodies=600)
     ks = np.diff(c2.body_first.astype(np.int64))
     assert c2.n_bodies == 600 and ks.min() >= 1 and ks.max() <= 512 and ks.max() >= 128
+    # the structure lattice: 37 frames, about 378,000 bricks after ungrounded pieces are pruned (none should be),
+    # glass only as window panels standing on slabs
+    lat = S.structure_lattice(seed=2)
+    assert len(lat.structure_ids()) == 37 and 370000 <= lat.n_static <= 390000
+    glass = lat.static_mat == S.GLASS
+    assert 0.03 < glass.mean() < 0.06 and (lat.static_infill[glass] == 1).all()
 
 
 def test_xorshift_matches_reference_stream():

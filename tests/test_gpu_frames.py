@@ -56,7 +56,7 @@ def run_frames(sf, oracle, sc, frames, warm_at=None, active=None):
 def test_frames_many_structures(sf, oracle):
     """Eight structures of 88-1,364 bricks, warmed at different frames: the warm-up budget carries over from frame
     to frame, the structural loop runs 6 sweeps (then more) for unsettled structures and 1 or 0 once converged."""
-    sc = S.config3_world(scale=0.05, n_struct=8)
+    sc = S.structure_lattice(scale=0.05, n_struct=8)
     ids = sc.structure_ids()
     warm_at = {s: 1 + 3 * k for k, s in enumerate(ids)}
     sw, ws, live = run_frames(sf, oracle, sc, 60, warm_at=warm_at)
@@ -66,8 +66,8 @@ def test_frames_many_structures(sf, oracle):
 def test_frames_frame_and_tower(sf, oracle):
     """The 5-storey frame (3,150 bricks: budget-limited warm-up of 38 sweeps a frame) and the 16-storey tower
     (47,760 bricks: over 15,000, one structural sweep a frame until converged) in one lattice."""
-    frame, _ = S.config1_frame()
-    tower, rm = S.config2_tower()
+    frame, _ = S.frame5_structure()
+    tower, rm = S.tower16_structure()
     tower = tower.without_static(rm)
     # the tower beside the frame: shift it 60 cells along x and give it structure id 1
     xyz = np.concatenate([frame.static_xyz, tower.static_xyz + np.array([60, 0, 0], np.int32)])

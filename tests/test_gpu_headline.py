@@ -1,13 +1,13 @@
 """Parity at the benchmark's own sizes, through the C ABI.
 
-The benchmark steps the whole 256-scene debris mix (config 4) in one world and solves all 37 structures of the
-structure lattice (config 3) at once; these tests check those runs against the CPU oracle:
+The benchmark steps the whole 256-scene debris mix in one world and solves all 37 structures of the
+structure lattice at once; these tests check those runs against the CPU oracle:
 
   * the 256-scene mix stepped to its contact peak in one batched world; then one more batched step, compared scene by
     scene (the smallest, the median and the largest, about 20,000 bodies) with the oracle stepping that scene alone
     from the GPU's state: contact lists, manifolds with their colours, islands and body state bit for bit;
   * 60 steps of the median scene from rest, bit for bit against the colour-order oracle;
-  * config 1 (the 5-storey frame and 1,024 loose bricks) for 200 steps, past the debris landing on the ground and
+  * the 5-storey frame with 1,024 loose bricks for 200 steps, past the debris landing on the ground and
     on the frame's roof, bit for bit;
   * the full structure lattice (about 375,000 bricks) solved in one call, each structure against the FP64
     red-black oracle at the same sweep cap: potentials, sweep counts and residuals bit for bit;
@@ -28,7 +28,7 @@ STATIC = 0xFFFFFFFF
 @pytest.fixture(scope="module")
 def mix():
     """The benchmark's mix: 256 scenes, body counts log-uniform in 500-20,000 (seed 3, as bench.py builds it)."""
-    return S.config4_scenes()
+    return S.debris_mix()
 
 
 def _by_size(scenes):
@@ -107,10 +107,10 @@ def test_median_scene_sixty_steps_from_rest(sf, oracle, mix):
     assert len(ids) > 1000
 
 
-def test_config1_past_landing(sf, oracle):
-    """Config 1 for 200 steps: the loose bricks start 2-12 m up beside the frame and have all landed (on the ground,
+def test_frame_with_debris_past_landing(sf, oracle):
+    """The 5-storey frame with its debris for 200 steps: the loose bricks start 2-12 m up beside the frame and have all landed (on the ground,
     on each other) well before the end; the reference's pinch removal is on, as in the reference."""
-    sc = S.config1_scene()
+    sc = S.frame5_debris_scene()
     w = sf.World(sc, iterations=8)
     ow = oracle.OracleWorld(sc)
     for _ in range(200):
@@ -130,7 +130,7 @@ def test_full_structure_lattice_against_fp64(sf, oracle):
     """All 37 structures (about 375,000 bricks) in one solve (the benchmark's call: one thread-block cluster per
     structure), stopped at 3,000 sweeps or the residual 1e-6; each structure equals the FP64 red-black oracle run
     alone to the same limits, bit for bit."""
-    sc = S.config3_world(seed=2)
+    sc = S.structure_lattice(seed=2)
     assert sc.n_static >= 370000 and len(sc.structure_ids()) == 37
     w = sf.World(sc)
     w.structure_solve(-1, omega=1.7, tol=1e-6, max_sweeps=3000)

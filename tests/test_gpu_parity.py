@@ -36,7 +36,7 @@ def test_body_setup_bit_exact(sf, oracle):
 
 
 def test_bonds_bit_exact(sf, oracle):
-    w3 = S.config3_world(scale=0.05, n_struct=6)
+    w3 = S.structure_lattice(scale=0.05, n_struct=6)
     w = sf.World(w3)
     ow = oracle.OracleWorld(w3)
     b, nb, _ = w.bonds()
@@ -48,7 +48,7 @@ def test_bonds_bit_exact(sf, oracle):
 # ---------------------------------------------------------------- load path
 @pytest.mark.parametrize("removed", [False, True])
 def test_sor_matches_fp64_redblack_at_same_residual(sf, oracle, removed):
-    sc, rm = S.config1_frame()
+    sc, rm = S.frame5_structure()
     if removed:
         sc = sc.without_static(rm)
     w = sf.World(sc)
@@ -62,7 +62,7 @@ def test_sor_matches_fp64_redblack_at_same_residual(sf, oracle, removed):
 
 
 def test_sor_within_tolerance_of_fp64_fixed_point(sf, oracle):
-    sc, rm = S.config1_frame()
+    sc, rm = S.frame5_structure()
     sc = sc.without_static(rm)
     w = sf.World(sc)
     w.structure_solve(0, omega=1.7, tol=1e-9, max_sweeps=100000)
@@ -74,7 +74,7 @@ def test_sor_within_tolerance_of_fp64_fixed_point(sf, oracle):
 
 
 def test_sor_many_structures_one_launch(sf, oracle):
-    sc = S.config3_world(scale=0.05, n_struct=8)
+    sc = S.structure_lattice(scale=0.05, n_struct=8)
     w = sf.World(sc)
     w.structure_solve(-1, omega=1.7, tol=1e-6, max_sweeps=50000)
     sw, rs = w.solve_detail()
@@ -99,7 +99,7 @@ def _joint_table(ids, vals, ns):
 
 @pytest.mark.parametrize("case", ["intact", "removed", "weak"])
 def test_joint_decisions_bit_exact(sf, oracle, case):
-    sc, rm = S.config1_frame()
+    sc, rm = S.frame5_structure()
     if case != "intact":
         sc = sc.without_static(rm)
     if case == "weak":
@@ -128,7 +128,7 @@ def test_joint_decisions_bit_exact(sf, oracle, case):
 def test_resting_loads_bit_exact(sf, oracle):
     """Debris falls on the 5-storey frame's roof; the loads it puts on the structure match the oracle's, computed
     from the same state (bodies and brick positions)."""
-    frame, _ = S.config1_frame()
+    frame, _ = S.frame5_structure()
     bf, bxyz, bmat, pose = S.loose_debris(300, seed=17, box_lo=(-5.0, 19.0, -5.0), box_hi=(5.0, 23.0, 5.0))
     frame.body_first, frame.body_brick_xyz, frame.body_brick_mat, frame.body_pose = bf, bxyz, bmat, pose
     sc = frame.contiguous()
@@ -247,8 +247,8 @@ def test_scenes_batched_equal_alone(sf):
         np.testing.assert_array_equal(s, bs)
 
 
-def test_config1_scene_runs(sf, oracle):
-    sc = S.config1_scene()
+def test_frame5_debris_scene_runs(sf, oracle):
+    sc = S.frame5_debris_scene()
     w = sf.World(sc, iterations=8)
     ow = oracle.OracleWorld(sc)
     for _ in range(20):
@@ -314,11 +314,11 @@ def test_box_sat_bit_exact(sf, oracle):
     assert hits > n // 4
 
 
-# ---------------------------------------------------------------- config 2: 16-storey tower with glass infill
-def test_config2_tower_sor_bit_exact(sf, oracle):
+# ---------------------------------------------------------------- the 16-storey tower with glass infill
+def test_tower16_structure_sor_bit_exact(sf, oracle):
     """The tower with 8 ground columns removed (47,760 bricks, infill panels that bond only downwards): the same
     red-black FP64 sweeps on both sides, stopped at the same sweep count."""
-    sc, rm = S.config2_tower()
+    sc, rm = S.tower16_structure()
     sc = sc.without_static(rm)
     w = sf.World(sc)
     rep = w.structure_solve(0, omega=1.7, tol=1e-9, max_sweeps=3000)
@@ -330,8 +330,8 @@ def test_config2_tower_sor_bit_exact(sf, oracle):
     np.testing.assert_array_equal(w.phi64(), ow.phi64())
 
 
-def test_config2_tower_joints_bit_exact(sf, oracle):
-    sc, rm = S.config2_tower()
+def test_tower16_structure_joints_bit_exact(sf, oracle):
+    sc, rm = S.tower16_structure()
     sc = sc.without_static(rm)
     w = sf.World(sc)
     rep = w.structure_solve(0, omega=1.7, tol=1e-6, max_sweeps=200000)
@@ -350,9 +350,9 @@ def test_config2_tower_joints_bit_exact(sf, oracle):
     assert rep.max_ratio == mr
 
 
-def test_config2_compound_bodies_bit_exact(sf, oracle):
+def test_tower_compound_bodies_bit_exact(sf, oracle):
     """Compound fragments of 1-512 bricks land on the tower's roof and around it: 100 steps, bit-exact."""
-    sc = S.config2_scene(n_bodies=1500, lift=54.0)
+    sc = S.tower16_debris_scene(n_bodies=1500, lift=54.0)
     w = sf.World(sc, iterations=8)
     ow = oracle.OracleWorld(sc)
     for _ in range(100):
@@ -481,8 +481,8 @@ def test_sor_cluster_path_equals_grid_path(sf):
     """One thread-block cluster per structure (cells in shared memory) gives the grid-wide kernel's potentials, sweep
     counts and residuals bit for bit: on many small structures at once, on the 16-storey tower, and on the 37-structure
     lattice of 275,618 bricks, whose large and small structures run as two launches side by side."""
-    cases = ((S.config3_world(scale=0.05, n_struct=8), 1e-7, 40000), (S.config2_tower()[0], 1e-7, 40000),
-             (S.config3_world(seed=2), 1e-6, 3000))
+    cases = ((S.structure_lattice(scale=0.05, n_struct=8), 1e-7, 40000), (S.tower16_structure()[0], 1e-7, 40000),
+             (S.structure_lattice(seed=2), 1e-6, 3000))
     for sc, tol, cap in cases:
         a = sf.World(sc, sor_cluster=1)
         b = sf.World(sc, sor_cluster=0)
@@ -507,7 +507,7 @@ def test_joint_decisions_against_reference_f32_solve(sf, oracle, case):
     own solve: lexicographic f32 sweeps to the same residual (src/lib.rs:1005-1040), run in the oracle. A decision
     may differ only where the two ratios straddle the threshold 1 and both lie within NEAR_THRESHOLD_BAND of it;
     those joints are listed (printed) and counted."""
-    sc, rm = S.config1_frame()
+    sc, rm = S.frame5_structure()
     sc = sc.without_static(rm)
     if case == "weak":
         sc.static_mat[(sc.static_xyz[:, 1] < 6)] = S.WOOD

@@ -69,8 +69,8 @@ def test_ranks_step_independent_scene_mixes():
     sys.path.insert(0, str(ROOT))
     import bench
     from shatterforge_b200 import scenes as S
-    a = S.config4_scenes(seed=bench.rank_seed(0), n_scenes=3, scale=0.02)
-    b = S.config4_scenes(seed=bench.rank_seed(1), n_scenes=3, scale=0.02)
+    a = S.debris_mix(seed=bench.rank_seed(0), n_scenes=3, scale=0.02)
+    b = S.debris_mix(seed=bench.rank_seed(1), n_scenes=3, scale=0.02)
     assert bench.rank_seed(0) != bench.rank_seed(1)
     assert not np.array_equal(a[0].body_pose[:10], b[0].body_pose[:10])
 

@@ -48,7 +48,7 @@ def test_column_joint_ratios_closed_form(oracle):
 
 def test_intact_frame_holds(oracle):
     """tests/stab.mjs: an intact structure loses nothing under its own weight."""
-    sc, _ = S.config1_frame()
+    sc, _ = S.frame5_structure()
     w = oracle.OracleWorld(sc)
     w.sor(0, omega=1.7, tol=1e-9, max_sweeps=100000, mode=oracle.MODE_REDBLACK_F64)
     ids, vals, mr = w.stress(0, live=True)
@@ -59,7 +59,7 @@ def test_intact_frame_holds(oracle):
 
 def test_frame_orders_agree(oracle):
     """Lexicographic (the reference's order) and red-black sweeps converge to the same FP64 fixed point."""
-    sc, rm = S.config1_frame()
+    sc, rm = S.frame5_structure()
     sc = sc.without_static(rm)
     a = oracle.OracleWorld(sc)
     a.sor(0, 1.7, 1e-13, 300000, mode=oracle.MODE_LEX_F64)
@@ -72,7 +72,7 @@ def test_frame_orders_agree(oracle):
 def test_reference_f32_sweeps_reach_residual(oracle):
     """The reference's own f32 lexicographic sweeps (sor_struct) reach its residual measure and stay near the
     FP64 fixed point; the red-black f32 variant behaves the same."""
-    sc, _ = S.config1_frame()
+    sc, _ = S.frame5_structure()
     ex = oracle.OracleWorld(sc)
     ex.sor(0, 1.7, 1e-13, 300000, mode=oracle.MODE_LEX_F64)
     exact = ex.phi64()

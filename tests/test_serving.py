@@ -81,7 +81,7 @@ def _arrivals(rng, n_scenes, n_struct, n, rate):
 def test_server_results_equal_alone(sf, sv, batching):
     rng = np.random.default_rng(9)
     scs = [scene(80 + k, int(rng.integers(60, 260))) for k in range(6)]
-    structs = S.config3_world(scale=0.03, n_struct=5)
+    structs = S.structure_lattice(scale=0.03, n_struct=5)
     big = cover(sv, scs, 1.05)
     # three slots for six scenes: scenes are evicted and restored while requests keep coming
     srv = sv.Server(slots=[big] * 3, structures=structs, batching=batching, sweeps_per_tick=64, iterations=8)
