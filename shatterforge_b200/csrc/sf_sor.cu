@@ -64,10 +64,13 @@ struct SorState {
     Tuner tune;   // blocks per SM of the red-black kernel, keyed on log2(chunks of the solve)
     // The solve's launch sequence captured in CUDA graphs, one per launch shape (the chunk list and the active
     // flags live in device buffers the graph reads, so a graph serves every solve of its shape).
-    struct Graph { uint32_t n_work, grid, mode, n_big, grid_small; cudaGraphExec_t exec; };
+    // a graph's launch shape: the chunk count or structure count, the grid of the red-black kernel, the path, and
+    // per cluster launch class its cluster count and cells a block (the structure order lives in device memory)
+    struct Graph { uint32_t n_work, grid, mode; uint32_t shape[8]; cudaGraphExec_t exec; };
     // the cluster path: one thread-block cluster per structure, the structure's cells in the cluster's shared memory
     bool cl_ready = false;
-    std::vector<uint32_t> h_cl_n, h_cl_per;
+    bool wide_ok = false;           // the device can run 16-block clusters of the wide structures
+    std::vector<uint32_t> h_cl_n, h_cl_per, h_cl_ncl;   // per structure: cells, cells a block, blocks of its cluster
     // per structure: its height in cells, and the sweeps its last solve took (0 = none yet); the launch split puts
     // the structures expected to take longest on the larger blocks
     std::vector<uint32_t> h_st_height, h_last_sweeps;
@@ -76,8 +79,8 @@ struct SorState {
     uint64_t cluster_solves = 0;
     // the small structures' clusters run beside the large ones', on a second stream forked from and joined to the
     // world's stream (inside the captured graph too)
-    cudaStream_t aux = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
     DBuf<SorParams> prm;
     DBuf<uint32_t> cap;             // per structure: its own sweep limit when SorParams::use_cap is set
     // the reference's per-frame schedule (src/lib.rs:1061-1079, 1268-1281): per structure its pending warm-up
@@ -336,7 +339,9 @@ __global__ void __launch_bounds__(SOR_BLOCK) k_sor_redblack(SorArgs A) {
 // halves, and the one that ends a sweep also publishes each block's residual maxima (two barriers per sweep). The
 // largest structures' clusters are listed first. Each update is the grid kernel's arithmetic on the same values in the same order, and the residual and
 // stopping rule are the same, so the potentials and sweep counts are identical to the grid kernel's.
-constexpr int SOR_CL = 8;
+constexpr int SOR_CL = 8;                        // blocks of a structure's cluster, or SOR_CL_WIDE for large ones
+constexpr int SOR_CL_WIDE = 16;                  // a non-portable cluster size: structures of SOR_CL_WIDE_MIN bricks
+constexpr uint32_t SOR_CL_WIDE_MIN = 20000;
 constexpr int SOR_CL_MAX_THREADS = 1024;         // threads per block: 256, 512 or 1024, picked per launch
 constexpr uint32_t SOR_CL_CAP = 8192;            // cells per block: 28 B each (phi 8, rhs 4, code 4, 6 neighbours 12)
 constexpr uint32_t SOR_CL_BYTES_PER_CELL = 28;
@@ -349,7 +354,8 @@ struct SorClusterArgs {
     const uint32_t *list;                        // the structure of each cluster
     const uint32_t *off, *n, *per, *even;        // per structure; even: per (structure, block)
     const uint32_t *cpos;                        // per listed cell: its place in the chunk layout
-    const uint16_t *nbr;                         // per listed cell: 6 neighbours as block rank << 13 | index in block
+    const uint16_t *nbr;                         // per listed cell: 6 neighbours as block rank << sh | index in block,
+                                                 // sh = 13 for 8-block clusters, 12 for 16-block ones
     double *cphi;
     const float *crhs;
     const uint32_t *ccode;
@@ -377,7 +383,7 @@ __global__ void __launch_bounds__(SOR_CL_MAX_THREADS) k_sor_cluster(SorClusterAr
     uint32_t *code = (uint32_t *)(rhs + P);
     uint16_t *nbr = (uint16_t *)(code + P);
     // this block's maxima of sweep s in slot s & 1, published before the barrier that ends the sweep; after it,
-    // thread 0 of every block reads all SOR_CL blocks' slots and takes the stop decision (the same in every block)
+    // warp 0 of every block reads all the cluster's blocks' slots and takes the stop decision (the same everywhere)
     __shared__ unsigned long long blk_d[2], blk_p[2];
     __shared__ unsigned long long wd[SOR_CL_MAX_THREADS / 32], wp[SOR_CL_MAX_THREADS / 32];
     __shared__ int s_stop;
@@ -392,10 +398,12 @@ __global__ void __launch_bounds__(SOR_CL_MAX_THREADS) k_sor_cluster(SorClusterAr
     }
     const unsigned long long one = (unsigned long long)__double_as_longlong(1.0);
     const uint32_t rank = cl.block_rank(), tid = threadIdx.x;
-    const uint32_t q = A.list[blockIdx.x / SOR_CL];
+    const uint32_t ncl = cl.num_blocks();        // 8 or 16: the structure's tables were cut for this many blocks
+    const uint32_t sh = ncl == (uint32_t)SOR_CL_WIDE ? 12u : 13u, lmask = (1u << sh) - 1u;
+    const uint32_t q = A.list[blockIdx.x / ncl];
     const uint32_t off = A.off[q], n = A.n[q], per = A.per[q];
     const uint32_t b0 = min(n, rank * per), b1 = min(n, b0 + per), my = b1 - b0;
-    const uint32_t ev = A.even[q * SOR_CL + rank];
+    const uint32_t ev = A.even[q * SOR_CL_WIDE + rank];
     for (uint32_t i = tid; i < my; i += blockDim.x) {
         const uint32_t g = off + b0 + i;
         const uint32_t at = A.cpos[g];
@@ -425,7 +433,7 @@ __global__ void __launch_bounds__(SOR_CL_MAX_THREADS) k_sor_cluster(SorClusterAr
                 if (lm == 0) continue;
                 const uint32_t g = nbr[i * 6 + d];
                 if (g == NO_CELL) { atomicOr(A.err, (unsigned)ERR_SOR_NONFINITE); continue; }
-                const uint32_t r = g >> 13, l = g & 8191u;
+                const uint32_t r = g >> sh, l = g & lmask;
                 const double pj = r == rank ? phi[l] : cl.map_shared_rank(phi, r)[l];
                 const double k = kt[2 * lm + ((d >> 1) == 1 ? 1 : 0)];
                 sk += k;
@@ -488,12 +496,12 @@ __global__ void __launch_bounds__(SOR_CL_MAX_THREADS) k_sor_cluster(SorClusterAr
         // the cluster's maxima: lane b of warp 0 reads block b's slot (the eight remote reads in flight together)
         if (tid < 32) {
             unsigned long long dm = 0ull, pm = one;
-            if (tid < (uint32_t)SOR_CL) {
+            if (tid < ncl) {
                 dm = cl.map_shared_rank(blk_d, tid)[slot];
                 pm = cl.map_shared_rank(blk_p, tid)[slot];
             }
 #pragma unroll
-            for (int o = 4; o > 0; o >>= 1) {
+            for (int o = 8; o > 0; o >>= 1) {
                 dm = max(dm, __shfl_xor_sync(0xffffffffu, dm, o));
                 pm = max(pm, __shfl_xor_sync(0xffffffffu, pm, o));
             }
@@ -884,8 +892,10 @@ void sor_destroy(sf_world *w) {
     if (w->sor) {
         for (auto &g : w->sor->graphs) cudaGraphExecDestroy(g.exec);
         if (w->sor->fork) cudaEventDestroy(w->sor->fork);
-        if (w->sor->join) cudaEventDestroy(w->sor->join);
-        if (w->sor->aux) cudaStreamDestroy(w->sor->aux);
+        for (int k = 0; k < 3; k++) {
+            if (w->sor->join[k]) cudaEventDestroy(w->sor->join[k]);
+            if (w->sor->aux[k]) cudaStreamDestroy(w->sor->aux[k]);
+        }
     }
     delete w->sor;
     w->sor = nullptr;
@@ -941,6 +951,27 @@ static sf_status sor_select_set(sf_world *w, const int32_t *ids, uint32_t n, std
 // with more than 65,535 bricks takes the grid kernel.
 static sf_status sor_cluster_tables(sf_world *w) {
     SorState *st = w->sor;
+    SF_CUDA(cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(SOR_CL_CAP * SOR_CL_BYTES_PER_CELL)));
+    SF_CUDA(cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared));
+    SF_CUDA(cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    {
+        // 16-block clusters only where the device can hold one (1,024-thread blocks with a wide structure's shared
+        // memory); otherwise every structure keeps 8-block tables
+        cudaLaunchConfig_t c = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = SOR_CL_WIDE; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+        c.gridDim = dim3(SOR_CL_WIDE);
+        c.blockDim = dim3(SOR_CL_MAX_THREADS);
+        c.dynamicSmemBytes = (size_t)4096 * SOR_CL_BYTES_PER_CELL;
+        c.attrs = at;
+        c.numAttrs = 1;
+        int nc = 0;
+        if (cudaOccupancyMaxActiveClusters(&nc, k_sor_cluster, &c) != cudaSuccess) { nc = 0; cudaGetLastError(); }
+        st->wide_ok = nc > 0;
+    }
     const uint32_t nst = w->n_struct, ns = w->ns;
     std::vector<uint32_t> h_ctab((size_t)w->n_scenes * NCT), h_cpool((size_t)std::max<uint32_t>(w->n_chunks, 1) * 512);
     SF_CUDA(cudaStreamSynchronize(w->stream));
@@ -961,10 +992,11 @@ static sf_status sor_cluster_tables(sf_world *w) {
         const uint32_t t = h_ctab[(size_t)sc * NCT + chunk_slot(x, y, z)];
         return t ? ((t - 1) << 9) | cell_in_chunk(x, y, z) : NONE;
     };
-    std::vector<uint32_t> idx(ns, NONE), cpos, even(std::max<size_t>((size_t)nst * SOR_CL, 1), 0);
+    std::vector<uint32_t> idx(ns, NONE), cpos, even(std::max<size_t>((size_t)nst * SOR_CL_WIDE, 1), 0);
     std::vector<uint16_t> nbr;
     st->h_cl_n.assign(nst, 0);
     st->h_cl_per.assign(nst, 0);
+    st->h_cl_ncl.assign(nst, SOR_CL);
     st->h_st_height.assign(nst, 0);
     st->h_last_sweeps.assign(nst, 0);
     std::vector<uint32_t> off(std::max<uint32_t>(nst, 1), 0), cnt(std::max<uint32_t>(nst, 1), 0), per(std::max<uint32_t>(nst, 1), 0);
@@ -975,15 +1007,18 @@ static sf_status sor_cluster_tables(sf_world *w) {
         std::vector<uint32_t> &b = bricks[q];
         if (b.empty() || b.size() >= NO_CELL) continue;
         std::sort(b.begin(), b.end(), [&](uint32_t u, uint32_t v) { return key(u) < key(v); });
-        const uint32_t n = (uint32_t)b.size(), pr = (n + SOR_CL - 1) / SOR_CL;
-        for (uint32_t r = 0; r < SOR_CL; r++) {
+        const uint32_t n = (uint32_t)b.size();
+        const uint32_t ncl = (st->wide_ok && n >= SOR_CL_WIDE_MIN) ? (uint32_t)SOR_CL_WIDE : (uint32_t)SOR_CL;
+        const uint32_t pr = (n + ncl - 1) / ncl, sh = ncl == (uint32_t)SOR_CL_WIDE ? 12u : 13u;
+        st->h_cl_ncl[q] = ncl;
+        for (uint32_t r = 0; r < ncl; r++) {
             auto lo = b.begin() + std::min(n, r * pr), hi = b.begin() + std::min(n, (r + 1) * pr);
             auto mid = std::stable_partition(lo, hi, [&](uint32_t i) {
                 int x, y, z;
                 unpack_cell(w->h_s_cell[i], x, y, z);
                 return ((x + y + z) & 1) == 0;
             });
-            even[(size_t)q * SOR_CL + r] = (uint32_t)(mid - lo);
+            even[(size_t)q * SOR_CL_WIDE + r] = (uint32_t)(mid - lo);
         }
         off[q] = (uint32_t)cpos.size();
         cnt[q] = n;
@@ -1001,7 +1036,9 @@ static sf_status sor_cluster_tables(sf_world *w) {
                     const uint32_t j1 = h_cpool[(size_t)(c >> 9) * 512 + (c & 511)];
                     if (j1 && w->h_sid[j1 - 1] == (int32_t)q) {
                         const uint32_t t = idx[j1 - 1];
-                        g = (uint16_t)(((t / pr) << 13) | (t % pr));   // pr <= 8192: the index fits 13 bits
+                        // pr <= 8192 (8 blocks) or 4096 (16): the index fits sh bits, and the last block holds
+                        // fewer than pr cells, so no neighbour packs to NO_CELL
+                        g = (uint16_t)(((t / pr) << sh) | (t % pr));
                     }
                 }
                 nbr.push_back(g);
@@ -1033,10 +1070,6 @@ static sf_status sor_cluster_tables(sf_world *w) {
     SF_CUDA(st->cl_list.alloc(std::max<uint32_t>(nst, 1)));
     SF_CUDA(st->cl_nbr.alloc(std::max<size_t>(nbr.size(), 1)));
     if (!nbr.empty()) SF_CUDA(cudaMemcpyAsync(st->cl_nbr.p, nbr.data(), nbr.size() * 2, cudaMemcpyHostToDevice, s));
-    SF_CUDA(cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(SOR_CL_CAP * SOR_CL_BYTES_PER_CELL)));
-    SF_CUDA(cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared));
     SF_CUDA(cudaStreamSynchronize(s));
     st->cl_ready = true;
     return SF_OK;
@@ -1067,41 +1100,52 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     }
     SF_CUDA(cudaMemcpyAsync(st->active0.p, act.data(), nst * 4, cudaMemcpyHostToDevice, s));
     std::vector<uint32_t> cl_order;
-    // two launches when the structures are of both sizes: the large ones' clusters with SOR_CL_MAX_THREADS threads a
-    // block (one block an SM), the small ones' with 256 threads and their own, smaller shared memory (several blocks
-    // an SM), side by side, so that all clusters are resident at once
-    uint32_t n_big = 0, per_big = 0, per_small = 0;
+    // Launch classes of the cluster path, run side by side: W, 16-block clusters of 1,024-thread blocks (the
+    // structures of SOR_CL_WIDE_MIN bricks or more, whose tables were cut for 16 blocks); L, M, S, 8-block clusters
+    // of 1,024, 512 and 256 threads. A structure's solve takes its sweeps (known from its last solve; a first solve
+    // guesses them from its height) times its time per sweep, modelled as a fixed 3 us plus 2.1 us per cell a thread
+    // (measured: the kernel is bound by instruction issue). The 8-block structures start in S and the slowest one is
+    // moved up a class while the SMs it needs are free (a W block takes an SM, L one SM, M half, S a quarter, by
+    // registers); within each class the slowest clusters are listed first, so they start first.
+    const int NCLS = 4;
+    static const unsigned cls_threads[NCLS] = {1024u, 1024u, 512u, 256u};
+    static const double cls_sm[NCLS] = {16.0, 8.0, 4.0, 2.0};
+    std::vector<uint32_t> by_cls[NCLS];
+    uint32_t cls_per[NCLS] = {0, 0, 0, 0};
     if (use_cl) {
-        // Critical path first. A structure's solve takes its sweeps times its time per sweep, and the sweeps are
-        // known from its last solve (a first solve guesses them from its height). The large blocks (1,024 threads)
-        // take every structure of more than SOR_CL_SPLIT cells a block, and also each small one that would be
-        // among the slowest on 256 threads; within each launch the slowest clusters are listed first, so they
-        // start first when not all are resident at once.
         auto expect = [&](uint32_t q) -> double {
             return st->h_last_sweeps[q] ? (double)st->h_last_sweeps[q] : 60.0 * std::max<uint32_t>(st->h_st_height[q], 1);
         };
-        auto cost_small = [&](uint32_t q) { return expect(q) * (1.0 + std::ceil(st->h_cl_per[q] / 512.0)); };
-        auto cost_large = [&](uint32_t q) { return expect(q) * (1.0 + std::ceil(st->h_cl_per[q] / 2048.0)); };
-        double worst = 0.0;
-        for (uint32_t q : req) worst = std::max(worst, st->h_cl_per[q] > SOR_CL_SPLIT ? cost_large(q) : cost_small(q));
-        std::vector<uint32_t> big, small;
+        auto t_of = [&](uint32_t q, int c) { return expect(q) * (3.0 + 2.1 * (double)st->h_cl_per[q] / cls_threads[c]); };
+        std::vector<int> cls(nst, 3);
+        double used = 0.0;
         for (uint32_t q : req) {
-            const bool large = st->h_cl_per[q] > SOR_CL_SPLIT || cost_small(q) >= 0.5 * worst;
-            (large ? big : small).push_back(q);
+            cls[q] = st->h_cl_ncl[q] == (uint32_t)SOR_CL_WIDE ? 0 : 3;
+            used += cls_sm[cls[q]];
         }
-        std::stable_sort(big.begin(), big.end(), [&](uint32_t a, uint32_t b) { return cost_large(a) > cost_large(b); });
-        std::stable_sort(small.begin(), small.end(), [&](uint32_t a, uint32_t b) { return cost_small(a) > cost_small(b); });
-        cl_order = big;
-        cl_order.insert(cl_order.end(), small.begin(), small.end());
-        n_big = (uint32_t)big.size();
-        for (uint32_t q : big) per_big = std::max(per_big, st->h_cl_per[q]);
-        for (uint32_t q : small) per_small = std::max(per_small, st->h_cl_per[q]);
-        if (n_big == 0 || n_big == cl_order.size()) { n_big = 0; per_small = 0; }   // one launch
+        for (;;) {
+            uint32_t worst = NONE;
+            for (uint32_t q : req) if (worst == NONE || t_of(q, cls[q]) > t_of(worst, cls[worst])) worst = q;
+            if (worst == NONE || cls[worst] <= 1) break;   // the slowest is wide or already on 1,024 threads
+            const int up = cls[worst] - 1;
+            if (used - cls_sm[cls[worst]] + cls_sm[up] > (double)w->sms) break;
+            used += cls_sm[up] - cls_sm[cls[worst]];
+            cls[worst] = up;
+        }
+        for (uint32_t q : req) by_cls[cls[q]].push_back(q);
+        cl_order.clear();
+        for (int c = 0; c < NCLS; c++) {
+            std::stable_sort(by_cls[c].begin(), by_cls[c].end(), [&](uint32_t a, uint32_t b) { return t_of(a, c) > t_of(b, c); });
+            for (uint32_t q : by_cls[c]) cls_per[c] = std::max(cls_per[c], st->h_cl_per[q]);
+            cl_order.insert(cl_order.end(), by_cls[c].begin(), by_cls[c].end());
+        }
         SF_CUDA(cudaMemcpyAsync(st->cl_list.p, cl_order.data(), cl_order.size() * 4, cudaMemcpyHostToDevice, s));
-        if (n_big && !st->aux) {
-            SF_CUDA(cudaStreamCreateWithFlags(&st->aux, cudaStreamNonBlocking));
+        if (!st->fork) {
             SF_CUDA(cudaEventCreateWithFlags(&st->fork, cudaEventDisableTiming));
-            SF_CUDA(cudaEventCreateWithFlags(&st->join, cudaEventDisableTiming));
+            for (int k = 0; k < 3; k++) {
+                SF_CUDA(cudaStreamCreateWithFlags(&st->aux[k], cudaStreamNonBlocking));
+                SF_CUDA(cudaEventCreateWithFlags(&st->join[k], cudaEventDisableTiming));
+            }
         }
     }
     else SF_CUDA(cudaMemcpyAsync(st->work.p, chunks.data(), chunks.size() * 4, cudaMemcpyHostToDevice, s));
@@ -1122,33 +1166,36 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     const int tb = Tuner::bucket(chunks.size());
     const unsigned per_sm = use_cl ? 1u : (unsigned)st->tune.choose(tb, tci);
     if (use_cl) tci = -1;
-    unsigned grid = use_cl ? (n_big ? per_big : per_max) : (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * per_sm);
+    unsigned grid = use_cl ? 0u : (unsigned)std::min<size_t>(chunks.size(), (size_t)w->sms * per_sm);
     const uint32_t n_launch = use_cl ? (uint32_t)req.size() : A.n_work;
     void *args[] = {&A};
-    SorClusterArgs CA;
-    CA.cap = st->cap.p;
-    CA.list = st->cl_list.p; CA.off = st->cl_off.p; CA.n = st->cl_n.p; CA.per = st->cl_per.p; CA.even = st->cl_even.p;
-    CA.cpos = st->cl_cpos.p; CA.nbr = st->cl_nbr.p; CA.cphi = st->cphi.p; CA.crhs = st->crhs.p; CA.ccode = st->ccode.p;
-    CA.csid = st->csid.p; CA.per_max = n_big ? per_big : per_max; CA.prm = st->prm.p; CA.sweeps = st->sweeps.p;
-    CA.resid = st->resid.p; CA.err = w->err.p;
-    SorClusterArgs CS = CA;   // the small structures' launch: the list after the large ones
-    CS.list = st->cl_list.p + n_big;
-    CS.per_max = per_small;
-    cudaLaunchAttribute cattr[1];
-    cattr[0].id = cudaLaunchAttributeClusterDimension;
-    cattr[0].val.clusterDim.x = SOR_CL; cattr[0].val.clusterDim.y = 1; cattr[0].val.clusterDim.z = 1;
-    cudaLaunchConfig_t ccfg = {}, scfg = {};
-    ccfg.gridDim = dim3((unsigned)((n_big ? n_big : req.size()) * SOR_CL));
-    ccfg.blockDim = dim3(n_big ? (unsigned)SOR_CL_MAX_THREADS : sor_cl_threads(CA.per_max));
-    ccfg.dynamicSmemBytes = (size_t)CA.per_max * SOR_CL_BYTES_PER_CELL;
-    ccfg.stream = s;
-    ccfg.attrs = cattr;
-    ccfg.numAttrs = 1;
-    scfg = ccfg;
-    scfg.gridDim = dim3((unsigned)((req.size() - n_big) * SOR_CL));
-    scfg.blockDim = dim3(256);
-    scfg.dynamicSmemBytes = (size_t)per_small * SOR_CL_BYTES_PER_CELL;
-    scfg.stream = st->aux;
+    SorClusterArgs CC[NCLS];
+    cudaLaunchConfig_t cfg[NCLS] = {};
+    cudaLaunchAttribute cattr[NCLS][1];
+    uint32_t shape[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    {
+        uint32_t first = 0;
+        for (int c = 0; c < NCLS; c++) {
+            SorClusterArgs &X = CC[c];
+            X.cap = st->cap.p;
+            X.list = st->cl_list.p + first; X.off = st->cl_off.p; X.n = st->cl_n.p; X.per = st->cl_per.p;
+            X.even = st->cl_even.p; X.cpos = st->cl_cpos.p; X.nbr = st->cl_nbr.p; X.cphi = st->cphi.p; X.crhs = st->crhs.p;
+            X.ccode = st->ccode.p; X.csid = st->csid.p; X.per_max = cls_per[c]; X.prm = st->prm.p;
+            X.sweeps = st->sweeps.p; X.resid = st->resid.p; X.err = w->err.p;
+            const unsigned ncl = c == 0 ? (unsigned)SOR_CL_WIDE : (unsigned)SOR_CL;
+            cattr[c][0].id = cudaLaunchAttributeClusterDimension;
+            cattr[c][0].val.clusterDim.x = ncl; cattr[c][0].val.clusterDim.y = 1; cattr[c][0].val.clusterDim.z = 1;
+            cfg[c].gridDim = dim3((unsigned)(by_cls[c].size() * ncl));
+            cfg[c].blockDim = dim3(cls_threads[c]);
+            cfg[c].dynamicSmemBytes = (size_t)cls_per[c] * SOR_CL_BYTES_PER_CELL;
+            cfg[c].stream = s;
+            cfg[c].attrs = cattr[c];
+            cfg[c].numAttrs = 1;
+            shape[2 * c] = (uint32_t)by_cls[c].size();
+            shape[2 * c + 1] = cls_per[c];
+            first += (uint32_t)by_cls[c].size();
+        }
+    }
     auto enqueue = [&]() -> cudaError_t {
         k_sor_clear<<<grid_for(ncell, 256), 256, 0, s>>>((uint32_t)ncell, st->ccode.p, st->csid.p);
         k_sor_scatter<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p,
@@ -1157,18 +1204,29 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
         k_sor_init<<<grid_for(nst, 256), 256, 0, s>>>(nst, st->resid_buf.p, st->sweeps.p, st->resid.p);
         cudaError_t e = cudaMemsetAsync(w->barrier.p, 0, sizeof(GridBarrier), s);
         if (e == cudaSuccess) e = cudaMemsetAsync(w->err.p, 0, sizeof(uint32_t), s);
-        if (use_cl && n_big) {
-            // the large clusters are submitted first: each of their blocks needs most of an SM (1,024 threads and
-            // up to 229 KB of shared memory), and the small blocks fill what the large ones leave
-            if (e == cudaSuccess) e = cudaEventRecord(st->fork, s);
-            if (e == cudaSuccess) e = cudaLaunchKernelEx(&ccfg, k_sor_cluster, CA);
-            if (e == cudaSuccess) e = cudaStreamWaitEvent(st->aux, st->fork, 0);
-            if (e == cudaSuccess) e = cudaLaunchKernelEx(&scfg, k_sor_cluster, CS);
-            if (e == cudaSuccess) e = cudaEventRecord(st->join, st->aux);
-            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, st->join, 0);
+        if (use_cl) {
+            // the classes' launches side by side, the widest first: their blocks need whole SMs (1,024 threads and
+            // large shared memory) and the narrower blocks fill what is left; the first class with clusters runs on
+            // the world's stream, each later one on its own stream forked after the set-up and joined back
+            int first = -1, forked = 0;
+            for (int c = 0; c < NCLS && e == cudaSuccess; c++) {
+                if (by_cls[c].empty()) continue;
+                if (first < 0) {
+                    first = c;
+                    e = cudaEventRecord(st->fork, s);
+                    if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg[c], k_sor_cluster, CC[c]);
+                    continue;
+                }
+                cudaStream_t a = st->aux[forked];
+                e = cudaStreamWaitEvent(a, st->fork, 0);
+                cfg[c].stream = a;
+                if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg[c], k_sor_cluster, CC[c]);
+                if (e == cudaSuccess) e = cudaEventRecord(st->join[forked], a);
+                if (e == cudaSuccess) e = cudaStreamWaitEvent(s, st->join[forked], 0);
+                forked++;
+            }
         } else if (e == cudaSuccess) {
-            e = use_cl ? cudaLaunchKernelEx(&ccfg, k_sor_cluster, CA)
-                       : cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s);
+            e = cudaLaunchCooperativeKernel((void *)k_sor_redblack, dim3(grid), dim3(SOR_BLOCK), args, 0, s);
         }
         if (e != cudaSuccess) return e;
         k_sor_gather<<<grid_for(w->ns, 256), 256, 0, s>>>(w->ns, w->s_cell.p, w->s_scene.p, w->s_mat.p, w->s_sid.p,
@@ -1179,8 +1237,8 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     // capture (a cooperative launch in a graph), the solve launches directly from then on
     cudaGraphExec_t ex = nullptr;
     for (auto &g : st->graphs)
-        if (g.n_work == n_launch && g.grid == grid && g.mode == (use_cl ? 1u : 0u) && g.n_big == n_big &&
-            g.grid_small == per_small)
+        if (g.n_work == n_launch && g.grid == grid && g.mode == (use_cl ? 1u : 0u) &&
+            std::memcmp(g.shape, shape, sizeof shape) == 0)
             ex = g.exec;
     if (!ex && st->graphs_ok) {
         cudaGraph_t gr = nullptr;
@@ -1196,7 +1254,10 @@ static sf_status solve_impl(sf_world *w, int32_t structure, const int32_t *ids, 
         if (!ex) { st->graphs_ok = false; cudaGetLastError(); }
         else {
             if (st->graphs.size() >= 8) { cudaGraphExecDestroy(st->graphs.front().exec); st->graphs.erase(st->graphs.begin()); }
-            st->graphs.push_back({n_launch, grid, use_cl ? 1u : 0u, n_big, per_small, ex});
+            SorState::Graph g{};
+            g.n_work = n_launch; g.grid = grid; g.mode = use_cl ? 1u : 0u; g.exec = ex;
+            std::memcpy(g.shape, shape, sizeof shape);
+            st->graphs.push_back(g);
         }
     }
     if (ex) { SF_CUDA(cudaGraphLaunch(ex, s)); st->graph_launches++; }
