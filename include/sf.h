@@ -10,6 +10,8 @@
  *   sf_structure_solve   replaces the load-path sweeps of `structural(w, dt)` and `warm_step(w)`
  *                        (sor_struct / sor_brick, src/lib.rs:1005-1079, 1268-1281)
  *   sf_structure_check   replaces the joint pass of `structural` (stress_brick, src/lib.rs:1153-1227, 1323-1339)
+ *   sf_world_connectivity replaces `connectivity(w)` (conn_struct, src/lib.rs:1085-1141), which `step` runs after
+ *                        the substeps and again after `structural` (src/lib.rs:3653, 3659)
  *
  * and for the read-outs the reference hands out as raw pointers (`ptr_stats`, `ptr_structs`, … src/lib.rs:4026-4057)
  * it offers copy-out readers into caller buffers. Plain pointers and sizes only; every call returns an sf_status
@@ -81,7 +83,9 @@ typedef struct sf_params {
     uint32_t sor_cluster;       /* 1: a structure of at most 65,534 bricks is solved by one thread-block cluster that
                                    keeps its cells in shared memory (same potentials and sweeps); 0: always the
                                    grid-wide kernel */
-    uint32_t reserved[6];
+    uint32_t detach_bodies;     /* spare bodies per scene for pieces that sf_structure_connect detaches (0 = none) */
+    uint32_t detach_bricks;     /* spare body bricks per scene for those pieces */
+    uint32_t reserved[4];
 } sf_params;
 
 typedef struct sf_stats {
@@ -215,6 +219,34 @@ sf_status sf_structure_warm(sf_world *w, int32_t structure);
 sf_status sf_structure_frame(sf_world *w, uint32_t frame, float dt, const int32_t *active, uint32_t n_active,
                              sf_frame_report *report);
 sf_status sf_read_structure_state(sf_world *w, int32_t *warm, uint8_t *solved, float *settle, double *resid);
+
+/* ---- connectivity and detachment (conn_struct, src/lib.rs:1085-1134; connectivity, src/lib.rs:1137-1141)
+ * A structure's static bricks that no longer reach a grounded footing through intact bonds become rigid bodies: one
+ * body per bonded piece, its bricks in the order of the reference's breadth-first walk (pieces seeded in brick order,
+ * neighbours in the order +x, -x, +y, -y, +z, -z), set up at rest with the identity rotation (setup_body,
+ * src/lib.rs:844-891), and every sleeping body within (radius + 1.5 m + its radius) of a new body is woken
+ * (wake_near, src/lib.rs:925-929). A new body takes the scene's next spare body and its bricks the next spare body
+ * bricks (sf_params.detach_bodies / detach_bricks); a piece that does not fit stays static and its structure stays
+ * pending, as the reference retries when its body pool is full. The detached static bricks are removed (material 0,
+ * potential and loads 0); their bonds, which now join body bricks, are kept.
+ * sf_structure_connect runs the listed structures in the given order; sf_world_connectivity runs, in structure
+ * order, every structure pending since the last call: one whose joint failed or whose brick was crushed in a joint
+ * pass (sf_structure_check or sf_structure_frame with live joints), or one left pending by a piece that did not fit.
+ * now / top (optional, indexed by structure id, n_structures entries) receive, for each structure walked, the bricks
+ * of it still standing and its height in cells (st_now, st_top, src/lib.rs:1126-1128); other entries are untouched. */
+typedef struct sf_connect_report {
+    uint32_t structures;        /* structures walked */
+    uint32_t pieces;            /* bodies created */
+    uint32_t detached;          /* static bricks that became body bricks */
+    uint32_t retry;             /* structures left pending because a piece did not fit */
+    uint64_t listed;            /* static bricks of unsupported pieces read back from the GPU for the walk */
+    double ms;                  /* host wall time of the call */
+} sf_connect_report;
+sf_status sf_structure_connect(sf_world *w, const int32_t *structures, uint32_t n, uint32_t *now, int32_t *top,
+                               sf_connect_report *report);
+sf_status sf_world_connectivity(sf_world *w, uint32_t *now, int32_t *top, sf_connect_report *report);
+/* per scene: static_off, n_static, body_off, body capacity, brick_off, brick capacity, bodies used, bricks used */
+sf_status sf_world_scene_ranges(const sf_world *w, uint32_t scene, uint32_t out8[8]);
 /* Per-structure sweeps and final residuals of the last sf_structure_solve (n_structures entries each). */
 sf_status sf_read_solve_detail(sf_world *w, uint32_t *sweeps, double *resid);
 

@@ -101,6 +101,10 @@ def load() -> C.CDLL:
     lib.ow_remove_static.argtypes = [C.c_void_p, C.c_uint32]
     lib.ow_structure_loads.argtypes = [C.c_void_p, _i32p, C.c_uint32]
     lib.ow_get_ext.argtypes = [C.c_void_p, _f32p]
+    lib.ow_set_capacity.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
+    lib.ow_connect.argtypes = [C.c_void_p, _i32p, C.c_uint32, _u32p, _u32p, _i32p]
+    lib.ow_connectivity.argtypes = [C.c_void_p, _u32p, _u32p, _i32p]
+    lib.ow_conn_pending.argtypes = [C.c_void_p, _u8p]
     lib.ow_collide_hulls.restype = C.c_int32
     lib.ow_collide_hulls.argtypes = [_f32p, _f32p, _f32p, C.c_float, C.c_int32, _f32p]
     lib.ow_ref_colouring.argtypes = [C.c_uint32, _u32p, _u32p, _u32p, _u8p, _u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
@@ -128,7 +132,17 @@ class OracleWorld:
                                     _p(s.body_brick_mat, C.c_uint8), _p(s.body_pose, C.c_float))
         if not self.h:
             raise ValueError("oracle rejected the scene")
-        self.ns, self.nd, self.nb = s.n_static, s.n_body_bricks, s.n_bodies
+        self.ns = s.n_static
+        self.n_struct = int(s.static_sid.max()) + 1 if s.n_static else 0
+
+    # body and body-brick counts grow when connectivity detaches pieces
+    @property
+    def nb(self):
+        return self.counts()["n_bodies"]
+
+    @property
+    def nd(self):
+        return self.counts()["n_body_bricks"]
 
     def close(self):
         if self.h:
@@ -260,6 +274,33 @@ class OracleWorld:
 
     def remove_static(self, i):
         self.lib.ow_remove_static(self.h, int(i))
+
+    def set_capacity(self, spare_bodies, spare_bricks):
+        """Room for detached pieces beyond the bodies and bricks the scene was created with."""
+        self.lib.ow_set_capacity(self.h, int(spare_bodies), int(spare_bricks))
+
+    def _conn_out(self):
+        n = max(self.n_struct, 1)
+        return np.zeros(3, np.uint32), np.zeros(n, np.uint32), np.zeros(n, np.int32)
+
+    def connect(self, structures):
+        """conn_struct of the listed structures in order; returns ((pieces, detached, pending), now, top)."""
+        ids = np.ascontiguousarray(structures, np.int32)
+        c, now, top = self._conn_out()
+        self.lib.ow_connect(self.h, _p(ids, C.c_int32), len(ids), _p(c, C.c_uint32), _p(now, C.c_uint32),
+                            _p(top, C.c_int32))
+        return tuple(int(x) for x in c), now, top
+
+    def connectivity(self):
+        """connectivity(): every pending structure in structure order; returns as connect."""
+        c, now, top = self._conn_out()
+        self.lib.ow_connectivity(self.h, _p(c, C.c_uint32), _p(now, C.c_uint32), _p(top, C.c_int32))
+        return tuple(int(x) for x in c), now, top
+
+    def pending(self):
+        f = np.zeros(max(self.n_struct, 1), np.uint8)
+        self.lib.ow_conn_pending(self.h, _p(f, C.c_uint8))
+        return f[:self.n_struct]
 
 
 def collide_hulls(hull_data, a, b, margin=0.02, reduce=False):

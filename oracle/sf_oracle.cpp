@@ -181,6 +181,9 @@ struct World {
     std::vector<uint8_t> st_solved;
     std::vector<float> st_settle;
     std::vector<double> st_resid;
+    std::vector<int64_t> st_size;    // bricks per structure at creation (the reference's st_hi - st_lo)
+    std::vector<uint8_t> st_conn;    // per structure: a joint failed or a brick was crushed since the last walk
+    uint32_t cap_bodies = 0, cap_bricks = 0;   // capacity for detached pieces (bodies, body bricks)
     uint32_t crush_n = 0;
 
     uint32_t gget(int x, int y, int z) const {
@@ -400,6 +403,8 @@ static SorResult sor_solve(World& w, int s, float omega, double tol, uint32_t ma
 // ---------------------------------------------------------------- joint checks (src/lib.rs:1153-1227)
 enum { J_HOLD = 0, J_FATIGUE = 1, J_FAIL = 2, J_CRUSH = 3 };
 struct Joint { uint32_t i, axis, j, decision, crushed; float ratio, bond_after; };
+// a failed joint or a crushed brick leaves its structure pending a connectivity walk (src/lib.rs:714, 1202, 1223)
+static void flag_conn(World& w, int32_t s) { if (s >= 0 && s < (int32_t)w.st_conn.size()) w.st_conn[s] = 1; }
 
 static float stress_brick(World& w, uint32_t i, float dt, bool live, std::vector<Joint>& out) {
     uint8_t mi = w.mat[i];
@@ -430,6 +435,7 @@ static float stress_brick(World& w, uint32_t i, float dt, bool live, std::vector
             if (nhp < w.bmax[(size_t)i * 4 + a] * 0.08f) {
                 if (up == 0.0f && fabs_(u) > 0.5f && w.crush_n < 300) {
                     w.crush_n++;
+                    if (!dynb) flag_conn(w, w.sid[i]);
                     uint32_t k = CAPV[w.mat[j]] < CAPV[mi] ? j : i;
                     jr.decision = J_CRUSH; jr.crushed = k; jr.bond_after = hp;
                     out.push_back(jr);
@@ -438,6 +444,7 @@ static float stress_brick(World& w, uint32_t i, float dt, bool live, std::vector
                     return maxf(maxr, r);
                 }
                 w.bond[(size_t)i * 4 + a] = 0.0f;
+                if (!dynb) flag_conn(w, w.sid[i]);
                 jr.decision = J_FAIL; jr.bond_after = 0.0f;
             } else {
                 w.bond[(size_t)i * 4 + a] = nhp;
@@ -455,7 +462,7 @@ static float stress_brick(World& w, uint32_t i, float dt, bool live, std::vector
         if (live && r > 1.0f) {
             float& b3 = w.bond[(size_t)i * 4 + 3];
             b3 -= b3 * dt * 2.2f * (r - 0.85f);
-            if (b3 < w.bmax[(size_t)i * 4 + 3] * 0.08f) { b3 = 0.0f; jr.decision = J_FAIL; }
+            if (b3 < w.bmax[(size_t)i * 4 + 3] * 0.08f) { b3 = 0.0f; jr.decision = J_FAIL; flag_conn(w, w.sid[i]); }
             else jr.decision = J_FATIGUE;
             jr.bond_after = b3;
         }
@@ -479,8 +486,7 @@ static double rb64_sweep(World& w, const std::vector<uint32_t>& list, double ome
     return md / mp;
 }
 static void sched_size(World& w) {
-    int32_t n = 0;
-    for (uint32_t i = 0; i < w.ns; i++) n = std::max(n, w.sid[i] + 1);
+    const int32_t n = (int32_t)w.st_size.size();
     if ((int32_t)w.st_warm.size() < n) {
         w.st_warm.resize(n, 0); w.st_solved.resize(n, 0); w.st_settle.resize(n, 0.0f); w.st_resid.resize(n, 0.0);
     }
@@ -501,12 +507,12 @@ static void structure_frame(World& w, uint32_t frame, float dt, const int32_t* a
     std::vector<int32_t> act;
     for (uint32_t t = 0; t < n_active; t++) {
         int32_t s = active[t];
-        if (s >= 0 && s < nst && w.st_solved[s] && !lists[s].empty()) act.push_back(s);
+        if (s >= 0 && s < nst && w.st_solved[s] && w.st_size[s] > 0) act.push_back(s);
     }
-    // the sweep loop of structural (src/lib.rs:1268-1281)
+    // the sweep loop of structural (src/lib.rs:1268-1281); a structure's size is its brick range at creation
     int64_t budget = 160000;
     for (int32_t s : act) {
-        const int64_t size = (int64_t)lists[s].size();
+        const int64_t size = w.st_size[s];
         const uint32_t nmin = w.st_resid[s] < 1e-4 ? (((frame + (uint32_t)s) % 3 == 0) ? 1u : 0u) : (size > 15000 ? 1u : 6u);
         if (nmin == 0) continue;
         uint32_t n = 0;
@@ -542,7 +548,7 @@ static void structure_frame(World& w, uint32_t frame, float dt, const int32_t* a
     // warm_step (src/lib.rs:1068-1079)
     int64_t wb = 120000;
     for (int32_t s = 0; s < nst; s++) {
-        const int64_t size = (int64_t)lists[s].size();
+        const int64_t size = w.st_size[s];
         if (size == 0) continue;
         while (w.st_warm[s] > 0 && wb > 0) {
             const float om = w.st_warm[s] > 60 ? 1.9f : 1.0f;
@@ -559,6 +565,89 @@ static void structure_frame(World& w, uint32_t frame, float dt, const int32_t* a
         counts[4] = over; counts[5] = failed; counts[6] = crushed;
         std::memcpy(&counts[7], &mr, 4);
     }
+}
+
+// ---------------------------------------------------------------- connectivity (src/lib.rs:925-929, 1085-1141)
+// wake_near (src/lib.rs:925-929)
+static void wake_near(World& w, V p, float r) {
+    for (uint32_t b = 0; b < w.nbody; b++)
+        if (w.alive[b] && w.asleep[b] && len(sub(w.pos[b], p)) < r + w.rad[b]) { w.asleep[b] = 0; w.sleep[b] = 0.0f; }
+}
+// A new body for a detached piece: the next body id, its bricks appended to the body bricks in walk order (the
+// reference keeps a brick's id when it changes owner; ids only order pair tests, and the library appends, so this
+// restatement appends too). False when the capacity given at creation is spent.
+static bool detach_piece(World& w, const std::vector<uint32_t>& lst) {
+    const uint32_t n = (uint32_t)lst.size();
+    if (w.nbody + 1 > w.cap_bodies || w.nd + n > w.cap_bricks) return false;
+    const uint32_t b = w.nbody++;
+    w.alive.push_back(0); w.asleep.push_back(0); w.wake.push_back(0);
+    w.first.push_back(NONE); w.count.push_back(0); w.nc.push_back(0);
+    w.pos.push_back(vv(0, 0, 0)); w.v.push_back(vv(0, 0, 0)); w.w.push_back(vv(0, 0, 0));
+    w.vpre.push_back(vv(0, 0, 0)); w.wpre.push_back(vv(0, 0, 0));
+    for (int k = 0; k < 4; k++) w.q.push_back(0.0f);
+    for (int k = 0; k < 9; k++) { w.rot.push_back(0.0f); w.iil.push_back(0.0f); w.iiw.push_back(0.0f); }
+    w.m.push_back(0.0f); w.im.push_back(0.0f); w.sleep.push_back(0.0f); w.rad.push_back(0.0f); w.maxr.push_back(0.0f);
+    w.island.push_back(NONE);
+    std::vector<uint32_t> nl;
+    for (uint32_t i : lst) {
+        const uint32_t k = w.ns + w.nd++;
+        w.mat.push_back(w.mat[i]); w.infill.push_back(0);
+        w.bx.push_back(w.bx[i]); w.by.push_back(w.by[i]); w.bz.push_back(w.bz[i]); w.sid.push_back(-1);
+        w.body.push_back(STATIC); w.next.push_back(NONE); w.sup.push_back(0);
+        w.local.push_back(lat_pos(w.bx[i], w.by[i], w.bz[i])); w.wpos.push_back(vv(0, 0, 0));
+        for (int d = 0; d < 6; d++) w.nb6.push_back(NONE);
+        for (int a = 0; a < 4; a++) { w.bond.push_back(0.0f); w.bmax.push_back(0.0f); }
+        w.phi.push_back(0.0f); w.ext.push_back(0.0f); w.stress.push_back(0.0f); w.phi64.push_back(0.0);
+        w.hnext.push_back(NONE);
+        nl.push_back(k);
+        // the static brick leaves the static set with potential and load 0 (src/lib.rs:1118)
+        w.gset(w.bx[i], w.by[i], w.bz[i], 0);
+        w.mat[i] = 0; w.phi[i] = 0.0f; w.phi64[i] = 0.0; w.ext[i] = 0.0f;
+    }
+    const float idm[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    const float q0[4] = {0, 0, 0, 1};
+    setup_body(w, b, nl.data(), n, vv(0, 0, 0), idm, q0, vv(0, 0, 0), vv(0, 0, 0));
+    wake_near(w, w.pos[b], w.rad[b] + 1.5f);
+    return true;
+}
+// conn_struct (src/lib.rs:1085-1134): the grounded walk from the footings, then one body per remaining piece in brick
+// order. counts: [0] pieces, [1] detached bricks, [2] 1 = a piece did not fit (the structure stays pending).
+static void conn_struct(World& w, int32_t s, uint32_t* counts) {
+    std::vector<uint8_t> stamp(w.ns, 0);
+    std::vector<uint32_t> q;
+    for (uint32_t i = 0; i < w.ns; i++)
+        if (w.in_struct(i, s) && w.by[i] == 0 && w.bond[(size_t)i * 4 + 3] > 0.0f) { stamp[i] = 1; q.push_back(i); }
+    for (size_t h = 0; h < q.size(); h++) {
+        const uint32_t i = q[h];
+        for (int d = 0; d < 6; d++) {
+            uint32_t j; float hp;
+            if (w.linked(i, d, j, hp) && !stamp[j]) { stamp[j] = 1; q.push_back(j); }
+        }
+    }
+    bool retry = false;
+    std::vector<uint32_t> lst;
+    for (uint32_t st = 0; st < w.ns; st++) {
+        if (!w.in_struct(st, s) || stamp[st]) continue;
+        lst.clear();
+        stamp[st] = 1;
+        lst.push_back(st);
+        for (size_t h = 0; h < lst.size(); h++) {
+            const uint32_t i = lst[h];
+            for (int d = 0; d < 6; d++) {
+                uint32_t j; float hp;
+                if (w.linked(i, d, j, hp) && !stamp[j]) { stamp[j] = 1; lst.push_back(j); }
+            }
+        }
+        if (!detach_piece(w, lst)) { retry = true; continue; }
+        counts[0]++;
+        counts[1] += (uint32_t)lst.size();
+    }
+    if (retry) { w.st_conn[s] = 1; counts[2]++; }
+}
+// st_now / st_top (src/lib.rs:1126-1128)
+static void struct_tally(const World& w, int32_t s, uint32_t& now, int32_t& top) {
+    now = 0; top = 0;
+    for (uint32_t i = 0; i < w.ns; i++) if (w.in_struct(i, s)) { now++; top = std::max(top, w.by[i] + 1); }
 }
 
 // ---------------------------------------------------------------- rigid step (src/lib.rs:1367-1783)
@@ -1221,6 +1310,12 @@ void* ow_create(uint32_t n_static, const int32_t* static_xyz, const uint8_t* sta
         w->local[i] = lat_pos(x, y, z); w->wpos[i] = w->local[i];
     }
     for (uint32_t i = 0; i < n_static; i++) finalize_brick(*w, i);
+    int32_t nst = 0;
+    for (uint32_t i = 0; i < n_static; i++) nst = std::max(nst, w->sid[i] + 1);
+    w->st_size.assign(nst, 0);
+    w->st_conn.assign(nst, 0);
+    for (uint32_t i = 0; i < n_static; i++) if (w->sid[i] >= 0) w->st_size[w->sid[i]]++;
+    w->cap_bodies = n_bodies; w->cap_bricks = nd;
     w->nbody = n_bodies;
     uint32_t nb = n_bodies;
     w->alive.assign(nb, 0); w->asleep.assign(nb, 0); w->wake.assign(nb, 0);
@@ -1364,6 +1459,33 @@ void ow_structure_state(void* h, int32_t* warm, uint8_t* solved, float* settle, 
         if (resid) resid[s] = w->st_resid[s];
     }
 }
+void ow_set_capacity(void* h, uint32_t spare_bodies, uint32_t spare_bricks) {
+    World* w = (World*)h;
+    w->cap_bodies = w->nbody + spare_bodies; w->cap_bricks = w->nd + spare_bricks;
+}
+// counts: pieces, detached bricks, structures left pending; now / top indexed by structure (NULL = not wanted)
+void ow_connect(void* h, const int32_t* ids, uint32_t n, uint32_t* counts, uint32_t* now, int32_t* top) {
+    World* w = (World*)h;
+    counts[0] = counts[1] = counts[2] = 0;
+    for (uint32_t k = 0; k < n; k++) {
+        const int32_t s = ids[k];
+        if (s < 0 || s >= (int32_t)w->st_conn.size()) continue;
+        w->st_conn[s] = 0;
+        conn_struct(*w, s, counts);
+        uint32_t c; int32_t t;
+        struct_tally(*w, s, c, t);
+        if (now) now[s] = c;
+        if (top) top[s] = t;
+    }
+}
+// connectivity (src/lib.rs:1137-1141): every pending structure in structure order
+void ow_connectivity(void* h, uint32_t* counts, uint32_t* now, int32_t* top) {
+    World* w = (World*)h;
+    std::vector<int32_t> ids;
+    for (size_t s = 0; s < w->st_conn.size(); s++) if (w->st_conn[s]) ids.push_back((int32_t)s);
+    ow_connect(h, ids.data(), (uint32_t)ids.size(), counts, now, top);
+}
+void ow_conn_pending(void* h, uint8_t* flags) { World* w = (World*)h; for (size_t s = 0; s < w->st_conn.size(); s++) flags[s] = w->st_conn[s]; }
 void ow_get_phi(void* h, float* phi) { World* w = (World*)h; for (uint32_t i = 0; i < w->ns; i++) phi[i] = w->phi[i]; }
 void ow_get_phi64(void* h, double* phi) { World* w = (World*)h; for (uint32_t i = 0; i < w->ns; i++) phi[i] = w->phi64[i]; }
 void ow_set_phi(void* h, const float* phi) { World* w = (World*)h; for (uint32_t i = 0; i < w->ns; i++) { w->phi[i] = phi[i]; w->phi64[i] = phi[i]; } }

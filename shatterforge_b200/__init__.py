@@ -54,7 +54,8 @@ class Params(C.Structure):
     _fields_ = [("substeps", C.c_uint32), ("iterations", C.c_uint32), ("sleep_mode", C.c_uint32),
                 ("pinch_kill", C.c_uint32), ("max_colors", C.c_uint32), ("contact_capacity", C.c_uint32),
                 ("verify", C.c_uint32), ("solve_blocks", C.c_uint32), ("manifold_chunk", C.c_uint32),
-                ("sor_cluster", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+                ("sor_cluster", C.c_uint32), ("detach_bodies", C.c_uint32), ("detach_bricks", C.c_uint32),
+                ("reserved", C.c_uint32 * 4)]
 
 
 class Stats(C.Structure):
@@ -89,6 +90,11 @@ class FrameReport(C.Structure):
     _fields_ = [("sweeps", C.c_uint32), ("warm_sweeps", C.c_uint32), ("brick_updates", C.c_uint64), ("ms", C.c_double),
                 ("live", C.c_uint32), ("max_ratio", C.c_float), ("joints", C.c_uint64), ("over", C.c_uint64),
                 ("failed", C.c_uint64), ("crushed", C.c_uint64)]
+
+
+class ConnectReport(C.Structure):
+    _fields_ = [("structures", C.c_uint32), ("pieces", C.c_uint32), ("detached", C.c_uint32), ("retry", C.c_uint32),
+                ("listed", C.c_uint64), ("ms", C.c_double)]
 
 
 class WorldInfo(C.Structure):
@@ -151,6 +157,9 @@ PROTOTYPES = {
     "sf_structure_warm": (C.c_int32, [C.c_void_p, C.c_int32]),
     "sf_structure_frame": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_float, _i32p, C.c_uint32, C.POINTER(FrameReport)]),
     "sf_read_structure_state": (C.c_int32, [C.c_void_p, _i32p, _u8p, _f32p, C.POINTER(C.c_double)]),
+    "sf_structure_connect": (C.c_int32, [C.c_void_p, _i32p, C.c_uint32, _u32p, _i32p, C.POINTER(ConnectReport)]),
+    "sf_world_connectivity": (C.c_int32, [C.c_void_p, _u32p, _i32p, C.POINTER(ConnectReport)]),
+    "sf_world_scene_ranges": (C.c_int32, [C.c_void_p, C.c_uint32, _u32p]),
     "sf_structure_loads": (C.c_int32, [C.c_void_p, _i32p, C.c_uint32]),
     "sf_world_get_info": (C.c_int32, [C.c_void_p, C.POINTER(WorldInfo)]),
     "sf_get_stats": (C.c_int32, [C.c_void_p, C.POINTER(Stats)]),
@@ -325,9 +334,11 @@ class World:
         info = WorldInfo()
         _check(lib.sf_world_get_info(h, C.byref(info)), "sf_world_get_info")
         self.info = info
-        self.static_off = np.cumsum([0] + [s.n_static for s in self.scenes])
-        self.body_off = np.cumsum([0] + [s.n_bodies for s in self.scenes])
-        self.brick_off = np.cumsum([0] + [s.n_body_bricks for s in self.scenes])
+        # per scene its ranges (capacities include the spare bodies and bricks for detached pieces)
+        r = np.array([self.scene_ranges(k) for k in range(len(self.scenes))], np.int64).reshape(-1, 8)
+        self.static_off = np.append(r[:, 0], r[-1, 0] + r[-1, 1]) if len(r) else np.zeros(1, np.int64)
+        self.body_off = np.append(r[:, 2], r[-1, 2] + r[-1, 3]) if len(r) else np.zeros(1, np.int64)
+        self.brick_off = np.append(r[:, 4], r[-1, 4] + r[-1, 5]) if len(r) else np.zeros(1, np.int64)
 
     # -- lifecycle
     def close(self):
@@ -426,6 +437,33 @@ class World:
                                                  _ptr(settle, C.c_float), _ptr(resid, C.c_double)), "sf_read_structure_state")
         k = self.info.n_structures
         return warm[:k], solved[:k], settle[:k], resid[:k]
+
+    def scene_ranges(self, scene: int):
+        """(static_off, n_static, body_off, body capacity, brick_off, brick capacity, bodies used, bricks used)."""
+        out = np.zeros(8, np.uint32)
+        _check(self._lib.sf_world_scene_ranges(self._h, int(scene), _ptr(out, C.c_uint32)), "sf_world_scene_ranges")
+        return tuple(int(x) for x in out)
+
+    def _conn_out(self):
+        n = max(self.info.n_structures, 1)
+        return np.zeros(n, np.uint32), np.zeros(n, np.int32), ConnectReport()
+
+    def structure_connect(self, structures):
+        """conn_struct of the listed structures, in order: unsupported pieces become bodies. Returns (report, now,
+        top) with now / top per structure id (bricks still standing, height in cells) for the listed ones."""
+        a = np.ascontiguousarray(structures, np.int32)
+        now, top, r = self._conn_out()
+        _check(self._lib.sf_structure_connect(self._h, _ptr(a, C.c_int32), len(a), _ptr(now, C.c_uint32),
+                                              _ptr(top, C.c_int32), C.byref(r)), "sf_structure_connect")
+        return r, now, top
+
+    def connectivity(self):
+        """connectivity(): every structure pending since the last call (a joint failed or a brick was crushed, or a
+        piece did not fit), in structure order. Returns as structure_connect."""
+        now, top, r = self._conn_out()
+        _check(self._lib.sf_world_connectivity(self._h, _ptr(now, C.c_uint32), _ptr(top, C.c_int32), C.byref(r)),
+               "sf_world_connectivity")
+        return r, now, top
 
     def structure_check(self, structure: int = -1, dt: float = 1.0 / 60.0, live: bool = True) -> CheckReport:
         r = CheckReport()

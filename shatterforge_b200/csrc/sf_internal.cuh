@@ -161,6 +161,7 @@ struct GridBarrier { unsigned count; unsigned gen; };
 
 struct StepState;    // sf_step.cu
 struct SorState;     // sf_sor.cu
+struct ConnState;    // sf_connect.cu
 uint64_t sor_launches(const SorState *st);
 const Tuner *sor_tuner(const SorState *st);
 uint64_t sor_graph_launches(const SorState *st);
@@ -194,11 +195,15 @@ cudaError_t finalize_on_buffers(uint32_t ns, const uint32_t *cell, const uint32_
                                 const uint8_t *infill, const int32_t *sid, const uint32_t *ctab, const uint32_t *cpool,
                                 uint32_t *nb6, float *bond, float *bmax, cudaStream_t s);
 
+// n_bodies and n_bricks are the scene's capacities; a world created with spare capacity for detached pieces holds
+// its bodies in [body_off, body_off + bodies_used) and their bricks in [brick_off, brick_off + bricks_used), the
+// rest dead (bodies) or owned by the sentinel body (bricks) until sf_structure_connect takes them.
 struct Scene {
     uint32_t static_off, n_static;
     uint32_t body_off, n_bodies;
     uint32_t brick_off, n_bricks;
     uint32_t chunk_off, n_chunks;
+    uint32_t bodies_used = 0, bricks_used = 0;
 };
 
 // A scene pool keeps fixed-capacity scene slots (the Scene ranges above are the capacities); a slot holds one
@@ -251,6 +256,12 @@ struct sf_world {
     sf::DBuf<uint8_t> stage_flags, stage_dirty;
     sf::DBuf<uint32_t> err;      // [0] error bits, [1..] counters
     sf::DBuf<sf::GridBarrier> barrier;
+
+    // connectivity: per structure, set on the GPU when a joint pass fails a joint or crushes a brick (pending walk);
+    // structures a full scene could not take are pending on the host
+    sf::DBuf<uint8_t> st_conn;
+    std::vector<uint8_t> h_conn_retry;
+    sf::ConnState *conn = nullptr;
 
     sf::SorState *sor = nullptr;
     sf::StepState *step = nullptr;
@@ -364,4 +375,32 @@ void step_mark_all_live(sf_world *w);
 void step_set_live(sf_world *w, uint32_t scene, bool live);
 cudaError_t step_reset_labels(sf_world *w, uint32_t first_body, uint32_t n);
 sf_status read_error_word(sf_world *w);
+void conn_destroy(sf_world *w);
+// setup_body (src/lib.rs:844-891) of bodies base .. base + nb - 1 from their bricks and poses (sf_world.cu)
+cudaError_t setup_bodies(sf_world *w, uint32_t base, uint32_t nb, const float *d_pose13);
+
+// Union-find over a parent array whose entries only ever point to smaller indices: a walk ends within n hops and a
+// link attempt fails only when another thread linked the same root first. The bounds are far beyond both; only a
+// corrupt parent array reaches them, which sets ERR_ISLANDS instead of looping.
+__device__ __forceinline__ uint32_t uf_find(uint32_t *parent, uint32_t x, uint32_t *err) {
+    for (int guard = 0; guard < (1 << 20); guard++) {
+        uint32_t p = __ldcg(&parent[x]);
+        if (p == x) return x;
+        uint32_t gp = __ldcg(&parent[p]);
+        if (gp != p) atomicCAS(&parent[x], p, gp);
+        x = p;
+    }
+    atomicOr(err, (unsigned)ERR_ISLANDS);
+    return x;
+}
+__device__ __forceinline__ void uf_union(uint32_t *parent, uint32_t x, uint32_t y, uint32_t *err) {
+    for (int it = 0; it < (1 << 16); it++) {
+        x = uf_find(parent, x, err);
+        y = uf_find(parent, y, err);
+        if (x == y) return;
+        if (x < y) { uint32_t t = x; x = y; y = t; }
+        if (atomicCAS(&parent[x], x, y) == x) return;
+    }
+    atomicOr(err, (unsigned)ERR_ISLANDS);
+}
 }  // namespace sf

@@ -610,7 +610,7 @@ __device__ __forceinline__ bool joint_later(uint32_t i2, int a2, uint32_t i, int
 __global__ void k_stress_apply(const uint32_t *cand, const uint32_t *ncand_p, const uint32_t *req, uint32_t nreq,
                                const int32_t *sid, uint8_t *mat, const uint32_t *nb6, const uint32_t *cell,
                                const uint32_t *scene, const uint32_t *ctab, uint32_t *cpool, float *bond, uint8_t *dec,
-                               float *bond_after, uint32_t *crushed) {
+                               float *bond_after, uint32_t *crushed, uint8_t *conn) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     uint32_t ncand = *ncand_p;
     uint32_t crush_n = 0;
@@ -628,6 +628,7 @@ __global__ void k_stress_apply(const uint32_t *cand, const uint32_t *ncand_p, co
                     if (crush_n >= 300) { d = J_FAIL; dec[o] = J_FAIL; bond_after[o] = 0.0f; crushed[o] = NONE; }
                     else {
                         crush_n++;
+                        conn[s] = 1;   // a removed brick may split the structure (remove_brick, src/lib.rs:705-718)
                         uint32_t k = crushed[o];
                         mat[k] = 0;
                         uint32_t chunk;
@@ -646,6 +647,7 @@ __global__ void k_stress_apply(const uint32_t *cand, const uint32_t *ncand_p, co
                     }
                 }
                 bond[o] = bond_after[o];
+                if (d == J_FAIL) conn[s] = 1;   // a broken joint may split the structure (src/lib.rs:1202, 1223)
             }
         }
     }
@@ -1517,7 +1519,7 @@ static sf_status check_impl(sf_world *w, int32_t structure, const int32_t *ids, 
     k_stress_compact<<<grid_for(ns, 256), 256, 0, s>>>(ns, st->cand_flag.p, st->cand_pos.p, st->cand_list.p);
     k_stress_apply<<<1, 32, 0, s>>>(st->cand_list.p, st->counters.p + 5, st->st_req.p, (uint32_t)req.size(), w->s_sid.p,
                                     w->s_mat.p, w->s_nb6.p, w->s_cell.p, w->s_scene.p, w->ctab.p, w->cpool.p, w->s_bond.p,
-                                    st->j_dec.p, st->j_bond.p, st->j_crushed.p);
+                                    st->j_dec.p, st->j_bond.p, st->j_crushed.p, w->st_conn.p);
     k_stress_tally<<<grid_for(ns, 256), 256, 0, s>>>(ns, st->j_dec.p, st->j_ratio.p, w->s_nb6.p, w->s_sid.p, st->active0.p,
                                                       w->s_stress.p, st->counters.p);
     SF_CUDA(cudaEventRecord(w->ev1, s));

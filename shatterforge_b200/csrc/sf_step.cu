@@ -1034,35 +1034,13 @@ __global__ void k_uf_init(uint32_t nb, const uint32_t *list, uint32_t *parent, u
     parent[b] = b;
     mint[b] = 0x7f7fffffu;
 }
-// Parents only ever point to smaller ids, so a walk ends within (number of bodies) hops and a link attempt fails only
-// when another thread linked the same root first; the bounds below are far beyond both and only a corrupt parent
-// array reaches them, which is reported (ERR_ISLANDS -> SF_ERR_VERIFY) rather than labelled wrongly in silence.
-__device__ __forceinline__ uint32_t uf_find(uint32_t *parent, uint32_t x, uint32_t *err) {
-    for (int guard = 0; guard < (1 << 20); guard++) {
-        uint32_t p = __ldcg(&parent[x]);
-        if (p == x) return x;
-        uint32_t gp = __ldcg(&parent[p]);
-        if (gp != p) atomicCAS(&parent[x], p, gp);
-        x = p;
-    }
-    atomicOr(err, (unsigned)ERR_ISLANDS);
-    return x;
-}
 __global__ void k_uf_union(const uint32_t *nm_p, const uint32_t *man_a, const uint32_t *man_b, uint32_t *parent,
                            uint32_t *err) {
     uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= *nm_p) return;
     uint32_t b = man_b[m];
     if (b == STATIC) return;
-    uint32_t x = man_a[m], y = b;
-    for (int it = 0; it < (1 << 16); it++) {
-        x = uf_find(parent, x, err);
-        y = uf_find(parent, y, err);
-        if (x == y) return;
-        if (x < y) { uint32_t t = x; x = y; y = t; }
-        if (atomicCAS(&parent[x], x, y) == x) return;
-    }
-    atomicOr(err, (unsigned)ERR_ISLANDS);
+    uf_union(parent, man_a[m], b, err);
 }
 __global__ void k_uf_label(uint32_t nb, const uint32_t *list, const uint8_t *alive, const uint8_t *asleep, uint32_t *parent,
                            uint32_t *label, uint32_t *dev, uint32_t *err) {

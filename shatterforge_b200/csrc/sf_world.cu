@@ -72,6 +72,17 @@ __global__ void k_setup_bodies(uint32_t nb, uint32_t base, const uint32_t *first
     if (lb >= nb) return;
     const uint32_t b = base + lb;
     uint32_t s = first[b], n = count[b];
+    if (n == 0) {   // a spare body (capacity for detached pieces) or the sentinel: dead, at rest, finite
+        pos[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f); q[b] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        v[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f); w[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (int k = 0; k < 9; k++) {
+            rot[(size_t)b * 9 + k] = (k % 4 == 0) ? 1.0f : 0.0f;
+            iil[(size_t)b * 9 + k] = 0.0f; iiw[(size_t)b * 9 + k] = 0.0f;
+        }
+        m[b] = 0.0f; im[b] = 0.0f; rad[b] = 0.0f; sleep[b] = 0.0f; maxr[b] = 0.0f;
+        alive[b] = 0; asleep[b] = 0; wake[b] = 0;
+        return;
+    }
     float mass = 0.0f;
     V3 cl = v3(0.0f, 0.0f, 0.0f);
     for (uint32_t t = 0; t < n; t++) {
@@ -259,6 +270,19 @@ static cudaError_t upload(sf::DBuf<T> &d, const std::vector<T> &h, cudaStream_t 
     return cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
 }
 
+namespace sf {
+cudaError_t setup_bodies(sf_world *w, uint32_t base, uint32_t nb, const float *d_pose13) {
+    if (nb == 0) return cudaSuccess;
+    k_setup_bodies<<<grid_for(nb, 128), 128, 0, w->stream>>>(nb, base, w->b_first.p, w->b_count.p, w->k_xyz.p, w->k_mat.p,
+                                                            d_pose13, w->k_local.p, w->k_wpos.p, w->k_body.p, w->b_pos.p,
+                                                            w->b_q.p, w->b_v.p, w->b_w.p, w->b_rot.p, w->b_iil.p,
+                                                            w->b_iiw.p, w->b_m.p, w->b_im.p, w->b_rad.p, w->b_sleep.p,
+                                                            w->b_maxr.p, w->b_alive.p, w->b_asleep.p, w->b_wake.p);
+    w->launches++;
+    return cudaGetLastError();
+}
+}  // namespace sf
+
 extern "C" {
 
 void sf_params_default(sf_params *p) {
@@ -319,10 +343,16 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
             for (int k = 0; k < 13; k++)
                 if (!std::isfinite(d.body_pose[(size_t)b * 13 + k])) { set_error("scene %u body %u: non-finite pose", s, b); return SF_ERR_ARG; }
         for (uint32_t i = 0; i < d.n_static; i++) max_sid = std::max(max_sid, d.static_sid[i]);
-        ns += d.n_static; nd += nbr; nb += d.n_bodies;
+        sc.bodies_used = d.n_bodies; sc.bricks_used = nbr;
+        sc.n_bodies += w->P.detach_bodies; sc.n_bricks += w->P.detach_bricks;
+        ns += d.n_static; nd += sc.n_bricks; nb += sc.n_bodies;
     }
+    // spare capacity for detached pieces: unused bricks belong to an always-dead sentinel body after the scenes'
+    const bool spare = w->P.detach_bodies || w->P.detach_bricks;
+    if (spare) nb += 1;
     if (ns >= 0x7fffffffu || nd >= 0x7fffffffu || nb >= 0x7fffffffu) { set_error("world too large"); return SF_ERR_CAPACITY; }
     w->ns = (uint32_t)ns; w->nd = (uint32_t)nd; w->nb = (uint32_t)nb;
+    if (spare) w->sentinel = (uint32_t)nb - 1;
     w->n_struct = (uint32_t)(max_sid + 1);
 
     // ---- static bricks and the chunk grid (host-side table build, uploaded once)
@@ -411,12 +441,12 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
             uint32_t gb = sc.body_off + b;
             b_first[gb] = sc.brick_off + d.body_first[b];
             b_count[gb] = d.body_first[b + 1] - d.body_first[b];
-            b_scene[gb] = s;
             std::memcpy(&pose[(size_t)gb * 13], d.body_pose + (size_t)b * 13, 13 * sizeof(float));
         }
-        if (sc.n_bricks) {
-            std::memcpy(&k_xyz[(size_t)sc.brick_off * 3], d.body_brick_xyz, (size_t)sc.n_bricks * 3 * sizeof(int32_t));
-            std::memcpy(&k_mat[sc.brick_off], d.body_brick_mat, sc.n_bricks);
+        for (uint32_t b = 0; b < sc.n_bodies; b++) b_scene[sc.body_off + b] = s;
+        if (sc.bricks_used) {
+            std::memcpy(&k_xyz[(size_t)sc.brick_off * 3], d.body_brick_xyz, (size_t)sc.bricks_used * 3 * sizeof(int32_t));
+            std::memcpy(&k_mat[sc.brick_off], d.body_brick_mat, sc.bricks_used);
         }
     }
     SF_CUDA(upload(w->b_first, b_first, st));
@@ -434,7 +464,12 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
     SF_CUDA(w->b_alive.alloc(nb)); SF_CUDA(w->b_asleep.alloc(nb)); SF_CUDA(w->b_wake.alloc(nb));
     SF_CUDA(w->b_nc.alloc(nb));
     SF_CUDA(cudaMemsetAsync(w->b_nc.p, 0, w->b_nc.bytes(), st));
-    SF_CUDA(w->k_local.alloc(nd)); SF_CUDA(w->k_wpos.alloc(nd)); SF_CUDA(w->k_body.alloc(nd));
+    SF_CUDA(w->k_local.alloc(nd)); SF_CUDA(w->k_wpos.alloc(nd));
+    SF_CUDA(upload(w->k_body, std::vector<uint32_t>(nd, spare ? w->sentinel : 0u), st));
+    if (spare) {
+        SF_CUDA(cudaMemsetAsync(w->k_local.p, 0, w->k_local.bytes(), st));
+        SF_CUDA(cudaMemsetAsync(w->k_wpos.p, 0, w->k_wpos.bytes(), st));
+    }
     if (nb) {
         k_setup_bodies<<<grid_for(nb, 128), 128, 0, st>>>((uint32_t)nb, 0u, w->b_first.p, w->b_count.p, w->k_xyz.p, w->k_mat.p,
                                                         d_pose.p, w->k_local.p, w->k_wpos.p, w->k_body.p, w->b_pos.p,
@@ -447,6 +482,9 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
     SF_CUDA(cudaMemsetAsync(w->err.p, 0, w->err.bytes(), st));
     SF_CUDA(w->barrier.alloc(4));
     SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, w->barrier.bytes(), st));
+    SF_CUDA(w->st_conn.alloc(std::max<uint32_t>(w->n_struct, 1)));
+    SF_CUDA(cudaMemsetAsync(w->st_conn.p, 0, w->st_conn.bytes(), st));
+    w->h_conn_retry.assign(w->n_struct, 0);
     sf_status r = sor_create(w.get());
     if (r != SF_OK) return r;
     r = step_create(w.get());
@@ -461,6 +499,7 @@ void sf_world_destroy(sf_world *w) {
     if (w->stream) cudaStreamSynchronize(w->stream);
     sor_destroy(w);
     step_destroy(w);
+    conn_destroy(w);
     if (w->ev0) cudaEventDestroy(w->ev0);
     if (w->ev1) cudaEventDestroy(w->ev1);
     cudaStream_t s = w->own_stream;
@@ -472,6 +511,17 @@ sf_status sf_world_get_info(const sf_world *w, sf_world_info *info) {
     if (!w || !info) return SF_ERR_ARG;
     info->n_scenes = w->n_scenes; info->n_static = w->ns; info->n_bodies = w->nb; info->n_body_bricks = w->nd;
     info->n_structures = w->n_struct; info->n_chunks = w->n_chunks;
+    return SF_OK;
+}
+
+sf_status sf_world_scene_ranges(const sf_world *w, uint32_t scene, uint32_t out8[8]) {
+    if (!w || !out8 || scene >= w->n_scenes) { set_error("no such scene"); return SF_ERR_ARG; }
+    const Scene &sc = w->scenes[scene];
+    const bool pool = !w->pool.empty();
+    out8[0] = sc.static_off; out8[1] = sc.n_static; out8[2] = sc.body_off; out8[3] = sc.n_bodies;
+    out8[4] = sc.brick_off; out8[5] = sc.n_bricks;
+    out8[6] = pool ? w->pool[scene].bodies : sc.bodies_used;
+    out8[7] = pool ? w->pool[scene].bricks : sc.bricks_used;
     return SF_OK;
 }
 
