@@ -367,6 +367,19 @@ struct SorClusterArgs {
     uint32_t *err;
 };
 
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// the address of the same shared-memory location in block `rank` of the cluster
+__device__ __forceinline__ uint32_t mapa_shared(uint32_t a, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ double ld_cluster_f64(uint32_t a) {
+    double v;
+    asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(a));
+    return v;
+}
+
 // threads per block for a launch whose largest block range holds per_max cells: about two cells per thread and sweep
 static unsigned sor_cl_threads(uint32_t per_max) {
     const uint32_t half = per_max / 2;
@@ -404,14 +417,28 @@ __global__ void __launch_bounds__(SOR_CL_MAX_THREADS) k_sor_cluster(SorClusterAr
     const uint32_t off = A.off[q], n = A.n[q], per = A.per[q];
     const uint32_t b0 = min(n, rank * per), b1 = min(n, b0 + per), my = b1 - b0;
     const uint32_t ev = A.even[q * SOR_CL_WIDE + rank];
+    // the shared::cluster address of every block's potentials: a neighbour's is s_base[its rank] + 8 x its index
+    __shared__ uint32_t s_base[SOR_CL_WIDE];
+    if (tid < ncl) s_base[tid] = mapa_shared(smem_addr(phi), tid);
     for (uint32_t i = tid; i < my; i += blockDim.x) {
         const uint32_t g = off + b0 + i;
         const uint32_t at = A.cpos[g];
         phi[i] = A.cphi[at];
         rhs[i] = A.crhs[at];
-        code[i] = A.csid[at] == (int32_t)q ? (A.ccode[at] | CELL_ACTIVE) : 0u;
+        const uint32_t cd = A.csid[at] == (int32_t)q ? (A.ccode[at] | CELL_ACTIVE) : 0u;
+        code[i] = cd;
+        // a face without a neighbour cell of this structure has no link (link code 0, conductance 0); it reads the
+        // cell's own potential, so every update does its six loads without a branch and adds zeros for the faces
+        // without a link (x + 0 = x: the sums are the grid kernel's)
 #pragma unroll
-        for (int d = 0; d < 6; d++) nbr[i * 6 + d] = A.nbr[(size_t)g * 6 + d];
+        for (int d = 0; d < 6; d++) {
+            uint16_t nb = A.nbr[(size_t)g * 6 + d];
+            if (nb == NO_CELL) {
+                if ((cd & CELL_ACTIVE) && ((cd >> (4 * d)) & 15u)) atomicOr(A.err, (unsigned)ERR_SOR_NONFINITE);
+                nb = (uint16_t)((rank << sh) | i);
+            }
+            nbr[i * 6 + d] = nb;
+        }
     }
     const double omega = A.prm->omega, tol = A.prm->tol;
     const uint32_t max_sweeps = A.prm->use_cap ? min(A.prm->max_sweeps, A.cap[q]) : A.prm->max_sweeps;
@@ -426,20 +453,20 @@ __global__ void __launch_bounds__(SOR_CL_MAX_THREADS) k_sor_cluster(SorClusterAr
         auto update = [&](uint32_t i, double &p, double &dabs) -> bool {
             const uint32_t cd = code[i];
             if (!(cd & CELL_ACTIVE)) return false;
+            double pj[6];
+#pragma unroll
+            for (int d = 0; d < 6; d++) {
+                const uint32_t g = nbr[i * 6 + d];
+                pj[d] = ld_cluster_f64(s_base[g >> sh] + ((g & lmask) << 3));
+            }
             double sk = 0.0, skp = 0.0;
 #pragma unroll
             for (int d = 0; d < 6; d++) {
-                const uint32_t lm = (cd >> (4 * d)) & 15u;
-                if (lm == 0) continue;
-                const uint32_t g = nbr[i * 6 + d];
-                if (g == NO_CELL) { atomicOr(A.err, (unsigned)ERR_SOR_NONFINITE); continue; }
-                const uint32_t r = g >> sh, l = g & lmask;
-                const double pj = r == rank ? phi[l] : cl.map_shared_rank(phi, r)[l];
-                const double k = kt[2 * lm + ((d >> 1) == 1 ? 1 : 0)];
+                const double k = kt[2 * ((cd >> (4 * d)) & 15u) + ((d >> 1) == 1 ? 1 : 0)];
                 sk += k;
-                skp += k * pj;
+                skp += k * pj[d];
             }
-            if (cd & (1u << 28)) sk += kt[32 + ((cd >> 24) & 15u)];
+            sk += (cd & (1u << 28)) ? kt[32 + ((cd >> 24) & 15u)] : 0.0;
             p = phi[i];
             dabs = 0.0;
             if (sk > 0.0) {
