@@ -85,7 +85,9 @@ typedef struct sf_params {
                                    grid-wide kernel */
     uint32_t detach_bodies;     /* spare bodies per scene for pieces that sf_structure_connect detaches (0 = none) */
     uint32_t detach_bricks;     /* spare body bricks per scene for those pieces */
-    uint32_t reserved[4];
+    uint32_t damage;            /* 1: damage on contact in every substep (impact_damage, src/lib.rs:1602-1702);
+                                   needs spare capacity */
+    uint32_t reserved[3];
 } sf_params;
 
 typedef struct sf_stats {
@@ -245,6 +247,54 @@ typedef struct sf_connect_report {
 sf_status sf_structure_connect(sf_world *w, const int32_t *structures, uint32_t n, uint32_t *now, int32_t *top,
                                sf_connect_report *report);
 sf_status sf_world_connectivity(sf_world *w, uint32_t *now, int32_t *top, sf_connect_report *report);
+/* ---- brick removal and body splitting (remove_brick, src/lib.rs:705-718; rebuild_body, src/lib.rs:930-1002)
+ * A world created with spare capacity (detach_bodies / detach_bricks) gives body bricks bonds: finalize_brick's rule
+ * between face-adjacent bricks of one body (glass is infill), or the bonds a detached piece's bricks had as static
+ * bricks. sf_world_remove_bricks removes static bricks (world static ids: material 0, out of the grid, their
+ * structures pending a connectivity walk) and body bricks (world body-brick ids: material 0, their bodies marked).
+ * sf_world_rebuild_bodies runs rebuild_body on every marked body in body order: removed bricks leave it, the rest
+ * split into components bonded by intact bonds (seeded in the body's brick order, breadth first); the first stays in
+ * the body, its bricks moved to the front of the body's brick range, each other takes the scene's next spare body and
+ * bricks (without room for all of them the body stays whole, as the reference when its pool is full); every piece is
+ * set up from its bricks' local offsets about the parent's pose and cached rotation, awake. With more than 1,500
+ * bodies of the scene awake, a lone-brick piece other than steel becomes debris (removed) with probability
+ * min((awake - 1500) / 2000, 0.85), drawn from h01 (src/lib.rs:341-345) of the scene's count of rebuilt bodies and
+ * the brick's place in its body instead of the world's random stream. A body left with no brick dies. */
+typedef struct sf_rebuild_report {
+    uint32_t bodies;            /* bodies rebuilt */
+    uint32_t pieces;            /* new bodies */
+    uint32_t removed;           /* bricks of material 0 that left their bodies */
+    uint32_t dissolved;         /* bodies that died with no brick left */
+    uint32_t lone;              /* lone-brick pieces turned to debris */
+    uint32_t reserved;
+    double ms;                  /* host wall time of the call */
+} sf_rebuild_report;
+sf_status sf_world_remove_bricks(sf_world *w, const uint32_t *statics, uint32_t n_statics, const uint32_t *body_bricks,
+                                 uint32_t n_body_bricks);
+sf_status sf_world_rebuild_bodies(sf_world *w, sf_rebuild_report *report);
+/* ---- damage on contact (impact_damage / crush_at, src/lib.rs:1602-1702), with sf_params.damage = 1
+ * Every substep, between the pinch clamps and integration: each contact's absorbed energy E = 1/2 jn vn0 (at least
+ * 150 J at an approach speed of at least 1 m/s) is split between its bricks in proportion to 1 / EB and crushes each
+ * side's bricks nearest the contact point, growing through intact bonds within the body or structure, one budget of
+ * 2,500 bricks per scene and substep in contact list order; the brick a share cannot afford is cracked (its bonds
+ * weakened by 0.6 E / EB of their capacity). A crushed brick is ground away with probability PULV of its material
+ * (drawn from h01 of a fixed seed and the scene's draw count), else severed. Removed or severed static bricks leave
+ * their structures pending a connectivity walk; bodies that lose or sever bricks are marked for
+ * sf_world_rebuild_bodies. The frame then runs, as `step` does (src/lib.rs:3650-3659): sf_world_step,
+ * sf_world_rebuild_bodies, sf_world_connectivity, the load-path calls, sf_world_connectivity.
+ * sf_read_damage returns the counters since the last read and, per structure, whether a hit woke it (a heavy hit
+ * with jn vn0 > 4,000, or a brick of it damaged: st_activate), then clears both. */
+typedef struct sf_damage_report {
+    uint64_t contacts;          /* candidate contacts walked */
+    uint64_t crushed;           /* bricks crushed */
+    uint64_t removed;           /* of them ground away */
+    uint64_t severed;           /* of them severed from their neighbours */
+    uint64_t cracked;           /* bricks whose bonds a leftover share weakened */
+} sf_damage_report;
+sf_status sf_read_damage(sf_world *w, sf_damage_report *report, uint8_t *activated);
+/* body bricks' bonds (4 each: +x, +y, +z, foundation) and face neighbours (6 each, world body-brick ids) */
+sf_status sf_read_body_bonds(sf_world *w, float *bond4, uint32_t *nb6);
+
 /* per scene: static_off, n_static, body_off, body capacity, brick_off, brick capacity, bodies used, bricks used */
 sf_status sf_world_scene_ranges(const sf_world *w, uint32_t scene, uint32_t out8[8]);
 /* Per-structure sweeps and final residuals of the last sf_structure_solve (n_structures entries each). */

@@ -28,7 +28,7 @@ _u64p = C.POINTER(C.c_uint64)
 
 class StepParams(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("substeps", C.c_uint32), ("order", C.c_uint32), ("sleep_mode", C.c_uint32),
-                ("pinch_kill", C.c_uint32), ("chunk", C.c_uint32)]
+                ("pinch_kill", C.c_uint32), ("chunk", C.c_uint32), ("damage", C.c_uint32)]
 
 
 _lib = None
@@ -105,6 +105,10 @@ def load() -> C.CDLL:
     lib.ow_connect.argtypes = [C.c_void_p, _i32p, C.c_uint32, _u32p, _u32p, _i32p]
     lib.ow_connectivity.argtypes = [C.c_void_p, _u32p, _u32p, _i32p]
     lib.ow_conn_pending.argtypes = [C.c_void_p, _u8p]
+    lib.ow_remove_bricks.argtypes = [C.c_void_p, _u32p, C.c_uint32, _u32p, C.c_uint32]
+    lib.ow_rebuild_bodies.argtypes = [C.c_void_p, _u32p]
+    lib.ow_body_bonds.argtypes = [C.c_void_p, _f32p, _u32p]
+    lib.ow_read_damage.argtypes = [C.c_void_p, _u64p, _u8p]
     lib.ow_collide_hulls.restype = C.c_int32
     lib.ow_collide_hulls.argtypes = [_f32p, _f32p, _f32p, C.c_float, C.c_int32, _f32p]
     lib.ow_ref_colouring.argtypes = [C.c_uint32, _u32p, _u32p, _u32p, _u8p, _u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
@@ -190,8 +194,9 @@ class OracleWorld:
         self.lib.ow_get_bonds(self.h, _p(b, C.c_float), _p(nb, C.c_uint32))
         return b, nb
 
-    def step(self, dt=1.0 / 60.0, iterations=10, substeps=2, order=ORDER_COLOR, sleep_mode=SLEEP_BODY, pinch_kill=1, chunk=16):
-        p = StepParams(iterations, substeps, order, sleep_mode, pinch_kill, chunk)
+    def step(self, dt=1.0 / 60.0, iterations=10, substeps=2, order=ORDER_COLOR, sleep_mode=SLEEP_BODY, pinch_kill=1, chunk=16,
+             damage=0):
+        p = StepParams(iterations, substeps, order, sleep_mode, pinch_kill, chunk, damage)
         self.lib.ow_step(self.h, float(dt), C.byref(p))
 
     def contacts(self):
@@ -296,6 +301,32 @@ class OracleWorld:
         c, now, top = self._conn_out()
         self.lib.ow_connectivity(self.h, _p(c, C.c_uint32), _p(now, C.c_uint32), _p(top, C.c_int32))
         return tuple(int(x) for x in c), now, top
+
+    def remove_bricks(self, statics=(), body_bricks=()):
+        """remove_brick of static bricks (static ids) and body bricks (ids counted from the first body brick)."""
+        a = np.ascontiguousarray(statics, np.uint32)
+        b = np.ascontiguousarray(body_bricks, np.uint32)
+        self.lib.ow_remove_bricks(self.h, _p(a, C.c_uint32), len(a), _p(b, C.c_uint32), len(b))
+
+    def rebuild_bodies(self):
+        """rebuild_body of every marked body; returns (bodies, pieces, removed, dissolved, lone)."""
+        c = np.zeros(5, np.uint32)
+        self.lib.ow_rebuild_bodies(self.h, _p(c, C.c_uint32))
+        return tuple(int(x) for x in c)
+
+    def body_bonds(self):
+        nd = self.nd
+        b = np.zeros((nd, 4), np.float32)
+        nb = np.zeros((nd, 6), np.uint32)
+        self.lib.ow_body_bonds(self.h, _p(b, C.c_float), _p(nb, C.c_uint32))
+        return b, nb
+
+    def read_damage(self):
+        """(candidates, crushed, removed, severed, cracked) since the last read, and per structure the hit flags."""
+        c = np.zeros(5, np.uint64)
+        h = np.zeros(max(self.n_struct, 1), np.uint8)
+        self.lib.ow_read_damage(self.h, _p(c, C.c_uint64), _p(h, C.c_uint8))
+        return tuple(int(x) for x in c), h[:self.n_struct]
 
     def pending(self):
         f = np.zeros(max(self.n_struct, 1), np.uint8)

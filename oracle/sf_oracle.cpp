@@ -42,6 +42,7 @@
 #include <cstdint>
 #include <cstring>
 #include <cmath>
+#include <unordered_map>
 #include <vector>
 #include <algorithm>
 #include <numeric>
@@ -108,8 +109,10 @@ const uint32_t HSIZE = 32768;
 const uint32_t NONE = 0xFFFFFFFFu;
 const uint32_t STATIC = 0xFFFFFFFFu;
 const uint32_t MAXC_REF = 30000;
-const uint8_t GLASS = 4, SLUG = 6;
+const uint8_t STEEL = 3, GLASS = 4, SLUG = 6;
 const float MASS[9] = {0.0f, 300.0f, 230.0f, 250.0f, 60.0f, 70.0f, 2000.0f, 8.0f, 44.0f};
+const float EB[9] = {0.0f, 15000.0f, 12000.0f, 1.5e6f, 300.0f, 6000.0f, 1e12f, 1e12f, 1e12f};   // src/lib.rs:178
+const float PULV[9] = {0.0f, 0.7f, 0.55f, 0.0f, 1.0f, 0.5f, 0.0f, 0.0f, 0.0f};                 // src/lib.rs:180
 const float CAPV[9] = {0.0f, 140000.0f, 50000.0f, 150000.0f, 1500.0f, 9000.0f, 1e12f, 1e12f, 1e12f};
 const float CAPH[9] = {0.0f, 12000.0f, 12000.0f, 90000.0f, 400.0f, 5000.0f, 1e12f, 1e12f, 1e12f};
 const float TENS[9] = {0.0f, 0.35f, 0.1f, 0.9f, 0.5f, 0.7f, 1.0f, 1.0f, 1.0f};
@@ -136,7 +139,7 @@ struct Contact {
 enum { ORDER_LIST = 0, ORDER_COLOR = 1 };
 enum { SLEEP_BODY = 0, SLEEP_ISLAND = 1 };
 
-struct StepParams { uint32_t iterations, substeps, order, sleep_mode, pinch_kill; };
+struct StepParams { uint32_t iterations, substeps, order, sleep_mode, pinch_kill, damage; };
 
 // manifold priority for the colouring: a fixed mix of the body pair (b' = 0 for the static side, else b + 1)
 static inline uint32_t pair_priority(uint32_t a, uint32_t bp) {
@@ -184,6 +187,12 @@ struct World {
     std::vector<int64_t> st_size;    // bricks per structure at creation (the reference's st_hi - st_lo)
     std::vector<uint8_t> st_conn;    // per structure: a joint failed or a brick was crushed since the last walk
     uint32_t cap_bodies = 0, cap_bricks = 0;   // capacity for detached pieces (bodies, body bricks)
+    std::vector<uint8_t> dirty;      // per body: a brick was removed since its last rebuild (bd_dirty)
+    std::vector<uint32_t> stamp;     // per brick: the crush that visited it last (src/lib.rs:1650)
+    uint32_t stamp_id = 0, dmg_draws = 0;
+    uint64_t dmg[5] = {0, 0, 0, 0, 0};  // candidates, crushed, removed, severed, cracked
+    std::vector<uint8_t> st_hit;     // per structure: woken by a hit since the last read (st_activate)
+    uint32_t rebuilds = 0;           // bodies rebuilt so far (the lone-brick rule's draw key)
     uint32_t crush_n = 0;
 
     uint32_t gget(int x, int y, int z) const {
@@ -587,16 +596,24 @@ static bool detach_piece(World& w, const std::vector<uint32_t>& lst) {
     for (int k = 0; k < 4; k++) w.q.push_back(0.0f);
     for (int k = 0; k < 9; k++) { w.rot.push_back(0.0f); w.iil.push_back(0.0f); w.iiw.push_back(0.0f); }
     w.m.push_back(0.0f); w.im.push_back(0.0f); w.sleep.push_back(0.0f); w.rad.push_back(0.0f); w.maxr.push_back(0.0f);
-    w.island.push_back(NONE);
+    w.island.push_back(NONE); w.dirty.push_back(0);
     std::vector<uint32_t> nl;
+    const uint32_t k0 = w.ns + w.nd;
+    std::unordered_map<uint32_t, uint32_t> place;
+    for (uint32_t t = 0; t < n; t++) place[lst[t]] = k0 + t;
     for (uint32_t i : lst) {
         const uint32_t k = w.ns + w.nd++;
         w.mat.push_back(w.mat[i]); w.infill.push_back(0);
         w.bx.push_back(w.bx[i]); w.by.push_back(w.by[i]); w.bz.push_back(w.bz[i]); w.sid.push_back(-1);
         w.body.push_back(STATIC); w.next.push_back(NONE); w.sup.push_back(0);
         w.local.push_back(lat_pos(w.bx[i], w.by[i], w.bz[i])); w.wpos.push_back(vv(0, 0, 0));
-        for (int d = 0; d < 6; d++) w.nb6.push_back(NONE);
-        for (int a = 0; a < 4; a++) { w.bond.push_back(0.0f); w.bmax.push_back(0.0f); }
+        // the brick keeps its bonds (src/lib.rs:1118); its neighbours are renumbered to the piece's new ids
+        for (int d = 0; d < 6; d++) {
+            const uint32_t j = w.nb6[(size_t)i * 6 + d];
+            const auto it = j == NONE ? place.end() : place.find(j);
+            w.nb6.push_back(it == place.end() ? NONE : it->second);
+        }
+        for (int a = 0; a < 4; a++) { w.bond.push_back(w.bond[(size_t)i * 4 + a]); w.bmax.push_back(w.bmax[(size_t)i * 4 + a]); }
         w.phi.push_back(0.0f); w.ext.push_back(0.0f); w.stress.push_back(0.0f); w.phi64.push_back(0.0);
         w.hnext.push_back(NONE);
         nl.push_back(k);
@@ -644,6 +661,182 @@ static void conn_struct(World& w, int32_t s, uint32_t* counts) {
     }
     if (retry) { w.st_conn[s] = 1; counts[2]++; }
 }
+// finalize_brick's bond rule (src/lib.rs:668-696) between face-adjacent bricks of one body (glass is infill; no
+// foundation bond), for the bodies the scene describes
+static void body_bonds(World& w) {
+    for (uint32_t b = 0; b < w.nbody; b++) {
+        if (!w.alive[b]) continue;
+        std::vector<uint32_t> lst;
+        for (uint32_t k = w.first[b]; k != NONE; k = w.next[k]) lst.push_back(k);
+        for (uint32_t i : lst) {
+            for (int d = 0; d < 6; d++) {
+                uint32_t nj = NONE;
+                for (uint32_t j : lst)
+                    if (w.bx[j] == w.bx[i] + DIRS[d][0] && w.by[j] == w.by[i] + DIRS[d][1] && w.bz[j] == w.bz[i] + DIRS[d][2]) nj = j;
+                w.nb6[(size_t)i * 6 + d] = nj;
+            }
+            const uint8_t ii = w.mat[i] == GLASS ? 1 : 0;
+            for (int a = 0; a < 3; a++) {
+                const uint32_t j = w.nb6[(size_t)i * 6 + a * 2];
+                float c = 0.0f;
+                if (j != NONE) {
+                    const uint8_t ij = w.mat[j] == GLASS ? 1 : 0;
+                    const bool gap = ii != ij && (a != 1 || ii == 1);
+                    if (!gap && w.mat[j] != 0) c = bond_cap(w.mat[i], w.mat[j], a);
+                }
+                w.bond[(size_t)i * 4 + a] = c; w.bmax[(size_t)i * 4 + a] = c;
+            }
+            w.bond[(size_t)i * 4 + 3] = 0.0f; w.bmax[(size_t)i * 4 + 3] = 0.0f;
+        }
+    }
+}
+// remove_brick (src/lib.rs:705-718): a static brick leaves the grid and its structure is pending; a body brick's body
+// is marked for rebuild
+static void remove_brick(World& w, uint32_t i) {
+    if (w.mat[i] == 0) return;
+    if (w.body[i] == STATIC) {
+        if (w.gget(w.bx[i], w.by[i], w.bz[i]) == i + 1) w.gset(w.bx[i], w.by[i], w.bz[i], 0);
+        w.mat[i] = 0;
+        flag_conn(w, w.sid[i]);
+    } else {
+        w.mat[i] = 0;
+        w.dirty[w.body[i]] = 1;
+    }
+}
+// h01 (src/lib.rs:341-345)
+static float h01(uint32_t h, uint32_t k) {
+    uint32_t x = h + k * 0x9E3779B9u;
+    x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+    return (float)(x >> 8) / 16777216.0f;
+}
+// rebuild_body (src/lib.rs:930-1002) with the library's brick layout: a body's bricks are the ids [first, first +
+// count); the first component moves to the front of that range in list order, every other takes the next body id and
+// the next brick ids; ids left over are unowned. The lone-brick rule draws h01(bodies rebuilt so far, place in body)
+// and counts the bodies awake now (the reference: its random stream and the last frame's awake count).
+static void rebuild_body(World& w, uint32_t id, uint32_t* counts) {
+    const uint32_t first = w.first[id], cnt = w.count[id];
+    const uint32_t key = w.rebuilds++;
+    w.dirty[id] = 0;
+    counts[0]++;
+    std::vector<uint32_t> lst;
+    for (uint32_t t = 0; t < cnt; t++) {
+        if (w.mat[first + t] != 0) lst.push_back(t);
+        else { w.body[first + t] = STATIC; counts[2]++; }
+    }
+    if (lst.empty()) { w.alive[id] = 0; w.first[id] = NONE; w.count[id] = 0; counts[3]++; return; }
+    std::vector<int32_t> comp(cnt, -1);
+    uint32_t ncomp = 0;
+    for (uint32_t t0 : lst) {
+        if (comp[t0] >= 0) continue;
+        comp[t0] = (int32_t)ncomp;
+        std::vector<uint32_t> q{t0};
+        for (size_t h = 0; h < q.size(); h++) {
+            const uint32_t i = first + q[h];
+            for (int d = 0; d < 6; d++) {
+                uint32_t j; float hp;
+                if (!w.linked(i, d, j, hp)) continue;
+                const uint32_t tj = j - first;
+                if (comp[tj] >= 0) continue;
+                comp[tj] = (int32_t)ncomp;
+                q.push_back(tj);
+            }
+        }
+        ncomp++;
+    }
+    uint32_t nc = ncomp;
+    if (nc > 1) {
+        uint32_t extra = 0;
+        for (uint32_t t : lst) if (comp[t] > 0) extra++;
+        if (w.nbody + (nc - 1) > w.cap_bodies || w.nd + extra > w.cap_bricks) { for (uint32_t t : lst) comp[t] = 0; nc = 1; }
+    }
+    std::vector<std::vector<uint32_t>> groups(nc);
+    for (uint32_t t : lst) groups[comp[t]].push_back(t);
+    // the parent's pose and cached rotation (src/lib.rs:968)
+    const V ppos = w.pos[id], pv = w.v[id], pw = w.w[id];
+    float pq[4], prot[9];
+    for (int k = 0; k < 4; k++) pq[k] = w.q[(size_t)id * 4 + k];
+    for (int k = 0; k < 9; k++) prot[k] = w.rot[(size_t)id * 9 + k];
+    uint32_t awake = 0;
+    for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b] && !w.asleep[b]) awake++;
+    // copies of the kept bricks (the first component's moves overwrite ids it reads)
+    struct Rec { uint8_t mat, infill; int32_t x, y, z, sid; V local; uint32_t nb6[6]; float bond[4], bmax[4]; uint32_t sup; };
+    std::vector<Rec> rec(cnt);
+    for (uint32_t t = 0; t < cnt; t++) {
+        const uint32_t i = first + t;
+        Rec& r = rec[t];
+        r.mat = w.mat[i]; r.infill = w.infill[i]; r.x = w.bx[i]; r.y = w.by[i]; r.z = w.bz[i]; r.sid = w.sid[i];
+        r.local = w.local[i]; r.sup = w.sup[i];
+        for (int d = 0; d < 6; d++) r.nb6[d] = w.nb6[(size_t)i * 6 + d];
+        for (int a = 0; a < 4; a++) { r.bond[a] = w.bond[(size_t)i * 4 + a]; r.bmax[a] = w.bmax[(size_t)i * 4 + a]; }
+    }
+    for (uint32_t t = 0; t < cnt; t++) {   // the whole range is unowned until written again
+        const uint32_t i = first + t;
+        w.mat[i] = 0; w.body[i] = STATIC; w.next[i] = NONE;
+        for (int d = 0; d < 6; d++) w.nb6[(size_t)i * 6 + d] = NONE;
+    }
+    std::vector<uint32_t> nid(cnt, NONE);
+    std::vector<uint32_t> cbody(nc, NONE), cfirst(nc, 0);
+    for (uint32_t c = 0; c < nc; c++) {
+        const std::vector<uint32_t>& g = groups[c];
+        if (c > 0 && g.size() == 1 && awake > 1500) {
+            const float p = minf((float)(awake - 1500) / 2000.0f, 0.85f);
+            if (rec[g[0]].mat != STEEL && h01(key, g[0]) < p) { counts[4]++; continue; }
+        }
+        if (c == 0) { cbody[c] = id; cfirst[c] = first; }
+        else {
+            const uint32_t b = w.nbody++;
+            w.alive.push_back(0); w.asleep.push_back(0); w.wake.push_back(0);
+            w.first.push_back(NONE); w.count.push_back(0); w.nc.push_back(0);
+            w.pos.push_back(vv(0, 0, 0)); w.v.push_back(vv(0, 0, 0)); w.w.push_back(vv(0, 0, 0));
+            w.vpre.push_back(vv(0, 0, 0)); w.wpre.push_back(vv(0, 0, 0));
+            for (int k = 0; k < 4; k++) w.q.push_back(0.0f);
+            for (int k = 0; k < 9; k++) { w.rot.push_back(0.0f); w.iil.push_back(0.0f); w.iiw.push_back(0.0f); }
+            w.m.push_back(0.0f); w.im.push_back(0.0f); w.sleep.push_back(0.0f); w.rad.push_back(0.0f); w.maxr.push_back(0.0f);
+            w.island.push_back(NONE); w.dirty.push_back(0);
+            cbody[c] = b;
+            cfirst[c] = w.ns + w.nd;
+            for (size_t t = 0; t < g.size(); t++) {
+                w.nd++;
+                w.mat.push_back(0); w.infill.push_back(0); w.bx.push_back(0); w.by.push_back(0); w.bz.push_back(0);
+                w.sid.push_back(-1); w.body.push_back(STATIC); w.next.push_back(NONE); w.sup.push_back(0);
+                w.local.push_back(vv(0, 0, 0)); w.wpos.push_back(vv(0, 0, 0));
+                for (int d = 0; d < 6; d++) w.nb6.push_back(NONE);
+                for (int a = 0; a < 4; a++) { w.bond.push_back(0.0f); w.bmax.push_back(0.0f); }
+                w.phi.push_back(0.0f); w.ext.push_back(0.0f); w.stress.push_back(0.0f); w.phi64.push_back(0.0);
+                w.hnext.push_back(NONE);
+            }
+            counts[1]++;
+        }
+        for (size_t t = 0; t < g.size(); t++) nid[g[t]] = cfirst[c] + (uint32_t)t;
+    }
+    for (uint32_t c = 0; c < nc; c++) {
+        if (cbody[c] == NONE) continue;
+        const std::vector<uint32_t>& g = groups[c];
+        std::vector<uint32_t> ids;
+        for (size_t t = 0; t < g.size(); t++) {
+            const Rec& r = rec[g[t]];
+            const uint32_t i = cfirst[c] + (uint32_t)t;
+            w.mat[i] = r.mat; w.infill[i] = r.infill; w.bx[i] = r.x; w.by[i] = r.y; w.bz[i] = r.z; w.sid[i] = r.sid;
+            w.local[i] = r.local; w.sup[i] = r.sup;
+            for (int d = 0; d < 6; d++) {
+                const uint32_t j = r.nb6[d];
+                uint32_t nj = NONE;
+                if (j != NONE && j >= first && j < first + cnt && comp[j - first] == (int32_t)c) nj = nid[j - first];
+                w.nb6[(size_t)i * 6 + d] = nj;
+            }
+            for (int a = 0; a < 4; a++) { w.bond[(size_t)i * 4 + a] = r.bond[a]; w.bmax[(size_t)i * 4 + a] = r.bmax[a]; }
+            ids.push_back(i);
+        }
+        setup_body(w, cbody[c], ids.data(), (uint32_t)ids.size(), ppos, prot, pq, pv, pw);
+    }
+}
+// step's loop over marked bodies (src/lib.rs:3652). counts: bodies, pieces, removed bricks, dissolved, lone.
+static void rebuild_bodies(World& w, uint32_t* counts) {
+    for (int k = 0; k < 5; k++) counts[k] = 0;
+    for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b] && w.dirty[b]) rebuild_body(w, b, counts);
+    for (uint32_t b = 0; b < w.nbody; b++) w.dirty[b] = 0;
+}
+
 // st_now / st_top (src/lib.rs:1126-1128)
 static void struct_tally(const World& w, int32_t s, uint32_t& now, int32_t& top) {
     now = 0; top = 0;
@@ -946,6 +1139,121 @@ static void integrate(World& w, float h, int sleep_mode) {
         if (w.wake[b]) { w.wake[b] = 0; if (w.alive[b]) { w.asleep[b] = 0; w.sleep[b] = 0.0f; } }
     }
 }
+// ---------------------------------------------------------------- damage on contact (src/lib.rs:1602-1702)
+static void st_hit(World& w, int32_t s) { if (s >= 0 && s < (int32_t)w.st_hit.size()) w.st_hit[s] = 1; }
+static V bpos(const World& w, uint32_t i) { return w.body[i] == STATIC ? lat_pos(w.bx[i], w.by[i], w.bz[i]) : w.wpos[i]; }
+// damage_brick (src/lib.rs:724-745)
+static uint32_t damage_brick(World& w, uint32_t i, float frac, float absolute) {
+    uint32_t broke = 0;
+    for (int d = 0; d < 6; d++) {
+        const uint32_t j = w.nb6[(size_t)i * 6 + d];
+        if (j == NONE || w.mat[j] == 0) continue;
+        const uint32_t o = (d & 1) == 0 ? i : j;
+        const int a = d >> 1;
+        float& b = w.bond[(size_t)o * 4 + a];
+        if (b > 0.0f) {
+            b -= w.bmax[(size_t)o * 4 + a] * frac + absolute;
+            if (b <= w.bmax[(size_t)o * 4 + a] * 0.03f) { b = 0.0f; broke++; }
+        }
+    }
+    float& b3 = w.bond[(size_t)i * 4 + 3];
+    if (b3 > 0.0f) {
+        b3 -= w.bmax[(size_t)i * 4 + 3] * frac * 0.5f + absolute * 0.5f;
+        if (b3 <= 0.0f) { b3 = 0.0f; broke++; }
+    }
+    if (w.body[i] == STATIC) { st_hit(w, w.sid[i]); if (broke > 0) flag_conn(w, w.sid[i]); }
+    else if (broke > 0) w.dirty[w.body[i]] = 1;
+    return broke;
+}
+// sever_brick (src/lib.rs:746-752)
+static void sever_brick(World& w, uint32_t i) {
+    for (int a = 0; a < 4; a++) w.bond[(size_t)i * 4 + a] = 0.0f;
+    for (int d = 1; d < 6; d += 2) {
+        const uint32_t j = w.nb6[(size_t)i * 6 + d];
+        if (j != NONE) w.bond[(size_t)j * 4 + (d >> 1)] = 0.0f;
+    }
+}
+static float h01(uint32_t h, uint32_t k);
+// crush_at (src/lib.rs:1641-1702); the pulverisation draw is h01 of a fixed seed and the world's draw count
+static uint32_t crush_at(World& w, uint32_t start, float e, V p, uint32_t cap) {
+    const uint8_t m0 = w.mat[start];
+    if (m0 == 0 || m0 >= SLUG) return 0;
+    if (e < EB[m0] * 0.15f) return 0;
+    const uint32_t body = w.body[start];
+    const int32_t sid = w.sid[start];
+    if (w.stamp.size() < w.mat.size()) w.stamp.resize(w.mat.size(), 0);
+    const uint32_t st = ++w.stamp_id;
+    std::vector<uint32_t> q{start};
+    w.stamp[start] = st;
+    size_t head = 0;
+    uint32_t crushed = 0;
+    const uint32_t maxn = std::min(cap, 600u);
+    std::vector<uint32_t> lst;
+    while (head < q.size() && crushed < maxn) {
+        size_t best = head;
+        float bd = 1e18f;
+        const size_t lim = std::min(head + 24, q.size());
+        for (size_t t = head; t < lim; t++) { V d = sub(bpos(w, q[t]), p); float dd = dot(d, d); if (dd < bd) { bd = dd; best = t; } }
+        std::swap(q[head], q[best]);
+        const uint32_t i = q[head]; head++;
+        const uint8_t m = w.mat[i];
+        if (m == 0) continue;
+        const float cost = EB[m];
+        if (e < cost) { damage_brick(w, i, 0.6f * e / cost, 0.0f); w.dmg[4]++; break; }
+        e -= cost;
+        lst.push_back(i);
+        crushed++;
+        for (int d = 0; d < 6; d++) {
+            uint32_t j; float hp;
+            if (!w.linked(i, d, j, hp) || w.stamp[j] == st || w.body[j] != body || w.sid[j] != sid) continue;
+            w.stamp[j] = st;
+            q.push_back(j);
+        }
+    }
+    for (uint32_t i : lst) {
+        const uint8_t m = w.mat[i];
+        if (m == 0) continue;
+        if (h01(0x243F6A88u, w.dmg_draws++) < PULV[m]) {
+            if (w.body[i] == STATIC) st_hit(w, w.sid[i]);   // remove_brick's st_static_change (src/lib.rs:713)
+            remove_brick(w, i);
+            w.dmg[2]++;
+        }
+        else {
+            sever_brick(w, i);
+            w.dmg[3]++;
+            if (body == STATIC) { flag_conn(w, w.sid[i]); st_hit(w, w.sid[i]); }
+            else w.dirty[body] = 1;
+        }
+    }
+    w.dmg[1] += crushed;
+    return crushed;
+}
+// impact_damage (src/lib.rs:1610-1640), one budget of 2,500 crushed bricks per substep
+static void impact_damage(World& w) {
+    uint32_t budget = 2500;
+    for (const Contact& c : w.cs) {
+        const uint32_t ia = c.ba;
+        const uint8_t ma = w.mat[ia];
+        if (ma == 0 || ma >= SLUG) continue;
+        const bool crush = c.vn0 >= 1.0f && 0.5f * c.jn * c.vn0 >= 150.0f;
+        const bool heavy = c.bb != NONE && c.bo == STATIC && c.jn * c.vn0 > 4000.0f;
+        if (crush || heavy) w.dmg[0]++;
+        if (heavy) { const uint32_t j = c.bb; if (w.mat[j] != 0 && w.body[j] == STATIC) st_hit(w, w.sid[j]); }
+        if (w.mat[ia] == 0) continue;
+        if (c.vn0 < 1.0f) continue;
+        const float e = 0.5f * c.jn * c.vn0;
+        if (e < 150.0f) continue;
+        const uint32_t jb = c.bb;
+        const uint8_t mb = jb != NONE ? w.mat[jb] : 0;
+        const float soft_a = 1.0f / EB[ma];
+        const float soft_b = (jb == NONE || mb == 0 || mb >= SLUG) ? 0.0f : 1.0f / EB[mb];
+        if (soft_a + soft_b <= 0.0f) continue;
+        const float ea = e * soft_a / (soft_a + soft_b);
+        if (ea > 0.0f && budget > 0) budget -= std::min(crush_at(w, ia, ea, c.p, budget), budget);
+        if (soft_b > 0.0f && budget > 0) budget -= std::min(crush_at(w, jb, e - ea, c.p, budget), budget);
+    }
+}
+
 static void substep(World& w, float h, const StepParams& P) {
     update_cache(w);
     for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b] && !w.asleep[b]) w.v[b][1] -= GR * h;
@@ -959,6 +1267,7 @@ static void substep(World& w, float h, const StepParams& P) {
         if (P.order == ORDER_COLOR) solve_colored(w); else solve_list(w);
     }
     pinch_check(w, P.pinch_kill != 0);
+    if (P.damage) impact_damage(w);
     integrate(w, h, (int)P.sleep_mode);
 }
 static void step(World& w, float dt, const StepParams& P) {
@@ -1283,7 +1592,7 @@ static void hc_reduce4(HC& c) {
 // ============================================================================================================
 extern "C" {
 
-struct ow_step_params { uint32_t iterations, substeps, order, sleep_mode, pinch_kill, chunk; };
+struct ow_step_params { uint32_t iterations, substeps, order, sleep_mode, pinch_kill, chunk, damage; };
 
 void* ow_create(uint32_t n_static, const int32_t* static_xyz, const uint8_t* static_mat, const int32_t* static_sid,
                 const uint8_t* static_infill, uint32_t n_bodies, const uint32_t* body_first, const int32_t* body_brick_xyz,
@@ -1314,6 +1623,7 @@ void* ow_create(uint32_t n_static, const int32_t* static_xyz, const uint8_t* sta
     for (uint32_t i = 0; i < n_static; i++) nst = std::max(nst, w->sid[i] + 1);
     w->st_size.assign(nst, 0);
     w->st_conn.assign(nst, 0);
+    w->st_hit.assign(nst, 0);
     for (uint32_t i = 0; i < n_static; i++) if (w->sid[i] >= 0) w->st_size[w->sid[i]]++;
     w->cap_bodies = n_bodies; w->cap_bricks = nd;
     w->nbody = n_bodies;
@@ -1341,6 +1651,8 @@ void* ow_create(uint32_t n_static, const int32_t* static_xyz, const uint8_t* sta
         q_to_m(ps + 3, prot);
         setup_body(*w, b, lst.data(), (uint32_t)lst.size(), vv(ps[0], ps[1], ps[2]), prot, ps + 3, vv(ps[7], ps[8], ps[9]), vv(ps[10], ps[11], ps[12]));
     }
+    w->dirty.assign(nb, 0);
+    body_bonds(*w);
     return w;
 }
 void ow_destroy(void* h) { delete (World*)h; }
@@ -1402,7 +1714,7 @@ void ow_get_bonds(void* h, float* bond4, uint32_t* nb6) {
 }
 
 void ow_step(void* h, float dt, const ow_step_params* p) {
-    StepParams P{p->iterations, p->substeps, p->order, p->sleep_mode, p->pinch_kill};
+    StepParams P{p->iterations, p->substeps, p->order, p->sleep_mode, p->pinch_kill, p->damage};
     ((World*)h)->chunk = p->chunk;
     step(*(World*)h, dt, P);
 }
@@ -1484,6 +1796,30 @@ void ow_connectivity(void* h, uint32_t* counts, uint32_t* now, int32_t* top) {
     std::vector<int32_t> ids;
     for (size_t s = 0; s < w->st_conn.size(); s++) if (w->st_conn[s]) ids.push_back((int32_t)s);
     ow_connect(h, ids.data(), (uint32_t)ids.size(), counts, now, top);
+}
+void ow_remove_bricks(void* h, const uint32_t* statics, uint32_t ns_, const uint32_t* body_bricks, uint32_t nb_) {
+    World* w = (World*)h;
+    for (uint32_t k = 0; k < ns_; k++) if (statics[k] < w->ns) remove_brick(*w, statics[k]);
+    for (uint32_t k = 0; k < nb_; k++) if (body_bricks[k] < w->nd) remove_brick(*w, w->ns + body_bricks[k]);
+}
+void ow_rebuild_bodies(void* h, uint32_t* counts) { rebuild_bodies(*(World*)h, counts); }
+// damage counters since the last read (candidates, crushed, removed, severed, cracked) and per structure whether a hit
+// woke it; both cleared by the read
+void ow_read_damage(void* h, uint64_t* counts, uint8_t* hit) {
+    World* w = (World*)h;
+    for (int k = 0; k < 5; k++) { counts[k] = w->dmg[k]; w->dmg[k] = 0; }
+    for (size_t s = 0; s < w->st_hit.size(); s++) { if (hit) hit[s] = w->st_hit[s]; w->st_hit[s] = 0; }
+}
+void ow_body_bonds(void* h, float* bond4, uint32_t* nb6) {
+    World* w = (World*)h;
+    for (uint32_t k = 0; k < w->nd; k++) {
+        const uint32_t i = w->ns + k;
+        for (int a = 0; a < 4; a++) bond4[(size_t)k * 4 + a] = w->bond[(size_t)i * 4 + a];
+        for (int d = 0; d < 6; d++) {
+            const uint32_t j = w->nb6[(size_t)i * 6 + d];
+            nb6[(size_t)k * 6 + d] = j == NONE ? NONE : j - w->ns;
+        }
+    }
 }
 void ow_conn_pending(void* h, uint8_t* flags) { World* w = (World*)h; for (size_t s = 0; s < w->st_conn.size(); s++) flags[s] = w->st_conn[s]; }
 void ow_get_phi(void* h, float* phi) { World* w = (World*)h; for (uint32_t i = 0; i < w->ns; i++) phi[i] = w->phi[i]; }

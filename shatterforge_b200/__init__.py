@@ -55,7 +55,7 @@ class Params(C.Structure):
                 ("pinch_kill", C.c_uint32), ("max_colors", C.c_uint32), ("contact_capacity", C.c_uint32),
                 ("verify", C.c_uint32), ("solve_blocks", C.c_uint32), ("manifold_chunk", C.c_uint32),
                 ("sor_cluster", C.c_uint32), ("detach_bodies", C.c_uint32), ("detach_bricks", C.c_uint32),
-                ("reserved", C.c_uint32 * 4)]
+                ("damage", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 class Stats(C.Structure):
@@ -95,6 +95,16 @@ class FrameReport(C.Structure):
 class ConnectReport(C.Structure):
     _fields_ = [("structures", C.c_uint32), ("pieces", C.c_uint32), ("detached", C.c_uint32), ("retry", C.c_uint32),
                 ("listed", C.c_uint64), ("ms", C.c_double)]
+
+
+class RebuildReport(C.Structure):
+    _fields_ = [("bodies", C.c_uint32), ("pieces", C.c_uint32), ("removed", C.c_uint32), ("dissolved", C.c_uint32),
+                ("lone", C.c_uint32), ("reserved", C.c_uint32), ("ms", C.c_double)]
+
+
+class DamageReport(C.Structure):
+    _fields_ = [("contacts", C.c_uint64), ("crushed", C.c_uint64), ("removed", C.c_uint64), ("severed", C.c_uint64),
+                ("cracked", C.c_uint64)]
 
 
 class WorldInfo(C.Structure):
@@ -160,6 +170,10 @@ PROTOTYPES = {
     "sf_structure_connect": (C.c_int32, [C.c_void_p, _i32p, C.c_uint32, _u32p, _i32p, C.POINTER(ConnectReport)]),
     "sf_world_connectivity": (C.c_int32, [C.c_void_p, _u32p, _i32p, C.POINTER(ConnectReport)]),
     "sf_world_scene_ranges": (C.c_int32, [C.c_void_p, C.c_uint32, _u32p]),
+    "sf_world_remove_bricks": (C.c_int32, [C.c_void_p, _u32p, C.c_uint32, _u32p, C.c_uint32]),
+    "sf_world_rebuild_bodies": (C.c_int32, [C.c_void_p, C.POINTER(RebuildReport)]),
+    "sf_read_body_bonds": (C.c_int32, [C.c_void_p, _f32p, _u32p]),
+    "sf_read_damage": (C.c_int32, [C.c_void_p, C.POINTER(DamageReport), _u8p]),
     "sf_structure_loads": (C.c_int32, [C.c_void_p, _i32p, C.c_uint32]),
     "sf_world_get_info": (C.c_int32, [C.c_void_p, C.POINTER(WorldInfo)]),
     "sf_get_stats": (C.c_int32, [C.c_void_p, C.POINTER(Stats)]),
@@ -464,6 +478,34 @@ class World:
         _check(self._lib.sf_world_connectivity(self._h, _ptr(now, C.c_uint32), _ptr(top, C.c_int32), C.byref(r)),
                "sf_world_connectivity")
         return r, now, top
+
+    def remove_bricks(self, statics=(), body_bricks=()):
+        """remove_brick of world static ids and world body-brick ids (sf_world_remove_bricks)."""
+        a = np.ascontiguousarray(statics, np.uint32)
+        b = np.ascontiguousarray(body_bricks, np.uint32)
+        _check(self._lib.sf_world_remove_bricks(self._h, _ptr(a, C.c_uint32), len(a), _ptr(b, C.c_uint32), len(b)),
+               "sf_world_remove_bricks")
+
+    def rebuild_bodies(self) -> RebuildReport:
+        """rebuild_body of every body marked since the last call (sf_world_rebuild_bodies)."""
+        r = RebuildReport()
+        _check(self._lib.sf_world_rebuild_bodies(self._h, C.byref(r)), "sf_world_rebuild_bodies")
+        return r
+
+    def damage(self):
+        """Damage counters since the last read and per structure whether a hit woke it (sf_read_damage)."""
+        r = DamageReport()
+        h = np.zeros(max(self.info.n_structures, 1), np.uint8)
+        _check(self._lib.sf_read_damage(self._h, C.byref(r), _ptr(h, C.c_uint8)), "sf_read_damage")
+        return r, h[:self.info.n_structures]
+
+    def body_bonds(self):
+        """Per body brick: bonds (+x, +y, +z, foundation) and face neighbours (world body-brick ids)."""
+        nd = self.info.n_body_bricks
+        b = np.zeros((nd, 4), np.float32)
+        nb = np.zeros((nd, 6), np.uint32)
+        _check(self._lib.sf_read_body_bonds(self._h, _ptr(b, C.c_float), _ptr(nb, C.c_uint32)), "sf_read_body_bonds")
+        return b, nb
 
     def structure_check(self, structure: int = -1, dt: float = 1.0 / 60.0, live: bool = True) -> CheckReport:
         r = CheckReport()

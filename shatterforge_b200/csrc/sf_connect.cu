@@ -24,7 +24,8 @@
 
 namespace sf {
 
-constexpr int STAGE_WORDS = 10;   // per read-back brick: 6 neighbours, 3 bonds (+x, +y, +z, as bits), material
+// per read-back brick: 6 neighbours, 4 bonds and 4 capacities (as bits), material
+constexpr int STAGE_WORDS = 15;
 
 struct ConnState {
     DBuf<uint32_t> parent;       // per static brick: union-find parent, NONE = not in a requested structure
@@ -37,6 +38,7 @@ struct ConnState {
     DBuf<float> pose;            // 13 per new body: at the origin, identity rotation, at rest
     DBuf<uint32_t> newb;         // per scene: first and end of the bodies this call created
     DBuf<uint32_t> tally;        // per structure: bricks left, top cell + 1
+    DBuf<uint32_t> bslot, brec;  // new body bricks and their neighbours, bonds and capacities (14 words each)
     std::vector<int32_t> where;  // per static brick: its index in the host copy of the list, -1 = not listed
 };
 
@@ -96,8 +98,8 @@ __global__ void k_cc_collect(uint32_t ns, uint32_t *parent, const uint8_t *groun
     if (out) list[base + __popc(m & ((1u << lane) - 1u))] = i;
 }
 
-__global__ void k_cc_gather(uint32_t n, const uint32_t *list, const uint32_t *nb6, const float *bond, const uint8_t *mat,
-                            uint32_t *stage) {
+__global__ void k_cc_gather(uint32_t n, const uint32_t *list, const uint32_t *nb6, const float *bond, const float *bmax,
+                            const uint8_t *mat, uint32_t *stage) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const uint32_t i = list[k];
@@ -105,8 +107,28 @@ __global__ void k_cc_gather(uint32_t n, const uint32_t *list, const uint32_t *nb
 #pragma unroll
     for (int d = 0; d < 6; d++) o[d] = nb6[(size_t)i * 6 + d];
 #pragma unroll
-    for (int a = 0; a < 3; a++) o[6 + a] = __float_as_uint(bond[(size_t)i * 4 + a]);
-    o[9] = mat[i];
+    for (int a = 0; a < 4; a++) {
+        o[6 + a] = __float_as_uint(bond[(size_t)i * 4 + a]);
+        o[10 + a] = __float_as_uint(bmax[(size_t)i * 4 + a]);
+    }
+    o[14] = mat[i];
+}
+
+// a detached piece's bricks keep their bonds (src/lib.rs:1118 leaves them): the new body bricks get the static
+// bricks' bonds and capacities, and their neighbours renumbered to the piece's new body bricks
+__global__ void k_cc_bonds(uint32_t n, const uint32_t *slot, const uint32_t *rec, uint32_t *k_nb6, float *k_bond,
+                           float *k_bmax) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t k = slot[t];
+    const uint32_t *r = rec + (size_t)t * 14;
+#pragma unroll
+    for (int d = 0; d < 6; d++) k_nb6[(size_t)k * 6 + d] = r[d];
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        k_bond[(size_t)k * 4 + a] = __uint_as_float(r[6 + a]);
+        k_bmax[(size_t)k * 4 + a] = __uint_as_float(r[10 + a]);
+    }
 }
 
 // ---------------------------------------------------------------- detachment
@@ -226,7 +248,8 @@ static sf_status conn_impl(sf_world *w, const std::vector<int32_t> &ids, uint32_
     std::vector<uint32_t> list(n), stage((size_t)n * STAGE_WORDS);
     if (n) {
         SF_CUDA(C.stage.grow((size_t)n * STAGE_WORDS));
-        k_cc_gather<<<grid_for(n, 256), 256, 0, st>>>(n, C.list.p, w->s_nb6.p, w->s_bond.p, w->s_mat.p, C.stage.p);
+        k_cc_gather<<<grid_for(n, 256), 256, 0, st>>>(n, C.list.p, w->s_nb6.p, w->s_bond.p, w->s_bmax.p, w->s_mat.p,
+                                                      C.stage.p);
         w->launches++;
         SF_CUDA(cudaGetLastError());
         SF_CUDA(cudaMemcpyAsync(list.data(), C.list.p, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
@@ -251,12 +274,13 @@ static sf_status conn_impl(sf_world *w, const std::vector<int32_t> &ids, uint32_
     for (uint32_t q = 0; q < w->n_scenes; q++) { used_b0[q] = w->scenes[q].bodies_used; used_k0[q] = w->scenes[q].bricks_used; }
     std::vector<uint8_t> stamp(n, 0);
     std::vector<uint32_t> piece;
+    std::vector<uint32_t> newslot(n, NONE), bslot, brec;   // body-brick slot of each listed brick; bond records
     for (int32_t s : ids) {
         bool retry = false;
         for (uint32_t k = 0; k < n; k++) {
             const uint32_t seed = list[order[k]];
             const uint32_t *rs = rec(seed);
-            if (stamp[C.where[seed]] || w->h_sid[seed] != s || rs[9] >= SLUG) continue;
+            if (stamp[C.where[seed]] || w->h_sid[seed] != s || rs[14] >= SLUG) continue;
             piece.clear();
             stamp[C.where[seed]] = 1;
             piece.push_back(seed);
@@ -285,11 +309,23 @@ static sf_status conn_impl(sf_world *w, const std::vector<int32_t> &ids, uint32_
             pieces.push_back(Piece{q, body, first, cnt});
             sc_first[q].push_back(first);
             sc_count[q].push_back(cnt);
+            for (uint32_t t = 0; t < cnt; t++) newslot[C.where[piece[t]]] = first + t;
+            for (uint32_t t = 0; t < cnt; t++) {
+                const uint32_t *ri = rec(piece[t]);
+                bslot.push_back(first + t);
+                for (int d = 0; d < 6; d++) {
+                    const uint32_t j = ri[d];
+                    const bool same = j != NONE && C.where[j] >= 0 && newslot[C.where[j]] != NONE &&
+                                      newslot[C.where[j]] >= first && newslot[C.where[j]] < first + cnt;
+                    brec.push_back(same ? newslot[C.where[j]] : NONE);
+                }
+                for (int a = 0; a < 8; a++) brec.push_back(ri[6 + a]);
+            }
             for (uint32_t i : piece) {
                 int x, y, z;
                 unpack_cell(w->h_s_cell[i], x, y, z);
                 sc_xyz[q].push_back(x); sc_xyz[q].push_back(y); sc_xyz[q].push_back(z);
-                sc_mat[q].push_back((uint8_t)rec(i)[9]);
+                sc_mat[q].push_back((uint8_t)rec(i)[14]);
                 removed.push_back(i);
             }
             rep.detached += cnt;
@@ -329,6 +365,16 @@ static sf_status conn_impl(sf_world *w, const std::vector<int32_t> &ids, uint32_
             SF_CUDA(setup_bodies(w, b0, nbq, C.pose.p + pose_at * 13));
             SF_CUDA(step_reset_labels(w, b0, nbq));
             pose_at += nbq;
+        }
+        if (w->k_nb6.p) {
+            SF_CUDA(C.bslot.grow(bslot.size()));
+            SF_CUDA(C.brec.grow(brec.size()));
+            SF_CUDA(cudaMemcpyAsync(C.bslot.p, bslot.data(), bslot.size() * 4, cudaMemcpyHostToDevice, st));
+            SF_CUDA(cudaMemcpyAsync(C.brec.p, brec.data(), brec.size() * 4, cudaMemcpyHostToDevice, st));
+            k_cc_bonds<<<grid_for(bslot.size(), 256), 256, 0, st>>>((uint32_t)bslot.size(), C.bslot.p, C.brec.p,
+                                                                   w->k_nb6.p, w->k_bond.p, w->k_bmax.p);
+            w->launches++;
+            SF_CUDA(cudaGetLastError());
         }
         SF_CUDA(cudaMemcpyAsync(C.newb.p, newb.data(), newb.size() * 4, cudaMemcpyHostToDevice, st));
         k_cc_wake<<<grid_for(w->nb, 256), 256, 0, st>>>(w->nb, w->b_scene.p, C.newb.p, w->b_alive.p, w->b_asleep.p,

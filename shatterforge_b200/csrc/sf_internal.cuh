@@ -20,12 +20,14 @@ constexpr int NX = 640, NY = 136, NZ = 640, CXN = NX / 8, CYN = NY / 8, CZN = NZ
 constexpr uint32_t HSIZE = 32768;
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 constexpr uint32_t STATIC = 0xFFFFFFFFu;
-constexpr uint8_t GLASS = 4, SLUG = 6;
+constexpr uint8_t STEEL = 3, GLASS = 4, SLUG = 6;
 constexpr int MAXCOL = 128;
 
 struct MatTables {
     float mass[9], capv[9], caph[9], tens[9], stiff[9], duct[9];
     float gk[9];       // GROUNDK * STIFF[m], rounded once as the reference computes it
+    float eb[9];       // energy that crushes one brick (J), src/lib.rs:178
+    float pulv[9];     // share of crushed bricks ground to dust rather than broken loose, src/lib.rs:180
 };
 void host_mat_tables(MatTables &t);
 // each translation unit that reads the tables holds its own copy and uploads it at world creation
@@ -162,6 +164,8 @@ struct GridBarrier { unsigned count; unsigned gen; };
 struct StepState;    // sf_step.cu
 struct SorState;     // sf_sor.cu
 struct ConnState;    // sf_connect.cu
+struct SplitState;   // sf_split.cu
+struct DamageState;  // sf_damage.cu
 uint64_t sor_launches(const SorState *st);
 const Tuner *sor_tuner(const SorState *st);
 uint64_t sor_graph_launches(const SorState *st);
@@ -257,11 +261,20 @@ struct sf_world {
     sf::DBuf<uint32_t> err;      // [0] error bits, [1..] counters
     sf::DBuf<sf::GridBarrier> barrier;
 
+    // body bricks' bonds, in worlds with spare capacity (the ones whose bodies can split): per body brick its six face
+    // neighbours in the same body (body-brick ids, NONE = none), four bonds and their capacities as static bricks have;
+    // per body: a brick was removed or a bond broke since its last rebuild
+    sf::DBuf<uint32_t> k_nb6;
+    sf::DBuf<float> k_bond, k_bmax;
+    sf::DBuf<uint8_t> b_dirty;
+    uint64_t rebuilds = 0;               // rebuild_body calls so far (a draw counter of the lone-brick rule)
     // connectivity: per structure, set on the GPU when a joint pass fails a joint or crushes a brick (pending walk);
     // structures a full scene could not take are pending on the host
     sf::DBuf<uint8_t> st_conn;
     std::vector<uint8_t> h_conn_retry;
     sf::ConnState *conn = nullptr;
+    sf::SplitState *split = nullptr;
+    sf::DamageState *damage = nullptr;
 
     sf::SorState *sor = nullptr;
     sf::StepState *step = nullptr;
@@ -376,8 +389,24 @@ void step_set_live(sf_world *w, uint32_t scene, bool live);
 cudaError_t step_reset_labels(sf_world *w, uint32_t first_body, uint32_t n);
 sf_status read_error_word(sf_world *w);
 void conn_destroy(sf_world *w);
-// setup_body (src/lib.rs:844-891) of bodies base .. base + nb - 1 from their bricks and poses (sf_world.cu)
+void split_destroy(sf_world *w);
+void damage_destroy(sf_world *w);
+// the substep's contacts in list order, for impact damage (sf_damage.cu)
+struct DamageIn {
+    uint32_t nc;
+    const uint32_t *L_a, *L_b, *L_bo, *L_ba, *L_bb, *invperm;
+    const float4 *L_p, *S_j, *S_rb;
+    Work *wk;
+};
+cudaError_t damage_substep(sf_world *w, const DamageIn &in, cudaStream_t s);
+// setup_body (src/lib.rs:844-891) of bodies base .. base + nb - 1 from their bricks' lattice cells and poses
+// (sf_world.cu)
 cudaError_t setup_bodies(sf_world *w, uint32_t base, uint32_t nb, const float *d_pose13);
+// setup_body of the listed bodies from their bricks' current local offsets, about a parent pose given with its
+// cached rotation: pose22 = position 3, quaternion 4, velocity 3, spin 3, rotation 9 (rebuild_body, src/lib.rs:995)
+cudaError_t setup_bodies_from_local(sf_world *w, const uint32_t *d_list, uint32_t n, const float *d_pose22);
+// finalize_brick's bond rule (src/lib.rs:668-696) between face-adjacent bricks of each body (sf_world.cu)
+cudaError_t body_bonds(sf_world *w);
 
 // Union-find over a parent array whose entries only ever point to smaller indices: a walk ends within n hops and a
 // link attempt fails only when another thread linked the same root first. The bounds are far beyond both; only a

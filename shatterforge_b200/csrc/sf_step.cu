@@ -1065,6 +1065,7 @@ struct IntArgs {
     const uint32_t *list;
     float h;
     int pinch_kill, island_mode;
+    int phase;   // 0: pinch clamps then integration; 1: the pinch clamps only; 2: integration only
     uint8_t *alive, *asleep;
     float4 *pos, *q, *v, *w;
     const float4 *vpre, *wpre;
@@ -1088,7 +1089,7 @@ __global__ void k_integrate(IntArgs A) {
     V3 w = v3(t4.x, t4.y, t4.z);
     const float rad = A.rad[b];
     // pinch_check (src/lib.rs:1746-1768)
-    {
+    if (A.phase != 2) {
         float4 p4 = A.wpre[b];
         V3 wpre = v3(p4.x, p4.y, p4.z);
         p4 = A.vpre[b];
@@ -1105,6 +1106,11 @@ __global__ void k_integrate(IntArgs A) {
                 return;
             }
             v = madd(vpre, dv, div_rn(8.0f, m));
+        }
+        if (A.phase == 1) {
+            A.v[b] = make_float4(v.x, v.y, v.z, 0.0f);
+            A.w[b] = make_float4(w.x, w.y, w.z, 0.0f);
+            return;
         }
     }
     // clamp_vel (src/lib.rs:917-924)
@@ -1771,6 +1777,18 @@ static sf_status substep(sf_world *w, float h) {
     I.alive = w->b_alive.p; I.asleep = w->b_asleep.p; I.pos = w->b_pos.p; I.q = w->b_q.p; I.v = w->b_v.p; I.w = w->b_w.p;
     I.vpre = w->b_vpre.p; I.wpre = w->b_wpre.p; I.rad = w->b_rad.p; I.sleep = w->b_sleep.p; I.maxr = w->b_maxr.p;
     I.nc = w->b_nc.p; I.count = w->b_count.p; I.first = w->b_first.p; I.kmat = w->k_mat.p;
+    I.phase = 0;
+    if (w->P.damage && nc) {
+        // impact_damage runs between the pinch clamps and integration (src/lib.rs:1780-1782)
+        I.phase = 1;
+        k_integrate<<<grid_for(nb, 128), 128, 0, s>>>(I);
+        DamageIn D;
+        D.nc = nc; D.L_a = S->L_a.p; D.L_b = S->L_b.p; D.L_bo = S->L_bo.p; D.L_ba = S->L_ba.p; D.L_bb = S->L_bb.p;
+        D.invperm = S->invperm.p; D.L_p = S->L_p.p; D.S_j = S->S_j.p; D.S_rb = S->S_rb.p; D.wk = &S->wk;
+        SF_CUDA(damage_substep(w, D, s));
+        I.phase = 2;
+        L++;
+    }
     k_integrate<<<grid_for(nb, 128), 128, 0, s>>>(I);
     if (I.island_mode) {
         k_island_min<<<grid_for(nb, 256), 256, 0, s>>>(nb, blist, w->b_alive.p, S->label.p, w->b_sleep.p, S->mint.p);

@@ -14,7 +14,10 @@ void host_mat_tables(MatTables &t) {
     const float tens[9] = {0.0f, 0.35f, 0.1f, 0.9f, 0.5f, 0.7f, 1.0f, 1.0f, 1.0f};
     const float stiff[9] = {0.0f, 1.0f, 0.8f, 2.0f, 0.02f, 0.4f, 1.0f, 1.0f, 1.0f};
     const float duct[9] = {0.0f, 6.0f, 12.0f, 3.0f, 40.0f, 8.0f, 1.0f, 1.0f, 1.0f};
+    const float eb[9] = {0.0f, 15000.0f, 12000.0f, 1.5e6f, 300.0f, 6000.0f, 1e12f, 1e12f, 1e12f};
+    const float pulv[9] = {0.0f, 0.7f, 0.55f, 0.0f, 1.0f, 0.5f, 0.0f, 0.0f, 0.0f};
     for (int k = 0; k < 9; k++) {
+        t.eb[k] = eb[k]; t.pulv[k] = pulv[k];
         t.mass[k] = mass[k]; t.capv[k] = capv[k]; t.caph[k] = caph[k]; t.tens[k] = tens[k]; t.stiff[k] = stiff[k];
         t.duct[k] = duct[k];
         volatile float g = GROUNDK;   // keep the product a runtime f32 multiply

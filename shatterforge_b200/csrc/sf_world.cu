@@ -62,15 +62,24 @@ __global__ void k_finalize_bricks(uint32_t ns, uint32_t base, const uint32_t *ce
 }
 
 // one thread per body, its bricks in list order (the sums must round in the reference's order); bodies
-// base .. base + nb - 1, their poses at pose13[0 ..]
-__global__ void k_setup_bodies(uint32_t nb, uint32_t base, const uint32_t *first, const uint32_t *count, const int32_t *xyz,
-                               const uint8_t *kmat, const float *pose13, float4 *local, float4 *wpos, uint32_t *kbody,
+// base .. base + nb - 1 (or list[0 .. nb - 1]), their parent poses at pose[0 ..], `stride` floats each. Stride 13:
+// the bricks' positions are their lattice cells' centres and the rotation follows from the quaternion (a body set up
+// from a description or a detached piece). Stride 22: the positions are the bricks' current local offsets and the
+// rotation is given after the 13 (rebuild_body passes the parent's cached rotation, src/lib.rs:968, 995).
+__global__ void k_setup_bodies(uint32_t nb, uint32_t base, const uint32_t *list, const uint32_t *first,
+                               const uint32_t *count, const int32_t *xyz, const uint8_t *kmat, const float *pose,
+                               uint32_t stride, float4 *local, float4 *wpos, uint32_t *kbody,
                                float4 *pos, float4 *q, float4 *v, float4 *w, float *rot, float *iil, float *iiw,
                                float *m, float *im, float *rad, float *sleep, float *maxr, uint8_t *alive, uint8_t *asleep,
                                uint8_t *wake) {
     const uint32_t lb = blockIdx.x * blockDim.x + threadIdx.x;
     if (lb >= nb) return;
-    const uint32_t b = base + lb;
+    const uint32_t b = list ? list[lb] : base + lb;
+    const bool from_local = stride == 22;
+    auto brick_pos = [&](uint32_t i) -> V3 {
+        if (from_local) { const float4 l = local[i]; return v3(l.x, l.y, l.z); }
+        return lat_pos(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+    };
     uint32_t s = first[b], n = count[b];
     if (n == 0) {   // a spare body (capacity for detached pieces) or the sentinel: dead, at rest, finite
         pos[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f); q[b] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
@@ -87,7 +96,7 @@ __global__ void k_setup_bodies(uint32_t nb, uint32_t base, const uint32_t *first
     V3 cl = v3(0.0f, 0.0f, 0.0f);
     for (uint32_t t = 0; t < n; t++) {
         uint32_t i = s + t;
-        V3 l = lat_pos(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        V3 l = brick_pos(i);
         float mm = c_mat.mass[kmat[i]];
         mass += mm;
         cl = madd(cl, l, mm);
@@ -98,7 +107,7 @@ __global__ void k_setup_bodies(uint32_t nb, uint32_t base, const uint32_t *first
     const float cube = S * S / 6.0f;
     for (uint32_t t = 0; t < n; t++) {
         uint32_t i = s + t;
-        V3 l = lat_pos(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        V3 l = brick_pos(i);
         float mm = c_mat.mass[kmat[i]];
         V3 r = sub(l, cl);
         local[i] = make_float4(r.x, r.y, r.z, 0.0f);
@@ -126,9 +135,10 @@ __global__ void k_setup_bodies(uint32_t nb, uint32_t base, const uint32_t *first
             inv[6] = c2 * id; inv[7] = (a[1] * a[6] - a[0] * a[7]) * id; inv[8] = (a[0] * a[4] - a[1] * a[3]) * id;
         }
     }
-    const float *ps = pose13 + (size_t)lb * 13;
+    const float *ps = pose + (size_t)lb * stride;
     float prot[9];
-    q_to_m(ps[3], ps[4], ps[5], ps[6], prot);
+    if (from_local) for (int k = 0; k < 9; k++) prot[k] = ps[13 + k];
+    else q_to_m(ps[3], ps[4], ps[5], ps[6], prot);
     V3 off = mv(prot, cl);
     V3 p = add(v3(ps[0], ps[1], ps[2]), off);
     V3 pv = v3(ps[7], ps[8], ps[9]), pw = v3(ps[10], ps[11], ps[12]);
@@ -271,13 +281,76 @@ static cudaError_t upload(sf::DBuf<T> &d, const std::vector<T> &h, cudaStream_t 
 }
 
 namespace sf {
-cudaError_t setup_bodies(sf_world *w, uint32_t base, uint32_t nb, const float *d_pose13) {
+static cudaError_t setup_launch(sf_world *w, uint32_t base, const uint32_t *list, uint32_t nb, const float *pose,
+                                uint32_t stride) {
     if (nb == 0) return cudaSuccess;
-    k_setup_bodies<<<grid_for(nb, 128), 128, 0, w->stream>>>(nb, base, w->b_first.p, w->b_count.p, w->k_xyz.p, w->k_mat.p,
-                                                            d_pose13, w->k_local.p, w->k_wpos.p, w->k_body.p, w->b_pos.p,
-                                                            w->b_q.p, w->b_v.p, w->b_w.p, w->b_rot.p, w->b_iil.p,
-                                                            w->b_iiw.p, w->b_m.p, w->b_im.p, w->b_rad.p, w->b_sleep.p,
-                                                            w->b_maxr.p, w->b_alive.p, w->b_asleep.p, w->b_wake.p);
+    k_setup_bodies<<<grid_for(nb, 128), 128, 0, w->stream>>>(nb, base, list, w->b_first.p, w->b_count.p, w->k_xyz.p,
+                                                            w->k_mat.p, pose, stride, w->k_local.p, w->k_wpos.p,
+                                                            w->k_body.p, w->b_pos.p, w->b_q.p, w->b_v.p, w->b_w.p,
+                                                            w->b_rot.p, w->b_iil.p, w->b_iiw.p, w->b_m.p, w->b_im.p,
+                                                            w->b_rad.p, w->b_sleep.p, w->b_maxr.p, w->b_alive.p,
+                                                            w->b_asleep.p, w->b_wake.p);
+    w->launches++;
+    return cudaGetLastError();
+}
+cudaError_t setup_bodies(sf_world *w, uint32_t base, uint32_t nb, const float *d_pose13) {
+    return setup_launch(w, base, nullptr, nb, d_pose13, 13u);
+}
+cudaError_t setup_bodies_from_local(sf_world *w, const uint32_t *d_list, uint32_t n, const float *d_pose22) {
+    return setup_launch(w, 0u, d_list, n, d_pose22, 22u);
+}
+
+// finalize_brick (src/lib.rs:668-696) between the bricks of one body: a face neighbour is a brick of the same body one
+// lattice cell away; the bond of each +x / +y / +z pair is the weaker brick's capacity on that axis unless an infill
+// gap separates them (glass is infill); bodies have no foundation bond. One thread per brick, scanning its body.
+__global__ void k_body_bonds(uint32_t nd, const uint32_t *kbody, const uint8_t *alive, const uint32_t *first,
+                             const uint32_t *count, const int32_t *xyz, const uint8_t *kmat, uint32_t *nb6, float *bond,
+                             float *bmax) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nd) return;
+    uint32_t nb[6] = {NONE, NONE, NONE, NONE, NONE, NONE};
+    const uint32_t b = kbody[i];
+    const uint8_t mi = kmat[i];
+    if (alive[b] && mi) {
+        const int x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+        const uint32_t f = first[b], n = count[b];
+        for (uint32_t t = 0; t < n; t++) {
+            const uint32_t j = f + t;
+            const int dx = xyz[3 * j] - x, dy = xyz[3 * j + 1] - y, dz = xyz[3 * j + 2] - z;
+            const int ad = abs(dx) + abs(dy) + abs(dz);
+            if (ad != 1) continue;
+            const int d = dx ? (dx > 0 ? 0 : 1) : dy ? (dy > 0 ? 2 : 3) : (dz > 0 ? 4 : 5);
+            nb[d] = j;
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 6; d++) nb6[(size_t)i * 6 + d] = nb[d];
+    const uint8_t inf_i = mi == GLASS ? 1 : 0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const uint32_t j = nb[2 * a];
+        float c = 0.0f;
+        if (j != NONE && mi) {
+            const uint8_t mj = kmat[j];
+            const uint8_t inf_j = mj == GLASS ? 1 : 0;
+            const bool gap = inf_i != inf_j && (a != 1 || inf_i == 1);
+            if (!gap && mj != 0) {
+                const float ca = a == 1 ? c_mat.capv[mi] : c_mat.caph[mi];
+                const float cb = a == 1 ? c_mat.capv[mj] : c_mat.caph[mj];
+                c = minf(ca, cb);
+            }
+        }
+        bond[(size_t)i * 4 + a] = c;
+        bmax[(size_t)i * 4 + a] = c;
+    }
+    bond[(size_t)i * 4 + 3] = 0.0f;
+    bmax[(size_t)i * 4 + 3] = 0.0f;
+}
+cudaError_t body_bonds(sf_world *w) {
+    if (w->nd == 0) return cudaSuccess;
+    k_body_bonds<<<grid_for(w->nd, 256), 256, 0, w->stream>>>(w->nd, w->k_body.p, w->b_alive.p, w->b_first.p,
+                                                             w->b_count.p, w->k_xyz.p, w->k_mat.p, w->k_nb6.p,
+                                                             w->k_bond.p, w->k_bmax.p);
     w->launches++;
     return cudaGetLastError();
 }
@@ -349,6 +422,7 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
     }
     // spare capacity for detached pieces: unused bricks belong to an always-dead sentinel body after the scenes'
     const bool spare = w->P.detach_bodies || w->P.detach_bricks;
+    if (w->P.damage && !spare) { set_error("damage needs spare capacity (detach_bodies, detach_bricks)"); return SF_ERR_ARG; }
     if (spare) nb += 1;
     if (ns >= 0x7fffffffu || nd >= 0x7fffffffu || nb >= 0x7fffffffu) { set_error("world too large"); return SF_ERR_CAPACITY; }
     w->ns = (uint32_t)ns; w->nd = (uint32_t)nd; w->nb = (uint32_t)nb;
@@ -471,8 +545,8 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
         SF_CUDA(cudaMemsetAsync(w->k_wpos.p, 0, w->k_wpos.bytes(), st));
     }
     if (nb) {
-        k_setup_bodies<<<grid_for(nb, 128), 128, 0, st>>>((uint32_t)nb, 0u, w->b_first.p, w->b_count.p, w->k_xyz.p, w->k_mat.p,
-                                                        d_pose.p, w->k_local.p, w->k_wpos.p, w->k_body.p, w->b_pos.p,
+        k_setup_bodies<<<grid_for(nb, 128), 128, 0, st>>>((uint32_t)nb, 0u, nullptr, w->b_first.p, w->b_count.p, w->k_xyz.p,
+                                                        w->k_mat.p, d_pose.p, 13u, w->k_local.p, w->k_wpos.p, w->k_body.p, w->b_pos.p,
                                                         w->b_q.p, w->b_v.p, w->b_w.p, w->b_rot.p, w->b_iil.p, w->b_iiw.p,
                                                         w->b_m.p, w->b_im.p, w->b_rad.p, w->b_sleep.p, w->b_maxr.p,
                                                         w->b_alive.p, w->b_asleep.p, w->b_wake.p);
@@ -482,6 +556,14 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
     SF_CUDA(cudaMemsetAsync(w->err.p, 0, w->err.bytes(), st));
     SF_CUDA(w->barrier.alloc(4));
     SF_CUDA(cudaMemsetAsync(w->barrier.p, 0, w->barrier.bytes(), st));
+    if (spare) {
+        SF_CUDA(w->k_nb6.alloc((size_t)std::max<uint64_t>(nd, 1) * 6));
+        SF_CUDA(w->k_bond.alloc((size_t)std::max<uint64_t>(nd, 1) * 4));
+        SF_CUDA(w->k_bmax.alloc((size_t)std::max<uint64_t>(nd, 1) * 4));
+        SF_CUDA(w->b_dirty.alloc(nb));
+        SF_CUDA(cudaMemsetAsync(w->b_dirty.p, 0, w->b_dirty.bytes(), st));
+        SF_CUDA(body_bonds(w.get()));
+    }
     SF_CUDA(w->st_conn.alloc(std::max<uint32_t>(w->n_struct, 1)));
     SF_CUDA(cudaMemsetAsync(w->st_conn.p, 0, w->st_conn.bytes(), st));
     w->h_conn_retry.assign(w->n_struct, 0);
@@ -500,6 +582,8 @@ void sf_world_destroy(sf_world *w) {
     sor_destroy(w);
     step_destroy(w);
     conn_destroy(w);
+    split_destroy(w);
+    damage_destroy(w);
     if (w->ev0) cudaEventDestroy(w->ev0);
     if (w->ev1) cudaEventDestroy(w->ev1);
     cudaStream_t s = w->own_stream;
@@ -862,8 +946,9 @@ sf_status sf_pool_load(sf_world *w, uint32_t slot, const sf_scene_desc *d) {
                                                                       w->s_sid.p, w->ctab.p, w->cpool.p, w->s_nb6.p,
                                                                       w->s_bond.p, w->s_bmax.p);
     if (d->n_bodies)
-        k_setup_bodies<<<grid_for(d->n_bodies, 128), 128, 0, st>>>(d->n_bodies, sc.body_off, w->b_first.p, w->b_count.p,
-                                                                 w->k_xyz.p, w->k_mat.p, d_pose.p, w->k_local.p,
+        k_setup_bodies<<<grid_for(d->n_bodies, 128), 128, 0, st>>>(d->n_bodies, sc.body_off, nullptr, w->b_first.p,
+                                                                 w->b_count.p, w->k_xyz.p, w->k_mat.p, d_pose.p, 13u,
+                                                                 w->k_local.p,
                                                                  w->k_wpos.p, w->k_body.p, w->b_pos.p, w->b_q.p, w->b_v.p,
                                                                  w->b_w.p, w->b_rot.p, w->b_iil.p, w->b_iiw.p, w->b_m.p,
                                                                  w->b_im.p, w->b_rad.p, w->b_sleep.p, w->b_maxr.p,
