@@ -109,6 +109,8 @@ def load() -> C.CDLL:
     lib.ow_rebuild_bodies.argtypes = [C.c_void_p, _u32p]
     lib.ow_body_bonds.argtypes = [C.c_void_p, _f32p, _u32p]
     lib.ow_read_damage.argtypes = [C.c_void_p, _u64p, _u8p]
+    lib.ow_crush_at.restype = C.c_uint32
+    lib.ow_crush_at.argtypes = [C.c_void_p, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_uint32]
     lib.ow_collide_hulls.restype = C.c_int32
     lib.ow_collide_hulls.argtypes = [_f32p, _f32p, _f32p, C.c_float, C.c_int32, _f32p]
     lib.ow_ref_colouring.argtypes = [C.c_uint32, _u32p, _u32p, _u32p, _u8p, _u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
@@ -320,6 +322,10 @@ class OracleWorld:
         nb = np.zeros((nd, 6), np.uint32)
         self.lib.ow_body_bonds(self.h, _p(b, C.c_float), _p(nb, C.c_uint32))
         return b, nb
+
+    def crush_at(self, start, e, p, cap=2500):
+        """crush_at on brick `start` (static id, or n_static + body-brick id); returns the bricks crushed."""
+        return int(self.lib.ow_crush_at(self.h, int(start), float(e), float(p[0]), float(p[1]), float(p[2]), int(cap)))
 
     def read_damage(self):
         """(candidates, crushed, removed, severed, cracked) since the last read, and per structure the hit flags."""

@@ -1803,6 +1803,12 @@ void ow_remove_bricks(void* h, const uint32_t* statics, uint32_t ns_, const uint
     for (uint32_t k = 0; k < nb_; k++) if (body_bricks[k] < w->nd) remove_brick(*w, w->ns + body_bricks[k]);
 }
 void ow_rebuild_bodies(void* h, uint32_t* counts) { rebuild_bodies(*(World*)h, counts); }
+// crush_at on one brick (a static id, or ns + a body-brick id) with energy e at point p; returns the bricks crushed
+uint32_t ow_crush_at(void* h, uint32_t start, float e, float px, float py, float pz, uint32_t cap) {
+    World* w = (World*)h;
+    if (start >= w->mat.size()) return 0;
+    return crush_at(*w, start, e, vv(px, py, pz), cap);
+}
 // damage counters since the last read (candidates, crushed, removed, severed, cracked) and per structure whether a hit
 // woke it; both cleared by the read
 void ow_read_damage(void* h, uint64_t* counts, uint8_t* hit) {
