@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--no-sor", action="store_true")
     ap.add_argument("--sor-max-sweeps", type=int, default=200000, help="sweep limit of the timed load-path solve")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-collapse", action="store_true")
+    ap.add_argument("--collapse-frames", type=int, default=240, help="frames of the collapse run (frame order, damage on)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-serve", action="store_true")
@@ -512,6 +514,67 @@ def plain_compare(sf, scenes, params, stream, args):
     return out
 
 
+def collapse_section(sf, S, args, stream):
+    """The 5-storey frame with two ground columns removed and 1,024 bricks of debris, run frame by frame in the
+    reference's order (substeps with damage on contact, rebuild of the marked bodies, connectivity, the resting loads
+    and the load-path frame, connectivity again; src/lib.rs:3650-3659): wall time per frame with its parts, and the
+    oracle running the same frames in the reference's list order on one host thread."""
+    import torch
+    sc = S.frame5_debris_scene(seed=1, n_debris=1024, removed=True)
+    ids = sc.structure_ids()
+    frames = args.collapse_frames
+    w = sf.World(sc, iterations=ITERS, detach_bodies=4000, detach_bricks=20000, damage=1)
+    w.set_stream(stream.cuda_stream)
+    for s in ids:
+        w.structure_warm(s)
+    parts = {"step": 0.0, "rebuild": 0.0, "connectivity": 0.0, "load_path": 0.0}
+    tally = {"crushed": 0, "pieces_split": 0, "pieces_detached": 0, "joints_failed": 0}
+    torch.cuda.synchronize()
+    t_all = time.perf_counter()
+    for f in range(1, frames + 1):
+        t = time.perf_counter(); w.step(DT); torch.cuda.synchronize(); parts["step"] += time.perf_counter() - t
+        t = time.perf_counter(); rb = w.rebuild_bodies(); parts["rebuild"] += time.perf_counter() - t
+        t = time.perf_counter(); c1, _, _ = w.connectivity(); parts["connectivity"] += time.perf_counter() - t
+        t = time.perf_counter()
+        w.structure_loads(ids)
+        fr = w.structure_frame(f, ids, dt=DT)
+        parts["load_path"] += time.perf_counter() - t
+        t = time.perf_counter(); c2, _, _ = w.connectivity(); parts["connectivity"] += time.perf_counter() - t
+        tally["pieces_split"] += rb.pieces
+        tally["pieces_detached"] += c1.pieces + c2.pieces
+        tally["joints_failed"] += int(fr.failed)
+        tally["crushed"] += int(w.damage()[0].crushed)
+    wall = time.perf_counter() - t_all
+    st = w.stats()
+    out = {"workload": f"5-storey frame (2 ground columns removed) + 1,024 debris bricks, {frames} frames, damage on",
+           "ms_per_frame": wall * 1e3 / frames, "parts_ms_per_frame": {k: v * 1e3 / frames for k, v in parts.items()},
+           "bodies_alive_at_end": int(st.alive), **tally}
+    w.close()
+    if not args.no_cpu:
+        from oracle import binding as orc
+        orc.use_native()
+        ow = orc.OracleWorld(sc)
+        ow.set_capacity(4000, 20000)
+        for s in ids:
+            ow.structure_warm(s)
+        t0 = time.perf_counter()
+        n = 0
+        for f in range(1, frames + 1):
+            ow.step(DT, iterations=ITERS, order=orc.ORDER_LIST, damage=1)
+            ow.rebuild_bodies()
+            ow.connectivity()
+            ow.structure_loads(ids)
+            ow.structure_frame(f, DT, ids)
+            ow.connectivity()
+            n = f
+            if time.perf_counter() - t0 > args.cpu_seconds:
+                break
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = {"ms_per_frame": cpu_s * 1e3 / n, "frames": n, "cores": 1, "kind": "port",
+                               "order": "reference list order"}
+    return out
+
+
 def our_arm(args, rank, world, local, pg):
     import torch
 
@@ -662,6 +725,10 @@ def our_arm(args, rank, world, local, pg):
                "roofline": roof}
         ws.close()
 
+    collapse = None
+    if not args.no_collapse and rank == 0:
+        collapse = collapse_section(sf, S, args, stream)
+
     # ---- CPU baseline: the oracle on a bounded sample of the same workload and step window
     cpu = None
     serve = None
@@ -712,6 +779,7 @@ def our_arm(args, rank, world, local, pg):
                       "awake": int(stats.awake)},
         "plain": plain,
         "sor": sor,
+        "collapse": collapse,
         "cpu_baseline": cpu,
         "serve": serve,
     }
