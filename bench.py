@@ -72,7 +72,8 @@ def parse():
     ap.add_argument("--sor-max-sweeps", type=int, default=200000, help="sweep limit of the timed load-path solve")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-collapse", action="store_true")
-    ap.add_argument("--collapse-frames", type=int, default=240, help="frames of the collapse run (frame order, damage on)")
+    ap.add_argument("--no-sat", action="store_true")
+    ap.add_argument("--collapse-frames", type=int, default=600, help="frames of the collapse run (frame order, damage on)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-serve", action="store_true")
@@ -515,15 +516,16 @@ def plain_compare(sf, scenes, params, stream, args):
 
 
 def collapse_section(sf, S, args, stream):
-    """The 5-storey frame with two ground columns removed and 1,024 bricks of debris, run frame by frame in the
-    reference's order (substeps with damage on contact, rebuild of the marked bodies, connectivity, the resting loads
-    and the load-path frame, connectivity again; src/lib.rs:3650-3659): wall time per frame with its parts, and the
-    oracle running the same frames in the reference's list order on one host thread."""
+    """The 16-storey tower (47,760 bricks) with eight ground columns removed, run frame by frame in the reference's
+    order (substeps with damage on contact, rebuild of the marked bodies, connectivity, the resting loads and the
+    load-path frame, connectivity again; src/lib.rs:3650-3659): wall time per frame with its parts, and the oracle
+    running the same frames in the reference's list order on one host thread."""
     import torch
-    sc = S.frame5_debris_scene(seed=1, n_debris=1024, removed=True)
+    tw, rm = S.tower16_structure()
+    sc = tw.without_static(rm)
     ids = sc.structure_ids()
     frames = args.collapse_frames
-    w = sf.World(sc, iterations=ITERS, detach_bodies=4000, detach_bricks=20000, damage=1)
+    w = sf.World(sc, iterations=ITERS, detach_bodies=8000, detach_bricks=60000, damage=1, max_colors=1024)
     w.set_stream(stream.cuda_stream)
     for s in ids:
         w.structure_warm(s)
@@ -531,7 +533,9 @@ def collapse_section(sf, S, args, stream):
     tally = {"crushed": 0, "pieces_split": 0, "pieces_detached": 0, "joints_failed": 0}
     torch.cuda.synchronize()
     t_all = time.perf_counter()
+    ft = []
     for f in range(1, frames + 1):
+        tf = time.perf_counter()
         t = time.perf_counter(); w.step(DT); torch.cuda.synchronize(); parts["step"] += time.perf_counter() - t
         t = time.perf_counter(); rb = w.rebuild_bodies(); parts["rebuild"] += time.perf_counter() - t
         t = time.perf_counter(); c1, _, _ = w.connectivity(); parts["connectivity"] += time.perf_counter() - t
@@ -544,9 +548,10 @@ def collapse_section(sf, S, args, stream):
         tally["pieces_detached"] += c1.pieces + c2.pieces
         tally["joints_failed"] += int(fr.failed)
         tally["crushed"] += int(w.damage()[0].crushed)
+        ft.append(time.perf_counter() - tf)
     wall = time.perf_counter() - t_all
     st = w.stats()
-    out = {"workload": f"5-storey frame (2 ground columns removed) + 1,024 debris bricks, {frames} frames, damage on",
+    out = {"workload": f"16-storey tower, 47,760 bricks, 8 ground columns removed, {frames} frames, damage on",
            "ms_per_frame": wall * 1e3 / frames, "parts_ms_per_frame": {k: v * 1e3 / frames for k, v in parts.items()},
            "bodies_alive_at_end": int(st.alive), **tally}
     w.close()
@@ -554,7 +559,7 @@ def collapse_section(sf, S, args, stream):
         from oracle import binding as orc
         orc.use_native()
         ow = orc.OracleWorld(sc)
-        ow.set_capacity(4000, 20000)
+        ow.set_capacity(8000, 60000)
         for s in ids:
             ow.structure_warm(s)
         t0 = time.perf_counter()
@@ -570,8 +575,60 @@ def collapse_section(sf, S, args, stream):
             if time.perf_counter() - t0 > args.cpu_seconds:
                 break
         cpu_s = time.perf_counter() - t0
-        out["cpu_baseline"] = {"ms_per_frame": cpu_s * 1e3 / n, "frames": n, "cores": 1, "kind": "port",
-                               "order": "reference list order"}
+        out["cpu_baseline"] = {"ms_per_frame": cpu_s * 1e3 / n, "frames": f"1..{n}", "cores": 1, "kind": "port",
+                               "order": "reference list order",
+                               "gpu_ms_per_frame_same_frames": sum(ft[:n]) * 1e3 / n}
+    return out
+
+
+def sat_section(sf, args):
+    """The batched narrow-phase calls: box-box SAT (engine/src/phys.rs:502-628) on 1M random overlapping pairs and
+    convex-cell SAT (gpu/gpu_world.js:421-530) on 200k pairs of the hull library, timed through the C ABI with host
+    arrays (device allocation, copies both ways and the kernel inside the timed call), best of three; the oracle's
+    restatement on one host thread on a sample of the same pairs."""
+    from shatterforge_b200 import hulls
+    rng = np.random.default_rng(7)
+
+    def quats(n):
+        q = rng.normal(size=(n, 4))
+        return q / np.linalg.norm(q, axis=1, keepdims=True)
+
+    nb = 1 << 20
+    ba = np.zeros((nb, 10), np.float32); bb = np.zeros((nb, 10), np.float32)
+    for x in (ba, bb):
+        x[:, :3] = rng.uniform(-0.6, 0.6, (nb, 3)); x[:, 3:7] = quats(nb); x[:, 7:] = rng.uniform(0.1, 0.6, (nb, 3))
+    data = hulls.library().packed()
+    nh = 200000
+    ha = np.zeros((nh, 11), np.float32); hb = np.zeros((nh, 11), np.float32)
+    for x in (ha, hb):
+        x[:, :3] = rng.uniform(-0.45, 0.45, (nh, 3)); x[:, 3:7] = quats(nh); x[:, 7:10] = rng.uniform(0.15, 0.5, (nh, 3))
+        x[:, 10] = rng.integers(0, len(data), nh)
+
+    def best(f):
+        t = []
+        for _ in range(3):
+            t0 = time.perf_counter(); r = f(); t.append(time.perf_counter() - t0)
+        return min(t), r
+    tb, (cb, _, _) = best(lambda: sf.collide_boxes(ba, bb, margin=0.02))
+    th, (ch, _, _) = best(lambda: sf.collide_hulls(data, ha, hb, margin=0.02))
+    out = {"boxes": {"pairs": nb, "pairs_per_s": nb / tb, "ms": tb * 1e3, "touching": int((cb > 0).sum()),
+                     "bytes_per_pair": 10 * 4 * 2 + 20 * 4 + 4},
+           "hulls": {"pairs": nh, "pairs_per_s": nh / th, "ms": th * 1e3, "touching": int((ch > 0).sum()),
+                     "bytes_per_pair": 11 * 4 * 2 + 36 * 4 + 4},
+           "note": "end to end through the C ABI with host arrays: allocation, host-device copies and the kernel"}
+    if not args.no_cpu:
+        from oracle import binding as orc
+        orc.use_native()
+        ns, nsh = 200000, 50000
+        t0 = time.perf_counter()
+        hits_b = orc.collide_batch_hits(ba[:ns], bb[:ns])
+        tcb = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        hits_h = orc.collide_batch_hits(ha[:nsh], hb[:nsh], hull_data=data)
+        tch = time.perf_counter() - t0
+        out["cpu_baseline"] = {"boxes_pairs_per_s": ns / tcb, "hulls_pairs_per_s": nsh / tch, "cores": 1,
+                               "kind": "port", "sample": f"the first {ns} box pairs and {nsh} hull pairs in one call "
+                               f"each ({hits_b} and {hits_h} touching)"}
     return out
 
 
@@ -728,6 +785,9 @@ def our_arm(args, rank, world, local, pg):
     collapse = None
     if not args.no_collapse and rank == 0:
         collapse = collapse_section(sf, S, args, stream)
+    sat = None
+    if not args.no_sat and rank == 0:
+        sat = sat_section(sf, args)
 
     # ---- CPU baseline: the oracle on a bounded sample of the same workload and step window
     cpu = None
@@ -780,6 +840,7 @@ def our_arm(args, rank, world, local, pg):
         "plain": plain,
         "sor": sor,
         "collapse": collapse,
+        "sat": sat,
         "cpu_baseline": cpu,
         "serve": serve,
     }

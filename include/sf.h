@@ -73,7 +73,8 @@ typedef struct sf_params {
     uint32_t iterations;        /* impulse iterations per substep (reference: 10, src/lib.rs:1779) */
     uint32_t sleep_mode;        /* SF_SLEEP_BODY or SF_SLEEP_ISLAND */
     uint32_t pinch_kill;        /* 1: small pinched bodies are removed as the reference does (src/lib.rs:1755) */
-    uint32_t max_colors;        /* manifold colour limit, <= 128 */
+    uint32_t max_colors;        /* manifold colour limit, <= 1024 (default 128): a body with thousands of contacts,
+                                   whose chunks all conflict, needs more */
     uint32_t contact_capacity;  /* 0 = automatic (grows between steps) */
     uint32_t verify;            /* 1: check the colouring is proper every substep (SF_ERR_VERIFY on failure) */
     uint32_t solve_blocks;      /* persistent-kernel blocks per SM for the solve (0 = autotuned) */

@@ -115,6 +115,10 @@ def load() -> C.CDLL:
     lib.ow_collide_hulls.argtypes = [_f32p, _f32p, _f32p, C.c_float, C.c_int32, _f32p]
     lib.ow_ref_colouring.argtypes = [C.c_uint32, _u32p, _u32p, _u32p, _u8p, _u8p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                      _u32p, _u32p]
+    lib.ow_collide_boxes_batch.restype = C.c_uint64
+    lib.ow_collide_boxes_batch.argtypes = [_f32p, _f32p, C.c_uint32, C.c_float, C.c_int32]
+    lib.ow_collide_hulls_batch.restype = C.c_uint64
+    lib.ow_collide_hulls_batch.argtypes = [_f32p, _f32p, _f32p, C.c_uint32, C.c_float, C.c_int32]
     lib.ow_collide_boxes.restype = C.c_int32
     lib.ow_collide_boxes.argtypes = [_f32p, _f32p, C.c_float, C.c_int32, _f32p]
     _lib = lib
@@ -357,6 +361,17 @@ def collide_boxes(a, b, margin=0.02, reduce=True):
     a = np.ascontiguousarray(a, np.float32); b = np.ascontiguousarray(b, np.float32)
     n = lib.ow_collide_boxes(_p(a, C.c_float), _p(b, C.c_float), float(margin), 1 if reduce else 0, _p(out, C.c_float))
     return n, out[:3].copy(), out[3:3 + 4 * n].reshape(n, 4).copy()
+
+
+def collide_batch_hits(a, b, hull_data=None, margin=0.02):
+    """Box pairs (hull_data None) or hull pairs, all in one call of the restatement; returns the touching count."""
+    lib = load()
+    if hull_data is None:
+        a = np.ascontiguousarray(a, np.float32).reshape(-1, 10); b = np.ascontiguousarray(b, np.float32).reshape(-1, 10)
+        return int(lib.ow_collide_boxes_batch(_p(a, C.c_float), _p(b, C.c_float), len(a), float(margin), 1))
+    h = np.ascontiguousarray(hull_data, np.float32)
+    a = np.ascontiguousarray(a, np.float32).reshape(-1, 11); b = np.ascontiguousarray(b, np.float32).reshape(-1, 11)
+    return int(lib.ow_collide_hulls_batch(_p(h, C.c_float), _p(a, C.c_float), _p(b, C.c_float), len(a), float(margin), 0))
 
 
 def ref_colouring(a, b, a_awake, b_awake, n_bodies, color_limit=16, rounds_s=2, rounds_a=4):

@@ -723,7 +723,11 @@ static void rebuild_body(World& w, uint32_t id, uint32_t* counts) {
         if (w.mat[first + t] != 0) lst.push_back(t);
         else { w.body[first + t] = STATIC; counts[2]++; }
     }
-    if (lst.empty()) { w.alive[id] = 0; w.first[id] = NONE; w.count[id] = 0; counts[3]++; return; }
+    if (lst.empty()) {   // the body dies; its ids are unowned, without neighbours, as the library frees them
+        for (uint32_t t = 0; t < cnt; t++) for (int d = 0; d < 6; d++) w.nb6[(size_t)(first + t) * 6 + d] = NONE;
+        w.alive[id] = 0; w.first[id] = NONE; w.count[id] = 0; counts[3]++;
+        return;
+    }
     std::vector<int32_t> comp(cnt, -1);
     uint32_t ncomp = 0;
     for (uint32_t t0 : lst) {
@@ -1913,6 +1917,20 @@ int32_t ow_collide_boxes(const float* A, const float* B, float margin, int32_t d
     out[0] = n.x; out[1] = n.y; out[2] = n.z;
     for (int k = 0; k < cnt; k++) { out[3 + 4 * k] = pts[k].p.x; out[4 + 4 * k] = pts[k].p.y; out[5 + 4 * k] = pts[k].p.z; out[6 + 4 * k] = pts[k].s; }
     return cnt;
+}
+
+// many pairs in one call (for timing the restatement without a call per pair): counts only
+uint64_t ow_collide_boxes_batch(const float* A, const float* B, uint32_t n, float margin, int32_t do_reduce) {
+    uint64_t hits = 0;
+    float out[3 + 8 * 4];
+    for (uint32_t i = 0; i < n; i++) hits += ow_collide_boxes(A + (size_t)i * 10, B + (size_t)i * 10, margin, do_reduce, out) > 0;
+    return hits;
+}
+uint64_t ow_collide_hulls_batch(const float* hulls, const float* A, const float* B, uint32_t n, float margin, int32_t do_reduce) {
+    uint64_t hits = 0;
+    float out[36];
+    for (uint32_t i = 0; i < n; i++) hits += ow_collide_hulls(hulls, A + (size_t)i * 11, B + (size_t)i * 11, margin, do_reduce, out) > 0;
+    return hits;
 }
 
 

@@ -21,7 +21,7 @@ constexpr uint32_t HSIZE = 32768;
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 constexpr uint32_t STATIC = 0xFFFFFFFFu;
 constexpr uint8_t STEEL = 3, GLASS = 4, SLUG = 6;
-constexpr int MAXCOL = 128;
+constexpr int MAXCOL = 1024;   // sf_params.max_colors at most (default 128)
 
 struct MatTables {
     float mass[9], capv[9], caph[9], tens[9], stiff[9], duct[9];

@@ -56,6 +56,7 @@ struct SorState {
     DBuf<uint32_t> st_req;          // requested structures list for the apply pass
     // resting-body loads
     DBuf<float> extn, share;
+    DBuf<uint32_t> lcount;          // per body: bricks resting on a listed structure, bricks on the ground
     DBuf<uint64_t> lkey, lkey_alt;
     DBuf<uint32_t> lval, lval_alt;
     Work wk;
@@ -736,21 +737,27 @@ __device__ __forceinline__ uint32_t load_target(const float4 p, uint32_t sc, con
     return (s >= 0 && listed[s]) ? j : NONE;
 }
 
-__global__ void k_loads_share(uint32_t nb, const uint32_t *first, const uint32_t *count, const uint8_t *alive,
-                              const uint32_t *bscene, const float4 *wpos, const float *m, const uint32_t *ctab,
-                              const uint32_t *cpool, const uint8_t *smat, const int32_t *sid, const uint32_t *listed,
-                              float *share) {
+// per body: its bricks with a listed static brick below (ns) and its bricks on the ground (ng), counted brick by brick
+// (a body of tens of thousands of bricks would otherwise be one thread's loop)
+__global__ void k_loads_count(uint32_t nd, const uint32_t *kbody, const uint8_t *alive, const uint32_t *bscene,
+                              const float4 *wpos, const uint32_t *ctab, const uint32_t *cpool, const uint8_t *smat,
+                              const int32_t *sid, const uint32_t *listed, uint32_t *cnt2) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nd) return;
+    const uint32_t b = kbody[i];
+    if (!alive[b]) return;
+    const float4 p = wpos[i];
+    if (p.y < RB + 0.05f) atomicAdd(&cnt2[2 * b + 1], 1u);
+    if (load_target(p, bscene[b], ctab, cpool, smat, sid, listed) != NONE) atomicAdd(&cnt2[2 * b], 1u);
+}
+
+// a body's weight share per supported brick: m / (ns + ng), none when no brick rests on a listed structure
+__global__ void k_loads_share(uint32_t nb, const uint8_t *alive, const float *m, const uint32_t *cnt2, float *share) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
     float sh = 0.0f;
     if (alive[b]) {
-        uint32_t ns = 0, ng = 0;
-        const uint32_t sc = bscene[b];
-        for (uint32_t t = 0; t < count[b]; t++) {
-            const float4 p = wpos[first[b] + t];
-            if (p.y < RB + 0.05f) ng++;
-            if (load_target(p, sc, ctab, cpool, smat, sid, listed) != NONE) ns++;
-        }
+        const uint32_t ns = cnt2[2 * b], ng = cnt2[2 * b + 1];
         if (ns) sh = div_rn(m[b], (float)(ns + ng));
     }
     share[b] = sh;
@@ -1590,15 +1597,18 @@ sf_status sf_structure_loads(sf_world *w, const int32_t *structures, uint32_t n_
         const uint64_t none_key = ns;
         int bits = 0;
         while (bits < 64 && (none_key >> bits)) bits++;
-        k_loads_share<<<grid_for(nb, 128), 128, 0, s>>>(nb, w->b_first.p, w->b_count.p, w->b_alive.p, w->b_scene.p, w->k_wpos.p,
-                                                        w->b_m.p, w->ctab.p, w->cpool.p, w->s_mat.p, w->s_sid.p, st->active0.p,
-                                                        st->share.p);
+        SF_CUDA(st->lcount.grow((size_t)nb * 2));
+        SF_CUDA(cudaMemsetAsync(st->lcount.p, 0, (size_t)nb * 8, s));
+        k_loads_count<<<grid_for(nd, 256), 256, 0, s>>>(nd, w->k_body.p, w->b_alive.p, w->b_scene.p, w->k_wpos.p,
+                                                        w->ctab.p, w->cpool.p, w->s_mat.p, w->s_sid.p, st->active0.p,
+                                                        st->lcount.p);
+        k_loads_share<<<grid_for(nb, 128), 128, 0, s>>>(nb, w->b_alive.p, w->b_m.p, st->lcount.p, st->share.p);
         k_loads_keys<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, w->k_body.p, w->b_scene.p, w->k_wpos.p, st->share.p,
                                                        w->ctab.p, w->cpool.p, w->s_mat.p, w->s_sid.p, st->active0.p,
                                                        st->lkey.p, st->lval.p);
         SF_CUDA(radix_sort_u64(st->lkey.p, st->lval.p, st->lkey_alt.p, st->lval_alt.p, nd, bits, st->wk, s));
         k_loads_sum<<<grid_for(nd, 256), 256, 0, s>>>(nd, none_key, st->lkey.p, st->lval.p, w->k_body.p, st->share.p, st->extn.p);
-        st->launches += 3;
+        st->launches += 4;
     }
     k_loads_apply<<<grid_for(ns, 256), 256, 0, s>>>(ns, w->s_sid.p, w->s_mat.p, st->active0.p, st->extn.p, w->s_ext.p);
     st->launches++;

@@ -707,6 +707,7 @@ struct JpArgs {
     const uint32_t *dom_m0, *dom_m1;  // per domain: its manifolds [m0, m1)
     uint32_t *dom_cnt;                // per domain: three rotating worklist counters
     uint32_t max_colors, max_rounds;
+    uint32_t mw;                      // colour-mask words per body: max_colors / 32 rounded up
     GridBarrier *gb;                  // per domain
     uint32_t *err;
 };
@@ -770,17 +771,18 @@ __global__ void __launch_bounds__(128) k_jp(JpArgs A) {
                 if (valid && blocked) wl_out[base + __popc(bal & ((1u << lane) - 1u))] = m;
             }
             if (!valid || blocked) continue;
-            uint32_t used[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++) used[k] = __ldcg(&A.masks[(size_t)a * 4 + k]) | (b != STATIC ? __ldcg(&A.masks[(size_t)b * 4 + k]) : 0u);
+            // the lowest colour free at both bodies
             uint32_t c = 0xFFFFFFFFu;
-#pragma unroll
-            for (int k = 0; k < 4; k++) if (c == 0xFFFFFFFFu && ~used[k]) c = 32 * k + (__ffs(~used[k]) - 1);
+            for (uint32_t k = 0; k < A.mw && c == 0xFFFFFFFFu; k++) {
+                const uint32_t used = __ldcg(&A.masks[(size_t)a * A.mw + k]) |
+                                      (b != STATIC ? __ldcg(&A.masks[(size_t)b * A.mw + k]) : 0u);
+                if (~used) c = 32 * k + (__ffs(~used) - 1);
+            }
             if (c >= A.max_colors) { atomicOr(A.err, (unsigned)ERR_CAPACITY_COLORS); c = A.max_colors - 1; }
             A.man_color[m] = c;
             atomicExch(&A.man_round[m], r);
-            atomicOr(&A.masks[(size_t)a * 4 + (c >> 5)], 1u << (c & 31));
-            if (b != STATIC) atomicOr(&A.masks[(size_t)b * 4 + (c >> 5)], 1u << (c & 31));
+            atomicOr(&A.masks[(size_t)a * A.mw + (c >> 5)], 1u << (c & 31));
+            if (b != STATIC) atomicOr(&A.masks[(size_t)b * A.mw + (c >> 5)], 1u << (c & 31));
         }
         if (!dom_sync(A.gb + d, nblk, A.err)) return;
     }
@@ -857,14 +859,14 @@ __global__ void k_seg_table(uint32_t nseg, const uint32_t *hist, const uint32_t 
 
 // proper-colouring check: no two manifolds of one colour at one awake body
 __global__ void k_col_verify(const uint32_t *nm_p, const uint32_t *man_a, const uint32_t *man_b, const uint32_t *man_color,
-                             uint32_t *vmasks, uint32_t *err) {
+                             uint32_t mw, uint32_t *vmasks, uint32_t *err) {
     uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= *nm_p) return;
     uint32_t c = man_color[m];
     uint32_t bit = 1u << (c & 31);
-    if (atomicOr(&vmasks[(size_t)man_a[m] * 4 + (c >> 5)], bit) & bit) atomicOr(err, (unsigned)ERR_VERIFY_COLOR);
+    if (atomicOr(&vmasks[(size_t)man_a[m] * mw + (c >> 5)], bit) & bit) atomicOr(err, (unsigned)ERR_VERIFY_COLOR);
     uint32_t b = man_b[m];
-    if (b != STATIC && (atomicOr(&vmasks[(size_t)b * 4 + (c >> 5)], bit) & bit)) atomicOr(err, (unsigned)ERR_VERIFY_COLOR);
+    if (b != STATIC && (atomicOr(&vmasks[(size_t)b * mw + (c >> 5)], bit) & bit)) atomicOr(err, (unsigned)ERR_VERIFY_COLOR);
 }
 
 // ---------------------------------------------------------------- the coloured sequential-impulse solve
@@ -1381,7 +1383,8 @@ sf_status step_create(sf_world *w) {
     SF_CUDA(S->slot_id.alloc((size_t)nd * CSLOTS)); SF_CUDA(S->slot_p.alloc((size_t)nd * CSLOTS)); SF_CUDA(S->slot_n.alloc((size_t)nd * CSLOTS));
     SF_CUDA(S->ccount.alloc((size_t)nd + 1)); SF_CUDA(S->coff.alloc((size_t)nd + 1));
     SF_CUDA(S->bm_count.alloc((size_t)nb + 1)); SF_CUDA(S->bm_start.alloc((size_t)nb + 1)); SF_CUDA(S->bm_fill.alloc((size_t)nb + 1));
-    SF_CUDA(S->masks.alloc((size_t)nb * 4 + 4)); SF_CUDA(S->vmasks.alloc((size_t)nb * 4 + 4));
+    const uint32_t mw = (w->P.max_colors + 31) / 32;
+    SF_CUDA(S->masks.alloc((size_t)nb * mw + mw)); SF_CUDA(S->vmasks.alloc((size_t)nb * mw + mw));
     {
         const size_t nseg = (size_t)DOM_MAX * w->P.max_colors;
         SF_CUDA(S->col_count.alloc(nseg * JDS_ROW + 1)); SF_CUDA(S->col_start.alloc(nseg + 2));
@@ -1691,7 +1694,8 @@ static sf_status substep(sf_world *w, float h) {
         // colouring, on the active list's body ids, each domain on its own blocks
         SF_CUDA(cudaMemsetAsync(S->bm_count.p, 0, ((size_t)nb + 1) * 4, s));
         SF_CUDA(cudaMemsetAsync(S->bm_fill.p, 0, ((size_t)nb + 1) * 4, s));
-        SF_CUDA(cudaMemsetAsync(S->masks.p, 0, (size_t)nb * 16, s));
+        const uint32_t mw = (w->P.max_colors + 31) / 32;
+        SF_CUDA(cudaMemsetAsync(S->masks.p, 0, (size_t)nb * mw * 4, s));
         SF_CUDA(cudaMemsetAsync(S->man_round.p, 0xFF, (size_t)nc * 4, s));
         k_bm_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_ca.p, S->man_cb.p, S->bm_count.p);
         SF_CUDA(exclusive_scan_u32(S->bm_count.p, S->bm_start.p, (size_t)nb + 1, nullptr, S->wk, s));
@@ -1702,7 +1706,7 @@ static sf_status substep(sf_world *w, float h) {
         J.man_a = S->man_ca.p; J.man_b = S->man_cb.p; J.prio = S->man_prio.p;
         J.bm_start = S->bm_start.p; J.bm_list = S->bm_list.p; J.man_round = S->man_round.p; J.man_color = S->man_color.p;
         J.masks = S->masks.p; J.wl0 = S->wl0.p; J.wl1 = S->wl1.p; J.dev = S->dev.p; J.blk_dom = S->blk_dom.p;
-        J.dom_m0 = S->dom_m0.p; J.dom_m1 = S->dom_m1.p; J.dom_cnt = S->dom_cnt.p; J.max_colors = w->P.max_colors;
+        J.dom_m0 = S->dom_m0.p; J.dom_m1 = S->dom_m1.p; J.dom_cnt = S->dom_cnt.p; J.max_colors = w->P.max_colors; J.mw = mw;
         J.max_rounds = 1u << 16; J.gb = S->dom_gb.p; J.err = w->err.p;
         void *jargs[] = {&J};
         SF_CUDA(cudaLaunchCooperativeKernel((void *)k_jp, dim3(R), dim3(SOLVE_BLOCK), jargs, 0, s));
@@ -1722,8 +1726,9 @@ static sf_status substep(sf_world *w, float h) {
                                                         S->dev.p + DV_MANIFOLDS, S->col_start.p, S->jds_off.p);
         L += 6;
         if (w->P.verify) {
-            SF_CUDA(cudaMemsetAsync(S->vmasks.p, 0, (size_t)nb * 16, s));
-            k_col_verify<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_ca.p, S->man_cb.p, S->man_color.p, S->vmasks.p, w->err.p);
+            SF_CUDA(cudaMemsetAsync(S->vmasks.p, 0, (size_t)nb * mw * 4, s));
+            k_col_verify<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_ca.p, S->man_cb.p, S->man_color.p, mw,
+                                              S->vmasks.p, w->err.p);
             L++;
         }
         prof_mark(w);

@@ -75,3 +75,41 @@ def test_damage_debris_on_the_frame_against_oracle(sf, oracle):
         if f % 25 == 0:
             compare_world(w, ow)
     assert crushed > 5
+
+
+def test_tower_collapse_with_damage_against_oracle(sf, oracle):
+    """The 16-storey tower (47,760 bricks) with eight ground columns removed, frame by frame in the reference's order
+    with damage on: its joints go live, footings fail and are crushed, the tower detaches as a 46,818-brick body
+    (frame 254) that then settles, crushing and shedding pieces. 300 frames; every frame's reports match, and the
+    whole world (bodies, set-up, brick positions, potentials, static and body bonds) at frames 260, 280 and 300."""
+    tw, rm = S.tower16_structure()
+    sc = tw.without_static(rm)
+    ids = sc.structure_ids()
+    w = sf.World(sc, iterations=IT, detach_bodies=4000, detach_bricks=60000, damage=1)
+    ow = oracle.OracleWorld(sc)
+    ow.set_capacity(4000, 60000)
+    for s in ids:
+        w.structure_warm(s)
+        ow.structure_warm(s)
+    detached = 0
+    for f in range(1, 301):
+        w.step(DT)
+        ow.step(DT, iterations=IT, damage=1)
+        damage_counts(w, ow)
+        rep = w.rebuild_bodies()
+        assert (rep.bodies, rep.pieces, rep.removed, rep.dissolved, rep.lone) == ow.rebuild_bodies(), f
+        r1, _, _ = w.connectivity()
+        (p1, d1, _), _, _ = ow.connectivity()
+        w.structure_loads(ids)
+        ow.structure_loads(ids)
+        fr_ = w.structure_frame(f, ids, dt=DT)
+        o = ow.structure_frame(f, DT, ids)
+        assert (fr_.sweeps, fr_.warm_sweeps, fr_.joints, fr_.failed, fr_.crushed) == (o[0], o[1], o[3], o[5], o[6]), f
+        r2, now, top = w.connectivity()
+        (p2, d2, _), onow, otop = ow.connectivity()
+        assert (r1.pieces, r1.detached, r2.pieces, r2.detached) == (p1, d1, p2, d2), f
+        detached += r1.detached + r2.detached
+        if f in (260, 280, 300):
+            compare_world(w, ow)
+            compare_bonds(w, ow)
+    assert detached > 45000
