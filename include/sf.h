@@ -296,6 +296,43 @@ sf_status sf_read_damage(sf_world *w, sf_damage_report *report, uint8_t *activat
 /* body bricks' bonds (4 each: +x, +y, +z, foundation) and face neighbours (6 each, world body-brick ids) */
 sf_status sf_read_body_bonds(sf_world *w, float *bond4, uint32_t *nb6);
 
+/* ---- the debris-body load field (structural's body part, src/lib.rs:1262-1266, 1282-1365), in a world with spare
+ * capacity. After the structures' frame (sf_structure_frame), per scene in body order:
+ *   - a piece of 8 or more bricks none of whose bricks a contact supported in the last 10 frames (a contact from
+ *     below: the ground, a static brick, or another body's brick; stamped in every substep) starts its potentials over;
+ *   - a loaded piece (alive, awake, in contact, 8 or more bricks, its first brick not slug) carries the inertial load
+ *     MASS (n - 1) per brick, n = |g - a| / g (at most 150), a = the change of the piece's velocity and spin over the
+ *     frame (dt at least 1 ms) at the brick's position; the peak n is kept;
+ *   - a loaded piece of at most 60,000 bricks whose field is not settled (residual below 2e-4 and peak below 1.5),
+ *     or is and whose id in its scene plus the frame count is a multiple of 4, is swept red-black in FP64 with
+ *     omega 1.8, a supporting brick resting on the ground: at least 2 sweeps, until the residual falls below 4e-4,
+ *     60 sweeps or the scene's budget of 160,000 brick updates (sweeps x brick count, shared in body order) is spent;
+ *   - its load time grows by dt; it is judged unless settled and off its fourth frame (settled: with 4 dt); its
+ *     joints are live once loaded 0.3 s with a residual below 1e-2 (or 0.6 s), or at once above a peak of 2.5.
+ *     A live over-stressed joint fatigues at the material's DUCT pace; below 8% of its capacity it fails, or, in
+ *     pure compression along a near-vertical axis while the frame's 300 crushes last (counted on from crushes_used,
+ *     the structures' joint pass's crushes, one budget for the call), the weaker brick is crushed. A failure or a
+ *     crush marks the piece for sf_world_rebuild_bodies;
+ *   - a live piece that is not loaded lets its load time run down by 2 dt.
+ * The frame order of `step` (src/lib.rs:3650-3659) is then sf_world_step, sf_world_rebuild_bodies,
+ * sf_world_connectivity, sf_structure_loads, sf_structure_frame, sf_bodies_frame, sf_world_connectivity.
+ * sf_read_body_fields returns per body brick the f64 potential and the inertial load, and per body the last
+ * residual, the peak load factor, the load time and the largest joint ratio of its last judgement (any NULL). */
+typedef struct sf_bodies_report {
+    uint32_t bodies;            /* pieces swept */
+    uint32_t sweeps;            /* their sweeps */
+    uint64_t brick_updates;     /* sweeps x brick count */
+    uint32_t judged;            /* pieces whose joints were judged */
+    uint32_t crushes_used;      /* the frame's crushes after this pass (structures' and pieces') */
+    uint64_t joints, over, failed, crushed;   /* the judged joints, as sf_check_report */
+    float max_ratio;            /* the judged joints' largest ratio */
+    float reserved;
+    double ms;                  /* host time of the call */
+} sf_bodies_report;
+sf_status sf_bodies_frame(sf_world *w, float dt, uint32_t crushes_used, sf_bodies_report *report);
+sf_status sf_read_body_fields(sf_world *w, double *phi64, float *ext, double *resid, float *nmax, float *lt,
+                              float *maxr);
+
 /* per scene: static_off, n_static, body_off, body capacity, brick_off, brick capacity, bodies used, bricks used */
 sf_status sf_world_scene_ranges(const sf_world *w, uint32_t scene, uint32_t out8[8]);
 /* Per-structure sweeps and final residuals of the last sf_structure_solve (n_structures entries each). */

@@ -109,6 +109,9 @@ def load() -> C.CDLL:
     lib.ow_rebuild_bodies.argtypes = [C.c_void_p, _u32p]
     lib.ow_body_bonds.argtypes = [C.c_void_p, _f32p, _u32p]
     lib.ow_read_damage.argtypes = [C.c_void_p, _u64p, _u8p]
+    lib.ow_body_frame.argtypes = [C.c_void_p, C.c_float, C.c_uint32, _u32p]
+    lib.ow_body_state.argtypes = [C.c_void_p, _f64p, _f32p, _f32p, _f32p]
+    lib.ow_body_phi.argtypes = [C.c_void_p, _f64p, _f32p]
     lib.ow_crush_at.restype = C.c_uint32
     lib.ow_crush_at.argtypes = [C.c_void_p, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float, C.c_uint32]
     lib.ow_collide_hulls.restype = C.c_int32
@@ -330,6 +333,25 @@ class OracleWorld:
     def crush_at(self, start, e, p, cap=2500):
         """crush_at on brick `start` (static id, or n_static + body-brick id); returns the bricks crushed."""
         return int(self.lib.ow_crush_at(self.h, int(start), float(e), float(p[0]), float(p[1]), float(p[2]), int(cap)))
+
+    def body_frame(self, dt=1.0 / 60.0, crushes_used=0):
+        """structural's debris-body part; returns (bodies swept, sweeps, brick updates, joints, over, failed, crushed,
+        max ratio, crushes after the pass)."""
+        c = np.zeros(9, np.uint32)
+        self.lib.ow_body_frame(self.h, float(dt), int(crushes_used), _p(c, C.c_uint32))
+        return tuple(int(x) for x in c[:7]) + (float(c[7:8].view(np.float32)[0]), int(c[8]))
+
+    def body_state(self):
+        nb = self.nb
+        r = np.zeros(nb, np.float64); n = np.zeros(nb, np.float32); lt = np.zeros(nb, np.float32); mr = np.zeros(nb, np.float32)
+        self.lib.ow_body_state(self.h, _p(r, C.c_double), _p(n, C.c_float), _p(lt, C.c_float), _p(mr, C.c_float))
+        return r, n, lt, mr
+
+    def body_phi(self):
+        nd = self.nd
+        p = np.zeros(nd, np.float64); e = np.zeros(nd, np.float32)
+        self.lib.ow_body_phi(self.h, _p(p, C.c_double), _p(e, C.c_float))
+        return p, e
 
     def read_damage(self):
         """(candidates, crushed, removed, severed, cracked) since the last read, and per structure the hit flags."""

@@ -188,6 +188,10 @@ struct World {
     std::vector<uint8_t> st_conn;    // per structure: a joint failed or a brick was crushed since the last walk
     uint32_t cap_bodies = 0, cap_bricks = 0;   // capacity for detached pieces (bodies, body bricks)
     std::vector<uint8_t> dirty;      // per body: a brick was removed since its last rebuild (bd_dirty)
+    // the debris-body load field, per body (src/lib.rs:246-252: bd_vlast, bd_wlast, bd_resid, bd_nmax, bd_lt)
+    std::vector<V> vlast, wlast;
+    std::vector<double> bresid;
+    std::vector<float> nmax, blt;
     std::vector<uint32_t> stamp;     // per brick: the crush that visited it last (src/lib.rs:1650)
     uint32_t stamp_id = 0, dmg_draws = 0;
     uint64_t dmg[5] = {0, 0, 0, 0, 0};  // candidates, crushed, removed, severed, cracked
@@ -303,6 +307,8 @@ static void setup_body(World& w, uint32_t b, const uint32_t* lst, uint32_t n, V 
     float t1[9], t2[9];
     mmul(prot, iil, t1); mt(prot, t2); mmul(t1, t2, &w.iiw[(size_t)b * 9]);
     w.sleep[b] = 0.0f; w.asleep[b] = 0; w.wake[b] = 0; w.maxr[b] = 0.0f;
+    // a new field (src/lib.rs:845, 882): the load time, the residual and the peak factor start over
+    w.blt[b] = 0.0f; w.bresid[b] = 1.0; w.nmax[b] = 1.0f; w.vlast[b] = w.v[b]; w.wlast[b] = pw;
     w.rad[b] = std::sqrt(rad) + H * 1.8f;
     for (uint32_t t = 0; t < n; t++) { uint32_t i = lst[t]; w.wpos[i] = add(w.pos[b], mv(prot, w.local[i])); }
 }
@@ -352,7 +358,9 @@ static double sor_brick64(World& w, uint32_t i, double omega) {
         double k = (double)w.cond_w(i, j, d >> 1);
         sk += k; skp += k * w.phi64[j];
     }
-    if (w.body[i] == STATIC && w.by[i] == 0 && w.bond[(size_t)i * 4 + 3] > 0.0f) sk += (double)(GROUNDK * STIFF[mi]);
+    if (w.body[i] == STATIC) { if (w.by[i] == 0 && w.bond[(size_t)i * 4 + 3] > 0.0f) sk += (double)(GROUNDK * STIFF[mi]); }
+    // a body brick with a supporting contact in the last 10 frames rests on the ground (src/lib.rs:1016)
+    else if ((uint32_t)(w.frame - w.sup[i]) < 10u) sk += (double)(GROUNDK * STIFF[mi]);
     if (sk > 0.0) {
         double target = ((double)(MASS[mi] + w.ext[i]) + skp) / sk;
         double d = omega * (target - w.phi64[i]);
@@ -414,6 +422,7 @@ enum { J_HOLD = 0, J_FATIGUE = 1, J_FAIL = 2, J_CRUSH = 3 };
 struct Joint { uint32_t i, axis, j, decision, crushed; float ratio, bond_after; };
 // a failed joint or a crushed brick leaves its structure pending a connectivity walk (src/lib.rs:714, 1202, 1223)
 static void flag_conn(World& w, int32_t s) { if (s >= 0 && s < (int32_t)w.st_conn.size()) w.st_conn[s] = 1; }
+static void remove_brick(World& w, uint32_t i);
 
 static float stress_brick(World& w, uint32_t i, float dt, bool live, std::vector<Joint>& out) {
     uint8_t mi = w.mat[i];
@@ -448,12 +457,12 @@ static float stress_brick(World& w, uint32_t i, float dt, bool live, std::vector
                     uint32_t k = CAPV[w.mat[j]] < CAPV[mi] ? j : i;
                     jr.decision = J_CRUSH; jr.crushed = k; jr.bond_after = hp;
                     out.push_back(jr);
-                    w.gset(w.bx[k], w.by[k], w.bz[k], 0);
-                    w.mat[k] = 0;
+                    remove_brick(w, k);   // a body brick's removal marks its body for rebuild (src/lib.rs:717)
                     return maxf(maxr, r);
                 }
                 w.bond[(size_t)i * 4 + a] = 0.0f;
                 if (!dynb) flag_conn(w, w.sid[i]);
+                else w.dirty[w.body[i]] = 1;   // src/lib.rs:1201
                 jr.decision = J_FAIL; jr.bond_after = 0.0f;
             } else {
                 w.bond[(size_t)i * 4 + a] = nhp;
@@ -597,6 +606,7 @@ static bool detach_piece(World& w, const std::vector<uint32_t>& lst) {
     for (int k = 0; k < 9; k++) { w.rot.push_back(0.0f); w.iil.push_back(0.0f); w.iiw.push_back(0.0f); }
     w.m.push_back(0.0f); w.im.push_back(0.0f); w.sleep.push_back(0.0f); w.rad.push_back(0.0f); w.maxr.push_back(0.0f);
     w.island.push_back(NONE); w.dirty.push_back(0);
+    w.vlast.push_back(vv(0, 0, 0)); w.wlast.push_back(vv(0, 0, 0)); w.bresid.push_back(1.0); w.nmax.push_back(1.0f); w.blt.push_back(0.0f);
     std::vector<uint32_t> nl;
     const uint32_t k0 = w.ns + w.nd;
     std::unordered_map<uint32_t, uint32_t> place;
@@ -763,13 +773,13 @@ static void rebuild_body(World& w, uint32_t id, uint32_t* counts) {
     uint32_t awake = 0;
     for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b] && !w.asleep[b]) awake++;
     // copies of the kept bricks (the first component's moves overwrite ids it reads)
-    struct Rec { uint8_t mat, infill; int32_t x, y, z, sid; V local; uint32_t nb6[6]; float bond[4], bmax[4]; uint32_t sup; };
+    struct Rec { uint8_t mat, infill; int32_t x, y, z, sid; V local; uint32_t nb6[6]; float bond[4], bmax[4]; uint32_t sup; float phi, ext; double phi64; };
     std::vector<Rec> rec(cnt);
     for (uint32_t t = 0; t < cnt; t++) {
         const uint32_t i = first + t;
         Rec& r = rec[t];
         r.mat = w.mat[i]; r.infill = w.infill[i]; r.x = w.bx[i]; r.y = w.by[i]; r.z = w.bz[i]; r.sid = w.sid[i];
-        r.local = w.local[i]; r.sup = w.sup[i];
+        r.local = w.local[i]; r.sup = w.sup[i]; r.phi = w.phi[i]; r.ext = w.ext[i]; r.phi64 = w.phi64[i];
         for (int d = 0; d < 6; d++) r.nb6[d] = w.nb6[(size_t)i * 6 + d];
         for (int a = 0; a < 4; a++) { r.bond[a] = w.bond[(size_t)i * 4 + a]; r.bmax[a] = w.bmax[(size_t)i * 4 + a]; }
     }
@@ -797,6 +807,7 @@ static void rebuild_body(World& w, uint32_t id, uint32_t* counts) {
             for (int k = 0; k < 9; k++) { w.rot.push_back(0.0f); w.iil.push_back(0.0f); w.iiw.push_back(0.0f); }
             w.m.push_back(0.0f); w.im.push_back(0.0f); w.sleep.push_back(0.0f); w.rad.push_back(0.0f); w.maxr.push_back(0.0f);
             w.island.push_back(NONE); w.dirty.push_back(0);
+    w.vlast.push_back(vv(0, 0, 0)); w.wlast.push_back(vv(0, 0, 0)); w.bresid.push_back(1.0); w.nmax.push_back(1.0f); w.blt.push_back(0.0f);
             cbody[c] = b;
             cfirst[c] = w.ns + w.nd;
             for (size_t t = 0; t < g.size(); t++) {
@@ -821,7 +832,7 @@ static void rebuild_body(World& w, uint32_t id, uint32_t* counts) {
             const Rec& r = rec[g[t]];
             const uint32_t i = cfirst[c] + (uint32_t)t;
             w.mat[i] = r.mat; w.infill[i] = r.infill; w.bx[i] = r.x; w.by[i] = r.y; w.bz[i] = r.z; w.sid[i] = r.sid;
-            w.local[i] = r.local; w.sup[i] = r.sup;
+            w.local[i] = r.local; w.sup[i] = r.sup; w.phi[i] = r.phi; w.ext[i] = r.ext; w.phi64[i] = r.phi64;
             for (int d = 0; d < 6; d++) {
                 const uint32_t j = r.nb6[d];
                 uint32_t nj = NONE;
@@ -831,7 +842,9 @@ static void rebuild_body(World& w, uint32_t id, uint32_t* counts) {
             for (int a = 0; a < 4; a++) { w.bond[(size_t)i * 4 + a] = r.bond[a]; w.bmax[(size_t)i * 4 + a] = r.bmax[a]; }
             ids.push_back(i);
         }
+        const float keep_lt = w.blt[cbody[c]];
         setup_body(w, cbody[c], ids.data(), (uint32_t)ids.size(), ppos, prot, pq, pv, pw);
+        if (c == 0) w.blt[cbody[c]] = keep_lt;   // the body keeps its load time (src/lib.rs:998)
     }
 }
 // step's loop over marked bodies (src/lib.rs:3652). counts: bodies, pieces, removed bricks, dissolved, lone.
@@ -839,6 +852,95 @@ static void rebuild_bodies(World& w, uint32_t* counts) {
     for (int k = 0; k < 5; k++) counts[k] = 0;
     for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b] && w.dirty[b]) rebuild_body(w, b, counts);
     for (uint32_t b = 0; b < w.nbody; b++) w.dirty[b] = 0;
+}
+
+// ---------------------------------------------------------------- the debris-body load field (src/lib.rs:1262-1365)
+static void update_cache(World& w);
+// body_loaded (src/lib.rs:1045-1047): awake, in contact, at least 8 bricks
+static bool body_loaded(const World& w, uint32_t b) {
+    return w.alive[b] && w.count[b] >= 8 && !w.asleep[b] && w.nc[b] > 0 && w.mat[w.first[b]] < SLUG;
+}
+static void body_list(const World& w, uint32_t b, std::vector<uint32_t>& out, bool only_present) {
+    out.clear();
+    for (uint32_t k = w.first[b]; k != NONE; k = w.next[k]) if (!only_present || w.mat[k] != 0) out.push_back(k);
+}
+// structural's body part after its loads: unsupported pieces start their field over, inertial loads g - a, the
+// field's sweeps (red-black FP64 over the body's bricks, as the structures' sweeps here) from a budget of 160,000
+// brick-updates in body order, then the pieces' joints (after the structures' joint pass, whose crush budget they
+// continue). counts: [0] bodies swept, [1] sweeps, [2] brick updates, [3] joints, [4] over, [5] failed, [6] crushed,
+// [7] the largest ratio's bits, [8] the frame's crushes after the pass. Brick updates count sweeps x bd_count, the
+// budget's unit; crush_used is the structures' joint pass's crushes, which the budget of 300 counts on from.
+static void body_frame(World& w, float dt, uint32_t crush_used, uint32_t* counts) {
+    for (int k = 0; k < 9; k++) counts[k] = 0;
+    w.crush_n = crush_used;
+    update_cache(w);
+    const uint32_t fr = w.frame;
+    std::vector<uint32_t> lst;
+    for (uint32_t b = 0; b < w.nbody; b++) {   // src/lib.rs:1262-1266
+        if (!w.alive[b] || w.count[b] < 8) continue;
+        body_list(w, b, lst, false);
+        bool any = false;
+        for (uint32_t k : lst) if ((uint32_t)(fr - w.sup[k]) < 10u) { any = true; break; }
+        if (!any) for (uint32_t k : lst) { w.phi[k] = 0.0f; w.phi64[k] = 0.0; }
+    }
+    const float idt = 1.0f / maxf(dt, 1e-3f);   // src/lib.rs:1288-1304
+    for (uint32_t b = 0; b < w.nbody; b++) {
+        if (!w.alive[b]) continue;
+        const V al = mul(sub(w.v[b], w.vlast[b]), idt), aa = mul(sub(w.w[b], w.wlast[b]), idt);
+        w.vlast[b] = w.v[b]; w.wlast[b] = w.w[b];
+        if (!body_loaded(w, b)) continue;
+        const V pb = w.pos[b];
+        float nm = 0.0f;
+        body_list(w, b, lst, true);
+        for (uint32_t k : lst) {
+            const V a = add(al, cross(aa, sub(w.wpos[k], pb)));
+            const V ge = vv(-a[0], -GR - a[1], -a[2]);
+            const float n = minf(len(ge) / GR, 150.0f);
+            if (n > nm) nm = n;
+            w.ext[k] = MASS[w.mat[k]] * (n - 1.0f);
+        }
+        w.nmax[b] = nm;
+    }
+    int64_t budget = 160000;   // src/lib.rs:1305-1316
+    for (uint32_t b = 0; b < w.nbody; b++) {
+        if (!body_loaded(w, b) || w.count[b] > 60000) continue;
+        if (w.bresid[b] < (double)2e-4f && w.nmax[b] < 1.5f && (fr + b) % 4 != 0) continue;
+        const int64_t size = w.count[b];
+        body_list(w, b, lst, true);
+        uint32_t n = 0;
+        for (;;) {
+            const double r = rb64_sweep(w, lst, (double)1.8f);
+            w.bresid[b] = r;
+            n++; budget -= size;
+            if (n >= 2 && (r < (double)4e-4f || n >= 60 || budget <= 0)) break;
+        }
+        for (uint32_t k : lst) w.phi[k] = (float)w.phi64[k];
+        counts[0]++; counts[1] += n; counts[2] += n * (uint32_t)size;
+    }
+    float gm = 0.0f;   // src/lib.rs:1340-1360
+    for (uint32_t b = 0; b < w.nbody; b++) {
+        if (!body_loaded(w, b) || w.count[b] > 60000) continue;
+        w.blt[b] += dt;
+        const bool settled = w.bresid[b] < (double)2e-4f && w.nmax[b] < 1.5f;
+        if (settled && (fr + b) % 4 != 0) continue;
+        const float dtb = settled ? dt * 4.0f : dt;
+        const bool live = (w.blt[b] > 0.3f && (w.bresid[b] < (double)1e-2f || w.blt[b] > 0.6f)) || w.nmax[b] > 2.5f;
+        float bm = 0.0f;
+        std::vector<Joint> out;
+        body_list(w, b, lst, false);
+        for (uint32_t k : lst) if (w.mat[k] != 0) { const float r = stress_brick(w, k, dtb, live, out); if (r > bm) bm = r; }
+        w.maxr[b] = bm;
+        if (bm > gm) gm = bm;
+        for (const Joint& j : out) {
+            counts[3]++;
+            if (j.ratio > 1.0f) counts[4]++;
+            if (j.decision == J_FAIL) counts[5]++;
+            if (j.decision == J_CRUSH) counts[6]++;
+        }
+    }
+    for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b] && !body_loaded(w, b)) w.blt[b] = maxf(w.blt[b] - 2.0f * dt, 0.0f);
+    std::memcpy(&counts[7], &gm, 4);
+    counts[8] = w.crush_n;
 }
 
 // st_now / st_top (src/lib.rs:1126-1128)
@@ -1041,20 +1143,26 @@ static void build_manifolds(World& w) {
     std::vector<uint32_t> order(nm);
     std::iota(order.begin(), order.end(), 0u);
     std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return prio[x] != prio[y] ? prio[x] > prio[y] : x < y; });
+    // per body the colours its manifolds hold (grown as needed: a body resting on thousands of contacts holds many)
     std::vector<std::vector<uint64_t>> used(w.nbody, std::vector<uint64_t>(4, 0));
+    auto held = [&](uint32_t x, uint32_t c) { return (c >> 6) < used[x].size() && ((used[x][c >> 6] >> (c & 63)) & 1); };
+    auto hold = [&](uint32_t x, uint32_t c) {
+        if ((c >> 6) >= used[x].size()) used[x].resize((c >> 6) + 1, 0);
+        used[x][c >> 6] |= 1ull << (c & 63);
+    };
     w.man_color.assign(nm, 0);
     w.ncolors = 0;
     for (uint32_t mi : order) {
         uint32_t a = w.man_a[mi], b = w.man_b[mi];
         uint32_t c = 0;
         for (;; c++) {
-            bool busy = (used[a][c >> 6] >> (c & 63)) & 1;
-            if (b != STATIC) busy = busy || ((used[b][c >> 6] >> (c & 63)) & 1);
+            bool busy = held(a, c);
+            if (b != STATIC) busy = busy || held(b, c);
             if (!busy) break;
         }
         w.man_color[mi] = c;
-        used[a][c >> 6] |= 1ull << (c & 63);
-        if (b != STATIC) used[b][c >> 6] |= 1ull << (c & 63);
+        hold(a, c);
+        if (b != STATIC) hold(b, c);
         if (c + 1 > w.ncolors) w.ncolors = c + 1;
     }
 }
@@ -1637,6 +1745,8 @@ void* ow_create(uint32_t n_static, const int32_t* static_xyz, const uint8_t* sta
     w->pos.assign(nb, vv(0, 0, 0)); w->v = w->pos; w->w = w->pos; w->vpre = w->pos; w->wpre = w->pos;
     w->q.assign((size_t)nb * 4, 0.0f); w->rot.assign((size_t)nb * 9, 0.0f); w->iil = w->rot; w->iiw = w->rot;
     w->m.assign(nb, 0.0f); w->im = w->m; w->sleep = w->m; w->rad = w->m; w->maxr = w->m;
+    w->vlast.assign(nb, vv(0, 0, 0)); w->wlast = w->vlast; w->bresid.assign(nb, 1.0); w->nmax.assign(nb, 1.0f);
+    w->blt.assign(nb, 0.0f);
     w->island.assign(nb, NONE);
     std::vector<uint32_t> lst;
     for (uint32_t b = 0; b < nb; b++) {
@@ -1807,6 +1917,17 @@ void ow_remove_bricks(void* h, const uint32_t* statics, uint32_t ns_, const uint
     for (uint32_t k = 0; k < nb_; k++) if (body_bricks[k] < w->nd) remove_brick(*w, w->ns + body_bricks[k]);
 }
 void ow_rebuild_bodies(void* h, uint32_t* counts) { rebuild_bodies(*(World*)h, counts); }
+void ow_body_frame(void* h, float dt, uint32_t crush_used, uint32_t* counts) { body_frame(*(World*)h, dt, crush_used, counts); }
+// per body: last residual, peak load factor, load time, largest joint ratio
+void ow_body_state(void* h, double* resid, float* nmax, float* lt, float* maxr) {
+    World* w = (World*)h;
+    for (uint32_t b = 0; b < w->nbody; b++) { resid[b] = w->bresid[b]; nmax[b] = w->nmax[b]; lt[b] = w->blt[b]; maxr[b] = w->maxr[b]; }
+}
+// per body brick: f64 potential and inertial load
+void ow_body_phi(void* h, double* phi64, float* ext) {
+    World* w = (World*)h;
+    for (uint32_t k = 0; k < w->nd; k++) { phi64[k] = w->phi64[w->ns + k]; ext[k] = w->ext[w->ns + k]; }
+}
 // crush_at on one brick (a static id, or ns + a body-brick id) with energy e at point p; returns the bricks crushed
 uint32_t ow_crush_at(void* h, uint32_t start, float e, float px, float py, float pz, uint32_t cap) {
     World* w = (World*)h;

@@ -107,6 +107,13 @@ class DamageReport(C.Structure):
                 ("cracked", C.c_uint64)]
 
 
+class BodiesReport(C.Structure):
+    _fields_ = [("bodies", C.c_uint32), ("sweeps", C.c_uint32), ("brick_updates", C.c_uint64),
+                ("judged", C.c_uint32), ("crushes_used", C.c_uint32), ("joints", C.c_uint64), ("over", C.c_uint64),
+                ("failed", C.c_uint64), ("crushed", C.c_uint64), ("max_ratio", C.c_float), ("reserved", C.c_float),
+                ("ms", C.c_double)]
+
+
 class WorldInfo(C.Structure):
     _fields_ = [("n_scenes", C.c_uint32), ("n_static", C.c_uint32), ("n_bodies", C.c_uint32),
                 ("n_body_bricks", C.c_uint32), ("n_structures", C.c_uint32), ("n_chunks", C.c_uint32)]
@@ -174,6 +181,9 @@ PROTOTYPES = {
     "sf_world_rebuild_bodies": (C.c_int32, [C.c_void_p, C.POINTER(RebuildReport)]),
     "sf_read_body_bonds": (C.c_int32, [C.c_void_p, _f32p, _u32p]),
     "sf_read_damage": (C.c_int32, [C.c_void_p, C.POINTER(DamageReport), _u8p]),
+    "sf_bodies_frame": (C.c_int32, [C.c_void_p, C.c_float, C.c_uint32, C.POINTER(BodiesReport)]),
+    "sf_read_body_fields": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double), _f32p, C.POINTER(C.c_double), _f32p, _f32p,
+                                        _f32p]),
     "sf_structure_loads": (C.c_int32, [C.c_void_p, _i32p, C.c_uint32]),
     "sf_world_get_info": (C.c_int32, [C.c_void_p, C.POINTER(WorldInfo)]),
     "sf_get_stats": (C.c_int32, [C.c_void_p, C.POINTER(Stats)]),
@@ -498,6 +508,24 @@ class World:
         h = np.zeros(max(self.info.n_structures, 1), np.uint8)
         _check(self._lib.sf_read_damage(self._h, C.byref(r), _ptr(h, C.c_uint8)), "sf_read_damage")
         return r, h[:self.info.n_structures]
+
+    def bodies_frame(self, dt: float = 1.0 / 60.0, crushes_used: int = 0) -> BodiesReport:
+        """The debris pieces' load field and joints for this frame (sf_bodies_frame), after structure_frame, whose
+        crushes (FrameReport.crushed) the pieces' crushes count on from."""
+        r = BodiesReport()
+        _check(self._lib.sf_bodies_frame(self._h, float(dt), int(crushes_used), C.byref(r)), "sf_bodies_frame")
+        return r
+
+    def body_fields(self):
+        """(phi64 and inertial load per body brick; residual, peak load factor, load time, largest ratio per body)."""
+        nd, nb = self.info.n_body_bricks, self.info.n_bodies
+        phi = np.zeros(max(nd, 1), np.float64); ext = np.zeros(max(nd, 1), np.float32)
+        resid = np.zeros(max(nb, 1), np.float64)
+        nmax, lt, maxr = (np.zeros(max(nb, 1), np.float32) for _ in range(3))
+        _check(self._lib.sf_read_body_fields(self._h, _ptr(phi, C.c_double), _ptr(ext, C.c_float),
+                                             _ptr(resid, C.c_double), _ptr(nmax, C.c_float), _ptr(lt, C.c_float),
+                                             _ptr(maxr, C.c_float)), "sf_read_body_fields")
+        return phi[:nd], ext[:nd], resid[:nb], nmax[:nb], lt[:nb], maxr[:nb]
 
     def body_bonds(self):
         """Per body brick: bonds (+x, +y, +z, foundation) and face neighbours (world body-brick ids)."""

@@ -166,6 +166,7 @@ struct SorState;     // sf_sor.cu
 struct ConnState;    // sf_connect.cu
 struct SplitState;   // sf_split.cu
 struct DamageState;  // sf_damage.cu
+struct BodyLoadState;  // sf_bodyload.cu
 uint64_t sor_launches(const SorState *st);
 const Tuner *sor_tuner(const SorState *st);
 uint64_t sor_graph_launches(const SorState *st);
@@ -268,6 +269,17 @@ struct sf_world {
     sf::DBuf<float> k_bond, k_bmax;
     sf::DBuf<uint8_t> b_dirty;
     uint64_t rebuilds = 0;               // rebuild_body calls so far (a draw counter of the lone-brick rule)
+    // the debris-body load field (structural's body part, src/lib.rs:1262-1365), in the same worlds: per body brick
+    // the frame a contact last supported it, its potential (f64, with the f32 copy the joints read) and its inertial
+    // load; per body the velocities of the last frame, the last sweep's residual, the peak load factor and the time
+    // its field has been loaded
+    sf::DBuf<uint32_t> k_sup;
+    sf::DBuf<double> k_phi64;
+    sf::DBuf<float> k_phi, k_ext;
+    sf::DBuf<float4> b_vlast, b_wlast;
+    sf::DBuf<double> b_resid;
+    sf::DBuf<float> b_nmax, b_lt;
+    sf::BodyLoadState *bodyload = nullptr;
     // connectivity: per structure, set on the GPU when a joint pass fails a joint or crushes a brick (pending walk);
     // structures a full scene could not take are pending on the host
     sf::DBuf<uint8_t> st_conn;
@@ -391,6 +403,10 @@ sf_status read_error_word(sf_world *w);
 void conn_destroy(sf_world *w);
 void split_destroy(sf_world *w);
 void damage_destroy(sf_world *w);
+void bodyload_destroy(sf_world *w);
+// the load-field state of bodies just set up (setup_body, src/lib.rs:845, 882): listed ids (d_list) or base..base+n;
+// d_keep (optional, per entry) keeps the body's load time
+cudaError_t body_load_setup(sf_world *w, const uint32_t *d_list, uint32_t base, uint32_t n, const uint8_t *d_keep);
 // the substep's contacts in list order, for impact damage (sf_damage.cu)
 struct DamageIn {
     uint32_t nc;

@@ -26,10 +26,12 @@
 
 namespace sf {
 
-constexpr int SPLIT_WORDS = 24;   // per read-back brick: xyz 3, mat, 6 neighbours, 4 bonds, 4 capacities, local 3, 3 spare
+constexpr int SPLIT_WORDS = 26;   // per read-back brick: xyz 3, mat, 6 neighbours, 4 bonds, 4 capacities, local 3,
+                                  // the load field's support stamp, f32 potential, load and f64 potential (2)
 
 struct SplitState {
     DBuf<uint32_t> list, count, bsel, brec, slots, words, freed, awake;
+    DBuf<uint8_t> keep;                 // per set-up body: the rebuilt body itself, which keeps its load time
     DBuf<float> pose;
     std::vector<uint32_t> scene_rebuilds;
 };
@@ -95,6 +97,7 @@ __global__ void k_body_snapshot(uint32_t n, const uint32_t *list, const uint32_t
 // the bricks of the listed slots, SPLIT_WORDS each
 __global__ void k_brick_snapshot(uint32_t n, const uint32_t *slots, const int32_t *xyz, const uint8_t *kmat,
                                  const uint32_t *nb6, const float *bond, const float *bmax, const float4 *local,
+                                 const uint32_t *sup, const float *phi, const float *ext, const double *phi64,
                                  uint32_t *out) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -109,12 +112,15 @@ __global__ void k_brick_snapshot(uint32_t n, const uint32_t *slots, const int32_
     }
     const float4 l = local[i];
     o[18] = __float_as_uint(l.x); o[19] = __float_as_uint(l.y); o[20] = __float_as_uint(l.z);
-    o[21] = o[22] = o[23] = 0;
+    o[21] = sup[i]; o[22] = __float_as_uint(phi[i]); o[23] = __float_as_uint(ext[i]);
+    const unsigned long long p = (unsigned long long)__double_as_longlong(phi64[i]);
+    o[24] = (uint32_t)p; o[25] = (uint32_t)(p >> 32);
 }
 
 // write brick records (same layout) to the listed slots
 __global__ void k_brick_write(uint32_t n, const uint32_t *slots, const uint32_t *in, int32_t *xyz, uint8_t *kmat,
-                              uint32_t *nb6, float *bond, float *bmax, float4 *local) {
+                              uint32_t *nb6, float *bond, float *bmax, float4 *local, uint32_t *sup, float *phi,
+                              float *ext, double *phi64) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const uint32_t i = slots[k];
@@ -127,6 +133,8 @@ __global__ void k_brick_write(uint32_t n, const uint32_t *slots, const uint32_t 
         bmax[(size_t)i * 4 + a] = __uint_as_float(r[14 + a]);
     }
     local[i] = make_float4(__uint_as_float(r[18]), __uint_as_float(r[19]), __uint_as_float(r[20]), 0.0f);
+    sup[i] = r[21]; phi[i] = __uint_as_float(r[22]); ext[i] = __uint_as_float(r[23]);
+    phi64[i] = __longlong_as_double((long long)(((unsigned long long)r[25] << 32) | r[24]));
 }
 
 // slots no body owns any more: material 0, owned by the sentinel, no neighbours
@@ -235,7 +243,8 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
         SF_CUDA(cudaMemcpyAsync(X.slots.p, slots.data(), slots.size() * 4, cudaMemcpyHostToDevice, st));
         k_brick_snapshot<<<grid_for(slots.size(), 256), 256, 0, st>>>((uint32_t)slots.size(), X.slots.p, w->k_xyz.p,
                                                                       w->k_mat.p, w->k_nb6.p, w->k_bond.p,
-                                                                      w->k_bmax.p, w->k_local.p, X.brec.p);
+                                                                      w->k_bmax.p, w->k_local.p, w->k_sup.p,
+                                                                      w->k_phi.p, w->k_ext.p, w->k_phi64.p, X.brec.p);
         w->launches++;
         SF_CUDA(cudaGetLastError());
         SF_CUDA(cudaMemcpyAsync(rec.data(), X.brec.p, rec.size() * 4, cudaMemcpyDeviceToHost, st));
@@ -245,6 +254,7 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
 
     // ---- rebuild_body's walk, body by body
     std::vector<uint32_t> wslots, wrec, freed, ranges, setup_ids;
+    std::vector<uint8_t> setup_keep;
     std::vector<float> poses;
     std::vector<uint8_t> live_scene(w->n_scenes, 0);
     for (uint32_t k = 0; k < nd_; k++) {
@@ -343,6 +353,7 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
             }
             ranges.insert(ranges.end(), {cbody[c], cfirst[c], (uint32_t)g.size()});
             setup_ids.push_back(cbody[c]);
+            setup_keep.push_back(c == 0 ? 1 : 0);
             for (int j = 0; j < 22; j++) { float f; std::memcpy(&f, &B[3 + j], 4); poses.push_back(f); }
         }
     }
@@ -370,7 +381,8 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
         SF_CUDA(cudaMemcpyAsync(X.brec.p, wrec.data(), wrec.size() * 4, cudaMemcpyHostToDevice, st));
         k_brick_write<<<grid_for(wslots.size(), 256), 256, 0, st>>>((uint32_t)wslots.size(), X.slots.p, X.brec.p,
                                                                     w->k_xyz.p, w->k_mat.p, w->k_nb6.p, w->k_bond.p,
-                                                                    w->k_bmax.p, w->k_local.p);
+                                                                    w->k_bmax.p, w->k_local.p, w->k_sup.p,
+                                                                    w->k_phi.p, w->k_ext.p, w->k_phi64.p);
         w->launches++;
     }
     const uint32_t nr = (uint32_t)(ranges.size() / 3);
@@ -386,6 +398,9 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
         SF_CUDA(cudaMemcpyAsync(X.list.p, setup_ids.data(), setup_ids.size() * 4, cudaMemcpyHostToDevice, st));
         SF_CUDA(cudaMemcpyAsync(X.pose.p, poses.data(), poses.size() * 4, cudaMemcpyHostToDevice, st));
         SF_CUDA(setup_bodies_from_local(w, X.list.p, (uint32_t)setup_ids.size(), X.pose.p));
+        SF_CUDA(X.keep.grow(setup_keep.size()));
+        SF_CUDA(cudaMemcpyAsync(X.keep.p, setup_keep.data(), setup_keep.size(), cudaMemcpyHostToDevice, st));
+        SF_CUDA(body_load_setup(w, X.list.p, 0u, (uint32_t)setup_ids.size(), X.keep.p));
     }
     SF_CUDA(cudaMemsetAsync(w->b_dirty.p, 0, w->b_dirty.bytes(), st));
     for (uint32_t q = 0; q < w->n_scenes; q++) if (live_scene[q]) step_set_live(w, q, true);

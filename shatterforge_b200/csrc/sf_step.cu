@@ -312,6 +312,8 @@ struct ContactArgs {
     uint32_t *ccount;
     const uint32_t *coff;
     uint8_t *wake;
+    uint32_t *sup;                     // per body brick: the frame a contact last supported it (nullptr: not kept)
+    uint32_t frame;
     // slot scratch, slot-major: slot k of active brick t at k * nd + t
     uint4 *slot_id;
     float4 *slot_p, *slot_n;
@@ -335,7 +337,10 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
         for (int c = 0; c < 8; c++) {
             V3 l = v3((c & 1) == 0 ? -H : H, (c & 2) == 0 ? -H : H, (c & 4) == 0 ? -H : H);
             V3 cp = add(p, mv(r, l));
-            if (cp.y < 0.0f) emit(STATIC, STATIC, NONE, cp, v3(0.0f, 1.0f, 0.0f), -cp.y);
+            if (cp.y < 0.0f) {
+                if (WAKE && A.sup) A.sup[i] = A.frame;
+                emit(STATIC, STATIC, NONE, cp, v3(0.0f, 1.0f, 0.0f), -cp.y);
+            }
         }
     }
     // static cells of the 3^3 block (src/lib.rs:1422-1440): the block spans at most 2 x 2 x 2 chunks, read once
@@ -372,6 +377,7 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
                         const float dist = len(d);
                         if (dist >= RB) continue;
                         if (dist > 1e-4f) {
+                            if (WAKE && A.sup && d.y > 0.3f * dist) A.sup[i] = A.frame;
                             emit(STATIC, STATIC, j, qq, mul(d, div_rn(1.0f, dist)), RB - dist);
                         } else {
                             const V3 r = sub(p, c);
@@ -444,6 +450,10 @@ __device__ __forceinline__ void gen_brick(const ContactArgs &A, uint32_t i, uint
                     const float dist = sqrt_rn(dd);
                     const V3 nn = mul(d, div_rn(1.0f, dist));
                     const V3 cp = madd(pj, nn, dist * 0.5f);
+                    if (WAKE && A.sup) {
+                        if (nn.y > 0.3f) A.sup[i] = A.frame;
+                        else if (nn.y < -0.3f) A.sup[j] = A.frame;
+                    }
                     if (other_awake) emit(bj, bj, j, cp, nn, 2.0f * RB - dist);
                     else {
                         if (WAKE && speed > 0.7f) A.wake[bj] = 1;
@@ -1618,6 +1628,7 @@ static sf_status substep(sf_world *w, float h) {
     C.alive = w->b_alive.p; C.asleep = w->b_asleep.p; C.smat = w->s_mat.p; C.wpos = w->k_wpos.p;
     C.v = w->b_v.p; C.w = w->b_w.p; C.rot = w->b_rot.p; C.rad = w->b_rad.p; C.bstart = S->bstart.p; C.srec = S->srec.p;
     C.sent = S->sent.p; C.ccount = S->ccount.p; C.coff = S->coff.p; C.wake = w->b_wake.p;
+    C.sup = w->k_sup.p; C.frame = w->frame;
     C.slot_id = S->slot_id.p; C.slot_p = S->slot_p.p; C.slot_n = S->slot_n.p;
     C.L_a = S->L_a.p; C.L_b = S->L_b.p; C.L_bo = S->L_bo.p; C.L_ba = S->L_ba.p; C.L_bb = S->L_bb.p; C.L_p = S->L_p.p; C.L_n = S->L_n.p;
     cudaEvent_t g0 = nullptr, g1 = nullptr;

@@ -294,7 +294,9 @@ static cudaError_t setup_launch(sf_world *w, uint32_t base, const uint32_t *list
     return cudaGetLastError();
 }
 cudaError_t setup_bodies(sf_world *w, uint32_t base, uint32_t nb, const float *d_pose13) {
-    return setup_launch(w, base, nullptr, nb, d_pose13, 13u);
+    const cudaError_t e = setup_launch(w, base, nullptr, nb, d_pose13, 13u);
+    if (e != cudaSuccess) return e;
+    return body_load_setup(w, nullptr, base, nb, nullptr);
 }
 cudaError_t setup_bodies_from_local(sf_world *w, const uint32_t *d_list, uint32_t n, const float *d_pose22) {
     return setup_launch(w, 0u, d_list, n, d_pose22, 22u);
@@ -563,6 +565,17 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
         SF_CUDA(w->b_dirty.alloc(nb));
         SF_CUDA(cudaMemsetAsync(w->b_dirty.p, 0, w->b_dirty.bytes(), st));
         SF_CUDA(body_bonds(w.get()));
+        // the debris-body load field: potentials and loads start at 0, no contact has supported a brick yet
+        const size_t ndd = std::max<uint64_t>(nd, 1);
+        SF_CUDA(w->k_sup.alloc(ndd)); SF_CUDA(w->k_phi64.alloc(ndd)); SF_CUDA(w->k_phi.alloc(ndd)); SF_CUDA(w->k_ext.alloc(ndd));
+        SF_CUDA(w->b_vlast.alloc(nb)); SF_CUDA(w->b_wlast.alloc(nb)); SF_CUDA(w->b_resid.alloc(nb));
+        SF_CUDA(w->b_nmax.alloc(nb)); SF_CUDA(w->b_lt.alloc(nb));
+        SF_CUDA(cudaMemsetAsync(w->k_sup.p, 0, w->k_sup.bytes(), st));
+        SF_CUDA(cudaMemsetAsync(w->k_phi64.p, 0, w->k_phi64.bytes(), st));
+        SF_CUDA(cudaMemsetAsync(w->k_phi.p, 0, w->k_phi.bytes(), st));
+        SF_CUDA(cudaMemsetAsync(w->k_ext.p, 0, w->k_ext.bytes(), st));
+        SF_CUDA(cudaMemsetAsync(w->b_lt.p, 0, w->b_lt.bytes(), st));
+        SF_CUDA(body_load_setup(w.get(), nullptr, 0u, (uint32_t)nb, nullptr));
     }
     SF_CUDA(w->st_conn.alloc(std::max<uint32_t>(w->n_struct, 1)));
     SF_CUDA(cudaMemsetAsync(w->st_conn.p, 0, w->st_conn.bytes(), st));
@@ -584,6 +597,7 @@ void sf_world_destroy(sf_world *w) {
     conn_destroy(w);
     split_destroy(w);
     damage_destroy(w);
+    bodyload_destroy(w);
     if (w->ev0) cudaEventDestroy(w->ev0);
     if (w->ev1) cudaEventDestroy(w->ev1);
     cudaStream_t s = w->own_stream;

@@ -174,6 +174,35 @@ def loose_debris(n: int, seed: int, box_lo=(8.0, 2.0, -5.0), box_hi=(18.0, 12.0,
     return np.arange(n + 1, dtype=np.uint32), xyz, mat, pose
 
 
+def body_blocks(n: int = 3, wx: int = 20, wz: int = 25, h: int = 8, gap: int = 4, mat: int = CONC) -> Scene:
+    """n rectangular concrete blocks of wx x h x wz bricks as bodies standing on the ground in a row along x, gap
+    cells apart, at rest: bodies whose load fields need many sweeps, for the frame's shared sweep budget."""
+    first, xyz = [0], []
+    for k in range(n):
+        x0 = k * (wx + gap)
+        c = np.array([[ORIGIN[0] + x0 + x, y, ORIGIN[2] + z] for y in range(h) for z in range(wz) for x in range(wx)],
+                     np.int32)
+        xyz.append(c)
+        first.append(first[-1] + len(c))
+    pose = np.zeros((n, 13), np.float32)
+    pose[:, 6] = 1.0
+    allx = np.concatenate(xyz)
+    return Scene(body_first=np.array(first, np.uint32), body_brick_xyz=allx,
+                 body_brick_mat=np.full(len(allx), mat, np.uint8), body_pose=pose, name="body_blocks").contiguous()
+
+
+def tilted_beam(length: int = 60, angle_deg: float = 45.0, height: int = 60, rows: int = 1, mat: int = CONC) -> Scene:
+    """A concrete beam of length x rows x 1 bricks as one body, rotated angle_deg about z and dropped from height
+    cells: it lands on one end, and the impact loads its joints past their strength."""
+    c = np.array([[ORIGIN[0] + x, y, ORIGIN[2]] for y in range(rows) for x in range(length)], np.int32)
+    pose = np.zeros((1, 13), np.float32)
+    a = np.float32(np.radians(angle_deg) / 2.0)
+    pose[0, 3:7] = [0.0, 0.0, np.sin(a), np.cos(a)]
+    pose[0, 1] = height * 0.5
+    return Scene(body_first=np.array([0, len(c)], np.uint32), body_brick_xyz=c,
+                 body_brick_mat=np.full(len(c), mat, np.uint8), body_pose=pose, name="tilted_beam").contiguous()
+
+
 def frame5_debris_scene(seed: int = 1, n_debris: int = 1024, removed: bool = False) -> Scene:
     """The 5-storey frame plus 1,024 loose single-brick bodies 2 m above the ground beside it."""
     frame, rm = frame5_structure(seed)
