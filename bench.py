@@ -517,9 +517,10 @@ def plain_compare(sf, scenes, params, stream, args):
 
 def collapse_section(sf, S, args, stream):
     """The 16-storey tower (47,760 bricks) with eight ground columns removed, run frame by frame in the reference's
-    order (substeps with damage on contact, rebuild of the marked bodies, connectivity, the resting loads and the
-    load-path frame, connectivity again; src/lib.rs:3650-3659): wall time per frame with its parts, and the oracle
-    running the same frames in the reference's list order on one host thread."""
+    order (substeps with damage on contact, rebuild of the marked bodies, connectivity, the resting loads, the
+    structures' load-path frame and the debris pieces' load fields and joints, connectivity again;
+    src/lib.rs:3650-3659): wall time per frame with its parts, and the oracle running the same frames in the
+    reference's list order on one host thread."""
     import torch
     tw, rm = S.tower16_structure()
     sc = tw.without_static(rm)
@@ -529,8 +530,9 @@ def collapse_section(sf, S, args, stream):
     w.set_stream(stream.cuda_stream)
     for s in ids:
         w.structure_warm(s)
-    parts = {"step": 0.0, "rebuild": 0.0, "connectivity": 0.0, "load_path": 0.0}
-    tally = {"crushed": 0, "pieces_split": 0, "pieces_detached": 0, "joints_failed": 0}
+    parts = {"step": 0.0, "rebuild": 0.0, "connectivity": 0.0, "load_path": 0.0, "piece_fields": 0.0}
+    tally = {"crushed": 0, "pieces_split": 0, "pieces_detached": 0, "joints_failed": 0, "piece_joints_failed": 0,
+             "piece_bricks_crushed": 0, "piece_brick_updates": 0}
     torch.cuda.synchronize()
     t_all = time.perf_counter()
     ft = []
@@ -543,7 +545,11 @@ def collapse_section(sf, S, args, stream):
         w.structure_loads(ids)
         fr = w.structure_frame(f, ids, dt=DT)
         parts["load_path"] += time.perf_counter() - t
+        t = time.perf_counter(); bf = w.bodies_frame(DT, fr.crushed); parts["piece_fields"] += time.perf_counter() - t
         t = time.perf_counter(); c2, _, _ = w.connectivity(); parts["connectivity"] += time.perf_counter() - t
+        tally["piece_joints_failed"] += int(bf.failed)
+        tally["piece_bricks_crushed"] += int(bf.crushed)
+        tally["piece_brick_updates"] += int(bf.brick_updates)
         tally["pieces_split"] += rb.pieces
         tally["pieces_detached"] += c1.pieces + c2.pieces
         tally["joints_failed"] += int(fr.failed)
@@ -569,7 +575,8 @@ def collapse_section(sf, S, args, stream):
             ow.rebuild_bodies()
             ow.connectivity()
             ow.structure_loads(ids)
-            ow.structure_frame(f, DT, ids)
+            o = ow.structure_frame(f, DT, ids)
+            ow.body_frame(DT, o[6])
             ow.connectivity()
             n = f
             if time.perf_counter() - t0 > args.cpu_seconds:
