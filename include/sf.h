@@ -88,7 +88,18 @@ typedef struct sf_params {
     uint32_t detach_bricks;     /* spare body bricks per scene for those pieces */
     uint32_t damage;            /* 1: damage on contact in every substep (impact_damage, src/lib.rs:1602-1702);
                                    needs spare capacity */
-    uint32_t reserved[3];
+    uint32_t reduce;            /* 1: contact reduction (gpu/gpu_world.js:834-920): a body pair with more than 32
+                                   contacts keeps, per direction to the 26 neighbours of a cube cell, the contact
+                                   whose point reaches furthest along it, and the deepest (ties to the later contact);
+                                   the rest are neither coloured nor solved and carry no impulse. Bounds a pair's
+                                   chunks, so a body resting on thousands of contacts needs few colours */
+    uint32_t warm_start;        /* 1: warm start (gpu/gpu_world.js:557-576, 615-683): a contact found in the last
+                                   substep's table by its key (its brick, the other side's kind and brick, its place
+                                   among the brick's contacts with that brick) starts from 0.8 of that substep's
+                                   normal impulse and friction (projected on its tangents, clamped to the cone),
+                                   applied once before the iterations in the solve's order. The table starts over
+                                   after a rebuild or a detachment moves brick ids */
+    uint32_t reserved[1];
 } sf_params;
 
 typedef struct sf_stats {

@@ -28,7 +28,8 @@ _u64p = C.POINTER(C.c_uint64)
 
 class StepParams(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("substeps", C.c_uint32), ("order", C.c_uint32), ("sleep_mode", C.c_uint32),
-                ("pinch_kill", C.c_uint32), ("chunk", C.c_uint32), ("damage", C.c_uint32)]
+                ("pinch_kill", C.c_uint32), ("chunk", C.c_uint32), ("damage", C.c_uint32), ("reduce", C.c_uint32),
+                ("warm", C.c_uint32)]
 
 
 _lib = None
@@ -204,8 +205,8 @@ class OracleWorld:
         return b, nb
 
     def step(self, dt=1.0 / 60.0, iterations=10, substeps=2, order=ORDER_COLOR, sleep_mode=SLEEP_BODY, pinch_kill=1, chunk=16,
-             damage=0):
-        p = StepParams(iterations, substeps, order, sleep_mode, pinch_kill, chunk, damage)
+             damage=0, reduce=0, warm=0):
+        p = StepParams(iterations, substeps, order, sleep_mode, pinch_kill, chunk, damage, reduce, warm)
         self.lib.ow_step(self.h, float(dt), C.byref(p))
 
     def contacts(self):

@@ -134,12 +134,13 @@ struct Contact {
     uint32_t a, b, bo, ba, bb;
     V n, p, ra, rb, t1, t2;
     float depth, mn, mt1, mt2, jn, jt1, jt2, bias, vn0;
+    uint32_t off;   // 1: left out by the contact reduction (not coloured, not solved, no impulse)
 };
 
 enum { ORDER_LIST = 0, ORDER_COLOR = 1 };
 enum { SLEEP_BODY = 0, SLEEP_ISLAND = 1 };
 
-struct StepParams { uint32_t iterations, substeps, order, sleep_mode, pinch_kill, damage; };
+struct StepParams { uint32_t iterations, substeps, order, sleep_mode, pinch_kill, damage, reduce, warm; };
 
 // manifold priority for the colouring: a fixed mix of the body pair (b' = 0 for the static side, else b + 1)
 static inline uint32_t pair_priority(uint32_t a, uint32_t bp) {
@@ -177,6 +178,13 @@ struct World {
     std::vector<uint32_t> man_a, man_b, man_color, man_start, man_count, man_contacts;
     uint32_t ncolors = 0;
     uint32_t chunk = 16;             // contacts per solve chunk of a body pair (0 = the whole pair)
+    // contact reduction and warm start (off unless the step asks): the last substep's impulses per contact key
+    struct WarmKey { uint64_t k1; uint32_t k2; bool operator==(const WarmKey& o) const { return k1 == o.k1 && k2 == o.k2; } };
+    struct WarmHash { size_t operator()(const WarmKey& k) const { return std::hash<uint64_t>()(k.k1 * 0x9E3779B97F4A7C15ull ^ k.k2); } };
+    struct WarmVal { float jn; V f; };
+    std::unordered_map<WarmKey, WarmVal, WarmHash> warm_tab;
+    bool warm_valid = false;
+    uint32_t reduce = 0, warm = 0;
     uint32_t frame = 0;
     uint64_t would_drop = 0;         // contacts the reference would have dropped past MAXC
     // the per-frame load-path schedule, per structure (src/lib.rs:241: st_warm, st_solved, st_settle, st_resid)
@@ -597,6 +605,7 @@ static void wake_near(World& w, V p, float r) {
 static bool detach_piece(World& w, const std::vector<uint32_t>& lst) {
     const uint32_t n = (uint32_t)lst.size();
     if (w.nbody + 1 > w.cap_bodies || w.nd + n > w.cap_bricks) return false;
+    w.warm_valid = false;   // brick ids move: the warm-start table starts over
     const uint32_t b = w.nbody++;
     w.alive.push_back(0); w.asleep.push_back(0); w.wake.push_back(0);
     w.first.push_back(NONE); w.count.push_back(0); w.nc.push_back(0);
@@ -852,6 +861,7 @@ static void rebuild_bodies(World& w, uint32_t* counts) {
     for (int k = 0; k < 5; k++) counts[k] = 0;
     for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b] && w.dirty[b]) rebuild_body(w, b, counts);
     for (uint32_t b = 0; b < w.nbody; b++) w.dirty[b] = 0;
+    if (counts[0]) w.warm_valid = false;   // brick ids move: the warm-start table starts over
 }
 
 // ---------------------------------------------------------------- the debris-body load field (src/lib.rs:1262-1365)
@@ -1066,7 +1076,67 @@ static void apply_imp(World& w, uint32_t a, uint32_t b, V ra, V rb, V p) {
         w.w[b] = sub(w.w[b], dw2);
     }
 }
+// ---------------------------------------------------------------- contact reduction and warm start
+// The GPU world's two devices for large contact sets (gpu/gpu_world.js:557-576, 834-920), restated for brick
+// contacts and off by default. Warm start: a contact is known from the last substep by its key (its brick, the other
+// side's kind and brick, and its place among the brick's contacts of that kind and brick); WARM_F of its normal
+// impulse and of its friction impulse, projected on the new tangents and clamped to the cone, start the new solve and
+// are applied once before the iterations. Reduction: a body pair with more than 32 contacts keeps, for each of the 26
+// directions to a cube cell's neighbours, the contact whose point lies furthest along it, and the deepest (ties to
+// the later contact); the others are neither coloured nor solved.
+static World::WarmKey warm_key(const Contact& c, uint32_t ord) {
+    const uint32_t kind = c.bb == NONE ? 0u : c.bo == STATIC ? 1u : c.b == STATIC ? 3u : 2u;
+    return World::WarmKey{((uint64_t)c.ba << 32) | (uint64_t)c.bb, (kind << 16) | ord};
+}
+// keys of the list's contacts: a brick's contacts are contiguous, and ord counts the earlier ones with the same kind
+// and other brick
+static std::vector<World::WarmKey> warm_keys(const World& w) {
+    std::vector<World::WarmKey> out(w.cs.size());
+    for (size_t k = 0; k < w.cs.size(); k++) {
+        const Contact& c = w.cs[k];
+        const uint32_t kind = c.bb == NONE ? 0u : c.bo == STATIC ? 1u : c.b == STATIC ? 3u : 2u;
+        uint32_t ord = 0;
+        for (size_t q = k; q-- > 0 && w.cs[q].ba == c.ba;) {
+            const Contact& e = w.cs[q];
+            const uint32_t ek = e.bb == NONE ? 0u : e.bo == STATIC ? 1u : e.b == STATIC ? 3u : 2u;
+            if (ek == kind && e.bb == c.bb) ord++;
+        }
+        out[k] = warm_key(c, ord);
+    }
+    return out;
+}
+static const uint32_t RED_K = 32, RED_D = 26;
+// the share of the last substep's impulses a contact starts from: with the whole of them, the velocity bias that
+// pushed a contact apart is carried too, and a stack of single bricks solved with 1 or 4 iterations toppled; at 0.8
+// it stands, sinking less than from zero (0.022 m against 0.046 m at 1 iteration, 0.012 against 0.017 at 4)
+static const float WARM_F = 0.8f;
+static inline uint32_t f2o(float x) { uint32_t b; std::memcpy(&b, &x, 4); return (b & 0x80000000u) ? ~b : (b | 0x80000000u); }
+// slot k < 26: the point's reach along the k-th direction to a cube cell's neighbours; slot 26: the depth
+static inline float red_score(const Contact& c, uint32_t k) {
+    if (k == RED_D) return c.depth;
+    const uint32_t j = k >= 13 ? k + 1 : k;
+    const float dx = (float)(j % 3) - 1.0f, dy = (float)((j / 3) % 3) - 1.0f, dz = (float)(j / 9) - 1.0f;
+    return c.p[0] * dx + c.p[1] * dy + c.p[2] * dz;
+}
+static inline void warm_apply(World& w, const Contact& c) {
+    apply_imp(w, c.a, c.b, c.ra, c.rb, add(mul(c.n, c.jn), add(mul(c.t1, c.jt1), mul(c.t2, c.jt2))));
+}
+static void warm_store(World& w) {
+    const std::vector<World::WarmKey> keys = warm_keys(w);
+    w.warm_tab.clear();
+    for (size_t k = 0; k < w.cs.size(); k++) {
+        const Contact& c = w.cs[k];
+        if (c.off) continue;
+        w.warm_tab[keys[k]] = World::WarmVal{c.jn, add(mul(c.t1, c.jt1), mul(c.t2, c.jt2))};
+    }
+    w.warm_valid = true;
+}
+
 static void prep_contacts(World& w, float h) {
+    std::vector<World::WarmKey> keys;
+    const bool look = w.warm && w.warm_valid;
+    if (look) keys = warm_keys(w);
+    size_t ci = 0;
     for (Contact& c : w.cs) {
         uint32_t a = c.a;
         c.ra = sub(c.p, w.pos[a]);
@@ -1088,6 +1158,16 @@ static void prep_contacts(World& w, float h) {
         float bias = minf(0.2f / h * maxf(c.depth - 0.01f, 0.0f), 1.0f);
         if (vn < -2.0f) bias = maxf(bias, -0.12f * vn);
         c.bias = bias;
+        if (look) {
+            auto it = w.warm_tab.find(keys[ci]);
+            if (it != w.warm_tab.end()) {
+                const float jn = it->second.jn * WARM_F, lim = MU * jn;
+                c.jn = jn;
+                c.jt1 = clampf(dot(it->second.f, c.t1) * WARM_F, -lim, lim);
+                c.jt2 = clampf(dot(it->second.f, c.t2) * WARM_F, -lim, lim);
+            }
+        }
+        ci++;
     }
 }
 static inline void solve_contact(World& w, Contact& c) {
@@ -1122,6 +1202,35 @@ static void build_manifolds(World& w) {
         return ((uint64_t)c.a << 32) | bp;
     };
     std::stable_sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
+    if (w.reduce) {
+        std::vector<uint32_t> kept;
+        kept.reserve(n);
+        for (size_t s0 = 0; s0 < n;) {
+            size_t e = s0 + 1;
+            while (e < n && key(idx[e]) == key(idx[s0])) e++;
+            if (e - s0 > RED_K) {
+                uint32_t best[RED_D + 1], win[RED_D + 1];
+                for (uint32_t k = 0; k <= RED_D; k++) { best[k] = 0; win[k] = 0; }
+                for (size_t t = s0; t < e; t++)
+                    for (uint32_t k = 0; k <= RED_D; k++) best[k] = std::max(best[k], f2o(red_score(w.cs[idx[t]], k)));
+                for (size_t t = s0; t < e; t++)
+                    for (uint32_t k = 0; k <= RED_D; k++)
+                        if (f2o(red_score(w.cs[idx[t]], k)) == best[k]) win[k] = std::max(win[k], idx[t] + 1);
+                for (size_t t = s0; t < e; t++) {
+                    bool keep = false;
+                    for (uint32_t k = 0; k <= RED_D; k++) keep = keep || win[k] == idx[t] + 1;
+                    Contact& c = w.cs[idx[t]];
+                    if (keep) kept.push_back(idx[t]);
+                    else { c.off = 1; c.jn = 0.0f; c.jt1 = 0.0f; c.jt2 = 0.0f; }
+                }
+            } else {
+                for (size_t t = s0; t < e; t++) kept.push_back(idx[t]);
+            }
+            s0 = e;
+        }
+        idx.swap(kept);
+        n = idx.size();
+    }
     w.man_a.clear(); w.man_b.clear(); w.man_start.clear(); w.man_count.clear(); w.man_contacts = idx;
     // a pair's contacts form chunks of at most K (K = 0: one chunk); the colouring and the solve see chunks
     std::vector<uint32_t> prio;
@@ -1166,7 +1275,7 @@ static void build_manifolds(World& w) {
         if (c + 1 > w.ncolors) w.ncolors = c + 1;
     }
 }
-static void solve_list(World& w) { for (Contact& c : w.cs) solve_contact(w, c); }
+static void solve_list(World& w) { for (Contact& c : w.cs) if (!c.off) solve_contact(w, c); }
 static void solve_colored(World& w) {
     // manifolds of one colour share no awake body, so their order inside a colour does not change the result
     std::vector<std::vector<uint32_t>> bycol(w.ncolors);
@@ -1367,6 +1476,8 @@ static void impact_damage(World& w) {
 }
 
 static void substep(World& w, float h, const StepParams& P) {
+    w.reduce = P.reduce; w.warm = P.warm;
+    if (!P.warm) w.warm_valid = false;
     update_cache(w);
     for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b] && !w.asleep[b]) w.v[b][1] -= GR * h;
     build_hash(w);
@@ -1375,9 +1486,21 @@ static void substep(World& w, float h, const StepParams& P) {
     for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b]) { w.vpre[b] = w.v[b]; w.wpre[b] = w.w[b]; }
     build_manifolds(w);
     islands(w);
+    if (P.warm && P.iterations) {   // the carried impulses, once, in the solve's order
+        if (P.order == ORDER_COLOR) {
+            std::vector<std::vector<uint32_t>> bycol(w.ncolors);
+            for (size_t m = 0; m < w.man_a.size(); m++) bycol[w.man_color[m]].push_back((uint32_t)m);
+            for (auto& lst : bycol)
+                for (uint32_t m : lst)
+                    for (uint32_t t = 0; t < w.man_count[m]; t++) warm_apply(w, w.cs[w.man_contacts[w.man_start[m] + t]]);
+        } else {
+            for (const Contact& c : w.cs) if (!c.off) warm_apply(w, c);
+        }
+    }
     for (uint32_t it = 0; it < P.iterations; it++) {
         if (P.order == ORDER_COLOR) solve_colored(w); else solve_list(w);
     }
+    if (P.warm) warm_store(w);
     pinch_check(w, P.pinch_kill != 0);
     if (P.damage) impact_damage(w);
     integrate(w, h, (int)P.sleep_mode);
@@ -1704,7 +1827,7 @@ static void hc_reduce4(HC& c) {
 // ============================================================================================================
 extern "C" {
 
-struct ow_step_params { uint32_t iterations, substeps, order, sleep_mode, pinch_kill, chunk, damage; };
+struct ow_step_params { uint32_t iterations, substeps, order, sleep_mode, pinch_kill, chunk, damage, reduce, warm; };
 
 void* ow_create(uint32_t n_static, const int32_t* static_xyz, const uint8_t* static_mat, const int32_t* static_sid,
                 const uint8_t* static_infill, uint32_t n_bodies, const uint32_t* body_first, const int32_t* body_brick_xyz,
@@ -1828,7 +1951,7 @@ void ow_get_bonds(void* h, float* bond4, uint32_t* nb6) {
 }
 
 void ow_step(void* h, float dt, const ow_step_params* p) {
-    StepParams P{p->iterations, p->substeps, p->order, p->sleep_mode, p->pinch_kill, p->damage};
+    StepParams P{p->iterations, p->substeps, p->order, p->sleep_mode, p->pinch_kill, p->damage, p->reduce, p->warm};
     ((World*)h)->chunk = p->chunk;
     step(*(World*)h, dt, P);
 }
@@ -1844,7 +1967,8 @@ void ow_contacts_only(void* h, float hsub, int with_prep) {
     islands(*w);
 }
 
-// contacts in list order. ids: a, b, bo, ba, bb (5 u32); f: p3 n3 depth (7 floats); s: jn jt1 jt2 mn mt1 mt2 bias vn0 (8)
+// contacts in list order. ids: a, b, bo, ba, bb (5 u32); f: p3 n3 depth (7 floats); s: jn jt1 jt2 mn mt1 mt2 bias vn0 (8),
+// zeros for a contact the reduction left out
 uint64_t ow_get_contacts(void* h, uint32_t* ids, float* f, float* s) {
     World* w = (World*)h;
     for (size_t k = 0; k < w->cs.size(); k++) {
@@ -1852,6 +1976,7 @@ uint64_t ow_get_contacts(void* h, uint32_t* ids, float* f, float* s) {
         uint32_t* o = ids + k * 5; o[0] = c.a; o[1] = c.b; o[2] = c.bo; o[3] = c.ba; o[4] = c.bb;
         float* g = f + k * 7; for (int t = 0; t < 3; t++) { g[t] = c.p[t]; g[3 + t] = c.n[t]; } g[6] = c.depth;
         float* x = s + k * 8; x[0] = c.jn; x[1] = c.jt1; x[2] = c.jt2; x[3] = c.mn; x[4] = c.mt1; x[5] = c.mt2; x[6] = c.bias; x[7] = c.vn0;
+        if (c.off) for (int t = 0; t < 8; t++) x[t] = 0.0f;
     }
     return w->cs.size();
 }

@@ -55,7 +55,8 @@ class Params(C.Structure):
                 ("pinch_kill", C.c_uint32), ("max_colors", C.c_uint32), ("contact_capacity", C.c_uint32),
                 ("verify", C.c_uint32), ("solve_blocks", C.c_uint32), ("manifold_chunk", C.c_uint32),
                 ("sor_cluster", C.c_uint32), ("detach_bodies", C.c_uint32), ("detach_bricks", C.c_uint32),
-                ("damage", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("damage", C.c_uint32), ("reduce", C.c_uint32), ("warm_start", C.c_uint32),
+                ("reserved", C.c_uint32 * 1)]
 
 
 class Stats(C.Structure):

@@ -225,6 +225,7 @@ __global__ void k_dmg_flags(uint32_t nc, DamageArgs A, uint32_t *flag) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nc) return;
     const uint32_t t = A.invperm[k];
+    if (t == NONE) { flag[k] = 0; return; }   // left out by the contact reduction: no impulse
     const float jn = A.S_j[t].x, vn0 = A.S_rb[t].w;
     const uint32_t ia = A.L_ba[k];
     const uint8_t ma = A.alive[A.k_body[ia]] ? A.k_mat[ia] : 0;

@@ -252,6 +252,7 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
     }
     auto bondf = [](uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; };
 
+    step_warm_invalidate(w);   // brick ids move
     // ---- rebuild_body's walk, body by body
     std::vector<uint32_t> wslots, wrec, freed, ranges, setup_ids;
     std::vector<uint8_t> setup_keep;

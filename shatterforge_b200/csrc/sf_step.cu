@@ -53,6 +53,14 @@ struct StepState {
     DBuf<uint32_t> mflag, mpos, pair_start, cflag, cpos;
     DBuf<uint32_t> man_a, man_b, man_start, man_count, man_prio, man_color, man_round;
     DBuf<float4> S_n, S_t1, S_t2, S_ra, S_rb, S_j;
+    // contact reduction: per pair a big flag and its place among the big pairs, per big pair 27 best scores and 27
+    // winners, per sorted contact a keep flag and its place among the kept
+    DBuf<uint32_t> red_big, red_pos, red_keep, red_kpos, red_slots;
+    // warm start: two open-addressing tables (the last substep's, the one being written), keyed by contact key
+    struct WarmTable { DBuf<uint32_t> claim; DBuf<unsigned long long> k1; DBuf<uint32_t> k2; DBuf<float4> val; uint32_t mask = 0; };
+    WarmTable warm[2];
+    int warm_cur = 0;                // the table the next substep reads
+    bool warm_valid = false;
     // colouring
     DBuf<uint32_t> bm_count, bm_start, bm_fill, bm_list;
     DBuf<uint32_t> masks, vmasks;
@@ -122,7 +130,7 @@ static void prof_mark(sf_world *w) {
 }
 
 enum { DV_CONTACTS = 0, DV_MANIFOLDS = 1, DV_COLORS = 2, DV_ROUNDS = 3, DV_WL0 = 4, DV_WL1 = 5, DV_WL2 = 6,
-       DV_ALIVE = 7, DV_AWAKE = 8, DV_ISLANDS = 9, DV_PAIRS = 10, DV_AWK = 11, DV_INC = 12, DV_N = 16 };
+       DV_ALIVE = 7, DV_AWAKE = 8, DV_ISLANDS = 9, DV_PAIRS = 10, DV_AWK = 11, DV_INC = 12, DV_NBIG = 13, DV_KEPT = 14, DV_N = 16 };
 constexpr int JDS_K = 32;   // the largest manifold chunk: the depth of the solve's contact layout
 
 // ---------------------------------------------------------------- pose cache
@@ -588,6 +596,147 @@ __global__ void k_man_count(const uint32_t *nm_p, uint32_t nc, const uint32_t *m
     man_count[m] = e - man_start[m];
 }
 
+// ---------------------------------------------------------------- contact reduction (gpu/gpu_world.js:834-920)
+// A body pair with more than RED_K contacts keeps, for each of the 26 directions to a cube cell's neighbours, the
+// contact whose point reaches furthest along it, and the deepest; ties go to the later contact in list order. The
+// pair's other contacts leave the sorted list before the manifolds are cut, so they are neither coloured nor solved.
+constexpr uint32_t RED_K = 32, RED_D = 26, RED_S = RED_D + 1;
+__device__ __forceinline__ uint32_t f2o(float x) {
+    const uint32_t b = __float_as_uint(x);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float red_score(float4 p, float depth, uint32_t k) {
+    if (k == RED_D) return depth;
+    const uint32_t j = k >= 13 ? k + 1 : k;
+    const float dx = (float)(j % 3) - 1.0f, dy = (float)((j / 3) % 3) - 1.0f, dz = (float)(j / 9) - 1.0f;
+    return p.x * dx + p.y * dy + p.z * dz;
+}
+// per pair: more than RED_K contacts (pairs past the count are 0 for the scan)
+__global__ void k_red_big(uint32_t nc, const uint32_t *np_p, const uint32_t *pair_start, uint32_t *big) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nc) return;
+    const uint32_t np = *np_p;
+    uint32_t b = 0;
+    if (p < np) b = ((p + 1 < np ? pair_start[p + 1] : nc) - pair_start[p]) > RED_K ? 1u : 0u;
+    big[p] = b;
+}
+__device__ __forceinline__ uint32_t pair_of(uint32_t t, const uint32_t *flag, const uint32_t *pos) {
+    return pos[t] + flag[t] - 1;
+}
+__global__ void k_red_score(uint32_t nc, const uint32_t *flag, const uint32_t *pos, const uint32_t *big,
+                            const uint32_t *bigpos, const uint32_t *perm, const float4 *L_p, const float4 *L_n,
+                            uint32_t *best) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nc) return;
+    const uint32_t p = pair_of(t, flag, pos);
+    if (!big[p]) return;
+    const uint32_t k = perm[t];
+    const float4 pt = L_p[k];
+    const float depth = L_n[k].w;
+    uint32_t *b = best + (size_t)bigpos[p] * RED_S;
+    for (uint32_t d = 0; d < RED_S; d++) atomicMax(&b[d], f2o(red_score(pt, depth, d)));
+}
+__global__ void k_red_pick(uint32_t nc, const uint32_t *flag, const uint32_t *pos, const uint32_t *big,
+                           const uint32_t *bigpos, const uint32_t *perm, const float4 *L_p, const float4 *L_n,
+                           const uint32_t *best, uint32_t *win) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nc) return;
+    const uint32_t p = pair_of(t, flag, pos);
+    if (!big[p]) return;
+    const uint32_t k = perm[t];
+    const float4 pt = L_p[k];
+    const float depth = L_n[k].w;
+    const size_t o = (size_t)bigpos[p] * RED_S;
+    for (uint32_t d = 0; d < RED_S; d++)
+        if (f2o(red_score(pt, depth, d)) == best[o + d]) atomicMax(&win[o + d], k + 1);
+}
+__global__ void k_red_keep(uint32_t nc, const uint32_t *flag, const uint32_t *pos, const uint32_t *big,
+                           const uint32_t *bigpos, const uint32_t *perm, const uint32_t *win, uint32_t *keep) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nc) return;
+    const uint32_t p = pair_of(t, flag, pos);
+    uint32_t on = 1;
+    if (big[p]) {
+        on = 0;
+        const uint32_t k = perm[t];
+        const size_t o = (size_t)bigpos[p] * RED_S;
+        for (uint32_t d = 0; d < RED_S; d++) on |= win[o + d] == k + 1 ? 1u : 0u;
+    }
+    keep[t] = on;
+}
+__global__ void k_red_compact(uint32_t nc, const uint32_t *keep, const uint32_t *kpos, const uint32_t *perm,
+                              const uint64_t *key, uint32_t *perm2, uint64_t *key2) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nc && keep[t]) { perm2[kpos[t]] = perm[t]; key2[kpos[t]] = key[t]; }
+}
+
+// ---------------------------------------------------------------- warm start (gpu/gpu_world.js:557-576, 615-683)
+// A contact's key: its brick, the other side's kind (0 ground, 1 static brick, 2 awake body's brick, 3 sleeping
+// body's brick) and brick, and its place among its brick's earlier contacts of that kind and brick (a brick's
+// contacts are contiguous in the list).
+__device__ __forceinline__ uint32_t contact_kind(uint32_t b, uint32_t bo, uint32_t bb) {
+    return bb == NONE ? 0u : bo == STATIC ? 1u : b == STATIC ? 3u : 2u;
+}
+__device__ __forceinline__ void warm_key(uint32_t k, const uint32_t *L_b, const uint32_t *L_bo, const uint32_t *L_ba,
+                                         const uint32_t *L_bb, unsigned long long &k1, uint32_t &k2) {
+    const uint32_t ba = L_ba[k], bb = L_bb[k];
+    const uint32_t kind = contact_kind(L_b[k], L_bo[k], bb);
+    uint32_t ord = 0;
+    for (uint32_t q = k; q-- > 0 && L_ba[q] == ba;)
+        if (L_bb[q] == bb && contact_kind(L_b[q], L_bo[q], L_bb[q]) == kind) ord++;
+    k1 = ((unsigned long long)ba << 32) | bb;
+    k2 = (kind << 16) | ord;
+}
+__device__ __forceinline__ uint32_t warm_hash(unsigned long long k1, uint32_t k2) {
+    unsigned long long h = k1 * 0x9E3779B97F4A7C15ull ^ ((unsigned long long)k2 * 0xC2B2AE3D27D4EB4Full);
+    h ^= h >> 29; h *= 0xBF58476D1CE4E5B9ull; h ^= h >> 32;
+    return (uint32_t)h;
+}
+// the share of the last substep's impulses a contact starts from (the whole carried the velocity bias too, and
+// stacks of single bricks solved with few iterations toppled)
+constexpr float WARM_F = 0.8f;
+struct WarmRef {
+    const uint32_t *claim;
+    const unsigned long long *k1;
+    const uint32_t *k2;
+    const float4 *val;
+    uint32_t mask;
+};
+// the slot holding the key, or NONE (an empty slot ends the probe; keys are unique)
+__device__ __forceinline__ uint32_t warm_find(const WarmRef &T, unsigned long long k1, uint32_t k2) {
+    uint32_t s = warm_hash(k1, k2) & T.mask;
+    for (uint32_t probe = 0; probe < 64; probe++) {
+        if (T.claim[s] == 0) return NONE;
+        if (T.k1[s] == k1 && T.k2[s] == k2) return s;
+        s = (s + 1) & T.mask;
+    }
+    return NONE;
+}
+// after the solve: every solved contact's normal impulse and friction vector under its key
+__global__ void k_warm_store(uint32_t nc, const uint32_t *invperm, const uint32_t *L_b, const uint32_t *L_bo,
+                             const uint32_t *L_ba, const uint32_t *L_bb, const float4 *S_t1, const float4 *S_t2,
+                             const float4 *S_j, uint32_t *claim, unsigned long long *tk1, uint32_t *tk2, float4 *val,
+                             uint32_t mask, uint32_t *err) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nc) return;
+    const uint32_t d = invperm[k];
+    if (d == NONE) return;
+    unsigned long long k1;
+    uint32_t k2;
+    warm_key(k, L_b, L_bo, L_ba, L_bb, k1, k2);
+    const float4 j = S_j[d], a = S_t1[d], b = S_t2[d];
+    const V3 f = add(mul(v3(a.x, a.y, a.z), j.y), mul(v3(b.x, b.y, b.z), j.z));
+    uint32_t s = warm_hash(k1, k2) & mask;
+    for (uint32_t probe = 0; probe < 64; probe++) {
+        if (atomicCAS(&claim[s], 0u, 1u) == 0u) {
+            tk1[s] = k1; tk2[s] = k2; val[s] = make_float4(j.x, f.x, f.y, f.z);
+            return;
+        }
+        s = (s + 1) & mask;
+    }
+    atomicOr(err, (unsigned)ERR_CAPACITY_CONTACTS);   // the table is sized so this cannot happen
+}
+
 // each domain's manifolds form one run (manifolds are ordered by body, bodies by scene, domains are runs of scenes)
 __global__ void k_dom_ranges(const uint32_t *nm_p, const uint32_t *man_dom, uint32_t *m0, uint32_t *m1) {
     const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -615,6 +764,10 @@ struct PrepArgs {
     const float *im, *iiw;
     float4 *S_n, *S_t1, *S_t2, *S_ra, *S_rb, *S_j;
     uint32_t *invperm;
+    // warm start: the last substep's table, read when `warm` is set
+    int warm;
+    WarmRef wt;
+    const uint32_t *L_b, *L_bo, *L_ba, *L_bb;
 };
 
 // One thread per manifold, in colour-list order (position p of segment c, a (domain, colour) pair): the two bodies
@@ -684,7 +837,20 @@ __global__ void k_prep(PrepArgs A) {
         A.S_t2[d] = make_float4(t2.x, t2.y, t2.z, mt2);
         A.S_ra[d] = make_float4(ra.x, ra.y, ra.z, bias);
         A.S_rb[d] = make_float4(rb.x, rb.y, rb.z, vn0);
-        A.S_j[d] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float4 j0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (A.warm) {
+            unsigned long long k1;
+            uint32_t k2;
+            warm_key(k, A.L_b, A.L_bo, A.L_ba, A.L_bb, k1, k2);
+            const uint32_t sl = warm_find(A.wt, k1, k2);
+            if (sl != NONE) {
+                const float4 o = A.wt.val[sl];
+                const float jn = o.x * WARM_F, lim = MU * jn;
+                const V3 f = v3(o.y, o.z, o.w);
+                j0 = make_float4(jn, clampf(dot(f, t1) * WARM_F, -lim, lim), clampf(dot(f, t2) * WARM_F, -lim, lim), 0.0f);
+            }
+        }
+        A.S_j[d] = j0;
         A.invperm[k] = d;
     }
 }
@@ -897,6 +1063,7 @@ struct SolveArgs {
     const float *im, *iiw;
     GridBarrier *gb;
     uint32_t *err;
+    uint32_t warm;                 // 1: a first pass applies the warm-started impulses
 };
 
 // Body velocities and impulses written by other blocks are read through L2 (__ldcg) in the grid-wide solve; in the
@@ -985,6 +1152,48 @@ __device__ __forceinline__ void solve_manifold(const SolveArgs &A, uint32_t m, u
     }
 }
 
+// the warm-started impulses of a manifold's contacts, applied once in its order (apply_imp with the whole impulse)
+template <bool ONE_BLOCK>
+__device__ __forceinline__ void warm_manifold(const SolveArgs &A, uint32_t m, uint32_t p, const uint32_t *off) {
+    const uint32_t a = A.man_a[m], b = A.man_b[m];
+    const bool hasb = b != STATIC;
+    const uint32_t cnt = A.man_count[m];
+    float4 t4 = ld_rw<ONE_BLOCK>(&A.v[a]);
+    V3 va = v3(t4.x, t4.y, t4.z);
+    t4 = ld_rw<ONE_BLOCK>(&A.w[a]);
+    V3 wa = v3(t4.x, t4.y, t4.z);
+    const float ima = A.im[a];
+    float ia[9], ib[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) ia[q] = A.iiw[(size_t)a * 9 + q];
+    V3 vb = v3(0.0f, 0.0f, 0.0f), wb = v3(0.0f, 0.0f, 0.0f);
+    float imb = 0.0f;
+    if (hasb) {
+        t4 = ld_rw<ONE_BLOCK>(&A.v[b]); vb = v3(t4.x, t4.y, t4.z);
+        t4 = ld_rw<ONE_BLOCK>(&A.w[b]); wb = v3(t4.x, t4.y, t4.z);
+        imb = A.im[b];
+#pragma unroll
+        for (int q = 0; q < 9; q++) ib[q] = A.iiw[(size_t)b * 9 + q];
+    }
+    for (uint32_t k = 0; k < cnt; k++) {
+        const uint32_t at = off[k] + p;
+        const float4 n4 = __ldg(&A.S_n[at]), t14 = __ldg(&A.S_t1[at]), t24 = __ldg(&A.S_t2[at]);
+        const float4 ra4 = __ldg(&A.S_ra[at]), rb4 = __ldg(&A.S_rb[at]), j4 = ld_rw<ONE_BLOCK>(&A.S_j[at]);
+        const V3 ra = v3(ra4.x, ra4.y, ra4.z), rb = v3(rb4.x, rb4.y, rb4.z);
+        const V3 P = add(mul(v3(n4.x, n4.y, n4.z), j4.x),
+                         add(mul(v3(t14.x, t14.y, t14.z), j4.y), mul(v3(t24.x, t24.y, t24.z), j4.z)));
+        va = madd(va, P, ima);
+        wa = add(wa, mv(ia, cross(ra, P)));
+        if (hasb) { vb = madd(vb, P, -imb); wb = sub(wb, mv(ib, cross(rb, P))); }
+    }
+    A.v[a] = make_float4(va.x, va.y, va.z, 0.0f);
+    A.w[a] = make_float4(wa.x, wa.y, wa.z, 0.0f);
+    if (hasb) {
+        A.v[b] = make_float4(vb.x, vb.y, vb.z, 0.0f);
+        A.w[b] = make_float4(wb.x, wb.y, wb.z, 0.0f);
+    }
+}
+
 constexpr int SOLVE_BLOCK = 128;
 
 // A colour's manifolds are listed by contact count, most first. Thread g takes position g of even rounds and the
@@ -1003,7 +1212,8 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) k_solve(SolveArgs A) {
     const uint32_t ncol = A.dom_ncol[d];
     const uint32_t stride = nblk * blockDim.x;
     const uint32_t g = bd.y * blockDim.x + threadIdx.x;
-    for (uint32_t it = 0; it < A.iterations; it++) {
+    for (uint32_t it = 0; it < A.iterations + A.warm; it++) {
+        const bool wp = A.warm && it == 0;
         for (uint32_t c = 0; c < ncol; c++) {
             const uint32_t seg = d * A.cstride + c;
             if (threadIdx.x < JDS_K) off[threadIdx.x] = A.jds_off[(size_t)seg * JDS_K + threadIdx.x];
@@ -1011,7 +1221,10 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) k_solve(SolveArgs A) {
             const uint32_t s0 = A.col_start[seg], n = A.col_start[seg + 1] - s0;
             for (uint32_t r = 0; r * stride < n; r++) {
                 const uint32_t p = snake_pos(r, g, stride);
-                if (p < n) solve_manifold<false>(A, A.col_list[s0 + p], p, off);
+                if (p < n) {
+                    if (wp) warm_manifold<false>(A, A.col_list[s0 + p], p, off);
+                    else solve_manifold<false>(A, A.col_list[s0 + p], p, off);
+                }
             }
             if (!dom_sync(A.gb + d, nblk, A.err)) return;
         }
@@ -1024,14 +1237,18 @@ constexpr uint32_t SOLVE_ONE_BLOCK_MAX_CONTACTS = 8192;
 __global__ void __launch_bounds__(SOLVE_ONE_BLOCK) k_solve_one_block(SolveArgs A) {
     __shared__ uint32_t off[JDS_K];
     const uint32_t ncol = A.dev[DV_COLORS];
-    for (uint32_t it = 0; it < A.iterations; it++) {
+    for (uint32_t it = 0; it < A.iterations + A.warm; it++) {
+        const bool wp = A.warm && it == 0;
         for (uint32_t c = 0; c < ncol; c++) {
             if (threadIdx.x < JDS_K) off[threadIdx.x] = A.jds_off[c * JDS_K + threadIdx.x];
             __syncthreads();
             const uint32_t s0 = A.col_start[c], n = A.col_start[c + 1] - s0;
             for (uint32_t r = 0; r * blockDim.x < n; r++) {
                 const uint32_t p = snake_pos(r, threadIdx.x, blockDim.x);
-                if (p < n) solve_manifold<true>(A, A.col_list[s0 + p], p, off);
+                if (p < n) {
+                    if (wp) warm_manifold<true>(A, A.col_list[s0 + p], p, off);
+                    else solve_manifold<true>(A, A.col_list[s0 + p], p, off);
+                }
             }
             __syncthreads();
         }
@@ -1372,10 +1589,16 @@ static cudaError_t grow_contacts(StepState *S, uint64_t need) {
     G(man_a); G(man_b); G(man_ca); G(man_cb); G(man_start); G(man_count); G(man_prio); G(man_color); G(man_round); G(man_dom);
     G(S_n); G(S_t1); G(S_t2); G(S_ra); G(S_rb); G(S_j);
     G(wl0); G(wl1); G(col_list);
+    G(red_big); G(red_pos); G(red_keep); G(red_kpos);
 #undef G
+    if ((e = S->red_slots.alloc(2 * 27 * (cap / 33 + 1))) != cudaSuccess) return e;
     if ((e = S->bm_list.alloc(2 * cap)) != cudaSuccess) return e;
     S->capacity = cap;
     return cudaSuccess;
+}
+
+void step_warm_invalidate(sf_world *w) {
+    if (w->step) w->step->warm_valid = false;
 }
 
 sf_status step_create(sf_world *w) {
@@ -1561,7 +1784,9 @@ static sf_status substep(sf_world *w, float h) {
         return SF_ERR_CAPACITY;
     }
     std::fill(S->act_brick_base.begin(), S->act_brick_base.end(), NONE);
+    if (!w->P.warm_start) S->warm_valid = false;
     if (nb == 0 || nd == 0) {
+        S->warm_valid = false;   // no contacts this substep: the next one finds none
         SF_CUDA(cudaMemsetAsync(S->dev.p, 0, DV_ALIVE * sizeof(uint32_t), s));
         SF_CUDA(cudaMemsetAsync(S->dev.p + DV_ISLANDS, 0, (DV_N - DV_ISLANDS) * sizeof(uint32_t), s));
         for (int p = 0; p <= SF_PHASES; p++) prof_mark(w);
@@ -1676,6 +1901,7 @@ static sf_status substep(sf_world *w, float h) {
     const unsigned R = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)w->sms * per_sm,
                                                                          (nc + SOLVE_BLOCK - 1) / SOLVE_BLOCK + 1));
     const uint32_t cstride = w->P.max_colors;
+    uint32_t ncm = nc;   // the contacts that enter the manifolds (fewer after a contact reduction)
     // manifolds
     if (nc) {
         sf_status pst = use_partition(w, R, one_block);
@@ -1690,13 +1916,38 @@ static sf_status substep(sf_world *w, float h) {
         k_man_flags<<<g_nc, 256, 0, s>>>(nc, S->mkey.p, S->mflag.p);
         SF_CUDA(exclusive_scan_u32(S->mflag.p, S->mpos.p, nc, S->dev.p + DV_PAIRS, S->wk, s));
         k_pair_start<<<g_nc, 256, 0, s>>>(nc, S->mflag.p, S->mpos.p, S->pair_start.p);
-        k_chunk_flags<<<g_nc, 256, 0, s>>>(nc, K, S->mflag.p, S->mpos.p, S->pair_start.p, S->cflag.p);
-        SF_CUDA(exclusive_scan_u32(S->cflag.p, S->cpos.p, nc, S->dev.p + DV_MANIFOLDS, S->wk, s));
-        k_man_write<<<g_nc, 256, 0, s>>>(nc, K, S->cflag.p, S->cpos.p, S->mflag.p, S->mpos.p, S->pair_start.p, S->perm.p,
+        if (w->P.reduce) {
+            k_red_big<<<g_nc, 256, 0, s>>>(nc, S->dev.p + DV_PAIRS, S->pair_start.p, S->red_big.p);
+            SF_CUDA(exclusive_scan_u32(S->red_big.p, S->red_pos.p, nc, S->dev.p + DV_NBIG, S->wk, s));
+            SF_CUDA(cudaMemsetAsync(S->red_slots.p, 0, S->red_slots.bytes(), s));
+            uint32_t *best = S->red_slots.p, *win = S->red_slots.p + S->red_slots.n / 2;
+            k_red_score<<<g_nc, 256, 0, s>>>(nc, S->mflag.p, S->mpos.p, S->red_big.p, S->red_pos.p, S->perm.p, S->L_p.p,
+                                             S->L_n.p, best);
+            k_red_pick<<<g_nc, 256, 0, s>>>(nc, S->mflag.p, S->mpos.p, S->red_big.p, S->red_pos.p, S->perm.p, S->L_p.p,
+                                            S->L_n.p, best, win);
+            k_red_keep<<<g_nc, 256, 0, s>>>(nc, S->mflag.p, S->mpos.p, S->red_big.p, S->red_pos.p, S->perm.p, win,
+                                            S->red_keep.p);
+            SF_CUDA(exclusive_scan_u32(S->red_keep.p, S->red_kpos.p, nc, S->dev.p + DV_KEPT, S->wk, s));
+            k_red_compact<<<g_nc, 256, 0, s>>>(nc, S->red_keep.p, S->red_kpos.p, S->perm.p, S->mkey.p, S->perm_alt.p,
+                                               S->mkey_alt.p);
+            S->perm.swap(S->perm_alt);
+            S->mkey.swap(S->mkey_alt);
+            SF_CUDA(cudaMemcpyAsync(S->h_dev + DV_KEPT, S->dev.p + DV_KEPT, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            SF_CUDA(cudaStreamSynchronize(s));
+            ncm = S->h_dev[DV_KEPT];
+            // the pairs again, over the kept contacts (every pair keeps at least one)
+            k_man_flags<<<g_nc, 256, 0, s>>>(ncm, S->mkey.p, S->mflag.p);
+            SF_CUDA(exclusive_scan_u32(S->mflag.p, S->mpos.p, ncm, S->dev.p + DV_PAIRS, S->wk, s));
+            k_pair_start<<<g_nc, 256, 0, s>>>(ncm, S->mflag.p, S->mpos.p, S->pair_start.p);
+            L += 8;
+        }
+        k_chunk_flags<<<g_nc, 256, 0, s>>>(ncm, K, S->mflag.p, S->mpos.p, S->pair_start.p, S->cflag.p);
+        SF_CUDA(exclusive_scan_u32(S->cflag.p, S->cpos.p, ncm, S->dev.p + DV_MANIFOLDS, S->wk, s));
+        k_man_write<<<g_nc, 256, 0, s>>>(ncm, K, S->cflag.p, S->cpos.p, S->mflag.p, S->mpos.p, S->pair_start.p, S->perm.p,
                                          S->L_a.p, S->L_b.p, S->body_off_of_body.p, S->cidx.p, w->b_scene.p, S->scene_act.p,
                                          S->dom_of_act.p, S->man_a.p, S->man_b.p, S->man_ca.p, S->man_cb.p, S->man_start.p,
                                          S->man_prio.p, S->man_dom.p);
-        k_man_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, nc, S->man_start.p, S->man_count.p);
+        k_man_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, ncm, S->man_start.p, S->man_count.p);
         SF_CUDA(cudaMemsetAsync(S->dom_m0.p, 0, (size_t)D * 4, s));
         SF_CUDA(cudaMemsetAsync(S->dom_m1.p, 0, (size_t)D * 4, s));
         k_dom_ranges<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_dom.p, S->dom_m0.p, S->dom_m1.p);
@@ -1751,6 +2002,12 @@ static sf_status substep(sf_world *w, float h) {
         PA.pos = w->b_pos.p; PA.v = w->b_v.p; PA.w = w->b_w.p; PA.im = w->b_im.p; PA.iiw = w->b_iiw.p;
         PA.S_n = S->S_n.p; PA.S_t1 = S->S_t1.p; PA.S_t2 = S->S_t2.p; PA.S_ra = S->S_ra.p; PA.S_rb = S->S_rb.p; PA.S_j = S->S_j.p;
         PA.invperm = S->invperm.p;
+        const bool warm_read = w->P.warm_start && S->warm_valid;
+        const StepState::WarmTable &WT = S->warm[S->warm_cur];
+        PA.warm = warm_read ? 1 : 0;
+        PA.wt = WarmRef{WT.claim.p, WT.k1.p, WT.k2.p, WT.val.p, WT.mask};
+        PA.L_b = S->L_b.p; PA.L_bo = S->L_bo.p; PA.L_ba = S->L_ba.p; PA.L_bb = S->L_bb.p;
+        if (w->P.reduce) SF_CUDA(cudaMemsetAsync(S->invperm.p, 0xFF, (size_t)nc * 4, s));   // left out: no slot
         k_prep<<<g_nc, 256, 0, s>>>(PA);
         L++;
     } else {
@@ -1767,6 +2024,7 @@ static sf_status substep(sf_world *w, float h) {
         A.jds_off = S->jds_off.p; A.man_a = S->man_a.p; A.man_b = S->man_b.p; A.man_count = S->man_count.p;
         A.S_n = S->S_n.p; A.S_t1 = S->S_t1.p; A.S_t2 = S->S_t2.p; A.S_ra = S->S_ra.p; A.S_rb = S->S_rb.p; A.S_j = S->S_j.p;
         A.v = w->b_v.p; A.w = w->b_w.p; A.im = w->b_im.p; A.iiw = w->b_iiw.p; A.gb = S->dom_gb.p; A.err = w->err.p;
+        A.warm = w->P.warm_start ? 1u : 0u;
         if (one_block) {
             k_solve_one_block<<<1, SOLVE_ONE_BLOCK, 0, s>>>(A);
         } else {
@@ -1778,7 +2036,27 @@ static sf_status substep(sf_world *w, float h) {
         }
         L++;
         S->solve_launches++;
-        S->solve_contact_iters += (uint64_t)nc * w->P.iterations;
+        S->solve_contact_iters += (uint64_t)ncm * w->P.iterations;
+    }
+    if (w->P.warm_start) {
+        // the table the next substep reads: every solved contact's impulses under its key
+        if (nc) {
+            StepState::WarmTable &T = S->warm[S->warm_cur ^ 1];
+            uint64_t want = 1024;
+            while (want < 4ull * nc) want <<= 1;
+            if ((uint64_t)T.mask + 1 < want) {
+                SF_CUDA(T.claim.alloc(want)); SF_CUDA(T.k1.alloc(want)); SF_CUDA(T.k2.alloc(want)); SF_CUDA(T.val.alloc(want));
+                T.mask = (uint32_t)(want - 1);
+            }
+            SF_CUDA(cudaMemsetAsync(T.claim.p, 0, ((size_t)T.mask + 1) * 4, s));
+            k_warm_store<<<g_nc, 256, 0, s>>>(nc, S->invperm.p, S->L_b.p, S->L_bo.p, S->L_ba.p, S->L_bb.p, S->S_t1.p,
+                                              S->S_t2.p, S->S_j.p, T.claim.p, T.k1.p, T.k2.p, T.val.p, T.mask, w->err.p);
+            L++;
+            S->warm_cur ^= 1;
+            S->warm_valid = true;
+        } else {
+            S->warm_valid = false;
+        }
     }
     prof_mark(w);
     // islands over the manifolds of this substep
@@ -2015,8 +2293,11 @@ sf_status sf_read_contacts(sf_world *w, uint32_t scene, uint32_t *ids5, float *f
         SF_CUDA(cudaStreamSynchronize(s));
     }
     std::vector<float4> sn, st1, st2, sra, srb, sj;
-    if (s8 && cnt) {
-        uint32_t mlo = *std::min_element(inv.begin(), inv.end()), mhi = *std::max_element(inv.begin(), inv.end()) + 1;
+    // contacts the reduction left out have no slot (NONE) and read as zeros
+    bool any_slot = false;
+    uint32_t mlo = NONE, mhi = 0;
+    for (uint32_t x : inv) if (x != NONE) { any_slot = true; mlo = std::min(mlo, x); mhi = std::max(mhi, x + 1); }
+    if (s8 && cnt && any_slot) {
         size_t m = mhi - mlo;
         sn.resize(m); st1.resize(m); st2.resize(m); sra.resize(m); srb.resize(m); sj.resize(m);
         SF_CUDA(cudaMemcpyAsync(sn.data(), S->S_n.p + mlo, m * 16, cudaMemcpyDeviceToHost, s));
@@ -2026,7 +2307,7 @@ sf_status sf_read_contacts(sf_world *w, uint32_t scene, uint32_t *ids5, float *f
         SF_CUDA(cudaMemcpyAsync(srb.data(), S->S_rb.p + mlo, m * 16, cudaMemcpyDeviceToHost, s));
         SF_CUDA(cudaMemcpyAsync(sj.data(), S->S_j.p + mlo, m * 16, cudaMemcpyDeviceToHost, s));
         SF_CUDA(cudaStreamSynchronize(s));
-        for (auto &x : inv) x -= mlo;
+        for (auto &x : inv) if (x != NONE) x -= mlo;
     }
     auto loc_body = [&](uint32_t g) { return g == STATIC ? STATIC : g - sc.body_off; };
     auto loc_dyn = [&](uint32_t g) { return sc.n_static + (g - sc.brick_off); };
@@ -2045,6 +2326,7 @@ sf_status sf_read_contacts(sf_world *w, uint32_t scene, uint32_t *ids5, float *f
         if (s8) {
             uint32_t t = inv[k];
             float *x = s8 + k * 8;
+            if (t == NONE || !any_slot) { for (int q = 0; q < 8; q++) x[q] = 0.0f; continue; }
             x[0] = sj[t].x; x[1] = sj[t].y; x[2] = sj[t].z; x[3] = sn[t].w; x[4] = st1[t].w; x[5] = st2[t].w; x[6] = sra[t].w; x[7] = srb[t].w;
         }
     }
