@@ -30,7 +30,8 @@
 
 namespace sf {
 
-constexpr int BL_SOR_THREADS = 256;
+constexpr int BL_SOR_THREADS = 256, BL_SOR_BIG_THREADS = 1024;
+constexpr uint32_t BL_BIG = 2048;   // bricks from which a body's sweeps take the larger block
 constexpr int64_t BL_BUDGET = 160000;   // brick updates a frame, per scene (src/lib.rs:1305)
 constexpr uint8_t BJ_HOLD = 0, BJ_FATIGUE = 1, BJ_FAIL = 2, BJ_CRUSH = 3, BJ_ABSENT = 255;
 
@@ -51,6 +52,8 @@ struct BodyLoadState {
     DBuf<uint8_t> j_dec;
     DBuf<uint32_t> j_crushed;
     DBuf<uint32_t> cand;          // per body brick: a joint decision changes something
+    DBuf<uint32_t> cpos, clist;   // their places, and the list of them ascending
+    Work wk;
     DBuf<uint32_t> jl, njl;       // judged bodies, ascending
     DBuf<uint32_t> counters;      // joints, over, failed, crushed, crushes after the pass, largest ratio's bits
     DBuf<uint32_t> maxr_bits;
@@ -178,10 +181,12 @@ __device__ __forceinline__ double body_update(const BodySorArgs &A, uint32_t b, 
 }
 
 // One block per listed body: red-black sweeps of its bricks (parity of the body lattice cell) until, after at least
-// 2, the residual max |dphi| / max(phi, 1) is below 4e-4, or 60 sweeps, or its cap
-__global__ void __launch_bounds__(BL_SOR_THREADS) k_bl_sor(const uint32_t *list, const uint32_t *caps, BodySorArgs A,
-                                                         uint32_t *sweeps_out, double *resid_out) {
-    __shared__ unsigned long long s_d[BL_SOR_THREADS / 32], s_p[BL_SOR_THREADS / 32];
+// 2, the residual max |dphi| / max(phi, 1) is below 4e-4, or 60 sweeps, or its cap. Bodies of BL_BIG bricks or more
+// take blocks of 1,024 threads, the rest 256 (the order inside a half-sweep does not change the result).
+template <int T>
+__global__ void __launch_bounds__(T) k_bl_sor(const uint32_t *list, const uint32_t *caps, BodySorArgs A,
+                                              uint32_t *sweeps_out, double *resid_out) {
+    __shared__ unsigned long long s_d[T / 32], s_p[T / 32];
     __shared__ int s_stop;
     __shared__ double s_r;
     const uint32_t b = list[blockIdx.x];
@@ -341,45 +346,46 @@ __device__ __forceinline__ bool bjoint_later(uint32_t i2, int a2, uint32_t i, in
 // The decisions in the reference's order: bodies ascending, each body's bricks in list order (its slots), each
 // brick's +x, +y, +z joint. A crush (while the frame's budget of 300 lasts, else a failure) removes the weaker brick
 // and ends that brick's pass; later joints touching the removed brick disappear.
-__global__ void k_bl_joint_apply(const uint32_t *jl, const uint32_t *njl_p, const uint32_t *first, const uint32_t *count,
-                                 uint32_t crush_used, const uint32_t *cand, const uint32_t *knb6, uint8_t *kmat,
-                                 float *kbond, uint8_t *dec, const float *bond_after, const uint32_t *crushed,
-                                 uint8_t *dirty, uint32_t *counters) {
+__global__ void k_bl_joint_apply(const uint32_t *clist, const uint32_t *ncand_p, const uint32_t *kbody,
+                                 uint32_t crush_used, const uint32_t *knb6, uint8_t *kmat, float *kbond, uint8_t *dec,
+                                 const float *bond_after, const uint32_t *crushed, uint8_t *dirty, uint32_t *counters) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     uint32_t crush_n = crush_used;
-    const uint32_t nj = *njl_p;
-    for (uint32_t q = 0; q < nj; q++) {
-        const uint32_t b = jl[q], f = first[b], c = count[b];
-        for (uint32_t t = 0; t < c; t++) {
-            const uint32_t i = f + t;
-            if (!cand[i]) continue;
-            for (int a = 0; a < 3; a++) {
-                const size_t o = (size_t)i * 3 + a;
-                uint8_t d = dec[o];
-                if (d == BJ_ABSENT || d == BJ_HOLD) continue;
-                if (kmat[i] == 0) { dec[o] = BJ_ABSENT; continue; }
-                if (d == BJ_CRUSH) {
-                    if (crush_n >= 300) { d = BJ_FAIL; dec[o] = BJ_FAIL; }
-                    else {
-                        crush_n++;
-                        const uint32_t k = crushed[o];
-                        kmat[k] = 0;
-                        dirty[b] = 1;
-                        for (int a2 = a + 1; a2 < 3; a2++) dec[(size_t)i * 3 + a2] = BJ_ABSENT;
-                        if (k > i) for (int a2 = 0; a2 < 3; a2++) dec[(size_t)k * 3 + a2] = BJ_ABSENT;
-                        for (int a2 = 0; a2 < 3; a2++) {
-                            const uint32_t i2 = knb6[(size_t)k * 6 + a2 * 2 + 1];
-                            if (i2 != NONE && bjoint_later(i2, a2, i, a)) dec[(size_t)i2 * 3 + a2] = BJ_ABSENT;
-                        }
-                        break;
+    const uint32_t n = *ncand_p;
+    // the bricks with a joint decision that changes something, ascending: bodies' brick ranges ascend with their ids,
+    // so this is body order and, in each body, list order
+    for (uint32_t q = 0; q < n; q++) {
+        const uint32_t i = clist[q], b = kbody[i];
+        for (int a = 0; a < 3; a++) {
+            const size_t o = (size_t)i * 3 + a;
+            uint8_t d = dec[o];
+            if (d == BJ_ABSENT || d == BJ_HOLD) continue;
+            if (kmat[i] == 0) { dec[o] = BJ_ABSENT; continue; }
+            if (d == BJ_CRUSH) {
+                if (crush_n >= 300) { d = BJ_FAIL; dec[o] = BJ_FAIL; }
+                else {
+                    crush_n++;
+                    const uint32_t k = crushed[o];
+                    kmat[k] = 0;
+                    dirty[b] = 1;
+                    for (int a2 = a + 1; a2 < 3; a2++) dec[(size_t)i * 3 + a2] = BJ_ABSENT;
+                    if (k > i) for (int a2 = 0; a2 < 3; a2++) dec[(size_t)k * 3 + a2] = BJ_ABSENT;
+                    for (int a2 = 0; a2 < 3; a2++) {
+                        const uint32_t i2 = knb6[(size_t)k * 6 + a2 * 2 + 1];
+                        if (i2 != NONE && bjoint_later(i2, a2, i, a)) dec[(size_t)i2 * 3 + a2] = BJ_ABSENT;
                     }
+                    break;
                 }
-                if (d == BJ_FAIL) { kbond[(size_t)i * 4 + a] = 0.0f; dirty[b] = 1; }
-                else kbond[(size_t)i * 4 + a] = bond_after[o];
             }
+            if (d == BJ_FAIL) { kbond[(size_t)i * 4 + a] = 0.0f; dirty[b] = 1; }
+            else kbond[(size_t)i * 4 + a] = bond_after[o];
         }
     }
     counters[4] = crush_n;
+}
+__global__ void k_bl_cand_list(uint32_t nd, const uint32_t *cand, const uint32_t *cpos, uint32_t *clist) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nd && cand[i]) clist[cpos[i]] = i;
 }
 
 // per judged body brick: its joints that were evaluated (not absent) counted, and the body's largest ratio
@@ -471,7 +477,7 @@ static sf_status bodies_frame_impl(sf_world *w, float dt, uint32_t crush_used, s
         SF_CUDA(B.caps.alloc(nb)); SF_CUDA(B.sweeps.alloc(nb)); SF_CUDA(B.sizes.alloc((size_t)nb * 2)); SF_CUDA(B.cut.alloc(nb)); SF_CUDA(B.resid_out.alloc(nb));
         SF_CUDA(B.phi_save.alloc(nd)); SF_CUDA(B.judged.alloc(nb)); SF_CUDA(B.jlive.alloc(nb)); SF_CUDA(B.jdt.alloc(nb));
         SF_CUDA(B.j_ratio.alloc((size_t)nd * 3)); SF_CUDA(B.j_bond.alloc((size_t)nd * 3)); SF_CUDA(B.j_dec.alloc((size_t)nd * 3));
-        SF_CUDA(B.j_crushed.alloc((size_t)nd * 3)); SF_CUDA(B.cand.alloc(nd)); SF_CUDA(B.jl.alloc(nb)); SF_CUDA(B.njl.alloc(2));
+        SF_CUDA(B.j_crushed.alloc((size_t)nd * 3)); SF_CUDA(B.cand.alloc(nd)); SF_CUDA(B.cpos.alloc(nd)); SF_CUDA(B.clist.alloc(nd)); SF_CUDA(B.jl.alloc(nb)); SF_CUDA(B.njl.alloc(2));
         SF_CUDA(B.counters.alloc(8)); SF_CUDA(B.maxr_bits.alloc(nb));
         B.ready = true;
     }
@@ -508,25 +514,49 @@ static sf_status bodies_frame_impl(sf_world *w, float dt, uint32_t crush_used, s
         k_bl_sizes<<<grid_for(ne, 256), 256, 0, st>>>(ne, B.elig.p, w->b_count.p, w->b_scene.p, B.sizes.p);
         std::vector<uint32_t> sz((size_t)ne * 2);
         SF_CUDA(cudaMemcpyAsync(sz.data(), B.sizes.p, (size_t)ne * 8, cudaMemcpyDeviceToHost, st));
-        // no body can sweep more than the scene's whole budget allows it: the first pass stops there
         SF_CUDA(cudaStreamSynchronize(st));
-        std::vector<uint32_t> cap_a(ne), caps(ne), nat(ne), cut_list, cut_caps;
-        for (uint32_t k = 0; k < ne; k++) {
-            const int64_t size = sz[2 * k];
-            cap_a[k] = (uint32_t)std::min<int64_t>(60, std::max<int64_t>(2, (BL_BUDGET + size - 1) / size));
-        }
-        SF_CUDA(cudaMemcpyAsync(B.caps.p, cap_a.data(), (size_t)ne * 4, cudaMemcpyHostToDevice, st));
-        SF_CUDA(cudaMemcpyAsync(B.phi_save.p, w->k_phi64.p, (size_t)nd * 8, cudaMemcpyDeviceToDevice, st));
         BodySorArgs A;
         A.first = w->b_first.p; A.count = w->b_count.p; A.kbody = w->k_body.p; A.knb6 = w->k_nb6.p; A.sup = w->k_sup.p;
         A.kmat = w->k_mat.p; A.kxyz = w->k_xyz.p; A.kbond = w->k_bond.p; A.rot = w->b_rot.p; A.kext = w->k_ext.p;
         A.phi64 = w->k_phi64.p; A.frame = frame;
-        k_bl_sor<<<ne, BL_SOR_THREADS, 0, st>>>(B.elig.p, B.caps.p, A, B.sweeps.p, B.resid_out.p);
-        k_bl_store<<<grid_for(ne, 256), 256, 0, st>>>(ne, B.elig.p, B.resid_out.p, w->b_resid.p);
-        w->launches += 3;
-        SF_CUDA(cudaGetLastError());
-        SF_CUDA(cudaMemcpyAsync(nat.data(), B.sweeps.p, (size_t)ne * 4, cudaMemcpyDeviceToHost, st));
-        SF_CUDA(cudaStreamSynchronize(st));
+        // the sweeps of listed bodies (ids, caps, sizes in body order): the small bodies' blocks first, then the big
+        // ones'; the residuals stored; returns the sweeps each ran, in body order
+        std::vector<uint32_t> dl, dc, pos_of;
+        auto run_sor = [&](const std::vector<uint32_t> &ids, const std::vector<uint32_t> &cp,
+                           const std::vector<uint32_t> &size, std::vector<uint32_t> &done) -> cudaError_t {
+            const uint32_t n = (uint32_t)ids.size();
+            dl.clear(); dc.clear(); pos_of.assign(n, 0);
+            for (int big = 0; big < 2; big++)
+                for (uint32_t k = 0; k < n; k++)
+                    if ((size[k] >= BL_BIG) == (big == 1)) { pos_of[k] = (uint32_t)dl.size(); dl.push_back(ids[k]); dc.push_back(cp[k]); }
+            const uint32_t n_small = (uint32_t)std::count_if(size.begin(), size.end(), [](uint32_t x) { return x < BL_BIG; });
+            cudaError_t e;
+            if ((e = cudaMemcpyAsync(B.cut.p, dl.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+            if ((e = cudaMemcpyAsync(B.caps.p, dc.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+            if (n_small)
+                k_bl_sor<BL_SOR_THREADS><<<n_small, BL_SOR_THREADS, 0, st>>>(B.cut.p, B.caps.p, A, B.sweeps.p, B.resid_out.p);
+            if (n > n_small)
+                k_bl_sor<BL_SOR_BIG_THREADS><<<n - n_small, BL_SOR_BIG_THREADS, 0, st>>>(
+                    B.cut.p + n_small, B.caps.p + n_small, A, B.sweeps.p + n_small, B.resid_out.p + n_small);
+            k_bl_store<<<grid_for(n, 256), 256, 0, st>>>(n, B.cut.p, B.resid_out.p, w->b_resid.p);
+            w->launches += 3;
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            std::vector<uint32_t> sw(n);
+            if ((e = cudaMemcpyAsync(sw.data(), B.sweeps.p, (size_t)n * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+            done.assign(n, 0);
+            for (uint32_t k = 0; k < n; k++) done[k] = sw[pos_of[k]];
+            return cudaSuccess;
+        };
+        // no body can sweep more than the scene's whole budget allows it: the first pass stops there
+        std::vector<uint32_t> cap_a(ne), caps(ne), nat, size_of(ne), cut_list, cut_caps, cut_size, cut_done;
+        for (uint32_t k = 0; k < ne; k++) {
+            const int64_t size = sz[2 * k];
+            size_of[k] = sz[2 * k];
+            cap_a[k] = (uint32_t)std::min<int64_t>(60, std::max<int64_t>(2, (BL_BUDGET + size - 1) / size));
+        }
+        SF_CUDA(cudaMemcpyAsync(B.phi_save.p, w->k_phi64.p, (size_t)nd * 8, cudaMemcpyDeviceToDevice, st));
+        SF_CUDA(run_sor(list, cap_a, size_of, nat));
         // the budget in body order: a body stops at the first n >= 2 after which the budget is spent
         int64_t budget = BL_BUDGET;
         uint32_t scene = NONE;
@@ -535,7 +565,7 @@ static sf_status bodies_frame_impl(sf_world *w, float dt, uint32_t crush_used, s
             const int64_t size = sz[2 * k];
             const int64_t need = budget <= 0 ? 2 : std::max<int64_t>(2, (budget + size - 1) / size);
             caps[k] = (uint32_t)std::min<int64_t>(nat[k], need);
-            if (caps[k] < nat[k]) { cut_list.push_back(list[k]); cut_caps.push_back(caps[k]); }
+            if (caps[k] < nat[k]) { cut_list.push_back(list[k]); cut_caps.push_back(caps[k]); cut_size.push_back(sz[2 * k]); }
             budget -= (int64_t)caps[k] * size;
             rep.sweeps += caps[k];
             rep.brick_updates += (uint64_t)caps[k] * (uint64_t)size;
@@ -544,12 +574,10 @@ static sf_status bodies_frame_impl(sf_world *w, float dt, uint32_t crush_used, s
         const uint32_t nc = (uint32_t)cut_list.size();
         if (nc) {
             SF_CUDA(cudaMemcpyAsync(B.cut.p, cut_list.data(), (size_t)nc * 4, cudaMemcpyHostToDevice, st));
-            SF_CUDA(cudaMemcpyAsync(B.caps.p, cut_caps.data(), (size_t)nc * 4, cudaMemcpyHostToDevice, st));
             k_bl_mark<<<grid_for(nc, 256), 256, 0, st>>>(nc, B.cut.p, B.judged.p);
             k_bl_restore<<<gd, 256, 0, st>>>(nd, w->k_body.p, B.judged.p, B.phi_save.p, w->k_phi64.p);
-            k_bl_sor<<<nc, BL_SOR_THREADS, 0, st>>>(B.cut.p, B.caps.p, A, B.sweeps.p, B.resid_out.p);
-            k_bl_store<<<grid_for(nc, 256), 256, 0, st>>>(nc, B.cut.p, B.resid_out.p, w->b_resid.p);
-            w->launches += 4;
+            w->launches += 2;
+            SF_CUDA(run_sor(cut_list, cut_caps, cut_size, cut_done));
         }
         k_bl_mark<<<grid_for(ne, 256), 256, 0, st>>>(ne, B.elig.p, B.judged.p);
         k_bl_phi32<<<gd, 256, 0, st>>>(nd, w->k_body.p, w->k_mat.p, B.judged.p, w->k_phi64.p, w->k_phi.p);
@@ -572,19 +600,16 @@ static sf_status bodies_frame_impl(sf_world *w, float dt, uint32_t crush_used, s
     SF_CUDA(cudaMemsetAsync(B.counters.p, 0, B.counters.bytes(), st));
     SF_CUDA(cudaMemsetAsync(B.maxr_bits.p, 0, (size_t)nb * 4, st));
     k_bl_collect<<<gb, 256, 0, st>>>(nb, B.judged.p, B.jl.p, B.njl.p);
-    // the judged bodies ascending, for the ordered pass
     uint32_t nj = 0;
     SF_CUDA(cudaMemcpyAsync(&nj, B.njl.p, 4, cudaMemcpyDeviceToHost, st));
     SF_CUDA(cudaStreamSynchronize(st));
     if (nj) {
-        std::vector<uint32_t> jl(nj);
-        SF_CUDA(cudaMemcpyAsync(jl.data(), B.jl.p, (size_t)nj * 4, cudaMemcpyDeviceToHost, st));
-        SF_CUDA(cudaStreamSynchronize(st));
-        std::sort(jl.begin(), jl.end());
-        SF_CUDA(cudaMemcpyAsync(B.jl.p, jl.data(), (size_t)nj * 4, cudaMemcpyHostToDevice, st));
-        k_bl_joint_apply<<<1, 32, 0, st>>>(B.jl.p, B.njl.p, w->b_first.p, w->b_count.p, crush_used, B.cand.p,
-                                           w->k_nb6.p, w->k_mat.p, w->k_bond.p, B.j_dec.p, B.j_bond.p, B.j_crushed.p,
-                                           w->b_dirty.p, B.counters.p);
+        // the bricks whose decisions change something, ascending, for the ordered pass
+        SF_CUDA(exclusive_scan_u32(B.cand.p, B.cpos.p, nd, B.njl.p + 1, B.wk, st));
+        k_bl_cand_list<<<gd, 256, 0, st>>>(nd, B.cand.p, B.cpos.p, B.clist.p);
+        k_bl_joint_apply<<<1, 32, 0, st>>>(B.clist.p, B.njl.p + 1, w->k_body.p, crush_used, w->k_nb6.p, w->k_mat.p,
+                                           w->k_bond.p, B.j_dec.p, B.j_bond.p, B.j_crushed.p, w->b_dirty.p,
+                                           B.counters.p);
         k_bl_joint_tally<<<gd, 256, 0, st>>>(nd, w->k_body.p, B.judged.p, B.j_dec.p, B.j_ratio.p, B.maxr_bits.p,
                                              B.counters.p);
         k_bl_maxr<<<gb, 256, 0, st>>>(nb, B.judged.p, B.maxr_bits.p, w->b_maxr.p);

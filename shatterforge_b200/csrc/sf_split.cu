@@ -272,8 +272,8 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
             if (R[(size_t)t * SPLIT_WORDS + 3] != 0) lst.push_back(t);
             else rep.removed++;
         }
-        for (uint32_t t = 0; t < cnt; t++) freed.push_back(first + t);   // re-written below where kept
         if (lst.empty()) {
+            for (uint32_t t = 0; t < cnt; t++) freed.push_back(first + t);
             ranges.insert(ranges.end(), {id, 0u, 0u});
             rep.dissolved++;
             continue;
@@ -315,6 +315,8 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
         // stable grouping by component
         std::vector<std::vector<uint32_t>> groups(nc);
         for (uint32_t t : lst) groups[comp[t]].push_back(t);
+        // the first piece stays at the front of the range; the rest of the range is free (new pieces take new slots)
+        for (uint32_t t = (uint32_t)groups[0].size(); t < cnt; t++) freed.push_back(first + t);
         // the new slot of each kept brick
         std::vector<uint32_t> nslot(cnt, NONE);
         std::vector<uint32_t> cbody(nc, NONE), cfirst(nc, 0);
@@ -357,15 +359,6 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
             setup_keep.push_back(c == 0 ? 1 : 0);
             for (int j = 0; j < 22; j++) { float f; std::memcpy(&f, &B[3 + j], 4); poses.push_back(f); }
         }
-    }
-    // slots written again are not free
-    std::sort(freed.begin(), freed.end());
-    {
-        std::vector<uint32_t> ws = wslots;
-        std::sort(ws.begin(), ws.end());
-        std::vector<uint32_t> f2;
-        std::set_difference(freed.begin(), freed.end(), ws.begin(), ws.end(), std::back_inserter(f2));
-        freed.swap(f2);
     }
     // ---- the GPU side
     if (!freed.empty()) {

@@ -61,64 +61,48 @@ __global__ void k_finalize_bricks(uint32_t ns, uint32_t base, const uint32_t *ce
     bmax[(size_t)i * 4 + 3] = f;
 }
 
-// one thread per body, its bricks in list order (the sums must round in the reference's order); bodies
-// base .. base + nb - 1 (or list[0 .. nb - 1]), their parent poses at pose[0 ..], `stride` floats each. Stride 13:
-// the bricks' positions are their lattice cells' centres and the rotation follows from the quaternion (a body set up
-// from a description or a detached piece). Stride 22: the positions are the bricks' current local offsets and the
-// rotation is given after the 13 (rebuild_body passes the parent's cached rotation, src/lib.rs:968, 995).
-__global__ void k_setup_bodies(uint32_t nb, uint32_t base, const uint32_t *list, const uint32_t *first,
-                               const uint32_t *count, const int32_t *xyz, const uint8_t *kmat, const float *pose,
-                               uint32_t stride, float4 *local, float4 *wpos, uint32_t *kbody,
-                               float4 *pos, float4 *q, float4 *v, float4 *w, float *rot, float *iil, float *iiw,
-                               float *m, float *im, float *rad, float *sleep, float *maxr, uint8_t *alive, uint8_t *asleep,
-                               uint8_t *wake) {
-    const uint32_t lb = blockIdx.x * blockDim.x + threadIdx.x;
-    if (lb >= nb) return;
-    const uint32_t b = list ? list[lb] : base + lb;
-    const bool from_local = stride == 22;
-    auto brick_pos = [&](uint32_t i) -> V3 {
-        if (from_local) { const float4 l = local[i]; return v3(l.x, l.y, l.z); }
-        return lat_pos(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
-    };
-    uint32_t s = first[b], n = count[b];
-    if (n == 0) {   // a spare body (capacity for detached pieces) or the sentinel: dead, at rest, finite
-        pos[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f); q[b] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-        v[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f); w[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        for (int k = 0; k < 9; k++) {
-            rot[(size_t)b * 9 + k] = (k % 4 == 0) ? 1.0f : 0.0f;
-            iil[(size_t)b * 9 + k] = 0.0f; iiw[(size_t)b * 9 + k] = 0.0f;
-        }
-        m[b] = 0.0f; im[b] = 0.0f; rad[b] = 0.0f; sleep[b] = 0.0f; maxr[b] = 0.0f;
-        alive[b] = 0; asleep[b] = 0; wake[b] = 0;
-        return;
+// setup_body (src/lib.rs:844-891) for bodies base .. base + nb - 1 (or list[0 .. nb - 1]), their parent poses at
+// pose[0 ..], `stride` floats each. Stride 13: the bricks' positions are their lattice cells' centres and the rotation
+// follows from the quaternion (a body set up from a description or a detached piece). Stride 22: the positions are
+// the bricks' current local offsets and the rotation is given after the 13 (rebuild_body passes the parent's cached
+// rotation, src/lib.rs:968, 995). The mass, centre and inertia sums must round in the reference's order (its bricks
+// in list order): a body of fewer than SETUP_BIG bricks is summed by one thread; a larger one by a block whose
+// threads form each brick's terms in parallel, tile by tile, while one thread adds them up in order.
+constexpr uint32_t SETUP_BIG = 512;
+constexpr int SETUP_T = 256;
+struct SetupArgs {
+    uint32_t nb, base;
+    const uint32_t *list, *first, *count;
+    const int32_t *xyz;
+    const uint8_t *kmat;
+    const float *pose;
+    uint32_t stride;
+    float4 *local, *wpos;
+    uint32_t *kbody;
+    float4 *pos, *q, *v, *w;
+    float *rot, *iil, *iiw, *m, *im, *rad, *sleep, *maxr;
+    uint8_t *alive, *asleep, *wake;
+};
+__device__ __forceinline__ V3 setup_brick_pos(const SetupArgs &A, uint32_t i) {
+    if (A.stride == 22) { const float4 l = A.local[i]; return v3(l.x, l.y, l.z); }
+    return lat_pos(A.xyz[3 * i], A.xyz[3 * i + 1], A.xyz[3 * i + 2]);
+}
+// a spare body (capacity for detached pieces) or the sentinel: dead, at rest, finite
+__device__ void setup_dead(const SetupArgs &A, uint32_t b) {
+    A.pos[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f); A.q[b] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    A.v[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f); A.w[b] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (int k = 0; k < 9; k++) {
+        A.rot[(size_t)b * 9 + k] = (k % 4 == 0) ? 1.0f : 0.0f;
+        A.iil[(size_t)b * 9 + k] = 0.0f; A.iiw[(size_t)b * 9 + k] = 0.0f;
     }
-    float mass = 0.0f;
-    V3 cl = v3(0.0f, 0.0f, 0.0f);
-    for (uint32_t t = 0; t < n; t++) {
-        uint32_t i = s + t;
-        V3 l = brick_pos(i);
-        float mm = c_mat.mass[kmat[i]];
-        mass += mm;
-        cl = madd(cl, l, mm);
-    }
-    cl = mul(cl, div_rn(1.0f, mass));
-    float it[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    float rr_max = 0.0f;
-    const float cube = S * S / 6.0f;
-    for (uint32_t t = 0; t < n; t++) {
-        uint32_t i = s + t;
-        V3 l = brick_pos(i);
-        float mm = c_mat.mass[kmat[i]];
-        V3 r = sub(l, cl);
-        local[i] = make_float4(r.x, r.y, r.z, 0.0f);
-        float rr = dot(r, r);
-        rr_max = maxf(rr_max, rr);
-        it[0] += mm * (rr - r.x * r.x + cube); it[4] += mm * (rr - r.y * r.y + cube); it[8] += mm * (rr - r.z * r.z + cube);
-        it[1] -= mm * r.x * r.y; it[2] -= mm * r.x * r.z; it[5] -= mm * r.y * r.z;
-        kbody[i] = b;
-    }
+    A.m[b] = 0.0f; A.im[b] = 0.0f; A.rad[b] = 0.0f; A.sleep[b] = 0.0f; A.maxr[b] = 0.0f;
+    A.alive[b] = 0; A.asleep[b] = 0; A.wake[b] = 0;
+}
+// the body's own fields from its sums: inverse inertia (minv, src/lib.rs:79-91), pose, velocity, radius; returns the
+// position and rotation its bricks' world positions follow from
+__device__ void setup_tail(const SetupArgs &A, uint32_t lb, uint32_t b, float mass, V3 cl, float *it, float rr_max,
+                           V3 &p, float *prot) {
     it[3] = it[1]; it[6] = it[2]; it[7] = it[5];
-    // minv (src/lib.rs:79-91)
     float inv[9];
     {
         const float *a = it;
@@ -135,32 +119,163 @@ __global__ void k_setup_bodies(uint32_t nb, uint32_t base, const uint32_t *list,
             inv[6] = c2 * id; inv[7] = (a[1] * a[6] - a[0] * a[7]) * id; inv[8] = (a[0] * a[4] - a[1] * a[3]) * id;
         }
     }
-    const float *ps = pose + (size_t)lb * stride;
-    float prot[9];
-    if (from_local) for (int k = 0; k < 9; k++) prot[k] = ps[13 + k];
+    const float *ps = A.pose + (size_t)lb * A.stride;
+    if (A.stride == 22) for (int k = 0; k < 9; k++) prot[k] = ps[13 + k];
     else q_to_m(ps[3], ps[4], ps[5], ps[6], prot);
     V3 off = mv(prot, cl);
-    V3 p = add(v3(ps[0], ps[1], ps[2]), off);
+    p = add(v3(ps[0], ps[1], ps[2]), off);
     V3 pv = v3(ps[7], ps[8], ps[9]), pw = v3(ps[10], ps[11], ps[12]);
     V3 vel = add(pv, cross(pw, off));
-    pos[b] = make_float4(p.x, p.y, p.z, 0.0f);
-    q[b] = make_float4(ps[3], ps[4], ps[5], ps[6]);
-    v[b] = make_float4(vel.x, vel.y, vel.z, 0.0f);
-    w[b] = make_float4(pw.x, pw.y, pw.z, 0.0f);
-    for (int k = 0; k < 9; k++) { rot[(size_t)b * 9 + k] = prot[k]; iil[(size_t)b * 9 + k] = inv[k]; }
+    A.pos[b] = make_float4(p.x, p.y, p.z, 0.0f);
+    A.q[b] = make_float4(ps[3], ps[4], ps[5], ps[6]);
+    A.v[b] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+    A.w[b] = make_float4(pw.x, pw.y, pw.z, 0.0f);
+    for (int k = 0; k < 9; k++) { A.rot[(size_t)b * 9 + k] = prot[k]; A.iil[(size_t)b * 9 + k] = inv[k]; }
     float t1[9], t2[9], t3[9];
     mmul(prot, inv, t1); mtr(prot, t2); mmul(t1, t2, t3);
-    for (int k = 0; k < 9; k++) iiw[(size_t)b * 9 + k] = t3[k];
-    m[b] = mass; im[b] = div_rn(1.0f, mass);
-    rad[b] = sqrt_rn(rr_max) + H * 1.8f;
-    sleep[b] = 0.0f; maxr[b] = 0.0f;
-    alive[b] = 1; asleep[b] = 0; wake[b] = 0;
+    for (int k = 0; k < 9; k++) A.iiw[(size_t)b * 9 + k] = t3[k];
+    A.m[b] = mass; A.im[b] = div_rn(1.0f, mass);
+    A.rad[b] = sqrt_rn(rr_max) + H * 1.8f;
+    A.sleep[b] = 0.0f; A.maxr[b] = 0.0f;
+    A.alive[b] = 1; A.asleep[b] = 0; A.wake[b] = 0;
+}
+// one thread per body of fewer than SETUP_BIG bricks
+__global__ void k_setup_bodies(SetupArgs A) {
+    const uint32_t lb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lb >= A.nb) return;
+    const uint32_t b = A.list ? A.list[lb] : A.base + lb;
+    uint32_t s = A.first[b], n = A.count[b];
+    if (n >= SETUP_BIG) return;
+    if (n == 0) { setup_dead(A, b); return; }
+    float mass = 0.0f;
+    V3 cl = v3(0.0f, 0.0f, 0.0f);
     for (uint32_t t = 0; t < n; t++) {
         uint32_t i = s + t;
-        float4 l = local[i];
-        V3 wp = add(p, mv(prot, v3(l.x, l.y, l.z)));
-        wpos[i] = make_float4(wp.x, wp.y, wp.z, 0.0f);
+        V3 l = setup_brick_pos(A, i);
+        float mm = c_mat.mass[A.kmat[i]];
+        mass += mm;
+        cl = madd(cl, l, mm);
     }
+    cl = mul(cl, div_rn(1.0f, mass));
+    float it[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    float rr_max = 0.0f;
+    const float cube = S * S / 6.0f;
+    for (uint32_t t = 0; t < n; t++) {
+        uint32_t i = s + t;
+        V3 l = setup_brick_pos(A, i);
+        float mm = c_mat.mass[A.kmat[i]];
+        V3 r = sub(l, cl);
+        A.local[i] = make_float4(r.x, r.y, r.z, 0.0f);
+        float rr = dot(r, r);
+        rr_max = maxf(rr_max, rr);
+        it[0] += mm * (rr - r.x * r.x + cube); it[4] += mm * (rr - r.y * r.y + cube); it[8] += mm * (rr - r.z * r.z + cube);
+        it[1] -= mm * r.x * r.y; it[2] -= mm * r.x * r.z; it[5] -= mm * r.y * r.z;
+        A.kbody[i] = b;
+    }
+    V3 p;
+    float prot[9];
+    setup_tail(A, lb, b, mass, cl, it, rr_max, p, prot);
+    for (uint32_t t = 0; t < n; t++) {
+        uint32_t i = s + t;
+        float4 l = A.local[i];
+        V3 wp = add(p, mv(prot, v3(l.x, l.y, l.z)));
+        A.wpos[i] = make_float4(wp.x, wp.y, wp.z, 0.0f);
+    }
+}
+// one block per body of SETUP_BIG bricks or more: each thread forms one brick's products of a tile, thread 0 adds
+// the tile's terms in list order (the same roundings as one thread), then the bricks' offsets and world positions are
+// written in parallel
+__global__ void __launch_bounds__(SETUP_T) k_setup_big(SetupArgs A) {
+    __shared__ float s_t[7][SETUP_T];
+    __shared__ float s_cl[3], s_p[3], s_rot[9];
+    const uint32_t lb = blockIdx.x;
+    const uint32_t b = A.list ? A.list[lb] : A.base + lb;
+    const uint32_t s = A.first[b], n = A.count[b];
+    if (n < SETUP_BIG) return;
+    const uint32_t k = threadIdx.x;
+    float mass = 0.0f;
+    V3 cl = v3(0.0f, 0.0f, 0.0f);
+    for (uint32_t t0 = 0; t0 < n; t0 += SETUP_T) {
+        if (t0 + k < n) {
+            const uint32_t i = s + t0 + k;
+            const V3 l = setup_brick_pos(A, i);
+            const float mm = c_mat.mass[A.kmat[i]];
+            s_t[0][k] = mm; s_t[1][k] = l.x * mm; s_t[2][k] = l.y * mm; s_t[3][k] = l.z * mm;
+        }
+        __syncthreads();
+        if (k == 0) {
+            const uint32_t e = min((uint32_t)SETUP_T, n - t0);
+            for (uint32_t q = 0; q < e; q++) {
+                mass += s_t[0][q];
+                cl = v3(cl.x + s_t[1][q], cl.y + s_t[2][q], cl.z + s_t[3][q]);
+            }
+        }
+        __syncthreads();
+    }
+    if (k == 0) {
+        cl = mul(cl, div_rn(1.0f, mass));
+        s_cl[0] = cl.x; s_cl[1] = cl.y; s_cl[2] = cl.z;
+    }
+    __syncthreads();
+    cl = v3(s_cl[0], s_cl[1], s_cl[2]);
+    float it[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    float rr_max = 0.0f;
+    const float cube = S * S / 6.0f;
+    for (uint32_t t0 = 0; t0 < n; t0 += SETUP_T) {
+        if (t0 + k < n) {
+            const uint32_t i = s + t0 + k;
+            const V3 l = setup_brick_pos(A, i);
+            const float mm = c_mat.mass[A.kmat[i]];
+            const V3 r = sub(l, cl);
+            const float rr = dot(r, r);
+            s_t[0][k] = mm * (rr - r.x * r.x + cube); s_t[1][k] = mm * (rr - r.y * r.y + cube);
+            s_t[2][k] = mm * (rr - r.z * r.z + cube);
+            s_t[3][k] = mm * r.x * r.y; s_t[4][k] = mm * r.x * r.z; s_t[5][k] = mm * r.y * r.z;
+            s_t[6][k] = rr;
+            A.local[i] = make_float4(r.x, r.y, r.z, 0.0f);
+            A.kbody[i] = b;
+        }
+        __syncthreads();
+        if (k == 0) {
+            const uint32_t e = min((uint32_t)SETUP_T, n - t0);
+            for (uint32_t q = 0; q < e; q++) {
+                it[0] += s_t[0][q]; it[4] += s_t[1][q]; it[8] += s_t[2][q];
+                it[1] -= s_t[3][q]; it[2] -= s_t[4][q]; it[5] -= s_t[5][q];
+                rr_max = maxf(rr_max, s_t[6][q]);
+            }
+        }
+        __syncthreads();
+    }
+    if (k == 0) {
+        V3 p;
+        float prot[9];
+        setup_tail(A, lb, b, mass, cl, it, rr_max, p, prot);
+        s_p[0] = p.x; s_p[1] = p.y; s_p[2] = p.z;
+        for (int q = 0; q < 9; q++) s_rot[q] = prot[q];
+    }
+    __syncthreads();
+    const V3 p = v3(s_p[0], s_p[1], s_p[2]);
+    for (uint32_t t = k; t < n; t += SETUP_T) {
+        const uint32_t i = s + t;
+        const float4 l = A.local[i];
+        const V3 wp = add(p, mv(s_rot, v3(l.x, l.y, l.z)));
+        A.wpos[i] = make_float4(wp.x, wp.y, wp.z, 0.0f);
+    }
+}
+static cudaError_t launch_setup(sf_world *w, cudaStream_t st, uint32_t nb, uint32_t base, const uint32_t *list,
+                                const float *pose, uint32_t stride) {
+    if (nb == 0) return cudaSuccess;
+    SetupArgs A;
+    A.nb = nb; A.base = base; A.list = list; A.first = w->b_first.p; A.count = w->b_count.p; A.xyz = w->k_xyz.p;
+    A.kmat = w->k_mat.p; A.pose = pose; A.stride = stride; A.local = w->k_local.p; A.wpos = w->k_wpos.p;
+    A.kbody = w->k_body.p; A.pos = w->b_pos.p; A.q = w->b_q.p; A.v = w->b_v.p; A.w = w->b_w.p; A.rot = w->b_rot.p;
+    A.iil = w->b_iil.p; A.iiw = w->b_iiw.p; A.m = w->b_m.p; A.im = w->b_im.p; A.rad = w->b_rad.p;
+    A.sleep = w->b_sleep.p; A.maxr = w->b_maxr.p; A.alive = w->b_alive.p; A.asleep = w->b_asleep.p;
+    A.wake = w->b_wake.p;
+    k_setup_bodies<<<grid_for(nb, 128), 128, 0, st>>>(A);
+    k_setup_big<<<nb, SETUP_T, 0, st>>>(A);
+    w->launches += 2;
+    return cudaGetLastError();
 }
 
 __global__ void k_pack_bodies(uint32_t nb, const float4 *pos, const float4 *q, const float4 *v, const float4 *w,
@@ -284,14 +399,7 @@ namespace sf {
 static cudaError_t setup_launch(sf_world *w, uint32_t base, const uint32_t *list, uint32_t nb, const float *pose,
                                 uint32_t stride) {
     if (nb == 0) return cudaSuccess;
-    k_setup_bodies<<<grid_for(nb, 128), 128, 0, w->stream>>>(nb, base, list, w->b_first.p, w->b_count.p, w->k_xyz.p,
-                                                            w->k_mat.p, pose, stride, w->k_local.p, w->k_wpos.p,
-                                                            w->k_body.p, w->b_pos.p, w->b_q.p, w->b_v.p, w->b_w.p,
-                                                            w->b_rot.p, w->b_iil.p, w->b_iiw.p, w->b_m.p, w->b_im.p,
-                                                            w->b_rad.p, w->b_sleep.p, w->b_maxr.p, w->b_alive.p,
-                                                            w->b_asleep.p, w->b_wake.p);
-    w->launches++;
-    return cudaGetLastError();
+    return launch_setup(w, w->stream, nb, base, list, pose, stride);
 }
 cudaError_t setup_bodies(sf_world *w, uint32_t base, uint32_t nb, const float *d_pose13) {
     const cudaError_t e = setup_launch(w, base, nullptr, nb, d_pose13, 13u);
@@ -547,11 +655,7 @@ sf_status sf_world_create(const sf_world_desc *desc, const sf_params *params, sf
         SF_CUDA(cudaMemsetAsync(w->k_wpos.p, 0, w->k_wpos.bytes(), st));
     }
     if (nb) {
-        k_setup_bodies<<<grid_for(nb, 128), 128, 0, st>>>((uint32_t)nb, 0u, nullptr, w->b_first.p, w->b_count.p, w->k_xyz.p,
-                                                        w->k_mat.p, d_pose.p, 13u, w->k_local.p, w->k_wpos.p, w->k_body.p, w->b_pos.p,
-                                                        w->b_q.p, w->b_v.p, w->b_w.p, w->b_rot.p, w->b_iil.p, w->b_iiw.p,
-                                                        w->b_m.p, w->b_im.p, w->b_rad.p, w->b_sleep.p, w->b_maxr.p,
-                                                        w->b_alive.p, w->b_asleep.p, w->b_wake.p);
+        SF_CUDA(launch_setup(w.get(), st, (uint32_t)nb, 0u, nullptr, d_pose.p, 13u));
         SF_CUDA(cudaGetLastError());
     }
     SF_CUDA(w->err.alloc(64));
@@ -960,13 +1064,7 @@ sf_status sf_pool_load(sf_world *w, uint32_t slot, const sf_scene_desc *d) {
                                                                       w->s_sid.p, w->ctab.p, w->cpool.p, w->s_nb6.p,
                                                                       w->s_bond.p, w->s_bmax.p);
     if (d->n_bodies)
-        k_setup_bodies<<<grid_for(d->n_bodies, 128), 128, 0, st>>>(d->n_bodies, sc.body_off, nullptr, w->b_first.p,
-                                                                 w->b_count.p, w->k_xyz.p, w->k_mat.p, d_pose.p, 13u,
-                                                                 w->k_local.p,
-                                                                 w->k_wpos.p, w->k_body.p, w->b_pos.p, w->b_q.p, w->b_v.p,
-                                                                 w->b_w.p, w->b_rot.p, w->b_iil.p, w->b_iiw.p, w->b_m.p,
-                                                                 w->b_im.p, w->b_rad.p, w->b_sleep.p, w->b_maxr.p,
-                                                                 w->b_alive.p, w->b_asleep.p, w->b_wake.p);
+        SF_CUDA(launch_setup(w, st, d->n_bodies, sc.body_off, nullptr, d_pose.p, 13u));
     w->launches += 2;
     SF_CUDA(cudaGetLastError());
     SF_CUDA(step_reset_labels(w, sc.body_off, sc.n_bodies));
