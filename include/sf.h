@@ -284,8 +284,13 @@ typedef struct sf_rebuild_report {
 sf_status sf_world_remove_bricks(sf_world *w, const uint32_t *statics, uint32_t n_statics, const uint32_t *body_bricks,
                                  uint32_t n_body_bricks);
 sf_status sf_world_rebuild_bodies(sf_world *w, sf_rebuild_report *report);
-/* ---- damage on contact (impact_damage / crush_at, src/lib.rs:1602-1702), with sf_params.damage = 1
- * Every substep, between the pinch clamps and integration: each contact's absorbed energy E = 1/2 jn vn0 (at least
+/* ---- damage on contact (impact_damage / crush_at / plough, src/lib.rs:1493-1550, 1602-1702), with sf_params.damage = 1
+ * Every substep, between the contacts and prep_contacts, plough: in list order, a body driving into a static brick at
+ * 2 m/s or more with momentum min(3 m / max(contacts, 3), m) vn of at least 0.35 CAPV of the brick damages it (a body
+ * of more than 40 bricks: damage_brick by mom / 1.5 CAPV within 0.15..0.9) or, while the scene has a spare body and
+ * brick, knocks it loose as a severed one-brick body moving at 0.75 of the body's velocity plus 2 m/s with a spin of
+ * 6 rad/s in random directions (rndv on the scene's draw count); the body keeps m / (m + 1.5 MASS) of its velocity and
+ * that contact and the later ones with the brick are switched off. Between the pinch clamps and integration: each contact's absorbed energy E = 1/2 jn vn0 (at least
  * 150 J at an approach speed of at least 1 m/s) is split between its bricks in proportion to 1 / EB and crushes each
  * side's bricks nearest the contact point, growing through intact bonds within the body or structure, one budget of
  * 2,500 bricks per scene and substep in contact list order; the brick a share cannot afford is cracked (its bonds
@@ -302,6 +307,8 @@ typedef struct sf_damage_report {
     uint64_t removed;           /* of them ground away */
     uint64_t severed;           /* of them severed from their neighbours */
     uint64_t cracked;           /* bricks whose bonds a leftover share weakened */
+    uint64_t ploughed;          /* static bricks a small body knocked loose (plough) */
+    uint64_t scraped;           /* static bricks a large body damaged in passing (plough) */
 } sf_damage_report;
 sf_status sf_read_damage(sf_world *w, sf_damage_report *report, uint8_t *activated);
 /* body bricks' bonds (4 each: +x, +y, +z, foundation) and face neighbours (6 each, world body-brick ids) */

@@ -354,12 +354,13 @@ class OracleWorld:
         self.lib.ow_body_phi(self.h, _p(p, C.c_double), _p(e, C.c_float))
         return p, e
 
-    def read_damage(self):
-        """(candidates, crushed, removed, severed, cracked) since the last read, and per structure the hit flags."""
-        c = np.zeros(5, np.uint64)
+    def read_damage(self, plough=False):
+        """(candidates, crushed, removed, severed, cracked) since the last read (with plough: + ploughed loose,
+        scraped), and per structure the hit flags."""
+        c = np.zeros(7, np.uint64)
         h = np.zeros(max(self.n_struct, 1), np.uint8)
         self.lib.ow_read_damage(self.h, _p(c, C.c_uint64), _p(h, C.c_uint8))
-        return tuple(int(x) for x in c), h[:self.n_struct]
+        return tuple(int(x) for x in c[:7 if plough else 5]), h[:self.n_struct]
 
     def pending(self):
         f = np.zeros(max(self.n_struct, 1), np.uint8)

@@ -202,7 +202,7 @@ struct World {
     std::vector<float> nmax, blt;
     std::vector<uint32_t> stamp;     // per brick: the crush that visited it last (src/lib.rs:1650)
     uint32_t stamp_id = 0, dmg_draws = 0;
-    uint64_t dmg[5] = {0, 0, 0, 0, 0};  // candidates, crushed, removed, severed, cracked
+    uint64_t dmg[7] = {0, 0, 0, 0, 0, 0, 0};  // candidates, crushed, removed, severed, cracked, ploughed loose, scraped
     std::vector<uint8_t> st_hit;     // per structure: woken by a hit since the last read (st_activate)
     uint32_t rebuilds = 0;           // bodies rebuilt so far (the lone-brick rule's draw key)
     uint32_t crush_n = 0;
@@ -602,10 +602,20 @@ static void wake_near(World& w, V p, float r) {
 // A new body for a detached piece: the next body id, its bricks appended to the body bricks in walk order (the
 // reference keeps a brick's id when it changes owner; ids only order pair tests, and the library appends, so this
 // restatement appends too). False when the capacity given at creation is spent.
+// a new body of the listed static bricks in the next spare body and bricks (the bricks keep their bonds, their
+// neighbours renumbered within the piece; the static bricks leave with potential and load 0), set up about the
+// origin with velocity pv; returns the body
+static uint32_t body_from_statics(World& w, const std::vector<uint32_t>& lst, V pv);
 static bool detach_piece(World& w, const std::vector<uint32_t>& lst) {
     const uint32_t n = (uint32_t)lst.size();
     if (w.nbody + 1 > w.cap_bodies || w.nd + n > w.cap_bricks) return false;
     w.warm_valid = false;   // brick ids move: the warm-start table starts over
+    const uint32_t b = body_from_statics(w, lst, vv(0, 0, 0));
+    wake_near(w, w.pos[b], w.rad[b] + 1.5f);
+    return true;
+}
+static uint32_t body_from_statics(World& w, const std::vector<uint32_t>& lst, V pv) {
+    const uint32_t n = (uint32_t)lst.size();
     const uint32_t b = w.nbody++;
     w.alive.push_back(0); w.asleep.push_back(0); w.wake.push_back(0);
     w.first.push_back(NONE); w.count.push_back(0); w.nc.push_back(0);
@@ -642,9 +652,8 @@ static bool detach_piece(World& w, const std::vector<uint32_t>& lst) {
     }
     const float idm[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     const float q0[4] = {0, 0, 0, 1};
-    setup_body(w, b, nl.data(), n, vv(0, 0, 0), idm, q0, vv(0, 0, 0), vv(0, 0, 0));
-    wake_near(w, w.pos[b], w.rad[b] + 1.5f);
-    return true;
+    setup_body(w, b, nl.data(), n, vv(0, 0, 0), idm, q0, pv, vv(0, 0, 0));
+    return b;
 }
 // conn_struct (src/lib.rs:1085-1134): the grounded walk from the footings, then one body per remaining piece in brick
 // order. counts: [0] pieces, [1] detached bricks, [2] 1 = a piece did not fit (the structure stays pending).
@@ -1202,6 +1211,9 @@ static void build_manifolds(World& w) {
         return ((uint64_t)c.a << 32) | bp;
     };
     std::stable_sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
+    // contacts plough switched off take no part
+    idx.erase(std::remove_if(idx.begin(), idx.end(), [&](uint32_t k) { return w.cs[k].off != 0; }), idx.end());
+    n = idx.size();
     if (w.reduce) {
         std::vector<uint32_t> kept;
         kept.reserve(n);
@@ -1395,6 +1407,62 @@ static void sever_brick(World& w, uint32_t i) {
     }
 }
 static float h01(uint32_t h, uint32_t k);
+// rndv (src/lib.rs:330-336) on the draw sequence: three draws in (-1, 1) until their length is in (0.1, 1], then
+// unit length
+static V rndv_draw(World& w) {
+    for (;;) {
+        const float x = h01(0x243F6A88u, w.dmg_draws++) * 2.0f - 1.0f;
+        const float y = h01(0x243F6A88u, w.dmg_draws++) * 2.0f - 1.0f;
+        const float z = h01(0x243F6A88u, w.dmg_draws++) * 2.0f - 1.0f;
+        const V v = vv(x, y, z);
+        const float l = dot(v, v);
+        if (l > 0.01f && l <= 1.0f) return mul(v, 1.0f / std::sqrt(l));
+    }
+}
+// plough (src/lib.rs:1493-1550), after the contacts and before prep_contacts: a body driving into a static brick at
+// 2 m/s or more with momentum of at least 0.35 of the brick's vertical capacity damages it (a body of more than 40
+// bricks: damage_brick by mom / 1.5 CAPV, within 0.15..0.9) or knocks it loose as a one-brick body (severed, with
+// 0.75 of the body's velocity plus 2 m/s and a spin of 6 rad/s in random directions; the body keeps m / (m + 1.5
+// MASS) of its velocity); the contact and the later contacts with that brick are switched off. The random
+// directions come from the damage draw sequence.
+static void plough(World& w) {
+    for (size_t k = 0; k < w.cs.size(); k++) {
+        Contact& c = w.cs[k];
+        if (c.b != STATIC || c.bb == NONE || c.bo != STATIC) continue;
+        const uint32_t j = c.bb;
+        if (w.mat[j] == 0 || w.body[j] != STATIC) { c.off = 1; continue; }
+        const uint32_t a = c.a;
+        const V ra = sub(c.p, w.pos[a]);
+        const float vn = -dot(vel_at(w, a, ra), c.n);
+        if (vn < 2.0f) continue;
+        const float meff = w.m[a] * 3.0f / maxf((float)w.nc[a], 3.0f);
+        const float mom = minf(meff, w.m[a]) * vn;
+        const uint8_t mj = w.mat[j];
+        if (mj >= SLUG || mom < CAPV[mj] * 0.35f) continue;
+        if (w.count[a] > 40) {
+            damage_brick(w, j, clampf(mom / (CAPV[mj] * 1.5f), 0.15f, 0.9f), 0.0f);
+            w.dmg[6]++;
+            continue;
+        }
+        if (w.nbody + 1 > w.cap_bodies || w.nd + 1 > w.cap_bricks) continue;   // ensure_bodies
+        sever_brick(w, j);
+        flag_conn(w, w.sid[j]);
+        st_hit(w, w.sid[j]);
+        const V rv = rndv_draw(w);
+        const V pv = madd(mul(w.v[a], 0.75f), rv, 2.0f);
+        const V ww = mul(rndv_draw(w), 6.0f);
+        const uint32_t b = body_from_statics(w, std::vector<uint32_t>{j}, pv);
+        w.w[b] = ww;
+        const float m = w.m[a];
+        w.v[a] = mul(w.v[a], m / (m + MASS[mj] * 1.5f));
+        w.dmg[5]++;
+        c.off = 1;
+        for (size_t t = k + 1; t < w.cs.size(); t++) {
+            Contact& e = w.cs[t];
+            if (e.bb == j && e.bo == STATIC && e.b == STATIC) e.off = 1;
+        }
+    }
+}
 // crush_at (src/lib.rs:1641-1702); the pulverisation draw is h01 of a fixed seed and the world's draw count
 static uint32_t crush_at(World& w, uint32_t start, float e, V p, uint32_t cap) {
     const uint8_t m0 = w.mat[start];
@@ -1453,6 +1521,7 @@ static uint32_t crush_at(World& w, uint32_t start, float e, V p, uint32_t cap) {
 static void impact_damage(World& w) {
     uint32_t budget = 2500;
     for (const Contact& c : w.cs) {
+        if (c.off) continue;   // switched off by plough or left out by the reduction
         const uint32_t ia = c.ba;
         const uint8_t ma = w.mat[ia];
         if (ma == 0 || ma >= SLUG) continue;
@@ -1482,6 +1551,7 @@ static void substep(World& w, float h, const StepParams& P) {
     for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b] && !w.asleep[b]) w.v[b][1] -= GR * h;
     build_hash(w);
     gen_contacts(w);
+    if (P.damage) plough(w);
     prep_contacts(w, h);
     for (uint32_t b = 0; b < w.nbody; b++) if (w.alive[b]) { w.vpre[b] = w.v[b]; w.wpre[b] = w.w[b]; }
     build_manifolds(w);
@@ -2061,9 +2131,10 @@ uint32_t ow_crush_at(void* h, uint32_t start, float e, float px, float py, float
 }
 // damage counters since the last read (candidates, crushed, removed, severed, cracked) and per structure whether a hit
 // woke it; both cleared by the read
+// counts: candidates, crushed, removed, severed, cracked, ploughed loose, scraped (since the last read)
 void ow_read_damage(void* h, uint64_t* counts, uint8_t* hit) {
     World* w = (World*)h;
-    for (int k = 0; k < 5; k++) { counts[k] = w->dmg[k]; w->dmg[k] = 0; }
+    for (int k = 0; k < 7; k++) { counts[k] = w->dmg[k]; w->dmg[k] = 0; }
     for (size_t s = 0; s < w->st_hit.size(); s++) { if (hit) hit[s] = w->st_hit[s]; w->st_hit[s] = 0; }
 }
 void ow_body_bonds(void* h, float* bond4, uint32_t* nb6) {

@@ -105,7 +105,7 @@ class RebuildReport(C.Structure):
 
 class DamageReport(C.Structure):
     _fields_ = [("contacts", C.c_uint64), ("crushed", C.c_uint64), ("removed", C.c_uint64), ("severed", C.c_uint64),
-                ("cracked", C.c_uint64)]
+                ("cracked", C.c_uint64), ("ploughed", C.c_uint64), ("scraped", C.c_uint64)]
 
 
 class BodiesReport(C.Structure):

@@ -31,6 +31,12 @@ constexpr uint32_t DRAW_SEED = 0x243F6A88u;
 struct DamageState {
     DBuf<uint32_t> flag, pos, cand, ncand, stamp_s, stamp_k, scratch, scene_draws, counters;
     DBuf<uint8_t> hit;
+    // plough: per static brick the contact that knocked it loose (NONE), per substep's new body its static brick, id,
+    // pose and spin (at most the spare bodies), the per-scene ranges and use, the substep's counts
+    DBuf<uint32_t> p_at, p_loose, p_newb, p_sc, p_count;
+    DBuf<float> p_pose;
+    DBuf<float4> p_spin;
+    uint64_t ploughed = 0, scraped = 0;   // since the last read
     bool ready = false;
 };
 
@@ -282,12 +288,155 @@ __global__ void k_dmg_apply(DamageArgs A) {
     }
 }
 
+// ---------------------------------------------------------------- plough (src/lib.rs:1493-1550)
+// After the contacts and before prep_contacts, in list order: a body driving into a static brick at 2 m/s or more with
+// momentum min(3 m / max(contacts, 3), m) vn of at least 0.35 of the brick's vertical capacity damages it (a body of
+// more than 40 bricks: damage_brick by mom / 1.5 CAPV within 0.15..0.9) or, while the scene has a spare body and
+// brick, knocks it loose: severed, taken out of the static set (potential and load 0) and set up as a one-brick body
+// with 0.75 of the body's velocity plus 2 m/s and a spin of 6 rad/s in random directions (rndv on the scene's damage
+// draws); the body keeps m / (m + 1.5 MASS) of its velocity, and that contact and the later ones with the brick are
+// switched off. A parallel pass keeps the contacts that could qualify (2 m/s reached with or without the body's
+// velocity, which only shrinks; enough momentum at that speed); one thread walks them in order.
+struct PloughArgs {
+    uint32_t nc;
+    const uint32_t *L_a, *L_b, *L_bo, *L_bb;
+    const float4 *L_p, *L_n;
+    const uint32_t *cand, *ncand;
+    uint8_t *off;
+    uint32_t *at;          // per static brick: the contact at which it was knocked loose, else NONE
+    uint32_t *loose;       // the static bricks knocked loose this substep
+    uint32_t *counters;    // [0] knocked loose, [1] scraped (damage_brick by a large body)
+    const float4 *pos, *w;
+    float4 *v;
+    const float *m;
+    const uint32_t *nc_b, *count;
+    uint32_t *sc;          // per scene: body_off, bodies, brick_off, bricks, bodies used, bricks used
+    int32_t *k_xyz;
+    uint32_t *k_nb6, *b_first, *b_count;
+    float *k_bmax;
+    float *pose;           // per new body: pose 13 (origin, identity, velocity, no spin)
+    float4 *spin;
+    uint32_t *newb;
+    float *s_phi, *s_ext;
+    double *s_phi64;
+};
+__device__ __forceinline__ bool plough_kind(uint32_t b, uint32_t bo, uint32_t bb) {
+    return b == STATIC && bo == STATIC && bb != NONE;
+}
+__global__ void k_plough_flags(PloughArgs P, DamageArgs A, uint32_t *flag) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.nc) return;
+    uint32_t on = 0;
+    if (plough_kind(P.L_b[k], P.L_bo[k], P.L_bb[k])) {
+        const uint32_t j = P.L_bb[k], a = P.L_a[k];
+        const uint8_t mj = A.s_mat[j];
+        if (mj != 0 && mj < SLUG) {
+            const float4 p4 = P.L_p[k], n4 = P.L_n[k], pa = P.pos[a], v4 = P.v[a], w4 = P.w[a];
+            const V3 n = v3(n4.x, n4.y, n4.z);
+            const V3 ra = sub(v3(p4.x, p4.y, p4.z), v3(pa.x, pa.y, pa.z));
+            const float spin = -dot(cross(v3(w4.x, w4.y, w4.z), ra), n);
+            const float full = -dot(add(v3(v4.x, v4.y, v4.z), cross(v3(w4.x, w4.y, w4.z), ra)), n);
+            const float vmax = maxf(full, spin);
+            const float mm = P.m[a];
+            const float meff = mm * 3.0f / maxf((float)P.nc_b[a], 3.0f);
+            on = vmax >= 1.99f && minf(meff, mm) * vmax >= c_mat.capv[mj] * 0.35f * 0.999f ? 1u : 0u;
+        }
+    }
+    flag[k] = on;
+}
+// rndv (src/lib.rs:330-336) on the scene's draw sequence (a rejection loop; 64 tries fail with probability 1e-20)
+__device__ V3 rndv_draw(uint32_t *ctr) {
+    for (int t = 0; t < 64; t++) {
+        const float x = h01_d(DRAW_SEED, (*ctr)++) * 2.0f - 1.0f;
+        const float y = h01_d(DRAW_SEED, (*ctr)++) * 2.0f - 1.0f;
+        const float z = h01_d(DRAW_SEED, (*ctr)++) * 2.0f - 1.0f;
+        const V3 v = v3(x, y, z);
+        const float l = dot(v, v);
+        if (l > 0.01f && l <= 1.0f) return mul(v, div_rn(1.0f, sqrt_rn(l)));
+    }
+    return v3(0.0f, 1.0f, 0.0f);
+}
+__global__ void k_plough_apply(PloughArgs P, DamageArgs A) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const Bricks K{A};
+    const uint32_t n = *P.ncand;
+    for (uint32_t c = 0; c < n; c++) {
+        const uint32_t k = P.cand[c];
+        const uint32_t j = P.L_bb[k], a = P.L_a[k];
+        if (A.s_mat[j] == 0) { P.off[k] = 1; continue; }   // knocked loose by an earlier contact of this pass
+        const float4 p4 = P.L_p[k], n4 = P.L_n[k], pa = P.pos[a], v4 = P.v[a], w4 = P.w[a];
+        const V3 ra = sub(v3(p4.x, p4.y, p4.z), v3(pa.x, pa.y, pa.z));
+        const V3 va = v3(v4.x, v4.y, v4.z);
+        const float vn = -dot(add(va, cross(v3(w4.x, w4.y, w4.z), ra)), v3(n4.x, n4.y, n4.z));
+        if (vn < 2.0f) continue;
+        const float mm = P.m[a];
+        const float meff = mm * 3.0f / maxf((float)P.nc_b[a], 3.0f);
+        const float mom = minf(meff, mm) * vn;
+        const uint8_t mj = A.s_mat[j];
+        if (mj >= SLUG || mom < c_mat.capv[mj] * 0.35f) continue;
+        if (P.count[a] > 40) {
+            K.damage(j, clampf(mom / (c_mat.capv[mj] * 1.5f), 0.15f, 0.9f), 0.0f);
+            P.counters[1]++;
+            continue;
+        }
+        const uint32_t q = A.b_scene[a];
+        uint32_t *S = P.sc + (size_t)q * 6;
+        if (S[4] + 1 > S[1] || S[5] + 1 > S[3]) continue;   // ensure_bodies
+        K.sever(j);
+        K.pending(A.s_sid[j]);
+        K.activate(A.s_sid[j]);
+        const V3 rv = rndv_draw(&A.scene_draws[q]);
+        const V3 pv = madd(mul(va, 0.75f), rv, 2.0f);
+        const V3 ww = mul(rndv_draw(&A.scene_draws[q]), 6.0f);
+        const uint32_t b = S[0] + S[4]++, kk = S[2] + S[5]++;
+        int x, y, z;
+        unpack_cell(A.s_cell[j], x, y, z);
+        P.k_xyz[3 * kk] = x; P.k_xyz[3 * kk + 1] = y; P.k_xyz[3 * kk + 2] = z;
+        A.k_mat[kk] = mj;
+        for (int d = 0; d < 6; d++) P.k_nb6[(size_t)kk * 6 + d] = NONE;
+        for (int t = 0; t < 4; t++) {
+            A.k_bond[(size_t)kk * 4 + t] = A.s_bond[(size_t)j * 4 + t];
+            P.k_bmax[(size_t)kk * 4 + t] = A.s_bmax[(size_t)j * 4 + t];
+        }
+        P.b_first[b] = kk;
+        P.b_count[b] = 1;
+        K.remove(j);
+        P.s_phi[j] = 0.0f; P.s_phi64[j] = 0.0; P.s_ext[j] = 0.0f;
+        const uint32_t e = P.counters[0]++;
+        float *po = P.pose + (size_t)e * 13;
+        const float f13[13] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, pv.x, pv.y, pv.z, 0.0f, 0.0f, 0.0f};
+        for (int t = 0; t < 13; t++) po[t] = f13[t];
+        P.spin[e] = make_float4(ww.x, ww.y, ww.z, 0.0f);
+        P.newb[e] = b;
+        P.loose[e] = j;
+        const V3 vs = mul(va, mm / (mm + c_mat.mass[mj] * 1.5f));
+        P.v[a] = make_float4(vs.x, vs.y, vs.z, 0.0f);
+        P.off[k] = 1;
+        P.at[j] = k;
+    }
+}
+// the contacts after the one that knocked their static brick loose are off
+__global__ void k_plough_off(PloughArgs P) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.nc || !plough_kind(P.L_b[t], P.L_bo[t], P.L_bb[t])) return;
+    const uint32_t k0 = P.at[P.L_bb[t]];
+    if (k0 != NONE && k0 < t) P.off[t] = 1;
+}
+__global__ void k_plough_reset(uint32_t n, const uint32_t *loose, uint32_t *at) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n) at[loose[e]] = NONE;
+}
+__global__ void k_plough_spin(uint32_t n, const uint32_t *newb, const float4 *spin, float4 *w) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n) w[newb[e]] = spin[e];
+}
+
 void damage_destroy(sf_world *w) {
     delete w->damage;
     w->damage = nullptr;
 }
 
-cudaError_t damage_substep(sf_world *w, const DamageIn &in, cudaStream_t s) {
+static cudaError_t damage_ready(sf_world *w, cudaStream_t s) {
     if (!w->damage) w->damage = new DamageState();
     DamageState &D = *w->damage;
     cudaError_t e;
@@ -306,16 +455,23 @@ cudaError_t damage_substep(sf_world *w, const DamageIn &in, cudaStream_t s) {
         cudaMemsetAsync(D.scene_draws.p, 0, D.scene_draws.bytes(), s);
         cudaMemsetAsync(D.counters.p, 0, D.counters.bytes(), s);
         cudaMemsetAsync(D.hit.p, 0, D.hit.bytes(), s);
+        uint32_t spare = 0;
+        for (uint32_t q = 0; q < w->n_scenes; q++) spare += w->scenes[q].n_bodies;
+        spare = std::max<uint32_t>(spare, 1);
+        if ((e = D.p_at.alloc(std::max<uint32_t>(w->ns, 1))) != cudaSuccess) return e;
+        if ((e = D.p_loose.alloc(spare)) != cudaSuccess) return e;
+        if ((e = D.p_newb.alloc(spare)) != cudaSuccess) return e;
+        if ((e = D.p_pose.alloc((size_t)spare * 13)) != cudaSuccess) return e;
+        if ((e = D.p_spin.alloc(spare)) != cudaSuccess) return e;
+        if ((e = D.p_sc.alloc((size_t)std::max<uint32_t>(w->n_scenes, 1) * 6)) != cudaSuccess) return e;
+        if ((e = D.p_count.alloc(2)) != cudaSuccess) return e;
+        cudaMemsetAsync(D.p_at.p, 0xFF, D.p_at.bytes(), s);
         D.ready = true;
     }
-    if (in.nc == 0) return cudaSuccess;
-    if ((e = D.flag.grow(in.nc)) != cudaSuccess) return e;
-    if ((e = D.pos.grow(in.nc)) != cudaSuccess) return e;
-    if ((e = D.cand.grow(in.nc)) != cudaSuccess) return e;
-    DamageArgs A;
+    return cudaGetLastError();
+}
+static void fill_damage_args(sf_world *w, DamageState &D, DamageArgs &A) {
     A.cand = D.cand.p; A.ncand = D.ncand.p;
-    A.L_a = in.L_a; A.L_b = in.L_b; A.L_bo = in.L_bo; A.L_ba = in.L_ba; A.L_bb = in.L_bb; A.invperm = in.invperm;
-    A.L_p = in.L_p; A.S_j = in.S_j; A.S_rb = in.S_rb;
     A.b_scene = w->b_scene.p; A.alive = w->b_alive.p;
     A.s_mat = w->s_mat.p; A.s_cell = w->s_cell.p; A.s_scene = w->s_scene.p; A.s_nb6 = w->s_nb6.p; A.ctab = w->ctab.p;
     A.cpool = w->cpool.p; A.s_sid = w->s_sid.p; A.s_bond = w->s_bond.p; A.s_bmax = w->s_bmax.p;
@@ -324,6 +480,86 @@ cudaError_t damage_substep(sf_world *w, const DamageIn &in, cudaStream_t s) {
     A.nst = w->n_struct;
     A.stamp_s = D.stamp_s.p; A.stamp_k = D.stamp_k.p; A.scratch = D.scratch.p; A.scene_draws = D.scene_draws.p;
     A.counters = D.counters.p;
+}
+
+cudaError_t plough_substep(sf_world *w, const PloughIn &in, cudaStream_t s, uint32_t *n_loose) {
+    *n_loose = 0;
+    cudaError_t e;
+    if ((e = damage_ready(w, s)) != cudaSuccess) return e;
+    if (in.nc == 0) return cudaSuccess;
+    DamageState &D = *w->damage;
+    if ((e = D.flag.grow(in.nc)) != cudaSuccess) return e;
+    if ((e = D.pos.grow(in.nc)) != cudaSuccess) return e;
+    if ((e = D.cand.grow(in.nc)) != cudaSuccess) return e;
+    std::vector<uint32_t> sc((size_t)w->n_scenes * 6);
+    for (uint32_t q = 0; q < w->n_scenes; q++) {
+        const Scene &c = w->scenes[q];
+        const uint32_t v[6] = {c.body_off, c.n_bodies, c.brick_off, c.n_bricks, c.bodies_used, c.bricks_used};
+        for (int t = 0; t < 6; t++) sc[(size_t)q * 6 + t] = v[t];
+    }
+    if ((e = cudaMemcpyAsync(D.p_sc.p, sc.data(), sc.size() * 4, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(in.off, 0, in.nc, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(D.p_count.p, 0, 8, s)) != cudaSuccess) return e;
+    DamageArgs A;
+    fill_damage_args(w, D, A);
+    PloughArgs P;
+    P.nc = in.nc; P.L_a = in.L_a; P.L_b = in.L_b; P.L_bo = in.L_bo; P.L_bb = in.L_bb; P.L_p = in.L_p; P.L_n = in.L_n;
+    P.cand = D.cand.p; P.ncand = D.ncand.p; P.off = in.off; P.at = D.p_at.p; P.loose = D.p_loose.p;
+    P.counters = D.p_count.p; P.pos = w->b_pos.p; P.w = w->b_w.p; P.v = w->b_v.p; P.m = w->b_m.p; P.nc_b = w->b_nc.p;
+    P.count = w->b_count.p; P.sc = D.p_sc.p; P.k_xyz = w->k_xyz.p; P.k_nb6 = w->k_nb6.p; P.b_first = w->b_first.p;
+    P.b_count = w->b_count.p; P.k_bmax = w->k_bmax.p; P.pose = D.p_pose.p; P.spin = D.p_spin.p; P.newb = D.p_newb.p;
+    P.s_phi = w->s_phi.p; P.s_ext = w->s_ext.p; P.s_phi64 = w->s_phi64.p;
+    const unsigned g = grid_for(in.nc, 256);
+    k_plough_flags<<<g, 256, 0, s>>>(P, A, D.flag.p);
+    if ((e = exclusive_scan_u32(D.flag.p, D.pos.p, in.nc, D.ncand.p, *in.wk, s)) != cudaSuccess) return e;
+    k_dmg_compact<<<g, 256, 0, s>>>(in.nc, D.flag.p, D.pos.p, D.cand.p);
+    k_plough_apply<<<1, 32, 0, s>>>(P, A);
+    w->launches += 3;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    uint32_t cnt[2];
+    if ((e = cudaMemcpyAsync(cnt, D.p_count.p, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    D.ploughed += cnt[0];
+    D.scraped += cnt[1];
+    if (cnt[0] == 0) return cudaSuccess;
+    // the later contacts with those bricks are off; the new bodies are set up scene by scene (ids and poses run in
+    // list order, so each scene's new bodies are consecutive), then given their spin
+    k_plough_off<<<g, 256, 0, s>>>(P);
+    k_plough_reset<<<grid_for(cnt[0], 256), 256, 0, s>>>(cnt[0], D.p_loose.p, D.p_at.p);
+    w->launches += 2;
+    std::vector<uint32_t> used(sc.size());
+    if ((e = cudaMemcpyAsync(used.data(), D.p_sc.p, sc.size() * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    size_t at = 0;
+    for (uint32_t q = 0; q < w->n_scenes; q++) {
+        Scene &c = w->scenes[q];
+        const uint32_t nq = used[(size_t)q * 6 + 4] - c.bodies_used;
+        if (!nq) continue;
+        const uint32_t b0 = c.body_off + c.bodies_used;
+        if ((e = setup_bodies(w, b0, nq, D.p_pose.p + at * 13)) != cudaSuccess) return e;
+        if ((e = step_reset_labels(w, b0, nq)) != cudaSuccess) return e;
+        c.bodies_used = used[(size_t)q * 6 + 4];
+        c.bricks_used = used[(size_t)q * 6 + 5];
+        at += nq;
+    }
+    k_plough_spin<<<grid_for(cnt[0], 256), 256, 0, s>>>(cnt[0], D.p_newb.p, D.p_spin.p, w->b_w.p);
+    w->launches++;
+    *n_loose = cnt[0];
+    return cudaGetLastError();
+}
+
+cudaError_t damage_substep(sf_world *w, const DamageIn &in, cudaStream_t s) {
+    cudaError_t e;
+    if ((e = damage_ready(w, s)) != cudaSuccess) return e;
+    DamageState &D = *w->damage;
+    if (in.nc == 0) return cudaSuccess;
+    if ((e = D.flag.grow(in.nc)) != cudaSuccess) return e;
+    if ((e = D.pos.grow(in.nc)) != cudaSuccess) return e;
+    if ((e = D.cand.grow(in.nc)) != cudaSuccess) return e;
+    DamageArgs A;
+    fill_damage_args(w, D, A);
+    A.L_a = in.L_a; A.L_b = in.L_b; A.L_bo = in.L_bo; A.L_ba = in.L_ba; A.L_bb = in.L_bb; A.invperm = in.invperm;
+    A.L_p = in.L_p; A.S_j = in.S_j; A.S_rb = in.S_rb;
     k_dmg_flags<<<grid_for(in.nc, 256), 256, 0, s>>>(in.nc, A, D.flag.p);
     if ((e = exclusive_scan_u32(D.flag.p, D.pos.p, in.nc, D.ncand.p, *in.wk, s)) != cudaSuccess) return e;
     k_dmg_compact<<<grid_for(in.nc, 256), 256, 0, s>>>(in.nc, D.flag.p, D.pos.p, D.cand.p);
@@ -350,6 +586,8 @@ sf_status sf_read_damage(sf_world *w, sf_damage_report *report, uint8_t *activat
         SF_CUDA(cudaMemsetAsync(D.hit.p, 0, D.hit.bytes(), w->stream));
         SF_CUDA(cudaStreamSynchronize(w->stream));
         r.contacts = c[0]; r.crushed = c[1]; r.removed = c[2]; r.severed = c[3]; r.cracked = c[4];
+        r.ploughed = D.ploughed; r.scraped = D.scraped;
+        D.ploughed = D.scraped = 0;
     } else if (activated && w->n_struct) {
         std::memset(activated, 0, w->n_struct);
     }

@@ -417,6 +417,16 @@ struct DamageIn {
     Work *wk;
 };
 cudaError_t damage_substep(sf_world *w, const DamageIn &in, cudaStream_t s);
+// plough (src/lib.rs:1493-1550) over the substep's contacts before prep: marks the contacts it switches off in `off`
+// (one byte per contact) and sets up the one-brick bodies it knocks loose; *n_loose = how many
+struct PloughIn {
+    uint32_t nc;
+    const uint32_t *L_a, *L_b, *L_bo, *L_bb;
+    const float4 *L_p, *L_n;
+    uint8_t *off;
+    Work *wk;
+};
+cudaError_t plough_substep(sf_world *w, const PloughIn &in, cudaStream_t s, uint32_t *n_loose);
 // setup_body (src/lib.rs:844-891) of bodies base .. base + nb - 1 from their bricks' lattice cells and poses
 // (sf_world.cu)
 cudaError_t setup_bodies(sf_world *w, uint32_t base, uint32_t nb, const float *d_pose13);

@@ -56,6 +56,7 @@ struct StepState {
     // contact reduction: per pair a big flag and its place among the big pairs, per big pair 27 best scores and 27
     // winners, per sorted contact a keep flag and its place among the kept
     DBuf<uint32_t> red_big, red_pos, red_keep, red_kpos, red_slots;
+    DBuf<uint8_t> c_off;            // per contact: switched off by plough this substep
     // warm start: two open-addressing tables (the last substep's, the one being written), keyed by contact key
     struct WarmTable { DBuf<uint32_t> claim; DBuf<unsigned long long> k1; DBuf<uint32_t> k2; DBuf<float4> val; uint32_t mask = 0; };
     WarmTable warm[2];
@@ -663,6 +664,11 @@ __global__ void k_red_keep(uint32_t nc, const uint32_t *flag, const uint32_t *po
         for (uint32_t d = 0; d < RED_S; d++) on |= win[o + d] == k + 1 ? 1u : 0u;
     }
     keep[t] = on;
+}
+// the sorted contacts plough left on
+__global__ void k_off_keep(uint32_t nc, const uint32_t *perm, const uint8_t *off, uint32_t *keep) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nc) keep[t] = off[perm[t]] ? 0u : 1u;
 }
 __global__ void k_red_compact(uint32_t nc, const uint32_t *keep, const uint32_t *kpos, const uint32_t *perm,
                               const uint64_t *key, uint32_t *perm2, uint64_t *key2) {
@@ -1887,6 +1893,15 @@ static sf_status substep(sf_world *w, float h) {
     const uint32_t g_nc = grid_for(std::max<uint32_t>(nc, 1), 256);
     if (nc) { k_body_nc<<<g_nc, 256, 0, s>>>(nc, S->L_a.p, S->L_b.p, w->b_nc.p); L++; }
     L += 1;
+    // plough (src/lib.rs:1776), with damage on: may knock static bricks loose as new bodies and switch contacts off
+    uint32_t n_loose = 0;
+    if (w->P.damage && nc) {
+        SF_CUDA(S->c_off.grow(nc));
+        PloughIn PI;
+        PI.nc = nc; PI.L_a = S->L_a.p; PI.L_b = S->L_b.p; PI.L_bo = S->L_bo.p; PI.L_bb = S->L_bb.p; PI.L_p = S->L_p.p;
+        PI.L_n = S->L_n.p; PI.off = S->c_off.p; PI.wk = &S->wk;
+        SF_CUDA(plough_substep(w, PI, s, &n_loose));
+    }
     if (S->profile) S->sub_nc.push_back(nc);
     prof_mark(w);
     // The launch size of the colouring and the solve, and its partition into sync domains. A substep with few contacts
@@ -1913,22 +1928,38 @@ static sf_status substep(sf_world *w, float h) {
         SF_CUDA(radix_sort_u64(S->mkey.p, S->perm.p, S->mkey_alt.p, S->perm_alt.p, nc, bits_for((uint64_t)w->nb * span + span), S->wk, s, &alt));
         if (alt) { S->mkey.swap(S->mkey_alt); S->perm.swap(S->perm_alt); }
         const uint32_t K = w->P.manifold_chunk;
-        k_man_flags<<<g_nc, 256, 0, s>>>(nc, S->mkey.p, S->mflag.p);
-        SF_CUDA(exclusive_scan_u32(S->mflag.p, S->mpos.p, nc, S->dev.p + DV_PAIRS, S->wk, s));
-        k_pair_start<<<g_nc, 256, 0, s>>>(nc, S->mflag.p, S->mpos.p, S->pair_start.p);
-        if (w->P.reduce) {
-            k_red_big<<<g_nc, 256, 0, s>>>(nc, S->dev.p + DV_PAIRS, S->pair_start.p, S->red_big.p);
-            SF_CUDA(exclusive_scan_u32(S->red_big.p, S->red_pos.p, nc, S->dev.p + DV_NBIG, S->wk, s));
-            SF_CUDA(cudaMemsetAsync(S->red_slots.p, 0, S->red_slots.bytes(), s));
-            uint32_t *best = S->red_slots.p, *win = S->red_slots.p + S->red_slots.n / 2;
-            k_red_score<<<g_nc, 256, 0, s>>>(nc, S->mflag.p, S->mpos.p, S->red_big.p, S->red_pos.p, S->perm.p, S->L_p.p,
-                                             S->L_n.p, best);
-            k_red_pick<<<g_nc, 256, 0, s>>>(nc, S->mflag.p, S->mpos.p, S->red_big.p, S->red_pos.p, S->perm.p, S->L_p.p,
-                                            S->L_n.p, best, win);
-            k_red_keep<<<g_nc, 256, 0, s>>>(nc, S->mflag.p, S->mpos.p, S->red_big.p, S->red_pos.p, S->perm.p, win,
-                                            S->red_keep.p);
+        uint32_t ncs = nc;   // the sorted contacts still on (plough switches some off)
+        if (n_loose) {
+            k_off_keep<<<g_nc, 256, 0, s>>>(nc, S->perm.p, S->c_off.p, S->red_keep.p);
             SF_CUDA(exclusive_scan_u32(S->red_keep.p, S->red_kpos.p, nc, S->dev.p + DV_KEPT, S->wk, s));
             k_red_compact<<<g_nc, 256, 0, s>>>(nc, S->red_keep.p, S->red_kpos.p, S->perm.p, S->mkey.p, S->perm_alt.p,
+                                               S->mkey_alt.p);
+            S->perm.swap(S->perm_alt);
+            S->mkey.swap(S->mkey_alt);
+            SF_CUDA(cudaMemcpyAsync(S->h_dev + DV_KEPT, S->dev.p + DV_KEPT, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            SF_CUDA(cudaStreamSynchronize(s));
+            ncs = S->h_dev[DV_KEPT];
+            L += 2;
+        }
+        ncm = ncs;
+        if (ncs) {
+        k_man_flags<<<g_nc, 256, 0, s>>>(ncs, S->mkey.p, S->mflag.p);
+        SF_CUDA(exclusive_scan_u32(S->mflag.p, S->mpos.p, ncs, S->dev.p + DV_PAIRS, S->wk, s));
+        k_pair_start<<<g_nc, 256, 0, s>>>(ncs, S->mflag.p, S->mpos.p, S->pair_start.p);
+        }
+        if (w->P.reduce && ncs) {
+            k_red_big<<<g_nc, 256, 0, s>>>(ncs, S->dev.p + DV_PAIRS, S->pair_start.p, S->red_big.p);
+            SF_CUDA(exclusive_scan_u32(S->red_big.p, S->red_pos.p, ncs, S->dev.p + DV_NBIG, S->wk, s));
+            SF_CUDA(cudaMemsetAsync(S->red_slots.p, 0, S->red_slots.bytes(), s));
+            uint32_t *best = S->red_slots.p, *win = S->red_slots.p + S->red_slots.n / 2;
+            k_red_score<<<g_nc, 256, 0, s>>>(ncs, S->mflag.p, S->mpos.p, S->red_big.p, S->red_pos.p, S->perm.p, S->L_p.p,
+                                             S->L_n.p, best);
+            k_red_pick<<<g_nc, 256, 0, s>>>(ncs, S->mflag.p, S->mpos.p, S->red_big.p, S->red_pos.p, S->perm.p, S->L_p.p,
+                                            S->L_n.p, best, win);
+            k_red_keep<<<g_nc, 256, 0, s>>>(ncs, S->mflag.p, S->mpos.p, S->red_big.p, S->red_pos.p, S->perm.p, win,
+                                            S->red_keep.p);
+            SF_CUDA(exclusive_scan_u32(S->red_keep.p, S->red_kpos.p, ncs, S->dev.p + DV_KEPT, S->wk, s));
+            k_red_compact<<<g_nc, 256, 0, s>>>(ncs, S->red_keep.p, S->red_kpos.p, S->perm.p, S->mkey.p, S->perm_alt.p,
                                                S->mkey_alt.p);
             S->perm.swap(S->perm_alt);
             S->mkey.swap(S->mkey_alt);
@@ -2007,7 +2038,7 @@ static sf_status substep(sf_world *w, float h) {
         PA.warm = warm_read ? 1 : 0;
         PA.wt = WarmRef{WT.claim.p, WT.k1.p, WT.k2.p, WT.val.p, WT.mask};
         PA.L_b = S->L_b.p; PA.L_bo = S->L_bo.p; PA.L_ba = S->L_ba.p; PA.L_bb = S->L_bb.p;
-        if (w->P.reduce) SF_CUDA(cudaMemsetAsync(S->invperm.p, 0xFF, (size_t)nc * 4, s));   // left out: no slot
+        if (w->P.reduce || n_loose) SF_CUDA(cudaMemsetAsync(S->invperm.p, 0xFF, (size_t)nc * 4, s));   // left out: no slot
         k_prep<<<g_nc, 256, 0, s>>>(PA);
         L++;
     } else {

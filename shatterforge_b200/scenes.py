@@ -203,6 +203,41 @@ def tilted_beam(length: int = 60, angle_deg: float = 45.0, height: int = 60, row
                  body_brick_mat=np.full(len(c), mat, np.uint8), body_pose=pose, name="tilted_beam").contiguous()
 
 
+def plough_scene(n_bricks: int = 12, speed: float = 8.0, block_speed: float = 8.0) -> Scene:
+    """Bodies driven into static bricks: a glass pane (structure 0, 10 x 6 bricks, one layer) with n_bricks single
+    concrete bricks flying at it at `speed` m/s, and a timber wall (structure 1, 10 x 8 x 2 bricks) with a 54-brick
+    concrete block driven at it at `block_speed` m/s: the bricks knock glass loose, the block scrapes the timber."""
+    ox, oz = ORIGIN[0], ORIGIN[2]
+    pane = [(ox + 10 + x, y, oz) for y in range(6) for x in range(10)]
+    wall = [(ox + 30 + x, y, oz + 10 + z) for z in range(2) for y in range(8) for x in range(10)]
+    sxyz = np.array(pane + wall, np.int32)
+    smat = np.array([GLASS] * len(pane) + [WOOD] * len(wall), np.uint8)
+    ssid = np.array([0] * len(pane) + [1] * len(wall), np.int32)
+    sinf = np.zeros(len(sxyz), np.uint8)
+    first, xyz, mat, pose = [0], [], [], []
+    for k in range(n_bricks):
+        xyz.append([ORIGIN[0], 0, ORIGIN[2]])
+        mat.append(CONC)
+        first.append(first[-1] + 1)
+        p = np.zeros(13, np.float32)
+        # the brick's lattice centre is (0.25, 0.25, 0.25) about the parent origin
+        p[0:3] = [5.25 + (k % 6) * 0.8 - 0.25, 0.8 + (k // 6) * 0.9 - 0.25, -3.0 - 0.25]
+        p[6] = 1.0
+        p[9] = speed
+        pose.append(p)
+    blk = [[ORIGIN[0] + x, y, ORIGIN[2] + z] for y in range(3) for z in range(3) for x in range(6)]
+    xyz.extend(blk)
+    mat.extend([CONC] * len(blk))
+    first.append(first[-1] + len(blk))
+    p = np.zeros(13, np.float32)
+    p[0:3] = [16.0, 0.6, 2.5]
+    p[6] = 1.0
+    p[9] = block_speed
+    pose.append(p)
+    return Scene(sxyz, smat, ssid, sinf, np.array(first, np.uint32), np.array(xyz, np.int32),
+                 np.array(mat, np.uint8), np.array(pose, np.float32), name="plough").contiguous()
+
+
 def frame5_debris_scene(seed: int = 1, n_debris: int = 1024, removed: bool = False) -> Scene:
     """The 5-storey frame plus 1,024 loose single-brick bodies 2 m above the ground beside it."""
     frame, rm = frame5_structure(seed)

@@ -15,8 +15,8 @@ pytestmark = pytest.mark.gpu
 
 def damage_counts(w, ow):
     r, hit = w.damage()
-    oc, ohit = ow.read_damage()
-    assert (r.contacts, r.crushed, r.removed, r.severed, r.cracked) == oc
+    oc, ohit = ow.read_damage(plough=True)
+    assert (r.contacts, r.crushed, r.removed, r.severed, r.cracked, r.ploughed, r.scraped) == oc
     np.testing.assert_array_equal(hit, ohit)
     return r
 
@@ -113,3 +113,28 @@ def test_tower_collapse_with_damage_against_oracle(sf, oracle):
             compare_world(w, ow)
             compare_bonds(w, ow)
     assert detached > 45000
+
+
+def test_plough_against_oracle(sf, oracle):
+    """plough (src/lib.rs:1493-1550) with damage on: single concrete bricks flying at a glass pane knock panes loose
+    as one-brick bodies (spare capacity, the scene's draws for their velocity and spin, the later contacts with them
+    switched off), and a 54-brick block driven into a timber wall scrapes it (damage_brick). 120 steps, every step's
+    damage counts and structures hit, the world (bodies, set-up, brick positions, static and body bonds) every 10."""
+    sc = S.plough_scene()
+    w = sf.World(sc, iterations=IT, detach_bodies=200, detach_bricks=400, damage=1)
+    ow = oracle.OracleWorld(sc)
+    ow.set_capacity(200, 400)
+    loose = scraped = 0
+    for k in range(120):
+        w.step(DT)
+        ow.step(DT, iterations=IT, damage=1)
+        r = damage_counts(w, ow)
+        loose += r.ploughed
+        scraped += r.scraped
+        rep = w.rebuild_bodies()
+        assert (rep.bodies, rep.pieces, rep.removed, rep.dissolved, rep.lone) == ow.rebuild_bodies(), k
+        if k % 10 == 9:
+            compare_world(w, ow)
+            compare_bonds(w, ow)
+    assert loose > 10 and scraped > 5
+

@@ -95,3 +95,39 @@ def test_damage_in_steps_respects_the_budget(oracle):
         crushed += cr
         pieces += ow.rebuild_bodies()[1]
     assert crushed > 50 and pieces > 10
+
+
+def run_plough(oracle, spare_bodies=200, steps=40):
+    sc = S.plough_scene()
+    ow = oracle.OracleWorld(sc)
+    ow.set_capacity(spare_bodies, 2 * spare_bodies)   # spare bodies and bricks, as sf_params.detach_*
+    loose = scraped = 0
+    hits = np.zeros(2, np.uint8)
+    for _ in range(steps):
+        ow.step(1.0 / 60.0, iterations=8, damage=1)
+        (cand, cr, removed, severed, cracked, lo, sc_), h = ow.read_damage(plough=True)
+        loose += lo
+        scraped += sc_
+        hits |= h
+    return sc, ow, loose, scraped, hits
+
+
+def test_plough_knocks_glass_loose_and_scrapes_timber(oracle):
+    """plough (src/lib.rs:1493-1550): concrete bricks flying at 8 m/s into a glass pane (momentum 300 kg x 8 m/s
+    against 0.35 x 1,500) knock panes loose as one-brick glass bodies; the 54-brick block (more than 40 bricks) at
+    8 m/s into timber (0.35 x 9,000) damages the bricks it hits instead. Both structures are hit and pending."""
+    sc, ow, loose, scraped, hits = run_plough(oracle)
+    assert loose > 10 and scraped > 5
+    assert hits.all()
+    assert ow.nb == sc.n_bodies + loose
+    assert (ow.pending()[:2] == 1).all()
+    st, _, fl = ow.bodies()
+    assert (fl[sc.n_bodies:] & 1).all()               # the loosened panes are live bodies
+
+
+def test_plough_needs_a_spare_body(oracle):
+    """Without spare capacity nothing is knocked loose (ensure_bodies fails: the contact stays on and is solved),
+    while the block still scrapes the timber."""
+    sc, ow, loose, scraped, hits = run_plough(oracle, spare_bodies=0)
+    assert loose == 0 and scraped > 5
+    assert ow.nb == sc.n_bodies
