@@ -404,10 +404,11 @@ sf_status sf_read_joints(sf_world *w, float *ratio4, float *bond4, uint8_t *deci
  * The solve stops at tol or at max_sweeps, whichever comes first, and returns SF_OK either way: the caller compares
  * *resid_out with tol. Every brick must reach the ground through bonds (a piece that does not has no finite
  * potential; its potentials grow sweep by sweep and the call returns SF_ERR_VERIFY only once one is non-finite).
- * Each call waits for its own work on `stream` to finish before it returns (it reads results back to the host).
- * The first call on a device looks up the array's device address (with that device current) and should come before
- * any stream capture; the address is kept for the life of the process, so the entry point must not be called again
- * on a device after cudaDeviceReset. Every call reuses the same array: calls whose work overlaps on the GPU race. */
+ * Each call is synchronous on `stream`: it waits for its own work to finish and reads the results back to the host,
+ * so no call can be recorded inside a stream capture. The first call on a device looks up the array's device
+ * address (with that device current); the address is kept for the life of the process, so the entry point must not
+ * be called again on a device after cudaDeviceReset. Every call reuses the same array: calls whose work overlaps on
+ * the GPU race. */
 #define SF_STATIC_MAX_BRICKS 8192
 #define SF_STATIC_MAX_CHUNKS 128
 #define SF_STATIC_SCRATCH_BYTES 2815744
