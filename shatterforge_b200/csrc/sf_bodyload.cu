@@ -26,12 +26,16 @@
 #include <cstring>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "sf_internal.cuh"
 
 namespace sf {
 
 constexpr int BL_SOR_THREADS = 256, BL_SOR_BIG_THREADS = 1024;
 constexpr uint32_t BL_BIG = 2048;   // bricks from which a body's sweeps take the larger block
+constexpr uint32_t BL_HUGE = 16384;  // bricks from which a body's sweeps take a cluster of BL_CL blocks
+constexpr int BL_CL = 16;
 constexpr int64_t BL_BUDGET = 160000;   // brick updates a frame, per scene (src/lib.rs:1305)
 constexpr uint8_t BJ_HOLD = 0, BJ_FATIGUE = 1, BJ_FAIL = 2, BJ_CRUSH = 3, BJ_ABSENT = 255;
 
@@ -58,6 +62,7 @@ struct BodyLoadState {
     DBuf<uint32_t> counters;      // joints, over, failed, crushed, crushes after the pass, largest ratio's bits
     DBuf<uint32_t> maxr_bits;
     bool ready = false;
+    bool cluster_ok = false;      // the device can hold a cluster of BL_CL 1,024-thread blocks
 };
 
 __device__ __forceinline__ bool body_loaded_d(uint32_t b, const uint8_t *alive, const uint32_t *count,
@@ -184,7 +189,7 @@ __device__ __forceinline__ double body_update(const BodySorArgs &A, uint32_t b, 
 // 2, the residual max |dphi| / max(phi, 1) is below 4e-4, or 60 sweeps, or its cap. Bodies of BL_BIG bricks or more
 // take blocks of 1,024 threads, the rest 256 (the order inside a half-sweep does not change the result).
 template <int T>
-__global__ void __launch_bounds__(T) k_bl_sor(const uint32_t *list, const uint32_t *caps, BodySorArgs A,
+__global__ void __launch_bounds__(T, 1) k_bl_sor(const uint32_t *list, const uint32_t *caps, BodySorArgs A,
                                               uint32_t *sweeps_out, double *resid_out) {
     __shared__ unsigned long long s_d[T / 32], s_p[T / 32];
     __shared__ int s_stop;
@@ -236,6 +241,81 @@ __global__ void __launch_bounds__(T) k_bl_sor(const uint32_t *list, const uint32
         sweeps_out[blockIdx.x] = done;
         resid_out[blockIdx.x] = done ? s_r : 0.0;
     }
+}
+// The same sweeps for a body of BL_HUGE bricks or more on a cluster of BL_CL blocks: the blocks share the body's
+// bricks (brick t to block t / 1,024 mod BL_CL), a cluster barrier ends each half-sweep's writes, and each block's
+// maxima go to its shared memory, from where every block's thread 0 reads all of the cluster's before the next
+// sweep (two barriers a sweep; the stop decision is the same everywhere).
+__global__ void __launch_bounds__(BL_SOR_BIG_THREADS, 1) k_bl_sor_cluster(const uint32_t *list, const uint32_t *caps,
+                                                                       BodySorArgs A, uint32_t *sweeps_out,
+                                                                       double *resid_out) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    __shared__ unsigned long long s_d[BL_SOR_BIG_THREADS / 32], s_p[BL_SOR_BIG_THREADS / 32];
+    __shared__ unsigned long long s_red[2][2];
+    __shared__ int s_stop;
+    __shared__ double s_r;
+    const uint32_t rank = cl.block_rank(), slot = blockIdx.x / BL_CL;
+    const uint32_t b = list[slot];
+    const uint32_t f = A.first[b], c = A.count[b];
+    const uint32_t cap = caps ? caps[slot] : 60u;
+    const double omega = (double)1.8f;
+    const unsigned long long one = (unsigned long long)__double_as_longlong(1.0);
+    const uint32_t t0 = rank * BL_SOR_BIG_THREADS + threadIdx.x, stride = BL_CL * BL_SOR_BIG_THREADS;
+    uint32_t done = 0;
+    for (uint32_t sweep = 0; sweep < cap; sweep++) {
+        unsigned long long md = 0ull;
+        for (int colour = 0; colour < 2; colour++) {
+            for (uint32_t t = t0; t < c; t += stride) {
+                const uint32_t i = f + t;
+                const uint8_t mi = A.kmat[i];
+                if (mi == 0) continue;
+                if (((A.kxyz[3 * i] + A.kxyz[3 * i + 1] + A.kxyz[3 * i + 2]) & 1) != colour) continue;
+                md = max(md, (unsigned long long)__double_as_longlong(body_update(A, b, i, mi, omega)));
+            }
+            if (colour == 0) cl.sync();
+        }
+        unsigned long long mp = one;
+        for (uint32_t t = t0; t < c; t += stride) {
+            const uint32_t i = f + t;
+            if (A.kmat[i] == 0) continue;
+            const double p = A.phi64[i];
+            if (p > 1.0) mp = max(mp, (unsigned long long)__double_as_longlong(p));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            md = max(md, __shfl_xor_sync(0xffffffffu, md, o));
+            mp = max(mp, __shfl_xor_sync(0xffffffffu, mp, o));
+        }
+        if ((threadIdx.x & 31u) == 0) { s_d[threadIdx.x >> 5] = md; s_p[threadIdx.x >> 5] = mp; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long dm = 0ull, pm = one;
+            for (uint32_t k = 0; k < BL_SOR_BIG_THREADS / 32; k++) { dm = max(dm, s_d[k]); pm = max(pm, s_p[k]); }
+            s_red[sweep & 1][0] = dm;
+            s_red[sweep & 1][1] = pm;
+        }
+        cl.sync();   // ends the sweep's writes and publishes the blocks' maxima
+        if (threadIdx.x == 0) {
+            unsigned long long dm = 0ull, pm = one;
+            for (uint32_t r = 0; r < BL_CL; r++) {
+                const unsigned long long *q = cl.map_shared_rank(&s_red[sweep & 1][0], r);
+                dm = max(dm, q[0]);
+                pm = max(pm, q[1]);
+            }
+            const double rr = __longlong_as_double((long long)dm) / __longlong_as_double((long long)pm);
+            s_r = rr;
+            s_stop = (sweep + 1 >= 2 && rr < (double)4e-4f) ? 1 : 0;
+        }
+        __syncthreads();
+        done = sweep + 1;
+        if (s_stop) break;
+    }
+    if (rank == 0 && threadIdx.x == 0) {
+        sweeps_out[slot] = done;
+        resid_out[slot] = done ? s_r : 0.0;
+    }
+    cl.sync();   // no block leaves while another may still read its shared memory
 }
 __global__ void k_bl_store(uint32_t n, const uint32_t *list, const double *resid_out, double *resid) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -479,6 +559,20 @@ static sf_status bodies_frame_impl(sf_world *w, float dt, uint32_t crush_used, s
         SF_CUDA(B.j_ratio.alloc((size_t)nd * 3)); SF_CUDA(B.j_bond.alloc((size_t)nd * 3)); SF_CUDA(B.j_dec.alloc((size_t)nd * 3));
         SF_CUDA(B.j_crushed.alloc((size_t)nd * 3)); SF_CUDA(B.cand.alloc(nd)); SF_CUDA(B.cpos.alloc(nd)); SF_CUDA(B.clist.alloc(nd)); SF_CUDA(B.jl.alloc(nb)); SF_CUDA(B.njl.alloc(2));
         SF_CUDA(B.counters.alloc(8)); SF_CUDA(B.maxr_bits.alloc(nb));
+        {
+            SF_CUDA(cudaFuncSetAttribute(k_bl_sor_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            cudaLaunchConfig_t c = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = BL_CL; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+            c.gridDim = dim3(BL_CL);
+            c.blockDim = dim3(BL_SOR_BIG_THREADS);
+            c.attrs = at;
+            c.numAttrs = 1;
+            int ncl = 0;
+            if (cudaOccupancyMaxActiveClusters(&ncl, k_bl_sor_cluster, &c) != cudaSuccess) { ncl = 0; cudaGetLastError(); }
+            B.cluster_ok = ncl > 0;
+        }
         B.ready = true;
     }
     // the poses after the last integrate (update_cache before structural, src/lib.rs:3654)
@@ -525,21 +619,38 @@ static sf_status bodies_frame_impl(sf_world *w, float dt, uint32_t crush_used, s
         auto run_sor = [&](const std::vector<uint32_t> &ids, const std::vector<uint32_t> &cp,
                            const std::vector<uint32_t> &size, std::vector<uint32_t> &done) -> cudaError_t {
             const uint32_t n = (uint32_t)ids.size();
+            // three classes in the device list: small bodies, big ones (one 1,024-thread block), huge ones (a cluster)
+            auto cls = [&](uint32_t x) { return x < BL_BIG ? 0 : (x < BL_HUGE || !B.cluster_ok) ? 1 : 2; };
             dl.clear(); dc.clear(); pos_of.assign(n, 0);
-            for (int big = 0; big < 2; big++)
+            uint32_t nk[3] = {0, 0, 0};
+            for (int k3 = 0; k3 < 3; k3++)
                 for (uint32_t k = 0; k < n; k++)
-                    if ((size[k] >= BL_BIG) == (big == 1)) { pos_of[k] = (uint32_t)dl.size(); dl.push_back(ids[k]); dc.push_back(cp[k]); }
-            const uint32_t n_small = (uint32_t)std::count_if(size.begin(), size.end(), [](uint32_t x) { return x < BL_BIG; });
+                    if (cls(size[k]) == k3) { pos_of[k] = (uint32_t)dl.size(); dl.push_back(ids[k]); dc.push_back(cp[k]); nk[k3]++; }
             cudaError_t e;
             if ((e = cudaMemcpyAsync(B.cut.p, dl.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
             if ((e = cudaMemcpyAsync(B.caps.p, dc.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
-            if (n_small)
-                k_bl_sor<BL_SOR_THREADS><<<n_small, BL_SOR_THREADS, 0, st>>>(B.cut.p, B.caps.p, A, B.sweeps.p, B.resid_out.p);
-            if (n > n_small)
-                k_bl_sor<BL_SOR_BIG_THREADS><<<n - n_small, BL_SOR_BIG_THREADS, 0, st>>>(
-                    B.cut.p + n_small, B.caps.p + n_small, A, B.sweeps.p + n_small, B.resid_out.p + n_small);
+            if (nk[0])
+                k_bl_sor<BL_SOR_THREADS><<<nk[0], BL_SOR_THREADS, 0, st>>>(B.cut.p, B.caps.p, A, B.sweeps.p, B.resid_out.p);
+            const uint32_t o1 = nk[0], o2 = nk[0] + nk[1];
+            if (nk[1])
+                k_bl_sor<BL_SOR_BIG_THREADS><<<nk[1], BL_SOR_BIG_THREADS, 0, st>>>(B.cut.p + o1, B.caps.p + o1, A,
+                                                                                 B.sweeps.p + o1, B.resid_out.p + o1);
+            if (nk[2]) {
+                cudaLaunchConfig_t cfg = {};
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = BL_CL; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+                cfg.gridDim = dim3(nk[2] * BL_CL);
+                cfg.blockDim = dim3(BL_SOR_BIG_THREADS);
+                cfg.stream = st;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                if ((e = cudaLaunchKernelEx(&cfg, k_bl_sor_cluster, (const uint32_t *)(B.cut.p + o2),
+                                            (const uint32_t *)(B.caps.p + o2), A, B.sweeps.p + o2,
+                                            B.resid_out.p + o2)) != cudaSuccess) return e;
+            }
             k_bl_store<<<grid_for(n, 256), 256, 0, st>>>(n, B.cut.p, B.resid_out.p, w->b_resid.p);
-            w->launches += 3;
+            w->launches += 1 + (nk[0] ? 1 : 0) + (nk[1] ? 1 : 0) + (nk[2] ? 1 : 0);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
             std::vector<uint32_t> sw(n);
             if ((e = cudaMemcpyAsync(sw.data(), B.sweeps.p, (size_t)n * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
