@@ -363,7 +363,7 @@ static sf_status conn_impl(sf_world *w, const std::vector<int32_t> &ids, uint32_
             SF_CUDA(cudaMemcpyAsync(w->k_xyz.p + (size_t)k0 * 3, sc_xyz[q].data(), (size_t)nkq * 12, cudaMemcpyHostToDevice, st));
             SF_CUDA(cudaMemcpyAsync(w->k_mat.p + k0, sc_mat[q].data(), nkq, cudaMemcpyHostToDevice, st));
             SF_CUDA(setup_bodies(w, b0, nbq, C.pose.p + pose_at * 13));
-            step_warm_invalidate(w);   // new body bricks take ids
+            step_warm_invalidate(w, q);   // new body bricks take ids
             SF_CUDA(step_reset_labels(w, b0, nbq));
             pose_at += nbq;
         }

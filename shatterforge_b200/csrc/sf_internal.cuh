@@ -397,8 +397,9 @@ cudaError_t refresh_poses(sf_world *w);
 // the step's active set: a scene marked live steps at the next step even if its bodies were asleep
 void step_mark_live(sf_world *w, uint32_t scene);
 void step_mark_all_live(sf_world *w);
-// brick ids moved (a rebuild or a detachment): the warm-start table of the last substep no longer applies
-void step_warm_invalidate(sf_world *w);
+// brick ids of a scene moved (a rebuild or a detachment): its entries in the last substep's warm-start table no
+// longer apply
+void step_warm_invalidate(sf_world *w, uint32_t scene);
 void step_set_live(sf_world *w, uint32_t scene, bool live);
 cudaError_t step_reset_labels(sf_world *w, uint32_t first_body, uint32_t n);
 sf_status read_error_word(sf_world *w);

@@ -252,7 +252,6 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
     }
     auto bondf = [](uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; };
 
-    step_warm_invalidate(w);   // brick ids move
     // ---- rebuild_body's walk, body by body
     std::vector<uint32_t> wslots, wrec, freed, ranges, setup_ids;
     std::vector<uint8_t> setup_keep;
@@ -266,6 +265,7 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
         const uint32_t draw_key = X.scene_rebuilds[q]++;
         rep.bodies++;
         live_scene[q] = 1;
+        step_warm_invalidate(w, q);   // brick ids move
         // bricks still there, in list order (a removed brick leaves the body)
         std::vector<uint32_t> lst;
         for (uint32_t t = 0; t < cnt; t++) {

@@ -62,6 +62,9 @@ struct StepState {
     WarmTable warm[2];
     int warm_cur = 0;                // the table the next substep reads
     bool warm_valid = false;
+    std::vector<uint8_t> warm_scene; // per scene: its entries in the table still apply (no brick ids moved since)
+    DBuf<uint8_t> warm_scene_dev;
+    bool warm_scene_dirty = true;
     // colouring
     DBuf<uint32_t> bm_count, bm_start, bm_fill, bm_list;
     DBuf<uint32_t> masks, vmasks;
@@ -774,6 +777,8 @@ struct PrepArgs {
     int warm;
     WarmRef wt;
     const uint32_t *L_b, *L_bo, *L_ba, *L_bb;
+    const uint8_t *wscene;                   // per scene: its table entries apply
+    const uint32_t *bscene;
 };
 
 // One thread per manifold, in colour-list order (position p of segment c, a (domain, colour) pair): the two bodies
@@ -844,7 +849,7 @@ __global__ void k_prep(PrepArgs A) {
         A.S_ra[d] = make_float4(ra.x, ra.y, ra.z, bias);
         A.S_rb[d] = make_float4(rb.x, rb.y, rb.z, vn0);
         float4 j0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (A.warm) {
+        if (A.warm && A.wscene[A.bscene[a]]) {
             unsigned long long k1;
             uint32_t k2;
             warm_key(k, A.L_b, A.L_bo, A.L_ba, A.L_bb, k1, k2);
@@ -1603,8 +1608,11 @@ static cudaError_t grow_contacts(StepState *S, uint64_t need) {
     return cudaSuccess;
 }
 
-void step_warm_invalidate(sf_world *w) {
-    if (w->step) w->step->warm_valid = false;
+void step_warm_invalidate(sf_world *w, uint32_t scene) {
+    StepState *S = w->step;
+    if (!S || scene >= S->warm_scene.size()) return;
+    S->warm_scene[scene] = 0;
+    S->warm_scene_dirty = true;
 }
 
 sf_status step_create(sf_world *w) {
@@ -1612,6 +1620,7 @@ sf_status step_create(sf_world *w) {
     w->step = S;
     uint32_t nb = w->nb, nd = w->nd;
     const uint32_t nsc = std::max<uint32_t>(w->n_scenes, 1);
+    S->warm_scene.assign(nsc, 0);
     cudaStream_t s = w->stream;
     SF_CUDA(S->ckey.alloc(nd)); SF_CUDA(S->ckey_alt.alloc(nd)); SF_CUDA(S->cval.alloc(nd));
     SF_CUDA(S->aw_flag.alloc(nd)); SF_CUDA(S->awk_pos.alloc(nd)); SF_CUDA(S->awk_list.alloc(nd));
@@ -2038,6 +2047,13 @@ static sf_status substep(sf_world *w, float h) {
         PA.warm = warm_read ? 1 : 0;
         PA.wt = WarmRef{WT.claim.p, WT.k1.p, WT.k2.p, WT.val.p, WT.mask};
         PA.L_b = S->L_b.p; PA.L_bo = S->L_bo.p; PA.L_ba = S->L_ba.p; PA.L_bb = S->L_bb.p;
+        if (warm_read && S->warm_scene_dirty) {
+            SF_CUDA(S->warm_scene_dev.grow(w->n_scenes));
+            SF_CUDA(cudaMemcpyAsync(S->warm_scene_dev.p, S->warm_scene.data(), w->n_scenes, cudaMemcpyHostToDevice, s));
+            SF_CUDA(cudaStreamSynchronize(s));   // the host vector is the copy's source
+            S->warm_scene_dirty = false;
+        }
+        PA.wscene = S->warm_scene_dev.p; PA.bscene = w->b_scene.p;
         if (w->P.reduce || n_loose) SF_CUDA(cudaMemsetAsync(S->invperm.p, 0xFF, (size_t)nc * 4, s));   // left out: no slot
         k_prep<<<g_nc, 256, 0, s>>>(PA);
         L++;
@@ -2085,6 +2101,8 @@ static sf_status substep(sf_world *w, float h) {
             L++;
             S->warm_cur ^= 1;
             S->warm_valid = true;
+            std::fill(S->warm_scene.begin(), S->warm_scene.end(), 1);
+            S->warm_scene_dirty = true;
         } else {
             S->warm_valid = false;
         }

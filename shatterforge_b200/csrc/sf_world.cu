@@ -1072,6 +1072,7 @@ sf_status sf_pool_load(sf_world *w, uint32_t slot, const sf_scene_desc *d) {
     PoolSlot &ps = w->pool[slot];
     ps.bodies = d->n_bodies; ps.bricks = nbr; ps.statics = d->n_static; ps.chunks = used; ps.loaded = true;
     step_set_live(w, slot, d->n_bodies > 0);
+    step_warm_invalidate(w, slot);   // another scene's bricks in this slot's ids
     return SF_OK;
 }
 
@@ -1087,6 +1088,7 @@ sf_status sf_pool_clear(sf_world *w, uint32_t slot) {
     SF_CUDA(cudaStreamSynchronize(st));
     w->pool[slot] = PoolSlot{};
     step_set_live(w, slot, false);
+    step_warm_invalidate(w, slot);
     return SF_OK;
 }
 

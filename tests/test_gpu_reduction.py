@@ -134,3 +134,45 @@ def test_tower_collapse_reduced_and_warm_against_oracle(sf, oracle):
             compare_world(w, ow)
             compare_bonds(w, ow)
     assert peak_colors <= 128
+
+
+def test_three_scenes_against_their_oracles(sf, oracle):
+    """Three scenes in one world with damage, contact reduction and warm start on: the blocks (the body frame's
+    budget per scene), the landing beam (failures, crushes, rebuilds, which start only that scene's warm-start
+    entries over) and the plough scene (bricks knocked loose from its glass pane into that scene's spare bodies, with
+    that scene's draws). Each scene equals its own oracle; the world's reports are the oracles' sums."""
+    scenes = [S.body_blocks(), S.tilted_beam(), S.plough_scene()]
+    w = sf.World(scenes, iterations=IT, detach_bodies=200, detach_bricks=400, damage=1, reduce=1, warm_start=1,
+                 max_colors=256)
+    ows = []
+    for sc in scenes:
+        ow = oracle.OracleWorld(sc)
+        ow.set_capacity(200, 400)
+        ows.append(ow)
+    loose = 0
+    for f in range(1, 181):
+        w.step(DT)
+        for ow in ows:
+            ow.step(DT, iterations=IT, damage=1, reduce=1, warm=1)
+        r, hit = w.damage()
+        oc = [ow.read_damage(plough=True) for ow in ows]
+        tot = tuple(sum(c[0][k] for c in oc) for k in range(7))
+        assert (r.contacts, r.crushed, r.removed, r.severed, r.cracked, r.ploughed, r.scraped) == tot, f
+        np.testing.assert_array_equal(hit, oc[2][1])
+        loose += r.ploughed
+        rep = w.rebuild_bodies()
+        orep = [ow.rebuild_bodies() for ow in ows]
+        osum = tuple(sum(x[k] for x in orep) for k in range(5))
+        assert (rep.bodies, rep.pieces, rep.removed, rep.dissolved, rep.lone) == osum, f
+        b = w.bodies_frame(DT, 0)
+        ob = [ow.body_frame(DT, 0) for ow in ows]
+        got = (b.bodies, b.sweeps, b.brick_updates, b.joints, b.over, b.failed, b.crushed, b.crushes_used)
+        want = tuple(sum(x[k] for x in ob) for k in (0, 1, 2, 3, 4, 5, 6, 8))
+        assert got == want, (f, got, want)
+        assert b.max_ratio == max(x[7] for x in ob), f
+        if f in (60, 180):
+            for k, ow in enumerate(ows):
+                compare_world(w, ow, scene=k)
+                compare_bonds(w, ow, scene=k)
+                compare_fields(w, ow, scene=k)
+    assert loose > 10
