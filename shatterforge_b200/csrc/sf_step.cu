@@ -979,6 +979,47 @@ __global__ void __launch_bounds__(128) k_jp(JpArgs A) {
     }
 }
 
+// A small substep's colouring in one pass: the manifolds sorted by priority (highest first, ties to the lower index)
+// and coloured one after another with the smallest colour free at both bodies, which is the colouring the
+// Jones-Plassmann rounds reach. A body with many chunks makes the rounds as many as its colours, each scanning all
+// its chunks again; this takes a few microseconds. One block, at most SEQ_COLOUR_MAX manifolds, one domain.
+constexpr uint32_t SEQ_COLOUR_MAX = 256;
+__global__ void __launch_bounds__(SEQ_COLOUR_MAX) k_colour_seq(JpArgs A) {
+    __shared__ unsigned long long key[SEQ_COLOUR_MAX];
+    const uint32_t nm = A.dom_m1[0] - A.dom_m0[0], m0 = A.dom_m0[0];
+    const uint32_t t = threadIdx.x;
+    key[t] = t < nm ? (((unsigned long long)A.prio[m0 + t] << 32) | (0xFFFFFFFFu - t)) : 0ull;
+    __syncthreads();
+    // bitonic sort, descending
+    for (uint32_t k = 2; k <= SEQ_COLOUR_MAX; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            const uint32_t ix = t ^ j;
+            if (ix > t) {
+                const unsigned long long x = key[t], y = key[ix];
+                const bool desc = (t & k) == 0;
+                if (desc ? (x < y) : (x > y)) { key[t] = y; key[ix] = x; }
+            }
+            __syncthreads();
+        }
+    }
+    if (t != 0) return;
+    for (uint32_t q = 0; q < nm; q++) {
+        const uint32_t m = m0 + (0xFFFFFFFFu - (uint32_t)(key[q] & 0xFFFFFFFFull));
+        const uint32_t a = A.man_a[m], b = A.man_b[m];
+        uint32_t c = 0xFFFFFFFFu;
+        for (uint32_t k = 0; k < A.mw && c == 0xFFFFFFFFu; k++) {
+            const uint32_t used = A.masks[(size_t)a * A.mw + k] | (b != STATIC ? A.masks[(size_t)b * A.mw + k] : 0u);
+            if (~used) c = 32 * k + (__ffs(~used) - 1);
+        }
+        if (c >= A.max_colors) { atomicOr(A.err, (unsigned)ERR_CAPACITY_COLORS); c = A.max_colors - 1; }
+        A.man_color[m] = c;
+        A.man_round[m] = q;
+        A.masks[(size_t)a * A.mw + (c >> 5)] |= 1u << (c & 31);
+        if (b != STATIC) A.masks[(size_t)b * A.mw + (c >> 5)] |= 1u << (c & 31);
+    }
+    atomicMax(&A.dev[DV_ROUNDS], nm);   // one manifold a round
+}
+
 // Warp-aggregated counter increment: the lanes that share a key take one atomicAdd on ctr[key] between them; each
 // gets old value + its rank among those lanes. Every lane of the warp must call it; invalid lanes take nothing.
 __device__ __forceinline__ uint32_t warp_add1(uint32_t *ctr, uint32_t key, bool valid) {
@@ -1245,6 +1286,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) k_solve(SolveArgs A) {
 // small substeps: one block, colours separated by __syncthreads instead of a grid barrier
 constexpr int SOLVE_ONE_BLOCK = 512;
 constexpr uint32_t SOLVE_ONE_BLOCK_MAX_CONTACTS = 8192;
+constexpr uint32_t SMALL_SUBSTEP_CONTACTS = 1024;
 __global__ void __launch_bounds__(SOLVE_ONE_BLOCK) k_solve_one_block(SolveArgs A) {
     __shared__ uint32_t off[JDS_K];
     const uint32_t ncol = A.dev[DV_COLORS];
@@ -1922,8 +1964,13 @@ static sf_status substep(sf_world *w, float h) {
     unsigned per_sm = w->P.solve_blocks ? std::min<unsigned>(w->P.solve_blocks, top_occ)
                                         : (unsigned)S->solve_t.choose(sb, sci);
     if (one_block) sci = -1;
-    const unsigned R = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)w->sms * per_sm,
-                                                                         (nc + SOLVE_BLOCK - 1) / SOLVE_BLOCK + 1));
+    // A small substep (at most SMALL_SUBSTEP_CONTACTS contacts) colours on one block, whose rounds end at
+    // __syncthreads instead of a grid barrier: a body with many chunks (a large piece on the ground) needs a round per
+    // colour, and the rounds, not the work, set the time.
+    const unsigned R = (one_block && nc <= SMALL_SUBSTEP_CONTACTS)
+                           ? 1u
+                           : (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)w->sms * per_sm,
+                                                                                (nc + SOLVE_BLOCK - 1) / SOLVE_BLOCK + 1));
     const uint32_t cstride = w->P.max_colors;
     uint32_t ncm = nc;   // the contacts that enter the manifolds (fewer after a contact reduction)
     // manifolds
@@ -2011,7 +2058,10 @@ static sf_status substep(sf_world *w, float h) {
         J.dom_m0 = S->dom_m0.p; J.dom_m1 = S->dom_m1.p; J.dom_cnt = S->dom_cnt.p; J.max_colors = w->P.max_colors; J.mw = mw;
         J.max_rounds = 1u << 16; J.gb = S->dom_gb.p; J.err = w->err.p;
         void *jargs[] = {&J};
-        SF_CUDA(cudaLaunchCooperativeKernel((void *)k_jp, dim3(R), dim3(SOLVE_BLOCK), jargs, 0, s));
+        if (one_block && nc <= SEQ_COLOUR_MAX && R == 1)
+            k_colour_seq<<<1, SEQ_COLOUR_MAX, 0, s>>>(J);
+        else
+            SF_CUDA(cudaLaunchCooperativeKernel((void *)k_jp, dim3(R), dim3(SOLVE_BLOCK), jargs, 0, s));
         // colour lists: each (domain, colour) segment's manifolds by contact count (most first), and the contact layout
         const uint32_t nseg = D * cstride;
         SF_CUDA(cudaMemsetAsync(S->col_count.p, 0, (size_t)nseg * JDS_ROW * 4, s));
@@ -2073,7 +2123,8 @@ static sf_status substep(sf_world *w, float h) {
         A.v = w->b_v.p; A.w = w->b_w.p; A.im = w->b_im.p; A.iiw = w->b_iiw.p; A.gb = S->dom_gb.p; A.err = w->err.p;
         A.warm = w->P.warm_start ? 1u : 0u;
         if (one_block) {
-            k_solve_one_block<<<1, SOLVE_ONE_BLOCK, 0, s>>>(A);
+            // a small substep's colours are short: one warp's barrier is cheaper than 16 warps'
+            k_solve_one_block<<<1, nc <= SMALL_SUBSTEP_CONTACTS / 2 ? 32 : SOLVE_ONE_BLOCK, 0, s>>>(A);
         } else {
             SF_CUDA(cudaMemsetAsync(S->dom_gb.p, 0, (size_t)S->part_D * sizeof(GridBarrier), s));
             void *sargs[] = {&A};
