@@ -134,7 +134,7 @@ static void prof_mark(sf_world *w) {
 }
 
 enum { DV_CONTACTS = 0, DV_MANIFOLDS = 1, DV_COLORS = 2, DV_ROUNDS = 3, DV_WL0 = 4, DV_WL1 = 5, DV_WL2 = 6,
-       DV_ALIVE = 7, DV_AWAKE = 8, DV_ISLANDS = 9, DV_PAIRS = 10, DV_AWK = 11, DV_INC = 12, DV_NBIG = 13, DV_KEPT = 14, DV_N = 16 };
+       DV_ALIVE = 7, DV_AWAKE = 8, DV_ISLANDS = 9, DV_PAIRS = 10, DV_AWK = 11, DV_INC = 12, DV_NBIG = 13, DV_KEPT = 14, DV_MAXDEG = 15, DV_N = 16 };
 constexpr int JDS_K = 32;   // the largest manifold chunk: the depth of the solve's contact layout
 
 // ---------------------------------------------------------------- pose cache
@@ -869,12 +869,15 @@ __global__ void k_prep(PrepArgs A) {
 // ---------------------------------------------------------------- colouring
 // The body-to-manifold lists and the colour masks are indexed by the body's place in the substep's active list
 // (man_ca / man_cb), so their size and clearing follow the active bodies only.
-__global__ void k_bm_count(const uint32_t *nm_p, const uint32_t *man_a, const uint32_t *man_b, uint32_t *bm_count) {
+// (and the largest count of manifolds at one body, which picks the colouring's form)
+__global__ void k_bm_count(const uint32_t *nm_p, const uint32_t *man_a, const uint32_t *man_b, uint32_t *bm_count,
+                           uint32_t *maxdeg) {
     uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= *nm_p) return;
-    atomicAdd(&bm_count[man_a[m]], 1u);
+    uint32_t d = atomicAdd(&bm_count[man_a[m]], 1u) + 1;
     uint32_t b = man_b[m];
-    if (b != STATIC) atomicAdd(&bm_count[b], 1u);
+    if (b != STATIC) d = max(d, atomicAdd(&bm_count[b], 1u) + 1);
+    atomicMax(maxdeg, d);
 }
 __global__ void k_bm_fill(const uint32_t *nm_p, const uint32_t *man_a, const uint32_t *man_b, const uint32_t *bm_start,
                           uint32_t *bm_fill, uint32_t *bm_list) {
@@ -897,6 +900,7 @@ struct JpArgs {
     uint32_t mw;                      // colour-mask words per body: max_colors / 32 rounded up
     GridBarrier *gb;                  // per domain
     uint32_t *err;
+    uint32_t seq_launched;            // k_colour_seq ran before (it colours the substeps it takes)
 };
 
 __device__ __forceinline__ bool jp_blocked(const JpArgs &A, uint32_t body, uint32_t m, uint32_t pm, uint32_t r) {
@@ -918,11 +922,20 @@ __device__ __forceinline__ bool dom_sync(GridBarrier *gb, uint32_t nblk, uint32_
     return grid_sync(gb, nblk, err);
 }
 
+// the substeps the one-pass colouring (k_colour_seq) takes: few manifolds, or a hub among them
+constexpr uint32_t SEQ_COLOUR_MAX = 4096, SEQ_COLOUR_SMALL = 256, SEQ_HUB = 64, SEQ_T = 1024;
+constexpr uint32_t SEQ_COLOUR_LAUNCH = 65536;   // contacts up to which the one-pass form is launched to decide
+__device__ __forceinline__ bool colour_seq_form(const uint32_t *dev) {
+    const uint32_t nm = dev[DV_MANIFOLDS];
+    return nm <= SEQ_COLOUR_MAX && (nm <= SEQ_COLOUR_SMALL || dev[DV_MAXDEG] > SEQ_HUB);
+}
+
 // Jones-Plassmann rounds, each domain on its own blocks: a round colours every manifold of the domain's worklist whose
 // higher-priority neighbours are all coloured (the smallest colour free at both bodies) and passes the others on.
 // Neighbouring manifolds share a body, hence a scene, hence a domain, so each domain's result is the greedy
 // colouring in priority order whatever the other domains do.
 __global__ void __launch_bounds__(128) k_jp(JpArgs A) {
+    if (A.seq_launched && colour_seq_form(A.dev)) return;   // k_colour_seq coloured them
     const uint4 bd = A.blk_dom[blockIdx.x];
     const uint32_t d = bd.x, rank = bd.y, nblk = bd.z;
     const uint32_t m0 = A.dom_m0[d], nm = A.dom_m1[d] - m0;
@@ -979,32 +992,38 @@ __global__ void __launch_bounds__(128) k_jp(JpArgs A) {
     }
 }
 
-// A small substep's colouring in one pass: the manifolds sorted by priority (highest first, ties to the lower index)
-// and coloured one after another with the smallest colour free at both bodies, which is the colouring the
-// Jones-Plassmann rounds reach. A body with many chunks makes the rounds as many as its colours, each scanning all
-// its chunks again; this takes a few microseconds. One block, at most SEQ_COLOUR_MAX manifolds, one domain.
-constexpr uint32_t SEQ_COLOUR_MAX = 256;
-__global__ void __launch_bounds__(SEQ_COLOUR_MAX) k_colour_seq(JpArgs A) {
+// The colouring in one pass, for a substep of at most SEQ_COLOUR_MAX manifolds that are few (at most 256) or meet
+// at a hub (a body holding more than SEQ_HUB of them, a large piece resting on many chunks): the manifolds sorted by
+// priority (highest first, ties to the lower index) and coloured one after another with the smallest colour free at
+// both bodies, which is the colouring the Jones-Plassmann rounds reach (domains do not share bodies, so one order over
+// all of them gives each domain its own result). At a hub the rounds are as many as its colours and each scans all
+// its manifolds again; this pass costs about 0.1 us a manifold. One block; k_jp returns at once when it runs.
+__global__ void __launch_bounds__(SEQ_T) k_colour_seq(JpArgs A) {
     __shared__ unsigned long long key[SEQ_COLOUR_MAX];
-    const uint32_t nm = A.dom_m1[0] - A.dom_m0[0], m0 = A.dom_m0[0];
-    const uint32_t t = threadIdx.x;
-    key[t] = t < nm ? (((unsigned long long)A.prio[m0 + t] << 32) | (0xFFFFFFFFu - t)) : 0ull;
+    if (!colour_seq_form(A.dev)) return;
+    const uint32_t nm = A.dev[DV_MANIFOLDS];
+    uint32_t n2 = 1;
+    while (n2 < nm) n2 <<= 1;
+    for (uint32_t t = threadIdx.x; t < n2; t += SEQ_T)
+        key[t] = t < nm ? (((unsigned long long)A.prio[t] << 32) | (0xFFFFFFFFu - t)) : 0ull;
     __syncthreads();
     // bitonic sort, descending
-    for (uint32_t k = 2; k <= SEQ_COLOUR_MAX; k <<= 1) {
+    for (uint32_t k = 2; k <= n2; k <<= 1) {
         for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            const uint32_t ix = t ^ j;
-            if (ix > t) {
-                const unsigned long long x = key[t], y = key[ix];
-                const bool desc = (t & k) == 0;
-                if (desc ? (x < y) : (x > y)) { key[t] = y; key[ix] = x; }
+            for (uint32_t t = threadIdx.x; t < n2; t += SEQ_T) {
+                const uint32_t ix = t ^ j;
+                if (ix > t) {
+                    const unsigned long long x = key[t], y = key[ix];
+                    const bool desc = (t & k) == 0;
+                    if (desc ? (x < y) : (x > y)) { key[t] = y; key[ix] = x; }
+                }
             }
             __syncthreads();
         }
     }
-    if (t != 0) return;
+    if (threadIdx.x != 0) return;
     for (uint32_t q = 0; q < nm; q++) {
-        const uint32_t m = m0 + (0xFFFFFFFFu - (uint32_t)(key[q] & 0xFFFFFFFFull));
+        const uint32_t m = 0xFFFFFFFFu - (uint32_t)(key[q] & 0xFFFFFFFFull);
         const uint32_t a = A.man_a[m], b = A.man_b[m];
         uint32_t c = 0xFFFFFFFFu;
         for (uint32_t k = 0; k < A.mw && c == 0xFFFFFFFFu; k++) {
@@ -2046,7 +2065,8 @@ static sf_status substep(sf_world *w, float h) {
         const uint32_t mw = (w->P.max_colors + 31) / 32;
         SF_CUDA(cudaMemsetAsync(S->masks.p, 0, (size_t)nb * mw * 4, s));
         SF_CUDA(cudaMemsetAsync(S->man_round.p, 0xFF, (size_t)nc * 4, s));
-        k_bm_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_ca.p, S->man_cb.p, S->bm_count.p);
+        k_bm_count<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_ca.p, S->man_cb.p, S->bm_count.p,
+                                        S->dev.p + DV_MAXDEG);
         SF_CUDA(exclusive_scan_u32(S->bm_count.p, S->bm_start.p, (size_t)nb + 1, nullptr, S->wk, s));
         k_bm_fill<<<g_nc, 256, 0, s>>>(S->dev.p + DV_MANIFOLDS, S->man_ca.p, S->man_cb.p, S->bm_start.p, S->bm_fill.p, S->bm_list.p);
         SF_CUDA(cudaMemsetAsync(S->dom_gb.p, 0, (size_t)D * sizeof(GridBarrier), s));
@@ -2058,10 +2078,9 @@ static sf_status substep(sf_world *w, float h) {
         J.dom_m0 = S->dom_m0.p; J.dom_m1 = S->dom_m1.p; J.dom_cnt = S->dom_cnt.p; J.max_colors = w->P.max_colors; J.mw = mw;
         J.max_rounds = 1u << 16; J.gb = S->dom_gb.p; J.err = w->err.p;
         void *jargs[] = {&J};
-        if (one_block && nc <= SEQ_COLOUR_MAX && R == 1)
-            k_colour_seq<<<1, SEQ_COLOUR_MAX, 0, s>>>(J);
-        else
-            SF_CUDA(cudaLaunchCooperativeKernel((void *)k_jp, dim3(R), dim3(SOLVE_BLOCK), jargs, 0, s));
+        J.seq_launched = nc <= SEQ_COLOUR_LAUNCH ? 1u : 0u;
+        if (J.seq_launched) k_colour_seq<<<1, SEQ_T, 0, s>>>(J);
+        SF_CUDA(cudaLaunchCooperativeKernel((void *)k_jp, dim3(R), dim3(SOLVE_BLOCK), jargs, 0, s));
         // colour lists: each (domain, colour) segment's manifolds by contact count (most first), and the contact layout
         const uint32_t nseg = D * cstride;
         SF_CUDA(cudaMemsetAsync(S->col_count.p, 0, (size_t)nseg * JDS_ROW * 4, s));
