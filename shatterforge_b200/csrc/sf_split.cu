@@ -26,11 +26,12 @@
 
 namespace sf {
 
-constexpr int SPLIT_WORDS = 26;   // per read-back brick: xyz 3, mat, 6 neighbours, 4 bonds, 4 capacities, local 3,
+constexpr int SPLIT_WORDS = 26;
+constexpr int LITE = 11, L_MAT = 0, L_NB6 = 1, L_BOND = 7;   // the words the host walk reads: 3 .. 13 of a record   // per read-back brick: xyz 3, mat, 6 neighbours, 4 bonds, 4 capacities, local 3,
                                   // the load field's support stamp, f32 potential, load and f64 potential (2)
 
 struct SplitState {
-    DBuf<uint32_t> list, count, bsel, brec, slots, words, freed, awake;
+    DBuf<uint32_t> list, count, bsel, brec, slots, words, freed, awake, moves, lite;
     DBuf<uint8_t> keep;                 // per set-up body: the rebuilt body itself, which keeps its load time
     DBuf<float> pose;
     std::vector<uint32_t> scene_rebuilds;
@@ -117,17 +118,41 @@ __global__ void k_brick_snapshot(uint32_t n, const uint32_t *slots, const int32_
     o[24] = (uint32_t)p; o[25] = (uint32_t)(p >> 32);
 }
 
-// write brick records (same layout) to the listed slots
-__global__ void k_brick_write(uint32_t n, const uint32_t *slots, const uint32_t *in, int32_t *xyz, uint8_t *kmat,
-                              uint32_t *nb6, float *bond, float *bmax, float4 *local, uint32_t *sup, float *phi,
-                              float *ext, double *phi64) {
+// the walk's words of each snapshot record, packed
+__global__ void k_brick_lite(uint32_t n, const uint32_t *rec, uint32_t *lite) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * LITE) return;
+    const uint32_t e = t / LITE, w = t - e * LITE;
+    lite[t] = rec[(size_t)e * SPLIT_WORDS + 3 + w];
+}
+
+// the kept bricks of the rebuilt bodies to their new slots, from the snapshot: fields as they were, neighbours
+// renumbered (a neighbour in the same piece to its new slot, any other to none)
+struct BrickMove {
+    const uint32_t *dst, *src, *body;   // per moved brick
+    const uint32_t *nmap, *ncomp;       // per snapshot entry
+    const uint32_t *brange;             // per rebuilt body: first slot, bricks, snapshot offset
+    const uint32_t *rec;                // the snapshot, SPLIT_WORDS per entry
+};
+__global__ void k_brick_move(uint32_t n, BrickMove M, int32_t *xyz, uint8_t *kmat, uint32_t *nb6, float *bond,
+                             float *bmax, float4 *local, uint32_t *sup, float *phi, float *ext, double *phi64) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const uint32_t i = slots[k];
-    const uint32_t *r = in + (size_t)k * SPLIT_WORDS;
+    const uint32_t i = M.dst[k], e = M.src[k], bk = M.body[k];
+    const uint32_t first = M.brange[3 * bk], cnt = M.brange[3 * bk + 1], at = M.brange[3 * bk + 2];
+    const uint32_t *r = M.rec + (size_t)e * SPLIT_WORDS;
+    const uint32_t c = M.ncomp[e];
     xyz[3 * i] = (int32_t)r[0]; xyz[3 * i + 1] = (int32_t)r[1]; xyz[3 * i + 2] = (int32_t)r[2];
     kmat[i] = (uint8_t)r[3];
-    for (int d = 0; d < 6; d++) nb6[(size_t)i * 6 + d] = r[4 + d];
+    for (int d = 0; d < 6; d++) {
+        const uint32_t js = r[4 + d];
+        uint32_t ns = NONE;
+        if (js != NONE && js >= first && js < first + cnt) {
+            const uint32_t e2 = at + (js - first);
+            if (M.ncomp[e2] == c && M.nmap[e2] != NONE) ns = M.nmap[e2];
+        }
+        nb6[(size_t)i * 6 + d] = ns;
+    }
     for (int a = 0; a < 4; a++) {
         bond[(size_t)i * 4 + a] = __uint_as_float(r[10 + a]);
         bmax[(size_t)i * 4 + a] = __uint_as_float(r[14 + a]);
@@ -236,10 +261,11 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
         for (uint32_t t = 0; t < c; t++) slots.push_back(f + t);
     }
     at[nd_] = slots.size();
-    std::vector<uint32_t> rec(slots.size() * SPLIT_WORDS);
+    // the walk reads, per brick, material, neighbours and bonds (LITE words); the records stay on the device
+    std::vector<uint32_t> rec(slots.size() * LITE);
     if (!slots.empty()) {
         SF_CUDA(X.slots.grow(slots.size()));
-        SF_CUDA(X.brec.grow(rec.size()));
+        SF_CUDA(X.brec.grow(slots.size() * SPLIT_WORDS));
         SF_CUDA(cudaMemcpyAsync(X.slots.p, slots.data(), slots.size() * 4, cudaMemcpyHostToDevice, st));
         k_brick_snapshot<<<grid_for(slots.size(), 256), 256, 0, st>>>((uint32_t)slots.size(), X.slots.p, w->k_xyz.p,
                                                                       w->k_mat.p, w->k_nb6.p, w->k_bond.p,
@@ -247,13 +273,17 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
                                                                       w->k_phi.p, w->k_ext.p, w->k_phi64.p, X.brec.p);
         w->launches++;
         SF_CUDA(cudaGetLastError());
-        SF_CUDA(cudaMemcpyAsync(rec.data(), X.brec.p, rec.size() * 4, cudaMemcpyDeviceToHost, st));
+        SF_CUDA(X.lite.grow(rec.size()));
+        k_brick_lite<<<grid_for(rec.size(), 256), 256, 0, st>>>((uint32_t)slots.size(), X.brec.p, X.lite.p);
+        w->launches++;
+        SF_CUDA(cudaMemcpyAsync(rec.data(), X.lite.p, rec.size() * 4, cudaMemcpyDeviceToHost, st));
         SF_CUDA(cudaStreamSynchronize(st));
     }
     auto bondf = [](uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; };
 
     // ---- rebuild_body's walk, body by body
-    std::vector<uint32_t> wslots, wrec, freed, ranges, setup_ids;
+    std::vector<uint32_t> wslots, wsrc, wbody, freed, ranges, setup_ids;
+    std::vector<uint32_t> nmap(slots.size(), NONE), pcomp(slots.size(), NONE);
     std::vector<uint8_t> setup_keep;
     std::vector<float> poses;
     std::vector<uint8_t> live_scene(w->n_scenes, 0);
@@ -261,7 +291,7 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
         const uint32_t *B = &bs[(size_t)k * 25];
         const uint32_t id = bodies[k], first = B[0], cnt = B[1], q = B[2];
         Scene &sc = w->scenes[q];
-        const uint32_t *R = &rec[at[k] * SPLIT_WORDS];
+        const uint32_t *R = &rec[at[k] * LITE];
         const uint32_t draw_key = X.scene_rebuilds[q]++;
         rep.bodies++;
         live_scene[q] = 1;
@@ -269,7 +299,7 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
         // bricks still there, in list order (a removed brick leaves the body)
         std::vector<uint32_t> lst;
         for (uint32_t t = 0; t < cnt; t++) {
-            if (R[(size_t)t * SPLIT_WORDS + 3] != 0) lst.push_back(t);
+            if (R[(size_t)t * LITE + L_MAT] != 0) lst.push_back(t);
             else rep.removed++;
         }
         if (lst.empty()) {
@@ -288,13 +318,13 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
             qu.assign(1, t0);
             for (size_t h = 0; h < qu.size(); h++) {
                 const uint32_t i = qu[h];
-                const uint32_t *ri = &R[(size_t)i * SPLIT_WORDS];
+                const uint32_t *ri = &R[(size_t)i * LITE];
                 for (int d = 0; d < 6; d++) {
-                    const uint32_t js = ri[4 + d];
+                    const uint32_t js = ri[L_NB6 + d];
                     if (js == NONE || js < first || js >= first + cnt) continue;
                     const uint32_t j = js - first;
-                    if (comp[j] >= 0 || R[(size_t)j * SPLIT_WORDS + 3] == 0) continue;
-                    const float hp = (d & 1) == 0 ? bondf(ri[10 + (d >> 1)]) : bondf(R[(size_t)j * SPLIT_WORDS + 10 + (d >> 1)]);
+                    if (comp[j] >= 0 || R[(size_t)j * LITE + L_MAT] == 0) continue;
+                    const float hp = (d & 1) == 0 ? bondf(ri[L_BOND + (d >> 1)]) : bondf(R[(size_t)j * LITE + L_BOND + (d >> 1)]);
                     if (!(hp > 0.0f)) continue;
                     comp[j] = (int32_t)ncomp;
                     qu.push_back(j);
@@ -323,7 +353,7 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
         for (uint32_t c = 0; c < nc; c++) {
             const std::vector<uint32_t> &g = groups[c];
             if (c > 0 && g.size() == 1 && awake[q] > 1500) {
-                const uint32_t m = R[(size_t)g[0] * SPLIT_WORDS + 3];
+                const uint32_t m = R[(size_t)g[0] * LITE + L_MAT];
                 const float p = std::min((float)(awake[q] - 1500) / 2000.0f, 0.85f);
                 if (m != STEEL && h01(draw_key, g[0]) < p) { rep.lone++; continue; }
             }
@@ -336,23 +366,19 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
             }
             for (uint32_t t = 0; t < g.size(); t++) nslot[g[t]] = cfirst[c] + t;
         }
+        // the per-brick map the GPU renumbers neighbours by: new slot and piece (a neighbour in another piece, or
+        // gone, is none)
+        for (uint32_t t = 0; t < cnt; t++) {
+            nmap[at[k] + t] = nslot[t];
+            pcomp[at[k] + t] = comp[t] < 0 ? NONE : (uint32_t)comp[t];
+        }
         for (uint32_t c = 0; c < nc; c++) {
             if (cbody[c] == NONE) continue;
             const std::vector<uint32_t> &g = groups[c];
             for (uint32_t t = 0; t < g.size(); t++) {
-                const uint32_t *ri = &R[(size_t)g[t] * SPLIT_WORDS];
                 wslots.push_back(cfirst[c] + t);
-                const size_t o = wrec.size();
-                wrec.insert(wrec.end(), ri, ri + SPLIT_WORDS);
-                for (int d = 0; d < 6; d++) {
-                    const uint32_t js = ri[4 + d];
-                    uint32_t ns = NONE;
-                    if (js != NONE && js >= first && js < first + cnt) {
-                        const uint32_t j = js - first;
-                        if (comp[j] == (int32_t)c && nslot[j] != NONE) ns = nslot[j];
-                    }
-                    wrec[o + 4 + d] = ns;
-                }
+                wsrc.push_back((uint32_t)(at[k] + g[t]));
+                wbody.push_back(k);
             }
             ranges.insert(ranges.end(), {cbody[c], cfirst[c], (uint32_t)g.size()});
             setup_ids.push_back(cbody[c]);
@@ -369,14 +395,26 @@ static sf_status rebuild_impl(sf_world *w, sf_rebuild_report *report) {
         w->launches++;
     }
     if (!wslots.empty()) {
-        SF_CUDA(X.slots.grow(wslots.size()));
-        SF_CUDA(X.brec.grow(wrec.size()));
-        SF_CUDA(cudaMemcpyAsync(X.slots.p, wslots.data(), wslots.size() * 4, cudaMemcpyHostToDevice, st));
-        SF_CUDA(cudaMemcpyAsync(X.brec.p, wrec.data(), wrec.size() * 4, cudaMemcpyHostToDevice, st));
-        k_brick_write<<<grid_for(wslots.size(), 256), 256, 0, st>>>((uint32_t)wslots.size(), X.slots.p, X.brec.p,
-                                                                    w->k_xyz.p, w->k_mat.p, w->k_nb6.p, w->k_bond.p,
-                                                                    w->k_bmax.p, w->k_local.p, w->k_sup.p,
-                                                                    w->k_phi.p, w->k_ext.p, w->k_phi64.p);
+        // per moved brick: destination, snapshot entry, body; per snapshot entry: new slot and piece; per body: its
+        // old range and snapshot offset
+        const size_t nw = wslots.size();
+        std::vector<uint32_t> up;
+        up.reserve(nw * 3 + slots.size() * 2 + (size_t)nd_ * 3);
+        up.insert(up.end(), wslots.begin(), wslots.end());
+        up.insert(up.end(), wsrc.begin(), wsrc.end());
+        up.insert(up.end(), wbody.begin(), wbody.end());
+        up.insert(up.end(), nmap.begin(), nmap.end());
+        up.insert(up.end(), pcomp.begin(), pcomp.end());
+        for (uint32_t k = 0; k < nd_; k++) { up.push_back(bs[(size_t)k * 25]); up.push_back(bs[(size_t)k * 25 + 1]); up.push_back((uint32_t)at[k]); }
+        SF_CUDA(X.moves.grow(up.size()));
+        SF_CUDA(cudaMemcpyAsync(X.moves.p, up.data(), up.size() * 4, cudaMemcpyHostToDevice, st));
+        BrickMove M;
+        M.dst = X.moves.p; M.src = M.dst + nw; M.body = M.src + nw; M.nmap = M.body + nw; M.ncomp = M.nmap + slots.size();
+        M.brange = M.ncomp + slots.size();
+        M.rec = X.brec.p;
+        k_brick_move<<<grid_for(nw, 256), 256, 0, st>>>((uint32_t)nw, M, w->k_xyz.p, w->k_mat.p, w->k_nb6.p,
+                                                        w->k_bond.p, w->k_bmax.p, w->k_local.p, w->k_sup.p, w->k_phi.p,
+                                                        w->k_ext.p, w->k_phi64.p);
         w->launches++;
     }
     const uint32_t nr = (uint32_t)(ranges.size() / 3);
