@@ -923,8 +923,8 @@ __device__ __forceinline__ bool dom_sync(GridBarrier *gb, uint32_t nblk, uint32_
 }
 
 // the substeps the one-pass colouring (k_colour_seq) takes: few manifolds, or a hub among them
-constexpr uint32_t SEQ_COLOUR_MAX = 4096, SEQ_COLOUR_SMALL = 256, SEQ_HUB = 64, SEQ_T = 1024;
-constexpr uint32_t SEQ_COLOUR_LAUNCH = 65536;   // contacts up to which the one-pass form is launched to decide
+constexpr uint32_t SEQ_COLOUR_MAX = 1024, SEQ_COLOUR_SMALL = 256, SEQ_HUB = 64, SEQ_T = 1024;
+constexpr uint32_t SEQ_COLOUR_LAUNCH = 16384;   // contacts up to which the one-pass form is launched to decide
 __device__ __forceinline__ bool colour_seq_form(const uint32_t *dev) {
     const uint32_t nm = dev[DV_MANIFOLDS];
     return nm <= SEQ_COLOUR_MAX && (nm <= SEQ_COLOUR_SMALL || dev[DV_MAXDEG] > SEQ_HUB);
@@ -997,9 +997,11 @@ __global__ void __launch_bounds__(128) k_jp(JpArgs A) {
 // priority (highest first, ties to the lower index) and coloured one after another with the smallest colour free at
 // both bodies, which is the colouring the Jones-Plassmann rounds reach (domains do not share bodies, so one order over
 // all of them gives each domain its own result). At a hub the rounds are as many as its colours and each scans all
-// its manifolds again; this pass costs about 0.1 us a manifold. One block; k_jp returns at once when it runs.
+// its manifolds again; this pass costs well under a microsecond a manifold. One block; k_jp returns at once when it
+// runs.
 __global__ void __launch_bounds__(SEQ_T) k_colour_seq(JpArgs A) {
     __shared__ unsigned long long key[SEQ_COLOUR_MAX];
+    __shared__ uint32_t s_m[SEQ_COLOUR_MAX], s_a[SEQ_COLOUR_MAX], s_b[SEQ_COLOUR_MAX];
     if (!colour_seq_form(A.dev)) return;
     const uint32_t nm = A.dev[DV_MANIFOLDS];
     uint32_t n2 = 1;
@@ -1021,10 +1023,15 @@ __global__ void __launch_bounds__(SEQ_T) k_colour_seq(JpArgs A) {
             __syncthreads();
         }
     }
+    // the manifolds' bodies in sorted order, fetched in parallel for the one thread that colours
+    for (uint32_t q = threadIdx.x; q < nm; q += SEQ_T) {
+        const uint32_t m = 0xFFFFFFFFu - (uint32_t)(key[q] & 0xFFFFFFFFull);
+        s_m[q] = m; s_a[q] = A.man_a[m]; s_b[q] = A.man_b[m];
+    }
+    __syncthreads();
     if (threadIdx.x != 0) return;
     for (uint32_t q = 0; q < nm; q++) {
-        const uint32_t m = 0xFFFFFFFFu - (uint32_t)(key[q] & 0xFFFFFFFFull);
-        const uint32_t a = A.man_a[m], b = A.man_b[m];
+        const uint32_t m = s_m[q], a = s_a[q], b = s_b[q];
         uint32_t c = 0xFFFFFFFFu;
         for (uint32_t k = 0; k < A.mw && c == 0xFFFFFFFFu; k++) {
             const uint32_t used = A.masks[(size_t)a * A.mw + k] | (b != STATIC ? A.masks[(size_t)b * A.mw + k] : 0u);
