@@ -441,6 +441,8 @@ typedef struct sf_pool_slot {
 /* Device bytes a pool of these slots takes (an estimate from the per-element sizes, initial contact capacity of 4
  * per brick included). */
 sf_status sf_pool_bytes(uint32_t n_slots, const sf_pool_slot *slots, uint64_t *bytes);
+/* A pool has no spare capacity for detached pieces: params with damage or detach_* set return SF_ERR_ARG (contact
+ * reduction and warm start are allowed; a slot's warm-start entries start over when it is loaded or cleared). */
 sf_status sf_pool_create(uint32_t n_slots, const sf_pool_slot *slots, const sf_params *params, sf_world **out);
 /* Load a scene into a slot (replacing what it held); SF_ERR_CAPACITY if it does not fit. */
 sf_status sf_pool_load(sf_world *w, uint32_t slot, const sf_scene_desc *scene);

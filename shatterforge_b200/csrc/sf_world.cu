@@ -916,6 +916,10 @@ sf_status sf_pool_create(uint32_t n_slots, const sf_pool_slot *slots, const sf_p
     if (params) w->P = *params; else sf_params_default(&w->P);
     if (w->P.substeps == 0) w->P.substeps = 2;
     if (w->P.max_colors == 0 || w->P.max_colors > (uint32_t)MAXCOL) w->P.max_colors = MAXCOL;
+    if (w->P.damage || w->P.detach_bodies || w->P.detach_bricks) {
+        set_error("a scene pool has no spare capacity for detached pieces: damage and detach_* are for sf_world_create");
+        return SF_ERR_ARG;
+    }
     SF_CUDA(cudaGetDevice(&w->device));
     SF_CUDA(cudaDeviceGetAttribute(&w->sms, cudaDevAttrMultiProcessorCount, w->device));
     SF_CUDA(cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking));

@@ -168,3 +168,26 @@ def test_server_scene_initial_state_equals_alone(sf, sv):
     w.step(1 / 60, nsteps=7)
     np.testing.assert_array_equal(r["state"], w.bodies()[0])
     srv.close()
+
+
+def test_pool_refuses_topology_params(sf, sv):
+    """A pool has no spare capacity for detached pieces: damage or detach capacity is refused (SF_ERR_ARG); a pool
+    with contact reduction and warm start steps a reloaded slot as a fresh world of the same scene does."""
+    s0 = scene(71, 90)
+    cap = cover(sv, [s0], 1.2)
+    for kw in ({"damage": 1}, {"detach_bodies": 4, "detach_bricks": 16}):
+        with pytest.raises(sf.SfError) as e:
+            sv.ScenePool([cap] * 2, iterations=8, **kw)
+        assert e.value.status == sf.SF_ERR_ARG
+    pool = sv.ScenePool([cap] * 2, iterations=8, reduce=1, warm_start=1)
+    pool.load(0, s0)
+    pool.step(1 / 60, nsteps=30)
+    pool.load(0, s0)                          # the same scene again: its warm-start entries start over
+    pool.step(1 / 60, nsteps=30)
+    w = sf.World(s0, iterations=8, reduce=1, warm_start=1)
+    w.step(1 / 60, nsteps=30)
+    st, sl, fl = pool.bodies(0)
+    wst, wsl, wfl = w.bodies()
+    np.testing.assert_array_equal(st, wst)
+    np.testing.assert_array_equal(fl, wfl)
+    pool.close()
