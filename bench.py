@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-collapse", action="store_true")
     ap.add_argument("--no-sat", action="store_true")
+    ap.add_argument("--no-boxes", action="store_true")
+    ap.add_argument("--box-steps", type=int, default=20, help="timed steps of the box world's pile")
+    ap.add_argument("--box-warmup", type=int, default=60, help="steps before the timed ones (the pile lands)")
     ap.add_argument("--collapse-frames", type=int, default=600, help="frames of the collapse run (frame order, damage on)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -639,6 +642,61 @@ def sat_section(sf, args):
     return out
 
 
+def boxes_section(args):
+    """The engine crate's box world (engine/src/phys.rs World::step) on the GPU: the reference's throughput pile of
+    20,000 boxes at 12 sub-steps without sleep (its published CPU figure: 226 ms a 60 Hz step on one core of a
+    2.8 GHz Xeon, docs/PHASE0.md:12), timed on the device after it has landed; a batch of 148 piles of 2,000 (one
+    scene a block); end to end through the C ABI (the boxes uploaded, the steps, the state read back); and the
+    oracle's list-order restatement of the same step on one host thread."""
+    from shatterforge_b200 import boxes as X
+    dt = np.float32(1.0 / 60.0)
+    p = X.box_params(allow_sleep=0)
+    big = X.pile(20000)
+    out = {"workload": "pile(20000) (engine/src/phys.rs:631-646), 12 sub-steps, no sleep, dt 1/60 s"}
+    w = X.BoxWorld(big, p)
+    w.step(dt, args.box_warmup)
+    w.step(dt, args.box_steps)
+    st = w.stats()
+    ms = st.ms / args.box_steps
+    out.update({"ms_per_step": ms, "box_steps_per_s": 20000 / (ms * 1e-3), "warmup_steps": args.box_warmup,
+                "timed_steps": args.box_steps, "pairs": int(st.pairs), "manifolds": int(st.manifolds),
+                "points": int(st.points), "colours": int(st.colours), "colour_rounds": int(st.rounds),
+                "reference_cpu_ms_per_step": 226.0,
+                "reference_note": "docs/PHASE0.md:12, native, 1 thread, 2.8 GHz Xeon VM (not rerunnable here)"})
+    w.close()
+    t0 = time.perf_counter()
+    w = X.BoxWorld(big, p)
+    w.step(dt, args.box_warmup + args.box_steps)
+    _ = w.state()
+    e2e_s = time.perf_counter() - t0
+    w.close()
+    out["e2e"] = {"ms_per_step": e2e_s * 1e3 / (args.box_warmup + args.box_steps),
+                  "note": "wall clock: create (host boxes uploaded), every step, state read back",
+                  "h2d_bytes": int(big.nbytes), "d2h_bytes": 20000 * 22 * 4}
+    batch = [X.pile(2000)] * 148
+    w = X.BoxWorld(batch, p)
+    w.step(dt, args.box_warmup)
+    w.step(dt, args.box_steps)
+    st = w.stats()
+    bms = st.ms / args.box_steps
+    out["batch"] = {"scenes": 148, "boxes": 148 * 2000, "ms_per_step": bms,
+                    "box_steps_per_s": 148 * 2000 / (bms * 1e-3)}
+    w.close()
+    if not args.no_cpu:
+        from oracle import binding as orc
+        orc.use_native()
+        ow = orc.OracleBoxWorld(big, p, orc.ORDER_LIST)
+        ow.step(dt, 2)
+        n, t0 = 0, time.perf_counter()
+        while n < args.box_steps and time.perf_counter() - t0 < args.cpu_seconds:
+            ow.step(dt)
+            n += 1
+        cms = (time.perf_counter() - t0) * 1e3 / n
+        out["cpu_baseline"] = {"ms_per_step": cms, "cores": 1, "kind": "port",
+                               "sample": f"steps 3..{2 + n} of the same pile in the reference's list order"}
+    return out
+
+
 def our_arm(args, rank, world, local, pg):
     import torch
 
@@ -795,6 +853,9 @@ def our_arm(args, rank, world, local, pg):
     sat = None
     if not args.no_sat and rank == 0:
         sat = sat_section(sf, args)
+    boxes = None
+    if not args.no_boxes and rank == 0:
+        boxes = boxes_section(args)
 
     # ---- CPU baseline: the oracle on a bounded sample of the same workload and step window
     cpu = None
@@ -848,6 +909,7 @@ def our_arm(args, rank, world, local, pg):
         "sor": sor,
         "collapse": collapse,
         "sat": sat,
+        "boxes": boxes,
         "cpu_baseline": cpu,
         "serve": serve,
     }

@@ -430,6 +430,53 @@ sf_status sf_collide_boxes(const float *boxes_a, const float *boxes_b, uint32_t 
 sf_status sf_collide_hulls(const float *hull_data, uint32_t n_hulls, const float *shapes_a, const float *shapes_b,
                            uint32_t n_pairs, float margin, int32_t reduce, float *out36, int32_t *count);
 
+/* ---- the engine crate's box world (engine/src/phys.rs World): oriented boxes, the hashed-grid broadphase, box SAT
+ * with face clipping, the soft-step solver (warm start, biased solve, integrate, relax) with anchored patch friction,
+ * and island sleep. It replaces World::new + add_box (phys.rs:124-146), World::step (phys.rs:152-243) and the reads
+ * of World::bodies / World::stats (phys.rs:108-121); many scenes (independent worlds) step in one launch. */
+typedef struct sf_box_world sf_box_world;
+typedef struct sf_box_params {       /* Params (engine/src/phys.rs:74-98); defaults phys.rs:99-106 */
+    float gravity[3];                /* (0, -9.81, 0) */
+    uint32_t substeps;               /* 12 */
+    float contact_hertz;             /* 0 = a sixth of the sub-step rate */
+    float damping_ratio;             /* 10 */
+    float max_push;                  /* 3 m/s */
+    float friction;                  /* 0.6 */
+    float speculative;               /* 0.02 m */
+    float sleep_lin, sleep_ang, sleep_time, sleep_dist, sleep_rot;   /* 0.05, 0.08, 0.5 s, 0.01 m, 0.02 rad */
+    int32_t allow_sleep;             /* 1 */
+    float cell;                      /* broadphase cell, 1 m */
+    float leak;                      /* 1: the soft-step impulse leak as Box2D v3 */
+    int32_t anchor;                  /* 1: friction anchors */
+    float anchor_push, anchor_slop;  /* 3 m/s, 0 m */
+    uint32_t reserved[4];
+} sf_box_params;
+typedef struct sf_box_stats {        /* Stats (phys.rs:108-110) of the last step, plus the solver's own counts */
+    uint32_t awake, pairs, manifolds, points;
+    uint32_t colours;                /* colours of the manifold colouring (solve passes per sub-step) */
+    uint32_t status;                 /* 0, or capacity flags: 1 grid entries, 2 pairs, 4 manifolds, 8 colours */
+    uint32_t rounds;                 /* colouring rounds */
+    uint32_t reserved;
+    float ms;                        /* device time of the last sf_box_world_step call, all its steps */
+    uint64_t steps;                  /* steps taken */
+} sf_box_stats;
+/* boxes: n records of 11 floats (centre 3, quaternion x y z w, half extents 3, density; density 0 = static), scene
+ * s = records [scene_first[s], scene_first[s + 1]). Capacities per scene, on average over its boxes: 27 grid entries,
+ * 48 broadphase pairs and 8 manifolds a box; and 128 colours. sf_box_world_step returns SF_ERR_CAPACITY past them
+ * (that scene's step is left undone; its status flags say which). */
+sf_status sf_box_world_create(const float *boxes, const uint32_t *scene_first, uint32_t n_scenes,
+                              const sf_box_params *params, sf_box_world **out);
+void sf_box_world_destroy(sf_box_world *w);
+/* nsteps steps of dt for every scene; synchronous. */
+sf_status sf_box_world_step(sf_box_world *w, float dt, uint32_t nsteps);
+/* 22 floats a box: centre 3, quaternion 4, velocity 3, spin 3, sleep timer, rest pose (centre 3, quaternion 4), awake */
+sf_status sf_box_world_read(sf_box_world *w, float *out22);
+sf_status sf_box_world_stats(sf_box_world *w, uint32_t scene, sf_box_stats *out);
+/* The last step's manifolds of a scene in key order (a, b; the ground as b = 0xFFFFFFFF after a's pairs), 16 words
+ * each: a, b, point count, sticking, normal 3, normal impulses 4, friction impulses 2, twist impulse (f32 bits),
+ * colour. *count gets the number of manifolds; at most cap are written. */
+sf_status sf_box_world_manifolds(sf_box_world *w, uint32_t scene, uint32_t *out16, uint32_t cap, uint32_t *count);
+
 /* ---- scene pools: the batched and served forms (no counterpart in the reference, which runs one world per wasm
  * instance). A pool is a world of fixed-capacity scene slots; a rigid scene (bodies plus loose static geometry, no
  * load-path structures) is loaded into a slot, stepped with the other slots by sf_world_step / sf_world_step_scenes

@@ -125,6 +125,14 @@ def load() -> C.CDLL:
     lib.ow_collide_hulls_batch.argtypes = [_f32p, _f32p, _f32p, C.c_uint32, C.c_float, C.c_int32]
     lib.ow_collide_boxes.restype = C.c_int32
     lib.ow_collide_boxes.argtypes = [_f32p, _f32p, C.c_float, C.c_int32, _f32p]
+    lib.obx_create.restype = C.c_void_p
+    lib.obx_create.argtypes = [_f32p, C.c_uint32, C.c_void_p, C.c_int32]
+    lib.obx_destroy.argtypes = [C.c_void_p]
+    lib.obx_step.argtypes = [C.c_void_p, C.c_float, C.c_uint32]
+    lib.obx_read.argtypes = [C.c_void_p, _f32p]
+    lib.obx_stats.argtypes = [C.c_void_p, _u32p]
+    lib.obx_manifolds.restype = C.c_uint32
+    lib.obx_manifolds.argtypes = [C.c_void_p, _u32p, C.c_uint32]
     _lib = lib
     return lib
 
@@ -417,3 +425,42 @@ def ref_colouring(a, b, a_awake, b_awake, n_bodies, color_limit=16, rounds_s=2, 
     lib.ow_ref_colouring(len(a), _p(a, C.c_uint32), _p(b, C.c_uint32), _p(salt, C.c_uint32), _p(aa, C.c_uint8), _p(bb, C.c_uint8), int(n_bodies),
                          int(color_limit), int(rounds_s), int(rounds_a), _p(col, C.c_uint32), _p(st, C.c_uint32))
     return col, int(st[0]), int(st[1])
+
+
+class OracleBoxWorld:
+    """The engine crate's box world (engine/src/phys.rs World) restated: `boxes` is an (n, 11) array of
+    p3 q4 h3 density records (World::add_box), `params` a ctypes structure with the layout of sf_box_params, `order`
+    ORDER_LIST (the reference's manifold list order) or ORDER_COLOR (key order solved colour by colour)."""
+
+    def __init__(self, boxes, params, order=ORDER_LIST):
+        self._lib = load()
+        b = np.ascontiguousarray(boxes, np.float32).reshape(-1, 11)
+        self.n = len(b)
+        self._h = self._lib.obx_create(_p(b, C.c_float), self.n, C.cast(C.pointer(params), C.c_void_p), int(order))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.obx_destroy(self._h)
+            self._h = None
+
+    def step(self, dt, n=1):
+        self._lib.obx_step(self._h, float(dt), int(n))
+
+    def state(self):
+        """(n, 22): p3 q4 v3 w3 sleep_t sleep_p3 sleep_q4 awake."""
+        out = np.zeros((self.n, 22), np.float32)
+        self._lib.obx_read(self._h, _p(out, C.c_float))
+        return out
+
+    def stats(self):
+        """awake, pairs, manifolds, points, colours of the last step."""
+        out = np.zeros(5, np.uint32)
+        self._lib.obx_stats(self._h, _p(out, C.c_uint32))
+        return tuple(int(x) for x in out)
+
+    def manifolds(self):
+        """(m, 16) words a manifold in the solver's list: a, b, cnt, stick, n3, jn4, jt1, jt2, jtw (f32 bits), colour."""
+        m = self._lib.obx_manifolds(self._h, None, 0)
+        out = np.zeros((m, 16), np.uint32)
+        self._lib.obx_manifolds(self._h, _p(out, C.c_uint32), m)
+        return out

@@ -2354,3 +2354,548 @@ void ow_ref_colouring(uint32_t n, const uint32_t* a, const uint32_t* b, const ui
 }
 
 }  // extern "C"
+
+// ============================================================================================================
+// The engine crate's box world (engine/src/phys.rs): World::step (phys.rs:152-243) with the hashed-grid broadphase
+// (phys.rs:356-408), ground and pair collisions (phys.rs:410-445), push_manifold with its warm start and friction
+// anchors (phys.rs:447-497), the soft-step warm start and solve (phys.rs:245-324) and island sleep
+// (phys.rs:326-354). BOX_LIST keeps the reference's manifold list order: ground manifolds in body order, then the
+// pairs in hash-slot order, solved one after another. BOX_COLOR takes the same manifolds in key order (a, b; the
+// ground as b = NONE after b's pairs), colours them greedily in a fixed priority order and solves colour by colour
+// (the GPU's order: inside a colour no two manifolds share a moving body, so the order inside it does not matter).
+// ============================================================================================================
+namespace {
+
+enum { BOX_LIST = 0, BOX_COLOR = 1 };
+static const uint32_t BNONE = 0xFFFFFFFFu;
+
+struct BoxParams {      // the layout of sf_box_params
+    float gravity[3]; uint32_t substeps;
+    float contact_hertz, damping_ratio, max_push, friction, speculative;
+    float sleep_lin, sleep_ang, sleep_time, sleep_dist, sleep_rot;
+    int32_t allow_sleep; float cell, leak; int32_t anchor; float anchor_push, anchor_slop;
+    uint32_t reserved[4];
+};
+struct Q4 { float x, y, z, w; };
+static inline Q4 q4(float x, float y, float z, float w) { return Q4{x, y, z, w}; }
+// Quat::mul, integrate, normalized, conj (engine/src/math.rs:36-48)
+static inline Q4 qmul(Q4 a, Q4 o) {
+    return q4(a.w * o.x + a.x * o.w + a.y * o.z - a.z * o.y,
+              a.w * o.y - a.x * o.z + a.y * o.w + a.z * o.x,
+              a.w * o.z + a.x * o.y - a.y * o.x + a.z * o.w,
+              a.w * o.w - a.x * o.x - a.y * o.y - a.z * o.z);
+}
+static inline Q4 qnormalized(Q4 q) {
+    float l = sqrt_e(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+    float k = l > 0.0f ? 1.0f / l : 1.0f;
+    return q4(q.x * k, q.y * k, q.z * k, q.w * k);
+}
+static inline Q4 qintegrate(Q4 q, P3 w, float h) {
+    Q4 dq = qmul(q4(w.x, w.y, w.z, 0.0f), q);
+    return qnormalized(q4(q.x + 0.5f * h * dq.x, q.y + 0.5f * h * dq.y, q.z + 0.5f * h * dq.z, q.w + 0.5f * h * dq.w));
+}
+static inline M3 q_m3(Q4 q) { float f[4] = {q.x, q.y, q.z, q.w}; return quat_m3(f); }
+static inline P3 m_mulv(const M3& r, P3 v) { return r.c[0] * v.x + r.c[1] * v.y + r.c[2] * v.z; }
+static inline P3 m_tmulv(const M3& r, P3 v) { return p3(pdot(r.c[0], v), pdot(r.c[1], v), pdot(r.c[2], v)); }
+static inline M3 m_sandwich(const M3& r, P3 d) {   // R diag(d) R^T (engine/src/math.rs:71-75)
+    P3 a = r.c[0] * d.x, b = r.c[1] * d.y, c = r.c[2] * d.z;
+    M3 o;
+    for (int j = 0; j < 3; j++) o.c[j] = a * pget(r.c[0], j) + b * pget(r.c[1], j) + c * pget(r.c[2], j);
+    return o;
+}
+static inline float plen_e(P3 a) { return sqrt_e(plen2(a)); }
+static inline P3 pnorm_e(P3 a) { float l = plen_e(a); return l > 1e-12f ? a * (1.0f / l) : p3(0, 0, 0); }
+static inline P3 pmax(P3 a, P3 b) { return p3(maxf(a.x, b.x), maxf(a.y, b.y), maxf(a.z, b.z)); }
+// tangents (phys.rs:500-503)
+static inline void btangents(P3 n, P3& t1, P3& t2) {
+    P3 t = fabs_(n.x) > 0.57f ? p3(n.y, -n.x, 0.0f) : p3(0.0f, n.z, -n.y);
+    t1 = pnorm_e(t);
+    t2 = pcross(n, t1);
+}
+// floor as engine/src/math.rs:94 (truncate, then step down)
+static inline float bfloor(float x) { float t = (float)(int32_t)x; return t > x ? t - 1.0f : t; }
+static inline int32_t bcell(float x, float inv_cell) { return (int32_t)bfloor(x * inv_cell); }
+static inline uint32_t bhash(int32_t x, int32_t y, int32_t z) {
+    return (uint32_t)x * 73856093u ^ (uint32_t)y * 19349663u ^ (uint32_t)z * 83492791u;
+}
+
+struct BBody {
+    P3 p; Q4 q; P3 v, w, h; float inv_m; P3 inv_i; bool awake; float sleep_t; P3 sleep_p; Q4 sleep_q;
+    M3 rot; P3 amin, amax;
+};
+struct BCp { P3 ra, rb, la, raxn, rbxn, iaxn, ibxn; float adj, nm, jn; };
+struct BMan {
+    uint32_t a, b, sa, sb; P3 n, t1, t2; float mu; uint32_t cnt; BCp cp[4];
+    P3 fa, fb, la_f, lb_f, e0; float tm1, tm2, twm, rad, jt1, jt2, jtw; bool stick;
+    P3 ca1, ca2, cb1, cb2, ia1, ia2, ib1, ib2, ian, ibn; float ima, imb;
+    uint32_t colour;
+};
+static inline uint64_t bkey(uint32_t a, uint32_t b) { return ((uint64_t)a << 32) | b; }
+
+struct BoxWorld {
+    std::vector<BBody> bodies;
+    BoxParams prm{};
+    int order = BOX_LIST;
+    std::vector<BMan> man, old;
+    std::unordered_map<uint64_t, uint32_t> old_map;
+    std::vector<P3> sv, sw, sdp, sth, sp0; std::vector<float> sim; std::vector<M3> sii; std::vector<Q4> sq;
+    std::vector<uint32_t> sbody, sidx, corder;
+    uint32_t ncolours = 0, st_awake = 0, st_pairs = 0, st_manifolds = 0, st_points = 0;
+
+    // World::add_box (phys.rs:137-146)
+    void add_box(P3 p, Q4 q, P3 h, float density) {
+        float m = density * 8.0f * h.x * h.y * h.z;
+        BBody b{};
+        if (m > 0.0f) {
+            float x2 = 4.0f * h.x * h.x, y2 = 4.0f * h.y * h.y, z2 = 4.0f * h.z * h.z;
+            b.inv_m = 1.0f / m;
+            b.inv_i = p3(12.0f / (m * (y2 + z2)), 12.0f / (m * (x2 + z2)), 12.0f / (m * (x2 + y2)));
+        }
+        b.p = p; b.q = q; b.h = h; b.awake = m > 0.0f; b.sleep_p = p; b.sleep_q = q;
+        b.rot = q_m3(q); b.amin = p; b.amax = p;
+        bodies.push_back(b);
+    }
+    uint32_t spush(P3 v, P3 w, float im, const M3& ii, Q4 q, P3 p0, uint32_t body) {
+        sv.push_back(v); sw.push_back(w); sdp.push_back(p3(0, 0, 0)); sth.push_back(p3(0, 0, 0)); sim.push_back(im);
+        sii.push_back(ii); sq.push_back(q); sp0.push_back(p0); sbody.push_back(body);
+        return (uint32_t)sv.size() - 1;
+    }
+    void sclear() {
+        sv.clear(); sw.clear(); sdp.clear(); sth.clear(); sim.clear(); sii.clear(); sq.clear(); sp0.clear(); sbody.clear();
+        M3 z; z.c[0] = z.c[1] = z.c[2] = p3(0, 0, 0);
+        spush(p3(0, 0, 0), p3(0, 0, 0), 0.0f, z, q4(0, 0, 0, 1), p3(0, 0, 0), BNONE);
+    }
+
+    void step(float dt) {
+        const uint32_t n = (uint32_t)bodies.size();
+        sidx.assign(n, 0);
+        sclear();
+        const float spec = prm.speculative;
+        for (uint32_t i = 0; i < n; i++) {           // phys.rs:157-171
+            BBody& b = bodies[i];
+            b.rot = q_m3(b.q);
+            P3 e = p3(fabs_(b.rot.c[0].x) * b.h.x + fabs_(b.rot.c[1].x) * b.h.y + fabs_(b.rot.c[2].x) * b.h.z,
+                      fabs_(b.rot.c[0].y) * b.h.x + fabs_(b.rot.c[1].y) * b.h.y + fabs_(b.rot.c[2].y) * b.h.z,
+                      fabs_(b.rot.c[0].z) * b.h.x + fabs_(b.rot.c[1].z) * b.h.y + fabs_(b.rot.c[2].z) * b.h.z);
+            float m = b.awake ? (plen_e(b.v) + plen_e(b.w) * plen_e(b.h)) * dt + 0.5f * spec : 0.5f * spec;
+            e = e + p3(m, m, m);
+            b.amin = b.p - e; b.amax = b.p + e;
+            if (b.awake) sidx[i] = spush(b.v, b.w, b.inv_m, m_sandwich(b.rot, b.inv_i), b.q, b.p, i);
+        }
+        std::swap(man, old);
+        man.clear();
+        st_pairs = 0;
+        collide_all(dt);
+        // masses (phys.rs:184-214)
+        const uint32_t sub = prm.substeps > 0 ? prm.substeps : 1;
+        const float h = dt / (float)sub;
+        const float inv_h = 1.0f / h;
+        const float hz = prm.contact_hertz > 0.0f ? prm.contact_hertz : inv_h / 6.0f;
+        const float PI_F = 3.14159265358979323846f;
+        const float omega = 2.0f * PI_F * hz;
+        const float a1 = 2.0f * prm.damping_ratio + h * omega;
+        const float a2 = h * omega * a1;
+        const float a3 = 1.0f / (1.0f + a2);
+        const float bias_rate = omega / a1, mass_scale = a2 * a3, imp_scale = a3 * prm.leak;
+        uint32_t pts = 0;
+        for (BMan& m : man) {
+            const float ima = sim[m.sa], imb = sim[m.sb];
+            const M3 iia = sii[m.sa], iib = sii[m.sb];
+            m.ima = ima; m.imb = imb;
+            const P3 nn = m.n;
+            for (uint32_t k = 0; k < m.cnt; k++) {
+                BCp& c = m.cp[k];
+                c.raxn = pcross(c.ra, nn); c.rbxn = pcross(c.rb, nn);
+                c.iaxn = m_mulv(iia, c.raxn); c.ibxn = m_mulv(iib, c.rbxn);
+                float kk = ima + imb + pdot(c.raxn, c.iaxn) + pdot(c.rbxn, c.ibxn);
+                c.nm = kk > 0.0f ? 1.0f / kk : 0.0f;
+            }
+            m.ca1 = pcross(m.fa, m.t1); m.ca2 = pcross(m.fa, m.t2); m.cb1 = pcross(m.fb, m.t1); m.cb2 = pcross(m.fb, m.t2);
+            m.ia1 = m_mulv(iia, m.ca1); m.ia2 = m_mulv(iia, m.ca2); m.ib1 = m_mulv(iib, m.cb1); m.ib2 = m_mulv(iib, m.cb2);
+            float k1 = ima + imb + pdot(m.ca1, m.ia1) + pdot(m.cb1, m.ib1);
+            float k2 = ima + imb + pdot(m.ca2, m.ia2) + pdot(m.cb2, m.ib2);
+            m.tm1 = k1 > 0.0f ? 1.0f / k1 : 0.0f; m.tm2 = k2 > 0.0f ? 1.0f / k2 : 0.0f;
+            m.ian = m_mulv(iia, nn); m.ibn = m_mulv(iib, nn);
+            float kt = pdot(nn, m.ian) + pdot(nn, m.ibn);
+            m.twm = kt > 0.0f ? 1.0f / kt : 0.0f;
+            pts += m.cnt;
+        }
+        st_manifolds = (uint32_t)man.size(); st_points = pts;
+        corder.resize(man.size());
+        for (uint32_t k = 0; k < man.size(); k++) corder[k] = k;
+        ncolours = 0;
+        if (order == BOX_COLOR) colour_manifolds();
+        // sub-steps (phys.rs:216-231)
+        const P3 g = p3(prm.gravity[0], prm.gravity[1], prm.gravity[2]);
+        const float wmax = 0.25f * PI_F * inv_h;
+        const uint32_t nb = (uint32_t)sv.size();
+        for (uint32_t s = 0; s < sub; s++) {
+            for (uint32_t i = 1; i < nb; i++) {
+                sv[i] = sv[i] + g * h;
+                P3 w = sw[i]; float wl = plen2(w);
+                if (wl > wmax * wmax) sw[i] = w * (wmax / sqrt_e(wl));
+            }
+            warm_start();
+            solve(true, inv_h, bias_rate, mass_scale, imp_scale);
+            for (uint32_t i = 1; i < nb; i++) {
+                P3 v = sv[i], w = sw[i];
+                sdp[i] = sdp[i] + v * h; sth[i] = sth[i] + w * h;
+                sq[i] = qintegrate(sq[i], w, h);
+            }
+            solve(false, inv_h, bias_rate, mass_scale, imp_scale);
+        }
+        for (uint32_t i = 1; i < nb; i++) {          // write back (phys.rs:233-236)
+            BBody& b = bodies[sbody[i]];
+            b.v = sv[i]; b.w = sw[i]; b.p = sp0[i] + sdp[i]; b.q = sq[i];
+        }
+        sleep_islands(dt);
+        old_map.clear();
+        for (uint32_t k = 0; k < man.size(); k++) old_map[bkey(man[k].a, man[k].b)] = k;
+        st_awake = nb - 1;
+    }
+
+    // phys.rs:245-263
+    void warm_start() {
+        for (uint32_t o = 0; o < man.size(); o++) {
+            const BMan& m = man[corder[o]];
+            const uint32_t sa = m.sa, sbi = m.sb;
+            P3 va = sv[sa], wa = sw[sa], vb = sv[sbi], wb = sw[sbi];
+            float pn = 0.0f;
+            for (uint32_t k = 0; k < m.cnt; k++) {
+                const BCp& c = m.cp[k];
+                pn += c.jn; wa = wa - c.iaxn * c.jn; wb = wb + c.ibxn * c.jn;
+            }
+            P3 p = m.n * pn + m.t1 * m.jt1 + m.t2 * m.jt2;
+            va = va - p * m.ima; vb = vb + p * m.imb;
+            wa = wa - (m.ia1 * m.jt1 + m.ia2 * m.jt2 + m.ian * m.jtw);
+            wb = wb + (m.ib1 * m.jt1 + m.ib2 * m.jt2 + m.ibn * m.jtw);
+            sv[sa] = va; sw[sa] = wa; sv[sbi] = vb; sw[sbi] = wb;
+            sv[0] = p3(0, 0, 0); sw[0] = p3(0, 0, 0);
+        }
+    }
+
+    // phys.rs:265-324
+    void solve(bool use_bias, float inv_h, float bias_rate, float mass_scale, float imp_scale) {
+        const float max_push = prm.max_push, ap = prm.anchor_push, slop = prm.anchor_slop;
+        for (uint32_t o = 0; o < man.size(); o++) {
+            BMan& m = man[corder[o]];
+            const uint32_t sa = m.sa, sbi = m.sb;
+            P3 va = sv[sa], wa = sw[sa], vb = sv[sbi], wb = sw[sbi];
+            const P3 tha = sth[sa], thb = sth[sbi];
+            const P3 n = m.n, t1 = m.t1, t2 = m.t2;
+            const P3 dpab = sdp[sbi] - sdp[sa];
+            const float dn = pdot(dpab, n);
+            const float ima = m.ima, imb = m.imb;
+            float tot = 0.0f;
+            for (uint32_t k = 0; k < m.cnt; k++) {
+                BCp& c = m.cp[k];
+                float s = c.adj + dn + pdot(thb, c.rbxn) - pdot(tha, c.raxn);
+                float bias, ms, is;
+                if (s > 0.0f) { bias = s * inv_h; ms = 1.0f; is = 0.0f; }
+                else if (use_bias) { bias = maxf(bias_rate * s, -max_push); ms = mass_scale; is = imp_scale; }
+                else { bias = 0.0f; ms = 1.0f; is = 0.0f; }
+                float vn = pdot(vb - va, n) + pdot(wb, c.rbxn) - pdot(wa, c.raxn);
+                float imp = -c.nm * ms * (vn + bias) - is * c.jn;
+                float nj = maxf(c.jn + imp, 0.0f);
+                imp = nj - c.jn; c.jn = nj; tot += nj;
+                va = va - n * (imp * ima); wa = wa - c.iaxn * imp;
+                vb = vb + n * (imp * imb); wb = wb + c.ibxn * imp;
+            }
+            const float lim = m.mu * tot;
+            const P3 dv = vb - va;
+            const float v1 = pdot(dv, t1) + pdot(wb, m.cb1) - pdot(wa, m.ca1);
+            const float v2 = pdot(dv, t2) + pdot(wb, m.cb2) - pdot(wa, m.ca2);
+            const bool anchored = use_bias && m.stick;
+            float b1 = 0.0f, b2 = 0.0f, ms = 1.0f, is = 0.0f;
+            if (anchored) {
+                float e1 = pdot(m.e0, t1) + pdot(dpab, t1) + pdot(thb, m.cb1) - pdot(tha, m.ca1);
+                float e2 = pdot(m.e0, t2) + pdot(dpab, t2) + pdot(thb, m.cb2) - pdot(tha, m.ca2);
+                auto sl = [&](float e) { return e > slop ? e - slop : (e < -slop ? e + slop : 0.0f); };
+                b1 = minf(maxf(bias_rate * sl(e1), -ap), ap);
+                b2 = minf(maxf(bias_rate * sl(e2), -ap), ap);
+                ms = mass_scale; is = imp_scale;
+            }
+            const float o1 = m.jt1, o2 = m.jt2;
+            float j1 = o1 - m.tm1 * ms * (v1 + b1) - is * o1;
+            float j2 = o2 - m.tm2 * ms * (v2 + b2) - is * o2;
+            const float l2 = j1 * j1 + j2 * j2;
+            if (l2 > lim * lim) { float kf = lim / sqrt_e(l2); j1 *= kf; j2 *= kf; m.stick = false; }
+            m.jt1 = j1; m.jt2 = j2;
+            const float d1 = j1 - o1, d2 = j2 - o2;
+            const P3 p = t1 * d1 + t2 * d2;
+            va = va - p * ima; wa = wa - (m.ia1 * d1 + m.ia2 * d2);
+            vb = vb + p * imb; wb = wb + (m.ib1 * d1 + m.ib2 * d2);
+            const float wl = lim * m.rad;
+            const float ot = m.jtw;
+            const float jt = minf(maxf(ot - m.twm * pdot(wb - wa, n), -wl), wl);
+            m.jtw = jt;
+            const float dtw = jt - ot;
+            wa = wa - m.ian * dtw; wb = wb + m.ibn * dtw;
+            sv[sa] = va; sw[sa] = wa; sv[sbi] = vb; sw[sbi] = wb;
+            sv[0] = p3(0, 0, 0); sw[0] = p3(0, 0, 0);
+        }
+    }
+
+    // phys.rs:326-354
+    void sleep_islands(float dt) {
+        const uint32_t n = (uint32_t)bodies.size();
+        std::vector<uint32_t> uf(n);
+        for (uint32_t i = 0; i < n; i++) uf[i] = i;
+        auto find = [&](uint32_t x) { while (uf[x] != x) { uint32_t p = uf[uf[x]]; uf[x] = p; x = p; } return x; };
+        for (const BMan& m : man) {
+            if (m.sa == 0 || m.sb == 0) continue;
+            uint32_t ra = find(m.a), rb = find(m.b);
+            if (ra != rb) uf[ra] = rb;
+        }
+        const float l2 = prm.sleep_lin * prm.sleep_lin, a2 = prm.sleep_ang * prm.sleep_ang;
+        for (BBody& b : bodies) {
+            if (!b.awake) continue;
+            Q4 dq = qmul(b.q, q4(-b.sleep_q.x, -b.sleep_q.y, -b.sleep_q.z, b.sleep_q.w));
+            float ang = 2.0f * sqrt_e(dq.x * dq.x + dq.y * dq.y + dq.z * dq.z);
+            bool near = plen2(b.p - b.sleep_p) < prm.sleep_dist * prm.sleep_dist && ang < prm.sleep_rot;
+            if (near && plen2(b.v) < 100.0f * l2 && plen2(b.w) < 100.0f * a2) b.sleep_t += dt;
+            else { b.sleep_t = 0.0f; b.sleep_p = b.p; b.sleep_q = b.q; }
+        }
+        if (!prm.allow_sleep) return;
+        std::vector<float> min_t(n, 3.4028235e38f);
+        for (uint32_t i = 0; i < n; i++) if (bodies[i].awake) { uint32_t r = find(i); min_t[r] = minf(min_t[r], bodies[i].sleep_t); }
+        for (uint32_t i = 0; i < n; i++) {
+            if (!bodies[i].awake) continue;
+            uint32_t r = find(i);
+            if (min_t[r] >= prm.sleep_time) { BBody& b = bodies[i]; b.awake = false; b.v = p3(0, 0, 0); b.w = p3(0, 0, 0); }
+        }
+    }
+
+    // the AABB-overlap pairs of the hashed grid (phys.rs:356-408), in hash-slot order, a < b
+    void broadphase(std::vector<std::pair<uint32_t, uint32_t>>& pairs) {
+        const uint32_t n = (uint32_t)bodies.size();
+        const float inv_cell = 1.0f / prm.cell;
+        struct Ent { uint32_t h, i; int32_t c[3]; };
+        std::vector<Ent> tmp;
+        for (uint32_t i = 0; i < n; i++) {
+            const BBody& b = bodies[i];
+            int32_t c0[3] = {bcell(b.amin.x, inv_cell), bcell(b.amin.y, inv_cell), bcell(b.amin.z, inv_cell)};
+            int32_t c1[3] = {bcell(b.amax.x, inv_cell), bcell(b.amax.y, inv_cell), bcell(b.amax.z, inv_cell)};
+            for (int32_t x = c0[0]; x <= c1[0]; x++) for (int32_t y = c0[1]; y <= c1[1]; y++) for (int32_t z = c0[2]; z <= c1[2]; z++)
+                tmp.push_back(Ent{bhash(x, y, z), i, {x, y, z}});
+        }
+        const size_t ne = tmp.size();
+        size_t tbl = 1; while (tbl < ne * 2) tbl <<= 1;
+        const uint32_t mask = (uint32_t)(tbl - 1);
+        std::vector<uint32_t> cnt(tbl + 1, 0);
+        for (const Ent& e : tmp) cnt[(e.h & mask) + 1]++;
+        for (size_t k = 0; k < tbl; k++) cnt[k + 1] += cnt[k];
+        std::vector<Ent> ent(ne);
+        std::vector<uint32_t> fill(cnt.begin(), cnt.begin() + tbl);
+        for (const Ent& e : tmp) ent[fill[e.h & mask]++] = e;
+        for (size_t s = 0; s < tbl; s++) {
+            const uint32_t lo = cnt[s], hi = cnt[s + 1];
+            if (hi - lo < 2) continue;
+            for (uint32_t x = lo; x < hi; x++) for (uint32_t y = x + 1; y < hi; y++) {
+                const Ent &ea = ent[x], &eb = ent[y];
+                if (ea.c[0] != eb.c[0] || ea.c[1] != eb.c[1] || ea.c[2] != eb.c[2] || ea.i == eb.i) continue;
+                const BBody &a = bodies[ea.i], &b = bodies[eb.i];
+                if (!a.awake && !b.awake) continue;
+                if (a.inv_m == 0.0f && b.inv_m == 0.0f) continue;
+                if (a.amin.x > b.amax.x || b.amin.x > a.amax.x || a.amin.y > b.amax.y || b.amin.y > a.amax.y ||
+                    a.amin.z > b.amax.z || b.amin.z > a.amax.z) continue;
+                P3 m = pmax(a.amin, b.amin);
+                if (bcell(m.x, inv_cell) != ea.c[0] || bcell(m.y, inv_cell) != ea.c[1] || bcell(m.z, inv_cell) != ea.c[2]) continue;
+                pairs.push_back(ea.i < eb.i ? std::make_pair(ea.i, eb.i) : std::make_pair(eb.i, ea.i));
+            }
+        }
+    }
+
+    // phys.rs:410-417
+    void wake(uint32_t i) {
+        BBody& b = bodies[i];
+        if (b.awake || b.inv_m == 0.0f) return;
+        b.awake = true; b.sleep_t = 0.0f; b.sleep_p = b.p; b.sleep_q = b.q;
+    }
+    // phys.rs:419-432: the corners below the margin, at half their height, depth = their height
+    void collide_ground(uint32_t i) {
+        const BBody& b = bodies[i];
+        CP pts[8]; int cnt = 0;
+        const float margin = prm.speculative + maxf(-b.v.y, 0.0f) * (1.0f / 60.0f);
+        for (int k = 0; k < 8; k++) {
+            P3 s = p3(k & 1 ? 1.0f : -1.0f, k & 2 ? 1.0f : -1.0f, k & 4 ? 1.0f : -1.0f);
+            P3 c = b.p + m_mulv(b.rot, p3(s.x * b.h.x, s.y * b.h.y, s.z * b.h.z));
+            if (c.y < margin) { pts[cnt].p = p3(c.x, 0.5f * c.y, c.z); pts[cnt].s = c.y; cnt++; }
+        }
+        if (cnt == 0) return;
+        const P3 n = p3(0.0f, -1.0f, 0.0f);
+        cnt = reduce4(pts, cnt, n);
+        push_manifold(i, BNONE, n, pts, cnt);
+    }
+    // phys.rs:434-445; `defer` collects the wakes (applied after all pairs) instead of waking at once: the woken set
+    // and every manifold are the same either way, since a wake only ever turns a sleeping body awake.
+    void collide_pair(uint32_t ia, uint32_t ib, std::vector<uint8_t>* defer) {
+        const BBody &a = bodies[ia], &b = bodies[ib];
+        const bool a_awake = a.awake, b_awake = b.awake, a_still = a.sleep_t != 0.0f, b_still = b.sleep_t != 0.0f;
+        const float rel = plen_e(b.v - a.v) + plen_e(a.w) * plen_e(a.h) + plen_e(b.w) * plen_e(b.h);
+        const float margin = prm.speculative + rel * (1.0f / 60.0f);
+        CP pts[8]; P3 n;
+        int cnt = collide_boxes(a.p, a.rot, a.h, b.p, b.rot, b.h, margin, pts, &n);
+        if (cnt == 0) return;
+        if (a_awake && !b_awake && !a_still) { if (defer) (*defer)[ib] = 1; else wake(ib); }
+        if (b_awake && !a_awake && !b_still) { if (defer) (*defer)[ia] = 1; else wake(ia); }
+        cnt = reduce4(pts, cnt, n);
+        push_manifold(ia, ib, n, pts, cnt);
+    }
+    // phys.rs:447-497
+    void push_manifold(uint32_t a, uint32_t b, P3 n, const CP* pts, int cnt) {
+        const BBody& ba = bodies[a];
+        const P3 pa = ba.p; const M3 ra = ba.rot;
+        const P3 pb = b != BNONE ? bodies[b].p : p3(0, 0, 0);
+        const uint32_t sa = sidx[a], sbi = b != BNONE ? sidx[b] : 0;
+        if (sa == 0 && sbi == 0) return;
+        BMan m{};
+        m.a = a; m.b = b; m.sa = sa; m.sb = sbi; m.n = n; btangents(n, m.t1, m.t2); m.mu = prm.friction;
+        m.cnt = (uint32_t)cnt; m.stick = prm.anchor != 0;
+        auto it = old_map.find(bkey(a, b));
+        const BMan* o = it == old_map.end() ? nullptr : &old[it->second];
+        M3 rbm; rbm.c[0] = p3(1, 0, 0); rbm.c[1] = p3(0, 1, 0); rbm.c[2] = p3(0, 0, 1);
+        if (b != BNONE) rbm = bodies[b].rot;
+        P3 cen = p3(0, 0, 0);
+        for (int k = 0; k < cnt; k++) cen = cen + pts[k].p;
+        cen = cen * (1.0f / (float)cnt);
+        float rad = 0.0f;
+        for (int k = 0; k < cnt; k++) rad += plen_e(pts[k].p - cen);
+        m.rad = rad / (float)cnt;
+        bool anchored = false;
+        if (o) {
+            if (o->stick) {
+                P3 wa = pa + m_mulv(ra, o->la_f);
+                P3 wb = b != BNONE ? pb + m_mulv(rbm, o->lb_f) : o->lb_f;
+                float lim = maxf(0.05f, m.rad);
+                if (plen2(wa - cen) < lim * lim && plen2(wb - wa) < 0.03f * 0.03f) {
+                    m.la_f = o->la_f; m.lb_f = o->lb_f; m.fa = wa - pa; m.fb = wb - pb; m.e0 = wb - wa; anchored = true;
+                }
+            }
+            P3 f = o->t1 * o->jt1 + o->t2 * o->jt2;
+            m.jt1 = pdot(f, m.t1); m.jt2 = pdot(f, m.t2); m.jtw = o->jtw * pdot(o->n, n);
+        }
+        if (!anchored) {
+            m.fa = cen - pa; m.fb = cen - pb; m.la_f = m_tmulv(ra, m.fa);
+            m.lb_f = b != BNONE ? m_tmulv(rbm, m.fb) : cen;
+            m.e0 = p3(0, 0, 0);
+        }
+        for (int k = 0; k < cnt; k++) {
+            BCp& c = m.cp[k];
+            c.ra = pts[k].p - pa;
+            c.rb = b != BNONE ? pts[k].p - pb : pts[k].p;
+            c.adj = pts[k].s;
+            c.la = m_tmulv(ra, c.ra);
+            if (o) {
+                float best = 0.03f * 0.03f; int bi = -1;
+                for (uint32_t q = 0; q < o->cnt; q++) { float d = plen2(o->cp[q].la - c.la); if (d < best) { best = d; bi = (int)q; } }
+                if (bi >= 0) c.jn = o->cp[bi].jn;
+            }
+        }
+        man.push_back(m);
+    }
+
+    void collide_all(float) {
+        const uint32_t n = (uint32_t)bodies.size();
+        std::vector<std::pair<uint32_t, uint32_t>> pairs;
+        if (order == BOX_LIST) {                     // phys.rs:361-407
+            for (uint32_t i = 0; i < n; i++) if (bodies[i].awake && bodies[i].amin.y < 0.0f) collide_ground(i);
+            broadphase(pairs);
+            st_pairs = (uint32_t)pairs.size();
+            for (auto& pr : pairs) collide_pair(pr.first, pr.second, nullptr);
+            return;
+        }
+        // key order: for each a its pairs (a, b) by b, then its ground manifold (a, NONE)
+        std::vector<uint8_t> ground(n, 0), defer(n, 0);
+        for (uint32_t i = 0; i < n; i++) ground[i] = bodies[i].awake && bodies[i].amin.y < 0.0f;
+        broadphase(pairs);
+        st_pairs = (uint32_t)pairs.size();
+        std::sort(pairs.begin(), pairs.end());
+        size_t q = 0;
+        for (uint32_t a = 0; a < n; a++) {
+            for (; q < pairs.size() && pairs[q].first == a; q++) collide_pair(a, pairs[q].second, &defer);
+            if (ground[a]) collide_ground(a);
+        }
+        for (uint32_t i = 0; i < n; i++) if (defer[i]) wake(i);
+    }
+
+    // greedy colouring in descending priority (pair_priority of the key, then the earlier manifold first); a colour
+    // is shared only by manifolds with no moving body in common
+    void colour_manifolds() {
+        const uint32_t M = (uint32_t)man.size();
+        std::vector<uint64_t> rank(M);
+        for (uint32_t k = 0; k < M; k++) {
+            const BMan& m = man[k];
+            rank[k] = ((uint64_t)pair_priority(m.a, m.b == BNONE ? 0u : m.b + 1) << 32) | (uint64_t)(0xFFFFFFFFu - k);
+        }
+        std::vector<uint32_t> by(M);
+        for (uint32_t k = 0; k < M; k++) by[k] = k;
+        std::sort(by.begin(), by.end(), [&](uint32_t x, uint32_t y) { return rank[x] > rank[y]; });
+        std::vector<std::vector<uint64_t>> used(sv.size());
+        auto has = [&](uint32_t s, uint32_t c) { return s != 0 && c / 64 < used[s].size() && (used[s][c / 64] >> (c % 64)) & 1; };
+        auto put = [&](uint32_t s, uint32_t c) {
+            if (s == 0) return;
+            if (used[s].size() <= c / 64) used[s].resize(c / 64 + 1, 0);
+            used[s][c / 64] |= 1ull << (c % 64);
+        };
+        for (uint32_t k : by) {
+            BMan& m = man[k];
+            uint32_t c = 0;
+            while (has(m.sa, c) || has(m.sb, c)) c++;
+            m.colour = c;
+            put(m.sa, c); put(m.sb, c);
+            ncolours = std::max(ncolours, c + 1);
+        }
+        std::stable_sort(corder.begin(), corder.end(), [&](uint32_t x, uint32_t y) { return man[x].colour < man[y].colour; });
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+// boxes: n records of p3 q4 h3 density (World::add_box)
+void* obx_create(const float* boxes, uint32_t n, const void* params, int32_t order) {
+    BoxWorld* w = new BoxWorld();
+    std::memcpy(&w->prm, params, sizeof(BoxParams));
+    w->order = order;
+    for (uint32_t i = 0; i < n; i++) {
+        const float* b = boxes + (size_t)i * 11;
+        w->add_box(p3(b[0], b[1], b[2]), q4(b[3], b[4], b[5], b[6]), p3(b[7], b[8], b[9]), b[10]);
+    }
+    return w;
+}
+void obx_destroy(void* w) { delete (BoxWorld*)w; }
+void obx_step(void* w, float dt, uint32_t nsteps) { for (uint32_t k = 0; k < nsteps; k++) ((BoxWorld*)w)->step(dt); }
+// 22 floats a body: p3 q4 v3 w3 sleep_t sleep_p3 sleep_q4 awake
+void obx_read(void* wp, float* out) {
+    BoxWorld* w = (BoxWorld*)wp;
+    for (size_t i = 0; i < w->bodies.size(); i++) {
+        const BBody& b = w->bodies[i];
+        float r[22] = {b.p.x, b.p.y, b.p.z, b.q.x, b.q.y, b.q.z, b.q.w, b.v.x, b.v.y, b.v.z, b.w.x, b.w.y, b.w.z,
+                       b.sleep_t, b.sleep_p.x, b.sleep_p.y, b.sleep_p.z, b.sleep_q.x, b.sleep_q.y, b.sleep_q.z, b.sleep_q.w,
+                       b.awake ? 1.0f : 0.0f};
+        std::memcpy(out + i * 22, r, sizeof(r));
+    }
+}
+// awake, pairs, manifolds, points, colours
+void obx_stats(void* wp, uint32_t* out) {
+    BoxWorld* w = (BoxWorld*)wp;
+    out[0] = w->st_awake; out[1] = w->st_pairs; out[2] = w->st_manifolds; out[3] = w->st_points; out[4] = w->ncolours;
+}
+// 16 words a manifold in list order: a, b, cnt, stick, n3, jn4, jt1, jt2, jtw, colour (floats as bits)
+uint32_t obx_manifolds(void* wp, uint32_t* out, uint32_t cap) {
+    BoxWorld* w = (BoxWorld*)wp;
+    uint32_t k = 0;
+    for (; k < w->man.size() && k < cap; k++) {
+        const BMan& m = w->man[k];
+        float f[12] = {m.n.x, m.n.y, m.n.z, m.cp[0].jn, m.cp[1].jn, m.cp[2].jn, m.cp[3].jn, m.jt1, m.jt2, m.jtw, 0, 0};
+        uint32_t* o = out + (size_t)k * 16;
+        o[0] = m.a; o[1] = m.b; o[2] = m.cnt; o[3] = m.stick;
+        std::memcpy(o + 4, f, 10 * sizeof(float));
+        o[14] = m.colour; o[15] = 0;
+    }
+    return (uint32_t)w->man.size();
+}
+
+}  // extern "C"

@@ -204,6 +204,12 @@ PROTOTYPES = {
     "sf_read_joints": (C.c_int32, [C.c_void_p, _f32p, _f32p, _u8p, _u32p]),
     "sf_collide_boxes": (C.c_int32, [_f32p, _f32p, C.c_uint32, C.c_float, _f32p, _i32p]),
     "sf_collide_hulls": (C.c_int32, [_f32p, C.c_uint32, _f32p, _f32p, C.c_uint32, C.c_float, C.c_int32, _f32p, _i32p]),
+    "sf_box_world_create": (C.c_int32, [_f32p, _u32p, C.c_uint32, C.c_void_p, C.POINTER(_vp)]),
+    "sf_box_world_destroy": (None, [_vp]),
+    "sf_box_world_step": (C.c_int32, [_vp, C.c_float, C.c_uint32]),
+    "sf_box_world_read": (C.c_int32, [_vp, _f32p]),
+    "sf_box_world_stats": (C.c_int32, [_vp, C.c_uint32, C.c_void_p]),
+    "sf_box_world_manifolds": (C.c_int32, [_vp, C.c_uint32, _u32p, C.c_uint32, _u32p]),
     "sf_structure_solve_static": (C.c_int32, [C.c_uint32, _i32p, _u8p, _u8p, _f32p, C.c_float, C.c_float, C.c_uint32,
                                               C.POINTER(C.c_double), _u32p, C.POINTER(C.c_double), C.c_void_p]),
     "sf_structure_solve_set": (C.c_int32, [_vp, _i32p, C.c_uint32, C.c_float, C.c_float, C.c_uint32, C.POINTER(SolveReport)]),
