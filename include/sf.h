@@ -459,6 +459,9 @@ typedef struct sf_box_stats {        /* Stats (phys.rs:108-110) of the last step
     uint32_t reserved;
     float ms;                        /* device time of the last sf_box_world_step call, all its steps */
     uint64_t steps;                  /* steps taken */
+    float phase_ms[5];               /* that call's time in this scene's broadphase, narrow phase and manifolds,
+                                      * colouring, sub-steps, write-back and sleep (Stats::t_broad, t_narrow, t_solve) */
+    uint32_t reserved2;
 } sf_box_stats;
 /* boxes: n records of 11 floats (centre 3, quaternion x y z w, half extents 3, density; density 0 = static), scene
  * s = records [scene_first[s], scene_first[s + 1]). Capacities per scene, on average over its boxes: 27 grid entries,

@@ -128,7 +128,7 @@ class BoxStats(C.Structure):
     """sf_box_stats: the last step's counts of one scene."""
     _fields_ = [("awake", C.c_uint32), ("pairs", C.c_uint32), ("manifolds", C.c_uint32), ("points", C.c_uint32),
                 ("colours", C.c_uint32), ("status", C.c_uint32), ("rounds", C.c_uint32), ("reserved", C.c_uint32),
-                ("ms", C.c_float), ("steps", C.c_uint64)]
+                ("ms", C.c_float), ("steps", C.c_uint64), ("phase_ms", C.c_float * 5), ("reserved2", C.c_uint32)]
 
 
 class BoxWorld:

@@ -18,6 +18,8 @@
 #include <cstring>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "sf_internal.cuh"
 #include "sf_boxsat.cuh"
 
@@ -31,6 +33,8 @@ constexpr uint32_t BX_SHORT = 32;    // pair lists up to this long are sorted by
 constexpr uint32_t BX_EPB = 27;      // grid entries a body may take, on average over its scene
 constexpr uint32_t BX_CPB = 8;       // manifolds a body may take, on average over its scene
 constexpr int BX_MAXC = 128;         // colours
+constexpr uint32_t BX_BIG = 4096;    // scenes above this many boxes step on a thread-block cluster
+constexpr int BX_CL = 16, BX_CL_THREADS = 512;
 enum { BXE_ENTRIES = 1, BXE_PAIRS = 2, BXE_MANIFOLDS = 4, BXE_COLOURS = 8, BXE_GUARD = 16 };
 
 struct DM3 { P3 c[3]; };
@@ -51,10 +55,13 @@ struct BxArgs {
     uint32_t *ent_body, *ent_next, *head; int32_t *ent_cell;
     uint32_t *cand_a, *cand_b, *hit; float *geom;
     DMan *man[2]; uint64_t *mkey[2]; uint32_t *mcount[2];
-    uint32_t *deg, *inc, *colour, *corder;
+    uint32_t *deg, *inc, *colour, *corder, *mwait;
+    uint64_t *mrank;
     P3 *sv, *sw, *sdp, *sth, *sp0; float *sim; DM3 *sii; float4 *sq;
     const uint32_t *sc_b0, *sc_n, *sc_e0, *sc_t0, *sc_tcap, *sc_c0, *sc_m0;   // candidates at c0, manifolds at m0
+    uint32_t *gs;        // BX_G words a scene: the team-wide words of a cluster team
     uint32_t *stats;     // 8 a scene: awake, pairs, manifolds, points, colours, status, JP rounds, 0
+    unsigned long long *tns;   // 5 a scene: ns in broadphase, narrow phase, colouring, sub-steps, write-back and sleep
     sf_box_params P;
 };
 
@@ -114,27 +121,10 @@ __device__ __forceinline__ uint64_t man_rank(uint32_t a, uint32_t b, uint32_t m)
     return ((uint64_t)pair_priority(a, b == BX_NONE ? 0u : b + 1) << 32) | (uint64_t)(0xFFFFFFFFu - m);
 }
 
-// exclusive scan of d[0, n) in place by the whole block; returns the total (to every thread)
-__device__ uint32_t block_scan(uint32_t *d, uint32_t n, uint32_t *wsum) {
-    const uint32_t t = threadIdx.x, T = blockDim.x, lane = t & 31, warp = t >> 5, nw = T >> 5;
-    const uint32_t per = (n + T - 1) / T, lo = min(n, t * per), hi = min(n, lo + per);
-    uint32_t s = 0;
-    for (uint32_t i = lo; i < hi; i++) s += d[i];
-    uint32_t x = s;
-    for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o); if (lane >= (uint32_t)o) x += y; }
-    if (lane == 31) wsum[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t w = lane < nw ? wsum[lane] : 0u;
-        for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o); if (lane >= (uint32_t)o) w += y; }
-        wsum[lane] = w;
-    }
-    __syncthreads();
-    uint32_t run = x - s + (warp ? wsum[warp - 1] : 0u);
-    const uint32_t total = wsum[nw - 1];
-    for (uint32_t i = lo; i < hi; i++) { uint32_t v = d[i]; d[i] = run; run += v; }
-    __syncthreads();
-    return total;
+__device__ __forceinline__ unsigned long long gtime() {
+    unsigned long long x;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(x));
+    return x;
 }
 
 __device__ __forceinline__ Box make_box(const BxBody &b, const DM3 &r) {
@@ -381,25 +371,83 @@ __device__ uint32_t walk_pairs(const BxArgs &A, uint32_t b0, uint32_t e0, uint32
     return k;
 }
 
-// One step of every scene: one block a scene (World::step, phys.rs:152-243).
-template <int T>
-__global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) k_box_step(BxArgs A, float dt, int par) {
+namespace cg = cooperative_groups;
+// team-wide words: errors, colours, grid entries (64-bit), counters, per-block scan totals, round flags, colour counts
+// and colour starts
+enum { G_ERR = 0, G_NCOL = 1, G_NE = 2, G_TOT = 8, G_CTA = 16, G_FLAG = 32, G_CCNT = 64, G_CBEG = 64 + BX_MAXC,
+       BX_G = 64 + 2 * BX_MAXC + 64 };
+
+template <int CL>
+__device__ __forceinline__ void team_sync() {
+    if constexpr (CL == 1) __syncthreads(); else cg::this_cluster().sync();
+}
+// the OR of p over the team; a cluster uses three flags in turn (the one it clears was last read two rounds back)
+template <int CL>
+__device__ __forceinline__ bool team_or(int p, uint32_t *G, uint32_t r, uint32_t t) {
+    if constexpr (CL == 1) {
+        return __syncthreads_or(p) != 0;
+    } else {
+        if (p) atomicOr(&G[G_FLAG + r % 3], 1u);
+        if (t == 0) ((volatile uint32_t *)G)[G_FLAG + (r + 1) % 3] = 0;
+        cg::this_cluster().sync();
+        return ((volatile uint32_t *)G)[G_FLAG + r % 3] != 0;
+    }
+}
+// exclusive scan of d[0, n) in place by the whole team; returns the total (to every thread)
+template <int T, int CL>
+__device__ uint32_t team_scan(uint32_t *d, uint32_t n, uint32_t *wsum, uint32_t *gcta, uint32_t tt, uint32_t rank) {
+    constexpr uint32_t TT = T * CL;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = T >> 5;
+    const uint32_t per = (n + TT - 1) / TT, lo = min(n, tt * per), hi = min(n, lo + per);
+    uint32_t s = 0;
+    for (uint32_t i = lo; i < hi; i++) s += d[i];
+    uint32_t x = s;
+    for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o); if (lane >= (uint32_t)o) x += y; }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < nw ? wsum[lane] : 0u;
+        for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o); if (lane >= (uint32_t)o) w += y; }
+        wsum[lane] = w;
+    }
+    __syncthreads();
+    uint32_t run = x - s + (warp ? wsum[warp - 1] : 0u);
+    uint32_t total = wsum[nw - 1];
+    if constexpr (CL > 1) {
+        if (threadIdx.x == 0) ((volatile uint32_t *)gcta)[rank] = total;
+        cg::this_cluster().sync();
+        uint32_t base = 0, all = 0;
+        for (uint32_t r = 0; r < CL; r++) { const uint32_t v = ((volatile uint32_t *)gcta)[r]; if (r < rank) base += v; all += v; }
+        run += base; total = all;
+    }
+    for (uint32_t i = lo; i < hi; i++) { uint32_t v = d[i]; d[i] = run; run += v; }
+    team_sync<CL>();
+    return total;
+}
+
+// One step of every scene (World::step, phys.rs:152-243): one team a scene, a block (CL = 1) or a thread-block cluster
+// of CL blocks whose barrier is the cluster's; team-wide counters live in shared memory for a block, in global memory
+// for a cluster.
+template <int T, int CL>
+__global__ void __launch_bounds__(T, CL == 1 && T <= 256 ? 2 : 1) k_box_step(BxArgs A, float dt, int par, const uint32_t *slist) {
     __shared__ uint32_t wsum[32];
-    __shared__ uint32_t tot[8];      // -, awake, entry fill, pairs, points, long pair lists
-    __shared__ uint32_t ccnt[BX_MAXC], cbeg[BX_MAXC + 1];
-    __shared__ uint32_t s_err, s_ncol;
-    __shared__ unsigned long long s_ne;
-    const uint32_t sc = blockIdx.x, t = threadIdx.x;
+    __shared__ __align__(8) uint32_t gsh[CL == 1 ? BX_G : 2];
+    constexpr uint32_t TT = T * CL;
+    const uint32_t rank = CL > 1 ? (uint32_t)cg::this_cluster().block_rank() : 0u;
+    const uint32_t sc = slist[blockIdx.x / CL], t = rank * T + threadIdx.x;
+    uint32_t *Gp = CL == 1 ? gsh : A.gs + (size_t)sc * BX_G;
+    volatile uint32_t *GV = Gp;
     const uint32_t b0 = A.sc_b0[sc], n = A.sc_n[sc], s0 = b0 + sc, e0 = A.sc_e0[sc], t0 = A.sc_t0[sc];
     const uint32_t c0 = A.sc_c0[sc], m0 = A.sc_m0[sc], ccap = (BX_PPB + 1) * n, mcap = BX_CPB * n + 64u;
     uint32_t *st = A.stats + (size_t)sc * 8;
     const sf_box_params &P = A.P;
-    if (t < 8) tot[t] = 0;
-    if (t == 0) { s_err = 0; s_ncol = 0; s_ne = 0; }
-    __syncthreads();
+    for (uint32_t k = t; k < G_CCNT; k += TT) GV[k] = 0;
+    unsigned long long *tns = A.tns + (size_t)sc * 5;
+    unsigned long long tm0 = t == 0 ? gtime() : 0ull, tm1 = 0;
+    team_sync<CL>();
     const float spec = P.speculative, inv_cell = __fdiv_rn(1.0f, P.cell);
     // ---- bodies: rotation, AABB with the speculative margin, solver slots (phys.rs:157-171)
-    for (uint32_t i = t; i < n; i += T) {
+    for (uint32_t i = t; i < n; i += TT) {
         const BxBody b = A.body[b0 + i];
         const DM3 r = qm3(b.q);
         P3 e = p3(fabsf(r.c[0].x) * b.h.x + fabsf(r.c[1].x) * b.h.y + fabsf(r.c[2].x) * b.h.z,
@@ -412,9 +460,9 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) k_box_step(BxArgs A, floa
         const uint64_t ne = (uint64_t)(bcell(hi.x, inv_cell) - bcell(lo.x, inv_cell) + 1) *
                             (uint64_t)(bcell(hi.y, inv_cell) - bcell(lo.y, inv_cell) + 1) *
                             (uint64_t)(bcell(hi.z, inv_cell) - bcell(lo.z, inv_cell) + 1);
-        if (ne > (uint64_t)BX_EPB * n) atomicOr(&s_err, (uint32_t)BXE_ENTRIES);
+        if (ne > (uint64_t)BX_EPB * n) atomicOr(&Gp[G_ERR], (uint32_t)BXE_ENTRIES);
         A.ecnt[b0 + i] = ne > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)ne;
-        atomicAdd(&s_ne, (unsigned long long)ne);
+        atomicAdd((unsigned long long *)(Gp + G_NE), (unsigned long long)ne);
         A.wake[b0 + i] = 0;
         A.uf[b0 + i] = i;
         uint32_t slot = 0;
@@ -424,7 +472,7 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) k_box_step(BxArgs A, floa
             A.sv[s] = b.v; A.sw[s] = b.w; A.sdp[s] = p3(0.0f, 0.0f, 0.0f); A.sth[s] = p3(0.0f, 0.0f, 0.0f);
             A.sim[s] = b.inv_m; A.sii[s] = m_sandwich(r, b.inv_i); A.sq[s] = make_float4(b.q[0], b.q[1], b.q[2], b.q[3]);
             A.sp0[s] = b.p;
-            atomicAdd(&tot[1], 1u);
+            atomicAdd(&Gp[G_TOT + 1], 1u);
         }
         A.sidx[b0 + i] = slot;
     }
@@ -434,51 +482,51 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) k_box_step(BxArgs A, floa
         A.sv[s0] = z; A.sw[s0] = z; A.sdp[s0] = z; A.sth[s0] = z; A.sim[s0] = 0.0f; A.sii[s0] = zm;
         A.sq[s0] = make_float4(0.0f, 0.0f, 0.0f, 1.0f); A.sp0[s0] = z;
     }
-    __syncthreads();
-    if (s_err || s_ne > (unsigned long long)BX_EPB * n) {
-        if (t == 0) { st[0] = tot[1]; st[1] = st[2] = st[3] = st[4] = 0; st[5] = BXE_ENTRIES; A.mcount[par][sc] = 0; }
+    team_sync<CL>();
+    if (GV[G_ERR] || (*(volatile unsigned long long *)(Gp + G_NE)) > (unsigned long long)BX_EPB * n) {
+        if (t == 0) { st[0] = GV[G_TOT + 1]; st[1] = st[2] = st[3] = st[4] = 0; st[5] = BXE_ENTRIES; A.mcount[par][sc] = 0; }
         return;
     }
-    const uint32_t ne_tot = (uint32_t)s_ne;
+    const uint32_t ne_tot = (uint32_t)(*(volatile unsigned long long *)(Gp + G_NE));
     uint32_t tbl = 1;
     while (tbl < ne_tot * 2u) tbl <<= 1;
     if (tbl > A.sc_tcap[sc]) {
-        if (t == 0) { st[0] = tot[1]; st[1] = st[2] = st[3] = st[4] = 0; st[5] = BXE_ENTRIES; A.mcount[par][sc] = 0; }
+        if (t == 0) { st[0] = GV[G_TOT + 1]; st[1] = st[2] = st[3] = st[4] = 0; st[5] = BXE_ENTRIES; A.mcount[par][sc] = 0; }
         return;
     }
     const uint32_t mask = tbl - 1;
-    for (uint32_t k = t; k < tbl; k += T) A.head[t0 + k] = BX_NONE;
-    __syncthreads();
+    for (uint32_t k = t; k < tbl; k += TT) A.head[t0 + k] = BX_NONE;
+    team_sync<CL>();
     // ---- grid: one entry per body and covered cell, chained per hash slot
-    for (uint32_t i = t; i < n; i += T) {
+    for (uint32_t i = t; i < n; i += TT) {
         const P3 lo = A.amin[b0 + i], hi = A.amax[b0 + i];
         const int32_t x0 = bcell(lo.x, inv_cell), y0 = bcell(lo.y, inv_cell), z0 = bcell(lo.z, inv_cell);
         const int32_t x1 = bcell(hi.x, inv_cell), y1 = bcell(hi.y, inv_cell), z1 = bcell(hi.z, inv_cell);
         for (int32_t x = x0; x <= x1; x++) for (int32_t y = y0; y <= y1; y++) for (int32_t z = z0; z <= z1; z++) {
-            const uint32_t e = atomicAdd(&tot[2], 1u);
+            const uint32_t e = atomicAdd(&Gp[G_TOT + 2], 1u);
             A.ent_body[e0 + e] = i;
             A.ent_cell[3 * (size_t)(e0 + e)] = x; A.ent_cell[3 * (size_t)(e0 + e) + 1] = y; A.ent_cell[3 * (size_t)(e0 + e) + 2] = z;
             A.ent_next[e0 + e] = atomicExch(&A.head[t0 + (bhash(x, y, z) & mask)], e);
         }
     }
-    __syncthreads();
+    team_sync<CL>();
     // ---- pairs (phys.rs:385-404): each body lists, sorted, the overlapping bodies above it that the grid reports in
     // the cell holding the larger of the two minimum corners; then its ground contact (phys.rs:362-365). Counted,
     // scanned, then written; a list of more than BX_SHORT pairs (a static slab under a pile) is sorted by the block.
-    for (uint32_t a = t; a < n; a += T) {
+    for (uint32_t a = t; a < n; a += TT) {
         const uint32_t k = walk_pairs(A, b0, e0, t0, mask, ne_tot, inv_cell, a, nullptr, nullptr);
-        atomicAdd(&tot[3], k);
+        atomicAdd(&Gp[G_TOT + 3], k);
         A.cand_n[b0 + a] = k + (A.body[b0 + a].awake && A.amin[b0 + a].y < 0.0f ? 1u : 0u);
     }
-    __syncthreads();
-    const uint32_t nc = block_scan(A.cand_n + b0, n, wsum);
+    team_sync<CL>();
+    const uint32_t nc = team_scan<T, CL>(A.cand_n + b0, n, wsum, Gp + G_CTA, t, rank);
     if (nc > ccap) {
-        if (t == 0) { st[0] = tot[1]; st[1] = tot[3]; st[2] = st[3] = st[4] = 0; st[5] = BXE_PAIRS; A.mcount[par][sc] = 0; }
+        if (t == 0) { st[0] = GV[G_TOT + 1]; st[1] = GV[G_TOT + 3]; st[2] = st[3] = st[4] = 0; st[5] = BXE_PAIRS; A.mcount[par][sc] = 0; }
         return;
     }
-    if (t == 0) tot[5] = 0;
-    __syncthreads();
-    for (uint32_t a = t; a < n; a += T) {
+    if (t == 0) GV[G_TOT + 5] = 0;
+    team_sync<CL>();
+    for (uint32_t a = t; a < n; a += TT) {
         const uint32_t off = A.cand_n[b0 + a];
         uint32_t *cb = A.cand_b + c0 + off;
         const uint32_t k = walk_pairs(A, b0, e0, t0, mask, ne_tot, inv_cell, a, A.cand_a + c0 + off, cb);
@@ -490,43 +538,44 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) k_box_step(BxArgs A, floa
                 cb[y] = v;
             }
         } else {
-            A.seglong[b0 + atomicAdd(&tot[5], 1u)] = a;
+            A.seglong[b0 + atomicAdd(&Gp[G_TOT + 5], 1u)] = a;
         }
         if (A.body[b0 + a].awake && A.amin[b0 + a].y < 0.0f) { A.cand_a[c0 + off + k] = a; A.cand_b[c0 + off + k] = BX_NONE; }
     }
-    __syncthreads();
+    team_sync<CL>();
     // long lists: the pair partners are distinct bodies, so a bitmap over the scene's bodies and a scan of its
     // population counts put them in order
-    const uint32_t nlong = tot[5], nwords = (n + 31) / 32;
+    const uint32_t nlong = GV[G_TOT + 5], nwords = (n + 31) / 32;
     for (uint32_t q = 0; q < nlong; q++) {
         const uint32_t a = A.seglong[b0 + q];
         const uint32_t off = A.cand_n[b0 + a], next = a + 1 < n ? A.cand_n[b0 + a + 1] : nc;
         const uint32_t k = next - off - (A.body[b0 + a].awake && A.amin[b0 + a].y < 0.0f ? 1u : 0u);
         uint32_t *bits = A.mint + b0, *pos = A.ecnt + b0, *cb = A.cand_b + c0 + off;
-        for (uint32_t x = t; x < nwords; x += T) bits[x] = 0;
-        __syncthreads();
-        for (uint32_t x = t; x < k; x += T) atomicOr(&bits[cb[x] >> 5], 1u << (cb[x] & 31));
-        __syncthreads();
-        for (uint32_t x = t; x < nwords; x += T) pos[x] = __popc(bits[x]);
-        __syncthreads();
-        block_scan(pos, nwords, wsum);
-        for (uint32_t x = t; x < nwords; x += T) {
+        for (uint32_t x = t; x < nwords; x += TT) bits[x] = 0;
+        team_sync<CL>();
+        for (uint32_t x = t; x < k; x += TT) atomicOr(&bits[cb[x] >> 5], 1u << (cb[x] & 31));
+        team_sync<CL>();
+        for (uint32_t x = t; x < nwords; x += TT) pos[x] = __popc(bits[x]);
+        team_sync<CL>();
+        team_scan<T, CL>(pos, nwords, wsum, Gp + G_CTA, t, rank);
+        for (uint32_t x = t; x < nwords; x += TT) {
             uint32_t wv = bits[x], r = pos[x];
             while (wv) { const uint32_t bit = __ffs(wv) - 1; cb[r++] = x * 32 + bit; wv &= wv - 1; }
         }
-        __syncthreads();
+        team_sync<CL>();
     }
+    if (t == 0) { tm1 = gtime(); tns[0] += tm1 - tm0; tm0 = tm1; }
     // ---- narrow phase, then the manifolds in key order (phys.rs:406-497)
-    for (uint32_t c = t; c < nc; c += T)
+    for (uint32_t c = t; c < nc; c += TT)
         A.hit[c0 + c] = collide_candidate(A, b0, A.cand_a[c0 + c], A.cand_b[c0 + c], A.geom + (size_t)(c0 + c) * 20) ? 1u : 0u;
-    __syncthreads();
-    const uint32_t M = block_scan(A.hit + c0, nc, wsum);
+    team_sync<CL>();
+    const uint32_t M = team_scan<T, CL>(A.hit + c0, nc, wsum, Gp + G_CTA, t, rank);
     if (M > mcap) {
-        if (t == 0) { st[0] = tot[1]; st[1] = tot[3]; st[2] = M; st[3] = st[4] = 0; st[5] = BXE_MANIFOLDS; A.mcount[par][sc] = 0; }
+        if (t == 0) { st[0] = GV[G_TOT + 1]; st[1] = GV[G_TOT + 3]; st[2] = M; st[3] = st[4] = 0; st[5] = BXE_MANIFOLDS; A.mcount[par][sc] = 0; }
         return;
     }
     const uint32_t nold = A.mcount[par ^ 1][sc];
-    for (uint32_t c = t; c < nc; c += T) {
+    for (uint32_t c = t; c < nc; c += TT) {
         const float *g = A.geom + (size_t)(c0 + c) * 20;
         const int cnt = __float_as_int(g[3]);
         if (!cnt) continue;
@@ -534,89 +583,116 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) k_box_step(BxArgs A, floa
         const uint32_t a = A.cand_a[c0 + c], b = A.cand_b[c0 + c];
         build_manifold(A, par, b0, s0, m0, nold, a, b, g, A.man[par][m0 + m]);
         A.mkey[par][m0 + m] = ((uint64_t)a << 32) | b;
-        atomicAdd(&tot[4], (uint32_t)cnt);
+        atomicAdd(&Gp[G_TOT + 4], (uint32_t)cnt);
     }
     // the wakes (phys.rs:410-417): the body joins the solver from the next step
-    for (uint32_t i = t; i < n; i += T) {
+    for (uint32_t i = t; i < n; i += TT) {
         if (!A.wake[b0 + i]) continue;
         BxBody &b = A.body[b0 + i];
         if (b.awake || b.inv_m == 0.0f) continue;
         b.awake = 1; b.sleep_t = 0.0f; b.sleep_p = b.p;
         b.sleep_q[0] = b.q[0]; b.sleep_q[1] = b.q[1]; b.sleep_q[2] = b.q[2]; b.sleep_q[3] = b.q[3];
     }
-    __syncthreads();
+    team_sync<CL>();
+    if (t == 0) { tm1 = gtime(); tns[1] += tm1 - tm0; tm0 = tm1; }
     // ---- colouring: greedy in descending priority, by Jones-Plassmann rounds. A manifold takes the smallest colour
     // its higher-priority neighbours (manifolds sharing a moving body) left free once all of them have one.
     const uint32_t ns = n + 1;
-    for (uint32_t k = t; k < ns; k += T) A.deg[s0 + k] = 0;
-    for (uint32_t m = t; m < M; m += T) A.colour[m0 + m] = BX_UNC;
-    __syncthreads();
-    for (uint32_t m = t; m < M; m += T) {
+    for (uint32_t k = t; k < ns; k += TT) A.deg[s0 + k] = 0;
+    for (uint32_t m = t; m < M; m += TT) A.colour[m0 + m] = BX_UNC;
+    team_sync<CL>();
+    for (uint32_t m = t; m < M; m += TT) {
         const DMan &mm = A.man[par][m0 + m];
         if (mm.sa) atomicAdd(&A.deg[s0 + mm.sa], 1u);
         if (mm.sb) atomicAdd(&A.deg[s0 + mm.sb], 1u);
     }
-    __syncthreads();
-    block_scan(A.deg + s0, ns, wsum);
-    for (uint32_t m = t; m < M; m += T) {
+    team_sync<CL>();
+    team_scan<T, CL>(A.deg + s0, ns, wsum, Gp + G_CTA, t, rank);
+    for (uint32_t m = t; m < M; m += TT) {
         const DMan &mm = A.man[par][m0 + m];
         if (mm.sa) A.inc[2 * (size_t)m0 + atomicAdd(&A.deg[s0 + mm.sa], 1u)] = m;
         if (mm.sb) A.inc[2 * (size_t)m0 + atomicAdd(&A.deg[s0 + mm.sb], 1u)] = m;
     }
-    __syncthreads();
-    // incident list of slot k: [k ? deg[k - 1] : 0, deg[k])
+    team_sync<CL>();
+    // incident list of slot k: [k ? deg[k - 1] : 0, deg[k]). Each manifold counts its higher-priority neighbours;
+    // a coloured manifold counts its lower-priority neighbours down, and one whose count reaches 0 takes its colour.
     volatile uint32_t *col = A.colour + m0;
+    uint64_t *prio = A.mrank + m0;
+    uint32_t *wait = A.mwait + m0;
+    for (uint32_t m = t; m < M; m += TT) { const DMan &mm = A.man[par][m0 + m]; prio[m] = man_rank(mm.a, mm.b, m); }
+    team_sync<CL>();
+    for (uint32_t m = t; m < M; m += TT) {
+        const DMan &mm = A.man[par][m0 + m];
+        const uint64_t rk = prio[m];
+        uint32_t hi_n = 0;
+        for (int side = 0; side < 2; side++) {
+            const uint32_t sl = side ? mm.sb : mm.sa;
+            if (!sl) continue;
+            for (uint32_t q = A.deg[s0 + sl - 1], e = A.deg[s0 + sl]; q < e; q++) {
+                const uint32_t o = A.inc[2 * (size_t)m0 + q];
+                if (o != m && prio[o] > rk) hi_n++;
+            }
+        }
+        wait[m] = hi_n;
+    }
+    team_sync<CL>();
     uint32_t rounds = 0;
     for (;;) {
         int pend = 0;
-        for (uint32_t m = t; m < M; m += T) {
+        for (uint32_t m = t; m < M; m += TT) {
             if (col[m] != BX_UNC) continue;
+            if (((volatile uint32_t *)wait)[m] != 0) { pend = 1; continue; }
+            if constexpr (CL == 1) __threadfence_block(); else __threadfence();
             const DMan &mm = A.man[par][m0 + m];
-            const uint64_t rk = man_rank(mm.a, mm.b, m);
+            const uint64_t rk = prio[m];
             uint64_t used0 = 0, used1 = 0;
-            bool ready = true;
-            for (int side = 0; side < 2 && ready; side++) {
+            for (int side = 0; side < 2; side++) {
                 const uint32_t sl = side ? mm.sb : mm.sa;
                 if (!sl) continue;
-                const uint32_t lo = sl ? A.deg[s0 + sl - 1] : 0u, hi = A.deg[s0 + sl];
-                for (uint32_t q = lo; q < hi; q++) {
+                for (uint32_t q = A.deg[s0 + sl - 1], e = A.deg[s0 + sl]; q < e; q++) {
                     const uint32_t o = A.inc[2 * (size_t)m0 + q];
-                    if (o == m) continue;
-                    const DMan &om = A.man[par][m0 + o];
-                    if (man_rank(om.a, om.b, o) < rk) continue;
+                    if (o == m || prio[o] < rk) continue;
                     const uint32_t oc = col[o];
-                    if (oc == BX_UNC) { ready = false; break; }
-                    if (oc < 64) used0 |= 1ull << oc; else used1 |= 1ull << (oc - 64);
+                    if (oc < 64) used0 |= 1ull << oc; else if (oc < 128) used1 |= 1ull << (oc - 64);
                 }
             }
-            if (!ready) { pend = 1; continue; }
             uint32_t c = ~used0 ? (uint32_t)__ffsll((long long)~used0) - 1 : (~used1 ? 64u + (uint32_t)__ffsll((long long)~used1) - 1 : (uint32_t)BX_MAXC);
-            if (c >= (uint32_t)BX_MAXC) { atomicOr(&s_err, (uint32_t)BXE_COLOURS); c = BX_MAXC - 1; }
+            if (c >= (uint32_t)BX_MAXC) { atomicOr(&Gp[G_ERR], (uint32_t)BXE_COLOURS); c = BX_MAXC - 1; }
             col[m] = c;
+            if constexpr (CL == 1) __threadfence_block(); else __threadfence();
+            for (int side = 0; side < 2; side++) {
+                const uint32_t sl = side ? mm.sb : mm.sa;
+                if (!sl) continue;
+                for (uint32_t q = A.deg[s0 + sl - 1], e = A.deg[s0 + sl]; q < e; q++) {
+                    const uint32_t o = A.inc[2 * (size_t)m0 + q];
+                    if (o != m && prio[o] < rk) atomicSub(&wait[o], 1u);
+                }
+            }
         }
         rounds++;
-        if (!__syncthreads_or(pend)) break;
-        if (rounds > M + 1) { if (t == 0) atomicOr(&s_err, (uint32_t)BXE_GUARD); break; }
+        if (!team_or<CL>(pend, Gp, rounds, t)) break;
+        if (rounds > M + 1) { if (t == 0) atomicOr(&Gp[G_ERR], (uint32_t)BXE_GUARD); break; }
     }
-    __syncthreads();
-    if (s_err) {
-        if (t == 0) { st[0] = tot[1]; st[1] = tot[3]; st[2] = M; st[3] = tot[4]; st[4] = 0; st[5] = s_err; A.mcount[par][sc] = 0; }
+    team_sync<CL>();
+    if (GV[G_ERR]) {
+        if (t == 0) { st[0] = GV[G_TOT + 1]; st[1] = GV[G_TOT + 3]; st[2] = M; st[3] = GV[G_TOT + 4]; st[4] = 0; st[5] = GV[G_ERR]; A.mcount[par][sc] = 0; }
         return;
     }
-    for (uint32_t k = t; k < BX_MAXC; k += T) ccnt[k] = 0;
-    __syncthreads();
-    for (uint32_t m = t; m < M; m += T) atomicAdd(&ccnt[col[m]], 1u);
-    __syncthreads();
+    for (uint32_t k = t; k < BX_MAXC; k += TT) GV[G_CCNT + k] = 0;
+    team_sync<CL>();
+    for (uint32_t m = t; m < M; m += TT) atomicAdd(&Gp[G_CCNT + col[m]], 1u);
+    team_sync<CL>();
     if (t == 0) {
         uint32_t run = 0, nc2 = 0;
-        for (int k = 0; k < BX_MAXC; k++) { cbeg[k] = run; run += ccnt[k]; if (ccnt[k]) nc2 = k + 1; ccnt[k] = cbeg[k]; }
-        cbeg[BX_MAXC] = run;
-        s_ncol = nc2;
+        for (int k = 0; k < BX_MAXC; k++) { GV[G_CBEG + k] = run; run += GV[G_CCNT + k]; if (GV[G_CCNT + k]) nc2 = k + 1; GV[G_CCNT + k] = GV[G_CBEG + k]; }
+        GV[G_CBEG + BX_MAXC] = run;
+        GV[G_NCOL] = nc2;
     }
-    __syncthreads();
-    for (uint32_t m = t; m < M; m += T) A.corder[m0 + atomicAdd(&ccnt[col[m]], 1u)] = m;
-    __syncthreads();
-    const uint32_t ncol = s_ncol;
+    team_sync<CL>();
+    for (uint32_t m = t; m < M; m += TT) A.corder[m0 + atomicAdd(&Gp[G_CCNT + col[m]], 1u)] = m;
+    team_sync<CL>();
+    const uint32_t ncol = GV[G_NCOL];
+    if (t == 0) { tm1 = gtime(); tns[2] += tm1 - tm0; tm0 = tm1; }
     // ---- sub-steps (phys.rs:182-231): gravity and the spin clamp, warm start, biased solve, integrate, relax
     const uint32_t sub = P.substeps > 0 ? P.substeps : 1u;
     const float h = dt / (float)sub;
@@ -633,7 +709,7 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) k_box_step(BxArgs A, floa
     DMan *man = A.man[par] + m0;
     const uint32_t *ord = A.corder + m0;
     for (uint32_t s = 0; s < sub; s++) {
-        for (uint32_t i = t; i < n; i += T) {
+        for (uint32_t i = t; i < n; i += TT) {
             const uint32_t sl = A.sidx[b0 + i];
             if (!sl) continue;
             A.sv[s0 + sl] = A.sv[s0 + sl] + g * h;
@@ -641,32 +717,33 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) k_box_step(BxArgs A, floa
             const float wl = plen2(w);
             if (wl > wmax * wmax) A.sw[s0 + sl] = w * __fdiv_rn(wmax, sqrt_e(wl));
         }
-        __syncthreads();
+        team_sync<CL>();
         for (uint32_t c = 0; c < ncol; c++) {
-            for (uint32_t k = cbeg[c] + t; k < cbeg[c + 1]; k += T) warm_manifold(A, s0, man[ord[k]]);
-            __syncthreads();
+            for (uint32_t k = GV[G_CBEG + c] + t; k < GV[G_CBEG + c + 1]; k += TT) warm_manifold(A, s0, man[ord[k]]);
+            team_sync<CL>();
         }
         for (uint32_t c = 0; c < ncol; c++) {
-            for (uint32_t k = cbeg[c] + t; k < cbeg[c + 1]; k += T)
+            for (uint32_t k = GV[G_CBEG + c] + t; k < GV[G_CBEG + c + 1]; k += TT)
                 solve_manifold(A, s0, man[ord[k]], true, inv_h, bias_rate, mass_scale, imp_scale);
-            __syncthreads();
+            team_sync<CL>();
         }
-        for (uint32_t i = t; i < n; i += T) {
+        for (uint32_t i = t; i < n; i += TT) {
             const uint32_t sl = A.sidx[b0 + i];
             if (!sl) continue;
             const P3 v = A.sv[s0 + sl], w = A.sw[s0 + sl];
             A.sdp[s0 + sl] = A.sdp[s0 + sl] + v * h; A.sth[s0 + sl] = A.sth[s0 + sl] + w * h;
             A.sq[s0 + sl] = qintegrate(A.sq[s0 + sl], w, h);
         }
-        __syncthreads();
+        team_sync<CL>();
         for (uint32_t c = 0; c < ncol; c++) {
-            for (uint32_t k = cbeg[c] + t; k < cbeg[c + 1]; k += T)
+            for (uint32_t k = GV[G_CBEG + c] + t; k < GV[G_CBEG + c + 1]; k += TT)
                 solve_manifold(A, s0, man[ord[k]], false, inv_h, bias_rate, mass_scale, imp_scale);
-            __syncthreads();
+            team_sync<CL>();
         }
     }
+    if (t == 0) { tm1 = gtime(); tns[3] += tm1 - tm0; tm0 = tm1; }
     // ---- write back (phys.rs:233-236), then islands and sleep (phys.rs:326-354)
-    for (uint32_t i = t; i < n; i += T) {
+    for (uint32_t i = t; i < n; i += TT) {
         const uint32_t sl = A.sidx[b0 + i];
         if (!sl) continue;
         BxBody &b = A.body[b0 + i];
@@ -675,8 +752,8 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) k_box_step(BxArgs A, floa
         b.q[0] = q.x; b.q[1] = q.y; b.q[2] = q.z; b.q[3] = q.w;
     }
     uint32_t *uf = A.uf + b0;
-    for (uint32_t i = t; i < n; i += T) A.mint[b0 + i] = 0x7F7FFFFFu;
-    for (uint32_t m = t; m < M; m += T) {
+    for (uint32_t i = t; i < n; i += TT) A.mint[b0 + i] = 0x7F7FFFFFu;
+    for (uint32_t m = t; m < M; m += TT) {
         const DMan &mm = man[m];
         if (!mm.sa || !mm.sb) continue;
         uint32_t x = mm.a, y = mm.b;
@@ -687,9 +764,9 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) k_box_step(BxArgs A, floa
             if (atomicCAS(&uf[x], x, y) == x) break;
         }
     }
-    __syncthreads();
+    team_sync<CL>();
     const float l2 = P.sleep_lin * P.sleep_lin, ang2 = P.sleep_ang * P.sleep_ang;
-    for (uint32_t i = t; i < n; i += T) {
+    for (uint32_t i = t; i < n; i += TT) {
         BxBody &b = A.body[b0 + i];
         if (!b.awake) continue;
         const float4 dq = qmul(make_float4(b.q[0], b.q[1], b.q[2], b.q[3]), make_float4(-b.sleep_q[0], -b.sleep_q[1], -b.sleep_q[2], b.sleep_q[3]));
@@ -702,9 +779,9 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) k_box_step(BxArgs A, floa
         }
         if (P.allow_sleep) atomicMin(&A.mint[b0 + uf_root(uf, i)], __float_as_uint(b.sleep_t));
     }
-    __syncthreads();
+    team_sync<CL>();
     if (P.allow_sleep) {
-        for (uint32_t i = t; i < n; i += T) {
+        for (uint32_t i = t; i < n; i += TT) {
             BxBody &b = A.body[b0 + i];
             if (!b.awake) continue;
             if (__uint_as_float(A.mint[b0 + uf_root(uf, i)]) >= P.sleep_time) {
@@ -713,7 +790,8 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) k_box_step(BxArgs A, floa
         }
     }
     if (t == 0) {
-        st[0] = tot[1]; st[1] = tot[3]; st[2] = M; st[3] = tot[4]; st[4] = ncol; st[5] = 0; st[6] = rounds; st[7] = 0;
+        st[0] = GV[G_TOT + 1]; st[1] = GV[G_TOT + 3]; st[2] = M; st[3] = GV[G_TOT + 4]; st[4] = ncol; st[5] = 0; st[6] = rounds; st[7] = 0;
+        tns[4] += gtime() - tm0;
         A.mcount[par][sc] = M;
     }
 }
@@ -733,11 +811,15 @@ struct sf_box_world {
     DBuf<float> sim, geom;
     DBuf<float4> sq;
     DBuf<uint32_t> ecnt, sidx, cand_n, seglong, uf, mint, ent_body, ent_next, head, cand_a, cand_b, hit, deg, inc, colour,
-        corder, stats, mcount0, mcount1, sc_b0, sc_n, sc_e0, sc_t0, sc_tcap, sc_c0, sc_m0;
+        corder, mwait, stats, mcount0, mcount1, sc_b0, sc_n, sc_e0, sc_t0, sc_tcap, sc_c0, sc_m0;
     DBuf<int32_t> ent_cell;
     DBuf<uint8_t> wake;
     DBuf<DMan> man0, man1;
-    DBuf<uint64_t> mkey0, mkey1;
+    DBuf<uint64_t> mkey0, mkey1, mrank;
+    DBuf<unsigned long long> tns;
+    DBuf<uint32_t> gs, slist;
+    uint32_t n_small = 0, n_big = 0;
+    bool cluster_ok = false;
     int par = 0;
     uint64_t steps = 0;
     float last_ms = 0.0f;
@@ -817,9 +899,10 @@ extern "C" sf_status sf_box_world_create(const float *boxes, const uint32_t *sce
     A(w->sim.alloc(ns)); A(w->sq.alloc(ns)); A(w->deg.alloc(ns));
     A(w->ent_body.alloc(et)); A(w->ent_next.alloc(et)); A(w->ent_cell.alloc(3 * et)); A(w->head.alloc(tt));
     A(w->cand_a.alloc(ct)); A(w->cand_b.alloc(ct)); A(w->hit.alloc(ct)); A(w->geom.alloc(20 * ct));
-    A(w->colour.alloc(mt)); A(w->corder.alloc(mt)); A(w->inc.alloc(2 * mt));
+    A(w->colour.alloc(mt)); A(w->corder.alloc(mt)); A(w->mwait.alloc(mt)); A(w->mrank.alloc(mt)); A(w->inc.alloc(2 * mt));
     A(w->man0.alloc(mt)); A(w->man1.alloc(mt)); A(w->mkey0.alloc(mt)); A(w->mkey1.alloc(mt));
-    A(w->stats.alloc((size_t)n_scenes * 8)); A(w->mcount0.alloc(n_scenes)); A(w->mcount1.alloc(n_scenes));
+    A(w->stats.alloc((size_t)n_scenes * 8)); A(w->tns.alloc((size_t)n_scenes * 5));
+    A(w->gs.alloc((size_t)n_scenes * BX_G)); A(w->slist.alloc(n_scenes)); A(w->mcount0.alloc(n_scenes)); A(w->mcount1.alloc(n_scenes));
     A(w->sc_b0.alloc(n_scenes)); A(w->sc_n.alloc(n_scenes)); A(w->sc_e0.alloc(n_scenes)); A(w->sc_t0.alloc(n_scenes));
     A(w->sc_tcap.alloc(n_scenes)); A(w->sc_c0.alloc(n_scenes)); A(w->sc_m0.alloc(n_scenes));
     if (bad) { delete w; set_error("device allocation failed"); return SF_ERR_CUDA; }
@@ -835,6 +918,27 @@ extern "C" sf_status sf_box_world_create(const float *boxes, const uint32_t *sce
     cudaMemcpy(w->sc_c0.p, w->c0.data(), n_scenes * 4, cudaMemcpyHostToDevice);
     if (cudaMemcpy(w->sc_m0.p, w->m0.data(), n_scenes * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
         delete w; set_error("upload failed"); return SF_ERR_CUDA;
+    }
+    {
+        std::vector<uint32_t> big, small;
+        for (uint32_t s = 0; s < n_scenes; s++) (w->nn[s] > BX_BIG ? big : small).push_back(s);
+        w->n_big = (uint32_t)big.size(); w->n_small = (uint32_t)small.size();
+        big.insert(big.end(), small.begin(), small.end());
+        cudaMemcpy(w->slist.p, big.data(), n_scenes * 4, cudaMemcpyHostToDevice);
+        if (w->n_big) {
+            cudaFuncSetAttribute(k_box_step<BX_CL_THREADS, BX_CL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            cudaLaunchConfig_t c = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = BX_CL; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+            c.gridDim = dim3(BX_CL);
+            c.blockDim = dim3(BX_CL_THREADS);
+            c.attrs = at;
+            c.numAttrs = 1;
+            int ncl = 0;
+            if (cudaOccupancyMaxActiveClusters(&ncl, k_box_step<BX_CL_THREADS, BX_CL>, &c) != cudaSuccess) { ncl = 0; cudaGetLastError(); }
+            w->cluster_ok = ncl > 0;
+        }
     }
     sf_status r = box_upload(w, boxes);
     if (r != SF_OK) { delete w; return r; }
@@ -854,15 +958,30 @@ extern "C" sf_status sf_box_world_step(sf_box_world *w, float dt, uint32_t nstep
     a.cand_a = w->cand_a.p; a.cand_b = w->cand_b.p; a.hit = w->hit.p; a.geom = w->geom.p;
     a.man[0] = w->man0.p; a.man[1] = w->man1.p; a.mkey[0] = w->mkey0.p; a.mkey[1] = w->mkey1.p;
     a.mcount[0] = w->mcount0.p; a.mcount[1] = w->mcount1.p;
-    a.deg = w->deg.p; a.inc = w->inc.p; a.colour = w->colour.p; a.corder = w->corder.p;
+    a.deg = w->deg.p; a.inc = w->inc.p; a.colour = w->colour.p; a.corder = w->corder.p; a.mwait = w->mwait.p; a.mrank = w->mrank.p;
     a.sv = w->sv.p; a.sw = w->sw.p; a.sdp = w->sdp.p; a.sth = w->sth.p; a.sp0 = w->sp0.p; a.sim = w->sim.p; a.sii = w->sii.p;
     a.sq = w->sq.p;
     a.sc_b0 = w->sc_b0.p; a.sc_n = w->sc_n.p; a.sc_e0 = w->sc_e0.p; a.sc_t0 = w->sc_t0.p; a.sc_tcap = w->sc_tcap.p;
-    a.sc_c0 = w->sc_c0.p; a.sc_m0 = w->sc_m0.p; a.stats = w->stats.p; a.P = w->P;
+    a.sc_c0 = w->sc_c0.p; a.sc_m0 = w->sc_m0.p; a.stats = w->stats.p; a.tns = w->tns.p; a.gs = w->gs.p; a.P = w->P;
+    SF_CUDA(cudaMemsetAsync(w->tns.p, 0, (size_t)w->n_scenes * 5 * sizeof(unsigned long long), w->stream));
     SF_CUDA(cudaEventRecord(w->ev0, w->stream));
     for (uint32_t k = 0; k < nsteps; k++) {
-        if (w->max_n > 4096) k_box_step<1024><<<w->n_scenes, 1024, 0, w->stream>>>(a, dt, w->par);
-        else k_box_step<256><<<w->n_scenes, 256, 0, w->stream>>>(a, dt, w->par);
+        // scenes of more than BX_BIG boxes: one 16-block cluster each; the rest: one block each
+        if (w->n_big && w->cluster_ok) {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = BX_CL; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(w->n_big * BX_CL);
+            cfg.blockDim = dim3(BX_CL_THREADS);
+            cfg.stream = w->stream;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            SF_CUDA(cudaLaunchKernelEx(&cfg, k_box_step<BX_CL_THREADS, BX_CL>, a, dt, w->par, (const uint32_t *)w->slist.p));
+        } else if (w->n_big) {
+            k_box_step<1024, 1><<<w->n_big, 1024, 0, w->stream>>>(a, dt, w->par, w->slist.p);
+        }
+        if (w->n_small) k_box_step<256, 1><<<w->n_small, 256, 0, w->stream>>>(a, dt, w->par, w->slist.p + w->n_big);
         w->par ^= 1;
     }
     SF_CUDA(cudaGetLastError());
@@ -902,6 +1021,9 @@ extern "C" sf_status sf_box_world_stats(sf_box_world *w, uint32_t scene, sf_box_
     SF_CUDA(cudaMemcpy(st, w->stats.p + (size_t)scene * 8, 32, cudaMemcpyDeviceToHost));
     out->awake = st[0]; out->pairs = st[1]; out->manifolds = st[2]; out->points = st[3]; out->colours = st[4];
     out->status = st[5]; out->rounds = st[6]; out->ms = w->last_ms; out->steps = w->steps;
+    unsigned long long tn[5];
+    SF_CUDA(cudaMemcpy(tn, w->tns.p + (size_t)scene * 5, sizeof(tn), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 5; k++) out->phase_ms[k] = (float)(tn[k] * 1e-6);
     return SF_OK;
 }
 
