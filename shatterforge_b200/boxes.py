@@ -187,3 +187,31 @@ class BoxWorld:
             self._check(self._lib.sf_box_world_manifolds(self._h, scene, self._ptr(out, C.c_uint32), cnt.value,
                                                          C.byref(cnt)), "sf_box_world_manifolds")
         return out
+
+
+def main(argv=None) -> None:
+    """Steps the reference's pile (or several copies of it, one scene each) and prints the device time a step:
+    python -m shatterforge_b200.boxes --boxes 20000 --scenes 1 --warmup 60 --steps 20"""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--boxes", type=int, default=20000)
+    ap.add_argument("--scenes", type=int, default=1)
+    ap.add_argument("--substeps", type=int, default=12)
+    ap.add_argument("--warmup", type=int, default=60)
+    ap.add_argument("--steps", type=int, default=20)
+    a = ap.parse_args(argv)
+    dt = np.float32(1.0 / 60.0)
+    w = BoxWorld([pile(a.boxes)] * a.scenes, box_params(allow_sleep=0, substeps=a.substeps))
+    w.step(dt, a.warmup)
+    w.step(dt, a.steps)
+    st = w.stats(0)
+    print(json.dumps({"boxes": a.boxes, "scenes": a.scenes, "substeps": a.substeps, "ms_per_step": st.ms / a.steps,
+                      "box_steps_per_s": a.boxes * a.scenes * a.steps / (st.ms * 1e-3), "pairs": st.pairs,
+                      "manifolds": st.manifolds, "colours": st.colours,
+                      "phase_ms_per_step": [x / a.steps for x in st.phase_ms]}))
+    w.close()
+
+
+if __name__ == "__main__":
+    main()
