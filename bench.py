@@ -673,6 +673,21 @@ def boxes_section(args):
     out["e2e"] = {"ms_per_step": e2e_s * 1e3 / (args.box_warmup + args.box_steps),
                   "note": "wall clock: create (host boxes uploaded), every step, state read back",
                   "h2d_bytes": int(big.nbytes), "d2h_bytes": 20000 * 22 * 4}
+    # the same pile with convex cells of the hull library in place of four boxes in five (the WebGPU world's hull
+    # shapes, their pairs through the convex-cell SAT)
+    from shatterforge_b200 import hulls
+    lib = hulls.library().packed()
+    ids = np.random.default_rng(3).integers(1, len(lib), 20000).astype(np.uint32)
+    ids[::5] = 0
+    w = X.BoxWorld(big, p)
+    w.set_hulls(lib, ids)
+    w.step(dt, args.box_warmup)
+    w.step(dt, args.box_steps)
+    st = w.stats()
+    out["cells"] = {"workload": "pile(20000), four boxes in five replaced by convex cells, 12 sub-steps, no sleep",
+                    "ms_per_step": st.ms / args.box_steps, "box_steps_per_s": 20000 / (st.ms / args.box_steps * 1e-3),
+                    "pairs": int(st.pairs), "manifolds": int(st.manifolds), "colours": int(st.colours)}
+    w.close()
     batch = [X.pile(2000)] * 148
     w = X.BoxWorld(batch, p)
     w.step(dt, args.box_warmup)

@@ -470,12 +470,19 @@ typedef struct sf_box_stats {        /* Stats (phys.rs:108-110) of the last step
 sf_status sf_box_world_create(const float *boxes, const uint32_t *scene_first, uint32_t n_scenes,
                               const sf_box_params *params, sf_box_world **out);
 void sf_box_world_destroy(sf_box_world *w);
+/* Convex cells in the box world (the WebGPU world's hull shapes, gpu/gpu_world.js:786-833): hull_data holds n_hulls
+ * cells of 80 float4 (the packed library, cell 0 the whole cube), hull_ids a cell per box (0 = a plain box). A pair
+ * with a cell goes through the convex-cell SAT (a plain box as the whole cube), a cell on the ground through its
+ * corners, the first four one patch and the rest a second (manifold b = 0xFFFFFFFE); each reduced to 4 points.
+ * The boxes keep their mass and inertia. Call before the first step. */
+sf_status sf_box_world_set_hulls(sf_box_world *w, const float *hull_data, uint32_t n_hulls, const uint32_t *hull_ids);
 /* nsteps steps of dt for every scene; synchronous. */
 sf_status sf_box_world_step(sf_box_world *w, float dt, uint32_t nsteps);
 /* 22 floats a box: centre 3, quaternion 4, velocity 3, spin 3, sleep timer, rest pose (centre 3, quaternion 4), awake */
 sf_status sf_box_world_read(sf_box_world *w, float *out22);
 sf_status sf_box_world_stats(sf_box_world *w, uint32_t scene, sf_box_stats *out);
-/* The last step's manifolds of a scene in key order (a, b; the ground as b = 0xFFFFFFFF after a's pairs), 16 words
+/* The last step's manifolds of a scene in key order (a, b; the ground as b = 0xFFFFFFFF after a's pairs and a
+ * cell's second ground patch), 16 words
  * each: a, b, point count, sticking, normal 3, normal impulses 4, friction impulses 2, twist impulse (f32 bits),
  * colour. *count gets the number of manifolds; at most cap are written. */
 sf_status sf_box_world_manifolds(sf_box_world *w, uint32_t scene, uint32_t *out16, uint32_t cap, uint32_t *count);

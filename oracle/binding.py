@@ -128,6 +128,7 @@ def load() -> C.CDLL:
     lib.obx_create.restype = C.c_void_p
     lib.obx_create.argtypes = [_f32p, C.c_uint32, C.c_void_p, C.c_int32]
     lib.obx_destroy.argtypes = [C.c_void_p]
+    lib.obx_set_hulls.argtypes = [C.c_void_p, _f32p, C.c_uint32, _u32p]
     lib.obx_step.argtypes = [C.c_void_p, C.c_float, C.c_uint32]
     lib.obx_read.argtypes = [C.c_void_p, _f32p]
     lib.obx_stats.argtypes = [C.c_void_p, _u32p]
@@ -442,6 +443,14 @@ class OracleBoxWorld:
         if getattr(self, "_h", None):
             self._lib.obx_destroy(self._h)
             self._h = None
+
+    def set_hulls(self, hull_data, hull_ids):
+        """The convex-cell library (hulls.library().packed()) and a cell per box (0 = a plain box)."""
+        d = np.ascontiguousarray(hull_data, np.float32).reshape(-1, 320)
+        ids = np.ascontiguousarray(hull_ids, np.uint32).reshape(-1)
+        assert len(ids) == self.n
+        self._hulls = d
+        self._lib.obx_set_hulls(self._h, _p(d, C.c_float), len(d), _p(ids, C.c_uint32))
 
     def step(self, dt, n=1):
         self._lib.obx_step(self._h, float(dt), int(n))

@@ -2367,7 +2367,9 @@ void ow_ref_colouring(uint32_t n, const uint32_t* a, const uint32_t* b, const ui
 namespace {
 
 enum { BOX_LIST = 0, BOX_COLOR = 1 };
-static const uint32_t BNONE = 0xFFFFFFFFu;
+static const uint32_t BNONE = 0xFFFFFFFFu;      // the ground
+static const uint32_t BGROUND2 = 0xFFFFFFFEu;   // a convex cell's second ground patch
+static inline bool bground(uint32_t b) { return b >= BGROUND2; }
 
 struct BoxParams {      // the layout of sf_box_params
     float gravity[3]; uint32_t substeps;
@@ -2422,6 +2424,7 @@ static inline uint32_t bhash(int32_t x, int32_t y, int32_t z) {
 struct BBody {
     P3 p; Q4 q; P3 v, w, h; float inv_m; P3 inv_i; bool awake; float sleep_t; P3 sleep_p; Q4 sleep_q;
     M3 rot; P3 amin, amax;
+    uint32_t hull;    // a convex cell of the library (0: a plain box)
 };
 struct BCp { P3 ra, rb, la, raxn, rbxn, iaxn, ibxn; float adj, nm, jn; };
 struct BMan {
@@ -2434,6 +2437,7 @@ static inline uint64_t bkey(uint32_t a, uint32_t b) { return ((uint64_t)a << 32)
 
 struct BoxWorld {
     std::vector<BBody> bodies;
+    std::vector<float> hulls;    // the convex-cell library, 320 floats a cell
     BoxParams prm{};
     int order = BOX_LIST;
     std::vector<BMan> man, old;
@@ -2713,8 +2717,31 @@ struct BoxWorld {
         b.awake = true; b.sleep_t = 0.0f; b.sleep_p = b.p; b.sleep_q = b.q;
     }
     // phys.rs:419-432: the corners below the margin, at half their height, depth = their height
+    HullShape hshape(const BBody& b) const { return HullShape{b.p, b.rot, b.h, hulls.data() + (size_t)b.hull * 320}; }
+    // a contact of the convex-cell SAT, reduced to 4 points (gpu/gpu_world.js:532-554, in emit), pushed as a manifold
+    void push_hc(uint32_t a, uint32_t b, HC c) {
+        hc_reduce4(c);
+        CP pts[8];
+        for (int k = 0; k < c.cnt; k++) { pts[k].p = p3(c.pt[k][0], c.pt[k][1], c.pt[k][2]); pts[k].s = c.pt[k][3]; }
+        push_manifold(a, b, c.n, pts, c.cnt);
+    }
+    // a convex cell on the ground (gpu/gpu_world.js:809-823): the corners under the margin; past four, the rest are a
+    // second patch, emitted first; `which` = 1 the second patch only, 2 the first only, 3 both
+    void collide_ground_cell(uint32_t i, int which) {
+        const BBody& b = bodies[i];
+        const float margin = prm.speculative + maxf(-b.v.y, 0.0f) * (1.0f / 60.0f);
+        HC c = hull_ground(hshape(b), margin);
+        if (c.cnt > 4) {
+            HC c2; c2.n = c.n; c2.cnt = c.cnt - 4;
+            for (int q = 0; q < c2.cnt; q++) for (int t = 0; t < 4; t++) c2.pt[q][t] = c.pt[4 + q][t];
+            c.cnt = 4;
+            if (which & 1) push_hc(i, BGROUND2, c2);
+        }
+        if (c.cnt > 0 && (which & 2)) push_hc(i, BNONE, c);
+    }
     void collide_ground(uint32_t i) {
         const BBody& b = bodies[i];
+        if (b.hull) { collide_ground_cell(i, 3); return; }
         CP pts[8]; int cnt = 0;
         const float margin = prm.speculative + maxf(-b.v.y, 0.0f) * (1.0f / 60.0f);
         for (int k = 0; k < 8; k++) {
@@ -2734,6 +2761,14 @@ struct BoxWorld {
         const bool a_awake = a.awake, b_awake = b.awake, a_still = a.sleep_t != 0.0f, b_still = b.sleep_t != 0.0f;
         const float rel = plen_e(b.v - a.v) + plen_e(a.w) * plen_e(a.h) + plen_e(b.w) * plen_e(b.h);
         const float margin = prm.speculative + rel * (1.0f / 60.0f);
+        if (a.hull || b.hull) {       // a pair with a convex cell (gpu/gpu_world.js:824-832); a box is the whole cube
+            HC c = hull_hull(hshape(a), hshape(b), margin);
+            if (c.cnt == 0) return;
+            if (a_awake && !b_awake && !a_still) { if (defer) (*defer)[ib] = 1; else wake(ib); }
+            if (b_awake && !a_awake && !b_still) { if (defer) (*defer)[ia] = 1; else wake(ia); }
+            push_hc(ia, ib, c);
+            return;
+        }
         CP pts[8]; P3 n;
         int cnt = collide_boxes(a.p, a.rot, a.h, b.p, b.rot, b.h, margin, pts, &n);
         if (cnt == 0) return;
@@ -2746,8 +2781,8 @@ struct BoxWorld {
     void push_manifold(uint32_t a, uint32_t b, P3 n, const CP* pts, int cnt) {
         const BBody& ba = bodies[a];
         const P3 pa = ba.p; const M3 ra = ba.rot;
-        const P3 pb = b != BNONE ? bodies[b].p : p3(0, 0, 0);
-        const uint32_t sa = sidx[a], sbi = b != BNONE ? sidx[b] : 0;
+        const P3 pb = !bground(b) ? bodies[b].p : p3(0, 0, 0);
+        const uint32_t sa = sidx[a], sbi = !bground(b) ? sidx[b] : 0;
         if (sa == 0 && sbi == 0) return;
         BMan m{};
         m.a = a; m.b = b; m.sa = sa; m.sb = sbi; m.n = n; btangents(n, m.t1, m.t2); m.mu = prm.friction;
@@ -2755,7 +2790,7 @@ struct BoxWorld {
         auto it = old_map.find(bkey(a, b));
         const BMan* o = it == old_map.end() ? nullptr : &old[it->second];
         M3 rbm; rbm.c[0] = p3(1, 0, 0); rbm.c[1] = p3(0, 1, 0); rbm.c[2] = p3(0, 0, 1);
-        if (b != BNONE) rbm = bodies[b].rot;
+        if (!bground(b)) rbm = bodies[b].rot;
         P3 cen = p3(0, 0, 0);
         for (int k = 0; k < cnt; k++) cen = cen + pts[k].p;
         cen = cen * (1.0f / (float)cnt);
@@ -2766,7 +2801,7 @@ struct BoxWorld {
         if (o) {
             if (o->stick) {
                 P3 wa = pa + m_mulv(ra, o->la_f);
-                P3 wb = b != BNONE ? pb + m_mulv(rbm, o->lb_f) : o->lb_f;
+                P3 wb = !bground(b) ? pb + m_mulv(rbm, o->lb_f) : o->lb_f;
                 float lim = maxf(0.05f, m.rad);
                 if (plen2(wa - cen) < lim * lim && plen2(wb - wa) < 0.03f * 0.03f) {
                     m.la_f = o->la_f; m.lb_f = o->lb_f; m.fa = wa - pa; m.fb = wb - pb; m.e0 = wb - wa; anchored = true;
@@ -2777,13 +2812,13 @@ struct BoxWorld {
         }
         if (!anchored) {
             m.fa = cen - pa; m.fb = cen - pb; m.la_f = m_tmulv(ra, m.fa);
-            m.lb_f = b != BNONE ? m_tmulv(rbm, m.fb) : cen;
+            m.lb_f = !bground(b) ? m_tmulv(rbm, m.fb) : cen;
             m.e0 = p3(0, 0, 0);
         }
         for (int k = 0; k < cnt; k++) {
             BCp& c = m.cp[k];
             c.ra = pts[k].p - pa;
-            c.rb = b != BNONE ? pts[k].p - pb : pts[k].p;
+            c.rb = !bground(b) ? pts[k].p - pb : pts[k].p;
             c.adj = pts[k].s;
             c.la = m_tmulv(ra, c.ra);
             if (o) {
@@ -2826,7 +2861,7 @@ struct BoxWorld {
         std::vector<uint64_t> rank(M);
         for (uint32_t k = 0; k < M; k++) {
             const BMan& m = man[k];
-            rank[k] = ((uint64_t)pair_priority(m.a, m.b == BNONE ? 0u : m.b + 1) << 32) | (uint64_t)(0xFFFFFFFFu - k);
+            rank[k] = ((uint64_t)pair_priority(m.a, bground(m.b) ? 0u : m.b + 1) << 32) | (uint64_t)(0xFFFFFFFFu - k);
         }
         std::vector<uint32_t> by(M);
         for (uint32_t k = 0; k < M; k++) by[k] = k;
@@ -2866,6 +2901,12 @@ void* obx_create(const float* boxes, uint32_t n, const void* params, int32_t ord
     return w;
 }
 void obx_destroy(void* w) { delete (BoxWorld*)w; }
+// the convex-cell library (n cells of 320 floats) and a cell per box (0 = a plain box)
+void obx_set_hulls(void* wp, const float* data, uint32_t n, const uint32_t* ids) {
+    BoxWorld* w = (BoxWorld*)wp;
+    w->hulls.assign(data, data + (size_t)n * 320);
+    for (size_t i = 0; i < w->bodies.size(); i++) w->bodies[i].hull = ids[i];
+}
 void obx_step(void* w, float dt, uint32_t nsteps) { for (uint32_t k = 0; k < nsteps; k++) ((BoxWorld*)w)->step(dt); }
 // 22 floats a body: p3 q4 v3 w3 sleep_t sleep_p3 sleep_q4 awake
 void obx_read(void* wp, float* out) {

@@ -207,6 +207,7 @@ PROTOTYPES = {
     "sf_box_world_create": (C.c_int32, [_f32p, _u32p, C.c_uint32, C.c_void_p, C.POINTER(_vp)]),
     "sf_box_world_destroy": (None, [_vp]),
     "sf_box_world_step": (C.c_int32, [_vp, C.c_float, C.c_uint32]),
+    "sf_box_world_set_hulls": (C.c_int32, [_vp, _f32p, C.c_uint32, _u32p]),
     "sf_box_world_read": (C.c_int32, [_vp, _f32p]),
     "sf_box_world_stats": (C.c_int32, [_vp, C.c_uint32, C.c_void_p]),
     "sf_box_world_manifolds": (C.c_int32, [_vp, C.c_uint32, _u32p, C.c_uint32, _u32p]),

@@ -154,6 +154,15 @@ class BoxWorld:
                                              C.byref(self.params), C.byref(h)), "sf_box_world_create")
         self._h = h
 
+    def set_hulls(self, hull_data: np.ndarray, hull_ids: np.ndarray):
+        """Convex cells (sf_box_world_set_hulls): hull_data the packed library (hulls.library().packed()), hull_ids a
+        cell per box over all scenes (0 = a plain box)."""
+        data = np.ascontiguousarray(hull_data, np.float32).reshape(-1, 320)
+        ids = np.ascontiguousarray(hull_ids, np.uint32).reshape(-1)
+        assert len(ids) == self.n
+        self._check(self._lib.sf_box_world_set_hulls(self._h, self._ptr(data, C.c_float), len(data),
+                                                     self._ptr(ids, C.c_uint32)), "sf_box_world_set_hulls")
+
     def close(self):
         if getattr(self, "_h", None):
             self._lib.sf_box_world_destroy(self._h)

@@ -26,7 +26,9 @@
 namespace sf {
 namespace {
 
-constexpr uint32_t BX_NONE = 0xFFFFFFFFu;
+constexpr uint32_t BX_NONE = 0xFFFFFFFFu;     // the ground
+constexpr uint32_t BX_GROUND2 = 0xFFFFFFFEu;  // the second ground patch of a convex cell (corners 5-8)
+__host__ __device__ __forceinline__ bool is_ground(uint32_t b) { return b >= BX_GROUND2; }
 constexpr uint32_t BX_UNC = 0xFFFFFFFFu;
 constexpr uint32_t BX_PPB = 48;      // pairs (with a higher-numbered body) a body may take, on average over its scene
 constexpr uint32_t BX_SHORT = 32;    // pair lists up to this long are sorted by their own thread
@@ -38,7 +40,7 @@ constexpr int BX_CL = 16, BX_CL_THREADS = 512;
 enum { BXE_ENTRIES = 1, BXE_PAIRS = 2, BXE_MANIFOLDS = 4, BXE_COLOURS = 8, BXE_GUARD = 16 };
 
 struct DM3 { P3 c[3]; };
-struct BxBody { P3 p; float q[4]; P3 v, w, h; float inv_m; P3 inv_i; float sleep_t; P3 sleep_p; float sleep_q[4]; uint32_t awake; };
+struct BxBody { P3 p; float q[4]; P3 v, w, h; float inv_m; P3 inv_i; float sleep_t; P3 sleep_p; float sleep_q[4]; uint32_t awake, hull; };
 struct DCp { P3 ra, rb, la, raxn, rbxn, iaxn, ibxn; float adj, nm, jn; };
 struct DMan {
     uint32_t a, b, sa, sb; P3 n, t1, t2; float mu; uint32_t cnt, stick;
@@ -49,6 +51,7 @@ struct DMan {
 
 struct BxArgs {
     BxBody *body;
+    const float4 *hulls;     // the convex-cell library, 80 float4 a cell; a body's hull 0 is the whole box
     DM3 *rot; P3 *amin, *amax;
     uint32_t *ecnt, *sidx, *cand_n, *seglong, *uf, *mint;
     uint8_t *wake;
@@ -118,7 +121,7 @@ __device__ __forceinline__ uint32_t pair_priority(uint32_t a, uint32_t bp) {
     return h;
 }
 __device__ __forceinline__ uint64_t man_rank(uint32_t a, uint32_t b, uint32_t m) {
-    return ((uint64_t)pair_priority(a, b == BX_NONE ? 0u : b + 1) << 32) | (uint64_t)(0xFFFFFFFFu - m);
+    return ((uint64_t)pair_priority(a, is_ground(b) ? 0u : b + 1) << 32) | (uint64_t)(0xFFFFFFFFu - m);
 }
 
 __device__ __forceinline__ unsigned long long gtime() {
@@ -133,6 +136,25 @@ __device__ __forceinline__ Box make_box(const BxBody &b, const DM3 &r) {
     return x;
 }
 
+__device__ __forceinline__ HShape hshape(const BxBody &b, const DM3 &r, const float4 *hulls) {
+    HShape s;
+    s.p = b.p; s.c[0] = r.c[0]; s.c[1] = r.c[1]; s.c[2] = r.c[2]; s.h = b.h; s.H = hulls + (size_t)b.hull * 80;
+    return s;
+}
+// a convex-cell contact reduced to 4 points (gpu/gpu_world.js:532-554, in emit) into the candidate's geometry words
+__device__ int hull_out(HContact &c, float *g) {
+    if (c.cnt) hc_reduce4(c);
+    g[0] = c.n.x; g[1] = c.n.y; g[2] = c.n.z; g[3] = __int_as_float(c.cnt);
+    for (int k = 0; k < 4; k++) {
+        const bool ok = k < c.cnt;
+        g[4 + 4 * k] = ok ? c.pt[k].x : 0.0f; g[5 + 4 * k] = ok ? c.pt[k].y : 0.0f;
+        g[6 + 4 * k] = ok ? c.pt[k].z : 0.0f; g[7 + 4 * k] = ok ? c.pt[k].w : 0.0f;
+    }
+    return c.cnt;
+}
+// the ground candidates of a body: its ground contact, and a convex cell's second patch before it
+__device__ __forceinline__ uint32_t ground_slots(const BxBody &b, P3 lo) { return b.awake && lo.y < 0.0f ? (b.hull ? 2u : 1u) : 0u; }
+
 // collide_ground (phys.rs:419-432) or collide_pair (phys.rs:434-445) of candidate (a, b); the geometry goes to
 // g[20] = normal 3, count, 4 x (point 3, depth). A wake is recorded (applied after every candidate has read the
 // flags): the woken set is the same as waking at once, since a wake only turns a sleeping body awake.
@@ -141,7 +163,34 @@ __device__ int collide_candidate(const BxArgs &A, uint32_t b0, uint32_t a, uint3
     const DM3 ra = A.rot[b0 + a];
     CPt pts[8]; P3 n = p3(0.0f, 0.0f, 0.0f);
     int cnt = 0;
-    if (b == BX_NONE) {
+    if (is_ground(b) && ba.hull) {
+        // a convex cell on the ground (gpu/gpu_world.js:809-823): its corners under the margin, the first four as
+        // one patch, the rest as a second
+        const float margin = A.P.speculative + maxf(-ba.v.y, 0.0f) * (1.0f / 60.0f);
+        HContact c;
+        hull_ground(hshape(ba, ra, A.hulls), margin, c);
+        const int lo = b == BX_GROUND2 ? 4 : 0, hi = b == BX_GROUND2 ? c.cnt : min(c.cnt, 4);
+        HContact d;
+        d.n = c.n; d.cnt = 0;
+        for (int k = lo; k < hi; k++) d.pt[d.cnt++] = c.pt[k];
+        return hull_out(d, g);
+    }
+    if (!is_ground(b) && (ba.hull || A.body[b0 + b].hull)) {
+        // a pair with a convex cell (gpu/gpu_world.js:824-832); a plain box is the library's whole cube
+        const BxBody bb = A.body[b0 + b];
+        const DM3 rb = A.rot[b0 + b];
+        const bool a_awake = ba.awake != 0, b_awake = bb.awake != 0, a_still = ba.sleep_t != 0.0f, b_still = bb.sleep_t != 0.0f;
+        const float rel = plen_e(bb.v - ba.v) + plen_e(ba.w) * plen_e(ba.h) + plen_e(bb.w) * plen_e(bb.h);
+        const float margin = A.P.speculative + rel * (1.0f / 60.0f);
+        HContact c;
+        hull_hull(hshape(ba, ra, A.hulls), hshape(bb, rb, A.hulls), margin, c);
+        if (c.cnt) {
+            if (a_awake && !b_awake && !a_still) A.wake[b0 + b] = 1;
+            if (b_awake && !a_awake && !b_still) A.wake[b0 + a] = 1;
+        }
+        return hull_out(c, g);
+    }
+    if (is_ground(b)) {
         const float margin = A.P.speculative + maxf(-ba.v.y, 0.0f) * (1.0f / 60.0f);
         for (int k = 0; k < 8; k++) {
             P3 s = p3(k & 1 ? 1.0f : -1.0f, k & 2 ? 1.0f : -1.0f, k & 4 ? 1.0f : -1.0f);
@@ -177,8 +226,8 @@ __device__ void build_manifold(const BxArgs &A, int par, uint32_t b0, uint32_t s
     const BxBody &ba = A.body[b0 + a];
     const P3 pa = ba.p;
     const DM3 ra = A.rot[b0 + a];
-    const P3 pb = b != BX_NONE ? A.body[b0 + b].p : p3(0.0f, 0.0f, 0.0f);
-    const uint32_t sa = A.sidx[b0 + a], sbi = b != BX_NONE ? A.sidx[b0 + b] : 0u;
+    const P3 pb = !is_ground(b) ? A.body[b0 + b].p : p3(0.0f, 0.0f, 0.0f);
+    const uint32_t sa = A.sidx[b0 + a], sbi = !is_ground(b) ? A.sidx[b0 + b] : 0u;
     const P3 n = p3(g[0], g[1], g[2]);
     const int cnt = __float_as_int(g[3]);
     m.a = a; m.b = b; m.sa = sa; m.sb = sbi; m.n = n; btangents(n, m.t1, m.t2); m.mu = A.P.friction;
@@ -192,7 +241,7 @@ __device__ void build_manifold(const BxArgs &A, int par, uint32_t b0, uint32_t s
     const DMan *o = (lo < nold && ok[lo] == key) ? A.man[par ^ 1] + m0 + lo : nullptr;
     DM3 rbm;
     rbm.c[0] = p3(1.0f, 0.0f, 0.0f); rbm.c[1] = p3(0.0f, 1.0f, 0.0f); rbm.c[2] = p3(0.0f, 0.0f, 1.0f);
-    if (b != BX_NONE) rbm = A.rot[b0 + b];
+    if (!is_ground(b)) rbm = A.rot[b0 + b];
     P3 pt[4]; float dep[4];
     for (int k = 0; k < 4; k++) { pt[k] = p3(g[4 + 4 * k], g[5 + 4 * k], g[6 + 4 * k]); dep[k] = g[7 + 4 * k]; }
     P3 cen = p3(0.0f, 0.0f, 0.0f);
@@ -205,7 +254,7 @@ __device__ void build_manifold(const BxArgs &A, int par, uint32_t b0, uint32_t s
     if (o) {
         if (o->stick) {
             P3 wa = pa + m_mulv(ra, o->la_f);
-            P3 wb = b != BX_NONE ? pb + m_mulv(rbm, o->lb_f) : o->lb_f;
+            P3 wb = !is_ground(b) ? pb + m_mulv(rbm, o->lb_f) : o->lb_f;
             float lim = maxf(0.05f, m.rad);
             if (plen2(wa - cen) < lim * lim && plen2(wb - wa) < 0.03f * 0.03f) {
                 m.la_f = o->la_f; m.lb_f = o->lb_f; m.fa = wa - pa; m.fb = wb - pb; m.e0 = wb - wa; anchored = true;
@@ -216,7 +265,7 @@ __device__ void build_manifold(const BxArgs &A, int par, uint32_t b0, uint32_t s
     }
     if (!anchored) {
         m.fa = cen - pa; m.fb = cen - pb; m.la_f = m_tmulv(ra, m.fa);
-        m.lb_f = b != BX_NONE ? m_tmulv(rbm, m.fb) : cen;
+        m.lb_f = !is_ground(b) ? m_tmulv(rbm, m.fb) : cen;
         m.e0 = p3(0.0f, 0.0f, 0.0f);
     }
     const float ima = A.sim[s0 + sa], imb = A.sim[s0 + sbi];
@@ -226,7 +275,7 @@ __device__ void build_manifold(const BxArgs &A, int par, uint32_t b0, uint32_t s
         DCp c;
         if (k < cnt) {
             c.ra = pt[k] - pa;
-            c.rb = b != BX_NONE ? pt[k] - pb : pt[k];
+            c.rb = !is_ground(b) ? pt[k] - pb : pt[k];
             c.adj = dep[k];
             c.la = m_tmulv(ra, c.ra);
             c.jn = 0.0f;
@@ -516,7 +565,7 @@ __global__ void __launch_bounds__(T, CL == 1 && T <= 256 ? 2 : 1) k_box_step(BxA
     for (uint32_t a = t; a < n; a += TT) {
         const uint32_t k = walk_pairs(A, b0, e0, t0, mask, ne_tot, inv_cell, a, nullptr, nullptr);
         atomicAdd(&Gp[G_TOT + 3], k);
-        A.cand_n[b0 + a] = k + (A.body[b0 + a].awake && A.amin[b0 + a].y < 0.0f ? 1u : 0u);
+        A.cand_n[b0 + a] = k + ground_slots(A.body[b0 + a], A.amin[b0 + a]);
     }
     team_sync<CL>();
     const uint32_t nc = team_scan<T, CL>(A.cand_n + b0, n, wsum, Gp + G_CTA, t, rank);
@@ -540,7 +589,8 @@ __global__ void __launch_bounds__(T, CL == 1 && T <= 256 ? 2 : 1) k_box_step(BxA
         } else {
             A.seglong[b0 + atomicAdd(&Gp[G_TOT + 5], 1u)] = a;
         }
-        if (A.body[b0 + a].awake && A.amin[b0 + a].y < 0.0f) { A.cand_a[c0 + off + k] = a; A.cand_b[c0 + off + k] = BX_NONE; }
+        const uint32_t ng = ground_slots(A.body[b0 + a], A.amin[b0 + a]);
+        for (uint32_t q = 0; q < ng; q++) { A.cand_a[c0 + off + k + q] = a; A.cand_b[c0 + off + k + q] = ng == 2 && q == 0 ? BX_GROUND2 : BX_NONE; }
     }
     team_sync<CL>();
     // long lists: the pair partners are distinct bodies, so a bitmap over the scene's bodies and a scan of its
@@ -549,7 +599,7 @@ __global__ void __launch_bounds__(T, CL == 1 && T <= 256 ? 2 : 1) k_box_step(BxA
     for (uint32_t q = 0; q < nlong; q++) {
         const uint32_t a = A.seglong[b0 + q];
         const uint32_t off = A.cand_n[b0 + a], next = a + 1 < n ? A.cand_n[b0 + a + 1] : nc;
-        const uint32_t k = next - off - (A.body[b0 + a].awake && A.amin[b0 + a].y < 0.0f ? 1u : 0u);
+        const uint32_t k = next - off - ground_slots(A.body[b0 + a], A.amin[b0 + a]);
         uint32_t *bits = A.mint + b0, *pos = A.ecnt + b0, *cb = A.cand_b + c0 + off;
         for (uint32_t x = t; x < nwords; x += TT) bits[x] = 0;
         team_sync<CL>();
@@ -796,6 +846,11 @@ __global__ void __launch_bounds__(T, CL == 1 && T <= 256 ? 2 : 1) k_box_step(BxA
     }
 }
 
+__global__ void k_box_hull_ids(BxBody *body, const uint32_t *ids, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) body[i].hull = ids[i];
+}
+
 }  // namespace
 }  // namespace sf
 
@@ -806,6 +861,8 @@ struct sf_box_world {
     uint32_t n_scenes = 0, n_bodies = 0, max_n = 0;
     std::vector<uint32_t> b0, nn, c0, m0;
     DBuf<BxBody> body;
+    DBuf<float4> hulls;
+    uint32_t n_hulls = 0;
     DBuf<DM3> rot, sii;
     DBuf<P3> amin, amax, sv, sw, sdp, sth, sp0;
     DBuf<float> sim, geom;
@@ -952,7 +1009,7 @@ extern "C" sf_status sf_box_world_step(sf_box_world *w, float dt, uint32_t nstep
     if (!w) { set_error("null world"); return SF_ERR_ARG; }
     if (!(dt > 0.0f)) { set_error("dt must be positive"); return SF_ERR_ARG; }
     BxArgs a;
-    a.body = w->body.p; a.rot = w->rot.p; a.amin = w->amin.p; a.amax = w->amax.p;
+    a.body = w->body.p; a.hulls = w->hulls.p; a.rot = w->rot.p; a.amin = w->amin.p; a.amax = w->amax.p;
     a.ecnt = w->ecnt.p; a.sidx = w->sidx.p; a.cand_n = w->cand_n.p; a.seglong = w->seglong.p; a.uf = w->uf.p; a.mint = w->mint.p;
     a.wake = w->wake.p; a.ent_body = w->ent_body.p; a.ent_next = w->ent_next.p; a.head = w->head.p; a.ent_cell = w->ent_cell.p;
     a.cand_a = w->cand_a.p; a.cand_b = w->cand_b.p; a.hit = w->hit.p; a.geom = w->geom.p;
@@ -1049,5 +1106,23 @@ extern "C" sf_status sf_box_world_manifolds(sf_box_world *w, uint32_t scene, uin
         std::memcpy(o + 4, f, sizeof(f));
         o[14] = col[i]; o[15] = 0;
     }
+    return SF_OK;
+}
+
+// hull_data: n_hulls cells of 80 float4 (shatterforge_b200/hulls.py packed(); cell 0 the whole cube); hull_ids: a cell
+// per box (0 = a plain box). Boxes keep their own mass and inertia (the record's density over the whole box).
+extern "C" sf_status sf_box_world_set_hulls(sf_box_world *w, const float *hull_data, uint32_t n_hulls, const uint32_t *hull_ids) {
+    if (!w || !hull_data || !hull_ids || n_hulls == 0) { set_error("null argument"); return SF_ERR_ARG; }
+    for (uint32_t i = 0; i < w->n_bodies; i++)
+        if (hull_ids[i] >= n_hulls) { set_error("box %u: hull %u of %u", i, hull_ids[i], n_hulls); return SF_ERR_ARG; }
+    if (w->hulls.alloc((size_t)n_hulls * 80) != cudaSuccess) { set_error("device allocation failed"); return SF_ERR_CUDA; }
+    w->n_hulls = n_hulls;
+    DBuf<uint32_t> ids;
+    if (ids.alloc(w->n_bodies) != cudaSuccess) { set_error("device allocation failed"); return SF_ERR_CUDA; }
+    SF_CUDA(cudaMemcpyAsync(w->hulls.p, hull_data, (size_t)n_hulls * 80 * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
+    SF_CUDA(cudaMemcpyAsync(ids.p, hull_ids, (size_t)w->n_bodies * 4, cudaMemcpyHostToDevice, w->stream));
+    if (w->n_bodies) k_box_hull_ids<<<grid_for(w->n_bodies, 256), 256, 0, w->stream>>>(w->body.p, ids.p, w->n_bodies);
+    SF_CUDA(cudaGetLastError());
+    SF_CUDA(cudaStreamSynchronize(w->stream));
     return SF_OK;
 }

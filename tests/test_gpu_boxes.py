@@ -102,3 +102,39 @@ def test_pile_20000_full_size_against_oracle(sf, oracle):
         assert stats_tuple(w.stats()) == ow.stats(), k
     compare(w, ow)
     assert w.stats().pairs > 50000
+
+
+def test_rubble_of_convex_cells_against_oracle(sf, oracle):
+    """Convex cells of the hull library in the box world (every fifth a plain box): pairs through the convex-cell SAT,
+    cells on the ground in one or two patches; 240 steps with sleep on, the counts every step, the state and the
+    manifolds every 20."""
+    from test_oracle_boxes import rubble
+    recs, lib, ids = rubble(500)
+    p = X.box_params()
+    w = X.BoxWorld(recs, p)
+    w.set_hulls(lib, ids)
+    ow = oracle.OracleBoxWorld(recs, p, oracle.ORDER_COLOR)
+    ow.set_hulls(lib, ids)
+    for k in range(1, 241):
+        w.step(DT)
+        ow.step(DT)
+        assert stats_tuple(w.stats()) == ow.stats(), k
+        if k % 20 == 0:
+            compare(w, ow)
+    assert (w.manifolds()[:, 1] == 0xFFFFFFFE).any()
+
+
+def test_rubble_6000_on_a_cluster_against_oracle(sf, oracle):
+    """6,000 boxes and cells (a cluster scene) for 30 steps at 12 sub-steps without sleep, bit-exact."""
+    from test_oracle_boxes import rubble
+    recs, lib, ids = rubble(6000, seed=5)
+    p = X.box_params(allow_sleep=0)
+    w = X.BoxWorld(recs, p)
+    w.set_hulls(lib, ids)
+    ow = oracle.OracleBoxWorld(recs, p, oracle.ORDER_COLOR)
+    ow.set_hulls(lib, ids)
+    for k in range(30):
+        w.step(DT)
+        ow.step(DT)
+        assert stats_tuple(w.stats()) == ow.stats(), k
+    compare(w, ow)

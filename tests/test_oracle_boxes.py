@@ -113,3 +113,52 @@ def test_colouring_is_proper_and_orders_agree(oracle):
     np.testing.assert_array_equal(ma[order][:, cols], mb[:, cols])
     assert a.stats()[:4] == b.stats()[:4]
     assert awake.any()
+
+
+def quat_rot(q):
+    x, y, z, w = [float(v) for v in q]
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+
+
+def rubble(n, seed=3, box_every=5):
+    """The reference's pile with most boxes replaced by convex cells of the hull library (every fifth a plain box)."""
+    from shatterforge_b200 import hulls
+    lib = hulls.library().packed()
+    ids = np.random.default_rng(seed).integers(1, len(lib), n).astype(np.uint32)
+    ids[::box_every] = 0
+    return X.pile(n), lib, ids
+
+
+@pytest.mark.parametrize("order", [0, 1])
+def test_convex_cell_comes_to_rest_on_its_corners(oracle, order):
+    """A convex cell dropped tilted from 1 m (the WebGPU world's hull shapes, gpu/gpu_world.js:786-833): after 5 s it
+    is at rest with its lowest corner on the ground (within 1 cm), and a cell resting on a face of more than four
+    corners has its corners in two ground patches."""
+    from shatterforge_b200 import hulls
+    lib = hulls.library().packed()
+    for cell in (1, 7, 30):
+        rec = X.tilted_box()
+        ow = oracle.OracleBoxWorld(rec, X.box_params(), order)
+        ow.set_hulls(lib, np.array([cell], np.uint32))
+        ow.step(DT, 300)
+        s = ow.state()[0]
+        assert np.linalg.norm(s[7:10]) < 0.05, (cell, s[7:10])
+        nv = int(lib[cell, 0, 0])
+        verts = lib[cell, 1:1 + nv, :3] * rec[0, 7:10]
+        wy = (verts @ quat_rot(s[3:7]).T)[:, 1] + s[1]
+        assert abs(wy.min()) < 0.01, (cell, wy.min())
+
+
+@pytest.mark.parametrize("order", [0, 1])
+def test_rubble_pile_settles(oracle, order):
+    recs, lib, ids = rubble(500)
+    ow = oracle.OracleBoxWorld(recs, X.box_params(), order)
+    ow.set_hulls(lib, ids)
+    ow.step(DT, 240)
+    s = ow.state()
+    assert np.isfinite(s).all()
+    assert s[:, 1].max() < 2.0 and np.linalg.norm(s[:, 7:10], axis=1).max() < 0.5
+    m = ow.manifolds()
+    assert (m[:, 1] == 0xFFFFFFFE).any()          # second ground patches of cells lying on a face
