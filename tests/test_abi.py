@@ -97,3 +97,24 @@ def test_grounded_mask_drops_floating_pieces():
     mat = np.full(4, S.CONC, np.uint8)
     keep = S.grounded_mask(xyz, mat, np.zeros(4, np.int32), np.zeros(4, np.uint8))
     assert keep.tolist() == [True, True, False, False]
+
+
+def test_box_world_rejects_bad_arguments(sf):
+    """sf_box_world_create checks its arguments before it touches a device: null pointers, scene bounds that go
+    down or do not start at 0, and a non-positive cell give SF_ERR_ARG."""
+    import ctypes as C
+    from shatterforge_b200 import boxes as X
+    lib = sf.load()
+    h = C.c_void_p()
+    p = X.box_params()
+    recs = X.stack(4)
+    rp = recs.ctypes.data_as(C.POINTER(C.c_float))
+    assert lib.sf_box_world_create(None, None, 1, C.byref(p), C.byref(h)) == sf.SF_ERR_ARG
+    for first in ([0, 4, 2], [1, 4]):
+        f = np.array(first, np.uint32)
+        assert lib.sf_box_world_create(rp, f.ctypes.data_as(C.POINTER(C.c_uint32)), len(first) - 1, C.byref(p),
+                                       C.byref(h)) == sf.SF_ERR_ARG
+    bad = X.box_params(cell=0.0)
+    f = np.array([0, 4], np.uint32)
+    assert lib.sf_box_world_create(rp, f.ctypes.data_as(C.POINTER(C.c_uint32)), 1, C.byref(bad), C.byref(h)) == sf.SF_ERR_ARG
+    assert lib.sf_box_world_step(None, 1.0 / 60.0, 1) == sf.SF_ERR_ARG

@@ -138,3 +138,23 @@ def test_rubble_6000_on_a_cluster_against_oracle(sf, oracle):
         ow.step(DT)
         assert stats_tuple(w.stats()) == ow.stats(), k
     compare(w, ow)
+
+
+def test_capacity_refusal_leaves_the_other_scenes_stepping(sf, oracle):
+    """A scene whose box covers millions of grid cells (half extents of 100 m) is past the grid's capacity: each step
+    returns SF_ERR_CAPACITY with that scene's status flag set and the scene left as it was, while the other scene steps
+    exactly as its oracle."""
+    giant = np.array([[0.0, 101.0, 0.0, 0, 0, 0, 1, 100.0, 100.0, 100.0, 1.0]], np.float32)
+    stk = X.stack(20)
+    p = X.box_params()
+    w = X.BoxWorld([stk, giant], p)
+    ow = oracle.OracleBoxWorld(stk, p, oracle.ORDER_COLOR)
+    before = w.state(1).copy()
+    for _ in range(30):
+        with pytest.raises(sf.SfError) as e:
+            w.step(DT)
+        assert e.value.status == sf.SF_ERR_CAPACITY
+        ow.step(DT)
+    assert w.stats(1).status == 1
+    np.testing.assert_array_equal(w.state(1), before)
+    compare(w, ow, scene=0)
