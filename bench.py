@@ -664,6 +664,14 @@ def boxes_section(args):
                 "reference_cpu_ms_per_step": 226.0,
                 "reference_note": "docs/PHASE0.md:12, native, 1 thread, 2.8 GHz Xeon VM (not rerunnable here)"})
     w.close()
+    # the reference's other published figure: the same pile at 4 sub-steps, 118 ms natively (docs/PHASE0.md:12)
+    w = X.BoxWorld(big, X.box_params(allow_sleep=0, substeps=4))
+    w.step(dt, args.box_warmup)
+    w.step(dt, args.box_steps)
+    st4 = w.stats()
+    out["substeps4"] = {"ms_per_step": st4.ms / args.box_steps, "box_steps_per_s": 20000 / (st4.ms / args.box_steps * 1e-3),
+                        "reference_cpu_ms_per_step": 118.0}
+    w.close()
     t0 = time.perf_counter()
     w = X.BoxWorld(big, p)
     w.step(dt, args.box_warmup + args.box_steps)
