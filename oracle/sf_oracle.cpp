@@ -23,6 +23,7 @@
 //   step (rigid part) ................... src/lib.rs:3640-3651
 //   union-find islands + island sleep ... engine/src/phys.rs:326-354, gpu/gpu_world.js:1634-1668
 //   box SAT collide_boxes / reduce4 ..... engine/src/phys.rs:507-628
+//   box world World::step ............. engine/src/phys.rs:152-354 (+ the WebGPU world's hull shapes, gpu/gpu_world.js:786-833)
 //
 // Floating point: every f32 expression keeps the reference's evaluation order, and the file is compiled with
 // -ffp-contract=off (wasm32 f32 has no fused multiply-add), so the restatement is op-for-op IEEE-equivalent.
@@ -31,6 +32,9 @@
 // hold no numeric golden vectors for this path. Numeric parity of this oracle is therefore UNPINNED; it is pinned
 // only by behavioural known answers (intact frames hold under self-weight, src/lib.rs stab test; sor fixed point
 // against an FP64 solve; hull library volumes) that tests/test_oracle.py checks.
+// The box world's list order is pinned by the reference's own published figures (the 20-box stack's 6.93 mm and
+// 1.7 mm/s, the 2,000-box pile's 0.117-4.828 m range), which it reproduces to their printed digits
+// (tests/test_oracle_boxes.py).
 //
 // Extensions beyond the reference, each behind a switch so the reference behaviour stays the default:
 //   * capacities are dynamic (the reference drops contacts past MAXC = 30000; the count it would drop is reported);
