@@ -80,14 +80,34 @@ __global__ void k_scan_reduce(const uint32_t *in, size_t n, uint32_t *sums) {
 // each thread owns SCAN_ITEMS consecutive values of the tile
 __global__ void k_scan_tile(const uint32_t *in, uint32_t *out, size_t n, const uint32_t *offsets, uint32_t *d_total) {
     size_t base = (size_t)blockIdx.x * SCAN_TILE + (size_t)threadIdx.x * SCAN_ITEMS;
+    // a full run of 8 values at 16-byte aligned arrays moves as two 16-byte words each way (the run starts at a
+    // multiple of 32 bytes from the array's start); in and out may be the same array (each thread reads its run
+    // before it writes it)
+    static_assert(SCAN_ITEMS == 8, "the vector path moves 8 values as two uint4");
+    const bool vec = base + SCAN_ITEMS <= n && ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u) == 0;
     uint32_t v[SCAN_ITEMS];
     uint32_t s = 0;
+    if (vec) {
+        const uint4 a = reinterpret_cast<const uint4 *>(in + base)[0], b = reinterpret_cast<const uint4 *>(in + base)[1];
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
 #pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; k++) { size_t i = base + k; v[k] = i < n ? in[i] : 0u; s += v[k]; }
+        for (int k = 0; k < SCAN_ITEMS; k++) s += v[k];
+    } else {
+#pragma unroll
+        for (int k = 0; k < SCAN_ITEMS; k++) { size_t i = base + k; v[k] = i < n ? in[i] : 0u; s += v[k]; }
+    }
     uint32_t tot;
     uint32_t run = block_exclusive_scan(s, &tot) + (offsets ? offsets[blockIdx.x] : 0u);
+    if (vec) {
+        uint32_t o[SCAN_ITEMS];
 #pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; k++) { size_t i = base + k; if (i < n) out[i] = run; run += v[k]; }
+        for (int k = 0; k < SCAN_ITEMS; k++) { o[k] = run; run += v[k]; }
+        reinterpret_cast<uint4 *>(out + base)[0] = make_uint4(o[0], o[1], o[2], o[3]);
+        reinterpret_cast<uint4 *>(out + base)[1] = make_uint4(o[4], o[5], o[6], o[7]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < SCAN_ITEMS; k++) { size_t i = base + k; if (i < n) out[i] = run; run += v[k]; }
+    }
     if (d_total && blockIdx.x == gridDim.x - 1 && threadIdx.x == SCAN_BLOCK - 1) *d_total = run;
 }
 
